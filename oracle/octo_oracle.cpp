@@ -1,0 +1,1500 @@
+// FP64 CPU oracle for the strong-strong PIC collision -- TEST INFRASTRUCTURE ONLY.
+//
+// A plain restatement of the reference's CPU path, used to check the CUDA
+// library: tests, the smoke check and the CPU-baseline leg of the benchmark
+// call it; the product never links it.  Every function cites the reference
+// file:line it follows (paths relative to the Octopus.jl checkout).
+//
+// Arithmetic is IEEE FP64 with no contraction (built with -ffp-contract=off),
+// evaluated in the reference's own left-to-right order, so scalar decisions
+// (grid geometry, Green-cache hits) reproduce the reference bit for bit.  The
+// FFT is this file's own (the reference calls FFTW 3.3.12), so field values
+// agree with the reference to rounding, not bitwise.
+#include "oracle.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef std::complex<double> cplx;
+
+namespace {
+
+struct OracleError : std::runtime_error {
+    int code;
+    OracleError(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+// Julia's IEEE min/max: NaN-propagating, -0.0 < +0.0 (base/math.jl semantics).
+inline double jmin(double a, double b) {
+    if (std::isnan(a) || std::isnan(b)) return a - b;
+    if (a < b) return a;
+    if (b < a) return b;
+    return std::signbit(a) ? a : b;
+}
+inline double jmax(double a, double b) {
+    if (std::isnan(a) || std::isnan(b)) return a - b;
+    if (a > b) return a;
+    if (b > a) return b;
+    return std::signbit(a) ? b : a;
+}
+inline double jclamp(double v, double lo, double hi) { return jmin(jmax(v, lo), hi); }
+inline long jclampi(long v, long lo, long hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// ---------------------------------------------------------------- counter RNG
+// counter_rng.jl:187-233, 341-349, 154-166, 410-430.
+const uint32_t PH_M0 = 0xD2511F53u, PH_M1 = 0xCD9E8D57u, PH_W0 = 0x9E3779B9u, PH_W1 = 0xBB67AE85u;
+
+inline uint64_t splitmix64(uint64_t x) {
+    uint64_t z = x + 0x9e3779b97f4a7c15ULL;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+inline void philox_block(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)PH_M0 * c[0];
+        uint64_t p1 = (uint64_t)PH_M1 * c[2];
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c[1] ^ k0, n1 = lo1, n2 = hi0 ^ c[3] ^ k1, n3 = lo0;
+        c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
+        k0 += PH_W0; k1 += PH_W1;
+    }
+}
+
+inline uint64_t counter_u64(uint64_t seed, uint64_t turn, uint64_t rng_id, uint64_t particle, uint64_t comp) {
+    uint32_t c[4] = {(uint32_t)particle, (uint32_t)(particle >> 32), (uint32_t)turn, (uint32_t)(turn >> 32)};
+    uint64_t key = splitmix64(seed) ^ splitmix64(rng_id + 0x9e3779b97f4a7c15ULL) ^
+                   splitmix64(comp + 0xbf58476d1ce4e5b9ULL);
+    philox_block(c, (uint32_t)key, (uint32_t)(key >> 32));
+    return ((uint64_t)c[0] << 32) | (uint64_t)c[1];
+}
+
+inline double uniform_open01(uint64_t v) {
+    uint64_t bits = v >> 12;
+    return ((double)bits + 0.5) * 2.220446049250313e-16;
+}
+
+inline double counter_normal(uint64_t seed, uint64_t turn, uint64_t rng_id, uint64_t particle, uint64_t comp) {
+    uint64_t pair = (comp + 1) / 2;
+    double u1 = uniform_open01(counter_u64(seed, turn, rng_id, particle, 2 * pair - 1));
+    double u2 = uniform_open01(counter_u64(seed, turn, rng_id, particle, 2 * pair));
+    double r = std::sqrt(-2.0 * std::log(u1));
+    double theta = 6.283185307179586476925286766559 * u2;
+    return (comp & 1) ? r * std::cos(theta) : r * std::sin(theta);
+}
+
+// Pairwise sum in the shape of Julia's `sum` (blocks of 1024, split in halves).
+double pairwise_sum(const double *v, int64_t n) {
+    if (n <= 1024) {
+        double s = 0.0;
+        for (int64_t i = 0; i < n; ++i) s += v[i];
+        return s;
+    }
+    int64_t h = n >> 1;
+    return pairwise_sum(v, h) + pairwise_sum(v + h, n - h);
+}
+
+// Beam.jl:148-160
+void standardize(double *v, int64_t n) {
+    double mu = pairwise_sum(v, n) / (double)n;
+    for (int64_t i = 0; i < n; ++i) v[i] -= mu;
+    std::vector<double> sq(n);
+    for (int64_t i = 0; i < n; ++i) sq[i] = v[i] * v[i];
+    double s2 = pairwise_sum(sq.data(), n) / (double)n;
+    double s = std::sqrt(std::max(s2, 0.0));
+    if (s == 0.0) {
+        for (int64_t i = 0; i < n; ++i) v[i] = 0.0;
+    } else {
+        for (int64_t i = 0; i < n; ++i) v[i] /= s;
+    }
+}
+
+// ------------------------------------------------------------------ erfinv
+// Inverse error function: Winitzki's closed-form start refined by Halley steps on
+// erf (|x| < 0.5) or erfc (|x| >= 0.5).  Replaces SpecialFunctions.erfinv
+// (SpecialMath.jl:174), which the reference calls in slicing.jl:425.
+double erfinv_impl(double x) {
+    if (std::isnan(x) || x < -1.0 || x > 1.0) return NAN;
+    if (x == 1.0) return INFINITY;
+    if (x == -1.0) return -INFINITY;
+    if (x == 0.0) return x;
+    double ax = std::fabs(x);
+    const double a = 0.147, pi = 3.141592653589793;
+    double ln = std::log1p(-ax * ax);
+    double t1 = 2.0 / (pi * a) + ln / 2.0;
+    double y = std::sqrt(std::sqrt(t1 * t1 - ln / a) - t1);
+    const double two_over_sqrtpi = 1.1283791670955126;
+    for (int it = 0; it < 4; ++it) {
+        double f = (ax < 0.5) ? (std::erf(y) - ax) : ((1.0 - ax) - std::erfc(y));
+        double fp = two_over_sqrtpi * std::exp(-y * y);
+        double step = f / fp;
+        y = y - step / (1.0 + y * step);
+    }
+    return x < 0 ? -y : y;
+}
+
+// ------------------------------------------------------------------ FFT
+// Own FFT (replaces FFTW.jl 1.10.0 / FFTW 3.3.12; call sites pic_cpu.jl:1954-1983).
+struct Fft1D {
+    int n = 0;
+    bool pow2 = false;
+    std::vector<cplx> w;      // exp(-2 pi i k / n)
+    std::vector<int> rev;
+    std::vector<cplx> tmp;
+    void init(int n_) {
+        n = n_;
+        w.resize(n);
+        for (int k = 0; k < n; ++k) {
+            double a = -2.0 * 3.141592653589793238462643 * (double)k / (double)n;
+            w[k] = cplx(std::cos(a), std::sin(a));
+        }
+        pow2 = (n & (n - 1)) == 0;
+        if (pow2) {
+            rev.resize(n);
+            int lg = 0;
+            while ((1 << lg) < n) ++lg;
+            for (int i = 0; i < n; ++i) {
+                int r = 0;
+                for (int b = 0; b < lg; ++b)
+                    if (i & (1 << b)) r |= 1 << (lg - 1 - b);
+                rev[i] = r;
+            }
+        }
+        tmp.resize(n);
+    }
+    // Recursive mixed-radix DIT for sizes 2^a 3^b 5^c (generic DFT otherwise).
+    void rec(const cplx *in, int stride, cplx *out, int m, bool inv) {
+        if (m == 1) { out[0] = in[0]; return; }
+        int r = (m % 4 == 0) ? 4 : (m % 2 == 0) ? 2 : (m % 3 == 0) ? 3 : (m % 5 == 0) ? 5 : m;
+        int q = m / r;
+        for (int p = 0; p < r; ++p) rec(in + p * stride, stride * r, out + p * q, q, inv);
+        int step = n / m;
+        cplx buf[16];
+        std::vector<cplx> big;
+        cplx *b = buf;
+        if (r > 16) { big.resize(r); b = big.data(); }
+        for (int k = 0; k < q; ++k) {
+            for (int p = 0; p < r; ++p) {
+                int e = (int)(((long)p * k * step) % n);
+                cplx tw = inv ? std::conj(w[e]) : w[e];
+                b[p] = out[p * q + k] * tw;
+            }
+            for (int mm = 0; mm < r; ++mm) {
+                cplx s = 0;
+                for (int p = 0; p < r; ++p) {
+                    int e = (int)(((long)p * mm * q * step) % n);
+                    cplx tw = inv ? std::conj(w[e]) : w[e];
+                    s += b[p] * tw;
+                }
+                out[mm * q + k] = s;
+            }
+        }
+    }
+    void run(cplx *a, bool inv) {
+        if (pow2) {
+            for (int i = 0; i < n; ++i)
+                if (i < rev[i]) std::swap(a[i], a[rev[i]]);
+            for (int len = 2; len <= n; len <<= 1) {
+                int half = len >> 1, step = n / len;
+                for (int i = 0; i < n; i += len)
+                    for (int j = 0; j < half; ++j) {
+                        cplx tw = inv ? std::conj(w[j * step]) : w[j * step];
+                        cplx u = a[i + j], v = a[i + j + half] * tw;
+                        a[i + j] = u + v;
+                        a[i + j + half] = u - v;
+                    }
+            }
+        } else {
+            std::vector<cplx> in(a, a + n);
+            rec(in.data(), 1, a, n, inv);
+        }
+    }
+};
+
+struct Fft2D {
+    int n1 = 0, n2 = 0;
+    Fft1D f1, f2;
+    std::vector<cplx> line;
+    void init(int a, int b) {
+        n1 = a; n2 = b;
+        f1.init(a); f2.init(b);
+        line.resize(b);
+    }
+    // Column-major (n1 fastest), unnormalised forward / 1/(n1 n2)-normalised inverse like FFTW's ifft.
+    void run(cplx *a, bool inv) {
+        for (int j = 0; j < n2; ++j) f1.run(a + (size_t)j * n1, inv);
+        for (int i = 0; i < n1; ++i) {
+            for (int j = 0; j < n2; ++j) line[j] = a[i + (size_t)j * n1];
+            f2.run(line.data(), inv);
+            for (int j = 0; j < n2; ++j) a[i + (size_t)j * n1] = line[j];
+        }
+        if (inv) {
+            double s = 1.0 / ((double)n1 * (double)n2);
+            for (size_t k = 0; k < (size_t)n1 * n2; ++k) a[k] *= s;
+        }
+    }
+};
+
+// ----------------------------------------------------------- PIC primitives
+// pic_cpu.jl:2182-2197
+inline void cic_weights(double u, int n, int &base, double w[2]) {
+    if (!(0.0 <= u && u <= (double)(n - 1))) { base = 1; w[0] = 0.0; w[1] = 0.0; return; }
+    base = (int)jclampi((long)std::floor(u) + 1, 1, n - 1);
+    double f = jclamp(u - (double)(base - 1), 0.0, 1.0);
+    w[0] = 1.0 - f; w[1] = f;
+}
+
+// pic_cpu.jl:2225-2252
+inline void tsc_weights(double u, int n, int &base, double w[3]) {
+    if (!(0.0 <= u && u <= (double)(n - 1))) { base = 1; w[0] = w[1] = w[2] = 0.0; return; }
+    double fl = std::floor(u);
+    long ix = (long)fl;
+    double f = u - fl;
+    long b;
+    if (f < 0.5) {
+        double t = f * f;
+        w[0] = 0.125 + 0.5 * (t - f); w[1] = 0.75 - t; w[2] = 0.125 + 0.5 * (t + f);
+        b = ix;
+    } else {
+        double fr = 1.0 - f;
+        double t = fr * fr;
+        w[0] = 0.125 + 0.5 * (t + fr); w[1] = 0.75 - t; w[2] = 0.125 + 0.5 * (t - fr);
+        b = ix + 1;
+    }
+    base = (int)jclampi(b, 1, n - 2);
+}
+
+// pic_cpu.jl:2254-2272
+inline double atan_ratio(double num, double den) {
+    if (den == 0) {
+        if (num == 0) return 0.0;
+        return std::copysign(3.141592653589793 / 2, num);
+    }
+    return std::atan(num / den);
+}
+inline double kernel_integral(double x, double y) {
+    double r2 = x * x + y * y;
+    if (r2 == 0.0) return 0.0;
+    return (std::log(r2) - 3) * x * y + atan_ratio(y, x) * x * x + atan_ratio(x, y) * y * y;
+}
+
+// pic_cpu.jl:2478-2509 (integrated / standard kernels)
+void green_table(int green_type, double fx0, double fy0, double sx0, double sy0, double hx, double hy, int nx, int ny,
+                 double *g) {
+    double half_hx = hx / 2, half_hy = hy / 2;
+    double hxihyi = -0.5 / (hx * hy);
+    for (int j = 0; j < 2 * ny; ++j)
+        for (int i = 0; i < 2 * nx; ++i) {
+            int ii = i < nx ? i : i - 2 * nx;
+            int jj = j < ny ? j : j - 2 * ny;
+            double x = fx0 - sx0 + (double)ii * hx;
+            double y = fy0 - sy0 + (double)jj * hy;
+            double val;
+            bool integrated = green_type == 0;
+            if (!integrated) {
+                double r2 = x * x + y * y;
+                if (r2 != 0.0) { g[i + (size_t)j * 2 * nx] = -0.5 * std::log(r2); continue; }
+            }
+            val = kernel_integral(x + half_hx, y + half_hy);
+            val += kernel_integral(x - half_hx, y - half_hy);
+            val -= kernel_integral(x + half_hx, y - half_hy);
+            val -= kernel_integral(x - half_hx, y + half_hy);
+            g[i + (size_t)j * 2 * nx] = hxihyi * val;
+        }
+}
+
+// pic_cpu.jl:2531-2591
+void field_from_phi(const double *phi, int nx, int ny, double hx, double hy, bool fourth, double *Ex, double *Ey) {
+    auto P = [&](int i, int j) { return phi[(i - 1) + (size_t)(j - 1) * nx]; };
+    auto EX = [&](int i, int j) -> double & { return Ex[(i - 1) + (size_t)(j - 1) * nx]; };
+    auto EY = [&](int i, int j) -> double & { return Ey[(i - 1) + (size_t)(j - 1) * nx]; };
+    double hxi = 1.0 / hx, hyi = 1.0 / hy;
+    double c4 = 1.0 / 12.0;
+    for (int i = 1; i <= nx; ++i) {
+        EY(i, 1) = hyi * (1.5 * P(i, 1) - 2 * P(i, 2) + 0.5 * P(i, 3));
+        EY(i, ny) = hyi * (-1.5 * P(i, ny) + 2 * P(i, ny - 1) - 0.5 * P(i, ny - 2));
+    }
+    if (fourth && ny >= 5) {
+        for (int i = 1; i <= nx; ++i) {
+            EY(i, 2) = 0.5 * hyi * (P(i, 1) - P(i, 3));
+            EY(i, ny - 1) = 0.5 * hyi * (P(i, ny - 2) - P(i, ny));
+        }
+        for (int j = 3; j <= ny - 2; ++j)
+            for (int i = 1; i <= nx; ++i)
+                EY(i, j) = c4 * hyi * ((P(i, j + 2) - P(i, j - 2)) + 8 * (P(i, j - 1) - P(i, j + 1)));
+    } else {
+        for (int j = 2; j <= ny - 1; ++j)
+            for (int i = 1; i <= nx; ++i) EY(i, j) = 0.5 * hyi * (P(i, j - 1) - P(i, j + 1));
+    }
+    for (int j = 1; j <= ny; ++j) {
+        EX(1, j) = hxi * (1.5 * P(1, j) - 2 * P(2, j) + 0.5 * P(3, j));
+        EX(nx, j) = hxi * (-1.5 * P(nx, j) + 2 * P(nx - 1, j) - 0.5 * P(nx - 2, j));
+        if (fourth && nx >= 5) {
+            EX(2, j) = 0.5 * hxi * (P(1, j) - P(3, j));
+            EX(nx - 1, j) = 0.5 * hxi * (P(nx - 2, j) - P(nx, j));
+            for (int i = 3; i <= nx - 2; ++i)
+                EX(i, j) = c4 * hxi * ((P(i + 2, j) - P(i - 2, j)) + 8 * (P(i - 1, j) - P(i + 1, j)));
+        } else {
+            for (int i = 2; i <= nx - 1; ++i) EX(i, j) = 0.5 * hxi * (P(i - 1, j) - P(i + 1, j));
+        }
+    }
+}
+
+// Fixed-point charge scale: every tap is rounded to a multiple of 2^-bits, with bits chosen so the
+// full source population fits a cell without overflow: bits = min(40, 62 - bitlength(nsrc)).
+inline int fixed_bits(int64_t n) {
+    int bl = 0;
+    uint64_t v = (uint64_t)(n < 1 ? 1 : n);
+    while (v) { ++bl; v >>= 1; }
+    int b = 62 - bl;
+    return b > 40 ? 40 : b;
+}
+
+struct Grid { double x0, y0, width, height; };
+struct Bounds { double xmin, xmax, ymin, ymax; };
+
+constexpr int DEPOSIT_CHUNKS = 16;           // interface.jl:663
+constexpr int64_t PARALLEL_DEPOSIT_MIN = 4096;  // interface.jl:615
+constexpr int64_t DEPOSIT_PER_CELL = 160;    // interface.jl:643
+constexpr double TEMPLATE_MARGIN_CELLS = 1.5;  // interface.jl:674
+constexpr int SLICE_FOLD_LANES = 4096;       // slicing.jl:223
+
+inline bool deposit_parallel(int64_t n, int nx, int ny) {  // interface.jl:649-651
+    return n >= PARALLEL_DEPOSIT_MIN && n >= DEPOSIT_PER_CELL * (int64_t)nx * ny;
+}
+
+// One particle's taps into a column-major grid with leading dimension ld (pic_cpu.jl:2129-2146).
+template <class Acc>
+inline void deposit_point(int method, double u, double v, int nx, int ny, Acc acc) {
+    if (method == 0) {
+        int ix, iy; double wx[2], wy[2];
+        cic_weights(u, nx, ix, wx);
+        cic_weights(v, ny, iy, wy);
+        for (int m = 0; m < 2; ++m)
+            for (int k = 0; k < 2; ++k) acc(ix + m, iy + k, wx[m] * wy[k]);
+    } else {
+        int ix, iy; double wx[3], wy[3];
+        tsc_weights(u, nx, ix, wx);
+        tsc_weights(v, ny, iy, wy);
+        for (int m = 0; m < 3; ++m)
+            for (int k = 0; k < 3; ++k) acc(ix + m, iy + k, wx[m] * wy[k]);
+    }
+}
+
+// pic_cpu.jl:2015-2146: serial below the chunk threshold, 16 fixed chunk grids above it.
+// drift=true deposits x + px*s; otherwise x (px unused).  fixed: int64 fixed-point accumulation.
+void deposit_grid(double *charge, int ld, int method, const double *x, const double *px, const double *y,
+                  const double *py, int64_t n, bool drift, double s, double x0, double y0, double hx, double hy,
+                  int nx, int ny, bool fixed, int64_t *qfix) {
+    double hxi = 1.0 / hx, hyi = 1.0 / hy;
+    auto pos = [&](int64_t i, double &u, double &v) {
+        double xd = drift ? x[i] + px[i] * s : x[i];
+        double yd = drift ? y[i] + py[i] * s : y[i];
+        u = (xd - x0) * hxi;
+        v = (yd - y0) * hyi;
+    };
+    if (fixed) {
+        int bits = fixed_bits(n);
+        double scale = std::ldexp(1.0, bits);
+        std::vector<int64_t> q((size_t)ld * (ny + 2), 0);
+        for (int64_t i = 0; i < n; ++i) {
+            double u, v;
+            pos(i, u, v);
+            deposit_point(method, u, v, nx, ny, [&](int a, int b, double w) {
+                q[(a - 1) + (size_t)(b - 1) * ld] += (int64_t)std::nearbyint(w * scale);
+            });
+        }
+        double inv = std::ldexp(1.0, -bits);
+        for (int b = 0; b < ny; ++b)
+            for (int a = 0; a < nx; ++a) {
+                int64_t val = q[a + (size_t)b * ld];
+                charge[a + (size_t)b * ld] += (double)val * inv;
+                if (qfix) qfix[a + (size_t)b * nx] = val;
+            }
+        return;
+    }
+    if (deposit_parallel(n, nx, ny)) {
+        std::vector<double> local((size_t)ld * (ny + 2));
+        for (int c = 1; c <= DEPOSIT_CHUNKS; ++c) {
+            std::fill(local.begin(), local.end(), 0.0);
+            int64_t lo = ((int64_t)(c - 1) * n) / DEPOSIT_CHUNKS, hi = ((int64_t)c * n) / DEPOSIT_CHUNKS;
+            for (int64_t i = lo; i < hi; ++i) {
+                double u, v;
+                pos(i, u, v);
+                deposit_point(method, u, v, nx, ny,
+                              [&](int a, int b, double w) { local[(a - 1) + (size_t)(b - 1) * ld] += w; });
+            }
+            for (int b = 0; b < ny; ++b)
+                for (int a = 0; a < nx; ++a) charge[a + (size_t)b * ld] += local[a + (size_t)b * ld];
+        }
+        return;
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        double u, v;
+        pos(i, u, v);
+        deposit_point(method, u, v, nx, ny,
+                      [&](int a, int b, double w) { charge[(a - 1) + (size_t)(b - 1) * ld] += w; });
+    }
+}
+
+struct Coords {
+    std::vector<double> x, px, y, py, z, pz;
+    size_t size() const { return x.size(); }
+    void resize(size_t n) { x.resize(n); px.resize(n); y.resize(n); py.resize(n); z.resize(n); pz.resize(n); }
+};
+
+struct Options {
+    oo_options o;
+    std::vector<double> pos1, pos2;
+    int lum_nx() const { return o.lum_nx > 0 ? o.lum_nx : o.nx; }
+    int lum_ny() const { return o.lum_ny > 0 ? o.lum_ny : o.ny; }
+    int lum_method() const { return o.lum_deposit_method >= 0 ? o.lum_deposit_method : o.deposit_method; }
+};
+
+// pic_cpu.jl:1646-1672
+void resolve_extent(const Options &O, double xspan, double yspan, double &w, double &h, const char *context) {
+    w = jmax(xspan, O.o.min_extent_x);
+    h = jmax(yspan, O.o.min_extent_y);
+    if (!(std::isfinite(w) && std::isfinite(h) && w > 0 && h > 0)) {
+        char buf[256];
+        snprintf(buf, sizeof buf, "%s requires finite, positive transverse extents; observed (x=%g, y=%g)", context,
+                 xspan, yspan);
+        throw OracleError(OO_ERR_EXTENT, buf);
+    }
+}
+
+// pic_cpu.jl:1877-1905
+void align_origins(int green_type, double s0, double f0, double h, double &so, double &fo) {
+    double f1 = s0 / h - std::floor(s0 / h);
+    double f2 = f0 / h - std::floor(f0 / h);
+    double t = (f2 - f1) / 2;
+    if (green_type == 1) {
+        t += t > 0 ? -0.25 : 0.25;
+    } else {
+        if (t > 0.5) t -= 0.5;
+        else if (t < -0.5) t += 0.5;
+    }
+    double shift = t * h;
+    so = s0 + shift;
+    fo = f0 - shift;
+}
+
+inline double quantize_extent(double w, double q) {  // pic_cpu.jl:1641-1644
+    if (!(q > 0 && std::isfinite(w) && w > 0)) return w;
+    return std::exp2(std::ceil(std::log2(w) / q) * q);
+}
+
+// pic_cpu.jl:1674-1718
+void interaction_grids(const Options &O, double sxmin, double sxmax, double symin, double symax, double fxmin,
+                       double fxmax, double fymin, double fymax, Grid &sg, Grid &fg) {
+    int nx = O.o.nx, ny = O.o.ny;
+    double width, height;
+    resolve_extent(O, jmax(sxmax - sxmin, fxmax - fxmin), jmax(symax - symin, fymax - fymin), width, height,
+                   "PIC interaction grid");
+    double tx = width / (double)(nx - 4);
+    double ty = height / (double)(ny - 4);
+    width += 3 * tx;
+    height += 3 * ty;
+    double q = O.o.grid_quantize;
+    if (q > 0) {
+        width = quantize_extent(width, q);
+        height = quantize_extent(height, q);
+        double hx = width / (double)(nx - 1), hy = height / (double)(ny - 1);
+        double sx0 = std::nearbyint(((sxmin + sxmax) / 2 - width / 2) / hx) * hx;
+        double sy0 = std::nearbyint(((symin + symax) / 2 - height / 2) / hy) * hy;
+        double fx0 = std::nearbyint(((fxmin + fxmax) / 2 - width / 2) / hx) * hx;
+        double fy0 = std::nearbyint(((fymin + fymax) / 2 - height / 2) / hy) * hy;
+        align_origins(O.o.green_type, sx0, fx0, hx, sx0, fx0);
+        align_origins(O.o.green_type, sy0, fy0, hy, sy0, fy0);
+        sg = {sx0, sy0, width, height};
+        fg = {fx0, fy0, width, height};
+        return;
+    }
+    double sx0 = sxmin - 1.5 * tx, sy0 = symin - 1.5 * ty;
+    double fx0 = fxmin - 1.5 * tx, fy0 = fymin - 1.5 * ty;
+    align_origins(O.o.green_type, sx0, fx0, tx, sx0, fx0);
+    align_origins(O.o.green_type, sy0, fy0, ty, sy0, fy0);
+    sg = {sx0, sy0, width, height};
+    fg = {fx0, fy0, width, height};
+}
+
+// pic_cpu.jl:1581-1593 and slicing.jl:667-668
+inline void axis_extent(int method, double &lo, double &hi, double origin, double ds, double ds2, int64_t n,
+                        double k) {
+    if (method == 0 || n < 2) return;
+    double invn = 1.0 / (double)n;
+    double mean_offset = ds * invn;
+    double m = origin + mean_offset;
+    // muladd(-a, a, b) (slicing.jl:667-668) is fused on FMA-capable hosts.
+    double var = jmax(std::fma(-mean_offset, mean_offset, ds2 * invn), 0.0);
+    double sd = std::sqrt(var);
+    double half = k * sd;
+    if (!(half > 0)) return;
+    lo = m - half;
+    hi = m + half;
+}
+
+struct FieldPlanes { std::vector<double> phi, Ex, Ey; void init(int n) { phi.assign(n, 0); Ex.assign(n, 0); Ey.assign(n, 0); } };
+
+struct Workspace {
+    int nx = 0, ny = 0;
+    std::vector<double> charge;  // (2nx)*(2ny)
+    std::vector<cplx> spectral;
+    std::vector<double> green;
+    Fft2D fft;
+    FieldPlanes left, right, mid;
+    int64_t dropped = 0;
+    std::vector<double> vx[2], vy[2];
+    std::vector<double> q1, q2;
+    void init(int nx_, int ny_) {
+        nx = nx_; ny = ny_;
+        charge.assign((size_t)4 * nx * ny, 0.0);
+        spectral.assign((size_t)4 * nx * ny, 0.0);
+        green.assign((size_t)4 * nx * ny, 0.0);
+        fft.init(2 * nx, 2 * ny);
+        left.init(nx * ny); right.init(nx * ny); mid.init(nx * ny);
+    }
+};
+
+struct GreenEntry {
+    bool valid = false;
+    Grid sg{}, fg{};
+    std::vector<cplx> gfft;
+    int64_t uses = 0, rebuilds = 0;
+};
+
+struct NodeMesh {
+    bool valid = false;
+    Grid sg{}, fg{};
+    std::vector<cplx> gfft;
+};
+
+// pic_cpu.jl:1928-1939
+void green_fft(const Options &O, Workspace &ws, const Grid &sg, const Grid &fg, std::vector<cplx> &out) {
+    int nx = O.o.nx, ny = O.o.ny;
+    double hx = sg.width / (double)(nx - 1), hy = sg.height / (double)(ny - 1);
+    green_table(O.o.green_type, fg.x0, fg.y0, sg.x0, sg.y0, hx, hy, nx, ny, ws.green.data());
+    out.resize((size_t)4 * nx * ny);
+    for (size_t k = 0; k < out.size(); ++k) out[k] = cplx(ws.green[k], 0.0);
+    ws.fft.run(out.data(), false);
+}
+
+// pic_cpu.jl:1965-1990
+void solve_drifted(const Options &O, Workspace &ws, FieldPlanes &fp, const Coords &src, double s, const Grid &sg,
+                   const std::vector<cplx> &gfft, bool drift = true) {
+    int nx = O.o.nx, ny = O.o.ny;
+    double hx = sg.width / (double)(nx - 1), hy = sg.height / (double)(ny - 1);
+    std::fill(ws.charge.begin(), ws.charge.end(), 0.0);
+    deposit_grid(ws.charge.data(), 2 * nx, O.o.deposit_method, src.x.data(), src.px.data(), src.y.data(),
+                 src.py.data(), (int64_t)src.size(), drift, s, sg.x0, sg.y0, hx, hy, nx, ny,
+                 O.o.fixed_point_deposit != 0, nullptr);
+    for (size_t k = 0; k < ws.charge.size(); ++k) ws.spectral[k] = cplx(ws.charge[k], 0.0);
+    ws.fft.run(ws.spectral.data(), false);
+    for (size_t k = 0; k < ws.spectral.size(); ++k) ws.spectral[k] *= gfft[k];
+    ws.fft.run(ws.spectral.data(), true);
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) fp.phi[i + (size_t)j * nx] = ws.spectral[i + (size_t)j * 2 * nx].real();
+    field_from_phi(fp.phi.data(), nx, ny, hx, hy, O.o.field_derivative == 4, fp.Ex.data(), fp.Ey.data());
+}
+
+// pic_cpu.jl:2596-2619 (two-node) ; the weights use the kick's deposit method
+inline void interpolate_kick(const Options &O, const Grid &g, double x, double y, const FieldPlanes &L,
+                             const FieldPlanes &R, double zL, double zR, double &Kx, double &Ky, double &Kz) {
+    int nx = O.o.nx, ny = O.o.ny;
+    double hx = g.width / (double)(nx - 1), hy = g.height / (double)(ny - 1);
+    Kx = 0; Ky = 0; Kz = 0;
+    auto body = [&](int ii, int jj, double w) {
+        size_t k = (ii - 1) + (size_t)(jj - 1) * nx;
+        Kx += w * (zL * L.Ex[k] + zR * R.Ex[k]);
+        Ky += w * (zL * L.Ey[k] + zR * R.Ey[k]);
+        Kz += w * (L.phi[k] - R.phi[k]);
+    };
+    deposit_point(O.o.deposit_method, (x - g.x0) / hx, (y - g.y0) / hy, nx, ny, body);
+}
+
+// pic_cpu.jl:2648-2680 (three-node)
+inline void interpolate_kick_quadratic(const Options &O, const Grid &g, double x, double y, const FieldPlanes &L,
+                                       const FieldPlanes &M, const FieldPlanes &R, double t, double &Kx,
+                                       double &Ky, double &Kz) {
+    int nx = O.o.nx, ny = O.o.ny;
+    double hx = g.width / (double)(nx - 1), hy = g.height / (double)(ny - 1);
+    double t2 = t * t;
+    double aL = 2.0 * t2 - 3.0 * t + 1.0, aM = 4.0 * t - 4.0 * t2, aR = 2.0 * t2 - t;
+    double bL = 3.0 - 4.0 * t, bM = 8.0 * t - 4.0, bR = 1.0 - 4.0 * t;
+    Kx = 0; Ky = 0; Kz = 0;
+    auto body = [&](int ii, int jj, double w) {
+        size_t k = (ii - 1) + (size_t)(jj - 1) * nx;
+        Kx += w * (aL * L.Ex[k] + aM * M.Ex[k] + aR * R.Ex[k]);
+        Ky += w * (aL * L.Ey[k] + aM * M.Ey[k] + aR * R.Ey[k]);
+        Kz += w * (bL * L.phi[k] + bM * M.phi[k] + bR * R.phi[k]);
+    };
+    deposit_point(O.o.deposit_method, (x - g.x0) / hx, (y - g.y0) / hy, nx, ny, body);
+}
+
+inline void slice_interp_params(double lb, double rb, double &hzi, double &zbias) {  // pic_cpu.jl:1540-1548
+    double denom = rb - lb;
+    if (!std::isfinite(denom) || denom == 0.0) { hzi = 0.0; zbias = 0.5; return; }
+    hzi = 1.0 / denom;
+    zbias = rb * hzi;
+}
+
+struct SliceParam { double weight, lb, center, rb; };
+
+struct Slices {
+    std::vector<double> center, weight, boundary;
+    std::vector<std::vector<int64_t>> indices;  // 0-based particle indices, ascending
+};
+
+// slicing.jl:226-257
+double lane_sum_all(const double *z, int64_t n, double mu, bool square) {
+    std::vector<double> acc(SLICE_FOLD_LANES, 0.0);
+    for (int64_t i = 0; i < n; ++i) {
+        double v = square ? (z[i] - mu) * (z[i] - mu) : z[i];
+        acc[i % SLICE_FOLD_LANES] += v;
+    }
+    double s = 0.0;
+    for (int t = 0; t < SLICE_FOLD_LANES; ++t) s += acc[t];
+    return s;
+}
+double lane_indexed_sum(const double *z, const std::vector<int64_t> &idx) {
+    std::vector<double> acc(SLICE_FOLD_LANES, 0.0);
+    for (size_t k = 0; k < idx.size(); ++k) acc[k % SLICE_FOLD_LANES] += z[idx[k]];
+    double s = 0.0;
+    for (int t = 0; t < SLICE_FOLD_LANES; ++t) s += acc[t];
+    return s;
+}
+
+// slicing.jl:51-75, 405-460, 523-559 and the :specified method slicing.jl:393-403
+Slices make_slices(int method, int ns, int center_position, const std::vector<double> &positions, const double *z,
+                   int64_t n) {
+    if (ns <= 0) throw OracleError(OO_ERR_ARG, "nslices must be positive");
+    if (n <= 0) throw OracleError(OO_ERR_ARG, "longitudinal slicing requires at least one particle");
+    double zmin = INFINITY, zmax = -INFINITY;
+    for (int64_t i = 0; i < n; ++i) { zmin = jmin(zmin, z[i]); zmax = jmax(zmax, z[i]); }
+    double mu = lane_sum_all(z, n, 0.0, false) / (double)n;
+    double s2 = lane_sum_all(z, n, mu, true);
+    double sigma = std::sqrt(jmax(s2 / (double)n, 0.0));
+    std::vector<double> b(ns + 1);
+    if (method == 0) {
+        if (sigma == 0.0) {
+            std::fill(b.begin(), b.end(), mu);
+        } else {
+            b[0] = zmin; b[ns] = zmax;
+            for (int s = 1; s <= ns - 1; ++s) {
+                double q = std::sqrt(2.0) * erfinv_impl((double)(2 * s) / (double)ns - 1.0);
+                b[s] = jclamp(mu + sigma * q, b[0], b[ns]);
+            }
+        }
+    } else if (method == 1) {
+        std::vector<double> internal;
+        for (double p : positions) internal.push_back(mu + p * sigma);
+        std::stable_sort(internal.begin(), internal.end());
+        b.assign(internal.size() + 2, 0.0);
+        b[0] = zmin; b[b.size() - 1] = zmax;
+        for (size_t i = 0; i < internal.size(); ++i) b[i + 1] = jclamp(internal[i], b[0], b[b.size() - 1]);
+        ns = (int)b.size() - 1;
+    } else {
+        throw OracleError(OO_ERR_UNSUPPORTED, "unsupported slicing method");
+    }
+    for (double v : b)
+        if (!std::isfinite(v)) throw OracleError(OO_ERR_NONFINITE, "non-finite beam coordinate (longitudinal slicing)");
+    Slices S;
+    S.boundary = b;
+    S.indices.assign(ns, {});
+    if (b[0] == b[ns]) {
+        for (int64_t i = 0; i < n; ++i) S.indices[0].push_back(i);
+    } else {
+        for (int64_t i = 0; i < n; ++i) {
+            // searchsortedlast(b, z) clamped to [1, ns]
+            int k = (int)(std::upper_bound(b.begin(), b.end(), z[i]) - b.begin());  // count of b <= z
+            int s = (int)jclampi(k, 1, ns);
+            S.indices[s - 1].push_back(i);
+        }
+    }
+    S.center.resize(ns);
+    S.weight.resize(ns);
+    for (int s = 0; s < ns; ++s) {
+        const auto &idx = S.indices[s];
+        S.weight[s] = (double)idx.size() / (double)n;
+        if (center_position == 0)
+            S.center[s] = idx.empty() ? (b[s] + b[s + 1]) / 2 : lane_indexed_sum(z, idx) / (double)idx.size();
+        else
+            S.center[s] = (b[s] + b[s + 1]) / 2;
+    }
+    return S;
+}
+
+struct OrderEntry { double t; int i, j; };
+
+// slicing.jl:561-568 (stable sort by collision time)
+std::vector<OrderEntry> collision_order(const std::vector<double> &c1, const std::vector<double> &c2) {
+    std::vector<OrderEntry> o;
+    for (size_t i = 0; i < c1.size(); ++i)
+        for (size_t j = 0; j < c2.size(); ++j) o.push_back({-(c1[i] + c2[j]) / 2, (int)i + 1, (int)j + 1});
+    std::stable_sort(o.begin(), o.end(), [](const OrderEntry &a, const OrderEntry &b) { return a.t < b.t; });
+    return o;
+}
+
+// slicing.jl:601-647
+std::vector<std::vector<OrderEntry>> pair_batches(const std::vector<double> &c1, const std::vector<double> &c2) {
+    auto pairs = collision_order(c1, c2);
+    std::vector<std::vector<OrderEntry>> batches;
+    int ns1 = (int)c1.size(), ns2 = (int)c2.size();
+    std::vector<std::vector<int>> by_i(ns1 + 1), by_j(ns2 + 1);
+    for (size_t k = 0; k < pairs.size(); ++k) {
+        by_i[pairs[k].i].push_back((int)k);
+        by_j[pairs[k].j].push_back((int)k);
+    }
+    std::vector<size_t> next_i(ns1 + 1, 0), next_j(ns2 + 1, 0);
+    std::vector<char> done(pairs.size(), 0);
+    size_t remaining = pairs.size();
+    while (remaining > 0) {
+        std::vector<OrderEntry> cur;
+        std::vector<char> used_i(ns1 + 1, 0), used_j(ns2 + 1, 0);
+        for (size_t k = 0; k < pairs.size(); ++k) {
+            if (done[k]) continue;
+            const auto &p = pairs[k];
+            if (used_i[p.i] || used_j[p.j]) continue;
+            bool ri = next_i[p.i] < by_i[p.i].size() && by_i[p.i][next_i[p.i]] == (int)k;
+            bool rj = next_j[p.j] < by_j[p.j].size() && by_j[p.j][next_j[p.j]] == (int)k;
+            if (ri && rj) {
+                cur.push_back(p);
+                used_i[p.i] = 1; used_j[p.j] = 1; done[k] = 1;
+                next_i[p.i]++; next_j[p.j]++;
+                --remaining;
+            }
+        }
+        if (cur.empty()) throw OracleError(OO_ERR_ARG, "internal collision scheduler error");
+        batches.push_back(cur);
+    }
+    return batches;
+}
+
+struct Ctx {
+    Options O;
+    int ns1 = 0, ns2 = 0;
+    std::vector<GreenEntry> cache;  // [(dir-1)][i-1][j-1]
+    int64_t hits = 0, misses = 0, rebuilds = 0;
+    int64_t dropped = 0;
+    std::vector<int> trace_i, trace_j;
+    std::vector<double> trace_lum;
+    std::string err;
+    GreenEntry &entry(int i, int j, int dir) { return cache[((size_t)(dir - 1) * ns1 + (i - 1)) * ns2 + (j - 1)]; }
+};
+
+std::string pair_ctx(int i, int j, int dir) {
+    char b[96];
+    snprintf(b, sizeof b, "slice pair (%d, %d), direction %d", i, j, dir);
+    return b;
+}
+
+[[noreturn]] void nonfinite(const char *role, const Coords &c, const std::string &where) {
+    int64_t first = -1;
+    for (size_t k = 0; k < c.size(); ++k)
+        if (!std::isfinite(c.x[k]) || !std::isfinite(c.px[k]) || !std::isfinite(c.y[k]) || !std::isfinite(c.py[k]) ||
+            !std::isfinite(c.z[k])) { first = (int64_t)k + 1; break; }
+    char b[256];
+    snprintf(b, sizeof b, "non-finite %s coordinate at slice particle %lld (%s)", role, (long long)first,
+             where.c_str());
+    throw OracleError(OO_ERR_NONFINITE, b);
+}
+
+// pic_cpu.jl:1780-1808
+bool grid_size_usable(const Grid &c, const Grid &r, double mr) {
+    return c.width >= r.width && c.height >= r.height && r.width >= mr * c.width && r.height >= mr * c.height;
+}
+bool grid_covers(const Options &O, const Grid &g, const Bounds &b) {
+    double hx = g.width / (double)(O.o.nx - 1), hy = g.height / (double)(O.o.ny - 1);
+    double m = TEMPLATE_MARGIN_CELLS;
+    return g.x0 + m * hx <= b.xmin && g.x0 + g.width - m * hx >= b.xmax && g.y0 + m * hy <= b.ymin &&
+           g.y0 + g.height - m * hy >= b.ymax;
+}
+Grid expand_grid(const Grid &g, double factor) {  // pic_cpu.jl:1810-1821
+    if (factor <= 1.0) return g;
+    double nw = g.width * factor, nh = g.height * factor;
+    return {g.x0 - (nw - g.width) / 2, g.y0 - (nh - g.height) / 2, nw, nh};
+}
+
+// pic_cpu.jl:1729-1778 ; returns (sg, fg, green)
+const std::vector<cplx> &slice_pair_green(Ctx &C, Workspace &ws, int i, int j, int dir, Grid &sg, Grid &fg,
+                                          const Bounds &sb, const Bounds &fb, std::vector<cplx> &own,
+                                          int64_t counters[3]) {
+    const Options &O = C.O;
+    if (O.o.green_cache == 1) {
+        GreenEntry &e = C.entry(i, j, dir);
+        bool usable = e.valid && grid_size_usable(e.sg, sg, O.o.green_min_ratio) &&
+                      grid_size_usable(e.fg, fg, O.o.green_min_ratio) && grid_covers(O, e.sg, sb) &&
+                      grid_covers(O, e.fg, fb);
+        if (usable) {
+            counters[0]++;
+            e.uses++;
+            sg = e.sg; fg = e.fg;
+            return e.gfft;
+        }
+        Grid es = expand_grid(sg, 1.0 + O.o.green_growth);
+        Grid ef = expand_grid(fg, 1.0 + O.o.green_growth);
+        if (O.o.green_type != 0) {  // pic_cpu.jl:1853-1862
+            double hx = es.width / (double)(O.o.nx - 1), hy = es.height / (double)(O.o.ny - 1);
+            double sx0, fx0, sy0, fy0;
+            align_origins(O.o.green_type, es.x0, ef.x0, hx, sx0, fx0);
+            align_origins(O.o.green_type, es.y0, ef.y0, hy, sy0, fy0);
+            es.x0 = sx0; ef.x0 = fx0; es.y0 = sy0; ef.y0 = fy0;
+        }
+        green_fft(O, ws, es, ef, e.gfft);
+        if (!e.valid) { counters[1]++; e.rebuilds = 0; }
+        else { counters[2]++; e.rebuilds++; }
+        e.valid = true; e.uses = 1; e.sg = es; e.fg = ef;
+        sg = es; fg = ef;
+        return e.gfft;
+    }
+    green_fft(O, ws, sg, fg, own);
+    return own;
+}
+
+int64_t count_outside(const std::vector<double> &xs, const std::vector<double> &ys, double xlo, double xhi,
+                      double ylo, double yhi) {
+    int64_t c = 0;
+    for (size_t i = 0; i < xs.size(); ++i) {
+        double x = xs[i], y = ys[i];
+        if (!(std::isfinite(x) && xlo <= x && x <= xhi && std::isfinite(y) && ylo <= y && y <= yhi)) ++c;
+    }
+    return c;
+}
+int64_t count_outside_drifted(const Coords &s, double sL, double sR, double xlo, double xhi, double ylo,
+                              double yhi) {
+    int64_t c = 0;
+    for (size_t i = 0; i < s.size(); ++i) {
+        double xl = s.x[i] + s.px[i] * sL, yl = s.y[i] + s.py[i] * sL;
+        double xr = s.x[i] + s.px[i] * sR, yr = s.y[i] + s.py[i] * sR;
+        if (!(std::isfinite(xl) && xlo <= xl && xl <= xhi && std::isfinite(yl) && ylo <= yl && yl <= yhi &&
+              std::isfinite(xr) && xlo <= xr && xr <= xhi && std::isfinite(yr) && ylo <= yr && yr <= yhi))
+            ++c;
+    }
+    return c;
+}
+
+void virtual_positions(const Coords &src, double sM, std::vector<double> &vx, std::vector<double> &vy) {
+    vx.resize(src.size());
+    vy.resize(src.size());
+    for (size_t i = 0; i < src.size(); ++i) {
+        vx[i] = src.x[i] + src.px[i] * sM;
+        vy[i] = src.y[i] + src.py[i] * sM;
+    }
+}
+
+// pic_cpu.jl:954-1144
+void interaction(Ctx &C, Workspace &ws, const Coords &source, const SliceParam &ps, Coords &field,
+                 const SliceParam &pf, double kbb, int i, int j, int dir, int vslot, int64_t counters[3]) {
+    const Options &O = C.O;
+    const int nsource = (int)source.size(), nfield = (int)field.size();
+    double sL = 0.5 * (ps.center - pf.lb);
+    double sR = 0.5 * (ps.center - pf.rb);
+    double sxl = source.x[0] + source.px[0] * sL, syl = source.y[0] + source.py[0] * sL;
+    double sxr = source.x[0] + source.px[0] * sR, syr = source.y[0] + source.py[0] * sR;
+    double sxmin = jmin(sxl, sxr), sxmax = jmax(sxl, sxr), symin = jmin(syl, syr), symax = jmax(syl, syr);
+    int ge = O.o.grid_extent;
+    double sx0 = sxl, sy0 = syl;
+    double sxs = 0, sxs2 = 0, sys = 0, sys2 = 0;
+    for (int k = 0; k < nsource; ++k) {
+        double xl = source.x[k] + source.px[k] * sL, yl = source.y[k] + source.py[k] * sL;
+        double xr = source.x[k] + source.px[k] * sR, yr = source.y[k] + source.py[k] * sR;
+        sxmin = jmin(jmin(sxmin, xl), xr); sxmax = jmax(jmax(sxmax, xl), xr);
+        symin = jmin(jmin(symin, yl), yr); symax = jmax(jmax(symax, yl), yr);
+        if (ge != 0) {
+            double dxl = xl - sx0, dxr = xr - sx0, dyl = yl - sy0, dyr = yr - sy0;
+            sxs += dxl + dxr; sxs2 += dxl * dxl + dxr * dxr;
+            sys += dyl + dyr; sys2 += dyl * dyl + dyr * dyr;
+        }
+    }
+    double kext = O.o.grid_extent_sigma;
+    axis_extent(ge, sxmin, sxmax, sx0, sxs, sxs2, 2 * (int64_t)nsource, kext);
+    axis_extent(ge, symin, symax, sy0, sys, sys2, 2 * (int64_t)nsource, kext);
+    if (!(std::isfinite(sxmin) && std::isfinite(sxmax) && std::isfinite(symin) && std::isfinite(symax)))
+        nonfinite("source", source, pair_ctx(i, j, dir));
+
+    double fxmin = field.x[0] + 0.5 * (field.z[0] - ps.center) * field.px[0];
+    double fxmax = fxmin;
+    double fymin = field.y[0] + 0.5 * (field.z[0] - ps.center) * field.py[0];
+    double fymax = fymin;
+    double fx0 = fxmin, fy0 = fymin;
+    double fxs = 0, fxs2 = 0, fys = 0, fys2 = 0;
+    for (int k = 0; k < nfield; ++k) {
+        double s = 0.5 * (field.z[k] - ps.center);
+        field.x[k] += s * field.px[k];
+        field.y[k] += s * field.py[k];
+        if (O.o.longitudinal_kick) field.pz[k] -= 0.25 * (field.px[k] * field.px[k] + field.py[k] * field.py[k]);
+        fxmin = jmin(fxmin, field.x[k]); fxmax = jmax(fxmax, field.x[k]);
+        fymin = jmin(fymin, field.y[k]); fymax = jmax(fymax, field.y[k]);
+        if (ge != 0) {
+            double dx = field.x[k] - fx0, dy = field.y[k] - fy0;
+            fxs += dx; fxs2 += dx * dx; fys += dy; fys2 += dy * dy;
+        }
+    }
+    axis_extent(ge, fxmin, fxmax, fx0, fxs, fxs2, nfield, kext);
+    axis_extent(ge, fymin, fymax, fy0, fys, fys2, nfield, kext);
+    if (!(std::isfinite(fxmin) && std::isfinite(fxmax) && std::isfinite(fymin) && std::isfinite(fymax)))
+        nonfinite("field", field, pair_ctx(i, j, dir));
+
+    Grid sg, fg;
+    interaction_grids(O, sxmin, sxmax, symin, symax, fxmin, fxmax, fymin, fymax, sg, fg);
+    Bounds sb{sxmin, sxmax, symin, symax}, fb{fxmin, fxmax, fymin, fymax};
+    std::vector<cplx> own;
+    const std::vector<cplx> &gfft = slice_pair_green(C, ws, i, j, dir, sg, fg, sb, fb, own, counters);
+    if (ge != 0) {
+        ws.dropped += count_outside(field.x, field.y, fg.x0, fg.x0 + fg.width, fg.y0, fg.y0 + fg.height);
+        ws.dropped += count_outside_drifted(source, sL, sR, sg.x0, sg.x0 + sg.width, sg.y0, sg.y0 + sg.height);
+    }
+    solve_drifted(O, ws, ws.left, source, sL, sg, gfft);
+    solve_drifted(O, ws, ws.right, source, sR, sg, gfft);
+    double ks = 2.0 * kbb;
+    double hzi, zbias;
+    slice_interp_params(pf.lb, pf.rb, hzi, zbias);
+    bool lk = O.o.longitudinal_kick != 0;
+    if (O.o.slice_interpolation == 1) {
+        double smid = 0.5 * (sL + sR);
+        solve_drifted(O, ws, ws.mid, source, smid, sg, gfft);
+        for (int k = 0; k < nfield; ++k) {
+            double zL = jclamp(-field.z[k] * hzi + zbias, 0.0, 1.0);
+            double Kx, Ky, Kz;
+            interpolate_kick_quadratic(O, fg, field.x[k], field.y[k], ws.left, ws.mid, ws.right, 1.0 - zL, Kx, Ky,
+                                       Kz);
+            field.px[k] += ks * Kx;
+            field.py[k] += ks * Ky;
+            if (lk) field.pz[k] += ks * Kz * hzi;
+            double s = 0.5 * (ps.center - field.z[k]);
+            field.x[k] += s * field.px[k];
+            field.y[k] += s * field.py[k];
+            if (lk) field.pz[k] += 0.25 * (field.px[k] * field.px[k] + field.py[k] * field.py[k]);
+        }
+    } else {
+        for (int k = 0; k < nfield; ++k) {
+            double zL = jclamp(-field.z[k] * hzi + zbias, 0.0, 1.0);
+            double zR = 1.0 - zL;
+            double Kx, Ky, Kz;
+            interpolate_kick(O, fg, field.x[k], field.y[k], ws.left, ws.right, zL, zR, Kx, Ky, Kz);
+            field.px[k] += ks * Kx;
+            field.py[k] += ks * Ky;
+            if (lk) field.pz[k] += ks * Kz * hzi;
+            double s = 0.5 * (ps.center - field.z[k]);
+            field.x[k] += s * field.px[k];
+            field.y[k] += s * field.py[k];
+            if (lk) field.pz[k] += 0.25 * (field.px[k] * field.px[k] + field.py[k] * field.py[k]);
+        }
+    }
+    double sM = 0.5 * (ps.center - pf.center);
+    virtual_positions(source, sM, ws.vx[vslot], ws.vy[vslot]);
+}
+
+// pic_cpu.jl:1448-1538
+void interaction_node(Ctx &C, Workspace &ws, const Coords &source, const SliceParam &ps, Coords &field,
+                      const SliceParam &pf, double kbb, const NodeMesh &gL, const NodeMesh &gR, int vslot) {
+    const Options &O = C.O;
+    bool lk = O.o.longitudinal_kick != 0;
+    double sL = 0.5 * (ps.center - pf.lb);
+    double sR = 0.5 * (ps.center - pf.rb);
+    int nfield = (int)field.size();
+    for (int k = 0; k < nfield; ++k) {
+        double s = 0.5 * (field.z[k] - ps.center);
+        field.x[k] += s * field.px[k];
+        field.y[k] += s * field.py[k];
+        if (lk) field.pz[k] -= 0.25 * (field.px[k] * field.px[k] + field.py[k] * field.py[k]);
+    }
+    ws.dropped += count_outside_drifted(source, sL, sL, gL.sg.x0, gL.sg.x0 + gL.sg.width, gL.sg.y0,
+                                        gL.sg.y0 + gL.sg.height);
+    ws.dropped += count_outside_drifted(source, sR, sR, gR.sg.x0, gR.sg.x0 + gR.sg.width, gR.sg.y0,
+                                        gR.sg.y0 + gR.sg.height);
+    ws.dropped += count_outside(field.x, field.y, gL.fg.x0, gL.fg.x0 + gL.fg.width, gL.fg.y0, gL.fg.y0 + gL.fg.height);
+    solve_drifted(O, ws, ws.left, source, sL, gL.sg, gL.gfft);
+    solve_drifted(O, ws, ws.right, source, sR, gR.sg, gR.gfft);
+    if (lk) solve_drifted(O, ws, ws.mid, source, sR, gL.sg, gL.gfft);
+    double ks = 2.0 * kbb;
+    double hzi, zbias;
+    slice_interp_params(pf.lb, pf.rb, hzi, zbias);
+    for (int k = 0; k < nfield; ++k) {
+        double zL = jclamp(-field.z[k] * hzi + zbias, 0.0, 1.0);
+        double zR = 1.0 - zL;
+        double x = field.x[k], y = field.y[k];
+        double KxL, KyL, KzL, KxR, KyR, KzR;
+        interpolate_kick(O, gL.fg, x, y, ws.left, ws.left, 1.0, 0.0, KxL, KyL, KzL);
+        interpolate_kick(O, gR.fg, x, y, ws.right, ws.right, 1.0, 0.0, KxR, KyR, KzR);
+        field.px[k] += ks * (zL * KxL + zR * KxR);
+        field.py[k] += ks * (zL * KyL + zR * KyR);
+        if (lk) {
+            double a, b, Kz;
+            // phiZ paired with the L transverse planes (pic_cpu.jl:1522-1523)
+            interpolate_kick(O, gL.fg, x, y, ws.left, ws.mid, 1.0, 0.0, a, b, Kz);
+            field.pz[k] += ks * Kz * hzi;
+        }
+        double s = 0.5 * (ps.center - field.z[k]);
+        field.x[k] += s * field.px[k];
+        field.y[k] += s * field.py[k];
+        if (lk) field.pz[k] += 0.25 * (field.px[k] * field.px[k] + field.py[k] * field.py[k]);
+    }
+    double sM = 0.5 * (ps.center - pf.center);
+    virtual_positions(source, sM, ws.vx[vslot], ws.vy[vslot]);
+}
+
+// pic_cpu.jl:1317-1382 : all node meshes of one (source slice, direction)
+void build_node_meshes(Ctx &C, Workspace &ws, const Coords &src, double center, const double *fb[6],
+                       const Slices &fs, std::vector<NodeMesh> &out) {
+    const Options &O = C.O;
+    int nb = (int)fs.boundary.size(), ns = nb - 1;
+    double c = center;
+    std::vector<double> drifts(nb);
+    for (int b = 0; b < nb; ++b) drifts[b] = 0.5 * (c - fs.boundary[b]);
+    std::vector<double> sxlo(nb, INFINITY), sxhi(nb, -INFINITY), sylo(nb, INFINITY), syhi(nb, -INFINITY);
+    for (size_t k = 0; k < src.size(); ++k) {
+        double x = src.x[k], px = src.px[k], y = src.y[k], py = src.py[k];
+        for (int b = 0; b < nb; ++b) {
+            double d = drifts[b];
+            double xv = x + px * d, yv = y + py * d;
+            sxlo[b] = jmin(sxlo[b], xv); sxhi[b] = jmax(sxhi[b], xv);
+            sylo[b] = jmin(sylo[b], yv); syhi[b] = jmax(syhi[b], yv);
+        }
+    }
+    std::vector<double> fxlo(ns, INFINITY), fxhi(ns, -INFINITY), fylo(ns, INFINITY), fyhi(ns, -INFINITY);
+    for (int sl = 0; sl < ns; ++sl)
+        for (int64_t i : fs.indices[sl]) {
+            double sh = 0.5 * (fb[4][i] - c);
+            double xv = fb[0][i] + sh * fb[1][i], yv = fb[2][i] + sh * fb[3][i];
+            fxlo[sl] = jmin(fxlo[sl], xv); fxhi[sl] = jmax(fxhi[sl], xv);
+            fylo[sl] = jmin(fylo[sl], yv); fyhi[sl] = jmax(fyhi[sl], yv);
+        }
+    for (int b = 0; b < nb; ++b)
+        if (std::isnan(sxlo[b]) || std::isnan(sxhi[b]) || std::isnan(sylo[b]) || std::isnan(syhi[b]))
+            throw OracleError(OO_ERR_NONFINITE, "non-finite source coordinate (node-mesh build)");
+    for (int b = 0; b < ns; ++b)
+        if (std::isnan(fxlo[b]) || std::isnan(fxhi[b]) || std::isnan(fylo[b]) || std::isnan(fyhi[b]))
+            throw OracleError(OO_ERR_NONFINITE, "non-finite field coordinate (node-mesh build)");
+    out.assign(nb, NodeMesh());
+    for (int b = 1; b <= nb; ++b) {
+        int bn = std::min(b + 1, nb);
+        double sxmin = jmin(sxlo[b - 1], sxlo[bn - 1]), sxmax = jmax(sxhi[b - 1], sxhi[bn - 1]);
+        double symin = jmin(sylo[b - 1], sylo[bn - 1]), symax = jmax(syhi[b - 1], syhi[bn - 1]);
+        double fxmin = INFINITY, fxmax = -INFINITY, fymin = INFINITY, fymax = -INFINITY;
+        for (int adj = b - 1; adj <= b; ++adj) {
+            if (!(1 <= adj && adj <= ns)) continue;
+            if (!std::isfinite(fxlo[adj - 1])) continue;
+            fxmin = jmin(fxmin, fxlo[adj - 1]); fxmax = jmax(fxmax, fxhi[adj - 1]);
+            fymin = jmin(fymin, fylo[adj - 1]); fymax = jmax(fymax, fyhi[adj - 1]);
+        }
+        if (!std::isfinite(fxmin)) continue;
+        NodeMesh &m = out[b - 1];
+        interaction_grids(O, sxmin, sxmax, symin, symax, fxmin, fxmax, fymin, fymax, m.sg, m.fg);
+        green_fft(O, ws, m.sg, m.fg, m.gfft);
+        m.valid = true;
+    }
+}
+
+// pic_cpu.jl:2700-2736
+double luminosity(const Options &O, const std::vector<double> &x1, const std::vector<double> &y1,
+                  const std::vector<double> &x2, const std::vector<double> &y2, double klum, Workspace &ws) {
+    int nx = O.lum_nx(), ny = O.lum_ny();
+    double xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
+    double a = INFINITY, b = -INFINITY, c = INFINITY, d = -INFINITY;
+    for (double v : x1) { a = jmin(a, v); b = jmax(b, v); }
+    for (double v : y1) { c = jmin(c, v); d = jmax(d, v); }
+    double a2 = INFINITY, b2 = -INFINITY, c2 = INFINITY, d2 = -INFINITY;
+    for (double v : x2) { a2 = jmin(a2, v); b2 = jmax(b2, v); }
+    for (double v : y2) { c2 = jmin(c2, v); d2 = jmax(d2, v); }
+    xmin = jmin(a, a2); xmax = jmax(b, b2); ymin = jmin(c, c2); ymax = jmax(d, d2);
+    double width, height;
+    resolve_extent(O, xmax - xmin, ymax - ymin, width, height, "PIC luminosity grid");
+    double tx = width / ((double)nx - 1.1);
+    double ty = height / ((double)ny - 1.1);
+    width += 0.1 * tx;
+    height += 0.1 * ty;
+    xmin -= 0.05 * tx;
+    ymin -= 0.05 * ty;
+    double hx = width / (double)(nx - 1), hy = height / (double)(ny - 1);
+    double hxi = 1.0 / hx, hyi = 1.0 / hy;
+    int ld = nx + 1;
+    ws.q1.assign((size_t)(nx + 1) * (ny + 1), 0.0);
+    ws.q2.assign((size_t)(nx + 1) * (ny + 1), 0.0);
+    int method = O.lum_method();
+    bool fixed = O.o.fixed_point_deposit != 0;
+    deposit_grid(ws.q1.data(), ld, method, x1.data(), nullptr, y1.data(), nullptr, (int64_t)x1.size(), false, 0.0,
+                 xmin, ymin, hx, hy, nx + 1, ny + 1, fixed, nullptr);
+    deposit_grid(ws.q2.data(), ld, method, x2.data(), nullptr, y2.data(), nullptr, (int64_t)x2.size(), false, 0.0,
+                 xmin, ymin, hx, hy, nx + 1, ny + 1, fixed, nullptr);
+    double lum = 0.0;
+    for (int j = 0; j < ny + 1; ++j)
+        for (int i = 0; i < nx + 1; ++i) lum += ws.q1[i + (size_t)j * ld] * ws.q2[i + (size_t)j * ld];
+    return lum * klum * hxi * hyi;
+}
+
+void gather(const double *b[6], const std::vector<int64_t> &idx, Coords &c) {
+    c.resize(idx.size());
+    for (size_t k = 0; k < idx.size(); ++k) {
+        int64_t i = idx[k];
+        c.x[k] = b[0][i]; c.px[k] = b[1][i]; c.y[k] = b[2][i];
+        c.py[k] = b[3][i]; c.z[k] = b[4][i]; c.pz[k] = b[5][i];
+    }
+}
+
+void validate(const Options &O) {
+    const oo_options &o = O.o;
+    if (o.nx < 5 || o.ny < 5) throw OracleError(OO_ERR_ARG, "PICPoissonSolver grid must be at least (5, 5)");
+    if (o.deposit_method < 0 || o.deposit_method > 1) throw OracleError(OO_ERR_ARG, "deposit_method");
+    if (o.green_type < 0 || o.green_type > 1) throw OracleError(OO_ERR_UNSUPPORTED, "green_type");
+    if (o.interaction_grid != 0 && o.interaction_grid != 2) throw OracleError(OO_ERR_UNSUPPORTED, "interaction_grid");
+    if (o.interaction_grid != 0 && o.grid_extent != 0)
+        throw OracleError(OO_ERR_UNSUPPORTED, "grid_extent != :extrema with interaction_grid != :slice_pair");
+    if (o.interaction_grid == 2 && o.slice_interpolation != 0)
+        throw OracleError(OO_ERR_UNSUPPORTED, "slice_interpolation = :quadratic with interaction_grid = :node");
+}
+
+int nslices_of(const oo_options &o, int which) {
+    int method = which == 1 ? o.slicing_method1 : o.slicing_method2;
+    int ns = which == 1 ? o.nslices1 : o.nslices2;
+    return method == 1 ? ns : ns;  // :specified uses nslices-1 positions (interface.jl:828-829)
+}
+
+// pic_cpu.jl:82-275
+double collide(Ctx &C, double *b1[6], int64_t n1, double *b2[6], int64_t n2, const oo_beam_params &p1,
+               const oo_beam_params &p2, bool compute_lum) {
+    Options &O = C.O;
+    validate(O);
+    Slices s1 = make_slices(O.o.slicing_method1, O.o.nslices1, O.o.center_position1, O.pos1, b1[4], n1);
+    Slices s2 = make_slices(O.o.slicing_method2, O.o.nslices2, O.o.center_position2, O.pos2, b2[4], n2);
+    int ns1 = (int)s1.center.size(), ns2 = (int)s2.center.size();
+    if (C.cache.empty() || ns1 != C.ns1 || ns2 != C.ns2) {
+        C.ns1 = ns1; C.ns2 = ns2;
+        C.cache.assign((size_t)2 * ns1 * ns2, GreenEntry());
+    }
+    // slicing.jl:77-91 and pic_cpu.jl:821-829
+    double kbb1p = O.o.has_kbb1 ? O.o.kbb1 : p1.charge * p2.charge * p1.r0 * p2.npart * p1.mc2 / p1.E0;
+    double kbb2p = O.o.has_kbb2 ? O.o.kbb2 : p1.charge * p2.charge * p2.r0 * p1.npart * p2.mc2 / p2.E0;
+    if (!O.o.has_kbb1 && !(std::isfinite(p1.E0) && p1.E0 != 0))
+        throw OracleError(OO_ERR_ARG, "beam1 E0 must be finite and nonzero when kbb1 is not specified");
+    if (!O.o.has_kbb2 && !(std::isfinite(p2.E0) && p2.E0 != 0))
+        throw OracleError(OO_ERR_ARG, "beam2 E0 must be finite and nonzero when kbb2 is not specified");
+    double kbb1 = kbb1p / (double)n2;
+    double kbb2 = kbb2p / (double)n1;
+    double klum = O.o.has_lum_scale ? O.o.lum_scale : p1.npart * p2.npart / (double)(n1 * n2);
+
+    int nx = O.o.nx, ny = O.o.ny;
+    bool node = O.o.interaction_grid == 2;
+    int nthreads = O.o.nthreads > 0 ? O.o.nthreads : 1;
+    std::vector<Workspace> wss(nthreads);
+    for (auto &w : wss) w.init(nx, ny);
+
+    std::vector<Coords> state1(ns1), state2(ns2), scratch2(ns2);
+    const double *cb1[6] = {b1[0], b1[1], b1[2], b1[3], b1[4], b1[5]};
+    const double *cb2[6] = {b2[0], b2[1], b2[2], b2[3], b2[4], b2[5]};
+    for (int s = 0; s < ns1; ++s) gather(cb1, s1.indices[s], state1[s]);
+    for (int s = 0; s < ns2; ++s) { gather(cb2, s2.indices[s], state2[s]); scratch2[s] = state2[s]; }
+
+    // pic_cpu.jl:1404-1419 : node meshes from the turn-start state
+    std::vector<std::vector<NodeMesh>> node1(ns1), node2(ns2);
+    std::string first_err;
+    int first_code = 0;
+    if (node) {
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic)
+        for (int t = 0; t < ns1 + ns2; ++t) {
+            try {
+#ifdef _OPENMP
+                Workspace &w = wss[omp_get_thread_num()];
+#else
+                Workspace &w = wss[0];
+#endif
+                if (t < ns1) {
+                    if (!s1.indices[t].empty()) build_node_meshes(C, w, state1[t], s1.center[t], cb2, s2, node1[t]);
+                } else {
+                    int s = t - ns1;
+                    if (!s2.indices[s].empty()) build_node_meshes(C, w, state2[s], s2.center[s], cb1, s1, node2[s]);
+                }
+            } catch (OracleError &e) {
+#pragma omp critical
+                if (!first_code) { first_code = e.code; first_err = e.what(); }
+            }
+        }
+        if (first_code) throw OracleError(first_code, first_err);
+    }
+
+    auto order = collision_order(s1.center, s2.center);
+    size_t npairs = order.size();
+    std::vector<int> pos_of((size_t)ns1 * ns2);
+    for (size_t p = 0; p < npairs; ++p) pos_of[(size_t)(order[p].i - 1) * ns2 + (order[p].j - 1)] = (int)p;
+    std::vector<double> lum_parts(npairs, 0.0);
+    std::vector<char> ran(npairs, 0);
+    auto batches = pair_batches(s1.center, s2.center);
+    std::vector<std::array<int64_t, 3>> counters(npairs, {0, 0, 0});
+
+    for (auto &batch : batches) {
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic)
+        for (int q = 0; q < (int)batch.size(); ++q) {
+#ifdef _OPENMP
+            Workspace &ws = wss[omp_get_thread_num()];
+#else
+            Workspace &ws = wss[0];
+#endif
+            int i = batch[q].i, j = batch[q].j;
+            int p = pos_of[(size_t)(i - 1) * ns2 + (j - 1)];
+            try {
+                if (s1.indices[i - 1].empty() || s2.indices[j - 1].empty()) continue;
+                SliceParam pa1{s1.weight[i - 1], s1.boundary[i - 1], s1.center[i - 1], s1.boundary[i]};
+                SliceParam pa2{s2.weight[j - 1], s2.boundary[j - 1], s2.center[j - 1], s2.boundary[j]};
+                Coords &coord1 = state1[i - 1];
+                Coords &coord2 = state2[j - 1];
+                Coords &field2 = scratch2[j - 1];
+                field2 = coord2;
+                if (node) {
+                    auto &nc1 = node1[i - 1];
+                    auto &nc2 = node2[j - 1];
+                    if (nc1.empty() || nc2.empty()) throw OracleError(OO_ERR_ARG, "node mesh cache missing");
+                    const NodeMesh &gL1 = nc1[j - 1], &gR1 = nc1[j], &gL2 = nc2[i - 1], &gR2 = nc2[i];
+                    if (!gL1.valid || !gR1.valid || !gL2.valid || !gR2.valid) continue;
+                    interaction_node(C, ws, coord1, pa1, field2, pa2, kbb2, gL1, gR1, 0);
+                    interaction_node(C, ws, coord2, pa2, coord1, pa1, kbb1, gL2, gR2, 1);
+                } else {
+                    interaction(C, ws, coord1, pa1, field2, pa2, kbb2, i, j, 1, 0, counters[p].data());
+                    interaction(C, ws, coord2, pa2, coord1, pa1, kbb1, i, j, 2, 1, counters[p].data());
+                }
+                std::swap(state2[j - 1], scratch2[j - 1]);
+                if (compute_lum) lum_parts[p] = luminosity(O, ws.vx[0], ws.vy[0], ws.vx[1], ws.vy[1], klum, ws);
+                ran[p] = 1;
+            } catch (OracleError &e) {
+#pragma omp critical
+                if (!first_code) { first_code = e.code; first_err = e.what(); }
+            }
+        }
+        if (first_code) throw OracleError(first_code, first_err);
+    }
+    for (auto &c : counters) { C.hits += c[0]; C.misses += c[1]; C.rebuilds += c[2]; }
+
+    // scatter back (pic_cpu.jl:255-256)
+    for (int s = 0; s < ns1; ++s)
+        for (size_t k = 0; k < s1.indices[s].size(); ++k) {
+            int64_t i = s1.indices[s][k];
+            const Coords &c = state1[s];
+            b1[0][i] = c.x[k]; b1[1][i] = c.px[k]; b1[2][i] = c.y[k]; b1[3][i] = c.py[k]; b1[4][i] = c.z[k]; b1[5][i] = c.pz[k];
+        }
+    for (int s = 0; s < ns2; ++s)
+        for (size_t k = 0; k < s2.indices[s].size(); ++k) {
+            int64_t i = s2.indices[s][k];
+            const Coords &c = state2[s];
+            b2[0][i] = c.x[k]; b2[1][i] = c.px[k]; b2[2][i] = c.y[k]; b2[3][i] = c.py[k]; b2[4][i] = c.z[k]; b2[5][i] = c.pz[k];
+        }
+    C.dropped = 0;
+    for (auto &w : wss) C.dropped += w.dropped;
+    C.trace_i.clear(); C.trace_j.clear(); C.trace_lum.clear();
+    double lum = NAN;
+    if (compute_lum) {
+        lum = 0.0;
+        for (size_t p = 0; p < npairs; ++p) {
+            if (!ran[p]) continue;
+            lum += lum_parts[p];
+            C.trace_i.push_back(order[p].i);
+            C.trace_j.push_back(order[p].j);
+            C.trace_lum.push_back(lum_parts[p]);
+        }
+    }
+    return lum;
+}
+
+Options make_options(const oo_options *o) {
+    Options O;
+    O.o = *o;
+    if (o->slicing_method1 == 1 && o->positions1) O.pos1.assign(o->positions1, o->positions1 + (o->nslices1 - 1));
+    if (o->slicing_method2 == 1 && o->positions2) O.pos2.assign(o->positions2, o->positions2 + (o->nslices2 - 1));
+    O.o.positions1 = nullptr;
+    O.o.positions2 = nullptr;
+    return O;
+}
+
+}  // namespace
+
+extern "C" {
+
+void oo_philox4x32_block(const uint32_t c[4], const uint32_t k[2], uint32_t out[4]) {
+    uint32_t w[4] = {c[0], c[1], c[2], c[3]};
+    philox_block(w, k[0], k[1]);
+    for (int i = 0; i < 4; ++i) out[i] = w[i];
+}
+uint64_t oo_counter_uint64(uint64_t seed, uint64_t turn, uint64_t rng_id, uint64_t particle, uint64_t component) {
+    return counter_u64(seed, turn, rng_id, particle, component);
+}
+double oo_normal(uint64_t seed, uint64_t turn, uint64_t rng_id, uint64_t particle, uint64_t component) {
+    return counter_normal(seed, turn, rng_id, particle, component);
+}
+
+// Beam.jl:475-515, 127-181, 545-553 (counter-RNG Gaussian beam, sigma/Twiss normalisation)
+void oo_beam_gaussian(int64_t n, uint64_t seed, uint64_t rng_id, const double beta[3], const double alpha[3],
+                      const double sigma[3], double cutoff, double *x, double *px, double *y, double *py, double *z,
+                      double *pz) {
+    double *c[6] = {x, px, y, py, z, pz};
+    for (int d = 0; d < 6; ++d) {
+        double *v = c[d];
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; ++i) {
+            double g = counter_normal(seed, 0, rng_id, (uint64_t)(i + 1), (uint64_t)(d + 1));
+            v[i] = std::isfinite(cutoff) ? jclamp(g, -cutoff, cutoff) : g;
+        }
+        standardize(v, n);
+    }
+    for (int a = 0; a < 3; ++a) {
+        double *q = c[2 * a], *p = c[2 * a + 1];
+        double f = sigma[a] / beta[a];
+        for (int64_t i = 0; i < n; ++i) p[i] = f * (p[i] - alpha[a] * q[i]);
+        for (int64_t i = 0; i < n; ++i) q[i] *= sigma[a];
+    }
+}
+
+double oo_erfinv(double x) { return erfinv_impl(x); }
+double oo_kernel_integral(double x, double y) { return kernel_integral(x, y); }
+double oo_atan_ratio(double num, double den) { return atan_ratio(num, den); }
+void oo_cic_weights(double u, int32_t n, int32_t *base, double w[2]) { int b; cic_weights(u, n, b, w); *base = b; }
+void oo_tsc_weights(double u, int32_t n, int32_t *base, double w[3]) { int b; tsc_weights(u, n, b, w); *base = b; }
+void oo_green_table(int32_t green_type, double fx0, double fy0, double sx0, double sy0, double hx, double hy,
+                    int32_t nx, int32_t ny, double *out) {
+    green_table(green_type, fx0, fy0, sx0, sy0, hx, hy, nx, ny, out);
+}
+void oo_fft2(double *re, double *im, int32_t n1, int32_t n2, int32_t inverse) {
+    Fft2D f;
+    f.init(n1, n2);
+    std::vector<cplx> a((size_t)n1 * n2);
+    for (size_t k = 0; k < a.size(); ++k) a[k] = cplx(re[k], im[k]);
+    f.run(a.data(), inverse != 0);
+    for (size_t k = 0; k < a.size(); ++k) { re[k] = a[k].real(); im[k] = a[k].imag(); }
+}
+void oo_field(const double *phi, int32_t nx, int32_t ny, double hx, double hy, int32_t fourth, double *Ex,
+              double *Ey) {
+    field_from_phi(phi, nx, ny, hx, hy, fourth != 0, Ex, Ey);
+}
+int32_t oo_fixed_scale_bits(int64_t nsrc) { return fixed_bits(nsrc); }
+void oo_deposit_drifted(int32_t method, const double *x, const double *px, const double *y, const double *py,
+                        int64_t n, double s, double x0, double y0, double hx, double hy, int32_t nx, int32_t ny,
+                        int32_t fixed, double *charge, int64_t *qfix) {
+    deposit_grid(charge, 2 * nx, method, x, px, y, py, n, true, s, x0, y0, hx, hy, nx, ny, fixed != 0, qfix);
+}
+void oo_solve_field(const oo_options *opt, const double *x, const double *y, int64_t n, double sx0, double sy0,
+                    double sw, double sh, double fx0, double fy0, double *phi, double *Ex, double *Ey) {
+    Options O = make_options(opt);
+    Workspace ws;
+    ws.init(O.o.nx, O.o.ny);
+    Grid sg{sx0, sy0, sw, sh}, fg{fx0, fy0, sw, sh};
+    std::vector<cplx> g;
+    green_fft(O, ws, sg, fg, g);
+    Coords src;
+    src.x.assign(x, x + n); src.y.assign(y, y + n);
+    src.px.assign(n, 0.0); src.py.assign(n, 0.0); src.z.assign(n, 0.0); src.pz.assign(n, 0.0);
+    solve_drifted(O, ws, ws.left, src, 0.0, sg, g, false);
+    size_t m = (size_t)O.o.nx * O.o.ny;
+    std::copy(ws.left.phi.begin(), ws.left.phi.begin() + m, phi);
+    std::copy(ws.left.Ex.begin(), ws.left.Ex.begin() + m, Ex);
+    std::copy(ws.left.Ey.begin(), ws.left.Ey.begin() + m, Ey);
+}
+void oo_interpolation_grids(const oo_options *opt, const double b[8], double out[8]) {
+    Options O = make_options(opt);
+    Grid sg, fg;
+    interaction_grids(O, b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], sg, fg);
+    out[0] = sg.x0; out[1] = sg.y0; out[2] = sg.width; out[3] = sg.height;
+    out[4] = fg.x0; out[5] = fg.y0; out[6] = fg.width; out[7] = fg.height;
+}
+
+int oo_slices(int32_t method, int32_t ns, int32_t center_position, const double *positions, const double *z,
+              int64_t n, double *boundary, double *center, double *weight, int64_t *count, int64_t *order) {
+    try {
+        std::vector<double> pos;
+        if (method == 1 && positions) pos.assign(positions, positions + (ns - 1));
+        Slices S = make_slices(method, ns, center_position, pos, z, n);
+        int m = (int)S.center.size();
+        for (int s = 0; s <= m; ++s) boundary[s] = S.boundary[s];
+        int64_t k = 0;
+        for (int s = 0; s < m; ++s) {
+            center[s] = S.center[s];
+            weight[s] = S.weight[s];
+            count[s] = (int64_t)S.indices[s].size();
+            for (int64_t i : S.indices[s]) order[k++] = i;
+        }
+        return OO_OK;
+    } catch (OracleError &e) {
+        return e.code;
+    }
+}
+
+int32_t oo_pair_batches(const double *c1, int32_t ns1, const double *c2, int32_t ns2, int32_t *batch_of,
+                        int32_t *pi, int32_t *pj, int32_t *order_i, int32_t *order_j) {
+    std::vector<double> a(c1, c1 + ns1), b(c2, c2 + ns2);
+    auto order = collision_order(a, b);
+    for (size_t k = 0; k < order.size(); ++k) { order_i[k] = order[k].i; order_j[k] = order[k].j; }
+    auto batches = pair_batches(a, b);
+    int k = 0;
+    for (size_t bi = 0; bi < batches.size(); ++bi)
+        for (auto &p : batches[bi]) { batch_of[k] = (int)bi; pi[k] = p.i; pj[k] = p.j; ++k; }
+    return (int32_t)batches.size();
+}
+
+void *oo_create(const oo_options *opt) {
+    Ctx *c = new Ctx();
+    c->O = make_options(opt);
+    return c;
+}
+void oo_destroy(void *ctx) { delete (Ctx *)ctx; }
+int oo_collide(void *ctx, double *b1[6], int64_t n1, double *b2[6], int64_t n2, const oo_beam_params *p1,
+               const oo_beam_params *p2, int32_t compute_luminosity, double *lum) {
+    Ctx &C = *(Ctx *)ctx;
+    try {
+        double l = collide(C, b1, n1, b2, n2, *p1, *p2, compute_luminosity != 0);
+        if (lum) *lum = l;
+        C.err.clear();
+        return OO_OK;
+    } catch (OracleError &e) {
+        C.err = e.what();
+        return e.code;
+    }
+}
+void oo_cache_stats(void *ctx, int64_t out[3]) {
+    Ctx &C = *(Ctx *)ctx;
+    out[0] = C.hits; out[1] = C.misses; out[2] = C.rebuilds;
+}
+int64_t oo_dropped(void *ctx) { return ((Ctx *)ctx)->dropped; }
+int64_t oo_pair_trace(void *ctx, int32_t *pi, int32_t *pj, double *lum, int64_t cap) {
+    Ctx &C = *(Ctx *)ctx;
+    int64_t n = (int64_t)C.trace_lum.size();
+    for (int64_t k = 0; k < n && k < cap; ++k) { pi[k] = C.trace_i[k]; pj[k] = C.trace_j[k]; lum[k] = C.trace_lum[k]; }
+    return n;
+}
+const char *oo_last_error(void *ctx) { return ((Ctx *)ctx)->err.c_str(); }
+
+// linear6d.jl:110-121
+void oo_linear6d(const double m[36], double *x, double *px, double *y, double *py, double *z, double *pz, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) {
+        double a = x[i], b = px[i], c = y[i], d = py[i], e = z[i], f = pz[i];
+        x[i] = m[0] * a + m[1] * b + m[2] * c + m[3] * d + m[4] * e + m[5] * f;
+        px[i] = m[6] * a + m[7] * b + m[8] * c + m[9] * d + m[10] * e + m[11] * f;
+        y[i] = m[12] * a + m[13] * b + m[14] * c + m[15] * d + m[16] * e + m[17] * f;
+        py[i] = m[18] * a + m[19] * b + m[20] * c + m[21] * d + m[22] * e + m[23] * f;
+        z[i] = m[24] * a + m[25] * b + m[26] * c + m[27] * d + m[28] * e + m[29] * f;
+        pz[i] = m[30] * a + m[31] * b + m[32] * c + m[33] * d + m[34] * e + m[35] * f;
+    }
+}
+// linear6d.jl:233-280 with equal Twiss at both ends and no coupling/dispersion: per-plane rotation.
+void oo_linear6d_matrix(const double beta[3], const double alpha[3], const double tune[3], double m[36]) {
+    for (int k = 0; k < 36; ++k) m[k] = 0.0;
+    for (int i = 0; i < 3; ++i) {
+        double mu = 2.0 * 3.141592653589793 * tune[i];
+        double s = std::sin(mu), c = std::cos(mu);
+        double b1 = beta[i], b2 = beta[i], a1 = alpha[i], a2 = alpha[i];
+        int r = 2 * i;
+        m[r * 6 + r] = std::sqrt(b2 / b1) * (c + a1 * s);
+        m[r * 6 + r + 1] = std::sqrt(b2 * b1) * s;
+        m[(r + 1) * 6 + r] = (-(1.0 + a1 * a2) * s + (a1 - a2) * c) / std::sqrt(b1 * b2);
+        m[(r + 1) * 6 + r + 1] = std::sqrt(b1 / b2) * (c - a2 * s);
+    }
+}
+
+}  // extern "C"

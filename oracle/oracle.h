@@ -1,0 +1,114 @@
+/*
+ * FP64 CPU oracle for the strong-strong PIC collision -- TEST INFRASTRUCTURE.
+ *
+ * This library is a CPU restatement of the reference's CPU PIC path
+ * (Octopus.jl `src/tasks/strongstrong/pic_cpu.jl`, `slicing.jl`,
+ * `src/beam/Beam.jl`, `src/math/counter_rng.jl`, `src/elements/linear6d.jl`).
+ * It exists only to check the CUDA path: tests, the smoke check and the CPU
+ * baseline leg of the benchmark load it; the product library never does.
+ *
+ * Parity pins: Philox4x32-10 Random123 known-answer vectors
+ * (counter_rng.jl:250-258), the integrated Green kernel's on-axis zeros
+ * (test/runtests.jl:2576-2591), the quadratic-interpolation identities
+ * (test/runtests.jl:9741-9776), the 4th-vs-2nd order Bassetti-Erskine field
+ * test (test/runtests.jl:9628-9693) and the production golden luminosity
+ * 1.0254361754701657e+30 (docs/history/cpu_benchmark_history.tsv:2).
+ */
+#ifndef OCTO_ORACLE_H
+#define OCTO_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { OO_OK = 0, OO_ERR_NONFINITE = 1, OO_ERR_UNSUPPORTED = 2, OO_ERR_EXTENT = 3, OO_ERR_ARG = 4 };
+
+/* POD twin of PICPoissonSolver's fields (interface.jl:1350-1382). */
+typedef struct {
+    int32_t nx, ny;                    /* grid */
+    int32_t deposit_method;            /* 0 = :CIC, 1 = :TSC */
+    int32_t lum_deposit_method;        /* -1 inherit, 0 CIC, 1 TSC */
+    int32_t lum_nx, lum_ny;            /* 0 = inherit grid */
+    int32_t green_type;                /* 0 = :integrated, 1 = :standard */
+    int32_t green_cache;               /* 0 = :none, 1 = :slice_pair */
+    int32_t field_derivative;          /* 2 = :second, 4 = :fourth */
+    int32_t slice_interpolation;       /* 0 = :linear, 1 = :quadratic */
+    int32_t interaction_grid;          /* 0 = :slice_pair, 2 = :node */
+    int32_t grid_extent;               /* 0 = :extrema, 1 = :sigma */
+    double grid_extent_sigma;
+    double min_extent_x, min_extent_y; /* min_transverse_extent */
+    double grid_quantize;
+    double green_min_ratio;            /* slice_pair_green_min_ratio */
+    double green_growth;               /* slice_pair_green_growth */
+    int32_t longitudinal_kick;
+    int32_t slicing_method1, slicing_method2;  /* 0 = :normal_quantile, 1 = :specified */
+    int32_t nslices1, nslices2;
+    int32_t center_position1, center_position2; /* 0 = :centroid, 1 = :midpoint */
+    const double *positions1, *positions2;      /* :specified internal positions (nslices-1) */
+    int32_t has_kbb1, has_kbb2, has_lum_scale;
+    double kbb1, kbb2, lum_scale;
+    int32_t fixed_point_deposit;       /* 1: int64 fixed-point charge grid (see oo_fixed_scale_bits) */
+    int32_t nthreads;                  /* OpenMP threads for the pair batches (results do not depend on it) */
+} oo_options;
+
+typedef struct { double charge, mc2, E0, r0, npart; } oo_beam_params;
+
+/* Counter RNG and beam construction (counter_rng.jl, Beam.jl). */
+void oo_philox4x32_block(const uint32_t c[4], const uint32_t k[2], uint32_t out[4]);
+uint64_t oo_counter_uint64(uint64_t seed, uint64_t turn, uint64_t rng_id, uint64_t particle, uint64_t component);
+double oo_normal(uint64_t seed, uint64_t turn, uint64_t rng_id, uint64_t particle, uint64_t component);
+void oo_beam_gaussian(int64_t n, uint64_t seed, uint64_t rng_id, const double beta[3], const double alpha[3],
+                      const double sigma[3], double cutoff, double *x, double *px, double *y, double *py,
+                      double *z, double *pz);
+double oo_erfinv(double x);
+
+/* Building blocks exposed for the analytic pins. */
+double oo_kernel_integral(double x, double y);
+double oo_atan_ratio(double num, double den);
+void oo_cic_weights(double u, int32_t n, int32_t *base, double w[2]);
+void oo_tsc_weights(double u, int32_t n, int32_t *base, double w[3]);
+void oo_green_table(int32_t green_type, double fx0, double fy0, double sx0, double sy0, double hx, double hy,
+                    int32_t nx, int32_t ny, double *out /* (2nx)*(2ny) column-major */);
+void oo_fft2(double *re, double *im, int32_t n1, int32_t n2, int32_t inverse);
+void oo_field(const double *phi, int32_t nx, int32_t ny, double hx, double hy, int32_t fourth, double *Ex, double *Ey);
+/* Fixed-point scale (bits) used for a plane with nsrc source particles. */
+int32_t oo_fixed_scale_bits(int64_t nsrc);
+/* Drifted deposit into a (2nx)*(2ny) column-major grid (only the nx*ny quadrant is written).
+   fixed != 0 accumulates round(w * 2^bits) in int64 and writes the integer grid to qfix as well. */
+void oo_deposit_drifted(int32_t method, const double *x, const double *px, const double *y, const double *py,
+                        int64_t n, double s, double x0, double y0, double hx, double hy, int32_t nx, int32_t ny,
+                        int32_t fixed, double *charge, int64_t *qfix);
+/* One field solve (deposit -> FFT -> x G^ -> iFFT -> E) on grid (x0,y0,w,h) against the Green
+   function of (source grid, field grid). Outputs nx*ny column-major phi, Ex, Ey. */
+void oo_solve_field(const oo_options *opt, const double *x, const double *y, int64_t n, double sx0, double sy0,
+                    double sw, double sh, double fx0, double fy0, double *phi, double *Ex, double *Ey);
+void oo_interpolation_grids(const oo_options *opt, const double b[8], double out[8]);
+
+/* Slicing (slicing.jl:51-75, :normal_quantile / :specified). Outputs: boundary[ns+1], center[ns],
+   weight[ns], count[ns], order[n] (slice-major member lists, ascending particle index). */
+int oo_slices(int32_t method, int32_t ns, int32_t center_position, const double *positions, const double *z,
+              int64_t n, double *boundary, double *center, double *weight, int64_t *count, int64_t *order);
+/* Collision order + wavefront batches (slicing.jl:561-647). pairs[k] = (batch, i, j) 0-based in order
+   of batches; returns the number of batches. */
+int32_t oo_pair_batches(const double *c1, int32_t ns1, const double *c2, int32_t ns2, int32_t *batch_of,
+                        int32_t *pi, int32_t *pj, int32_t *order_i, int32_t *order_j);
+
+/* A collide context keeps the slice-pair Green cache across calls, as task.runtime_cache does. */
+void *oo_create(const oo_options *opt);
+void oo_destroy(void *ctx);
+int oo_collide(void *ctx, double *b1[6], int64_t n1, double *b2[6], int64_t n2, const oo_beam_params *p1,
+               const oo_beam_params *p2, int32_t compute_luminosity, double *luminosity);
+void oo_cache_stats(void *ctx, int64_t out[3]);
+int64_t oo_dropped(void *ctx);
+/* Per-pair luminosity of the last collide in collision order (i, j 1-based); returns count. */
+int64_t oo_pair_trace(void *ctx, int32_t *pi, int32_t *pj, double *lum, int64_t cap);
+const char *oo_last_error(void *ctx);
+/* Linear 6D one-turn map (linear6d.jl:110-121) with a row-major 6x6 matrix. */
+void oo_linear6d(const double m[36], double *x, double *px, double *y, double *py, double *z, double *pz, int64_t n);
+void oo_linear6d_matrix(const double beta[3], const double alpha[3], const double tune[3], double m[36]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

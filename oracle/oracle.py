@@ -1,0 +1,316 @@
+"""ctypes binding of the FP64 CPU oracle (oracle/octo_oracle.cpp) -- TEST INFRASTRUCTURE.
+
+Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` use
+this module, as the checker.  The product library never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "build", "liboctooracle.so")
+
+OK, ERR_NONFINITE, ERR_UNSUPPORTED, ERR_EXTENT, ERR_ARG = 0, 1, 2, 3, 4
+
+# Physical constants (src/constants/Constants.jl:11-20).
+RE = 2.8179403205e-15
+EMASS_EV = 0.51099895069e6
+ME0 = EMASS_EV
+PMASS_EV = 938.27208943e6
+
+
+def build() -> str:
+    src = os.path.join(HERE, "octo_oracle.cpp")
+    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+class OOOptions(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32),
+        ("deposit_method", C.c_int32), ("lum_deposit_method", C.c_int32),
+        ("lum_nx", C.c_int32), ("lum_ny", C.c_int32),
+        ("green_type", C.c_int32), ("green_cache", C.c_int32),
+        ("field_derivative", C.c_int32), ("slice_interpolation", C.c_int32),
+        ("interaction_grid", C.c_int32), ("grid_extent", C.c_int32),
+        ("grid_extent_sigma", C.c_double),
+        ("min_extent_x", C.c_double), ("min_extent_y", C.c_double),
+        ("grid_quantize", C.c_double),
+        ("green_min_ratio", C.c_double), ("green_growth", C.c_double),
+        ("longitudinal_kick", C.c_int32),
+        ("slicing_method1", C.c_int32), ("slicing_method2", C.c_int32),
+        ("nslices1", C.c_int32), ("nslices2", C.c_int32),
+        ("center_position1", C.c_int32), ("center_position2", C.c_int32),
+        ("positions1", C.POINTER(C.c_double)), ("positions2", C.POINTER(C.c_double)),
+        ("has_kbb1", C.c_int32), ("has_kbb2", C.c_int32), ("has_lum_scale", C.c_int32),
+        ("kbb1", C.c_double), ("kbb2", C.c_double), ("lum_scale", C.c_double),
+        ("fixed_point_deposit", C.c_int32),
+        ("nthreads", C.c_int32),
+    ]
+
+
+class OOBeamParams(C.Structure):
+    _fields_ = [("charge", C.c_double), ("mc2", C.c_double), ("E0", C.c_double),
+                ("r0", C.c_double), ("npart", C.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(build())
+        d, i32, i64, u64, vp = C.c_double, C.c_int32, C.c_int64, C.c_uint64, C.c_void_p
+        P = C.POINTER
+        L = _lib
+        L.oo_philox4x32_block.argtypes = [P(C.c_uint32), P(C.c_uint32), P(C.c_uint32)]
+        L.oo_counter_uint64.restype = u64
+        L.oo_counter_uint64.argtypes = [u64] * 5
+        L.oo_normal.restype = d
+        L.oo_normal.argtypes = [u64] * 5
+        L.oo_beam_gaussian.argtypes = [i64, u64, u64, P(d), P(d), P(d), d] + [P(d)] * 6
+        L.oo_erfinv.restype = d
+        L.oo_erfinv.argtypes = [d]
+        L.oo_kernel_integral.restype = d
+        L.oo_kernel_integral.argtypes = [d, d]
+        L.oo_atan_ratio.restype = d
+        L.oo_atan_ratio.argtypes = [d, d]
+        L.oo_cic_weights.argtypes = [d, i32, P(i32), P(d)]
+        L.oo_tsc_weights.argtypes = [d, i32, P(i32), P(d)]
+        L.oo_green_table.argtypes = [i32, d, d, d, d, d, d, i32, i32, P(d)]
+        L.oo_fft2.argtypes = [P(d), P(d), i32, i32, i32]
+        L.oo_field.argtypes = [P(d), i32, i32, d, d, i32, P(d), P(d)]
+        L.oo_fixed_scale_bits.restype = i32
+        L.oo_fixed_scale_bits.argtypes = [i64]
+        L.oo_deposit_drifted.argtypes = [i32, P(d), P(d), P(d), P(d), i64, d, d, d, d, d, i32, i32, i32,
+                                         P(d), P(i64)]
+        L.oo_solve_field.argtypes = [P(OOOptions), P(d), P(d), i64, d, d, d, d, d, d, P(d), P(d), P(d)]
+        L.oo_interpolation_grids.argtypes = [P(OOOptions), P(d), P(d)]
+        L.oo_slices.restype = C.c_int
+        L.oo_slices.argtypes = [i32, i32, i32, P(d), P(d), i64, P(d), P(d), P(d), P(i64), P(i64)]
+        L.oo_pair_batches.restype = i32
+        L.oo_pair_batches.argtypes = [P(d), i32, P(d), i32, P(i32), P(i32), P(i32), P(i32), P(i32)]
+        L.oo_create.restype = vp
+        L.oo_create.argtypes = [P(OOOptions)]
+        L.oo_destroy.argtypes = [vp]
+        L.oo_collide.restype = C.c_int
+        L.oo_collide.argtypes = [vp, P(P(d)), i64, P(P(d)), i64, P(OOBeamParams), P(OOBeamParams), i32, P(d)]
+        L.oo_cache_stats.argtypes = [vp, P(i64)]
+        L.oo_dropped.restype = i64
+        L.oo_dropped.argtypes = [vp]
+        L.oo_pair_trace.restype = i64
+        L.oo_pair_trace.argtypes = [vp, P(i32), P(i32), P(d), i64]
+        L.oo_last_error.restype = C.c_char_p
+        L.oo_last_error.argtypes = [vp]
+        L.oo_linear6d.argtypes = [P(d)] + [P(d)] * 6 + [i64]
+        L.oo_linear6d_matrix.argtypes = [P(d), P(d), P(d), P(d)]
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+_SYM = {
+    "deposit_method": {"CIC": 0, "TSC": 1},
+    "green_type": {"integrated": 0, "standard": 1},
+    "green_cache": {"none": 0, "slice_pair": 1},
+    "field_derivative": {"second": 2, "fourth": 4},
+    "slice_interpolation": {"linear": 0, "quadratic": 1},
+    "interaction_grid": {"slice_pair": 0, "node": 2},
+    "grid_extent": {"extrema": 0, "sigma": 1},
+    "method": {"normal_quantile": 0, "gaussian": 0, "Gaussian": 0, "specified": 1},
+    "center_position": {"centroid": 0, "midpoint": 1},
+}
+
+
+@dataclass
+class OracleOptions:
+    """Keyword twin of PICPoissonSolver (interface.jl:1384-1411) for the oracle."""
+    grid: tuple = (128, 128)
+    deposit_method: str = "CIC"
+    luminosity_deposit_method: Optional[str] = None
+    luminosity_grid: Optional[tuple] = None
+    green_type: str = "integrated"
+    green_cache: str = "slice_pair"
+    field_derivative: str = "second"
+    slice_interpolation: str = "linear"
+    interaction_grid: str = "slice_pair"
+    grid_extent: str = "extrema"
+    grid_extent_sigma: float = 6.0
+    min_transverse_extent: tuple = (0.0, 0.0)
+    grid_quantize: float = 0.0
+    slice_pair_green_min_ratio: float = 0.5
+    slice_pair_green_growth: float = 0.25
+    longitudinal_kick: bool = True
+    nslices1: int = 1
+    nslices2: int = 1
+    method1: str = "normal_quantile"
+    method2: str = "normal_quantile"
+    center_position1: str = "centroid"
+    center_position2: str = "centroid"
+    positions1: Sequence[float] = field(default_factory=list)
+    positions2: Sequence[float] = field(default_factory=list)
+    kbb1: Optional[float] = None
+    kbb2: Optional[float] = None
+    luminosity_scale: Optional[float] = None
+    fixed_point_deposit: bool = False
+    nthreads: int = 1
+
+    def to_c(self) -> OOOptions:
+        o = OOOptions()
+        o.nx, o.ny = int(self.grid[0]), int(self.grid[1])
+        o.deposit_method = _SYM["deposit_method"][self.deposit_method]
+        o.lum_deposit_method = -1 if self.luminosity_deposit_method is None else \
+            _SYM["deposit_method"][self.luminosity_deposit_method]
+        lg = self.luminosity_grid or (0, 0)
+        o.lum_nx, o.lum_ny = int(lg[0]), int(lg[1])
+        o.green_type = _SYM["green_type"][self.green_type]
+        o.green_cache = _SYM["green_cache"][self.green_cache]
+        o.field_derivative = _SYM["field_derivative"][self.field_derivative]
+        o.slice_interpolation = _SYM["slice_interpolation"][self.slice_interpolation]
+        o.interaction_grid = _SYM["interaction_grid"][self.interaction_grid]
+        o.grid_extent = _SYM["grid_extent"][self.grid_extent]
+        o.grid_extent_sigma = self.grid_extent_sigma
+        o.min_extent_x, o.min_extent_y = map(float, self.min_transverse_extent)
+        o.grid_quantize = self.grid_quantize
+        o.green_min_ratio = self.slice_pair_green_min_ratio
+        o.green_growth = self.slice_pair_green_growth
+        o.longitudinal_kick = int(bool(self.longitudinal_kick))
+        o.slicing_method1 = _SYM["method"][self.method1]
+        o.slicing_method2 = _SYM["method"][self.method2]
+        o.nslices1, o.nslices2 = int(self.nslices1), int(self.nslices2)
+        o.center_position1 = _SYM["center_position"][self.center_position1]
+        o.center_position2 = _SYM["center_position"][self.center_position2]
+        self._p1 = np.ascontiguousarray(self.positions1, dtype=np.float64)
+        self._p2 = np.ascontiguousarray(self.positions2, dtype=np.float64)
+        o.positions1 = _dp(self._p1) if self._p1.size else None
+        o.positions2 = _dp(self._p2) if self._p2.size else None
+        o.has_kbb1 = int(self.kbb1 is not None)
+        o.has_kbb2 = int(self.kbb2 is not None)
+        o.has_lum_scale = int(self.luminosity_scale is not None)
+        o.kbb1 = self.kbb1 or 0.0
+        o.kbb2 = self.kbb2 or 0.0
+        o.lum_scale = self.luminosity_scale or 0.0
+        o.fixed_point_deposit = int(bool(self.fixed_point_deposit))
+        o.nthreads = int(self.nthreads)
+        return o
+
+
+def philox4x32_block(c, k):
+    ci = (C.c_uint32 * 4)(*c)
+    ki = (C.c_uint32 * 2)(*k)
+    out = (C.c_uint32 * 4)()
+    lib().oo_philox4x32_block(ci, ki, out)
+    return tuple(out)
+
+
+def beam_gaussian(n, *, seed=123456789, rng_id, beta, alpha=(0.0, 0.0, 0.0), sigma, cutoff=5.0):
+    """Seeded 6D Gaussian beam as Beam(n, CPUThreadsBackend, Float64; ...) builds it (Beam.jl:475-515)."""
+    out = np.empty((6, int(n)), dtype=np.float64)
+    b = np.asarray(beta, np.float64); a = np.asarray(alpha, np.float64); s = np.asarray(sigma, np.float64)
+    lib().oo_beam_gaussian(int(n), int(seed), int(rng_id), _dp(b), _dp(a), _dp(s), float(cutoff),
+                           *[_dp(out[k]) for k in range(6)])
+    return out
+
+
+def beam_params(charge, mass, energy, npart, r0=None):
+    return OOBeamParams(charge, mass, energy, RE * ME0 / mass if r0 is None else r0, npart)
+
+
+def erfinv(x):
+    return lib().oo_erfinv(float(x))
+
+
+class Oracle:
+    """A collide context holding the slice-pair Green cache across calls (task.runtime_cache)."""
+
+    def __init__(self, options: OracleOptions):
+        self.options = options
+        self._copt = options.to_c()
+        self._ctx = lib().oo_create(C.byref(self._copt))
+
+    def __del__(self):
+        if getattr(self, "_ctx", None):
+            lib().oo_destroy(self._ctx)
+            self._ctx = None
+
+    def collide(self, beam1: np.ndarray, beam2: np.ndarray, p1: OOBeamParams, p2: OOBeamParams,
+                compute_luminosity=True) -> float:
+        """In-place collide of (6, n) float64 beams; returns the luminosity (NaN if not computed)."""
+        P = C.POINTER(C.c_double)
+        a1 = (P * 6)(*[_dp(beam1[k]) for k in range(6)])
+        a2 = (P * 6)(*[_dp(beam2[k]) for k in range(6)])
+        lum = C.c_double(np.nan)
+        rc = lib().oo_collide(self._ctx, a1, beam1.shape[1], a2, beam2.shape[1], C.byref(p1), C.byref(p2),
+                              int(bool(compute_luminosity)), C.byref(lum))
+        if rc != OK:
+            raise OracleErrorPy(rc, lib().oo_last_error(self._ctx).decode())
+        return lum.value
+
+    def cache_stats(self):
+        out = (C.c_int64 * 3)()
+        lib().oo_cache_stats(self._ctx, out)
+        return tuple(out)
+
+    def dropped(self):
+        return lib().oo_dropped(self._ctx)
+
+    def pair_trace(self):
+        cap = 4096
+        pi = (C.c_int32 * cap)(); pj = (C.c_int32 * cap)(); lum = (C.c_double * cap)()
+        n = lib().oo_pair_trace(self._ctx, pi, pj, lum, cap)
+        return [(pi[k], pj[k], lum[k]) for k in range(min(n, cap))]
+
+
+class OracleErrorPy(Exception):
+    def __init__(self, code, msg):
+        super().__init__(f"oracle error {code}: {msg}")
+        self.code = code
+
+
+def slices(z, ns, method="normal_quantile", center_position="centroid", positions=()):
+    z = np.ascontiguousarray(z, dtype=np.float64)
+    n = z.size
+    b = np.empty(ns + 1); c = np.empty(ns); w = np.empty(ns)
+    cnt = np.empty(ns, np.int64); order = np.empty(n, np.int64)
+    pos = np.ascontiguousarray(positions, np.float64)
+    rc = lib().oo_slices(_SYM["method"][method], ns, _SYM["center_position"][center_position],
+                         _dp(pos) if pos.size else None, _dp(z), n, _dp(b), _dp(c), _dp(w),
+                         cnt.ctypes.data_as(C.POINTER(C.c_int64)), order.ctypes.data_as(C.POINTER(C.c_int64)))
+    if rc != OK:
+        raise OracleErrorPy(rc, "slicing")
+    return b, c, w, cnt, order
+
+
+def pair_batches(c1, c2):
+    c1 = np.ascontiguousarray(c1, np.float64); c2 = np.ascontiguousarray(c2, np.float64)
+    m = c1.size * c2.size
+    I32 = C.POINTER(C.c_int32)
+    arrs = [np.empty(m, np.int32) for _ in range(5)]
+    nb = lib().oo_pair_batches(_dp(c1), c1.size, _dp(c2), c2.size, *[a.ctypes.data_as(I32) for a in arrs])
+    batch_of, pi, pj, oi, oj = arrs
+    batches = [[] for _ in range(nb)]
+    for b, i, j in zip(batch_of, pi, pj):
+        batches[b].append((int(i), int(j)))
+    return batches, list(zip(oi.tolist(), oj.tolist()))
+
+
+def linear6d_matrix(beta, alpha, tune):
+    m = np.empty(36)
+    lib().oo_linear6d_matrix(_dp(np.asarray(beta, np.float64)), _dp(np.asarray(alpha, np.float64)),
+                             _dp(np.asarray(tune, np.float64)), _dp(m))
+    return m
+
+
+def linear6d(m, beam):
+    lib().oo_linear6d(_dp(np.ascontiguousarray(m, np.float64)), *[_dp(beam[k]) for k in range(6)], beam.shape[1])
