@@ -1,0 +1,148 @@
+/*
+ * libocto_b200 -- B200 (sm_100a) strong-strong PIC collision backend, C ABI.
+ *
+ * Drop-in boundary for Octopus.jl's
+ *   collide!(solver::PICPoissonSolver, beam1::Beam, beam2::Beam, backend[, ctx]) -> Float64
+ * (src/tasks/strongstrong/interface.jl:13-74, 508-509; CPU method pic_cpu.jl:1-32;
+ * CUDA method pic_cuda.jl:94-143).  Plain pointers and sizes only: a Julia `ccall`,
+ * a Python `ctypes` binding or C/C++ code can drive every entry point.
+ *
+ * Threading: one context per (task, collision label); a context is not re-entrant.
+ * Independent contexts may run concurrently on different streams or devices.
+ * Errors never cross the ABI as exceptions: every call returns an OCTO_* status and
+ * octo_last_error() returns the message.
+ */
+#ifndef OCTO_B200_H
+#define OCTO_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The Julia shim maps every non-OK code to ArgumentError with the
+ * message, as the reference raises from interface.jl:541-599 (non-finite),
+ * pic_cpu.jl:517-576 / 730-809 (unsupported option combinations) and
+ * pic_cpu.jl:1663-1670 (degenerate extent). */
+#define OCTO_OK 0
+#define OCTO_ERR_NONFINITE 1   /* non-finite coordinate; report carries role, pair, turn, first index */
+#define OCTO_ERR_UNSUPPORTED 2 /* an option combination this backend does not implement */
+#define OCTO_ERR_EXTENT 3      /* zero-width transverse extent without min_transverse_extent */
+#define OCTO_ERR_ARG 4         /* invalid argument (sizes, pointers, option values) */
+#define OCTO_ERR_CUDA 5        /* CUDA runtime failure */
+#define OCTO_ERR_TIMEOUT 6     /* a bounded device-side wait gave up */
+
+/* Enumerations of the PICPoissonSolver symbols (interface.jl:1384-1411). */
+#define OCTO_CIC 0
+#define OCTO_TSC 1
+#define OCTO_GREEN_INTEGRATED 0
+#define OCTO_GREEN_STANDARD 1
+#define OCTO_CACHE_NONE 0
+#define OCTO_CACHE_SLICE_PAIR 1
+#define OCTO_GRID_SLICE_PAIR 0
+#define OCTO_GRID_NODE 2
+#define OCTO_SLICING_NORMAL_QUANTILE 0
+#define OCTO_SLICING_SPECIFIED 1
+#define OCTO_CENTER_CENTROID 0
+#define OCTO_CENTER_MIDPOINT 1
+
+/* One beam: structure-of-arrays device pointers (Phase6DRep, Beam.jl:45-55), caller-owned
+ * and updated in place.  dtype 0 = float64. */
+typedef struct {
+    int64_t n;
+    int32_t dtype;
+    int32_t reserved;
+    void *x, *px, *y, *py, *z, *pz;
+} octo_beam;
+
+/* BeamParams (Beam.jl:29-35). */
+typedef struct {
+    double charge, mc2, E0, r0, npart;
+} octo_beam_params;
+
+/* POD twin of PICPoissonSolver's fields (interface.jl:1350-1382) and of the two
+ * LongitudinalSlicing configurations (interface.jl:762-831). */
+typedef struct {
+    int32_t nx, ny;                    /* grid */
+    int32_t deposit_method;            /* OCTO_CIC / OCTO_TSC */
+    int32_t lum_deposit_method;        /* -1 = inherit deposit_method */
+    int32_t lum_nx, lum_ny;            /* luminosity_grid; 0 = inherit grid */
+    int32_t green_type;                /* OCTO_GREEN_* */
+    int32_t green_cache;               /* OCTO_CACHE_* */
+    int32_t field_derivative;          /* 2 = :second, 4 = :fourth */
+    int32_t slice_interpolation;       /* 0 = :linear, 1 = :quadratic */
+    int32_t interaction_grid;          /* OCTO_GRID_* (:source_slice is CPU-only in the reference too) */
+    int32_t grid_extent;               /* 0 = :extrema (the reference CUDA backend rejects :sigma) */
+    double grid_extent_sigma;
+    double min_extent_x, min_extent_y; /* min_transverse_extent */
+    double grid_quantize;
+    double green_min_ratio;            /* slice_pair_green_min_ratio */
+    double green_growth;               /* slice_pair_green_growth */
+    int32_t longitudinal_kick;
+    int32_t slicing_method1, slicing_method2;   /* OCTO_SLICING_* */
+    int32_t nslices1, nslices2;
+    int32_t center_position1, center_position2; /* OCTO_CENTER_* */
+    const double *positions1, *positions2;      /* :specified internal positions (nslices-1 each) */
+    int32_t has_kbb1, has_kbb2, has_lum_scale;
+    double kbb1, kbb2, lum_scale;
+    int32_t precision;                 /* 0 = FP64 plain form */
+    int32_t reserved[7];
+} octo_pic_options;
+
+/* What a collide reports besides the luminosity. */
+typedef struct {
+    int32_t status;
+    int32_t role;            /* 0 none, 1 source, 2 field, 3 beam (slicing) */
+    int32_t pair_i, pair_j;  /* 1-based slice pair of the first failure */
+    int32_t direction;       /* 1 or 2 */
+    int32_t n_batches;       /* wavefronts executed */
+    int64_t turn;
+    int64_t first_index;     /* 1-based particle index (caller order) of the first non-finite coordinate */
+    int64_t dropped;         /* particles outside their mesh (pic_cpu.jl:394-457) */
+    int64_t green_hits, green_misses, green_rebuilds;  /* cumulative, as Contracts.jl:947-960 compares */
+    int64_t kernel_launches; /* device kernels this call launched */
+} octo_collide_report;
+
+typedef struct octo_ctx octo_ctx;
+
+/* Context holding device workspaces, the slice-pair Green cache (pic_cpu.jl:1729-1821)
+ * and twiddle tables; the twin of task.runtime_cache (pic_cpu.jl:23-32, 499-515). */
+octo_ctx *octo_create(int32_t device, const octo_pic_options *options);
+void octo_destroy(octo_ctx *ctx);
+
+/* collide! (pic_cpu.jl:82-275 / pic_cuda.jl:298-516): slices both beams, runs every slice pair
+ * in collision-time wavefronts, kicks both beams in place and returns the luminosity
+ * (NaN when compute_luminosity == 0, as for a skipped luminosity_schedule turn).
+ * stream: a cudaStream_t or NULL for the legacy default stream. */
+int32_t octo_pic_collide(octo_ctx *ctx, octo_beam *beam1, octo_beam *beam2, const octo_beam_params *p1,
+                         const octo_beam_params *p2, int64_t turn, int32_t compute_luminosity,
+                         double *luminosity, octo_collide_report *report, void *stream);
+
+/* Green-cache counters (the contract of Contracts.jl:947-960). */
+int32_t octo_green_cache_stats(octo_ctx *ctx, int64_t *hits, int64_t *misses, int64_t *rebuilds);
+
+/* Per-pair luminosity of the last collide in collision order: the sink of interface.jl:389-410,
+ * compared by Contracts.jl:916-945.  Writes up to cap entries; returns the count. */
+int64_t octo_pair_luminosity_trace(octo_ctx *ctx, int32_t *pair_i, int32_t *pair_j, double *lum, int64_t cap);
+
+/* Linear 6D one-turn map (linear6d.jl:110-121), row-major 6x6, applied `turns` times in place. */
+int32_t octo_linear6d(octo_ctx *ctx, octo_beam *beam, const double matrix[36], int32_t turns, void *stream);
+
+/* Seeded Gaussian beam on the device as Beam(n, backend, Float64; beta, alpha, sigma, cutoff, rng_id)
+ * builds it (Beam.jl:475-515; counter RNG counter_rng.jl:154-233). */
+int32_t octo_beam_gaussian(octo_ctx *ctx, octo_beam *beam, uint64_t seed, uint64_t rng_id, const double beta[3],
+                           const double alpha[3], const double sigma[3], double cutoff, void *stream);
+
+/* Message of the last failing call on this context (NUL-terminated, truncated to len). */
+int32_t octo_last_error(octo_ctx *ctx, char *buf, int64_t len);
+
+/* Host-side helpers shared with the slicing: the normal quantile sqrt(2)*erfinv(2s/ns - 1)
+ * used for :normal_quantile boundaries (slicing.jl:420-429), and the library version. */
+double octo_normal_quantile(int32_t s, int32_t ns);
+double octo_erfinv(double x);
+int32_t octo_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

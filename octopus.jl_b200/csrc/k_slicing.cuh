@@ -1,0 +1,240 @@
+// Longitudinal slicing on the device (slicing.jl:51-75, 405-460, 523-559).
+//
+// Order-dependent statistics use the reference's canonical 4096-lane fold (slicing.jl:208-257):
+// lane t folds elements t, t+4096, ... in order and the lanes are folded serially, so the
+// mean, sigma and slice centroids are bit-identical to the reference's.  Membership is a
+// stable partition: each slice's members keep ascending particle order, the order the
+// reference's index lists have, and the particles are gathered into slice-contiguous
+// structure-of-arrays buffers in the same pass.
+#pragma once
+#include "octo_internal.cuh"
+
+namespace octo {
+
+struct SliceInfo {          // device-resident, read back once per collide
+    double boundary[kMaxSlices + 1];
+    double center[kMaxSlices];
+    double weight[kMaxSlices];
+    long long count[kMaxSlices];
+    long long start[kMaxSlices];
+    double mu, sigma, zmin, zmax;
+    int ns;
+    int zero_width;
+    int nonfinite;
+    int pad;
+};
+
+// Lane partial sums / extrema over all particles.  square != 0 folds (z - mu)^2.
+__global__ void k_lane_fold(const double *__restrict__ z, long long n, const SliceInfo *info, int square,
+                            double *lane_sum, double *lane_min, double *lane_max) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= kFoldLanes) return;
+    double mu = square ? info->mu : 0.0;
+    double s = 0.0, lo = INFINITY, hi = -INFINITY;
+    for (long long i = t; i < n; i += kFoldLanes) {
+        double v = z[i];
+        if (square) {
+            double d = v - mu;
+            s += d * d;
+        } else {
+            s += v;
+            lo = jmin(lo, v);
+            hi = jmax(hi, v);
+        }
+    }
+    lane_sum[t] = s;
+    if (!square) { lane_min[t] = lo; lane_max[t] = hi; }
+}
+
+// Serial fold of the lanes (one thread).  stage 0: mean and extrema; stage 1: sigma and boundaries.
+// q[s] for s = 1..ns-1 holds sqrt(2)*erfinv(2s/ns - 1) (:normal_quantile) or the :specified positions.
+__global__ void k_fold_stats(const double *lane_sum, const double *lane_min, const double *lane_max, long long n,
+                             int stage, int method, int ns, const double *q, SliceInfo *info) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double s = 0.0;
+    for (int t = 0; t < kFoldLanes; ++t) s += lane_sum[t];
+    if (stage == 0) {
+        double lo = INFINITY, hi = -INFINITY;
+        for (int t = 0; t < kFoldLanes; ++t) { lo = jmin(lo, lane_min[t]); hi = jmax(hi, lane_max[t]); }
+        info->mu = s / (double)n;
+        info->zmin = lo;
+        info->zmax = hi;
+        return;
+    }
+    double mu = info->mu;
+    double sigma = sqrt(jmax(s / (double)n, 0.0));
+    info->sigma = sigma;
+    double *b = info->boundary;
+    int nb = ns;
+    if (method == 0) {  // :normal_quantile (slicing.jl:405-429)
+        if (sigma == 0.0) {
+            for (int k = 0; k <= ns; ++k) b[k] = mu;
+        } else {
+            b[0] = info->zmin;
+            b[ns] = info->zmax;
+            for (int k = 1; k <= ns - 1; ++k) b[k] = jclamp(mu + sigma * q[k], b[0], b[ns]);
+        }
+    } else {  // :specified (slicing.jl:393-403): internal = sort(mu + p*sigma)
+        double internal[kMaxSlices];
+        int m = ns - 1;
+        for (int k = 0; k < m; ++k) internal[k] = mu + q[k + 1] * sigma;
+        for (int a = 1; a < m; ++a) {  // stable insertion sort
+            double v = internal[a];
+            int c = a - 1;
+            while (c >= 0 && v < internal[c]) { internal[c + 1] = internal[c]; --c; }
+            internal[c + 1] = v;
+        }
+        b[0] = info->zmin;
+        b[ns] = info->zmax;
+        for (int k = 0; k < m; ++k) b[k + 1] = jclamp(internal[k], b[0], b[ns]);
+    }
+    int bad = 0;
+    for (int k = 0; k <= nb; ++k)
+        if (!isfinite(b[k])) bad = 1;
+    info->nonfinite = bad;
+    info->zero_width = (b[0] == b[ns]) ? 1 : 0;
+    info->ns = ns;
+}
+
+// searchsortedlast(boundary, z) clamped to [1, ns], returned 0-based (slicing.jl:454-457).
+__device__ __forceinline__ int slice_of(double z, const double *b, int ns, int zero_width) {
+    if (zero_width) return 0;
+    int k = 0;
+    for (int t = 0; t <= ns; ++t) k += (b[t] <= z) ? 1 : 0;
+    k = k < 1 ? 1 : (k > ns ? ns : k);
+    return k - 1;
+}
+
+// Per-block slice counts over contiguous chunks.
+__global__ void k_slice_count(const double *__restrict__ z, long long n, long long chunk, const SliceInfo *info,
+                              int *counts) {
+    __shared__ double b[kMaxSlices + 1];
+    __shared__ int c[kMaxSlices];
+    int ns = info->ns;
+    for (int t = threadIdx.x; t <= ns; t += blockDim.x) b[t] = info->boundary[t];
+    for (int t = threadIdx.x; t < ns; t += blockDim.x) c[t] = 0;
+    __syncthreads();
+    int zw = info->zero_width;
+    long long lo = (long long)blockIdx.x * chunk, hi = min(n, lo + chunk);
+    for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) atomicAdd(&c[slice_of(z[i], b, ns, zw)], 1);
+    __syncthreads();
+    for (int t = threadIdx.x; t < ns; t += blockDim.x) counts[(long long)blockIdx.x * ns + t] = c[t];
+}
+
+// Slice starts (aligned to `align` elements) and per-block write offsets.  One block.
+__global__ void k_slice_offsets(const int *counts, int nblocks, int align, SliceInfo *info, long long *blockoff) {
+    int ns = info->ns;
+    __shared__ long long tot[kMaxSlices];
+    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+        long long acc = 0;
+        for (int b = 0; b < nblocks; ++b) acc += counts[(long long)b * ns + s];
+        tot[s] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long pos = 0;
+        for (int s = 0; s < ns; ++s) {
+            info->start[s] = pos;
+            info->count[s] = tot[s];
+            pos += (tot[s] + align - 1) / align * align;
+        }
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+        long long acc = info->start[s];
+        for (int b = 0; b < nblocks; ++b) {
+            blockoff[(long long)b * ns + s] = acc;
+            acc += counts[(long long)b * ns + s];
+        }
+    }
+}
+
+// Stable scatter into slice-contiguous SoA buffers; perm[pos] = original index.
+// Each block walks its chunk in tiles of blockDim particles, ranking within warps by match_any.
+__global__ void k_slice_scatter(const double *__restrict__ x, const double *__restrict__ px,
+                                const double *__restrict__ y, const double *__restrict__ py,
+                                const double *__restrict__ z, const double *__restrict__ pz, long long n,
+                                long long chunk, const SliceInfo *info, const long long *blockoff, double *sx,
+                                double *spx, double *sy, double *spy, double *sz, double *spz, int *perm) {
+    __shared__ double b[kMaxSlices + 1];
+    __shared__ long long run[kMaxSlices];
+    __shared__ int wcount[32][kMaxSlices];
+    int ns = info->ns;
+    int zw = info->zero_width;
+    for (int t = threadIdx.x; t <= ns; t += blockDim.x) b[t] = info->boundary[t];
+    for (int t = threadIdx.x; t < ns; t += blockDim.x) run[t] = blockoff[(long long)blockIdx.x * ns + t];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    long long lo = (long long)blockIdx.x * chunk, hi = min(n, lo + chunk);
+    __syncthreads();
+    for (long long base = lo; base < hi; base += blockDim.x) {
+        for (int t = threadIdx.x; t < 32 * ns; t += blockDim.x) wcount[t / ns][t % ns] = 0;
+        __syncthreads();
+        long long i = base + threadIdx.x;
+        bool live = i < hi;
+        int s = live ? slice_of(z[i], b, ns, zw) : -1;
+        unsigned peers = __match_any_sync(0xffffffffu, s);
+        int rank = __popc(peers & ((1u << lane) - 1u));
+        if (live && rank == 0) wcount[warp][s] = __popc(peers);
+        __syncthreads();
+        if (live) {
+            long long pos = run[s] + rank;
+            for (int w = 0; w < warp; ++w) pos += wcount[w][s];
+            perm[pos] = (int)i;
+            sx[pos] = x[i]; spx[pos] = px[i]; sy[pos] = y[i];
+            spy[pos] = py[i]; sz[pos] = z[i]; spz[pos] = pz[i];
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < ns; t += blockDim.x) {
+            int add = 0;
+            for (int w = 0; w < nwarps; ++w) add += wcount[w][t];
+            run[t] += add;
+        }
+        __syncthreads();
+    }
+}
+
+// Centroid lane sums per slice: lane t folds members t, t+4096, ... of the slice list (slicing.jl:240-257).
+__global__ void k_slice_lanes(const double *__restrict__ sz, const SliceInfo *info, double *lanes) {
+    int s = blockIdx.y;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= kFoldLanes || s >= info->ns) return;
+    long long st = info->start[s], cnt = info->count[s];
+    double acc = 0.0;
+    for (long long k = t; k < cnt; k += kFoldLanes) acc += sz[st + k];
+    lanes[(long long)s * kFoldLanes + t] = acc;
+}
+
+// Serial lane fold per slice; centers and weights (slicing.jl:523-559).
+__global__ void k_slice_finish(const double *lanes, long long n, int center_position, SliceInfo *info) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= info->ns) return;
+    long long cnt = info->count[s];
+    info->weight[s] = (double)cnt / (double)n;
+    const double *b = info->boundary;
+    if (center_position == 0) {
+        if (cnt == 0) {
+            info->center[s] = (b[s] + b[s + 1]) / 2;
+        } else {
+            double acc = 0.0;
+            for (int t = 0; t < kFoldLanes; ++t) acc += lanes[(long long)s * kFoldLanes + t];
+            info->center[s] = acc / (double)cnt;
+        }
+    } else {
+        info->center[s] = (b[s] + b[s + 1]) / 2;
+    }
+}
+
+// Write the kicked slice-sorted coordinates back in caller order.
+__global__ void k_unsort(const int *__restrict__ perm, long long total, const double *sx, const double *spx,
+                         const double *sy, const double *spy, const double *sz, const double *spz, double *x,
+                         double *px, double *y, double *py, double *z, double *pz, const SliceInfo *info) {
+    // total = padded length; padding positions carry perm = -1
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= total) return;
+    int i = perm[p];
+    if (i < 0) return;
+    x[i] = sx[p]; px[i] = spx[p]; y[i] = sy[p];
+    py[i] = spy[p]; z[i] = sz[p]; pz[i] = spz[p];
+}
+
+}  // namespace octo

@@ -1,0 +1,999 @@
+// libocto_b200: host runtime and C ABI of the B200 strong-strong PIC collision backend.
+//
+// One collide is: device slicing of both beams (one small readback of the slice table),
+// a host-built collision-time wavefront schedule (slicing.jl:561-647) uploaded once, and
+// per wavefront a fixed sequence of batched kernels -- bounds, on-device grid/Green-cache
+// planning, Green spectra, luminosity, fixed-point deposition, the Hockney FFT convolution
+// with the field derivative fused into the inverse pass, and the synchro-beam kick.  The
+// luminosity parts and status are read back once at the end.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/octo_b200.h"
+#include "k_misc.cuh"
+#include "k_pic.cuh"
+#include "k_slicing.cuh"
+
+using namespace octo;
+
+namespace {
+
+struct CudaFail {
+    std::string msg;
+};
+struct OctoFail {
+    int code;
+    std::string msg;
+};
+
+#define CK(call)                                                                                           \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess) throw CudaFail{std::string(#call) + ": " + cudaGetErrorString(e_)};         \
+    } while (0)
+
+// Inverse error function: Winitzki start, Halley steps on erf / erfc.  Used only for the
+// :normal_quantile slice quantiles sqrt(2)*erfinv(2s/ns-1) (slicing.jl:425).
+double erfinv_host(double x) {
+    if (std::isnan(x) || x < -1.0 || x > 1.0) return NAN;
+    if (x == 1.0) return INFINITY;
+    if (x == -1.0) return -INFINITY;
+    if (x == 0.0) return x;
+    double ax = std::fabs(x);
+    const double a = 0.147, pi = 3.141592653589793;
+    double ln = std::log1p(-ax * ax);
+    double t1 = 2.0 / (pi * a) + ln / 2.0;
+    double y = std::sqrt(std::sqrt(t1 * t1 - ln / a) - t1);
+    const double c = 1.1283791670955126;  // 2/sqrt(pi)
+    for (int it = 0; it < 4; ++it) {
+        double f = (ax < 0.5) ? (std::erf(y) - ax) : ((1.0 - ax) - std::erfc(y));
+        double step = f / (c * std::exp(-y * y));
+        y = y - step / (1.0 + y * step);
+    }
+    return x < 0 ? -y : y;
+}
+
+struct OrderEntry {
+    double t;
+    int i, j;
+};
+
+// slicing.jl:561-568 (stable sort by collision time -(c1+c2)/2)
+std::vector<OrderEntry> collision_order(const double *c1, int ns1, const double *c2, int ns2) {
+    std::vector<OrderEntry> o;
+    o.reserve((size_t)ns1 * ns2);
+    for (int i = 0; i < ns1; ++i)
+        for (int j = 0; j < ns2; ++j) o.push_back({-(c1[i] + c2[j]) / 2, i + 1, j + 1});
+    std::stable_sort(o.begin(), o.end(), [](const OrderEntry &a, const OrderEntry &b) { return a.t < b.t; });
+    return o;
+}
+
+// slicing.jl:601-647 : greedy ready, conflict-free batches.
+std::vector<std::vector<OrderEntry>> pair_batches(const std::vector<OrderEntry> &pairs, int ns1, int ns2) {
+    std::vector<std::vector<OrderEntry>> batches;
+    std::vector<std::vector<int>> by_i(ns1 + 1), by_j(ns2 + 1);
+    for (size_t k = 0; k < pairs.size(); ++k) {
+        by_i[pairs[k].i].push_back((int)k);
+        by_j[pairs[k].j].push_back((int)k);
+    }
+    std::vector<size_t> next_i(ns1 + 1, 0), next_j(ns2 + 1, 0);
+    std::vector<char> done(pairs.size(), 0);
+    size_t remaining = pairs.size();
+    while (remaining > 0) {
+        std::vector<OrderEntry> cur;
+        std::vector<char> used_i(ns1 + 1, 0), used_j(ns2 + 1, 0);
+        for (size_t k = 0; k < pairs.size(); ++k) {
+            if (done[k]) continue;
+            const OrderEntry &p = pairs[k];
+            if (used_i[p.i] || used_j[p.j]) continue;
+            bool ri = next_i[p.i] < by_i[p.i].size() && by_i[p.i][next_i[p.i]] == (int)k;
+            bool rj = next_j[p.j] < by_j[p.j].size() && by_j[p.j][next_j[p.j]] == (int)k;
+            if (ri && rj) {
+                cur.push_back(p);
+                used_i[p.i] = 1; used_j[p.j] = 1; done[k] = 1;
+                next_i[p.i]++; next_j[p.j]++;
+                --remaining;
+            }
+        }
+        if (cur.empty()) throw OctoFail{OCTO_ERR_ARG, "internal collision scheduler error: no ready slice pair"};
+        batches.push_back(cur);
+    }
+    return batches;
+}
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    void ensure(size_t m) {
+        if (m <= n) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        CK(cudaMalloc(&p, std::max<size_t>(m, 1) * sizeof(T)));
+        n = m;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+template <class T>
+struct PinBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    void ensure(size_t m) {
+        if (m <= n) return;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        CK(cudaMallocHost(&p, std::max<size_t>(m, 1) * sizeof(T)));
+        n = m;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+constexpr int kAlign = 32;           // slice start alignment (elements)
+constexpr long long kChunk = 8192;   // particles per slicing block
+
+struct BeamWS {
+    DevBuf<double> s[6];
+    DevBuf<int> perm;
+    DevBuf<SliceInfo> info;
+    DevBuf<double> lane_sum, lane_min, lane_max, lanes, q;
+    DevBuf<int> counts;
+    DevBuf<long long> blockoff;
+    SliceInfo host;
+    long long total = 0;
+    void release() {
+        for (auto &b : s) b.release();
+        perm.release(); info.release(); lane_sum.release(); lane_min.release(); lane_max.release();
+        lanes.release(); q.release(); counts.release(); blockoff.release();
+    }
+};
+
+}  // namespace
+
+struct octo_ctx {
+    int device = 0;
+    octo_pic_options opt{};
+    std::vector<double> pos[2];
+    DevOptions dopt{};
+    std::string err;
+    int ns[2] = {0, 0};
+    BeamWS bw[2];
+    DevBuf<double2> tw_x, tw_y;
+    DevBuf<Task> tasks;
+    DevBuf<Plane> planes;
+    DevBuf<LumJob> lumjobs;
+    DevBuf<TaskGeom> geom;
+    DevBuf<int2> blockmap;
+    DevBuf<CacheEntry> cache;
+    DevBuf<NodeMesh> nodes;
+    DevBuf<LumGeom> lumgeom;
+    DevBuf<unsigned long long> bnd, lumb, nodebox_s, nodebox_f;
+    DevBuf<int> nanflag, nodenan;
+    DevBuf<DevStatus> status;
+    DevBuf<double2> ghat;
+    DevBuf<long long> qgrid, lq;
+    DevBuf<double2> spec;
+    DevBuf<double> fields, lum_parts, node_ref, stats, partial;
+    DevBuf<double *> soa_ptrs;
+    PinBuf<char> stage;
+    PinBuf<double> h_lum;
+    PinBuf<DevStatus> h_status;
+    PinBuf<NodeMesh> h_nodes;
+    long long gstride = 0;
+    int nslots = 0;
+    int cache_ready = 0;
+    std::vector<int> trace_i, trace_j;
+    std::vector<double> trace_lum;
+    long long last_launches = 0;
+};
+
+namespace {
+
+void set_error(octo_ctx *c, const std::string &m) { c->err = m; }
+
+bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+
+int validate_options(const octo_pic_options &o, std::string &msg) {
+    if (o.nx < 5 || o.ny < 5) { msg = "PICPoissonSolver grid must be at least (5, 5)"; return OCTO_ERR_ARG; }
+    if (!is_pow2(o.nx) || !is_pow2(o.ny) || o.nx > 512 || o.ny > 512) {
+        msg = "this backend's FFT needs power-of-two grid dimensions <= 512";
+        return OCTO_ERR_UNSUPPORTED;
+    }
+    if (o.deposit_method != OCTO_CIC && o.deposit_method != OCTO_TSC) { msg = "deposit_method must be :CIC or :TSC"; return OCTO_ERR_ARG; }
+    int lm = o.lum_deposit_method < 0 ? o.deposit_method : o.lum_deposit_method;
+    if (lm != OCTO_CIC && lm != OCTO_TSC) { msg = "luminosity_deposit_method must resolve to :CIC or :TSC"; return OCTO_ERR_ARG; }
+    int lnx = o.lum_nx > 0 ? o.lum_nx : o.nx, lny = o.lum_ny > 0 ? o.lum_ny : o.ny;
+    if (lnx < 3 || lny < 3) { msg = "luminosity_grid dimensions must both be at least 3"; return OCTO_ERR_ARG; }
+    if (o.green_type != OCTO_GREEN_INTEGRATED && o.green_type != OCTO_GREEN_STANDARD) {
+        msg = "green_type must be :integrated or :standard on this backend (:lattice is an experimental CPU study kernel)";
+        return OCTO_ERR_UNSUPPORTED;
+    }
+    if (o.green_cache != OCTO_CACHE_NONE && o.green_cache != OCTO_CACHE_SLICE_PAIR) { msg = "green_cache must be :none or :slice_pair"; return OCTO_ERR_ARG; }
+    if (o.field_derivative != 2 && o.field_derivative != 4) { msg = "field_derivative must be :second or :fourth"; return OCTO_ERR_ARG; }
+    if (o.slice_interpolation != 0 && o.slice_interpolation != 1) { msg = "slice_interpolation must be :linear or :quadratic"; return OCTO_ERR_ARG; }
+    if (o.interaction_grid != OCTO_GRID_SLICE_PAIR && o.interaction_grid != OCTO_GRID_NODE) {
+        msg = "interaction_grid = :source_slice is implemented only by the CPU PICPoissonSolver path (pic_cpu.jl:730-809)";
+        return OCTO_ERR_UNSUPPORTED;
+    }
+    if (o.grid_extent != 0) {
+        msg = "grid_extent = :sigma is not implemented by the GPU PIC backend; set grid_extent = :extrema";
+        return OCTO_ERR_UNSUPPORTED;
+    }
+    if (o.interaction_grid == OCTO_GRID_NODE && o.slice_interpolation != 0) {
+        msg = "slice_interpolation = :quadratic is not implemented for interaction_grid = :node";
+        return OCTO_ERR_UNSUPPORTED;
+    }
+    if (!(o.green_min_ratio > 0.0 && o.green_min_ratio <= 1.0)) { msg = "slice_pair_green_min_ratio must be in (0, 1]"; return OCTO_ERR_ARG; }
+    if (!(o.green_growth >= 0.0)) { msg = "slice_pair_green_growth must be non-negative"; return OCTO_ERR_ARG; }
+    if (!(o.grid_quantize >= 0.0)) { msg = "grid_quantize must be non-negative"; return OCTO_ERR_ARG; }
+    for (int b = 0; b < 2; ++b) {
+        int ns = b == 0 ? o.nslices1 : o.nslices2;
+        int m = b == 0 ? o.slicing_method1 : o.slicing_method2;
+        if (ns < 1 || ns > kMaxSlices) { msg = "nslices must be in 1..64 on this backend"; return OCTO_ERR_ARG; }
+        if (m != OCTO_SLICING_NORMAL_QUANTILE && m != OCTO_SLICING_SPECIFIED) {
+            msg = "slicing method must be :normal_quantile or :specified on this backend";
+            return OCTO_ERR_UNSUPPORTED;
+        }
+        const double *p = b == 0 ? o.positions1 : o.positions2;
+        if (m == OCTO_SLICING_SPECIFIED && ns > 1 && !p) { msg = "specified slicing requires nslices-1 internal positions"; return OCTO_ERR_ARG; }
+    }
+    if (o.precision != 0) { msg = "only the FP64 plain form (precision = 0) is available"; return OCTO_ERR_UNSUPPORTED; }
+    return OCTO_OK;
+}
+
+void upload_twiddles(DevBuf<double2> &buf, int L) {
+    std::vector<double2> h(L / 2);
+    for (int k = 0; k < L / 2; ++k) {
+        double a = 2.0 * 3.141592653589793238462643 * (double)k / (double)L;
+        h[k] = make_double2(std::cos(a), -std::sin(a));
+    }
+    buf.ensure(L / 2);
+    CK(cudaMemcpy(buf.p, h.data(), sizeof(double2) * (L / 2), cudaMemcpyHostToDevice));
+}
+
+long long padded_total(long long n, int ns) { return n + (long long)ns * kAlign; }
+
+__global__ void k_init_bounds(unsigned long long *bnd, int ntasks, unsigned long long *lumb, int npairs, int *nanflag,
+                              DevStatus *st, int reset_status) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < ntasks) {
+        for (int k = 0; k < 8; ++k) bnd[(long long)t * 8 + k] = (k & 1) ? kOrdMaxInit : kOrdMinInit;
+        nanflag[t] = 0;
+    }
+    if (t < npairs)
+        for (int k = 0; k < 4; ++k) lumb[(long long)t * 4 + k] = (k & 1) ? kOrdMaxInit : kOrdMinInit;
+    if (t == 0 && reset_status) {
+        st->first_bad = ~0ull;
+        st->code = 0;
+        st->role = 0;
+        st->dropped = 0;
+    }
+}
+
+__global__ void k_init_boxes(unsigned long long *box, long long n4) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n4) box[t] = (t & 1) ? kOrdMaxInit : kOrdMinInit;
+}
+
+// Device slicing of one beam; returns after enqueueing (the slice table is read back by the caller).
+void slice_beam(octo_ctx *c, int b, const octo_beam &beam, cudaStream_t st, long long &launches) {
+    BeamWS &W = c->bw[b];
+    const long long n = beam.n;
+    const int ns = c->ns[b];
+    const long long total = padded_total(n, ns);
+    for (auto &a : W.s) a.ensure(total);
+    W.perm.ensure(total);
+    W.info.ensure(1);
+    W.lane_sum.ensure(kFoldLanes); W.lane_min.ensure(kFoldLanes); W.lane_max.ensure(kFoldLanes);
+    W.lanes.ensure((size_t)kFoldLanes * ns);
+    const long long nblocks = (n + kChunk - 1) / kChunk;
+    W.counts.ensure((size_t)nblocks * ns);
+    W.blockoff.ensure((size_t)nblocks * ns);
+    W.total = total;
+    const double *z = (const double *)beam.z;
+    int method = b == 0 ? c->opt.slicing_method1 : c->opt.slicing_method2;
+    int cpos = b == 0 ? c->opt.center_position1 : c->opt.center_position2;
+    k_lane_fold<<<kFoldLanes / 256, 256, 0, st>>>(z, n, W.info.p, 0, W.lane_sum.p, W.lane_min.p, W.lane_max.p);
+    k_fold_stats<<<1, 1, 0, st>>>(W.lane_sum.p, W.lane_min.p, W.lane_max.p, n, 0, method, ns, W.q.p, W.info.p);
+    k_lane_fold<<<kFoldLanes / 256, 256, 0, st>>>(z, n, W.info.p, 1, W.lane_sum.p, W.lane_min.p, W.lane_max.p);
+    k_fold_stats<<<1, 1, 0, st>>>(W.lane_sum.p, W.lane_min.p, W.lane_max.p, n, 1, method, ns, W.q.p, W.info.p);
+    k_slice_count<<<(unsigned)nblocks, 256, 0, st>>>(z, n, kChunk, W.info.p, W.counts.p);
+    k_slice_offsets<<<1, 64, 0, st>>>(W.counts.p, (int)nblocks, kAlign, W.info.p, W.blockoff.p);
+    CK(cudaMemsetAsync(W.perm.p, 0xff, sizeof(int) * total, st));
+    k_slice_scatter<<<(unsigned)nblocks, 256, 0, st>>>(
+        (const double *)beam.x, (const double *)beam.px, (const double *)beam.y, (const double *)beam.py, z,
+        (const double *)beam.pz, n, kChunk, W.info.p, W.blockoff.p, W.s[0].p, W.s[1].p, W.s[2].p, W.s[3].p, W.s[4].p,
+        W.s[5].p, W.perm.p);
+    k_slice_lanes<<<dim3(kFoldLanes / 256, ns), 256, 0, st>>>(W.s[4].p, W.info.p, W.lanes.p);
+    k_slice_finish<<<1, 64, 0, st>>>(W.lanes.p, n, cpos, W.info.p);
+    launches += 10;
+    CK(cudaGetLastError());
+}
+
+long long first_nonfinite_host(const octo_beam &beam, cudaStream_t st, bool z_only) {
+    std::vector<double> h(beam.n);
+    void *arr[6] = {beam.x, beam.px, beam.y, beam.py, beam.z, beam.pz};
+    long long first = -1;
+    for (int k = 0; k < 6; ++k) {
+        if (z_only && k != 4) continue;
+        CK(cudaMemcpyAsync(h.data(), arr[k], sizeof(double) * beam.n, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (long long i = 0; i < beam.n; ++i)
+            if (!std::isfinite(h[i])) { if (first < 0 || i < first) first = i; break; }
+    }
+    return first;
+}
+
+int check_beam(const octo_beam *b, std::string &msg) {
+    if (!b) { msg = "beam pointer is NULL"; return OCTO_ERR_ARG; }
+    if (b->n <= 0) { msg = "longitudinal slicing requires at least one particle"; return OCTO_ERR_ARG; }
+    if (b->n >= (1LL << 31) - 4096) { msg = "beam too large for 32-bit particle indices"; return OCTO_ERR_ARG; }
+    if (b->dtype != 0) { msg = "only float64 beams are supported"; return OCTO_ERR_UNSUPPORTED; }
+    if (!b->x || !b->px || !b->y || !b->py || !b->z || !b->pz) { msg = "beam coordinate pointer is NULL"; return OCTO_ERR_ARG; }
+    return OCTO_OK;
+}
+
+template <class F>
+void launch_method(int method, F f) {
+    if (method == 0) f(std::integral_constant<int, 0>());
+    else f(std::integral_constant<int, 1>());
+}
+
+
+// Dynamic shared memory of the FFT kernels for line lengths NX, NY (4 warps per block).
+size_t fft_smem(int L) { return sizeof(double2) * (size_t)(L / 2 + 4 * L); }
+// k_conv_field: twiddles (NX/2) + 4 lines (4*NX) complex, plus a (tile+4) x nx phi tile; NX = 2*nx.
+size_t field_smem(int NX) { return sizeof(double2) * (size_t)(NX / 2 + 4 * NX) + sizeof(double) * (size_t)(kFieldTile + 4) * (NX / 2); }
+constexpr size_t kSmemLimit = 227 * 1024;
+
+// Enqueue the node meshes of both directions (pic_cpu.jl:1404-1419), then read back validity.
+void build_node_meshes(octo_ctx *c, Collide &C, const SliceInfo &S1, const SliceInfo &S2, cudaStream_t st,
+                       long long &launches) {
+    const int ns1 = c->ns[0], ns2 = c->ns[1];
+    const int nnode = ns1 * (ns2 + 1) + ns2 * (ns1 + 1);
+    c->nodes.ensure(nnode);
+    c->nodenan.ensure(1);
+    CK(cudaMemsetAsync(c->nodenan.p, 0, sizeof(int), st));
+    for (int dir = 1; dir <= 2; ++dir) {
+        const SliceInfo &SS = dir == 1 ? S1 : S2;
+        const SliceInfo &SF = dir == 1 ? S2 : S1;
+        const int nss = dir == 1 ? ns1 : ns2, nsf = dir == 1 ? ns2 : ns1, nb = nsf + 1;
+        const int sbeam = dir - 1, fbeam = 2 - dir;
+        const int mesh0 = dir == 1 ? 0 : ns1 * (ns2 + 1);
+        std::vector<double> ref((size_t)nss * nb + nss);
+        for (int i = 0; i < nss; ++i) {
+            for (int b = 0; b < nb; ++b) ref[(size_t)i * nb + b] = 0.5 * (SS.center[i] - SF.boundary[b]);
+            ref[(size_t)nss * nb + i] = SS.center[i];
+        }
+        c->node_ref.ensure(ref.size() * 2);
+        double *dref = c->node_ref.p + (dir - 1) * (size_t)(c->node_ref.n / 2);
+        CK(cudaMemcpyAsync(dref, ref.data(), sizeof(double) * ref.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));  // `ref` is a host temporary
+        c->nodebox_s.ensure((size_t)nss * nb * 4);
+        c->nodebox_f.ensure((size_t)nsf * nss * 4);
+        long long ns4 = (long long)nss * nb * 4, nf4 = (long long)nsf * nss * 4;
+        k_init_boxes<<<(unsigned)((ns4 + 255) / 256), 256, 0, st>>>(c->nodebox_s.p, ns4);
+        k_init_boxes<<<(unsigned)((nf4 + 255) / 256), 256, 0, st>>>(c->nodebox_f.p, nf4);
+        NodeBoxArgs A{};
+        const BeamWS &WS = c->bw[sbeam], &WF = c->bw[fbeam];
+        A.x = WS.s[0].p; A.px = WS.s[1].p; A.y = WS.s[2].p; A.py = WS.s[3].p; A.z = WS.s[4].p;
+        long long maxn = 1;
+        for (int s = 0; s < nss; ++s) { A.start[s] = SS.start[s]; A.count[s] = SS.count[s]; maxn = std::max(maxn, SS.count[s]); }
+        A.ref = dref;
+        A.boxes = c->nodebox_s.p;
+        A.nanf = c->nodenan.p;
+        A.nsl = nss; A.nref = nb; A.field_mode = 0;
+        unsigned bx = (unsigned)std::min<long long>(64, (maxn + 4095) / 4096);
+        k_node_boxes<<<dim3(bx, nss), 256, 0, st>>>(A);
+        NodeBoxArgs F{};
+        F.x = WF.s[0].p; F.px = WF.s[1].p; F.y = WF.s[2].p; F.py = WF.s[3].p; F.z = WF.s[4].p;
+        maxn = 1;
+        for (int s = 0; s < nsf; ++s) { F.start[s] = SF.start[s]; F.count[s] = SF.count[s]; maxn = std::max(maxn, SF.count[s]); }
+        F.ref = dref + (size_t)nss * nb;
+        F.boxes = c->nodebox_f.p;
+        F.nanf = c->nodenan.p;
+        F.nsl = nsf; F.nref = nss; F.field_mode = 1;
+        bx = (unsigned)std::min<long long>(64, (maxn + 4095) / 4096);
+        k_node_boxes<<<dim3(bx, nsf), 256, 0, st>>>(F);
+        // counts of the source slices for the plan
+        c->stats.ensure(kMaxSlices * 2);
+        long long cnt[kMaxSlices];
+        for (int s = 0; s < nss; ++s) cnt[s] = SS.count[s];
+        long long *dcnt = (long long *)c->stats.p + (dir - 1) * kMaxSlices;
+        CK(cudaMemcpyAsync(dcnt, cnt, sizeof(long long) * nss, cudaMemcpyHostToDevice, st));
+        k_node_plan<<<(nss * nb + 63) / 64, 64, 0, st>>>(c->dopt, c->nodebox_s.p, c->nodebox_f.p, nss, nb, dcnt,
+                                                         c->nodes.p + mesh0, c->status.p);
+        CK(cudaStreamSynchronize(st));  // box buffers are reused by the next direction; cnt is a host temporary
+        launches += 5;
+    }
+    int nanf = 0;
+    CK(cudaMemcpy(&nanf, c->nodenan.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (nanf) throw OctoFail{OCTO_ERR_NONFINITE, "non-finite coordinate (node-mesh build)"};
+    // Green spectra of every valid node mesh
+    const int NX = 2 * c->opt.nx, NY = 2 * c->opt.ny;
+    C.nodes = c->nodes.p;
+    k_green_rows<<<dim3((NY / 2 + 3) / 4, nnode), 128, fft_smem(NX), st>>>(C, 1, 0, 0);
+    k_green_cols<<<dim3((c->opt.nx + 1 + 3) / 4, nnode), 128, fft_smem(NY), st>>>(C, 1, 0, 0);
+    launches += 2;
+    c->h_nodes.ensure(nnode);
+    CK(cudaMemcpyAsync(c->h_nodes.p, c->nodes.p, sizeof(NodeMesh) * nnode, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+}
+
+double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_params *p1, const octo_beam_params *p2,
+                    int64_t turn, int compute_lum, octo_collide_report *rep, cudaStream_t st) {
+    const octo_pic_options &o = c->opt;
+    long long launches = 0;
+    std::string msg;
+    int rc = check_beam(b1, msg);
+    if (rc == OCTO_OK) rc = check_beam(b2, msg);
+    if (rc != OCTO_OK) throw OctoFail{rc, msg};
+    if (!p1 || !p2) throw OctoFail{OCTO_ERR_ARG, "beam params pointer is NULL"};
+    CK(cudaSetDevice(c->device));
+    // kbb and luminosity scale (slicing.jl:77-91, pic_cpu.jl:821-829)
+    if (!o.has_kbb1 && !(std::isfinite(p1->E0) && p1->E0 != 0))
+        throw OctoFail{OCTO_ERR_ARG, "beam1 E0 must be finite and nonzero when kbb1 is not specified"};
+    if (!o.has_kbb2 && !(std::isfinite(p2->E0) && p2->E0 != 0))
+        throw OctoFail{OCTO_ERR_ARG, "beam2 E0 must be finite and nonzero when kbb2 is not specified"};
+    const long long n1 = b1->n, n2 = b2->n;
+    const double kbb1p = o.has_kbb1 ? o.kbb1 : p1->charge * p2->charge * p1->r0 * p2->npart * p1->mc2 / p1->E0;
+    const double kbb2p = o.has_kbb2 ? o.kbb2 : p1->charge * p2->charge * p2->r0 * p1->npart * p2->mc2 / p2->E0;
+    const double kbb1 = kbb1p / (double)n2, kbb2 = kbb2p / (double)n1;
+    const double klum = o.has_lum_scale ? o.lum_scale : p1->npart * p2->npart / (double)(n1 * n2);
+
+    // ---- slicing (one readback of the slice tables)
+    slice_beam(c, 0, *b1, st, launches);
+    slice_beam(c, 1, *b2, st, launches);
+    CK(cudaMemcpyAsync(&c->bw[0].host, c->bw[0].info.p, sizeof(SliceInfo), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&c->bw[1].host, c->bw[1].info.p, sizeof(SliceInfo), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int b = 0; b < 2; ++b) {
+        if (c->bw[b].host.nonfinite) {
+            long long first = first_nonfinite_host(b == 0 ? *b1 : *b2, st, true);
+            if (rep) { rep->role = 3; rep->first_index = first + 1; }
+            char m[192];
+            snprintf(m, sizeof m, "non-finite beam%d coordinate z at particle %lld (longitudinal slicing, turn %lld)",
+                     b + 1, first + 1, (long long)turn);
+            throw OctoFail{OCTO_ERR_NONFINITE, m};
+        }
+    }
+    const SliceInfo S1 = c->bw[0].host, S2 = c->bw[1].host;
+    const int ns1 = c->ns[0], ns2 = c->ns[1];
+    const int nx = o.nx, ny = o.ny, NX = 2 * nx, NY = 2 * ny;
+    const int lnx = c->dopt.lnx, lny = c->dopt.lny;
+    const bool node = o.interaction_grid == OCTO_GRID_NODE;
+    const bool lk = o.longitudinal_kick != 0;
+    const bool quad = o.slice_interpolation == 1;
+    const int method = o.deposit_method;
+    const int lmethod = c->dopt.lum_method;
+
+    Collide C{};
+    C.o = c->dopt;
+    C.klum = klum;
+    for (int b = 0; b < 2; ++b)
+        for (int k = 0; k < 6; ++k) C.beam[b].c[k] = c->bw[b].s[k].p;
+    C.tw_x = c->tw_x.p;
+    C.tw_y = c->tw_y.p;
+    C.gstride = c->gstride;
+
+    // ---- Green slots / cache / status
+    const int maxw = std::min(ns1, ns2);
+    const int nnode = node ? ns1 * (ns2 + 1) + ns2 * (ns1 + 1) : 0;
+    const int nslots = node ? nnode : (o.green_cache ? 2 * ns1 * ns2 : 2 * maxw);
+    if ((size_t)nslots * c->gstride > c->ghat.n) c->ghat.ensure((size_t)nslots * c->gstride);
+    c->status.ensure(1);
+    if (!c->cache_ready) {
+        DevStatus z{};
+        z.first_bad = ~0ull;
+        CK(cudaMemcpyAsync(c->status.p, &z, sizeof z, cudaMemcpyHostToDevice, st));
+        if (!node && o.green_cache) {
+            c->cache.ensure((size_t)2 * ns1 * ns2);
+            CK(cudaMemsetAsync(c->cache.p, 0, sizeof(CacheEntry) * 2 * ns1 * ns2, st));
+        }
+        CK(cudaStreamSynchronize(st));
+        c->cache_ready = 1;
+    }
+    C.cache = c->cache.p;
+    C.status = c->status.p;
+    C.ghat = c->ghat.p;
+
+    // ---- schedule (slicing.jl:561-647), skipping pairs with an empty slice (pic_cpu.jl:302)
+    auto order = collision_order(S1.center, ns1, S2.center, ns2);
+    auto batches = pair_batches(order, ns1, ns2);
+    std::vector<int> pos_of((size_t)ns1 * ns2);
+    for (size_t p = 0; p < order.size(); ++p) pos_of[(size_t)(order[p].i - 1) * ns2 + (order[p].j - 1)] = (int)p;
+
+    // ---- status reset for this call (cache counters stay cumulative)
+    k_init_bounds<<<1, 1, 0, st>>>(nullptr, 0, nullptr, 0, nullptr, c->status.p, 1);
+    launches += 1;
+
+    // ---- node meshes at turn start
+    if (node) build_node_meshes(c, C, S1, S2, st, launches);
+    auto node_id = [&](int dir, int src_slice0, int node1) {
+        return dir == 1 ? src_slice0 * (ns2 + 1) + (node1 - 1) : ns1 * (ns2 + 1) + src_slice0 * (ns1 + 1) + (node1 - 1);
+    };
+
+    std::vector<Task> tasks;
+    std::vector<Plane> planes;
+    std::vector<LumJob> lumjobs;
+    std::vector<int2> blockmap;
+    struct Front { int t0, nt, p0, np, l0, nl, b0, nb; long long maxsrc, maxlum; };
+    std::vector<Front> fronts;
+    const int nplanes_task = node ? (lk ? 3 : 2) : (quad ? 3 : 2);
+    std::vector<char> ran(order.size(), 0);
+    for (size_t f = 0; f < batches.size(); ++f) {
+        Front F{(int)tasks.size(), 0, (int)planes.size(), 0, (int)lumjobs.size(), 0, (int)blockmap.size(), 0, 1, 1};
+        for (const OrderEntry &pr : batches[f]) {
+            const int i = pr.i, j = pr.j;
+            if (S1.count[i - 1] == 0 || S2.count[j - 1] == 0) continue;
+            if (node) {
+                bool ok = c->h_nodes.p[node_id(1, i - 1, j)].valid && c->h_nodes.p[node_id(1, i - 1, j + 1)].valid &&
+                          c->h_nodes.p[node_id(2, j - 1, i)].valid && c->h_nodes.p[node_id(2, j - 1, i + 1)].valid;
+                if (!ok) continue;
+            }
+            const int p = pos_of[(size_t)(i - 1) * ns2 + (j - 1)];
+            ran[p] = 1;
+            for (int dir = 1; dir <= 2; ++dir) {
+                Task T{};
+                T.dir = dir; T.i = i; T.j = j;
+                T.src_beam = dir - 1;
+                T.fld_beam = 2 - dir;
+                const SliceInfo &SS = dir == 1 ? S1 : S2, &SF = dir == 1 ? S2 : S1;
+                const int ss = dir == 1 ? i - 1 : j - 1, sf = dir == 1 ? j - 1 : i - 1;
+                T.key = ((dir - 1) * ns1 + (i - 1)) * ns2 + (j - 1);
+                T.pair = p;
+                T.front = (int)f;
+                T.src_start = SS.start[ss]; T.src_n = SS.count[ss];
+                T.fld_start = SF.start[sf]; T.fld_n = SF.count[sf];
+                T.c_src = SS.center[ss];
+                T.c_fld = SF.center[sf];
+                T.lb_fld = SF.boundary[sf];
+                T.rb_fld = SF.boundary[sf + 1];
+                T.sL = 0.5 * (T.c_src - T.lb_fld);
+                T.sR = 0.5 * (T.c_src - T.rb_fld);
+                T.sM = 0.5 * (T.c_src - T.c_fld);
+                T.ks = 2.0 * (dir == 1 ? kbb2 : kbb1);
+                const double denom = T.rb_fld - T.lb_fld;  // pic_cpu.jl:1540-1548
+                if (!std::isfinite(denom) || denom == 0.0) { T.hzi = 0.0; T.zbias = 0.5; }
+                else { T.hzi = 1.0 / denom; T.zbias = T.rb_fld * T.hzi; }
+                T.nodeL = node ? node_id(dir, ss, sf + 1) : -1;
+                T.nodeR = node ? node_id(dir, ss, sf + 2) : -1;
+                T.plane0 = (int)planes.size();
+                T.nplanes = nplanes_task;
+                const int tid = (int)tasks.size();
+                const int bits = fixed_bits_for(T.src_n);
+                for (int k = 0; k < nplanes_task; ++k) {
+                    Plane P{};
+                    P.task = tid;
+                    P.src_beam = T.src_beam;
+                    P.src_start = T.src_start;
+                    P.src_n = T.src_n;
+                    P.fixed_bits = bits;
+                    if (node) {
+                        // L: sL on gL ; R: sR on gR ; Z: sR on gL (pic_cpu.jl:1506-1516)
+                        P.kind = k == 0 ? 0 : (k == 1 ? 1 : 3);
+                        P.s = k == 0 ? T.sL : T.sR;
+                        P.geom = (k == 1) ? T.nodeR : T.nodeL;
+                        P.green = P.geom;
+                        P.count_dropped = k < 2 ? 1 : 0;
+                    } else {
+                        P.kind = k == 0 ? 0 : (k == 1 ? 1 : 2);
+                        P.s = k == 0 ? T.sL : (k == 1 ? T.sR : 0.5 * (T.sL + T.sR));
+                        P.geom = -1;
+                        P.green = -1;
+                        P.count_dropped = 0;
+                    }
+                    planes.push_back(P);
+                }
+                for (long long off = 0; off < T.fld_n; off += 256) blockmap.push_back(make_int2(tid, (int)off));
+                F.maxsrc = std::max<long long>(F.maxsrc, T.src_n);
+                tasks.push_back(T);
+            }
+            if (compute_lum) {
+                LumJob J{};
+                J.pair = p;
+                J.s1_start = S1.start[i - 1]; J.s1_n = S1.count[i - 1];
+                J.s2_start = S2.start[j - 1]; J.s2_n = S2.count[j - 1];
+                J.sM1 = 0.5 * (S1.center[i - 1] - S2.center[j - 1]);
+                J.sM2 = 0.5 * (S2.center[j - 1] - S1.center[i - 1]);
+                J.bits1 = fixed_bits_for(J.s1_n);
+                J.bits2 = fixed_bits_for(J.s2_n);
+                F.maxlum = std::max<long long>(F.maxlum, std::max<long long>(J.s1_n, J.s2_n));
+                lumjobs.push_back(J);
+            }
+        }
+        F.nt = (int)tasks.size() - F.t0;
+        F.np = (int)planes.size() - F.p0;
+        F.nl = (int)lumjobs.size() - F.l0;
+        F.nb = (int)blockmap.size() - F.b0;
+        if (F.nt) fronts.push_back(F);
+    }
+    const int ntasks = (int)tasks.size();
+    const int npairs_total = (int)order.size();
+    int max_planes = 1, max_lum = 1;
+    for (auto &F : fronts) { max_planes = std::max(max_planes, F.np); max_lum = std::max(max_lum, F.nl); }
+
+    // ---- device buffers and one upload of the whole schedule
+    c->tasks.ensure(std::max(ntasks, 1));
+    c->planes.ensure(std::max<size_t>(planes.size(), 1));
+    c->lumjobs.ensure(std::max<size_t>(lumjobs.size(), 1));
+    c->geom.ensure(std::max(ntasks, 1));
+    c->blockmap.ensure(std::max<size_t>(blockmap.size(), 1));
+    c->bnd.ensure((size_t)std::max(ntasks, 1) * 8);
+    c->nanflag.ensure(std::max(ntasks, 1));
+    c->lumb.ensure((size_t)std::max(npairs_total, 1) * 4);
+    c->lumgeom.ensure(std::max(npairs_total, 1));
+    c->lum_parts.ensure(std::max(npairs_total, 1));
+    const size_t cells = (size_t)nx * ny;
+    const size_t lcells = (size_t)(lnx + 1) * (lny + 1);
+    if (c->qgrid.n < (size_t)max_planes * cells) {
+        c->qgrid.ensure((size_t)max_planes * cells);
+        CK(cudaMemsetAsync(c->qgrid.p, 0, sizeof(long long) * c->qgrid.n, st));
+    }
+    c->spec.ensure((size_t)max_planes * (nx + 1) * ny);
+    c->fields.ensure((size_t)max_planes * 3 * cells);
+    if (c->lq.n < (size_t)2 * max_lum * lcells) {
+        c->lq.ensure((size_t)2 * max_lum * lcells);
+        CK(cudaMemsetAsync(c->lq.p, 0, sizeof(long long) * c->lq.n, st));
+    }
+    const size_t bytes = sizeof(Task) * tasks.size() + sizeof(Plane) * planes.size() + sizeof(LumJob) * lumjobs.size() +
+                         sizeof(int2) * blockmap.size() + 64;
+    c->stage.ensure(bytes);
+    char *h = c->stage.p;
+    auto put = [&](void *dst, const void *src, size_t nbytes) {
+        if (!nbytes) return;
+        std::memcpy(h, src, nbytes);
+        CK(cudaMemcpyAsync(dst, h, nbytes, cudaMemcpyHostToDevice, st));
+        h += nbytes;
+    };
+    put(c->tasks.p, tasks.data(), sizeof(Task) * tasks.size());
+    put(c->planes.p, planes.data(), sizeof(Plane) * planes.size());
+    put(c->lumjobs.p, lumjobs.data(), sizeof(LumJob) * lumjobs.size());
+    put(c->blockmap.p, blockmap.data(), sizeof(int2) * blockmap.size());
+    CK(cudaMemsetAsync(c->lum_parts.p, 0, sizeof(double) * npairs_total, st));
+    k_init_bounds<<<(std::max(ntasks, npairs_total) + 255) / 256, 256, 0, st>>>(c->bnd.p, ntasks, c->lumb.p, npairs_total,
+                                                                                c->nanflag.p, c->status.p, 0);
+    launches += 1;
+    C.tasks = c->tasks.p;
+    C.planes = c->planes.p;
+    C.lumjobs = c->lumjobs.p;
+    C.geom = c->geom.p;
+    C.lumgeom = c->lumgeom.p;
+    C.bnd = c->bnd.p;
+    C.lumb = c->lumb.p;
+    C.nanflag = c->nanflag.p;
+    C.qgrid = c->qgrid.p;
+    C.spec = c->spec.p;
+    C.fields = c->fields.p;
+    C.lq = c->lq.p;
+    C.lum_parts = c->lum_parts.p;
+    C.nodes = c->nodes.p;
+
+    const bool dep_smem = cells * sizeof(long long) <= kSmemLimit;
+    const bool lum_smem = lcells * sizeof(long long) <= kSmemLimit;
+    const size_t dep_bytes = dep_smem ? cells * sizeof(long long) : 0;
+    const size_t lum_bytes = lum_smem ? lcells * sizeof(long long) : 0;
+
+    // ---- wavefronts
+    for (const Front &F : fronts) {
+        const int npf = F.nt / 2;
+        if (!node || compute_lum) {
+            unsigned bps = (unsigned)std::max<long long>(1, std::min<long long>(32, (F.maxsrc + 8191) / 8192));
+            k_pair_bounds<<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
+            launches++;
+        }
+        if (!node) {
+            k_plan<<<(F.nt + 63) / 64, 64, 0, st>>>(C, F.t0, F.nt, 0);
+            k_green_rows<<<dim3((NY / 2 + 3) / 4, F.nt), 128, fft_smem(NX), st>>>(C, 0, F.t0, 0);
+            k_green_cols<<<dim3((nx + 1 + 3) / 4, F.nt), 128, fft_smem(NY), st>>>(C, 0, F.t0, 0);
+            launches += 3;
+        }
+        if (compute_lum && F.nl) {
+            k_lum_plan<<<(F.nl + 63) / 64, 64, 0, st>>>(C, F.l0, F.nl, F.t0);
+            unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(16, (F.maxlum + 16383) / 16384));
+            launch_method(lmethod, [&](auto M) {
+                k_lum_deposit<decltype(M)::value><<<dim3(bpp, 2 * F.nl), 512, lum_bytes, st>>>(C, F.l0, lum_smem ? 1 : 0);
+            });
+            k_lum_overlap<<<F.nl, 256, 0, st>>>(C, F.l0);
+            launches += 3;
+        }
+        {
+            unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(16, (F.maxsrc + 16383) / 16384));
+            launch_method(method, [&](auto M) {
+                k_deposit<decltype(M)::value><<<dim3(bpp, F.np), 512, dep_bytes, st>>>(C, F.p0, dep_smem ? 1 : 0);
+            });
+            k_conv_rows<<<dim3((ny / 2 + 3) / 4, F.np), 128, fft_smem(NX), st>>>(C, F.p0);
+            k_conv_cols<<<dim3((nx + 1 + 3) / 4, F.np), 128, fft_smem(NY), st>>>(C, F.p0);
+            k_conv_field<<<dim3((ny + kFieldTile - 1) / kFieldTile, F.np), 128, field_smem(NX), st>>>(C, F.p0);
+            launch_method(method, [&](auto M) {
+                k_kick<decltype(M)::value><<<F.nb, 256, 0, st>>>(C, F.p0, c->blockmap.p + F.b0);
+            });
+            launches += 5;
+        }
+    }
+    CK(cudaGetLastError());
+
+    // ---- back to caller order
+    for (int b = 0; b < 2; ++b) {
+        const BeamWS &W = c->bw[b];
+        const octo_beam &B = b == 0 ? *b1 : *b2;
+        k_unsort<<<(unsigned)((W.total + 255) / 256), 256, 0, st>>>(
+            W.perm.p, W.total, W.s[0].p, W.s[1].p, W.s[2].p, W.s[3].p, W.s[4].p, W.s[5].p, (double *)B.x,
+            (double *)B.px, (double *)B.y, (double *)B.py, (double *)B.z, (double *)B.pz, W.info.p);
+        launches++;
+    }
+    c->h_lum.ensure(std::max(npairs_total, 1));
+    c->h_status.ensure(1);
+    CK(cudaMemcpyAsync(c->h_lum.p, c->lum_parts.p, sizeof(double) * npairs_total, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(c->h_status.p, c->status.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    const DevStatus DS = *c->h_status.p;
+    c->last_launches = launches;
+    if (rep) {
+        rep->n_batches = (int)batches.size();
+        rep->turn = turn;
+        rep->dropped = DS.dropped;
+        rep->green_hits = DS.hits;
+        rep->green_misses = DS.misses;
+        rep->green_rebuilds = DS.rebuilds;
+        rep->kernel_launches = launches;
+    }
+    if (DS.first_bad != ~0ull) {
+        const int t = (int)(DS.first_bad >> 16), code = (int)((DS.first_bad >> 8) & 0xff), role = (int)(DS.first_bad & 0xff);
+        char m[256];
+        if (code == OCTO_ERR_NONFINITE && t < ntasks) {
+            const Task &T = tasks[t];
+            if (rep) { rep->role = role; rep->pair_i = T.i; rep->pair_j = T.j; rep->direction = T.dir; }
+            const octo_beam &B = (role == 1 ? T.src_beam : T.fld_beam) == 0 ? *b1 : *b2;
+            long long first = first_nonfinite_host(B, st, false);
+            if (rep) rep->first_index = first + 1;
+            snprintf(m, sizeof m, "non-finite %s coordinate at particle %lld of beam%d (slice pair (%d, %d), direction %d, turn %lld)",
+                     role == 1 ? "source" : "field", first + 1, (role == 1 ? T.src_beam : T.fld_beam) + 1, T.i, T.j, T.dir,
+                     (long long)turn);
+            throw OctoFail{OCTO_ERR_NONFINITE, m};
+        }
+        snprintf(m, sizeof m, "PIC interaction grid requires finite, positive transverse extents; supply a positive "
+                              "min_transverse_extent for every degenerate axis (turn %lld)", (long long)turn);
+        throw OctoFail{code ? code : OCTO_ERR_EXTENT, m};
+    }
+    // luminosity fold in collision order (pic_cpu.jl:258-271)
+    c->trace_i.clear(); c->trace_j.clear(); c->trace_lum.clear();
+    double lum = NAN;
+    if (compute_lum) {
+        lum = 0.0;
+        for (size_t p = 0; p < order.size(); ++p) {
+            if (!ran[p]) continue;
+            lum += c->h_lum.p[p];
+            c->trace_i.push_back(order[p].i);
+            c->trace_j.push_back(order[p].j);
+            c->trace_lum.push_back(c->h_lum.p[p]);
+        }
+    }
+    return lum;
+}
+
+int fail(octo_ctx *c, int code, const std::string &m) {
+    if (c) c->err = m;
+    return code;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+int32_t octo_version(void) { return 1; }
+
+double octo_erfinv(double x) { return erfinv_host(x); }
+
+double octo_normal_quantile(int32_t s, int32_t ns) {
+    return std::sqrt(2.0) * erfinv_host((double)(2 * s) / (double)ns - 1.0);
+}
+
+octo_ctx *octo_create(int32_t device, const octo_pic_options *options) {
+    if (!options) return nullptr;
+    octo_ctx *c = new octo_ctx();
+    c->device = device;
+    c->opt = *options;
+    std::string msg;
+    int rc = validate_options(c->opt, msg);
+    if (rc != OCTO_OK) { c->err = msg; c->opt.nx = 0; return c; }
+    for (int b = 0; b < 2; ++b) {
+        int ns = b == 0 ? options->nslices1 : options->nslices2;
+        const double *p = b == 0 ? options->positions1 : options->positions2;
+        int m = b == 0 ? options->slicing_method1 : options->slicing_method2;
+        if (m == OCTO_SLICING_SPECIFIED && p) c->pos[b].assign(p, p + (ns - 1));
+        c->ns[b] = ns;
+    }
+    c->opt.positions1 = nullptr;
+    c->opt.positions2 = nullptr;
+    DevOptions &d = c->dopt;
+    d.nx = options->nx; d.ny = options->ny;
+    d.method = options->deposit_method;
+    d.lum_method = options->lum_deposit_method < 0 ? options->deposit_method : options->lum_deposit_method;
+    d.lnx = options->lum_nx > 0 ? options->lum_nx : options->nx;
+    d.lny = options->lum_ny > 0 ? options->lum_ny : options->ny;
+    d.green_type = options->green_type;
+    d.green_cache = options->green_cache;
+    d.fourth = options->field_derivative == 4;
+    d.quadratic = options->slice_interpolation == 1;
+    d.node = options->interaction_grid == OCTO_GRID_NODE;
+    d.longitudinal_kick = options->longitudinal_kick;
+    d.min_ex = options->min_extent_x;
+    d.min_ey = options->min_extent_y;
+    d.quantize = options->grid_quantize;
+    d.min_ratio = options->green_min_ratio;
+    d.growth = options->green_growth;
+    try {
+        CK(cudaSetDevice(device));
+        upload_twiddles(c->tw_x, 2 * options->nx);
+        upload_twiddles(c->tw_y, 2 * options->ny);
+        c->gstride = (long long)(options->nx + 1) * 2 * options->ny;
+        for (int b = 0; b < 2; ++b) {
+            int ns = c->ns[b];
+            int m = b == 0 ? options->slicing_method1 : options->slicing_method2;
+            std::vector<double> q(kMaxSlices + 1, 0.0);
+            for (int s = 1; s <= ns - 1; ++s)
+                q[s] = m == OCTO_SLICING_NORMAL_QUANTILE ? std::sqrt(2.0) * erfinv_host((double)(2 * s) / (double)ns - 1.0)
+                                                         : c->pos[b][s - 1];
+            c->bw[b].q.ensure(kMaxSlices + 1);
+            CK(cudaMemcpy(c->bw[b].q.p, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice));
+        }
+        size_t dep = (size_t)options->nx * options->ny * sizeof(long long);
+        size_t lum = (size_t)(d.lnx + 1) * (d.lny + 1) * sizeof(long long);
+        int dsm = (int)std::min(dep, kSmemLimit), lsm = (int)std::min(lum, kSmemLimit);
+        CK(cudaFuncSetAttribute(k_deposit<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
+        CK(cudaFuncSetAttribute(k_deposit<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
+        CK(cudaFuncSetAttribute(k_lum_deposit<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
+        CK(cudaFuncSetAttribute(k_lum_deposit<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
+        int fx = (int)fft_smem(2 * options->nx), fy = (int)fft_smem(2 * options->ny), ff = (int)field_smem(2 * options->nx);
+        CK(cudaFuncSetAttribute(k_green_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, fx));
+        CK(cudaFuncSetAttribute(k_green_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, fy));
+        CK(cudaFuncSetAttribute(k_conv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, fx));
+        CK(cudaFuncSetAttribute(k_conv_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, fy));
+        CK(cudaFuncSetAttribute(k_conv_field, cudaFuncAttributeMaxDynamicSharedMemorySize, ff));
+    } catch (CudaFail &e) {
+        c->err = e.msg;
+        c->opt.nx = 0;
+    }
+    return c;
+}
+
+void octo_destroy(octo_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaDeviceSynchronize();
+    for (auto &b : c->bw) b.release();
+    c->tw_x.release(); c->tw_y.release(); c->tasks.release(); c->planes.release(); c->lumjobs.release();
+    c->geom.release(); c->blockmap.release(); c->cache.release(); c->nodes.release(); c->lumgeom.release();
+    c->bnd.release(); c->lumb.release(); c->nodebox_s.release(); c->nodebox_f.release(); c->nanflag.release();
+    c->nodenan.release(); c->status.release(); c->ghat.release(); c->qgrid.release(); c->lq.release();
+    c->spec.release(); c->fields.release(); c->lum_parts.release(); c->node_ref.release(); c->stats.release();
+    c->partial.release(); c->soa_ptrs.release();
+    c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_nodes.release();
+    delete c;
+}
+
+int32_t octo_pic_collide(octo_ctx *c, octo_beam *beam1, octo_beam *beam2, const octo_beam_params *p1,
+                         const octo_beam_params *p2, int64_t turn, int32_t compute_luminosity, double *luminosity,
+                         octo_collide_report *report, void *stream) {
+    if (!c) return OCTO_ERR_ARG;
+    if (report) { std::memset(report, 0, sizeof(*report)); report->turn = turn; }
+    if (c->opt.nx == 0) return fail(c, OCTO_ERR_UNSUPPORTED, c->err.empty() ? "invalid context" : c->err);
+    try {
+        double lum = collide_impl(c, beam1, beam2, p1, p2, turn, compute_luminosity, report, (cudaStream_t)stream);
+        if (luminosity) *luminosity = lum;
+        c->err.clear();
+        if (report) report->status = OCTO_OK;
+        return OCTO_OK;
+    } catch (OctoFail &e) {
+        if (report) report->status = e.code;
+        return fail(c, e.code, e.msg);
+    } catch (CudaFail &e) {
+        if (report) report->status = OCTO_ERR_CUDA;
+        return fail(c, OCTO_ERR_CUDA, e.msg);
+    }
+}
+
+int32_t octo_green_cache_stats(octo_ctx *c, int64_t *hits, int64_t *misses, int64_t *rebuilds) {
+    if (!c) return OCTO_ERR_ARG;
+    DevStatus s{};
+    if (c->status.p) {
+        if (cudaMemcpy(&s, c->status.p, sizeof s, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return fail(c, OCTO_ERR_CUDA, "reading the Green-cache counters failed");
+    }
+    if (hits) *hits = s.hits;
+    if (misses) *misses = s.misses;
+    if (rebuilds) *rebuilds = s.rebuilds;
+    return OCTO_OK;
+}
+
+int64_t octo_pair_luminosity_trace(octo_ctx *c, int32_t *pi, int32_t *pj, double *lum, int64_t cap) {
+    if (!c) return 0;
+    int64_t n = (int64_t)c->trace_lum.size();
+    for (int64_t k = 0; k < n && k < cap; ++k) {
+        if (pi) pi[k] = c->trace_i[k];
+        if (pj) pj[k] = c->trace_j[k];
+        if (lum) lum[k] = c->trace_lum[k];
+    }
+    return n;
+}
+
+int32_t octo_linear6d(octo_ctx *c, octo_beam *beam, const double matrix[36], int32_t turns, void *stream) {
+    if (!c || !beam || !matrix) return OCTO_ERR_ARG;
+    std::string msg;
+    int rc = check_beam(beam, msg);
+    if (rc != OCTO_OK) return fail(c, rc, msg);
+    try {
+        CK(cudaSetDevice(c->device));
+        Mat6 M;
+        for (int k = 0; k < 36; ++k) M.m[k] = matrix[k];
+        k_linear6d<<<(unsigned)((beam->n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+            (double *)beam->x, (double *)beam->px, (double *)beam->y, (double *)beam->py, (double *)beam->z,
+            (double *)beam->pz, beam->n, M, turns);
+        CK(cudaGetLastError());
+        return OCTO_OK;
+    } catch (CudaFail &e) {
+        return fail(c, OCTO_ERR_CUDA, e.msg);
+    }
+}
+
+int32_t octo_beam_gaussian(octo_ctx *c, octo_beam *beam, uint64_t seed, uint64_t rng_id, const double beta[3],
+                           const double alpha[3], const double sigma[3], double cutoff, void *stream) {
+    if (!c || !beam || !beta || !alpha || !sigma) return OCTO_ERR_ARG;
+    std::string msg;
+    int rc = check_beam(beam, msg);
+    if (rc != OCTO_OK) return fail(c, rc, msg);
+    cudaStream_t st = (cudaStream_t)stream;
+    try {
+        CK(cudaSetDevice(c->device));
+        const long long n = beam->n;
+        double *comp[6] = {(double *)beam->x, (double *)beam->px, (double *)beam->y, (double *)beam->py,
+                           (double *)beam->z, (double *)beam->pz};
+        const int nb = 256;
+        c->partial.ensure(nb);
+        c->stats.ensure(kMaxSlices * 2);
+        double *stats = c->stats.p;
+        for (int d = 0; d < 6; ++d) {
+            k_beam_normals<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(comp[d], n, seed, rng_id, d + 1, cutoff);
+            k_partial_sum<<<nb, 256, 0, st>>>(comp[d], n, stats, 0, c->partial.p);
+            k_fold_partials<<<1, 1, 0, st>>>(c->partial.p, nb, n, 0, stats);
+            k_partial_sum<<<nb, 256, 0, st>>>(comp[d], n, stats, 1, c->partial.p);
+            k_fold_partials<<<1, 1, 0, st>>>(c->partial.p, nb, n, 1, stats);
+            k_standardize<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(comp[d], n, stats);
+        }
+        for (int a = 0; a < 3; ++a)
+            k_twiss<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(comp[2 * a], comp[2 * a + 1], n, sigma[a], beta[a], alpha[a]);
+        CK(cudaGetLastError());
+        return OCTO_OK;
+    } catch (CudaFail &e) {
+        return fail(c, OCTO_ERR_CUDA, e.msg);
+    }
+}
+
+int32_t octo_last_error(octo_ctx *c, char *buf, int64_t len) {
+    if (!c || !buf || len <= 0) return OCTO_ERR_ARG;
+    size_t n = std::min<size_t>(c->err.size(), (size_t)len - 1);
+    std::memcpy(buf, c->err.data(), n);
+    buf[n] = 0;
+    return OCTO_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,192 @@
+// Internal types and device helpers shared by the libocto_b200 translation units.
+//
+// Precision contract of this FP64 build: the library is compiled with -fmad=false, so
+// every scalar expression below rounds exactly like the reference's (Julia does not
+// contract a*b+c).  Grid geometry and Green-cache decisions therefore come out bit-equal
+// to the reference's on equal inputs, and fixed-point charge grids bit-equal to the CPU
+// restatement's.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+
+namespace octo {
+
+constexpr int kFoldLanes = 4096;           // slicing.jl:223 (_SLICE_FOLD_LANES)
+constexpr int kMaxSlices = 64;
+constexpr double kTemplateMarginCells = 1.5;  // interface.jl:674
+
+struct Grid {
+    double x0, y0, w, h;
+};
+
+// One directed interaction of a slice pair: `src` slice sources the field that kicks `fld`.
+// Direction 1: source = beam 1 slice i, field = beam 2 slice j; direction 2 the reverse
+// (pic_cpu.jl:364-377).
+struct Task {
+    int32_t dir, i, j;           // 1-based pair, direction
+    int32_t src_beam, fld_beam;  // 0 / 1
+    int32_t key;                 // Green-cache slot ((dir-1)*S1 + i-1)*S2 + j-1
+    int32_t nodeL, nodeR;        // node-mesh ids (interaction_grid = :node), else -1
+    int32_t pair;                // position in collision order
+    int32_t front;               // wavefront index
+    int32_t plane0, nplanes;     // field-solve planes of this task
+    int64_t src_start, src_n, fld_start, fld_n;  // ranges in the slice-sorted arrays
+    double c_src, c_fld, lb_fld, rb_fld;
+    double sL, sR, sM, ks, hzi, zbias;
+};
+
+// One deposit+solve plane.  kind: 0 = L (sL), 1 = R (sR), 2 = M (midpoint), 3 = Z (:node, sR on gL).
+struct Plane {
+    int32_t task, kind;
+    int32_t geom;        // node mesh id, or -1 to use the task's planned source grid
+    int32_t green;       // Green slot (resolved on the device for slice-pair tasks when -1)
+    int32_t fixed_bits;  // fixed-point scale of the int64 charge grid
+    int32_t count_dropped;
+    int32_t src_beam;
+    int32_t pad;
+    int64_t src_start, src_n;
+    double s;            // drift of the deposit
+};
+
+// Planned geometry of a slice-pair task (written by the plan kernel).
+struct TaskGeom {
+    Grid sg, fg;
+    int32_t green;       // Green slot used
+    int32_t rebuild;     // 1 when this task (re)builds its Green slot in this front
+};
+
+struct CacheEntry {
+    Grid sg, fg;
+    int32_t valid;
+    int32_t rebuilds;
+    int64_t uses;
+};
+
+struct NodeMesh {
+    Grid sg, fg;
+    int32_t valid;
+    int32_t pad;
+};
+
+// Luminosity of one slice pair (pic_cpu.jl:2700-2736).
+struct LumJob {
+    int32_t pair;
+    int32_t bits1, bits2;
+    int32_t pad;
+    int64_t s1_start, s1_n, s2_start, s2_n;  // beam-1 slice i, beam-2 slice j
+    double sM1, sM2;
+};
+
+struct LumGeom {
+    double x0, y0, hx, hy;
+    int32_t ok;
+    int32_t pad;
+};
+
+// Cumulative device counters and the first error.
+struct DevStatus {
+    unsigned long long first_bad;   // (task index << 1) | 0 ; ~0ull when none
+    int32_t code;
+    int32_t role;
+    long long hits, misses, rebuilds;
+    long long dropped;
+};
+
+// ---------------------------------------------------------------- ordered doubles
+// Monotone map double -> uint64 so integer atomicMin/atomicMax order doubles the way
+// Julia's min/max do (-0.0 < +0.0).  NaN never enters: callers flag it separately.
+__host__ __device__ inline unsigned long long ord_encode(double v) {
+    unsigned long long u;
+    memcpy(&u, &v, 8);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__host__ __device__ inline double ord_decode(unsigned long long u) {
+    u = (u >> 63) ? (u & 0x7fffffffffffffffull) : ~u;
+    double v;
+    memcpy(&v, &u, 8);
+    return v;
+}
+constexpr unsigned long long kOrdMinInit = 0xffffffffffffffffull;  // decodes to NaN -> "+inf" sentinel
+constexpr unsigned long long kOrdMaxInit = 0x0000000000000000ull;
+
+// Julia semantics (base/math.jl): NaN-propagating, -0.0 < +0.0.
+__host__ __device__ inline double jmin(double a, double b) {
+    if (a != a || b != b) return a - b;
+    if (a < b) return a;
+    if (b < a) return b;
+    return signbit(a) ? a : b;
+}
+__host__ __device__ inline double jmax(double a, double b) {
+    if (a != a || b != b) return a - b;
+    if (a > b) return a;
+    if (b > a) return b;
+    return signbit(a) ? b : a;
+}
+// Julia clamp(x, lo, hi) = ifelse(x > hi, hi, ifelse(x < lo, lo, x)).
+__host__ __device__ inline double jclamp(double x, double lo, double hi) {
+    return x > hi ? hi : (x < lo ? lo : x);
+}
+
+// ---------------------------------------------------------------- weights
+// CIC (pic_cpu.jl:2182-2197): 1-based base, zero weights outside [0, n-1] or non-finite.
+__device__ __forceinline__ void cic_weights(double u, int n, int &base, double w[2]) {
+    if (!(0.0 <= u && u <= (double)(n - 1))) {
+        base = 1; w[0] = 0.0; w[1] = 0.0;
+        return;
+    }
+    long b = (long)floor(u) + 1;
+    b = b < 1 ? 1 : (b > n - 1 ? n - 1 : b);
+    base = (int)b;
+    double f = jclamp(u - (double)(base - 1), 0.0, 1.0);
+    w[0] = 1.0 - f;
+    w[1] = f;
+}
+
+// TSC (pic_cpu.jl:2225-2252).
+__device__ __forceinline__ void tsc_weights(double u, int n, int &base, double w[3]) {
+    if (!(0.0 <= u && u <= (double)(n - 1))) {
+        base = 1; w[0] = 0.0; w[1] = 0.0; w[2] = 0.0;
+        return;
+    }
+    double fl = floor(u);
+    long ix = (long)fl;
+    double f = u - fl;
+    long b;
+    if (f < 0.5) {
+        double t = f * f;
+        w[0] = 0.125 + 0.5 * (t - f);
+        w[1] = 0.75 - t;
+        w[2] = 0.125 + 0.5 * (t + f);
+        b = ix;
+    } else {
+        double fr = 1.0 - f;
+        double t = fr * fr;
+        w[0] = 0.125 + 0.5 * (t + fr);
+        w[1] = 0.75 - t;
+        w[2] = 0.125 + 0.5 * (t - fr);
+        b = ix + 1;
+    }
+    b = b < 1 ? 1 : (b > n - 2 ? n - 2 : b);
+    base = (int)b;
+}
+
+// Fixed-point scale: taps are rounded to multiples of 2^-bits with
+// bits = min(40, 62 - bitlength(nsrc)), so a whole slice fits one int64 cell.
+inline int fixed_bits_for(int64_t n) {
+    int bl = 0;
+    uint64_t v = (uint64_t)(n < 1 ? 1 : n);
+    while (v) { ++bl; v >>= 1; }
+    int b = 62 - bl;
+    return b > 40 ? 40 : b;
+}
+
+// ---------------------------------------------------------------- options (device copy)
+struct DevOptions {
+    int nx, ny, method, lum_method, lnx, lny;
+    int green_type, green_cache, fourth, quadratic, node, longitudinal_kick;
+    double min_ex, min_ey, quantize, min_ratio, growth;
+};
+
+}  // namespace octo

@@ -1,0 +1,119 @@
+"""ctypes binding of libocto_b200.so (include/octo_b200.h).
+
+The library is built in-tree (``octopus.jl_b200/build/libocto_b200.so``) by
+``octopus.jl_b200/build.py``.  Loading fails loudly when it is missing: there is no
+CPU fallback for the collision.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "build", "libocto_b200.so")
+
+OCTO_OK, OCTO_ERR_NONFINITE, OCTO_ERR_UNSUPPORTED, OCTO_ERR_EXTENT, OCTO_ERR_ARG, OCTO_ERR_CUDA, OCTO_ERR_TIMEOUT = range(7)
+
+ERROR_NAMES = {
+    OCTO_ERR_NONFINITE: "NONFINITE", OCTO_ERR_UNSUPPORTED: "UNSUPPORTED", OCTO_ERR_EXTENT: "EXTENT",
+    OCTO_ERR_ARG: "ARG", OCTO_ERR_CUDA: "CUDA", OCTO_ERR_TIMEOUT: "TIMEOUT",
+}
+
+# Every symbol include/octo_b200.h declares.
+EXPORTS = (
+    "octo_create", "octo_destroy", "octo_pic_collide", "octo_green_cache_stats",
+    "octo_pair_luminosity_trace", "octo_linear6d", "octo_beam_gaussian", "octo_last_error",
+    "octo_normal_quantile", "octo_erfinv", "octo_version",
+)
+
+
+class OctoBeam(C.Structure):
+    _fields_ = [("n", C.c_int64), ("dtype", C.c_int32), ("reserved", C.c_int32),
+                ("x", C.c_void_p), ("px", C.c_void_p), ("y", C.c_void_p),
+                ("py", C.c_void_p), ("z", C.c_void_p), ("pz", C.c_void_p)]
+
+
+class OctoBeamParams(C.Structure):
+    _fields_ = [("charge", C.c_double), ("mc2", C.c_double), ("E0", C.c_double),
+                ("r0", C.c_double), ("npart", C.c_double)]
+
+
+class OctoPicOptions(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32),
+        ("deposit_method", C.c_int32), ("lum_deposit_method", C.c_int32),
+        ("lum_nx", C.c_int32), ("lum_ny", C.c_int32),
+        ("green_type", C.c_int32), ("green_cache", C.c_int32),
+        ("field_derivative", C.c_int32), ("slice_interpolation", C.c_int32),
+        ("interaction_grid", C.c_int32), ("grid_extent", C.c_int32),
+        ("grid_extent_sigma", C.c_double),
+        ("min_extent_x", C.c_double), ("min_extent_y", C.c_double),
+        ("grid_quantize", C.c_double),
+        ("green_min_ratio", C.c_double), ("green_growth", C.c_double),
+        ("longitudinal_kick", C.c_int32),
+        ("slicing_method1", C.c_int32), ("slicing_method2", C.c_int32),
+        ("nslices1", C.c_int32), ("nslices2", C.c_int32),
+        ("center_position1", C.c_int32), ("center_position2", C.c_int32),
+        ("positions1", C.POINTER(C.c_double)), ("positions2", C.POINTER(C.c_double)),
+        ("has_kbb1", C.c_int32), ("has_kbb2", C.c_int32), ("has_lum_scale", C.c_int32),
+        ("kbb1", C.c_double), ("kbb2", C.c_double), ("lum_scale", C.c_double),
+        ("precision", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+    ]
+
+
+class OctoCollideReport(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32), ("role", C.c_int32), ("pair_i", C.c_int32), ("pair_j", C.c_int32),
+        ("direction", C.c_int32), ("n_batches", C.c_int32), ("turn", C.c_int64), ("first_index", C.c_int64),
+        ("dropped", C.c_int64), ("green_hits", C.c_int64), ("green_misses", C.c_int64),
+        ("green_rebuilds", C.c_int64), ("kernel_launches", C.c_int64),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load libocto_b200.so; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"libocto_b200.so not found at {LIB_PATH}; build it with `python octopus.jl_b200/build.py` "
+            "(the collision has no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64, d, u64 = C.c_void_p, C.c_int32, C.c_int64, C.c_double, C.c_uint64
+    P = C.POINTER
+    L.octo_create.restype = vp
+    L.octo_create.argtypes = [i32, P(OctoPicOptions)]
+    L.octo_destroy.restype = None
+    L.octo_destroy.argtypes = [vp]
+    L.octo_pic_collide.restype = i32
+    L.octo_pic_collide.argtypes = [vp, P(OctoBeam), P(OctoBeam), P(OctoBeamParams), P(OctoBeamParams), i64, i32,
+                                   P(d), P(OctoCollideReport), vp]
+    L.octo_green_cache_stats.restype = i32
+    L.octo_green_cache_stats.argtypes = [vp, P(i64), P(i64), P(i64)]
+    L.octo_pair_luminosity_trace.restype = i64
+    L.octo_pair_luminosity_trace.argtypes = [vp, P(i32), P(i32), P(d), i64]
+    L.octo_linear6d.restype = i32
+    L.octo_linear6d.argtypes = [vp, P(OctoBeam), P(d), i32, vp]
+    L.octo_beam_gaussian.restype = i32
+    L.octo_beam_gaussian.argtypes = [vp, P(OctoBeam), u64, u64, P(d), P(d), P(d), d, vp]
+    L.octo_last_error.restype = i32
+    L.octo_last_error.argtypes = [vp, C.c_char_p, i64]
+    L.octo_normal_quantile.restype = d
+    L.octo_normal_quantile.argtypes = [i32, i32]
+    L.octo_erfinv.restype = d
+    L.octo_erfinv.argtypes = [d]
+    L.octo_version.restype = i32
+    L.octo_version.argtypes = []
+    _lib = L
+    return L
+
+
+def last_error(ctx) -> str:
+    buf = C.create_string_buffer(1024)
+    lib().octo_last_error(ctx, buf, len(buf))
+    return buf.value.decode(errors="replace")

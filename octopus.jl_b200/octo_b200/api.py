@@ -1,0 +1,184 @@
+"""``collide`` -- the drop-in for Octopus.jl's ``collide!(::PICPoissonSolver, beam1, beam2, backend[, ctx])``
+(interface.jl:13-74, 508-509), running on libocto_b200.
+
+The bare call builds a fresh context (cold Green cache) per call, as the reference's public
+``collide!`` does (pic_cpu.jl:1-21).  Passing a ``StrongStrongRuntime`` keeps the context and
+its slice-pair Green cache across calls, as ``task.runtime_cache`` does on the task path
+(pic_cpu.jl:23-32, 499-515).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+from typing import Dict, Optional, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib
+from .beam import Beam
+from .solver import ArgumentError, LongitudinalSlicing, PICPoissonSolver
+
+
+class CUDABackend:
+    """Backend tag (src/Octopus.jl:10-25)."""
+
+
+class CollisionError(ArgumentError):
+    """Raised for a failed collide; ``code`` is the OCTO_* status, ``report`` the collide report."""
+
+    def __init__(self, code: int, message: str, report=None):
+        super().__init__(message)
+        self.code = code
+        self.report = report
+
+
+@dataclass
+class TrackingContext:
+    """The subset of TrackingContext the collision reads: the turn (for messages and schedules)."""
+    turn: int = -1
+
+
+class Context:
+    """One libocto_b200 context: device workspaces plus the slice-pair Green cache."""
+
+    def __init__(self, solver: PICPoissonSolver, device: int = 0):
+        self.solver = solver
+        self.device = device
+        self._opts = solver.to_c()
+        self._ptr = _lib.lib().octo_create(int(device), C.byref(self._opts))
+        if not self._ptr:
+            raise RuntimeError("octo_create failed")
+        self.last_report = None
+
+    def close(self):
+        if getattr(self, "_ptr", None):
+            _lib.lib().octo_destroy(self._ptr)
+            self._ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def ptr(self):
+        return self._ptr
+
+    def collide(self, beam1: Beam, beam2: Beam, turn: int = -1, compute_luminosity: bool = True,
+                stream: Optional[torch.cuda.Stream] = None) -> float:
+        b1, b2 = beam1.to_c(), beam2.to_c()
+        p1, p2 = beam1.params.to_c(), beam2.params.to_c()
+        lum = C.c_double(float("nan"))
+        rep = _lib.OctoCollideReport()
+        st = (stream or torch.cuda.current_stream(beam1.coords.device)).cuda_stream
+        rc = _lib.lib().octo_pic_collide(self._ptr, C.byref(b1), C.byref(b2), C.byref(p1), C.byref(p2), int(turn),
+                                         int(bool(compute_luminosity)), C.byref(lum), C.byref(rep), C.c_void_p(st))
+        self.last_report = rep
+        if rc != _lib.OCTO_OK:
+            raise CollisionError(rc, f"{_lib.ERROR_NAMES.get(rc, rc)}: {_lib.last_error(self._ptr)}", rep)
+        return lum.value
+
+    def green_cache_stats(self) -> Tuple[int, int, int]:
+        h, m, r = C.c_int64(), C.c_int64(), C.c_int64()
+        _lib.lib().octo_green_cache_stats(self._ptr, C.byref(h), C.byref(m), C.byref(r))
+        return h.value, m.value, r.value
+
+    def pair_luminosity_trace(self):
+        cap = 1 << 14
+        pi = (C.c_int32 * cap)(); pj = (C.c_int32 * cap)(); lum = (C.c_double * cap)()
+        n = _lib.lib().octo_pair_luminosity_trace(self._ptr, pi, pj, lum, cap)
+        return [(pi[k], pj[k], lum[k]) for k in range(min(n, cap))]
+
+
+class StrongStrongRuntime:
+    """Twin of task.runtime_cache: one persistent context per (label, solver)."""
+
+    def __init__(self):
+        self._ctx: Dict[tuple, Context] = {}
+
+    def context(self, label: str, solver: PICPoissonSolver, device: int) -> Context:
+        key = (label, solver, device)
+        ctx = self._ctx.get(key)
+        if ctx is None:
+            ctx = Context(solver, device)
+            self._ctx[key] = ctx
+        return ctx
+
+    def close(self):
+        for c in self._ctx.values():
+            c.close()
+        self._ctx.clear()
+
+
+def compute_luminosity(solver: PICPoissonSolver, ctx: Optional[TrackingContext]) -> bool:
+    """_pic_compute_luminosity (interface.jl:2596-2630): every turn unless a schedule says otherwise."""
+    sched = solver.luminosity_schedule
+    if ctx is None or sched is None:
+        return True
+    return bool(sched(ctx.turn)) if callable(sched) else True
+
+
+def collide(solver: PICPoissonSolver, beam1: Beam, beam2: Beam, backend=CUDABackend,
+            ctx: Optional[TrackingContext] = None, runtime: Optional[StrongStrongRuntime] = None,
+            label: str = "ip") -> float:
+    """collide!(solver, beam1, beam2, backend[, ctx]) -> luminosity (Float64; NaN when not scheduled).
+
+    Kicks both beams in place.  Raises ``CollisionError`` (an ``ArgumentError``) with the reference's
+    non-finite / extent / unsupported-option messages."""
+    if backend is not CUDABackend:
+        raise ArgumentError("this backend implements collide! for CUDABackend beams only")
+    if beam1.coords.device != beam2.coords.device:
+        raise ArgumentError("both beams must be on the same device (interface.jl:2461-2464)")
+    device = beam1.coords.device.index or 0
+    turn = -1 if ctx is None else int(ctx.turn)
+    lum_on = compute_luminosity(solver, ctx)
+    if runtime is None:
+        c = Context(solver, device)
+        try:
+            return c.collide(beam1, beam2, turn=turn, compute_luminosity=lum_on)
+        finally:
+            c.close()
+    return runtime.context(label, solver, device).collide(beam1, beam2, turn=turn, compute_luminosity=lum_on)
+
+
+_scratch: Dict[int, int] = {}
+
+
+def _scratch_ctx(device: int):
+    """A small context used for beam construction and one-turn maps."""
+    if device not in _scratch:
+        s = PICPoissonSolver(grid=(8, 8), slicing=LongitudinalSlicing(nslices=1, method="normal_quantile"))
+        c = Context(s, device)
+        _scratch[device] = c
+    return _scratch[device].ptr
+
+
+class Linear6D:
+    """Linear 6D one-turn map (linear6d.jl:85-123, 233-280) for an uncoupled lattice without dispersion:
+    per-plane rotation by 2*pi*tune with equal Twiss parameters at both ends."""
+
+    def __init__(self, beta, alpha, tune):
+        m = np.zeros(36)
+        for i in range(3):
+            mu = 2.0 * math.pi * tune[i]
+            s, c = math.sin(mu), math.cos(mu)
+            b1 = b2 = float(beta[i]); a1 = a2 = float(alpha[i])
+            r = 2 * i
+            m[r * 6 + r] = math.sqrt(b2 / b1) * (c + a1 * s)
+            m[r * 6 + r + 1] = math.sqrt(b2 * b1) * s
+            m[(r + 1) * 6 + r] = (-(1.0 + a1 * a2) * s + (a1 - a2) * c) / math.sqrt(b1 * b2)
+            m[(r + 1) * 6 + r + 1] = math.sqrt(b1 / b2) * (c - a2 * s)
+        self.matrix = m
+
+    def track(self, beam: Beam, turns: int = 1, stream=None):
+        b = beam.to_c()
+        m = (C.c_double * 36)(*self.matrix.tolist())
+        st = (stream or torch.cuda.current_stream(beam.coords.device)).cuda_stream
+        ctx = _scratch_ctx(beam.coords.device.index or 0)
+        rc = _lib.lib().octo_linear6d(ctx, C.byref(b), m, int(turns), C.c_void_p(st))
+        if rc != _lib.OCTO_OK:
+            raise RuntimeError(_lib.last_error(ctx))
+        return beam

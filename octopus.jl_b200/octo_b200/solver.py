@@ -1,0 +1,207 @@
+"""Keyword mirror of the reference's solver and slicing configuration.
+
+``PICPoissonSolver`` follows interface.jl:1384-1507 (keywords, defaults and eager
+validation) and ``LongitudinalSlicing`` interface.jl:816-831.  Invalid values raise
+``ArgumentError`` with the reference's wording; combinations this GPU backend does not
+implement are rejected when the solver is bound to the backend (the reference's
+``_require_cuda_pic_options``, pic_cpu.jl:730-777), never silently ignored.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence, Tuple
+
+from . import _lib
+
+
+class ArgumentError(ValueError):
+    """Raised where the reference raises Julia's ArgumentError."""
+
+
+_SLICING_METHODS = ("equal_area", "equal_count", "equal_width", "equal_spaced", "normal_quantile", "gaussian",
+                    "Gaussian", "specified")
+
+
+@dataclass(frozen=True)
+class LongitudinalSlicing:
+    """LongitudinalSlicing(; nslices=1, method=:equal_area, resolution=100, center_position=:centroid,
+    positions=Float64[]) -- interface.jl:816-831."""
+    nslices: int = 1
+    method: str = "equal_area"
+    resolution: int = 100
+    center_position: str = "centroid"
+    positions: Tuple[float, ...] = ()
+
+    def __post_init__(self):
+        if self.nslices <= 0:
+            raise ArgumentError("nslices must be positive")
+        if self.resolution <= 0:
+            raise ArgumentError("slicing resolution must be positive")
+        if self.method not in _SLICING_METHODS:
+            raise ArgumentError(f"unsupported longitudinal slicing method :{self.method}")
+        if self.center_position not in ("centroid", "midpoint"):
+            raise ArgumentError("center_position must be :centroid or :midpoint")
+        object.__setattr__(self, "positions", tuple(float(p) for p in self.positions))
+        if self.method == "specified" and len(self.positions) != self.nslices - 1:
+            raise ArgumentError("specified slicing requires nslices-1 internal positions")
+
+
+@dataclass(frozen=True)
+class PICPoissonSolver:
+    """PICPoissonSolver(; ...) -- the keyword surface of interface.jl:1384-1411."""
+    kbb1: Optional[float] = None
+    kbb2: Optional[float] = None
+    luminosity_scale: Optional[float] = None
+    grid: Tuple[int, int] = (128, 128)
+    deposit_method: str = "CIC"
+    green_type: str = "integrated"
+    green_cache: str = "slice_pair"
+    field_derivative: str = "second"
+    slice_interpolation: str = "linear"
+    interaction_grid: str = "slice_pair"
+    grid_extent: str = "extrema"
+    grid_extent_sigma: float = 6.0
+    min_transverse_extent: Tuple[float, float] = (0.0, 0.0)
+    grid_quantize: float = 0.0
+    slice_pair_green_min_ratio: float = 0.50
+    slice_pair_green_growth: float = 0.25
+    longitudinal_kick: bool = True
+    batch_mode: str = "wavefront"
+    cuda_async: bool = True
+    cuda_batch_fft: bool = True
+    cuda_wavefront_fft: bool = True
+    cuda_indexed_wavefront: bool = True
+    luminosity_grid: Optional[Tuple[int, int]] = None
+    luminosity_deposit_method: Optional[str] = None
+    luminosity_schedule: Optional[object] = None
+    slicing: LongitudinalSlicing = field(default_factory=LongitudinalSlicing)
+    slicing1: Optional[LongitudinalSlicing] = None
+    slicing2: Optional[LongitudinalSlicing] = None
+
+    def __post_init__(self):
+        if not (0.0 < self.slice_pair_green_min_ratio <= 1.0):
+            raise ArgumentError(
+                f"slice_pair_green_min_ratio must be in (0, 1]; got {self.slice_pair_green_min_ratio}.")
+        if not (self.slice_pair_green_growth >= 0.0):
+            raise ArgumentError(f"slice_pair_green_growth must be non-negative; got {self.slice_pair_green_growth}.")
+        g = (int(self.grid[0]), int(self.grid[1]))
+        if min(g) < 5:
+            raise ArgumentError(f"PICPoissonSolver grid dimensions must both be at least 5; got {self.grid}.")
+        object.__setattr__(self, "grid", g)
+        _choice("deposit_method", self.deposit_method, ("CIC", "TSC"))
+        _choice("green_type", self.green_type, ("integrated", "standard", "lattice"))
+        _choice("green_cache", self.green_cache, ("none", "slice_pair"))
+        _choice("field_derivative", self.field_derivative, ("second", "fourth"))
+        _choice("slice_interpolation", self.slice_interpolation, ("linear", "quadratic"))
+        _choice("grid_extent", self.grid_extent, ("extrema", "sigma"))
+        if not self.grid_extent_sigma > 0:
+            raise ArgumentError(f"grid_extent_sigma must be positive; got {self.grid_extent_sigma}.")
+        mte = self.min_transverse_extent
+        if isinstance(mte, (int, float)):
+            mte = (float(mte), float(mte))
+        mte = (float(mte[0]), float(mte[1]))
+        if not all(v >= 0 and v == v and v != float("inf") for v in mte):
+            raise ArgumentError(f"min_transverse_extent must be finite and non-negative; got {self.min_transverse_extent}.")
+        object.__setattr__(self, "min_transverse_extent", mte)
+        if not self.grid_quantize >= 0:
+            raise ArgumentError(f"grid_quantize must be non-negative (0 disables); got {self.grid_quantize}.")
+        _choice("interaction_grid", self.interaction_grid, ("slice_pair", "source_slice", "node"))
+        if self.interaction_grid != "slice_pair" and self.grid_extent != "extrema":
+            raise ArgumentError(
+                f"grid_extent = :{self.grid_extent} is not implemented for interaction_grid = "
+                f":{self.interaction_grid}: that mode sizes its mesh from the union/per-node extrema of its own "
+                "particle sets and applies no extent estimator, so a non-default value would be silently ignored. "
+                "Use interaction_grid = :slice_pair, or set grid_extent = :extrema.")
+        _choice("batch_mode", self.batch_mode, ("sequential", "wavefront"))
+        if self.luminosity_grid is not None:
+            lg = (int(self.luminosity_grid[0]), int(self.luminosity_grid[1]))
+            if min(lg) < 3:
+                raise ArgumentError(f"luminosity_grid dimensions must both be at least 3; got {self.luminosity_grid}.")
+            object.__setattr__(self, "luminosity_grid", lg)
+        if self.luminosity_deposit_method not in (None, "CIC", "TSC"):
+            raise ArgumentError("luminosity_deposit_method must be nothing, :CIC, or :TSC; got "
+                                f":{self.luminosity_deposit_method}.")
+        if self.interaction_grid == "node" and self.slice_interpolation != "linear":
+            raise ArgumentError(
+                f"slice_interpolation = :{self.slice_interpolation} is not implemented for interaction_grid = :node: "
+                "the node-plane path applies its own interpolation. Use interaction_grid = :slice_pair for "
+                ":quadratic, or slice_interpolation = :linear.")
+
+    @property
+    def resolved_slicing1(self) -> LongitudinalSlicing:
+        return self.slicing1 if self.slicing1 is not None else self.slicing
+
+    @property
+    def resolved_slicing2(self) -> LongitudinalSlicing:
+        return self.slicing2 if self.slicing2 is not None else self.slicing
+
+    def to_c(self) -> "_lib.OctoPicOptions":
+        """Bind to the GPU backend: the POD options, rejecting what this backend does not implement."""
+        _require_gpu_options(self)
+        o = _lib.OctoPicOptions()
+        o.nx, o.ny = self.grid
+        o.deposit_method = 0 if self.deposit_method == "CIC" else 1
+        o.lum_deposit_method = -1 if self.luminosity_deposit_method is None else \
+            (0 if self.luminosity_deposit_method == "CIC" else 1)
+        lg = self.luminosity_grid or (0, 0)
+        o.lum_nx, o.lum_ny = lg
+        o.green_type = {"integrated": 0, "standard": 1}[self.green_type]
+        o.green_cache = {"none": 0, "slice_pair": 1}[self.green_cache]
+        o.field_derivative = 2 if self.field_derivative == "second" else 4
+        o.slice_interpolation = 0 if self.slice_interpolation == "linear" else 1
+        o.interaction_grid = {"slice_pair": 0, "node": 2}[self.interaction_grid]
+        o.grid_extent = 0
+        o.grid_extent_sigma = float(self.grid_extent_sigma)
+        o.min_extent_x, o.min_extent_y = self.min_transverse_extent
+        o.grid_quantize = float(self.grid_quantize)
+        o.green_min_ratio = float(self.slice_pair_green_min_ratio)
+        o.green_growth = float(self.slice_pair_green_growth)
+        o.longitudinal_kick = int(bool(self.longitudinal_kick))
+        keep = []
+        for k, s in ((1, self.resolved_slicing1), (2, self.resolved_slicing2)):
+            setattr(o, f"slicing_method{k}", 1 if s.method == "specified" else 0)
+            setattr(o, f"nslices{k}", int(s.nslices))
+            setattr(o, f"center_position{k}", 0 if s.center_position == "centroid" else 1)
+            if s.method == "specified" and s.positions:
+                arr = (C.c_double * len(s.positions))(*s.positions)
+                keep.append(arr)
+                setattr(o, f"positions{k}", C.cast(arr, C.POINTER(C.c_double)))
+        o.has_kbb1 = int(self.kbb1 is not None)
+        o.has_kbb2 = int(self.kbb2 is not None)
+        o.has_lum_scale = int(self.luminosity_scale is not None)
+        o.kbb1 = float(self.kbb1 or 0.0)
+        o.kbb2 = float(self.kbb2 or 0.0)
+        o.lum_scale = float(self.luminosity_scale or 0.0)
+        o.precision = 0
+        o._keep = keep  # positions arrays must outlive octo_create
+        return o
+
+
+def _choice(name, value, allowed):
+    if value not in allowed:
+        opts = ", ".join(":" + a for a in allowed)
+        raise ArgumentError(f"{name} must be one of {opts}; got :{value}.")
+
+
+def _require_gpu_options(s: PICPoissonSolver):
+    """The GPU backend's route checks (the reference CUDA backend's, pic_cpu.jl:730-777)."""
+    if s.interaction_grid == "source_slice":
+        raise ArgumentError(
+            "interaction_grid = :source_slice is not implemented by the GPU PIC backend; only the CPU "
+            "PICPoissonSolver path supports :source_slice. Set interaction_grid = :slice_pair.")
+    if s.grid_extent != "extrema":
+        raise ArgumentError(
+            f"grid_extent = :{s.grid_extent} is not implemented by the GPU PIC backend; set grid_extent = :extrema.")
+    if s.green_type == "lattice":
+        raise ArgumentError("green_type = :lattice (an experimental CPU study kernel) is not implemented by the GPU "
+                            "PIC backend; use :integrated or :standard.")
+    for k, sl in ((1, s.resolved_slicing1), (2, s.resolved_slicing2)):
+        if sl.method not in ("normal_quantile", "gaussian", "Gaussian", "specified"):
+            raise ArgumentError(f"slicing{k} method :{sl.method} is not implemented by the GPU PIC backend; use "
+                                ":normal_quantile (the production method) or :specified.")
+        if sl.nslices > 64:
+            raise ArgumentError("the GPU PIC backend supports at most 64 slices per beam")
+    for n in s.grid:
+        if n & (n - 1) or n > 512:
+            raise ArgumentError(f"the GPU PIC backend's FFT needs power-of-two grid dimensions <= 512; got {s.grid}")

@@ -1,0 +1,111 @@
+"""CUDA path vs the FP64 oracle on identical seeded beams.
+
+Tolerances are the reference's own: StrongStrongPICBackendConsistencyContract compares all six
+coordinates and the luminosity at atol = rtol = 1e-10 and requires identical Green-cache
+hit/miss/rebuild histories (Contracts.jl:99-136, 947-960)."""
+import numpy as np
+import pytest
+
+from helpers import beams, oracle_options, oracle_params, within, E_PARAMS, P_PARAMS
+
+pytestmark = pytest.mark.gpu
+
+ATOL = RTOL = 1e-10
+
+
+def _gpu():
+    import octo_b200 as ob
+    return ob
+
+
+def _device_beams(ob, e, p):
+    be = ob.Beam.from_numpy(e, ob.BeamParams(E_PARAMS["charge"], E_PARAMS["mass"], E_PARAMS["energy"], E_PARAMS["r0"],
+                                             E_PARAMS["npart"]))
+    bp = ob.Beam.from_numpy(p, ob.BeamParams(P_PARAMS["charge"], P_PARAMS["mass"], P_PARAMS["energy"], P_PARAMS["r0"],
+                                             P_PARAMS["npart"]))
+    return be, bp
+
+
+def run_both(solver, n1, n2, turns=1, e_sigma=None, p_sigma=None, seed=123456789):
+    from oracle import oracle as orc
+    ob = _gpu()
+    e, p = beams(n1, n2, e_sigma, p_sigma, seed=seed)
+    be, bp = _device_beams(ob, e, p)
+    rt = ob.StrongStrongRuntime()
+    ctx = rt.context("ip", solver, 0)
+    oracle = orc.Oracle(oracle_options(solver))
+    pe, pp = oracle_params()
+    out = []
+    for t in range(turns):
+        lum_g = ctx.collide(be, bp, turn=t + 1)
+        lum_o = oracle.collide(e, p, pe, pp)
+        out.append(dict(lum_g=lum_g, lum_o=lum_o, cache_g=ctx.green_cache_stats(), cache_o=oracle.cache_stats(),
+                        trace_g=ctx.pair_luminosity_trace(), trace_o=oracle.pair_trace(),
+                        e_err=within(be.numpy(), e, ATOL, RTOL), p_err=within(bp.numpy(), p, ATOL, RTOL),
+                        e_abs=float(np.abs(be.numpy() - e).max()), p_abs=float(np.abs(bp.numpy() - p).max())))
+    rt.close()
+    return out
+
+
+def check(out, lum_rtol=1e-10):
+    for r in out:
+        assert r["e_err"] <= 1.0 and r["p_err"] <= 1.0, r
+        assert abs(r["lum_g"] / r["lum_o"] - 1) <= lum_rtol, (r["lum_g"], r["lum_o"])
+        assert r["cache_g"] == r["cache_o"], (r["cache_g"], r["cache_o"])
+        assert [(a, b) for a, b, _ in r["trace_g"]] == [(a, b) for a, b, _ in r["trace_o"]]
+        for (_, _, lg), (_, _, lo) in zip(r["trace_g"], r["trace_o"]):
+            assert abs(lg - lo) <= lum_rtol * abs(lo) + 1e-300
+
+
+def test_contract_fixture_cic():
+    """Contracts.jl:1096-1257 defaults: 1024/beam, 32^2, 3 :normal_quantile slices, 2 turns."""
+    ob = _gpu()
+    s = ob.PICPoissonSolver(grid=(32, 32), slicing=ob.LongitudinalSlicing(nslices=3, method="normal_quantile"))
+    out = run_both(s, 1024, 1024, turns=2)
+    check(out)
+    assert out[1]["cache_g"][0] > 0  # at least one reuse
+
+
+def test_contract_fixture_tsc():
+    ob = _gpu()
+    s = ob.PICPoissonSolver(grid=(32, 32), deposit_method="TSC",
+                            slicing=ob.LongitudinalSlicing(nslices=3, method="normal_quantile"))
+    check(run_both(s, 1024, 1024, turns=2))
+
+
+def test_route_fixture():
+    """runtests.jl:12222-12273 shape: 5000/beam, 5 slices, 64^2."""
+    ob = _gpu()
+    s = ob.PICPoissonSolver(grid=(64, 64), slicing=ob.LongitudinalSlicing(nslices=5, method="normal_quantile"))
+    out = run_both(s, 5000, 5000, turns=2, seed=91)
+    check(out)
+    for r in out:
+        assert r["e_abs"] < 1e-13 and r["p_abs"] < 1e-13, r
+
+
+@pytest.mark.parametrize("opts", [
+    dict(field_derivative="fourth"),
+    dict(slice_interpolation="quadratic"),
+    dict(green_cache="none"),
+    dict(green_type="standard", green_cache="none"),
+    dict(luminosity_deposit_method="TSC", luminosity_grid=(48, 40)),
+    dict(deposit_method="TSC", field_derivative="fourth", slice_interpolation="quadratic"),
+])
+def test_option_variants(opts):
+    ob = _gpu()
+    s = ob.PICPoissonSolver(grid=(64, 64), slicing=ob.LongitudinalSlicing(nslices=4, method="normal_quantile"), **opts)
+    check(run_both(s, 6000, 4000, turns=2))
+
+
+def test_node_mode():
+    ob = _gpu()
+    s = ob.PICPoissonSolver(grid=(64, 64), interaction_grid="node",
+                            slicing=ob.LongitudinalSlicing(nslices=7, method="normal_quantile"))
+    check(run_both(s, 20000, 10000, turns=2, e_sigma=(95e-6, 8.5e-6, 0.7e-2), p_sigma=(95e-6, 8.5e-6, 6e-2)))
+
+
+def test_config0_round_beams():
+    """Plain PIC, CPU-runnable case: 100k/100k round 50 um, 5 slices, 64^2 :slice_pair, one collision."""
+    ob = _gpu()
+    s = ob.PICPoissonSolver(grid=(64, 64), slicing=ob.LongitudinalSlicing(nslices=5, method="normal_quantile"))
+    check(run_both(s, 100000, 100000, turns=1, e_sigma=(50e-6, 50e-6, 7e-3), p_sigma=(50e-6, 50e-6, 60e-3)))
