@@ -1,0 +1,306 @@
+#!/usr/bin/env python
+"""Benchmark: PIC seconds per turn of the strong-strong collision at the production point.
+
+Workload (one "step" = one turn): 2.56M electron / 1.024M proton seeded 6D Gaussian macroparticles,
+flat beams sigma_x = 95 um, sigma_y = 8.5 um, sigma_z = 7 mm / 60 mm, delta_rms 5.5e-4 / 6.6e-4,
+N = 1.7e11 / 6.9e10, E = 10 / 275 GeV; 15 :normal_quantile centroid slices, 128x128 :node interaction
+grids, CIC, second-order field, linear slice interpolation, luminosity every turn; then the linear
+uncoupled 6D one-turn map of each ring (tunes e 0.08/0.06, p 0.228/0.210; synchrotron tunes -0.069 /
+-0.01 as in the reference's production example).  FP64 throughout (the plain form).
+
+`python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]` prints one JSON line.
+Under torchrun each rank runs an independent replica of the collision (a single collision does not
+shard); `value` is the whole-job seconds per turn (max-over-ranks step time / turns done by all ranks).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (ROOT, os.path.join(ROOT, "octopus.jl_b200")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "PIC s/turn (2.56M e/1.02M p, 15 sl, 128²) plain vs fast form at ≤1% field err"
+UNIT = "s/turn"
+N_E, N_P = 2_560_000, 1_024_000
+SLICES, GRID = 15, 128
+E_BEAM = dict(beta=(0.55, 0.056, 0.7e-2 / 5.5e-4), sigma=(95e-6, 8.5e-6, 7e-3), rng_id=1)
+P_BEAM = dict(beta=(0.8, 0.072, 6e-2 / 6.6e-4), sigma=(95e-6, 8.5e-6, 6e-2), rng_id=2)
+E_TUNES, P_TUNES = (0.08, 0.06, -0.069), (0.228, 0.210, -0.01)
+SEED = 123456789
+CONFIG = {
+    "workload": "production EIC-like plain PIC, one turn = collide + one-turn maps",
+    "n_electrons": N_E, "n_protons": N_P, "nslices": SLICES, "grid": [GRID, GRID],
+    "interaction_grid": "node", "deposit": "CIC", "field_derivative": "second", "slice_interpolation": "linear",
+    "luminosity": "every turn", "precision": "fp64 plain form (int64 fixed-point charge grids)",
+    "l2": "inputs larger than L2 (172 MB of particle coordinates per turn)",
+}
+# DRAM bytes per kick-kernel launch per field particle, from `ncu` (see profiles/kick_node_c1.md);
+# None until measured.
+KICK_TRAFFIC_BYTES_PER_PARTICLE = None
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    import datetime
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist.get_rank(), dist.get_world_size(), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def _solver(ob):
+    return ob.PICPoissonSolver(grid=(GRID, GRID), interaction_grid="node", deposit_method="CIC",
+                               slicing=ob.LongitudinalSlicing(nslices=SLICES, method="normal_quantile",
+                                                              center_position="centroid"))
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (clocks and throttle reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def _cpu_baseline(steps_hint: int = 1):
+    """The FP64 CPU oracle (a port of the reference's CPU PIC path) on one full turn of the same workload,
+    with every host thread; returns (s/turn, threads, sample description)."""
+    import numpy as np
+    from oracle import oracle as orc
+    threads = os.cpu_count() or 1
+    e = orc.beam_gaussian(N_E, seed=SEED, rng_id=1, beta=E_BEAM["beta"], sigma=E_BEAM["sigma"])
+    p = orc.beam_gaussian(N_P, seed=SEED, rng_id=2, beta=P_BEAM["beta"], sigma=P_BEAM["sigma"])
+    pe = orc.beam_params(-1.0, orc.EMASS_EV, 10e9, 1.7e11)
+    pp = orc.beam_params(1.0, orc.PMASS_EV, 275e9, 6.9e10)
+    oracle = orc.Oracle(orc.OracleOptions(grid=(GRID, GRID), interaction_grid="node", nslices1=SLICES,
+                                          nslices2=SLICES, nthreads=threads))
+    me = orc.linear6d_matrix(E_BEAM["beta"], (0, 0, 0), E_TUNES)
+    mp = orc.linear6d_matrix(P_BEAM["beta"], (0, 0, 0), P_TUNES)
+    times = []
+    for _ in range(max(1, steps_hint)):
+        t0 = time.perf_counter()
+        oracle.collide(e, p, pe, pp)
+        orc.linear6d(me, e)
+        orc.linear6d(mp, p)
+        times.append(time.perf_counter() - t0)
+    return statistics.median(times), threads, f"{len(times)} full turn(s) of the benchmark workload (collide + maps)"
+
+
+def run_reference(args, rank):
+    """Reference arm: the reference's CPU algorithm (FP64 CPU oracle port; Julia is not available here)."""
+    if rank != 0:
+        return 0
+    budget = 180.0
+    t0 = time.perf_counter()
+    one, threads, _ = _cpu_baseline(1)  # also serves as warm-up
+    per = one
+    n_time = max(1, min(args.steps, int(max(1.0, (budget - (time.perf_counter() - t0)) / max(per, 1e-3)))))
+    val, threads, sample = _cpu_baseline(n_time)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": n_time,
+        "warmup": 1, "ms_per_step": val * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded counter-RNG Gaussian beams)", "config": CONFIG,
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CPU PIC path restated in C++ (Julia is absent on this machine); all host threads",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import octo_b200 as ob
+
+    dev = torch.device(f"cuda:{local_rank}")
+    torch.cuda.set_device(dev)
+    solver = _solver(ob)
+    e = ob.Beam.gaussian(N_E, seed=SEED, charge=-1.0, mc2=ob.EMASS_EV, E0=10e9, npart=1.7e11, device=dev, **E_BEAM)
+    p = ob.Beam.gaussian(N_P, seed=SEED, charge=1.0, mc2=ob.PMASS_EV, E0=275e9, npart=6.9e10, device=dev, **P_BEAM)
+    me = ob.Linear6D(E_BEAM["beta"], (0, 0, 0), E_TUNES)
+    mp = ob.Linear6D(P_BEAM["beta"], (0, 0, 0), P_TUNES)
+    rt = ob.StrongStrongRuntime()
+    ctx = rt.context("ip", solver, local_rank)
+    stream = torch.cuda.current_stream(dev)
+    e0, p0 = e.coords.clone(), p.coords.clone()
+
+    def turn(t):
+        lum = ctx.collide(e, p, turn=t, stream=stream)
+        me.track(e, stream=stream)
+        mp.track(p, stream=stream)
+        return lum
+
+    for t in range(args.warmup):
+        turn(t)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    clocks = Clocks(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    ctx.set_timing(True)
+    launches = 0
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for t in range(args.steps):
+        lum = turn(args.warmup + t)
+        launches += ctx.last_report.kernel_launches + 2
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    phases = ctx.timing_report()
+    ctx.set_timing(False)
+
+    # end to end through the public API with host-resident beams (pinned), copies inside the region
+    he = torch.empty_like(e0, device="cpu").pin_memory()
+    hp = torch.empty_like(p0, device="cpu").pin_memory()
+    he.copy_(e0); hp.copy_(p0)
+    e2e_steps = max(3, min(args.steps, 20))
+    torch.cuda.synchronize()
+    barrier()
+    w0 = time.perf_counter()
+    ev0.record(stream)
+    for t in range(e2e_steps):
+        e.coords.copy_(he, non_blocking=True)
+        p.coords.copy_(hp, non_blocking=True)
+        lum_e2e = turn(10_000 + t)
+        he.copy_(e.coords, non_blocking=True)
+        hp.copy_(p.coords, non_blocking=True)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - w0) / e2e_steps
+    barrier()
+    e2e_ms = ev0.elapsed_time(ev1) / e2e_steps
+    clk = clocks.stop()
+
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms, e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(tt[0]), float(tt[1])
+
+    if rank != 0:
+        return 0
+    value = ms / 1e3 / world
+    kick_ms, kick_launches, kick_bytes = phases["kick"]
+    dom = max(phases.items(), key=lambda kv: kv[1][0])
+    roof = None
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    if kick_ms > 0:
+        achieved = kick_bytes / (kick_ms / 1e3) / 1e9
+        traffic = None
+        if KICK_TRAFFIC_BYTES_PER_PARTICLE is not None and kick_launches:
+            traffic = KICK_TRAFFIC_BYTES_PER_PARTICLE * (kick_bytes / 88.0) / kick_launches
+        roof = {"kernel": "k_kick (gather + 6D synchro-beam kick)", "bound": "hbm", "achieved": achieved,
+                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "algorithmic_bytes_per_launch": kick_bytes / max(kick_launches, 1),
+                "avg_launch_ms": kick_ms / max(kick_launches, 1)}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        v, threads, sample = _cpu_baseline(1)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+    beam_bytes = (N_E + N_P) * 6 * 8
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded counter-RNG Gaussian beams)",
+        "config": dict(CONFIG, parallelism=f"replicas{world}"),
+        "e2e": {"value": e2e_ms / 1e3 / world, "unit": UNIT, "h2d_bytes_per_step": beam_bytes,
+                "d2h_bytes_per_step": beam_bytes + 8, "wall_s_per_step": wall},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "luminosity": lum,
+        "dominant_phase": dom[0],
+        "phases_ms_per_turn": {k: v[0] / args.steps for k, v in phases.items()},
+    }
+    print(json.dumps(line), flush=True)
+    rt.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, world, local_rank = _dist()
+    try:
+        if args.impl == "reference":
+            return run_reference(args, rank)
+        return run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -136,6 +136,27 @@ int32_t octo_beam_gaussian(octo_ctx *ctx, octo_beam *beam, uint64_t seed, uint64
 /* Message of the last failing call on this context (NUL-terminated, truncated to len). */
 int32_t octo_last_error(octo_ctx *ctx, char *buf, int64_t len);
 
+/* Per-phase device timing, the twin of the reference's pic_timing diagnostics
+ * (StrongStrongDiagnostics, interface.jl:301-386; _CUDAPICTimingStats, pic_cuda.jl:552-700).
+ * While enabled, CUDA events bracket each launch group; octo_timing_report returns the
+ * accumulated device milliseconds, launch counts and algorithmic HBM bytes per phase
+ * (bytes: kick 11 values, deposit 4, bounds 5, luminosity 4 per particle visit, FP64). */
+#define OCTO_PHASE_SLICING 0
+#define OCTO_PHASE_BOUNDS 1
+#define OCTO_PHASE_PLAN 2
+#define OCTO_PHASE_GREEN 3
+#define OCTO_PHASE_LUMINOSITY 4
+#define OCTO_PHASE_DEPOSIT 5
+#define OCTO_PHASE_FFT 6
+#define OCTO_PHASE_FIELD 7
+#define OCTO_PHASE_KICK 8
+#define OCTO_PHASE_UNSORT 9
+#define OCTO_PHASE_NODE 10
+#define OCTO_NPHASES 11
+int32_t octo_set_timing(octo_ctx *ctx, int32_t enable); /* enabling also clears the accumulators */
+int32_t octo_timing_report(octo_ctx *ctx, double ms[OCTO_NPHASES], int64_t launches[OCTO_NPHASES],
+                           double bytes[OCTO_NPHASES]);
+
 /* Host-side helpers shared with the slicing: the normal quantile sqrt(2)*erfinv(2s/ns - 1)
  * used for :normal_quantile boundaries (slicing.jl:420-429), and the library version. */
 double octo_normal_quantile(int32_t s, int32_t ns);

@@ -201,9 +201,55 @@ struct octo_ctx {
     std::vector<int> trace_i, trace_j;
     std::vector<double> trace_lum;
     long long last_launches = 0;
+    // per-phase device timing (octo_set_timing): event pairs recorded around each launch group
+    int timing = 0;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_marks;
+    double phase_ms[OCTO_NPHASES] = {0};
+    long long phase_launches[OCTO_NPHASES] = {0};
+    double phase_bytes[OCTO_NPHASES] = {0};
 };
 
 namespace {
+
+// ---- per-phase timing: a scope records an event pair on the stream around a launch group
+cudaEvent_t take_event(octo_ctx *c) {
+    if (c->ev_used == c->ev_pool.size()) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        c->ev_pool.push_back(e);
+    }
+    return c->ev_pool[c->ev_used++];
+}
+struct PhaseScope {
+    octo_ctx *c;
+    int phase;
+    cudaStream_t st;
+    cudaEvent_t a = nullptr;
+    int nlaunch;
+    double bytes;
+    PhaseScope(octo_ctx *c_, int ph, cudaStream_t s, int nl = 1, double b = 0.0) : c(c_), phase(ph), st(s), nlaunch(nl), bytes(b) {
+        if (c->timing) { a = take_event(c); CK(cudaEventRecord(a, st)); }
+    }
+    ~PhaseScope() {
+        if (c->timing && a) {
+            cudaEvent_t b = take_event(c);
+            if (cudaEventRecord(b, st) == cudaSuccess) c->ev_marks.push_back({phase, {a, b}});
+            c->phase_launches[phase] += nlaunch;
+            c->phase_bytes[phase] += bytes;
+        }
+    }
+};
+void harvest_timing(octo_ctx *c) {
+    if (!c->timing) return;
+    for (auto &m : c->ev_marks) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, m.second.first, m.second.second) == cudaSuccess) c->phase_ms[m.first] += ms;
+    }
+    c->ev_marks.clear();
+    c->ev_used = 0;
+}
 
 void set_error(octo_ctx *c, const std::string &m) { c->err = m; }
 
@@ -458,8 +504,11 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
     const double klum = o.has_lum_scale ? o.lum_scale : p1->npart * p2->npart / (double)(n1 * n2);
 
     // ---- slicing (one readback of the slice tables)
-    slice_beam(c, 0, *b1, st, launches);
-    slice_beam(c, 1, *b2, st, launches);
+    {
+        PhaseScope ps(c, OCTO_PHASE_SLICING, st, 20);
+        slice_beam(c, 0, *b1, st, launches);
+        slice_beam(c, 1, *b2, st, launches);
+    }
     CK(cudaMemcpyAsync(&c->bw[0].host, c->bw[0].info.p, sizeof(SliceInfo), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(&c->bw[1].host, c->bw[1].info.p, sizeof(SliceInfo), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -524,7 +573,10 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
     launches += 1;
 
     // ---- node meshes at turn start
-    if (node) build_node_meshes(c, C, S1, S2, st, launches);
+    if (node) {
+        PhaseScope ps(c, OCTO_PHASE_NODE, st, 16);
+        build_node_meshes(c, C, S1, S2, st, launches);
+    }
     auto node_id = [&](int dir, int src_slice0, int node1) {
         return dir == 1 ? src_slice0 * (ns2 + 1) + (node1 - 1) : ns1 * (ns2 + 1) + src_slice0 * (ns1 + 1) + (node1 - 1);
     };
@@ -693,18 +745,27 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
     // ---- wavefronts
     for (const Front &F : fronts) {
         const int npf = F.nt / 2;
+        double slice_bytes = 0.0, src_bytes = 0.0, fld_bytes = 0.0;
+        for (int t = F.t0; t < F.t0 + F.nt; t += 2) slice_bytes += (double)(tasks[t].src_n + tasks[t].fld_n);
+        for (int t = F.t0; t < F.t0 + F.nt; ++t) { src_bytes += (double)tasks[t].src_n; fld_bytes += (double)tasks[t].fld_n; }
         if (!node || compute_lum) {
+            PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, 1, slice_bytes * 5 * sizeof(double));
             unsigned bps = (unsigned)std::max<long long>(1, std::min<long long>(32, (F.maxsrc + 8191) / 8192));
             k_pair_bounds<<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
             launches++;
         }
         if (!node) {
-            k_plan<<<(F.nt + 63) / 64, 64, 0, st>>>(C, F.t0, F.nt, 0);
+            {
+                PhaseScope ps(c, OCTO_PHASE_PLAN, st, 1);
+                k_plan<<<(F.nt + 63) / 64, 64, 0, st>>>(C, F.t0, F.nt, 0);
+            }
+            PhaseScope ps(c, OCTO_PHASE_GREEN, st, 2);
             k_green_rows<<<dim3((NY / 2 + 3) / 4, F.nt), 128, fft_smem(NX), st>>>(C, 0, F.t0, 0);
             k_green_cols<<<dim3((nx + 1 + 3) / 4, F.nt), 128, fft_smem(NY), st>>>(C, 0, F.t0, 0);
             launches += 3;
         }
         if (compute_lum && F.nl) {
+            PhaseScope ps(c, OCTO_PHASE_LUMINOSITY, st, 3, slice_bytes * 4 * sizeof(double));
             k_lum_plan<<<(F.nl + 63) / 64, 64, 0, st>>>(C, F.l0, F.nl, F.t0);
             unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(16, (F.maxlum + 16383) / 16384));
             launch_method(lmethod, [&](auto M) {
@@ -714,29 +775,42 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
             launches += 3;
         }
         {
+            PhaseScope ps(c, OCTO_PHASE_DEPOSIT, st, 1, src_bytes * 4 * sizeof(double));
             unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(16, (F.maxsrc + 16383) / 16384));
             launch_method(method, [&](auto M) {
                 k_deposit<decltype(M)::value><<<dim3(bpp, F.np), 512, dep_bytes, st>>>(C, F.p0, dep_smem ? 1 : 0);
             });
+        }
+        {
+            PhaseScope ps(c, OCTO_PHASE_FFT, st, 2);
             k_conv_rows<<<dim3((ny / 2 + 3) / 4, F.np), 128, fft_smem(NX), st>>>(C, F.p0);
             k_conv_cols<<<dim3((nx + 1 + 3) / 4, F.np), 128, fft_smem(NY), st>>>(C, F.p0);
+        }
+        {
+            PhaseScope ps(c, OCTO_PHASE_FIELD, st, 1);
             k_conv_field<<<dim3((ny + kFieldTile - 1) / kFieldTile, F.np), 128, field_smem(NX), st>>>(C, F.p0);
+        }
+        {
+            PhaseScope ps(c, OCTO_PHASE_KICK, st, 1, fld_bytes * 11 * sizeof(double));
             launch_method(method, [&](auto M) {
                 k_kick<decltype(M)::value><<<F.nb, 256, 0, st>>>(C, F.p0, c->blockmap.p + F.b0);
             });
-            launches += 5;
         }
+        launches += 5;
     }
     CK(cudaGetLastError());
 
     // ---- back to caller order
-    for (int b = 0; b < 2; ++b) {
-        const BeamWS &W = c->bw[b];
-        const octo_beam &B = b == 0 ? *b1 : *b2;
-        k_unsort<<<(unsigned)((W.total + 255) / 256), 256, 0, st>>>(
-            W.perm.p, W.total, W.s[0].p, W.s[1].p, W.s[2].p, W.s[3].p, W.s[4].p, W.s[5].p, (double *)B.x,
-            (double *)B.px, (double *)B.y, (double *)B.py, (double *)B.z, (double *)B.pz, W.info.p);
-        launches++;
+    {
+        PhaseScope ps(c, OCTO_PHASE_UNSORT, st, 2, (double)(n1 + n2) * 12 * sizeof(double));
+        for (int b = 0; b < 2; ++b) {
+            const BeamWS &W = c->bw[b];
+            const octo_beam &B = b == 0 ? *b1 : *b2;
+            k_unsort<<<(unsigned)((W.total + 255) / 256), 256, 0, st>>>(
+                W.perm.p, W.total, W.s[0].p, W.s[1].p, W.s[2].p, W.s[3].p, W.s[4].p, W.s[5].p, (double *)B.x,
+                (double *)B.px, (double *)B.y, (double *)B.py, (double *)B.z, (double *)B.pz, W.info.p);
+            launches++;
+        }
     }
     c->h_lum.ensure(std::max(npairs_total, 1));
     c->h_status.ensure(1);
@@ -744,6 +818,7 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
     CK(cudaMemcpyAsync(c->h_status.p, c->status.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     CK(cudaGetLastError());
+    harvest_timing(c);
     const DevStatus DS = *c->h_status.p;
     c->last_launches = launches;
     if (rep) {
@@ -888,6 +963,7 @@ void octo_destroy(octo_ctx *c) {
     c->spec.release(); c->fields.release(); c->lum_parts.release(); c->node_ref.release(); c->stats.release();
     c->partial.release(); c->soa_ptrs.release();
     c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_nodes.release();
+    for (auto e : c->ev_pool) cudaEventDestroy(e);
     delete c;
 }
 
@@ -986,6 +1062,26 @@ int32_t octo_beam_gaussian(octo_ctx *c, octo_beam *beam, uint64_t seed, uint64_t
     } catch (CudaFail &e) {
         return fail(c, OCTO_ERR_CUDA, e.msg);
     }
+}
+
+int32_t octo_set_timing(octo_ctx *c, int32_t enable) {
+    if (!c) return OCTO_ERR_ARG;
+    c->timing = enable ? 1 : 0;
+    for (int k = 0; k < OCTO_NPHASES; ++k) { c->phase_ms[k] = 0; c->phase_launches[k] = 0; c->phase_bytes[k] = 0; }
+    c->ev_marks.clear();
+    c->ev_used = 0;
+    return OCTO_OK;
+}
+
+int32_t octo_timing_report(octo_ctx *c, double ms[OCTO_NPHASES], int64_t launches[OCTO_NPHASES],
+                           double bytes[OCTO_NPHASES]) {
+    if (!c) return OCTO_ERR_ARG;
+    for (int k = 0; k < OCTO_NPHASES; ++k) {
+        if (ms) ms[k] = c->phase_ms[k];
+        if (launches) launches[k] = c->phase_launches[k];
+        if (bytes) bytes[k] = c->phase_bytes[k];
+    }
+    return OCTO_OK;
 }
 
 int32_t octo_last_error(octo_ctx *c, char *buf, int64_t len) {

@@ -1,0 +1,174 @@
+"""
+    OctopusB200
+
+Julia side of the drop-in: routes Octopus.jl's strong-strong PIC collision to libocto_b200.so
+(hand-written sm_100a kernels behind a C ABI, include/octo_b200.h) with `ccall`.
+
+`B200PICPoissonSolver` composes an ordinary `PICPoissonSolver` (the pattern of
+`GaussianPICPoissonSolver`, src/tasks/strongstrong/gaussian_pic.jl:87-92), so the
+`PICPoissonSolver` keywords stay the API and no method of `collide!(::PICPoissonSolver, ...)`
+is overwritten.  Beams stay `Beam{CUDABackend}` with `CuArray` SoA coordinates; the library
+kicks them in place on the task's stream.
+
+This file is loaded after Octopus (`include("OctopusB200.jl")` or as a package extension).
+"""
+module OctopusB200
+
+using CUDA
+import Octopus
+using Octopus: Beam, CUDABackend, TrackingContext, PICPoissonSolver, LongitudinalSlicing,
+               AbstractPoissonSolver, StrongStrongTask
+
+const LIB = get(ENV, "OCTO_B200_LIB", joinpath(@__DIR__, "..", "build", "libocto_b200.so"))
+
+# include/octo_b200.h: octo_beam
+struct OctoBeam
+    n::Int64
+    dtype::Int32
+    reserved::Int32
+    x::CuPtr{Float64}; px::CuPtr{Float64}; y::CuPtr{Float64}
+    py::CuPtr{Float64}; z::CuPtr{Float64}; pz::CuPtr{Float64}
+end
+
+# include/octo_b200.h: octo_beam_params (BeamParams, src/beam/Beam.jl:29-35)
+struct OctoBeamParams
+    charge::Float64; mc2::Float64; E0::Float64; r0::Float64; npart::Float64
+end
+
+# include/octo_b200.h: octo_pic_options (PICPoissonSolver fields, interface.jl:1350-1382)
+struct OctoPicOptions
+    nx::Int32; ny::Int32; deposit_method::Int32; lum_deposit_method::Int32
+    lum_nx::Int32; lum_ny::Int32; green_type::Int32; green_cache::Int32
+    field_derivative::Int32; slice_interpolation::Int32; interaction_grid::Int32; grid_extent::Int32
+    grid_extent_sigma::Float64; min_extent_x::Float64; min_extent_y::Float64; grid_quantize::Float64
+    green_min_ratio::Float64; green_growth::Float64
+    longitudinal_kick::Int32; slicing_method1::Int32; slicing_method2::Int32
+    nslices1::Int32; nslices2::Int32; center_position1::Int32; center_position2::Int32
+    positions1::Ptr{Float64}; positions2::Ptr{Float64}
+    has_kbb1::Int32; has_kbb2::Int32; has_lum_scale::Int32
+    kbb1::Float64; kbb2::Float64; lum_scale::Float64
+    precision::Int32; reserved::NTuple{7,Int32}
+end
+
+# include/octo_b200.h: octo_collide_report
+mutable struct OctoCollideReport
+    status::Int32; role::Int32; pair_i::Int32; pair_j::Int32; direction::Int32; n_batches::Int32
+    turn::Int64; first_index::Int64; dropped::Int64
+    green_hits::Int64; green_misses::Int64; green_rebuilds::Int64; kernel_launches::Int64
+    OctoCollideReport() = new(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
+end
+
+"""
+    B200PICPoissonSolver(; kwargs...)
+
+`PICPoissonSolver(; kwargs...)` run on libocto_b200.  Every keyword is the reference's.
+"""
+struct B200PICPoissonSolver{T<:Real} <: AbstractPoissonSolver
+    pic::PICPoissonSolver{T}
+end
+B200PICPoissonSolver(; kwargs...) = B200PICPoissonSolver(PICPoissonSolver(; kwargs...))
+
+_sym(v, table) = Int32(table[Symbol(v)])
+
+function _slicing_fields(s::LongitudinalSlicing)
+    s.method in (:normal_quantile, :gaussian, :Gaussian, :specified) || throw(ArgumentError(
+        "slicing method $(repr(s.method)) is not implemented by the B200 backend; use :normal_quantile or :specified"))
+    return (s.method === :specified ? Int32(1) : Int32(0), Int32(s.nslices),
+            s.center_position === :centroid ? Int32(0) : Int32(1))
+end
+
+function _options(p::PICPoissonSolver, keep::Vector{Any})
+    m1, n1, c1 = _slicing_fields(p.slicing1)
+    m2, n2, c2 = _slicing_fields(p.slicing2)
+    pos1 = Float64.(p.slicing1.positions); pos2 = Float64.(p.slicing2.positions)
+    push!(keep, pos1, pos2)
+    lg = p.luminosity_grid === nothing ? (0, 0) : p.luminosity_grid
+    ldm = p.luminosity_deposit_method === nothing ? Int32(-1) : _sym(p.luminosity_deposit_method, Dict(:CIC => 0, :TSC => 1))
+    ig = Symbol(p.interaction_grid)
+    ig === :source_slice && throw(ArgumentError(
+        "interaction_grid = :source_slice is implemented only by the CPU PICPoissonSolver path"))
+    return OctoPicOptions(
+        Int32(p.grid[1]), Int32(p.grid[2]), _sym(p.deposit_method, Dict(:CIC => 0, :TSC => 1)), ldm,
+        Int32(lg[1]), Int32(lg[2]), _sym(p.green_type, Dict(:integrated => 0, :standard => 1, :lattice => 2)),
+        _sym(p.green_cache, Dict(:none => 0, :slice_pair => 1)),
+        p.field_derivative === :fourth ? Int32(4) : Int32(2), p.slice_interpolation === :quadratic ? Int32(1) : Int32(0),
+        ig === :node ? Int32(2) : Int32(0), p.grid_extent === :extrema ? Int32(0) : Int32(1),
+        Float64(p.grid_extent_sigma), Float64(p.min_transverse_extent[1]), Float64(p.min_transverse_extent[2]),
+        Float64(p.grid_quantize), Float64(p.slice_pair_green_min_ratio), Float64(p.slice_pair_green_growth),
+        Int32(p.longitudinal_kick), m1, m2, n1, n2, c1, c2,
+        isempty(pos1) ? Ptr{Float64}(C_NULL) : pointer(pos1), isempty(pos2) ? Ptr{Float64}(C_NULL) : pointer(pos2),
+        Int32(p.kbb1 !== nothing), Int32(p.kbb2 !== nothing), Int32(p.luminosity_scale !== nothing),
+        p.kbb1 === nothing ? 0.0 : Float64(p.kbb1), p.kbb2 === nothing ? 0.0 : Float64(p.kbb2),
+        p.luminosity_scale === nothing ? 0.0 : Float64(p.luminosity_scale), Int32(0), ntuple(_ -> Int32(0), 7))
+end
+
+"""Context: device workspaces and the slice-pair Green cache (the twin of task.runtime_cache)."""
+mutable struct Context
+    ptr::Ptr{Cvoid}
+    function Context(p::PICPoissonSolver)
+        keep = Any[]
+        opts = Ref(_options(p, keep))
+        ptr = GC.@preserve keep ccall((:octo_create, LIB), Ptr{Cvoid}, (Int32, Ref{OctoPicOptions}),
+                                      Int32(CUDA.device().handle), opts)
+        ptr == C_NULL && error("octo_create failed")
+        c = new(ptr)
+        finalizer(c) do c
+            c.ptr == C_NULL || ccall((:octo_destroy, LIB), Cvoid, (Ptr{Cvoid},), c.ptr)
+            c.ptr = C_NULL
+        end
+        return c
+    end
+end
+
+function _last_error(ctx::Context)
+    buf = Vector{UInt8}(undef, 1024)
+    ccall((:octo_last_error, LIB), Int32, (Ptr{Cvoid}, Ptr{UInt8}, Int64), ctx.ptr, buf, length(buf))
+    return unsafe_string(pointer(buf))
+end
+
+_octo_beam(b::Beam) = OctoBeam(Int64(length(b.rep.x)), Int32(0), Int32(0),
+    pointer(b.rep.x), pointer(b.rep.px), pointer(b.rep.y), pointer(b.rep.py), pointer(b.rep.z), pointer(b.rep.pz))
+_octo_params(b::Beam) = OctoBeamParams(Float64(b.params.charge), Float64(b.params.mc2), Float64(b.params.E0),
+                                       Float64(b.params.r0), Float64(b.params.npart))
+
+function _collide!(ctx::Context, solver::B200PICPoissonSolver, beam1::Beam, beam2::Beam, turn::Integer)
+    eltype(beam1.rep.x) === Float64 && eltype(beam2.rep.x) === Float64 || throw(ArgumentError(
+        "the B200 backend's plain form takes Float64 beams"))
+    b1 = Ref(_octo_beam(beam1)); b2 = Ref(_octo_beam(beam2))
+    p1 = Ref(_octo_params(beam1)); p2 = Ref(_octo_params(beam2))
+    lum = Ref(NaN)
+    rep = OctoCollideReport()
+    compute = Octopus._pic_compute_luminosity(solver.pic, turn < 0 ? nothing : TrackingContext(turn=Int64(turn)))
+    rc = ccall((:octo_pic_collide, LIB), Int32,
+               (Ptr{Cvoid}, Ref{OctoBeam}, Ref{OctoBeam}, Ref{OctoBeamParams}, Ref{OctoBeamParams}, Int64, Int32,
+                Ref{Float64}, Ref{OctoCollideReport}, Ptr{Cvoid}),
+               ctx.ptr, b1, b2, p1, p2, Int64(turn), Int32(compute), lum, rep, CUDA.stream().handle)
+    rc == 0 || throw(ArgumentError(_last_error(ctx)))
+    Octopus._pic_report_dropped_count(rep.dropped)   # warns exactly as pic_cpu.jl:445-457 does
+    return Float64(lum[])
+end
+
+"""collide!(solver, beam1, beam2, CUDABackend[, ctx]) on libocto_b200: a fresh (cold) context per call,
+as the reference's public collide! builds a fresh Green cache (pic_cuda.jl:94-126)."""
+function Octopus.collide!(solver::B200PICPoissonSolver, beam1::Beam, beam2::Beam, ::Type{CUDABackend},
+                          ctx::Union{Nothing,TrackingContext}=nothing)
+    c = Context(solver.pic)
+    try
+        return _collide!(c, solver, beam1, beam2, ctx === nothing ? -1 : ctx.turn)
+    finally
+        finalize(c)
+    end
+end
+
+# Task path: one persistent context per (label, solver) in task.runtime_cache (pic_cuda.jl:127-137).
+function Octopus._strong_strong_collide_backend!(task::StrongStrongTask, label::Symbol,
+                                                 solver::B200PICPoissonSolver, beam1::Beam, beam2::Beam,
+                                                 ::Type{CUDABackend}, ctx::TrackingContext)
+    key = (:octo_b200_context, label, solver.pic.grid, objectid(solver))
+    c = get!(() -> Context(solver.pic), task.runtime_cache, key)::Context
+    return _collide!(c, solver, beam1, beam2, ctx.turn)
+end
+
+Octopus._pic_compute_luminosity(solver::B200PICPoissonSolver, ctx) = Octopus._pic_compute_luminosity(solver.pic, ctx)
+
+end # module

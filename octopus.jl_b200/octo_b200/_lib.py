@@ -23,8 +23,10 @@ ERROR_NAMES = {
 EXPORTS = (
     "octo_create", "octo_destroy", "octo_pic_collide", "octo_green_cache_stats",
     "octo_pair_luminosity_trace", "octo_linear6d", "octo_beam_gaussian", "octo_last_error",
-    "octo_normal_quantile", "octo_erfinv", "octo_version",
+    "octo_normal_quantile", "octo_erfinv", "octo_version", "octo_set_timing", "octo_timing_report",
 )
+
+PHASES = ("slicing", "bounds", "plan", "green", "luminosity", "deposit", "fft", "field", "kick", "unsort", "node")
 
 
 class OctoBeam(C.Structure):
@@ -109,6 +111,10 @@ def lib():
     L.octo_erfinv.argtypes = [d]
     L.octo_version.restype = i32
     L.octo_version.argtypes = []
+    L.octo_set_timing.restype = i32
+    L.octo_set_timing.argtypes = [vp, i32]
+    L.octo_timing_report.restype = i32
+    L.octo_timing_report.argtypes = [vp, P(d), P(i64), P(d)]
     _lib = L
     return L
 

@@ -86,6 +86,17 @@ class Context:
         _lib.lib().octo_green_cache_stats(self._ptr, C.byref(h), C.byref(m), C.byref(r))
         return h.value, m.value, r.value
 
+    def set_timing(self, enable: bool = True):
+        """Per-phase device timing (the reference's pic_timing diagnostics); enabling clears it."""
+        _lib.lib().octo_set_timing(self._ptr, int(bool(enable)))
+
+    def timing_report(self):
+        """{phase: (device ms, launches, algorithmic bytes)} accumulated since set_timing(True)."""
+        n = len(_lib.PHASES)
+        ms = (C.c_double * n)(); la = (C.c_int64 * n)(); by = (C.c_double * n)()
+        _lib.lib().octo_timing_report(self._ptr, ms, la, by)
+        return {name: (ms[k], la[k], by[k]) for k, name in enumerate(_lib.PHASES)}
+
     def pair_luminosity_trace(self):
         cap = 1 << 14
         pi = (C.c_int32 * cap)(); pj = (C.c_int32 * cap)(); lum = (C.c_double * cap)()

@@ -47,7 +47,8 @@ inline double jmax(double a, double b) {
     if (b > a) return b;
     return std::signbit(a) ? b : a;
 }
-inline double jclamp(double v, double lo, double hi) { return jmin(jmax(v, lo), hi); }
+// Julia clamp(x, lo, hi) = ifelse(x > hi, hi, ifelse(x < lo, lo, x)).
+inline double jclamp(double x, double lo, double hi) { return x > hi ? hi : (x < lo ? lo : x); }
 inline long jclampi(long v, long lo, long hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 // ---------------------------------------------------------------- counter RNG
@@ -1403,6 +1404,40 @@ void oo_interpolation_grids(const oo_options *opt, const double b[8], double out
     interaction_grids(O, b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], sg, fg);
     out[0] = sg.x0; out[1] = sg.y0; out[2] = sg.width; out[3] = sg.height;
     out[4] = fg.x0; out[5] = fg.y0; out[6] = fg.width; out[7] = fg.height;
+}
+
+void oo_interpolate(const oo_options *opt, const double grid[4], double x, double y, const double *phiL,
+                    const double *ExL, const double *EyL, const double *phiM, const double *ExM, const double *EyM,
+                    const double *phiR, const double *ExR, const double *EyR, int32_t quadratic, double param,
+                    double out[3]) {
+    Options O = make_options(opt);
+    size_t m = (size_t)O.o.nx * O.o.ny;
+    FieldPlanes L, M, R;
+    L.phi.assign(phiL, phiL + m); L.Ex.assign(ExL, ExL + m); L.Ey.assign(EyL, EyL + m);
+    R.phi.assign(phiR, phiR + m); R.Ex.assign(ExR, ExR + m); R.Ey.assign(EyR, EyR + m);
+    Grid g{grid[0], grid[1], grid[2], grid[3]};
+    if (quadratic) {
+        M.phi.assign(phiM, phiM + m); M.Ex.assign(ExM, ExM + m); M.Ey.assign(EyM, EyM + m);
+        interpolate_kick_quadratic(O, g, x, y, L, M, R, param, out[0], out[1], out[2]);
+    } else {
+        interpolate_kick(O, g, x, y, L, R, param, 1.0 - param, out[0], out[1], out[2]);
+    }
+}
+
+double oo_luminosity(const oo_options *opt, const double *x1, const double *y1, int64_t n1, const double *x2,
+                     const double *y2, int64_t n2, double klum, double *q1, double *q2) {
+    Options O = make_options(opt);
+    Workspace ws;
+    std::vector<double> a(x1, x1 + n1), b(y1, y1 + n1), c(x2, x2 + n2), d(y2, y2 + n2);
+    double lum;
+    try {
+        lum = luminosity(O, a, b, c, d, klum, ws);
+    } catch (OracleError &) {
+        return NAN;
+    }
+    if (q1) std::copy(ws.q1.begin(), ws.q1.end(), q1);
+    if (q2) std::copy(ws.q2.begin(), ws.q2.end(), q2);
+    return lum;
 }
 
 int oo_slices(int32_t method, int32_t ns, int32_t center_position, const double *positions, const double *z,

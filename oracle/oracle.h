@@ -84,6 +84,15 @@ void oo_deposit_drifted(int32_t method, const double *x, const double *px, const
 void oo_solve_field(const oo_options *opt, const double *x, const double *y, int64_t n, double sx0, double sy0,
                     double sw, double sh, double fx0, double fy0, double *phi, double *Ex, double *Ey);
 void oo_interpolation_grids(const oo_options *opt, const double b[8], double out[8]);
+/* _pic_interpolate_kick / _pic_interpolate_kick_quadratic on an nx*ny mesh (grid = x0, y0, w, h).
+   quadratic = 0: two-node with zL = param, zR = 1 - zL ; 1: three-node at t = param.  out = Kx, Ky, Kz. */
+void oo_interpolate(const oo_options *opt, const double grid[4], double x, double y, const double *phiL,
+                    const double *ExL, const double *EyL, const double *phiM, const double *ExM, const double *EyM,
+                    const double *phiR, const double *ExR, const double *EyR, int32_t quadratic, double param,
+                    double out[3]);
+/* _pic_luminosity! (pic_cpu.jl:2700-2736); q1, q2 receive the (lnx+1)*(lny+1) column-major deposits. */
+double oo_luminosity(const oo_options *opt, const double *x1, const double *y1, int64_t n1, const double *x2,
+                     const double *y2, int64_t n2, double klum, double *q1, double *q2);
 
 /* Slicing (slicing.jl:51-75, :normal_quantile / :specified). Outputs: boundary[ns+1], center[ns],
    weight[ns], count[ns], order[n] (slice-major member lists, ascending particle index). */

@@ -94,6 +94,9 @@ def lib():
                                          P(d), P(i64)]
         L.oo_solve_field.argtypes = [P(OOOptions), P(d), P(d), i64, d, d, d, d, d, d, P(d), P(d), P(d)]
         L.oo_interpolation_grids.argtypes = [P(OOOptions), P(d), P(d)]
+        L.oo_interpolate.argtypes = [P(OOOptions), P(d), d, d] + [P(d)] * 9 + [i32, d, P(d)]
+        L.oo_luminosity.restype = d
+        L.oo_luminosity.argtypes = [P(OOOptions), P(d), P(d), i64, P(d), P(d), i64, d, P(d), P(d)]
         L.oo_slices.restype = C.c_int
         L.oo_slices.argtypes = [i32, i32, i32, P(d), P(d), i64, P(d), P(d), P(d), P(i64), P(i64)]
         L.oo_pair_batches.restype = i32
@@ -314,3 +317,48 @@ def linear6d_matrix(beta, alpha, tune):
 
 def linear6d(m, beam):
     lib().oo_linear6d(_dp(np.ascontiguousarray(m, np.float64)), *[_dp(beam[k]) for k in range(6)], beam.shape[1])
+
+
+def solve_field(options: OracleOptions, x, y, source_grid, field_grid):
+    """One field solve on the oracle: returns (phi, Ex, Ey) as (nx, ny) column-major arrays."""
+    nx, ny = options.grid
+    x = np.ascontiguousarray(x, np.float64); y = np.ascontiguousarray(y, np.float64)
+    phi = np.empty(nx * ny); ex = np.empty(nx * ny); ey = np.empty(nx * ny)
+    o = options.to_c()
+    sx0, sy0, sw, sh = source_grid
+    fx0, fy0 = field_grid[0], field_grid[1]
+    lib().oo_solve_field(C.byref(o), _dp(x), _dp(y), x.size, sx0, sy0, sw, sh, fx0, fy0, _dp(phi), _dp(ex), _dp(ey))
+    f = lambda a: a.reshape(ny, nx).T.copy()  # column-major (i fastest) -> [i, j]
+    return f(phi), f(ex), f(ey)
+
+
+def interaction_grids(options: OracleOptions, sxmin, sxmax, symin, symax, fxmin, fxmax, fymin, fymax):
+    o = options.to_c()
+    b = np.array([sxmin, sxmax, symin, symax, fxmin, fxmax, fymin, fymax], np.float64)
+    out = np.empty(8)
+    lib().oo_interpolation_grids(C.byref(o), _dp(b), _dp(out))
+    return tuple(out[:4]), tuple(out[4:])
+
+
+def interpolate(options: OracleOptions, grid, x, y, L, R, param, M=None):
+    """Two-node (M is None, param = zL) or three-node (param = t) kick interpolation; planes are
+    (phi, Ex, Ey) tuples of (nx, ny) arrays indexed [i, j]."""
+    o = options.to_c()
+    g = np.asarray(grid, np.float64)
+    cm = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).T)  # [i, j] -> column-major memory
+    Ls = [cm(a) for a in L]; Rs = [cm(a) for a in R]; Ms = [cm(a) for a in (M if M is not None else L)]
+    out = np.empty(3)
+    lib().oo_interpolate(C.byref(o), _dp(g), float(x), float(y), *[_dp(a) for a in Ls], *[_dp(a) for a in Ms],
+                         *[_dp(a) for a in Rs], int(M is not None), float(param), _dp(out))
+    return tuple(out)
+
+
+def luminosity(options: OracleOptions, x1, y1, x2, y2, klum):
+    o = options.to_c()
+    nx, ny = options.luminosity_grid or options.grid
+    q1 = np.empty((nx + 1) * (ny + 1)); q2 = np.empty_like(q1)
+    a = [np.ascontiguousarray(v, np.float64) for v in (x1, y1, x2, y2)]
+    lum = lib().oo_luminosity(C.byref(o), _dp(a[0]), _dp(a[1]), a[0].size, _dp(a[2]), _dp(a[3]), a[2].size,
+                              float(klum), _dp(q1), _dp(q2))
+    f = lambda q: q.reshape(ny + 1, nx + 1).T.copy()
+    return lum, f(q1), f(q2)

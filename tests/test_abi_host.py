@@ -1,0 +1,103 @@
+"""C-ABI and host-side checks that need no GPU: the library loads and exports every declared entry
+point, the ctypes structures match the header's layout, the host quantiles match the oracle's, and
+the PICPoissonSolver mirror validates like the reference."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+import octo_b200 as ob
+from octo_b200 import _lib
+from oracle import oracle as orc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "octo_b200.h")
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    declared = set(re.findall(r"\b(octo_[a-z0-9_]+)\s*\(", open(HEADER).read()))
+    lib = _lib.lib()
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert declared == set(_lib.EXPORTS)
+    assert lib.octo_version() >= 1
+
+
+def _c_layout():
+    src = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "octo_b200.h"
+#define F(T, m) printf(#T " " #m " %zu\n", offsetof(T, m));
+int main(void) {
+  printf("octo_pic_options size %zu\n", sizeof(octo_pic_options));
+  printf("octo_beam size %zu\n", sizeof(octo_beam));
+  printf("octo_collide_report size %zu\n", sizeof(octo_collide_report));
+  F(octo_pic_options, grid_extent_sigma) F(octo_pic_options, longitudinal_kick) F(octo_pic_options, positions1)
+  F(octo_pic_options, kbb1) F(octo_pic_options, precision) F(octo_beam, x) F(octo_beam, pz)
+  F(octo_collide_report, turn) F(octo_collide_report, kernel_launches)
+  return 0;
+}
+"""
+    import tempfile
+    d = tempfile.mkdtemp()
+    c = os.path.join(d, "l.c")
+    open(c, "w").write(src)
+    exe = os.path.join(d, "l")
+    subprocess.run(["gcc", "-I", os.path.dirname(HEADER), c, "-o", exe], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+    return {tuple(line.split()[:2]): int(line.split()[2]) for line in out.splitlines()}
+
+
+def test_ctypes_structures_match_header_layout():
+    lay = _c_layout()
+    assert lay[("octo_pic_options", "size")] == C.sizeof(_lib.OctoPicOptions)
+    assert lay[("octo_beam", "size")] == C.sizeof(_lib.OctoBeam)
+    assert lay[("octo_collide_report", "size")] == C.sizeof(_lib.OctoCollideReport)
+    for (t, m), v in lay.items():
+        if m == "size":
+            continue
+        cls = {"octo_pic_options": _lib.OctoPicOptions, "octo_beam": _lib.OctoBeam,
+               "octo_collide_report": _lib.OctoCollideReport}[t]
+        assert getattr(cls, m).offset == v, (t, m)
+
+
+def test_host_quantiles_match_the_oracle_bitwise():
+    L = _lib.lib()
+    for ns in range(1, 65):
+        for s in range(1, ns):
+            x = 2 * s / ns - 1
+            assert L.octo_erfinv(x) == orc.erfinv(x)
+            assert L.octo_normal_quantile(s, ns) == 2 ** 0.5 * orc.erfinv(x)
+
+
+def test_solver_defaults_and_validation():
+    s = ob.PICPoissonSolver()
+    assert s.grid == (128, 128) and s.deposit_method == "CIC" and s.green_cache == "slice_pair"
+    assert s.slice_pair_green_min_ratio == 0.5 and s.slice_pair_green_growth == 0.25
+    with pytest.raises(ob.ArgumentError):
+        ob.PICPoissonSolver(field_derivative="sixth")
+    with pytest.raises(ob.ArgumentError):
+        ob.PICPoissonSolver(grid=(4, 16))
+    with pytest.raises(ob.ArgumentError):
+        ob.PICPoissonSolver(slice_pair_green_min_ratio=0.0)
+    with pytest.raises(ob.ArgumentError):
+        ob.PICPoissonSolver(interaction_grid="node", slice_interpolation="quadratic")
+    with pytest.raises(ob.ArgumentError):
+        ob.PICPoissonSolver(interaction_grid="node", grid_extent="sigma")
+    with pytest.raises(ob.ArgumentError):
+        ob.LongitudinalSlicing(nslices=3, method="specified", positions=[0.0])
+
+
+def test_gpu_backend_rejects_what_it_does_not_implement():
+    sl = ob.LongitudinalSlicing(nslices=3, method="normal_quantile")
+    for kw in (dict(interaction_grid="source_slice"), dict(grid_extent="sigma"), dict(green_type="lattice"),
+               dict(grid=(96, 96))):
+        with pytest.raises(ob.ArgumentError):
+            ob.PICPoissonSolver(slicing=sl, **kw).to_c()
+    with pytest.raises(ob.ArgumentError):
+        ob.PICPoissonSolver(slicing=ob.LongitudinalSlicing(nslices=3, method="equal_area")).to_c()
+    o = ob.PICPoissonSolver(slicing=sl, deposit_method="TSC", field_derivative="fourth").to_c()
+    assert (o.nx, o.deposit_method, o.field_derivative, o.nslices1) == (128, 1, 4, 3)
