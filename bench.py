@@ -209,7 +209,7 @@ def run_ours(args, rank, world, local_rank):
     he = torch.empty_like(e0, device="cpu").pin_memory()
     hp = torch.empty_like(p0, device="cpu").pin_memory()
     he.copy_(e0); hp.copy_(p0)
-    e2e_steps = max(3, min(args.steps, 20))
+    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, 20))
     torch.cuda.synchronize()
     barrier()
     w0 = time.perf_counter()
@@ -222,9 +222,9 @@ def run_ours(args, rank, world, local_rank):
         hp.copy_(p.coords, non_blocking=True)
     ev1.record(stream)
     torch.cuda.synchronize()
-    wall = (time.perf_counter() - w0) / e2e_steps
+    wall = (time.perf_counter() - w0) / max(e2e_steps, 1)
     barrier()
-    e2e_ms = ev0.elapsed_time(ev1) / e2e_steps
+    e2e_ms = ev0.elapsed_time(ev1) / e2e_steps if e2e_steps else float("nan")
     clk = clocks.stop()
 
     if world > 1:
@@ -288,6 +288,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
