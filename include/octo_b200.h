@@ -157,6 +157,28 @@ int32_t octo_set_timing(octo_ctx *ctx, int32_t enable); /* enabling also clears 
 int32_t octo_timing_report(octo_ctx *ctx, double ms[OCTO_NPHASES], int64_t launches[OCTO_NPHASES],
                            double bytes[OCTO_NPHASES]);
 
+/* Seeded Gaussian beam construction that allocates no device memory.
+ *
+ * This entry point has no counterpart in the reference.  It exists for callers that cannot call
+ * cudaMalloc: hosts whose device memory is owned by a pool allocator (Julia's CUDA.jl pool or
+ * PyTorch's caching allocator reserve the device up front, so an out-of-band allocation can fail
+ * or fragment their pool), and long-running services that forbid allocation after start-up.
+ * It needs no octo_ctx (creating one allocates).  Its reduction scratch lives in a fixed 32 KiB
+ * static device array inside libocto_b200.so, which every GPU that loads the library holds until
+ * process exit.  The limit that follows: n <= OCTO_NOALLOC_MAX_PARTICLES particles per call; larger
+ * beams are rejected with OCTO_ERR_ARG and a message in err.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current; make that first call before any stream capture.  All calls share the one array,
+ * so calls that overlap on the GPU (different streams, threads or processes sharing a context)
+ * race: serialise them.  The caller owns beam, and err (may be NULL) receives a message on failure.
+ * Output matches octo_beam_gaussian to rounding (its reduction uses a different block count). */
+#define OCTO_NOALLOC_PARTICLES_PER_BLOCK 8192
+#define OCTO_NOALLOC_MAX_BLOCKS 4094
+#define OCTO_NOALLOC_MAX_PARTICLES (OCTO_NOALLOC_PARTICLES_PER_BLOCK * OCTO_NOALLOC_MAX_BLOCKS)
+int32_t octo_beam_gaussian_noalloc(int32_t device, octo_beam *beam, uint64_t seed, uint64_t rng_id,
+                                   const double beta[3], const double alpha[3], const double sigma[3],
+                                   double cutoff, void *stream, char *err, int64_t err_len);
+
 /* Host-side helpers shared with the slicing: the normal quantile sqrt(2)*erfinv(2s/ns - 1)
  * used for :normal_quantile boundaries (slicing.jl:420-429), and the library version. */
 double octo_normal_quantile(int32_t s, int32_t ns);

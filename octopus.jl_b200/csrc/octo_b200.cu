@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1080,6 +1081,98 @@ int32_t octo_timing_report(octo_ctx *c, double ms[OCTO_NPHASES], int64_t launche
         if (ms) ms[k] = c->phase_ms[k];
         if (launches) launches[k] = c->phase_launches[k];
         if (bytes) bytes[k] = c->phase_bytes[k];
+    }
+    return OCTO_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- allocation-free beam construction
+// Reduction scratch of octo_beam_gaussian_noalloc: OCTO_NOALLOC_MAX_BLOCKS block partial sums followed
+// by the mean and sigma slots.  4096 doubles = 32 KiB, resident on every device that loads the library.
+static __device__ __align__(256) double g_noalloc_scratch[OCTO_NOALLOC_MAX_BLOCKS + 2];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+// Device address of g_noalloc_scratch per device, looked up once with that device current.  In host
+// code the symbol itself is only a host-side stand-in, so kernels are always given this address.
+double *g_noalloc_addr[kNoallocMaxDevices] = {nullptr};
+std::mutex g_noalloc_mutex;
+
+void noalloc_message(char *err, int64_t len, const std::string &m) {
+    if (!err || len <= 0) return;
+    size_t n = std::min<size_t>(m.size(), (size_t)len - 1);
+    std::memcpy(err, m.data(), n);
+    err[n] = 0;
+}
+}  // namespace
+
+extern "C" {
+
+int32_t octo_beam_gaussian_noalloc(int32_t device, octo_beam *beam, uint64_t seed, uint64_t rng_id,
+                                   const double beta[3], const double alpha[3], const double sigma[3], double cutoff,
+                                   void *stream, char *err, int64_t err_len) {
+    if (!beam || !beta || !alpha || !sigma) {
+        noalloc_message(err, err_len, "beam, beta, alpha and sigma must be non-NULL");
+        return OCTO_ERR_ARG;
+    }
+    std::string msg;
+    int rc = check_beam(beam, msg);
+    if (rc != OCTO_OK) {
+        noalloc_message(err, err_len, msg);
+        return rc;
+    }
+    if (beam->n > (int64_t)OCTO_NOALLOC_MAX_PARTICLES) {
+        noalloc_message(err, err_len, "octo_beam_gaussian_noalloc: " + std::to_string(beam->n) +
+                                          " particles exceed its fixed scratch limit of " +
+                                          std::to_string((long long)OCTO_NOALLOC_MAX_PARTICLES) +
+                                          "; use octo_beam_gaussian with a context");
+        return OCTO_ERR_ARG;
+    }
+    if (device < 0 || device >= kNoallocMaxDevices) {
+        noalloc_message(err, err_len, "device index out of range");
+        return OCTO_ERR_ARG;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) {
+        noalloc_message(err, err_len, "cudaSetDevice failed");
+        return OCTO_ERR_CUDA;
+    }
+    double *scratch;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_addr[device]) {
+            void *p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p) {
+                noalloc_message(err, err_len, std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+                return OCTO_ERR_CUDA;
+            }
+            g_noalloc_addr[device] = (double *)p;
+        }
+        scratch = g_noalloc_addr[device];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long n = beam->n;
+    const int nb = (int)std::max<long long>(1, (n + OCTO_NOALLOC_PARTICLES_PER_BLOCK - 1) / OCTO_NOALLOC_PARTICLES_PER_BLOCK);
+    double *partial = scratch;                         // nb entries, every one rewritten each pass
+    double *stats = scratch + OCTO_NOALLOC_MAX_BLOCKS;  // mean, sigma: written by the folds before use
+    double *comp[6] = {(double *)beam->x, (double *)beam->px, (double *)beam->y, (double *)beam->py,
+                       (double *)beam->z, (double *)beam->pz};
+    const unsigned grid = (unsigned)((n + 255) / 256);
+    for (int d = 0; d < 6; ++d) {
+        k_beam_normals<<<grid, 256, 0, st>>>(comp[d], n, seed, rng_id, d + 1, cutoff);
+        k_partial_sum<<<nb, 256, 0, st>>>(comp[d], n, stats, 0, partial);
+        k_fold_partials<<<1, 1, 0, st>>>(partial, nb, n, 0, stats);
+        k_partial_sum<<<nb, 256, 0, st>>>(comp[d], n, stats, 1, partial);
+        k_fold_partials<<<1, 1, 0, st>>>(partial, nb, n, 1, stats);
+        k_standardize<<<grid, 256, 0, st>>>(comp[d], n, stats);
+    }
+    for (int a = 0; a < 3; ++a)
+        k_twiss<<<grid, 256, 0, st>>>(comp[2 * a], comp[2 * a + 1], n, sigma[a], beta[a], alpha[a]);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        noalloc_message(err, err_len, std::string("kernel launch failed: ") + cudaGetErrorString(e));
+        return OCTO_ERR_CUDA;
     }
     return OCTO_OK;
 }
