@@ -20,20 +20,46 @@ __device__ __forceinline__ double2 conjg(double2 a) { return make_double2(a.x, -
 
 __device__ __forceinline__ int bitrev(int k, int lg) { return (int)(__brev((unsigned)k) >> (32 - lg)); }
 
-// Butterfly passes on a buffer already loaded in bit-reversed order.
+// Butterfly passes on a buffer already loaded in bit-reversed order.  Pairs of radix-2 DIT stages
+// (half-sizes h and 2h) are merged into one radix-2^2 pass over groups of four elements
+// {i, i+h, i+2h, i+3h}: half the shared-memory round trips and warp syncs of plain radix-2, with the
+// same twiddles (the second-stage twiddle of the odd pair is -i times that of the even pair, applied
+// exactly by a swap and a sign change).  An odd log2(L) starts with one radix-2 pass.
 __device__ __forceinline__ void warp_fft_passes(double2 *a, int L, const double2 *tw, bool inv) {
     const int lane = threadIdx.x & 31;
     __syncwarp();
-    for (int half = 1, step = L >> 1; half < L; half <<= 1, step >>= 1) {
+    int half = 1, step = L >> 1;
+    const int lg = 31 - __clz(L);
+    if (lg & 1) {  // one radix-2 pass (half = 1, twiddle 1)
         for (int b = lane; b < (L >> 1); b += 32) {
-            int j = b & (half - 1);
-            int i0 = ((b & ~(half - 1)) << 1) | j;
-            double2 w = tw[j * step];
-            if (inv) w.y = -w.y;
-            double2 u = a[i0];
-            double2 v = cmul(a[i0 + half], w);
+            const int i0 = b << 1;
+            const double2 u = a[i0], v = a[i0 + 1];
             a[i0] = cadd(u, v);
-            a[i0 + half] = csub(u, v);
+            a[i0 + 1] = csub(u, v);
+        }
+        __syncwarp();
+        half = 2;
+        step >>= 1;
+    }
+    for (; half < L; half <<= 2, step >>= 2) {
+        // groups of 4h elements; within each, j in [0, h): elements j, j+h, j+2h, j+3h
+        const int quads = L >> 2;
+        for (int b = lane; b < quads; b += 32) {
+            const int j = b & (half - 1);
+            const int i0 = ((b & ~(half - 1)) << 2) | j;
+            double2 w1 = tw[j * step];          // W_{2h}^j
+            double2 w2 = tw[j * (step >> 1)];   // W_{4h}^j
+            if (inv) { w1.y = -w1.y; w2.y = -w2.y; }
+            const double2 x0 = a[i0], x1 = a[i0 + half], x2 = a[i0 + 2 * half], x3 = a[i0 + 3 * half];
+            const double2 t1 = cmul(x1, w1), t3 = cmul(x3, w1);
+            const double2 a0 = cadd(x0, t1), a1 = csub(x0, t1), a2 = cadd(x2, t3), a3 = csub(x2, t3);
+            const double2 u2 = cmul(a2, w2), v3 = cmul(a3, w2);
+            // w3 = W_{4h}^{j+h} = w2 * (-i) forward, w2 * (+i) inverse
+            const double2 u3 = inv ? make_double2(-v3.y, v3.x) : make_double2(v3.y, -v3.x);
+            a[i0] = cadd(a0, u2);
+            a[i0 + 2 * half] = csub(a0, u2);
+            a[i0 + half] = cadd(a1, u3);
+            a[i0 + 3 * half] = csub(a1, u3);
         }
         __syncwarp();
     }

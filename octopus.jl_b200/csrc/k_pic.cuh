@@ -30,9 +30,10 @@ struct Collide {           // device pointers for one collide (passed by value)
     int scratch_green0;        // first scratch Green slot (green_cache = :none)
     long long *qgrid;          // int64 charge grids: plane-in-front * nx*ny
     double2 *spec;             // spectral scratch: plane-in-front * (nx+1)*ny
-    double *fields;            // plane-in-front * 3 * nx*ny  (phi, Ex, Ey)
+    double2 *fields;           // plane-in-front * 2 * nx*ny: per cell (phi, Ex), (Ey, 0)
     long long *lq;             // luminosity grids: (pair-in-front*2 + side) * (lnx+1)*(lny+1)
     double *lum_parts;         // [pair position]
+    double *lum_partial;       // [pair-in-front][kLumSplit] overlap partial sums
     const double2 *tw_x, *tw_y;  // twiddles for 2nx and 2ny
     SoA beam[2];
     double klum;
@@ -57,7 +58,11 @@ __device__ __forceinline__ unsigned long long shfl_max_u64(unsigned long long v)
 // Extremes of one slice of a pair in all three roles it plays: source of one direction
 // (drifted to sL and sR, pic_cpu.jl:961-1003), field of the other (drifted to its collision
 // point, pic_cpu.jl:1005-1035) and luminosity source (drifted to sM, pic_cpu.jl:1279-1287).
+// LUM_ONLY (interaction_grid = :node, whose meshes are prebuilt) keeps only the luminosity role.
+// Per-thread extrema use the native min/max (NaN is flagged separately; a +-0 tie cannot change any
+// geometry built from them), encoded to ordered integers once per block for the atomics.
 // grid: (blocks per side, 2 * pairs in front).
+template <bool LUM_ONLY>
 __global__ void __launch_bounds__(256) k_pair_bounds(Collide C, int task0) {
     const int q = blockIdx.y >> 1, side = blockIdx.y & 1;
     const int t1 = task0 + 2 * q, t2 = t1 + 1;
@@ -68,42 +73,42 @@ __global__ void __launch_bounds__(256) k_pair_bounds(Collide C, int task0) {
     const SoA S = C.beam[side];
     const long long st = src_task.src_start, n = src_task.src_n;
     const double sL = src_task.sL, sR = src_task.sR, sM = src_task.sM, cf = fld_task.c_src;
-    unsigned long long mn[6], mx[6];
-    for (int k = 0; k < 6; ++k) { mn[k] = kOrdMinInit; mx[k] = kOrdMaxInit; }
+    double mn[6], mx[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) { mn[k] = INFINITY; mx[k] = -INFINITY; }
     bool nan_s = false, nan_f = false, nan_l = false;
+    const double *X = S.c[0] + st, *PX = S.c[1] + st, *Y = S.c[2] + st, *PY = S.c[3] + st, *Z = S.c[4] + st;
+#pragma unroll 4
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-        double x = S.c[0][st + k], px = S.c[1][st + k], y = S.c[2][st + k], py = S.c[3][st + k], z = S.c[4][st + k];
-        double v[6];
-        v[0] = x + px * sL;
-        v[1] = x + px * sR;
-        v[2] = y + py * sL;
-        v[3] = y + py * sR;
-        double s = 0.5 * (z - cf);
-        v[4] = x + s * px;
-        v[5] = y + s * py;
-        double lx = x + px * sM, ly = y + py * sM;
-        nan_s |= (v[0] != v[0]) | (v[1] != v[1]) | (v[2] != v[2]) | (v[3] != v[3]);
-        nan_f |= (v[4] != v[4]) | (v[5] != v[5]);
+        const double x = X[k], px = PX[k], y = Y[k], py = PY[k];
+        const double lx = x + px * sM, ly = y + py * sM;
         nan_l |= (lx != lx) | (ly != ly);
-        unsigned long long e;
-        // source x (0), source y (1), field x (2), field y (3), lum x (4), lum y (5)
-        e = ord_encode(v[0]); mn[0] = min(mn[0], e); mx[0] = max(mx[0], e);
-        e = ord_encode(v[1]); mn[0] = min(mn[0], e); mx[0] = max(mx[0], e);
-        e = ord_encode(v[2]); mn[1] = min(mn[1], e); mx[1] = max(mx[1], e);
-        e = ord_encode(v[3]); mn[1] = min(mn[1], e); mx[1] = max(mx[1], e);
-        e = ord_encode(v[4]); mn[2] = min(mn[2], e); mx[2] = max(mx[2], e);
-        e = ord_encode(v[5]); mn[3] = min(mn[3], e); mx[3] = max(mx[3], e);
-        e = ord_encode(lx); mn[4] = min(mn[4], e); mx[4] = max(mx[4], e);
-        e = ord_encode(ly); mn[5] = min(mn[5], e); mx[5] = max(mx[5], e);
+        mn[4] = fmin(mn[4], lx); mx[4] = fmax(mx[4], lx);
+        mn[5] = fmin(mn[5], ly); mx[5] = fmax(mx[5], ly);
+        if (!LUM_ONLY) {
+            const double z = Z[k];
+            const double a = x + px * sL, b = x + px * sR, c = y + py * sL, d = y + py * sR;
+            const double s = 0.5 * (z - cf);
+            const double fx = x + s * px, fy = y + s * py;
+            nan_s |= (a != a) | (b != b) | (c != c) | (d != d);
+            nan_f |= (fx != fx) | (fy != fy);
+            mn[0] = fmin(mn[0], fmin(a, b)); mx[0] = fmax(mx[0], fmax(a, b));
+            mn[1] = fmin(mn[1], fmin(c, d)); mx[1] = fmax(mx[1], fmax(c, d));
+            mn[2] = fmin(mn[2], fx); mx[2] = fmax(mx[2], fx);
+            mn[3] = fmin(mn[3], fy); mx[3] = fmax(mx[3], fy);
+        }
     }
     __shared__ unsigned long long red[8][12];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
     for (int k = 0; k < 6; ++k) {
-        unsigned long long a = shfl_min_u64(mn[k]), b = shfl_max_u64(mx[k]);
+        if (LUM_ONLY && k < 4) continue;
+        unsigned long long a = shfl_min_u64(mn[k] == INFINITY ? kOrdMinInit : ord_encode(mn[k]));
+        unsigned long long b = shfl_max_u64(mx[k] == -INFINITY ? kOrdMaxInit : ord_encode(mx[k]));
         if (lane == 0) { red[warp][2 * k] = a; red[warp][2 * k + 1] = b; }
     }
     int any_s = __syncthreads_or(nan_s), any_f = __syncthreads_or(nan_f), any_l = __syncthreads_or(nan_l);
-    if (threadIdx.x < 12) {
+    if (threadIdx.x < 12 && !(LUM_ONLY && threadIdx.x < 8)) {
         int k = threadIdx.x;
         unsigned long long r = red[0][k];
         for (int w = 1; w < (int)(blockDim.x >> 5); ++w) r = (k & 1) ? max(r, red[w][k]) : min(r, red[w][k]);
@@ -262,15 +267,21 @@ __device__ __forceinline__ double green_value(int green_type, int i, int j, int 
     return hxihyi * val;
 }
 
-// Green table rows evaluated in registers and transformed along x: two table rows per warp as one
-// complex line, written as the nx+1 non-redundant x-frequencies of each row into the slot.
+// Green table rows transformed along x: two table rows per warp as one complex line, written as
+// the nx+1 non-redundant x-frequencies of each row into the slot.  A block covers kGreenRows
+// consecutive table rows.  For :integrated the four corner integrals of a cell are shared with its
+// neighbours: the block evaluates F once on the (2nx+1) x (kGreenRows+1) corner lattice in shared
+// memory (corner a is (dx0 + (a-1)hx) + hx/2, bit-equal to the reference's "+" corner of cell a-1),
+// 3.5x fewer log/atan evaluations than four per cell.
 // mode 0: blockIdx.y = task of the front (only tasks that rebuild); mode 1: blockIdx.y = node mesh.
+constexpr int kGreenRows = 8;
 __global__ void __launch_bounds__(128) k_green_rows(Collide C, int mode, int base, int node_slot0) {
     extern __shared__ double2 sm[];
     const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx, NY = 2 * ny;
-    int lgx = 31 - __clz(NX);
+    const int lgx = 31 - __clz(NX);
     double2 *tw = sm;
-    double2 *line = sm + NX / 2 + (threadIdx.x >> 5) * NX;
+    double2 *lines = sm + NX / 2;
+    double *corner = (double *)(lines + 4 * NX);  // (kGreenRows + 1) x (NX + 1)
     Grid sg, fg;
     int slot;
     if (mode == 0) {
@@ -283,27 +294,58 @@ __global__ void __launch_bounds__(128) k_green_rows(Collide C, int mode, int bas
         sg = M.sg; fg = M.fg; slot = node_slot0 + base + blockIdx.y;
     }
     load_twiddles(tw, C.tw_x, NX);
-    __syncthreads();
     const double hx = sg.w / (double)(nx - 1), hy = sg.h / (double)(ny - 1);
     const double dx0 = fg.x0 - sg.x0, dy0 = fg.y0 - sg.y0;
-    const int lane = threadIdx.x & 31;
-    const int pair = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (2 * pair >= NY) return;
-    const int j0 = 2 * pair, j1 = j0 + 1;
-    for (int i = lane; i < NX; i += 32) {
-        double a = green_value(C.o.green_type, i, j0, nx, ny, dx0, dy0, hx, hy);
-        double b = green_value(C.o.green_type, i, j1, nx, ny, dx0, dy0, hx, hy);
-        line[bitrev(i, lgx)] = make_double2(a, b);
+    const double half_hx = hx / 2, half_hy = hy / 2;
+    const int j0 = blockIdx.x * kGreenRows;             // table rows j0 .. j0+7 (never straddle ny)
+    const int jj0 = j0 < ny ? j0 : j0 - NY;             // wrapped row index of j0
+    const bool integrated = C.o.green_type == 0;
+    if (integrated) {
+        for (int e = threadIdx.x; e < (kGreenRows + 1) * (NX + 1); e += blockDim.x) {
+            const int rb = e / (NX + 1), ca = e % (NX + 1);
+            const int b = jj0 + rb, a = ca - nx;           // corner indices: cell b-1 "+" corner
+            const double X = a > -nx ? (dx0 + (double)(a - 1) * hx) + half_hx : (dx0 + (double)a * hx) - half_hx;
+            const double Y = b > -ny ? (dy0 + (double)(b - 1) * hy) + half_hy : (dy0 + (double)b * hy) - half_hy;
+            corner[e] = kernel_integral(X, Y);
+        }
     }
-    warp_fft_passes(line, NX, tw, false);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double hxihyi = -0.5 / (hx * hy);
+    double2 *line = lines + warp * NX;
     double2 *out = C.ghat + (long long)slot * C.gstride;
-    for (int k = lane; k <= nx; k += 32) {
-        double2 zk = line[k], zm = conjg(line[(NX - k) & (NX - 1)]);
-        double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y + zm.y));
-        double2 D = csub(zk, zm);
-        double2 Bv = make_double2(0.5 * D.y, -0.5 * D.x);
-        out[(long long)k * NY + j0] = A;
-        out[(long long)k * NY + j1] = Bv;
+    for (int pr = warp; 2 * pr < kGreenRows; pr += 4) {
+        const int r0 = 2 * pr;  // local rows r0, r0+1
+        for (int i = lane; i < NX; i += 32) {
+            const int ii = i < nx ? i : i - NX;
+            double g[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int r = r0 + q;
+                if (integrated) {
+                    const double *lo = corner + r * (NX + 1), *hi = corner + (r + 1) * (NX + 1);
+                    const int a = ii + nx;  // corner column of the cell's "-" x corner
+                    double val = hi[a + 1];  // F(x+, y+)
+                    val += lo[a];            // F(x-, y-)
+                    val -= lo[a + 1];        // F(x+, y-)
+                    val -= hi[a];            // F(x-, y+)
+                    g[q] = hxihyi * val;
+                } else {
+                    g[q] = green_value(C.o.green_type, i, j0 + r, nx, ny, dx0, dy0, hx, hy);
+                }
+            }
+            line[bitrev(i, lgx)] = make_double2(g[0], g[1]);
+        }
+        warp_fft_passes(line, NX, tw, false);
+        const int ja = j0 + r0, jb = ja + 1;
+        for (int k = lane; k <= nx; k += 32) {
+            double2 zk = line[k], zm = conjg(line[(NX - k) & (NX - 1)]);
+            double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y + zm.y));
+            double2 D = csub(zk, zm);
+            out[(long long)k * NY + ja] = A;
+            out[(long long)k * NY + jb] = make_double2(0.5 * D.y, -0.5 * D.x);
+        }
+        __syncwarp();
     }
 }
 
@@ -335,40 +377,48 @@ __global__ void __launch_bounds__(128) k_green_cols(Collide C, int mode, int bas
 }
 
 // ------------------------------------------------------------------ deposition
-// Fixed-point deposit of a particle range into an int64 grid (ld = nw) with CIC/TSC weights:
-// (pic_cpu.jl:2129-2146).  Taps are round(w * 2^bits); zero taps are skipped.
+// Fixed-point CIC/TSC taps of one particle (pic_cpu.jl:2129-2146): q = round(w * 2^bits) added to an int64
+// grid (a block-private shared-memory copy, merged into the plane's grid at the end of the block).
+// The shared grid is addressed through an opaque generic pointer (generic_ptr): measured on B200, a
+// 64-bit atomic add to shared memory issued on a generic address runs at 10.3 per clock per SM (4.1 under
+// 4-way conflicts) against 5.2 (1.6) when the compiler sees the shared address space.  Measured
+// alternatives, all slower on the production turn: 32-bit split accumulators (two atomics per tap),
+// warp-aggregated runs of equal cells, batched loads, and spatially sorted particles.
+template <class T>
+__device__ __forceinline__ T *generic_ptr(T *p) {
+    asm("" : "+l"(p));  // hide the address space from the compiler
+    return p;
+}
 template <int METHOD>
-__device__ __forceinline__ void deposit_taps(double u, double v, int nw, int nh, double scale, long long *grid, int ld,
-                                             bool shared_grid) {
-    if (METHOD == 0) {
-        int ix, iy; double wx[2], wy[2];
-        cic_weights(u, nw, ix, wx);
-        cic_weights(v, nh, iy, wy);
+__device__ __forceinline__ void deposit_taps(double u, double v, int nw, int nh, double scale, long long *grid, int ld) {
+    constexpr int NT = METHOD == 0 ? 2 : 3;
+    int ix, iy;
+    double wx[NT], wy[NT];
+    if (METHOD == 0) { cic_weights(u, nw, ix, wx); cic_weights(v, nh, iy, wy); }
+    else { tsc_weights(u, nw, ix, wx); tsc_weights(v, nh, iy, wy); }
+    const int c0 = (iy - 1) * ld + (ix - 1);
 #pragma unroll
-        for (int m = 0; m < 2; ++m)
+    for (int m = 0; m < NT; ++m)
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                long long qv = __double2ll_rn(wx[m] * wy[k] * scale);
-                if (qv) atomicAdd((unsigned long long *)&grid[(iy + k - 1) * ld + (ix + m - 1)], (unsigned long long)qv);
-            }
-    } else {
-        int ix, iy; double wx[3], wy[3];
-        tsc_weights(u, nw, ix, wx);
-        tsc_weights(v, nh, iy, wy);
-#pragma unroll
-        for (int m = 0; m < 3; ++m)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                long long qv = __double2ll_rn(wx[m] * wy[k] * scale);
-                if (qv) atomicAdd((unsigned long long *)&grid[(iy + k - 1) * ld + (ix + m - 1)], (unsigned long long)qv);
-            }
+        for (int k = 0; k < NT; ++k) {
+            const long long qv = __double2ll_rn(wx[m] * wy[k] * scale);
+            if (qv) atomicAdd((unsigned long long *)&grid[c0 + k * ld + m], (unsigned long long)qv);
+        }
+}
+
+// Merge a block's shared-memory grid into the plane's int64 grid.
+__device__ __forceinline__ void merge_grid(const long long *sq, long long *g, int cells) {
+    for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+        const long long v = sq[c];
+        if (v) atomicAdd((unsigned long long *)&g[c], (unsigned long long)v);
     }
 }
 
-// Field-solve planes of a front.  grid: (blocks per plane, planes in front); dynamic shared memory
-// holds a private int64 copy of the nx*ny grid when it fits (use_smem), merged with global atomics.
+// Field-solve planes of a front.  grid: (blocks per plane, planes in front); each block deposits a
+// grid-stride share of its plane's source slice into a private int64 copy of the nx*ny grid in shared
+// memory, then merges it with global atomics (the consumer, k_conv_rows, clears the grid it reads).
 template <int METHOD>
-__global__ void __launch_bounds__(512) k_deposit(Collide C, int plane0, int use_smem) {
+__global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
     extern __shared__ long long sq[];
     const int pl = blockIdx.y;
     const Plane &P = C.planes[plane0 + pl];
@@ -381,89 +431,76 @@ __global__ void __launch_bounds__(512) k_deposit(Collide C, int plane0, int use_
         if (G.green < 0) return;
         sg = G.sg;
     }
+    for (int c = threadIdx.x; c < cells; c += blockDim.x) sq[c] = 0;
+    __syncthreads();
+    long long *acc = generic_ptr(sq);
     const double hx = sg.w / (double)(nx - 1), hy = sg.h / (double)(ny - 1);
     const double hxi = 1.0 / hx, hyi = 1.0 / hy;
     const double scale = ldexp(1.0, P.fixed_bits);
-    long long *gq = C.qgrid + (long long)pl * cells;
-    long long *dst = use_smem ? sq : gq;
-    if (use_smem) {
-        for (int c = threadIdx.x; c < cells; c += blockDim.x) sq[c] = 0;
-        __syncthreads();
-    }
     const SoA S = C.beam[P.src_beam];
     const double s = P.s;
     const double xlo = sg.x0, xhi = sg.x0 + sg.w, ylo = sg.y0, yhi = sg.y0 + sg.h;
     int outside = 0;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < P.src_n; k += (long long)gridDim.x * blockDim.x) {
-        long long p = P.src_start + k;
-        double xd = S.c[0][p] + S.c[1][p] * s;
-        double yd = S.c[2][p] + S.c[3][p] * s;
+        const long long p = P.src_start + k;
+        const double xd = S.c[0][p] + S.c[1][p] * s;
+        const double yd = S.c[2][p] + S.c[3][p] * s;
         if (P.count_dropped && !(isfinite(xd) && xlo <= xd && xd <= xhi && isfinite(yd) && ylo <= yd && yd <= yhi))
             ++outside;
-        deposit_taps<METHOD>((xd - sg.x0) * hxi, (yd - sg.y0) * hyi, nx, ny, scale, dst, nx, use_smem);
+        deposit_taps<METHOD>((xd - sg.x0) * hxi, (yd - sg.y0) * hyi, nx, ny, scale, acc, nx);
     }
     if (P.count_dropped) {
         for (int o = 16; o; o >>= 1) outside += __shfl_xor_sync(0xffffffffu, outside, o);
         if ((threadIdx.x & 31) == 0 && outside) atomicAdd((unsigned long long *)&C.status->dropped, (unsigned long long)outside);
     }
-    if (use_smem) {
-        __syncthreads();
-        for (int c = threadIdx.x; c < cells; c += blockDim.x) {
-            long long v = sq[c];
-            if (v) atomicAdd((unsigned long long *)&gq[c], (unsigned long long)v);
-        }
-    }
+    __syncthreads();
+    merge_grid(sq, C.qgrid + (long long)pl * cells, cells);
 }
 
 // Luminosity planes: 2 per pair (side 0 = beam-1 slice i at sM1, side 1 = beam-2 slice j at sM2)
 // on the (lnx+1) x (lny+1) overlap mesh (pic_cpu.jl:2724-2735).
 template <int METHOD>
-__global__ void __launch_bounds__(512) k_lum_deposit(Collide C, int lj0, int use_smem) {
+__global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0) {
     extern __shared__ long long sq[];
     const int ql = blockIdx.y >> 1, side = blockIdx.y & 1;
     const LumJob &J = C.lumjobs[lj0 + ql];
     const LumGeom &L = C.lumgeom[J.pair];
     if (!L.ok) return;
     const int nw = C.o.lnx + 1, nh = C.o.lny + 1, cells = nw * nh;
-    long long *gq = C.lq + (long long)blockIdx.y * cells;
-    long long *dst = use_smem ? sq : gq;
-    if (use_smem) {
-        for (int c = threadIdx.x; c < cells; c += blockDim.x) sq[c] = 0;
-        __syncthreads();
-    }
+    for (int c = threadIdx.x; c < cells; c += blockDim.x) sq[c] = 0;
+    __syncthreads();
+    long long *acc = generic_ptr(sq);
     const SoA S = C.beam[side];
     const long long st = side ? J.s2_start : J.s1_start, n = side ? J.s2_n : J.s1_n;
     const double s = side ? J.sM2 : J.sM1;
     const double scale = ldexp(1.0, side ? J.bits2 : J.bits1);
     const double hxi = 1.0 / L.hx, hyi = 1.0 / L.hy;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-        long long p = st + k;
-        double vx = S.c[0][p] + S.c[1][p] * s;
-        double vy = S.c[2][p] + S.c[3][p] * s;
-        deposit_taps<METHOD>((vx - L.x0) * hxi, (vy - L.y0) * hyi, nw, nh, scale, dst, nw, use_smem);
+        const long long p = st + k;
+        const double vx = S.c[0][p] + S.c[1][p] * s;
+        const double vy = S.c[2][p] + S.c[3][p] * s;
+        deposit_taps<METHOD>((vx - L.x0) * hxi, (vy - L.y0) * hyi, nw, nh, scale, acc, nw);
     }
-    if (use_smem) {
-        __syncthreads();
-        for (int c = threadIdx.x; c < cells; c += blockDim.x) {
-            long long v = sq[c];
-            if (v) atomicAdd((unsigned long long *)&gq[c], (unsigned long long)v);
-        }
-    }
+    __syncthreads();
+    merge_grid(sq, C.lq + (long long)blockIdx.y * cells, cells);
 }
 
-// Overlap integral per pair: sum q1*q2 over the full (nx+1)(ny+1) extent times klum/(hx hy)
-// (pic_cpu.jl:2725-2736).  Clears both grids for the next front.
+// Overlap integral per pair: sum q1*q2 over the full (nx+1)(ny+1) extent (pic_cpu.jl:2725-2736),
+// split over kLumSplit blocks per pair into fixed partial sums (deterministic), clearing both grids for
+// the next front.  k_lum_fold adds the partials in order and applies klum/(hx hy).
+constexpr int kLumSplit = 16;
 __global__ void __launch_bounds__(256) k_lum_overlap(Collide C, int lj0) {
-    const int ql = blockIdx.x;
+    const int ql = blockIdx.y, part = blockIdx.x;
     const LumJob &J = C.lumjobs[lj0 + ql];
-    const LumGeom &L = C.lumgeom[J.pair];
     const int cells = (C.o.lnx + 1) * (C.o.lny + 1);
+    const int per = (cells + kLumSplit - 1) / kLumSplit;
+    const int c0 = part * per, c1 = min(cells, c0 + per);
     long long *q1 = C.lq + (long long)(2 * ql) * cells;
     long long *q2 = q1 + cells;
     const double i1 = ldexp(1.0, -J.bits1), i2 = ldexp(1.0, -J.bits2);
     double acc = 0.0;
-    for (int c = threadIdx.x; c < cells; c += blockDim.x) {
-        long long a = q1[c], b = q2[c];
+    for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+        const long long a = q1[c], b = q2[c];
         if (a && b) acc += ((double)a * i1) * ((double)b * i2);
         if (a) q1[c] = 0;
         if (b) q2[c] = 0;
@@ -475,10 +512,19 @@ __global__ void __launch_bounds__(256) k_lum_overlap(Collide C, int lj0) {
         if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
         __syncthreads();
     }
-    if (threadIdx.x == 0 && L.ok) {
-        double hxi = 1.0 / L.hx, hyi = 1.0 / L.hy;
-        C.lum_parts[J.pair] = red[0] * C.klum * hxi * hyi;
-    }
+    if (threadIdx.x == 0) C.lum_partial[(long long)ql * kLumSplit + part] = red[0];
+}
+
+__global__ void k_lum_fold(Collide C, int lj0, int nl) {
+    const int ql = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ql >= nl) return;
+    const LumJob &J = C.lumjobs[lj0 + ql];
+    const LumGeom &L = C.lumgeom[J.pair];
+    if (!L.ok) return;
+    double s = 0.0;
+    for (int k = 0; k < kLumSplit; ++k) s += C.lum_partial[(long long)ql * kLumSplit + k];
+    const double hxi = 1.0 / L.hx, hyi = 1.0 / L.hy;
+    C.lum_parts[J.pair] = s * C.klum * hxi * hyi;
 }
 
 // ------------------------------------------------------------------ FFT convolution
@@ -509,11 +555,11 @@ __global__ void __launch_bounds__(128) k_conv_rows(Collide C, int plane0) {
     for (int i = lane; i < NX; i += 32) {
         double a = 0.0, b = 0.0;
         if (i < nx) {
-            long long qa = q[(long long)j0 * nx + i];
+            const long long qa = q[(long long)j0 * nx + i];
             a = (double)qa * inv;
             if (qa) q[(long long)j0 * nx + i] = 0;
             if (j1 < ny) {
-                long long qb = q[(long long)j1 * nx + i];
+                const long long qb = q[(long long)j1 * nx + i];
                 b = (double)qb * inv;
                 if (qb) q[(long long)j1 * nx + i] = 0;
             }
@@ -614,7 +660,7 @@ __global__ void __launch_bounds__(128) k_conv_field(Collide C, int plane0) {
     const double hxi = 1.0 / hx, hyi = 1.0 / hy;
     const double c4 = 1.0 / 12.0;
     const bool fourth = C.o.fourth != 0;
-    double *F = C.fields + (long long)pl * 3 * nx * ny;
+    double2 *F = C.fields + (long long)pl * 2 * nx * ny;
     auto Pv = [&](int i, int j) { return phi[(j - ja0) * nx + i]; };  // 0-based i, j
     for (int idx = threadIdx.x; idx < (jt1 - jt0) * nx; idx += blockDim.x) {
         const int j = jt0 + idx / nx, i = idx % nx;
@@ -632,141 +678,201 @@ __global__ void __launch_bounds__(128) k_conv_field(Collide C, int plane0) {
         else if (fourth) ex = c4 * hxi * ((Pv(i + 2, j) - Pv(i - 2, j)) + 8 * (Pv(i - 1, j) - Pv(i + 1, j)));
         else ex = 0.5 * hxi * (Pv(i - 1, j) - Pv(i + 1, j));
         long long o = (long long)j * nx + i;
-        F[o] = Pv(i, j);
-        F[(long long)nx * ny + o] = ex;
-        F[2LL * nx * ny + o] = ey;
+        F[2 * o] = make_double2(Pv(i, j), ex);
+        F[2 * o + 1] = make_double2(ey, 0.0);
     }
 }
 
 // ------------------------------------------------------------------ kick
-// Gather E and phi at one particle; two-node planes L and R (pic_cpu.jl:2596-2619).
+// Field planes are interleaved per cell as (phi, Ex), (Ey, 0), so one tap of one plane is a single
+// 32-byte sector.  Weights and taps follow _pic_interpolate_kick (pic_cpu.jl:2596-2619), x-outer.
 template <int METHOD>
-__device__ __forceinline__ void gather_lr(const DevOptions &o, const Grid &g, double x, double y, const double *L,
-                                          const double *R, double zL, double zR, bool same, double &Kx, double &Ky,
-                                          double &Kz) {
-    const int nx = o.nx, ny = o.ny;
-    const long long pc = (long long)nx * ny;
-    double hx = g.w / (double)(nx - 1), hy = g.h / (double)(ny - 1);
-    double u = (x - g.x0) / hx, v = (y - g.y0) / hy;
-    Kx = 0.0; Ky = 0.0; Kz = 0.0;
-    constexpr int NT = METHOD == 0 ? 2 : 3;
-    int ix, iy; double wx[NT], wy[NT];
-    if (METHOD == 0) { cic_weights(u, nx, ix, wx); cic_weights(v, ny, iy, wy); }
-    else { tsc_weights(u, nx, ix, wx); tsc_weights(v, ny, iy, wy); }
+struct Taps {
+    static constexpr int NT = METHOD == 0 ? 2 : 3;
+    int c0;          // first cell (x-outer, y-inner order follows from c0 + m + k*nx)
+    double w[NT * NT];
+    // hxi, hyi: reciprocals of the mesh spacing g.w/(nx-1), g.h/(ny-1), computed once per block.  The
+    // reference divides by the spacing (pic_cpu.jl:2601-2602); the product differs from that quotient
+    // by at most 1.5 ulp of u, a ~1e-14 relative change of the interpolation weights.
+    __device__ __forceinline__ Taps(const DevOptions &o, const Grid &g, double hxi, double hyi, double x, double y) {
+        const double u = (x - g.x0) * hxi, v = (y - g.y0) * hyi;
+        int ix, iy; double wx[NT], wy[NT];
+        if (METHOD == 0) { cic_weights(u, o.nx, ix, wx); cic_weights(v, o.ny, iy, wy); }
+        else { tsc_weights(u, o.nx, ix, wx); tsc_weights(v, o.ny, iy, wy); }
+        c0 = (iy - 1) * o.nx + (ix - 1);
 #pragma unroll
-    for (int m = 0; m < NT; ++m)
+        for (int m = 0; m < NT; ++m)
 #pragma unroll
-        for (int k = 0; k < NT; ++k) {
-            long long c = (long long)(iy + k - 1) * nx + (ix + m - 1);
-            double w = wx[m] * wy[k];
-            if (same) {  // zL = 1, zR = 0: 1*E + 0*E == E for finite E
-                Kx += w * (zL * L[pc + c] + zR * L[pc + c]);
-                Ky += w * (zL * L[2 * pc + c] + zR * L[2 * pc + c]);
-                Kz += w * (L[c] - R[c]);
-            } else {
-                Kx += w * (zL * L[pc + c] + zR * R[pc + c]);
-                Ky += w * (zL * L[2 * pc + c] + zR * R[2 * pc + c]);
-                Kz += w * (L[c] - R[c]);
-            }
-        }
-}
+            for (int k = 0; k < NT; ++k) w[m * NT + k] = wx[m] * wy[k];
+    }
+    __device__ __forceinline__ int cell(int t, int nx) const { return c0 + (t / NT) + (t % NT) * nx; }
+};
 
-// Three-node planes (pic_cpu.jl:2648-2680).
-template <int METHOD>
-__device__ __forceinline__ void gather_lmr(const DevOptions &o, const Grid &g, double x, double y, const double *L,
-                                           const double *M, const double *R, double t, double &Kx, double &Ky,
-                                           double &Kz) {
-    const int nx = o.nx, ny = o.ny;
-    const long long pc = (long long)nx * ny;
-    double hx = g.w / (double)(nx - 1), hy = g.h / (double)(ny - 1);
-    double u = (x - g.x0) / hx, v = (y - g.y0) / hy;
-    double t2 = t * t;
-    double aL = 2.0 * t2 - 3.0 * t + 1.0, aM = 4.0 * t - 4.0 * t2, aR = 2.0 * t2 - t;
-    double bL = 3.0 - 4.0 * t, bM = 8.0 * t - 4.0, bR = 1.0 - 4.0 * t;
-    Kx = 0.0; Ky = 0.0; Kz = 0.0;
-    constexpr int NT = METHOD == 0 ? 2 : 3;
-    int ix, iy; double wx[NT], wy[NT];
-    if (METHOD == 0) { cic_weights(u, nx, ix, wx); cic_weights(v, ny, iy, wy); }
-    else { tsc_weights(u, nx, ix, wx); tsc_weights(v, ny, iy, wy); }
-#pragma unroll
-    for (int m = 0; m < NT; ++m)
-#pragma unroll
-        for (int k = 0; k < NT; ++k) {
-            long long c = (long long)(iy + k - 1) * nx + (ix + m - 1);
-            double w = wx[m] * wy[k];
-            Kx += w * (aL * L[pc + c] + aM * M[pc + c] + aR * R[pc + c]);
-            Ky += w * (aL * L[2 * pc + c] + aM * M[2 * pc + c] + aR * R[2 * pc + c]);
-            Kz += w * (bL * L[c] + bM * M[c] + bR * R[c]);
-        }
+__device__ __forceinline__ void load_cell(const double2 *F, long long c, double &phi, double &ex, double &ey) {
+    const double2 a = F[2 * c], b = F[2 * c + 1];
+    phi = a.x; ex = a.y; ey = b.x;
 }
 
 // Synchro-beam kick of every field particle of the front's tasks: drift in, interpolated kick,
 // drift out (pic_cpu.jl:1005-1017, 1218-1243, 1248-1273; :node form 1448-1538).
-// Blocks map to (task, particle chunk) through `blockmap` (task index, first particle).
+// Blocks map to (task, chunk of kKickChunk particles) through `blockmap`; the block reads its task
+// and meshes once into shared memory, then each thread kicks kKickChunk / blockDim particles.
+constexpr int kKickThreads = 256;
+constexpr int kKickChunk = 2048;
+struct KickJob {
+    Grid gL, gR;
+    double hxL, hyL, hxR, hyR;  // reciprocal spacings
+    double c_src, hzi, zbias, ks;
+    long long fld_start, fld_n, plane_off;
+    int fld_beam, ok;
+};
+
+struct Coord6 {
+    double x, px, y, py, z, pz;
+};
+__device__ __forceinline__ Coord6 load_coord(const SoA &S, long long p) {
+    return Coord6{S.c[0][p], S.c[1][p], S.c[2][p], S.c[3][p], S.c[4][p], S.c[5][p]};
+}
+
 template <int METHOD>
-__global__ void __launch_bounds__(256) k_kick(Collide C, int plane0_front, const int2 *blockmap) {
-    const int2 bm = blockmap[blockIdx.x];
-    const Task &T = C.tasks[bm.x];
-    const long long k = (long long)bm.y + threadIdx.x;
-    if (k >= T.fld_n) return;
+__device__ __forceinline__ void kick_particle(const Collide &C, const KickJob &J, long long p, const Coord6 &q) {
+    constexpr int NT2 = Taps<METHOD>::NT * Taps<METHOD>::NT;
     const DevOptions &o = C.o;
     const long long pc = (long long)o.nx * o.ny;
-    const double *base = C.fields + (long long)(T.plane0 - plane0_front) * 3 * pc;
-    Grid gL, gR;
-    if (o.node) {
-        gL = C.nodes[T.nodeL].fg;
-        gR = C.nodes[T.nodeR].fg;
-    } else {
-        const TaskGeom &G = C.geom[bm.x];
-        if (G.green < 0) return;
-        gL = G.fg;
-        gR = G.fg;
-    }
-    const SoA S = C.beam[T.fld_beam];
-    const long long p = T.fld_start + k;
-    double x = S.c[0][p], px = S.c[1][p], y = S.c[2][p], py = S.c[3][p], z = S.c[4][p], pz = S.c[5][p];
+    const double2 *base = C.fields + J.plane_off * 2 * pc;
+    const SoA S = C.beam[J.fld_beam];
+    double x = q.x, px = q.px, y = q.y, py = q.py;
+    const double z = q.z;
+    double pz = q.pz;
     const bool lk = o.longitudinal_kick != 0;
-    double s = 0.5 * (z - T.c_src);
+    const double s = 0.5 * (z - J.c_src);
     x += s * px;
     y += s * py;
     if (lk) pz -= 0.25 * (px * px + py * py);
-    const double zL = jclamp(-z * T.hzi + T.zbias, 0.0, 1.0);
+    const double zL = jclamp(-z * J.hzi + J.zbias, 0.0, 1.0);
     const double zR = 1.0 - zL;
-    const double ks = T.ks;
+    const double ks = J.ks;
     if (o.node) {
-        const double *L = base, *R = base + 3 * pc, *Z = base + 6 * pc;
+        // L on gL, R on gR, Z (the R drift deposited on gL) on gL; with zL = 1, zR = 0 the reference's
+        // single-plane interpolations reduce exactly to w * E (pic_cpu.jl:1517-1528).
+        const Grid &gL = J.gL, &gR = J.gR;
+        const double2 *FL = base, *FR = base + 2 * pc, *FZ = base + 4 * pc;
         if (!(isfinite(x) && gL.x0 <= x && x <= gL.x0 + gL.w && isfinite(y) && gL.y0 <= y && y <= gL.y0 + gL.h))
             atomicAdd((unsigned long long *)&C.status->dropped, 1ull);
-        double KxL, KyL, KzL, KxR, KyR, KzR;
-        gather_lr<METHOD>(o, gL, x, y, L, L, 1.0, 0.0, true, KxL, KyL, KzL);
-        gather_lr<METHOD>(o, gR, x, y, R, R, 1.0, 0.0, true, KxR, KyR, KzR);
+        double KxL = 0, KyL = 0, Kz = 0, KxR = 0, KyR = 0;
+        {
+            const Taps<METHOD> tp(o, gL, J.hxL, J.hyL, x, y);
+#pragma unroll
+            for (int t = 0; t < NT2; ++t) {
+                double phl, exl, eyl;
+                load_cell(FL, tp.cell(t, o.nx), phl, exl, eyl);
+                const double phz = FZ[2 * tp.cell(t, o.nx)].x;
+                KxL += tp.w[t] * exl;
+                KyL += tp.w[t] * eyl;
+                Kz += tp.w[t] * (phl - phz);
+            }
+        }
+        {
+            const Taps<METHOD> tp(o, gR, J.hxR, J.hyR, x, y);
+#pragma unroll
+            for (int t = 0; t < NT2; ++t) {
+                double ph, ex, ey;
+                load_cell(FR, tp.cell(t, o.nx), ph, ex, ey);
+                KxR += tp.w[t] * ex;
+                KyR += tp.w[t] * ey;
+            }
+        }
         px += ks * (zL * KxL + zR * KxR);
         py += ks * (zL * KyL + zR * KyR);
-        if (lk) {
-            double a, b, Kz;
-            gather_lr<METHOD>(o, gL, x, y, L, Z, 1.0, 0.0, true, a, b, Kz);
-            pz += ks * Kz * T.hzi;
-        }
+        if (lk) pz += ks * Kz * J.hzi;
     } else if (o.quadratic) {
-        const double *L = base, *R = base + 3 * pc, *M = base + 6 * pc;
-        double Kx, Ky, Kz;
-        gather_lmr<METHOD>(o, gL, x, y, L, M, R, 1.0 - zL, Kx, Ky, Kz);
+        // three nodes L, R, M (pic_cpu.jl:2648-2680) at t = 1 - zL
+        const double2 *FL = base, *FR = base + 2 * pc, *FM = base + 4 * pc;
+        const double t = 1.0 - zL;
+        const double t2 = t * t;
+        const double aL = 2.0 * t2 - 3.0 * t + 1.0, aM = 4.0 * t - 4.0 * t2, aR = 2.0 * t2 - t;
+        const double bL = 3.0 - 4.0 * t, bM = 8.0 * t - 4.0, bR = 1.0 - 4.0 * t;
+        const Taps<METHOD> tp(o, J.gL, J.hxL, J.hyL, x, y);
+        double Kx = 0, Ky = 0, Kz = 0;
+#pragma unroll
+        for (int q = 0; q < NT2; ++q) {
+            double pl, el, fl, pm, em, fm, pr, er, fr;
+            load_cell(FL, tp.cell(q, o.nx), pl, el, fl);
+            load_cell(FM, tp.cell(q, o.nx), pm, em, fm);
+            load_cell(FR, tp.cell(q, o.nx), pr, er, fr);
+            Kx += tp.w[q] * (aL * el + aM * em + aR * er);
+            Ky += tp.w[q] * (aL * fl + aM * fm + aR * fr);
+            Kz += tp.w[q] * (bL * pl + bM * pm + bR * pr);
+        }
         px += ks * Kx;
         py += ks * Ky;
-        if (lk) pz += ks * Kz * T.hzi;
+        if (lk) pz += ks * Kz * J.hzi;
     } else {
-        const double *L = base, *R = base + 3 * pc;
-        double Kx, Ky, Kz;
-        gather_lr<METHOD>(o, gL, x, y, L, R, zL, zR, false, Kx, Ky, Kz);
+        const double2 *FL = base, *FR = base + 2 * pc;
+        const Taps<METHOD> tp(o, J.gL, J.hxL, J.hyL, x, y);
+        double Kx = 0, Ky = 0, Kz = 0;
+#pragma unroll
+        for (int q = 0; q < NT2; ++q) {
+            double pl, el, fl, pr, er, fr;
+            load_cell(FL, tp.cell(q, o.nx), pl, el, fl);
+            load_cell(FR, tp.cell(q, o.nx), pr, er, fr);
+            Kx += tp.w[q] * (zL * el + zR * er);
+            Ky += tp.w[q] * (zL * fl + zR * fr);
+            Kz += tp.w[q] * (pl - pr);
+        }
         px += ks * Kx;
         py += ks * Ky;
-        if (lk) pz += ks * Kz * T.hzi;
+        if (lk) pz += ks * Kz * J.hzi;
     }
-    double s2 = 0.5 * (T.c_src - z);
+    const double s2 = 0.5 * (J.c_src - z);
     x += s2 * px;
     y += s2 * py;
     if (lk) pz += 0.25 * (px * px + py * py);
     S.c[0][p] = x; S.c[1][p] = px; S.c[2][p] = y; S.c[3][p] = py; S.c[5][p] = pz;
+}
+
+template <int METHOD>
+__global__ void __launch_bounds__(kKickThreads) k_kick(Collide C, int plane0_front, const int2 *blockmap) {
+    __shared__ KickJob J;
+    if (threadIdx.x == 0) {
+        const int2 bm = blockmap[blockIdx.x];
+        const Task &T = C.tasks[bm.x];
+        J.ok = 1;
+        if (C.o.node) {
+            J.gL = C.nodes[T.nodeL].fg;
+            J.gR = C.nodes[T.nodeR].fg;
+        } else {
+            const TaskGeom &G = C.geom[bm.x];
+            J.ok = G.green >= 0;
+            J.gL = G.fg;
+            J.gR = G.fg;
+        }
+        J.hxL = 1.0 / (J.gL.w / (double)(C.o.nx - 1)); J.hyL = 1.0 / (J.gL.h / (double)(C.o.ny - 1));
+        J.hxR = 1.0 / (J.gR.w / (double)(C.o.nx - 1)); J.hyR = 1.0 / (J.gR.h / (double)(C.o.ny - 1));
+        J.c_src = T.c_src; J.hzi = T.hzi; J.zbias = T.zbias; J.ks = T.ks;
+        J.fld_start = T.fld_start + bm.y;
+        const long long rest = T.fld_n - (long long)bm.y;
+        J.fld_n = rest < (long long)kKickChunk ? rest : (long long)kKickChunk;
+        J.plane_off = T.plane0 - plane0_front;
+        J.fld_beam = T.fld_beam;
+    }
+    __syncthreads();
+    if (!J.ok) return;
+    // The next particle's coordinates are loaded before the current one is kicked, so two
+    // particles' HBM loads are in flight per thread.
+    const SoA S = C.beam[J.fld_beam];
+    int k = threadIdx.x;
+    if (k >= J.fld_n) return;
+    Coord6 cur = load_coord(S, J.fld_start + k);
+    for (;;) {
+        const int kn = k + kKickThreads;
+        Coord6 nxt;
+        if (kn < J.fld_n) nxt = load_coord(S, J.fld_start + kn);
+        kick_particle<METHOD>(C, J, J.fld_start + k, cur);
+        if (kn >= J.fld_n) break;
+        cur = nxt;
+        k = kn;
+    }
 }
 
 // ------------------------------------------------------------------ node meshes

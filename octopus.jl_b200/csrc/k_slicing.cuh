@@ -25,37 +25,74 @@ struct SliceInfo {          // device-resident, read back once per collide
 };
 
 // Lane partial sums / extrema over all particles.  square != 0 folds (z - mu)^2.
-__global__ void k_lane_fold(const double *__restrict__ z, long long n, const SliceInfo *info, int square,
-                            double *lane_sum, double *lane_min, double *lane_max) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= kFoldLanes) return;
-    double mu = square ? info->mu : 0.0;
+// Lane t must add elements t, t+4096, ... strictly in order, so the parallelism is across lanes; to
+// keep enough loads in flight each block stages a tile of kTileIters iterations x 32 lanes in shared
+// memory with all its threads, then one thread per lane adds its column in order.
+constexpr int kTileIters = 64;
+__global__ void __launch_bounds__(256) k_lane_fold(const double *__restrict__ z, long long n, const SliceInfo *info,
+                                                   int square, double *lane_sum, double *lane_min, double *lane_max) {
+    __shared__ double tile[kTileIters][33];
+    const int lane0 = blockIdx.x * 32;
+    const double mu = square ? info->mu : 0.0;
+    const long long iters = (n + kFoldLanes - 1) / kFoldLanes;
     double s = 0.0, lo = INFINITY, hi = -INFINITY;
-    for (long long i = t; i < n; i += kFoldLanes) {
-        double v = z[i];
-        if (square) {
-            double d = v - mu;
-            s += d * d;
-        } else {
-            s += v;
-            lo = jmin(lo, v);
-            hi = jmax(hi, v);
+    const int t = threadIdx.x;
+    for (long long k0 = 0; k0 < iters; k0 += kTileIters) {
+        for (int e = t; e < kTileIters * 32; e += blockDim.x) {
+            const int kk = e >> 5, l = e & 31;
+            const long long i = (k0 + kk) * kFoldLanes + lane0 + l;
+            tile[kk][l] = i < n ? z[i] : 0.0;
         }
+        __syncthreads();
+        if (t < 32) {
+            const long long kmax = min((long long)kTileIters, iters - k0);
+            for (int kk = 0; kk < kmax; ++kk) {
+                const long long i = (k0 + kk) * kFoldLanes + lane0 + t;
+                if (i >= n) break;
+                const double v = tile[kk][t];
+                if (square) {
+                    const double d = v - mu;
+                    s += d * d;
+                } else {
+                    s += v;
+                    lo = jmin(lo, v);
+                    hi = jmax(hi, v);
+                }
+            }
+        }
+        __syncthreads();
     }
-    lane_sum[t] = s;
-    if (!square) { lane_min[t] = lo; lane_max[t] = hi; }
+    if (t < 32) {
+        lane_sum[lane0 + t] = s;
+        if (!square) { lane_min[lane0 + t] = lo; lane_max[lane0 + t] = hi; }
+    }
 }
 
-// Serial fold of the lanes (one thread).  stage 0: mean and extrema; stage 1: sigma and boundaries.
+// Serial fold of the lanes (slicing.jl:254-257), staged through shared memory so the single adding
+// thread reads at shared-memory latency.  stage 0: mean and extrema; stage 1: sigma and boundaries.
 // q[s] for s = 1..ns-1 holds sqrt(2)*erfinv(2s/ns - 1) (:normal_quantile) or the :specified positions.
-__global__ void k_fold_stats(const double *lane_sum, const double *lane_min, const double *lane_max, long long n,
-                             int stage, int method, int ns, const double *q, SliceInfo *info) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__global__ void __launch_bounds__(1024) k_fold_stats(const double *lane_sum, const double *lane_min,
+                                                     const double *lane_max, long long n, int stage, int method,
+                                                     int ns, const double *q, SliceInfo *info) {
+    __shared__ double sl[kFoldLanes];
+    __shared__ double rlo[32], rhi[32];
+    for (int t = threadIdx.x; t < kFoldLanes; t += blockDim.x) sl[t] = lane_sum[t];
+    if (stage == 0) {  // extrema are order independent: parallel reduce
+        double lo = INFINITY, hi = -INFINITY;
+        for (int t = threadIdx.x; t < kFoldLanes; t += blockDim.x) { lo = jmin(lo, lane_min[t]); hi = jmax(hi, lane_max[t]); }
+        for (int o = 16; o; o >>= 1) {
+            lo = jmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = jmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if ((threadIdx.x & 31) == 0) { rlo[threadIdx.x >> 5] = lo; rhi[threadIdx.x >> 5] = hi; }
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
     double s = 0.0;
-    for (int t = 0; t < kFoldLanes; ++t) s += lane_sum[t];
+    for (int t = 0; t < kFoldLanes; ++t) s += sl[t];
     if (stage == 0) {
         double lo = INFINITY, hi = -INFINITY;
-        for (int t = 0; t < kFoldLanes; ++t) { lo = jmin(lo, lane_min[t]); hi = jmax(hi, lane_max[t]); }
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { lo = jmin(lo, rlo[w]); hi = jmax(hi, rhi[w]); }
         info->mu = s / (double)n;
         info->zmin = lo;
         info->zmax = hi;
@@ -65,7 +102,6 @@ __global__ void k_fold_stats(const double *lane_sum, const double *lane_min, con
     double sigma = sqrt(jmax(s / (double)n, 0.0));
     info->sigma = sigma;
     double *b = info->boundary;
-    int nb = ns;
     if (method == 0) {  // :normal_quantile (slicing.jl:405-429)
         if (sigma == 0.0) {
             for (int k = 0; k <= ns; ++k) b[k] = mu;
@@ -89,7 +125,7 @@ __global__ void k_fold_stats(const double *lane_sum, const double *lane_min, con
         for (int k = 0; k < m; ++k) b[k + 1] = jclamp(internal[k], b[0], b[ns]);
     }
     int bad = 0;
-    for (int k = 0; k <= nb; ++k)
+    for (int k = 0; k <= ns; ++k)
         if (!isfinite(b[k])) bad = 1;
     info->nonfinite = bad;
     info->zero_width = (b[0] == b[ns]) ? 1 : 0;
@@ -204,21 +240,25 @@ __global__ void k_slice_lanes(const double *__restrict__ sz, const SliceInfo *in
     lanes[(long long)s * kFoldLanes + t] = acc;
 }
 
-// Serial lane fold per slice; centers and weights (slicing.jl:523-559).
-__global__ void k_slice_finish(const double *lanes, long long n, int center_position, SliceInfo *info) {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
+// Serial lane fold per slice (one block per slice, lanes staged in shared memory); centers and
+// weights (slicing.jl:523-559).
+__global__ void __launch_bounds__(1024) k_slice_finish(const double *lanes, long long n, int center_position,
+                                                       SliceInfo *info) {
+    __shared__ double sl[kFoldLanes];
+    const int s = blockIdx.x;
     if (s >= info->ns) return;
-    long long cnt = info->count[s];
+    const long long cnt = info->count[s];
+    const bool fold = center_position == 0 && cnt > 0;
+    if (fold)
+        for (int t = threadIdx.x; t < kFoldLanes; t += blockDim.x) sl[t] = lanes[(long long)s * kFoldLanes + t];
+    __syncthreads();
+    if (threadIdx.x != 0) return;
     info->weight[s] = (double)cnt / (double)n;
     const double *b = info->boundary;
-    if (center_position == 0) {
-        if (cnt == 0) {
-            info->center[s] = (b[s] + b[s + 1]) / 2;
-        } else {
-            double acc = 0.0;
-            for (int t = 0; t < kFoldLanes; ++t) acc += lanes[(long long)s * kFoldLanes + t];
-            info->center[s] = acc / (double)cnt;
-        }
+    if (fold) {
+        double acc = 0.0;
+        for (int t = 0; t < kFoldLanes; ++t) acc += sl[t];
+        info->center[s] = acc / (double)cnt;
     } else {
         info->center[s] = (b[s] + b[s + 1]) / 2;
     }

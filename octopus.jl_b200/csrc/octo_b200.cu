@@ -150,7 +150,7 @@ constexpr int kAlign = 32;           // slice start alignment (elements)
 constexpr long long kChunk = 8192;   // particles per slicing block
 
 struct BeamWS {
-    DevBuf<double> s[6];
+    DevBuf<double> s[6];  // slice-sorted coordinates
     DevBuf<int> perm;
     DevBuf<SliceInfo> info;
     DevBuf<double> lane_sum, lane_min, lane_max, lanes, q;
@@ -190,7 +190,8 @@ struct octo_ctx {
     DevBuf<double2> ghat;
     DevBuf<long long> qgrid, lq;
     DevBuf<double2> spec;
-    DevBuf<double> fields, lum_parts, node_ref, stats, partial;
+    DevBuf<double2> fields;
+    DevBuf<double> lum_parts, lum_partial, node_ref, stats, partial;
     DevBuf<double *> soa_ptrs;
     PinBuf<char> stage;
     PinBuf<double> h_lum;
@@ -356,10 +357,10 @@ void slice_beam(octo_ctx *c, int b, const octo_beam &beam, cudaStream_t st, long
     const double *z = (const double *)beam.z;
     int method = b == 0 ? c->opt.slicing_method1 : c->opt.slicing_method2;
     int cpos = b == 0 ? c->opt.center_position1 : c->opt.center_position2;
-    k_lane_fold<<<kFoldLanes / 256, 256, 0, st>>>(z, n, W.info.p, 0, W.lane_sum.p, W.lane_min.p, W.lane_max.p);
-    k_fold_stats<<<1, 1, 0, st>>>(W.lane_sum.p, W.lane_min.p, W.lane_max.p, n, 0, method, ns, W.q.p, W.info.p);
-    k_lane_fold<<<kFoldLanes / 256, 256, 0, st>>>(z, n, W.info.p, 1, W.lane_sum.p, W.lane_min.p, W.lane_max.p);
-    k_fold_stats<<<1, 1, 0, st>>>(W.lane_sum.p, W.lane_min.p, W.lane_max.p, n, 1, method, ns, W.q.p, W.info.p);
+    k_lane_fold<<<kFoldLanes / 32, 256, 0, st>>>(z, n, W.info.p, 0, W.lane_sum.p, W.lane_min.p, W.lane_max.p);
+    k_fold_stats<<<1, 1024, 0, st>>>(W.lane_sum.p, W.lane_min.p, W.lane_max.p, n, 0, method, ns, W.q.p, W.info.p);
+    k_lane_fold<<<kFoldLanes / 32, 256, 0, st>>>(z, n, W.info.p, 1, W.lane_sum.p, W.lane_min.p, W.lane_max.p);
+    k_fold_stats<<<1, 1024, 0, st>>>(W.lane_sum.p, W.lane_min.p, W.lane_max.p, n, 1, method, ns, W.q.p, W.info.p);
     k_slice_count<<<(unsigned)nblocks, 256, 0, st>>>(z, n, kChunk, W.info.p, W.counts.p);
     k_slice_offsets<<<1, 64, 0, st>>>(W.counts.p, (int)nblocks, kAlign, W.info.p, W.blockoff.p);
     CK(cudaMemsetAsync(W.perm.p, 0xff, sizeof(int) * total, st));
@@ -368,7 +369,7 @@ void slice_beam(octo_ctx *c, int b, const octo_beam &beam, cudaStream_t st, long
         (const double *)beam.pz, n, kChunk, W.info.p, W.blockoff.p, W.s[0].p, W.s[1].p, W.s[2].p, W.s[3].p, W.s[4].p,
         W.s[5].p, W.perm.p);
     k_slice_lanes<<<dim3(kFoldLanes / 256, ns), 256, 0, st>>>(W.s[4].p, W.info.p, W.lanes.p);
-    k_slice_finish<<<1, 64, 0, st>>>(W.lanes.p, n, cpos, W.info.p);
+    k_slice_finish<<<ns, 1024, 0, st>>>(W.lanes.p, n, cpos, W.info.p);
     launches += 10;
     CK(cudaGetLastError());
 }
@@ -405,6 +406,8 @@ void launch_method(int method, F f) {
 
 // Dynamic shared memory of the FFT kernels for line lengths NX, NY (4 warps per block).
 size_t fft_smem(int L) { return sizeof(double2) * (size_t)(L / 2 + 4 * L); }
+// k_green_rows: twiddles + 4 lines + the (kGreenRows+1) x (NX+1) corner lattice of F.
+size_t green_smem(int NX) { return fft_smem(NX) + sizeof(double) * (size_t)(kGreenRows + 1) * (NX + 1); }
 // k_conv_field: twiddles (NX/2) + 4 lines (4*NX) complex, plus a (tile+4) x nx phi tile; NX = 2*nx.
 size_t field_smem(int NX) { return sizeof(double2) * (size_t)(NX / 2 + 4 * NX) + sizeof(double) * (size_t)(kFieldTile + 4) * (NX / 2); }
 constexpr size_t kSmemLimit = 227 * 1024;
@@ -475,7 +478,7 @@ void build_node_meshes(octo_ctx *c, Collide &C, const SliceInfo &S1, const Slice
     // Green spectra of every valid node mesh
     const int NX = 2 * c->opt.nx, NY = 2 * c->opt.ny;
     C.nodes = c->nodes.p;
-    k_green_rows<<<dim3((NY / 2 + 3) / 4, nnode), 128, fft_smem(NX), st>>>(C, 1, 0, 0);
+    k_green_rows<<<dim3(NY / kGreenRows, nnode), 128, green_smem(NX), st>>>(C, 1, 0, 0);
     k_green_cols<<<dim3((c->opt.nx + 1 + 3) / 4, nnode), 128, fft_smem(NY), st>>>(C, 1, 0, 0);
     launches += 2;
     c->h_nodes.ensure(nnode);
@@ -654,7 +657,7 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
                     }
                     planes.push_back(P);
                 }
-                for (long long off = 0; off < T.fld_n; off += 256) blockmap.push_back(make_int2(tid, (int)off));
+                for (long long off = 0; off < T.fld_n; off += kKickChunk) blockmap.push_back(make_int2(tid, (int)off));
                 F.maxsrc = std::max<long long>(F.maxsrc, T.src_n);
                 tasks.push_back(T);
             }
@@ -700,7 +703,8 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
         CK(cudaMemsetAsync(c->qgrid.p, 0, sizeof(long long) * c->qgrid.n, st));
     }
     c->spec.ensure((size_t)max_planes * (nx + 1) * ny);
-    c->fields.ensure((size_t)max_planes * 3 * cells);
+    c->fields.ensure((size_t)max_planes * 2 * cells);
+    c->lum_partial.ensure((size_t)max_lum * kLumSplit);
     if (c->lq.n < (size_t)2 * max_lum * lcells) {
         c->lq.ensure((size_t)2 * max_lum * lcells);
         CK(cudaMemsetAsync(c->lq.p, 0, sizeof(long long) * c->lq.n, st));
@@ -736,12 +740,11 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
     C.fields = c->fields.p;
     C.lq = c->lq.p;
     C.lum_parts = c->lum_parts.p;
+    C.lum_partial = c->lum_partial.p;
     C.nodes = c->nodes.p;
 
-    const bool dep_smem = cells * sizeof(long long) <= kSmemLimit;
-    const bool lum_smem = lcells * sizeof(long long) <= kSmemLimit;
-    const size_t dep_bytes = dep_smem ? cells * sizeof(long long) : 0;
-    const size_t lum_bytes = lum_smem ? lcells * sizeof(long long) : 0;
+    const size_t dep_bytes = cells * sizeof(long long);
+    const size_t lum_bytes = lcells * sizeof(long long);
 
     // ---- wavefronts
     for (const Front &F : fronts) {
@@ -751,8 +754,9 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
         for (int t = F.t0; t < F.t0 + F.nt; ++t) { src_bytes += (double)tasks[t].src_n; fld_bytes += (double)tasks[t].fld_n; }
         if (!node || compute_lum) {
             PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, 1, slice_bytes * 5 * sizeof(double));
-            unsigned bps = (unsigned)std::max<long long>(1, std::min<long long>(32, (F.maxsrc + 8191) / 8192));
-            k_pair_bounds<<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
+            unsigned bps = (unsigned)std::max<long long>(1, std::min<long long>(128, (F.maxsrc + 2047) / 2048));
+            if (node) k_pair_bounds<true><<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
+            else k_pair_bounds<false><<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
             launches++;
         }
         if (!node) {
@@ -761,25 +765,26 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
                 k_plan<<<(F.nt + 63) / 64, 64, 0, st>>>(C, F.t0, F.nt, 0);
             }
             PhaseScope ps(c, OCTO_PHASE_GREEN, st, 2);
-            k_green_rows<<<dim3((NY / 2 + 3) / 4, F.nt), 128, fft_smem(NX), st>>>(C, 0, F.t0, 0);
+            k_green_rows<<<dim3(NY / kGreenRows, F.nt), 128, green_smem(NX), st>>>(C, 0, F.t0, 0);
             k_green_cols<<<dim3((nx + 1 + 3) / 4, F.nt), 128, fft_smem(NY), st>>>(C, 0, F.t0, 0);
             launches += 3;
         }
         if (compute_lum && F.nl) {
-            PhaseScope ps(c, OCTO_PHASE_LUMINOSITY, st, 3, slice_bytes * 4 * sizeof(double));
+            PhaseScope ps(c, OCTO_PHASE_LUMINOSITY, st, 4, slice_bytes * 4 * sizeof(double));
             k_lum_plan<<<(F.nl + 63) / 64, 64, 0, st>>>(C, F.l0, F.nl, F.t0);
-            unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(16, (F.maxlum + 16383) / 16384));
+            unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(8, (F.maxlum + 32767) / 32768));
             launch_method(lmethod, [&](auto M) {
-                k_lum_deposit<decltype(M)::value><<<dim3(bpp, 2 * F.nl), 512, lum_bytes, st>>>(C, F.l0, lum_smem ? 1 : 0);
+                k_lum_deposit<decltype(M)::value><<<dim3(bpp, 2 * F.nl), 1024, lum_bytes, st>>>(C, F.l0);
             });
-            k_lum_overlap<<<F.nl, 256, 0, st>>>(C, F.l0);
-            launches += 3;
+            k_lum_overlap<<<dim3(kLumSplit, F.nl), 256, 0, st>>>(C, F.l0);
+            k_lum_fold<<<(F.nl + 63) / 64, 64, 0, st>>>(C, F.l0, F.nl);
+            launches += 4;
         }
         {
             PhaseScope ps(c, OCTO_PHASE_DEPOSIT, st, 1, src_bytes * 4 * sizeof(double));
-            unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(16, (F.maxsrc + 16383) / 16384));
+            unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(8, (F.maxsrc + 32767) / 32768));
             launch_method(method, [&](auto M) {
-                k_deposit<decltype(M)::value><<<dim3(bpp, F.np), 512, dep_bytes, st>>>(C, F.p0, dep_smem ? 1 : 0);
+                k_deposit<decltype(M)::value><<<dim3(bpp, F.np), 1024, dep_bytes, st>>>(C, F.p0);
             });
         }
         {
@@ -794,7 +799,7 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
         {
             PhaseScope ps(c, OCTO_PHASE_KICK, st, 1, fld_bytes * 11 * sizeof(double));
             launch_method(method, [&](auto M) {
-                k_kick<decltype(M)::value><<<F.nb, 256, 0, st>>>(C, F.p0, c->blockmap.p + F.b0);
+                k_kick<decltype(M)::value><<<F.nb, kKickThreads, 0, st>>>(C, F.p0, c->blockmap.p + F.b0);
             });
         }
         launches += 5;
@@ -934,13 +939,15 @@ octo_ctx *octo_create(int32_t device, const octo_pic_options *options) {
         }
         size_t dep = (size_t)options->nx * options->ny * sizeof(long long);
         size_t lum = (size_t)(d.lnx + 1) * (d.lny + 1) * sizeof(long long);
-        int dsm = (int)std::min(dep, kSmemLimit), lsm = (int)std::min(lum, kSmemLimit);
+        if (dep > kSmemLimit || lum > kSmemLimit)
+            throw CudaFail{"grid too large for the shared-memory deposit (at most 168 x 168 cells on this backend)"};
+        int dsm = (int)dep, lsm = (int)lum;
         CK(cudaFuncSetAttribute(k_deposit<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
         CK(cudaFuncSetAttribute(k_deposit<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
         CK(cudaFuncSetAttribute(k_lum_deposit<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
         CK(cudaFuncSetAttribute(k_lum_deposit<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
         int fx = (int)fft_smem(2 * options->nx), fy = (int)fft_smem(2 * options->ny), ff = (int)field_smem(2 * options->nx);
-        CK(cudaFuncSetAttribute(k_green_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, fx));
+        CK(cudaFuncSetAttribute(k_green_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)green_smem(2 * options->nx)));
         CK(cudaFuncSetAttribute(k_green_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, fy));
         CK(cudaFuncSetAttribute(k_conv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, fx));
         CK(cudaFuncSetAttribute(k_conv_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, fy));
@@ -961,7 +968,7 @@ void octo_destroy(octo_ctx *c) {
     c->geom.release(); c->blockmap.release(); c->cache.release(); c->nodes.release(); c->lumgeom.release();
     c->bnd.release(); c->lumb.release(); c->nodebox_s.release(); c->nodebox_f.release(); c->nanflag.release();
     c->nodenan.release(); c->status.release(); c->ghat.release(); c->qgrid.release(); c->lq.release();
-    c->spec.release(); c->fields.release(); c->lum_parts.release(); c->node_ref.release(); c->stats.release();
+    c->spec.release(); c->fields.release(); c->lum_parts.release(); c->lum_partial.release(); c->node_ref.release(); c->stats.release();
     c->partial.release(); c->soa_ptrs.release();
     c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_nodes.release();
     for (auto e : c->ev_pool) cudaEventDestroy(e);

@@ -136,9 +136,9 @@ __device__ __forceinline__ void cic_weights(double u, int n, int &base, double w
         base = 1; w[0] = 0.0; w[1] = 0.0;
         return;
     }
-    long b = (long)floor(u) + 1;
+    int b = __double2int_rd(u) + 1;  // floor(u) + 1; u is in [0, n-1] here
     b = b < 1 ? 1 : (b > n - 1 ? n - 1 : b);
-    base = (int)b;
+    base = b;
     double f = jclamp(u - (double)(base - 1), 0.0, 1.0);
     w[0] = 1.0 - f;
     w[1] = f;
@@ -150,10 +150,9 @@ __device__ __forceinline__ void tsc_weights(double u, int n, int &base, double w
         base = 1; w[0] = 0.0; w[1] = 0.0; w[2] = 0.0;
         return;
     }
-    double fl = floor(u);
-    long ix = (long)fl;
-    double f = u - fl;
-    long b;
+    const int ix = __double2int_rd(u);  // floor(u); u is in [0, n-1] here
+    double f = u - (double)ix;
+    int b;
     if (f < 0.5) {
         double t = f * f;
         w[0] = 0.125 + 0.5 * (t - f);
@@ -169,7 +168,7 @@ __device__ __forceinline__ void tsc_weights(double u, int n, int &base, double w
         b = ix + 1;
     }
     b = b < 1 ? 1 : (b > n - 2 ? n - 2 : b);
-    base = (int)b;
+    base = b;
 }
 
 // Fixed-point scale: taps are rounded to multiples of 2^-bits with
