@@ -42,9 +42,9 @@ CONFIG = {
     "luminosity": "every turn", "precision": "fp64 plain form (int64 fixed-point charge grids)",
     "l2": "inputs larger than L2 (172 MB of particle coordinates per turn)",
 }
-# DRAM bytes per kick-kernel launch per field particle, from `ncu` (see profiles/kick_node_c1.md);
-# None until measured.
-KICK_TRAFFIC_BYTES_PER_PARTICLE = None
+# DRAM bytes (read + write) per field particle of one kick launch, from one `ncu --set full` capture of
+# the 15-pair front of this workload (285.4 MB for 3.584M field particles; profiles/kick_node_production.md).
+KICK_TRAFFIC_BYTES_PER_PARTICLE = 79.6
 
 
 def _dist():
