@@ -425,6 +425,7 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
     const int nx = C.o.nx, ny = C.o.ny, cells = nx * ny;
     Grid sg;
     if (P.geom >= 0) {
+        if (!C.nodes[P.geom].valid) return;
         sg = C.nodes[P.geom].sg;
     } else {
         const TaskGeom &G = C.geom[P.task];
@@ -839,6 +840,7 @@ __global__ void __launch_bounds__(kKickThreads) k_kick(Collide C, int plane0_fro
         const Task &T = C.tasks[bm.x];
         J.ok = 1;
         if (C.o.node) {
+            J.ok = C.nodes[T.nodeL].valid && C.nodes[T.nodeR].valid;
             J.gL = C.nodes[T.nodeL].fg;
             J.gR = C.nodes[T.nodeR].fg;
         } else {
@@ -945,13 +947,20 @@ __global__ void __launch_bounds__(256) k_node_boxes(NodeBoxArgs A) {
 // Node meshes of one direction (pic_cpu.jl:1359-1381): mesh (i, b) from the source drift boxes
 // of nodes b and b+1 and the field boxes of the slices adjacent to node b.  sbox: [i][b][4],
 // fbox: [field slice][i][4].  Meshes are written at meshes[i*nb + b-1].
+// A non-finite coordinate seen by k_node_boxes (*nanf) invalidates every mesh, so no later kernel of the
+// collide touches the beams, and is reported through the status with the smallest key (task 0, code 0,
+// role 4 = node-mesh build): the reference fails at the turn-start mesh build, before any pair.
 __global__ void k_node_plan(DevOptions o, const unsigned long long *sbox, const unsigned long long *fbox, int ns_src,
-                            int nb, const long long *src_count, NodeMesh *meshes, DevStatus *st) {
+                            int nb, const long long *src_count, const int *nanf, NodeMesh *meshes, DevStatus *st) {
     int id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= ns_src * nb) return;
     const int i = id / nb, b = id % nb + 1;  // b is 1-based
     NodeMesh &M = meshes[id];
     M.valid = 0;
+    if (*nanf) {
+        if (id == 0) atomicMin(&st->first_bad, 4ull);
+        return;
+    }
     if (src_count[i] == 0) return;
     const int ns = nb - 1;
     const int bn = min(b + 1, nb);

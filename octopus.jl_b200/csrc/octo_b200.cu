@@ -196,7 +196,7 @@ struct octo_ctx {
     PinBuf<char> stage;
     PinBuf<double> h_lum;
     PinBuf<DevStatus> h_status;
-    PinBuf<NodeMesh> h_nodes;
+    PinBuf<double> h_noderef;
     long long gstride = 0;
     int nslots = 0;
     int cache_ready = 0;
@@ -412,7 +412,9 @@ size_t green_smem(int NX) { return fft_smem(NX) + sizeof(double) * (size_t)(kGre
 size_t field_smem(int NX) { return sizeof(double2) * (size_t)(NX / 2 + 4 * NX) + sizeof(double) * (size_t)(kFieldTile + 4) * (NX / 2); }
 constexpr size_t kSmemLimit = 227 * 1024;
 
-// Enqueue the node meshes of both directions (pic_cpu.jl:1404-1419), then read back validity.
+// Enqueue the node meshes of both directions (pic_cpu.jl:1404-1419) with no host synchronisation: the
+// per-direction drift tables and slice counts are staged in pinned memory owned by the context, and
+// mesh validity is known on the host from the slice counts (node_mesh_valid).
 void build_node_meshes(octo_ctx *c, Collide &C, const SliceInfo &S1, const SliceInfo &S2, cudaStream_t st,
                        long long &launches) {
     const int ns1 = c->ns[0], ns2 = c->ns[1];
@@ -420,33 +422,41 @@ void build_node_meshes(octo_ctx *c, Collide &C, const SliceInfo &S1, const Slice
     c->nodes.ensure(nnode);
     c->nodenan.ensure(1);
     CK(cudaMemsetAsync(c->nodenan.p, 0, sizeof(int), st));
+    // staging per direction: ref [nss*nb + nss] doubles, then nss counts
+    const size_t per_dir = (size_t)kMaxSlices * (kMaxSlices + 2) + kMaxSlices;
+    c->h_noderef.ensure(2 * per_dir);
+    c->node_ref.ensure(2 * per_dir);
+    const int nbox_s = std::max(ns1 * (ns2 + 1), ns2 * (ns1 + 1)), nbox_f = ns1 * ns2;
+    c->nodebox_s.ensure((size_t)2 * nbox_s * 4);
+    c->nodebox_f.ensure((size_t)2 * nbox_f * 4);
     for (int dir = 1; dir <= 2; ++dir) {
         const SliceInfo &SS = dir == 1 ? S1 : S2;
         const SliceInfo &SF = dir == 1 ? S2 : S1;
         const int nss = dir == 1 ? ns1 : ns2, nsf = dir == 1 ? ns2 : ns1, nb = nsf + 1;
         const int sbeam = dir - 1, fbeam = 2 - dir;
         const int mesh0 = dir == 1 ? 0 : ns1 * (ns2 + 1);
-        std::vector<double> ref((size_t)nss * nb + nss);
+        double *href = c->h_noderef.p + (dir - 1) * per_dir;
+        double *dref = c->node_ref.p + (dir - 1) * per_dir;
         for (int i = 0; i < nss; ++i) {
-            for (int b = 0; b < nb; ++b) ref[(size_t)i * nb + b] = 0.5 * (SS.center[i] - SF.boundary[b]);
-            ref[(size_t)nss * nb + i] = SS.center[i];
+            for (int b = 0; b < nb; ++b) href[(size_t)i * nb + b] = 0.5 * (SS.center[i] - SF.boundary[b]);
+            href[(size_t)nss * nb + i] = SS.center[i];
         }
-        c->node_ref.ensure(ref.size() * 2);
-        double *dref = c->node_ref.p + (dir - 1) * (size_t)(c->node_ref.n / 2);
-        CK(cudaMemcpyAsync(dref, ref.data(), sizeof(double) * ref.size(), cudaMemcpyHostToDevice, st));
-        CK(cudaStreamSynchronize(st));  // `ref` is a host temporary
-        c->nodebox_s.ensure((size_t)nss * nb * 4);
-        c->nodebox_f.ensure((size_t)nsf * nss * 4);
+        long long *hcnt = (long long *)(href + (size_t)nss * nb + nss);
+        long long *dcnt = (long long *)(dref + (size_t)nss * nb + nss);
+        for (int s = 0; s < nss; ++s) hcnt[s] = SS.count[s];
+        CK(cudaMemcpyAsync(dref, href, sizeof(double) * ((size_t)nss * nb + 2 * nss), cudaMemcpyHostToDevice, st));
+        unsigned long long *sbox = c->nodebox_s.p + (size_t)(dir - 1) * nbox_s * 4;
+        unsigned long long *fbox = c->nodebox_f.p + (size_t)(dir - 1) * nbox_f * 4;
         long long ns4 = (long long)nss * nb * 4, nf4 = (long long)nsf * nss * 4;
-        k_init_boxes<<<(unsigned)((ns4 + 255) / 256), 256, 0, st>>>(c->nodebox_s.p, ns4);
-        k_init_boxes<<<(unsigned)((nf4 + 255) / 256), 256, 0, st>>>(c->nodebox_f.p, nf4);
+        k_init_boxes<<<(unsigned)((ns4 + 255) / 256), 256, 0, st>>>(sbox, ns4);
+        k_init_boxes<<<(unsigned)((nf4 + 255) / 256), 256, 0, st>>>(fbox, nf4);
         NodeBoxArgs A{};
         const BeamWS &WS = c->bw[sbeam], &WF = c->bw[fbeam];
         A.x = WS.s[0].p; A.px = WS.s[1].p; A.y = WS.s[2].p; A.py = WS.s[3].p; A.z = WS.s[4].p;
         long long maxn = 1;
         for (int s = 0; s < nss; ++s) { A.start[s] = SS.start[s]; A.count[s] = SS.count[s]; maxn = std::max(maxn, SS.count[s]); }
         A.ref = dref;
-        A.boxes = c->nodebox_s.p;
+        A.boxes = sbox;
         A.nanf = c->nodenan.p;
         A.nsl = nss; A.nref = nb; A.field_mode = 0;
         unsigned bx = (unsigned)std::min<long long>(64, (maxn + 4095) / 4096);
@@ -456,34 +466,30 @@ void build_node_meshes(octo_ctx *c, Collide &C, const SliceInfo &S1, const Slice
         maxn = 1;
         for (int s = 0; s < nsf; ++s) { F.start[s] = SF.start[s]; F.count[s] = SF.count[s]; maxn = std::max(maxn, SF.count[s]); }
         F.ref = dref + (size_t)nss * nb;
-        F.boxes = c->nodebox_f.p;
+        F.boxes = fbox;
         F.nanf = c->nodenan.p;
         F.nsl = nsf; F.nref = nss; F.field_mode = 1;
         bx = (unsigned)std::min<long long>(64, (maxn + 4095) / 4096);
         k_node_boxes<<<dim3(bx, nsf), 256, 0, st>>>(F);
-        // counts of the source slices for the plan
-        c->stats.ensure(kMaxSlices * 2);
-        long long cnt[kMaxSlices];
-        for (int s = 0; s < nss; ++s) cnt[s] = SS.count[s];
-        long long *dcnt = (long long *)c->stats.p + (dir - 1) * kMaxSlices;
-        CK(cudaMemcpyAsync(dcnt, cnt, sizeof(long long) * nss, cudaMemcpyHostToDevice, st));
-        k_node_plan<<<(nss * nb + 63) / 64, 64, 0, st>>>(c->dopt, c->nodebox_s.p, c->nodebox_f.p, nss, nb, dcnt,
+        k_node_plan<<<(nss * nb + 63) / 64, 64, 0, st>>>(c->dopt, sbox, fbox, nss, nb, dcnt, c->nodenan.p,
                                                          c->nodes.p + mesh0, c->status.p);
-        CK(cudaStreamSynchronize(st));  // box buffers are reused by the next direction; cnt is a host temporary
         launches += 5;
     }
-    int nanf = 0;
-    CK(cudaMemcpy(&nanf, c->nodenan.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (nanf) throw OctoFail{OCTO_ERR_NONFINITE, "non-finite coordinate (node-mesh build)"};
     // Green spectra of every valid node mesh
     const int NX = 2 * c->opt.nx, NY = 2 * c->opt.ny;
     C.nodes = c->nodes.p;
     k_green_rows<<<dim3(NY / kGreenRows, nnode), 128, green_smem(NX), st>>>(C, 1, 0, 0);
     k_green_cols<<<dim3((c->opt.nx + 1 + 3) / 4, nnode), 128, fft_smem(NY), st>>>(C, 1, 0, 0);
     launches += 2;
-    c->h_nodes.ensure(nnode);
-    CK(cudaMemcpyAsync(c->h_nodes.p, c->nodes.p, sizeof(NodeMesh) * nnode, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+}
+
+// Validity of node mesh (source slice src0, node b1 in 1..nsf+1) as k_node_plan decides it for finite
+// inputs: the source slice is non-empty and one of the field slices adjacent to the node is non-empty.
+bool node_mesh_valid(const SliceInfo &SS, const SliceInfo &SF, int nsf, int src0, int b1) {
+    if (SS.count[src0] == 0) return false;
+    for (int adj = b1 - 1; adj <= b1; ++adj)
+        if (1 <= adj && adj <= nsf && SF.count[adj - 1] > 0) return true;
+    return false;
 }
 
 double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_params *p1, const octo_beam_params *p2,
@@ -599,8 +605,8 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
             const int i = pr.i, j = pr.j;
             if (S1.count[i - 1] == 0 || S2.count[j - 1] == 0) continue;
             if (node) {
-                bool ok = c->h_nodes.p[node_id(1, i - 1, j)].valid && c->h_nodes.p[node_id(1, i - 1, j + 1)].valid &&
-                          c->h_nodes.p[node_id(2, j - 1, i)].valid && c->h_nodes.p[node_id(2, j - 1, i + 1)].valid;
+                bool ok = node_mesh_valid(S1, S2, ns2, i - 1, j) && node_mesh_valid(S1, S2, ns2, i - 1, j + 1) &&
+                          node_mesh_valid(S2, S1, ns1, j - 1, i) && node_mesh_valid(S2, S1, ns1, j - 1, i + 1);
                 if (!ok) continue;
             }
             const int p = pos_of[(size_t)(i - 1) * ns2 + (j - 1)];
@@ -839,6 +845,15 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
     if (DS.first_bad != ~0ull) {
         const int t = (int)(DS.first_bad >> 16), code = (int)((DS.first_bad >> 8) & 0xff), role = (int)(DS.first_bad & 0xff);
         char m[256];
+        if (role == 4) {  // non-finite coordinate at the node-mesh build (turn start)
+            long long f1 = first_nonfinite_host(*b1, st, false), f2 = first_nonfinite_host(*b2, st, false);
+            const int bb = f1 >= 0 ? 1 : 2;
+            const long long first = f1 >= 0 ? f1 : f2;
+            if (rep) { rep->role = 4; rep->first_index = first + 1; }
+            snprintf(m, sizeof m, "non-finite coordinate at particle %lld of beam%d (node-mesh build, turn %lld)", first + 1,
+                     bb, (long long)turn);
+            throw OctoFail{OCTO_ERR_NONFINITE, m};
+        }
         if (code == OCTO_ERR_NONFINITE && t < ntasks) {
             const Task &T = tasks[t];
             if (rep) { rep->role = role; rep->pair_i = T.i; rep->pair_j = T.j; rep->direction = T.dir; }
@@ -970,7 +985,7 @@ void octo_destroy(octo_ctx *c) {
     c->nodenan.release(); c->status.release(); c->ghat.release(); c->qgrid.release(); c->lq.release();
     c->spec.release(); c->fields.release(); c->lum_parts.release(); c->lum_partial.release(); c->node_ref.release(); c->stats.release();
     c->partial.release(); c->soa_ptrs.release();
-    c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_nodes.release();
+    c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_noderef.release();
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     delete c;
 }

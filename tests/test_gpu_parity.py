@@ -109,3 +109,28 @@ def test_config0_round_beams():
     ob = _gpu()
     s = ob.PICPoissonSolver(grid=(64, 64), slicing=ob.LongitudinalSlicing(nslices=5, method="normal_quantile"))
     check(run_both(s, 100000, 100000, turns=1, e_sigma=(50e-6, 50e-6, 7e-3), p_sigma=(50e-6, 50e-6, 60e-3)))
+
+
+@pytest.mark.parametrize("grid_mode,row,role", [("slice_pair", 0, 1), ("node", 2, 4), ("slice_pair", 4, 3)])
+def test_nonfinite_input_reports_location(grid_mode, row, role):
+    """A NaN coordinate fails the collide with OCTO_ERR_NONFINITE naming the particle (interface.jl:541-599):
+    x in :slice_pair is caught as a source coordinate, y in :node at the turn-start mesh build, z by the
+    slicing.  The error is host-visible status, not a device fault."""
+    ob = _gpu()
+    e, p = beams(3000, 2000)
+    e[row, 1234] = np.nan
+    be, bp = _device_beams(ob, e, p)
+    s = ob.PICPoissonSolver(grid=(32, 32), interaction_grid=grid_mode,
+                            slicing=ob.LongitudinalSlicing(nslices=4, method="normal_quantile"))
+    rt = ob.StrongStrongRuntime()
+    ctx = rt.context("ip", s, 0)
+    with pytest.raises(ob.CollisionError) as err:
+        ctx.collide(be, bp, turn=7)
+    assert err.value.code == 1, err.value
+    assert "1235" in str(err.value) and "turn 7" in str(err.value), str(err.value)
+    assert err.value.report.role == role
+    # the context stays usable after the error
+    e2, p2 = beams(3000, 2000)
+    be2, bp2 = _device_beams(ob, e2, p2)
+    assert np.isfinite(ctx.collide(be2, bp2, turn=8))
+    rt.close()
