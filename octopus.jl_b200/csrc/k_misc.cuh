@@ -8,9 +8,9 @@ struct Mat6 {
     double m[36];
 };
 
-// Linear 6D map (linear6d.jl:110-121), applied `turns` times; 128-bit loads of a particle pair.
-__global__ void __launch_bounds__(256) k_linear6d(double *x, double *px, double *y, double *py, double *z, double *pz,
-                                                  long long n, Mat6 M, int turns) {
+// Linear 6D map (linear6d.jl:110-121), applied `turns` times in FP64 to coordinates of element type R.
+template <class R>
+__global__ void __launch_bounds__(256) k_linear6d(R *x, R *px, R *y, R *py, R *z, R *pz, long long n, Mat6 M, int turns) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double a = x[i], b = px[i], c = y[i], d = py[i], e = z[i], f = pz[i];
@@ -24,7 +24,7 @@ __global__ void __launch_bounds__(256) k_linear6d(double *x, double *px, double 
         double pz1 = m[30] * a + m[31] * b + m[32] * c + m[33] * d + m[34] * e + m[35] * f;
         a = x1; b = px1; c = y1; d = py1; e = z1; f = pz1;
     }
-    x[i] = a; px[i] = b; y[i] = c; py[i] = d; z[i] = e; pz[i] = f;
+    x[i] = (R)a; px[i] = (R)b; y[i] = (R)c; py[i] = (R)d; z[i] = (R)e; pz[i] = (R)f;
 }
 
 // ---------------------------------------------------------------- counter RNG (counter_rng.jl)

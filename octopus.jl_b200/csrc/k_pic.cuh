@@ -9,8 +9,13 @@
 namespace octo {
 
 struct SoA {
-    double *c[6];  // x, px, y, py, z, pz (slice-sorted)
+    void *c[6];  // x, px, y, py, z, pz (slice-sorted), element type R of the collide
 };
+template <class R>
+__device__ __forceinline__ R *col(const SoA &S, int k) { return static_cast<R *>(S.c[k]); }
+
+// Dynamic shared memory, typed per kernel (one declaration serves every template instantiation).
+extern __shared__ __align__(16) unsigned char g_smem[];
 
 struct Collide {           // device pointers for one collide (passed by value)
     DevOptions o;
@@ -29,12 +34,13 @@ struct Collide {           // device pointers for one collide (passed by value)
     long long gstride;         // (nx+1) * 2ny
     int scratch_green0;        // first scratch Green slot (green_cache = :none)
     long long *qgrid;          // int64 charge grids: plane-in-front * nx*ny
-    double2 *spec;             // spectral scratch: plane-in-front * (nx+1)*ny
-    double2 *fields;           // plane-in-front * 2 * nx*ny: per cell (phi, Ex), (Ey, 0)
+    void *spec;                // spectral scratch (RealT<R>::C2): plane-in-front * (nx+1)*ny
+    void *fields;              // field planes (RealT<R>::FC): plane-in-front * kCellVec * nx*ny
     long long *lq;             // luminosity grids: (pair-in-front*2 + side) * (lnx+1)*(lny+1)
     double *lum_parts;         // [pair position]
     double *lum_partial;       // [pair-in-front][kLumSplit] overlap partial sums
-    const double2 *tw_x, *tw_y;  // twiddles for 2nx and 2ny
+    const double2 *tw_x, *tw_y;  // FP64 twiddles for 2nx and 2ny (Green spectra)
+    const void *twr_x, *twr_y;   // the same in RealT<R>::C2 (charge convolution)
     SoA beam[2];
     double klum;
 };
@@ -62,7 +68,7 @@ __device__ __forceinline__ unsigned long long shfl_max_u64(unsigned long long v)
 // Per-thread extrema use the native min/max (NaN is flagged separately; a +-0 tie cannot change any
 // geometry built from them), encoded to ordered integers once per block for the atomics.
 // grid: (blocks per side, 2 * pairs in front).
-template <bool LUM_ONLY>
+template <class R, bool LUM_ONLY>
 __global__ void __launch_bounds__(256) k_pair_bounds(Collide C, int task0) {
     const int q = blockIdx.y >> 1, side = blockIdx.y & 1;
     const int t1 = task0 + 2 * q, t2 = t1 + 1;
@@ -72,24 +78,25 @@ __global__ void __launch_bounds__(256) k_pair_bounds(Collide C, int task0) {
     const Task &fld_task = side == 0 ? B : A;  // ... and the field of fld_task
     const SoA S = C.beam[side];
     const long long st = src_task.src_start, n = src_task.src_n;
-    const double sL = src_task.sL, sR = src_task.sR, sM = src_task.sM, cf = fld_task.c_src;
-    double mn[6], mx[6];
+    const R sL = (R)src_task.sL, sR = (R)src_task.sR, sM = (R)src_task.sM, cf = (R)fld_task.c_src;
+    R mn[6], mx[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) { mn[k] = INFINITY; mx[k] = -INFINITY; }
+    for (int k = 0; k < 6; ++k) { mn[k] = R(INFINITY); mx[k] = R(-INFINITY); }
     bool nan_s = false, nan_f = false, nan_l = false;
-    const double *X = S.c[0] + st, *PX = S.c[1] + st, *Y = S.c[2] + st, *PY = S.c[3] + st, *Z = S.c[4] + st;
+    const R *X = col<R>(S, 0) + st, *PX = col<R>(S, 1) + st, *Y = col<R>(S, 2) + st, *PY = col<R>(S, 3) + st,
+            *Z = col<R>(S, 4) + st;
 #pragma unroll 4
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-        const double x = X[k], px = PX[k], y = Y[k], py = PY[k];
-        const double lx = x + px * sM, ly = y + py * sM;
+        const R x = X[k], px = PX[k], y = Y[k], py = PY[k];
+        const R lx = x + px * sM, ly = y + py * sM;
         nan_l |= (lx != lx) | (ly != ly);
         mn[4] = fmin(mn[4], lx); mx[4] = fmax(mx[4], lx);
         mn[5] = fmin(mn[5], ly); mx[5] = fmax(mx[5], ly);
         if (!LUM_ONLY) {
-            const double z = Z[k];
-            const double a = x + px * sL, b = x + px * sR, c = y + py * sL, d = y + py * sR;
-            const double s = 0.5 * (z - cf);
-            const double fx = x + s * px, fy = y + s * py;
+            const R z = Z[k];
+            const R a = x + px * sL, b = x + px * sR, c = y + py * sL, d = y + py * sR;
+            const R s = R(0.5) * (z - cf);
+            const R fx = x + s * px, fy = y + s * py;
             nan_s |= (a != a) | (b != b) | (c != c) | (d != d);
             nan_f |= (fx != fx) | (fy != fy);
             mn[0] = fmin(mn[0], fmin(a, b)); mx[0] = fmax(mx[0], fmax(a, b));
@@ -103,8 +110,8 @@ __global__ void __launch_bounds__(256) k_pair_bounds(Collide C, int task0) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
         if (LUM_ONLY && k < 4) continue;
-        unsigned long long a = shfl_min_u64(mn[k] == INFINITY ? kOrdMinInit : ord_encode(mn[k]));
-        unsigned long long b = shfl_max_u64(mx[k] == -INFINITY ? kOrdMaxInit : ord_encode(mx[k]));
+        unsigned long long a = shfl_min_u64(mn[k] == R(INFINITY) ? kOrdMinInit : ord_encode((double)mn[k]));
+        unsigned long long b = shfl_max_u64(mx[k] == R(-INFINITY) ? kOrdMaxInit : ord_encode((double)mx[k]));
         if (lane == 0) { red[warp][2 * k] = a; red[warp][2 * k + 1] = b; }
     }
     int any_s = __syncthreads_or(nan_s), any_f = __syncthreads_or(nan_f), any_l = __syncthreads_or(nan_l);
@@ -276,7 +283,7 @@ __device__ __forceinline__ double green_value(int green_type, int i, int j, int 
 // mode 0: blockIdx.y = task of the front (only tasks that rebuild); mode 1: blockIdx.y = node mesh.
 constexpr int kGreenRows = 8;
 __global__ void __launch_bounds__(128) k_green_rows(Collide C, int mode, int base, int node_slot0) {
-    extern __shared__ double2 sm[];
+    double2 *sm = (double2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx, NY = 2 * ny;
     const int lgx = 31 - __clz(NX);
     double2 *tw = sm;
@@ -351,7 +358,7 @@ __global__ void __launch_bounds__(128) k_green_rows(Collide C, int mode, int bas
 
 // Column transforms of the Green slots (length 2ny, in place, natural-order output).
 __global__ void __launch_bounds__(128) k_green_cols(Collide C, int mode, int base, int node_slot0) {
-    extern __shared__ double2 sm[];
+    double2 *sm = (double2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NY = 2 * ny;
     int lgy = 31 - __clz(NY);
     double2 *tw = sm;
@@ -389,11 +396,11 @@ __device__ __forceinline__ T *generic_ptr(T *p) {
     asm("" : "+l"(p));  // hide the address space from the compiler
     return p;
 }
-template <int METHOD>
-__device__ __forceinline__ void deposit_taps(double u, double v, int nw, int nh, double scale, long long *grid, int ld) {
+template <class R, int METHOD>
+__device__ __forceinline__ void deposit_taps(R u, R v, int nw, int nh, R scale, long long *grid, int ld) {
     constexpr int NT = METHOD == 0 ? 2 : 3;
     int ix, iy;
-    double wx[NT], wy[NT];
+    R wx[NT], wy[NT];
     if (METHOD == 0) { cic_weights(u, nw, ix, wx); cic_weights(v, nh, iy, wy); }
     else { tsc_weights(u, nw, ix, wx); tsc_weights(v, nh, iy, wy); }
     const int c0 = (iy - 1) * ld + (ix - 1);
@@ -401,7 +408,7 @@ __device__ __forceinline__ void deposit_taps(double u, double v, int nw, int nh,
     for (int m = 0; m < NT; ++m)
 #pragma unroll
         for (int k = 0; k < NT; ++k) {
-            const long long qv = __double2ll_rn(wx[m] * wy[k] * scale);
+            const long long qv = round_ll(wx[m] * wy[k] * scale);
             if (qv) atomicAdd((unsigned long long *)&grid[c0 + k * ld + m], (unsigned long long)qv);
         }
 }
@@ -417,9 +424,9 @@ __device__ __forceinline__ void merge_grid(const long long *sq, long long *g, in
 // Field-solve planes of a front.  grid: (blocks per plane, planes in front); each block deposits a
 // grid-stride share of its plane's source slice into a private int64 copy of the nx*ny grid in shared
 // memory, then merges it with global atomics (the consumer, k_conv_rows, clears the grid it reads).
-template <int METHOD>
+template <class R, int METHOD>
 __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
-    extern __shared__ long long sq[];
+    long long *sq = (long long *)g_smem;
     const int pl = blockIdx.y;
     const Plane &P = C.planes[plane0 + pl];
     const int nx = C.o.nx, ny = C.o.ny, cells = nx * ny;
@@ -436,19 +443,21 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
     __syncthreads();
     long long *acc = generic_ptr(sq);
     const double hx = sg.w / (double)(nx - 1), hy = sg.h / (double)(ny - 1);
-    const double hxi = 1.0 / hx, hyi = 1.0 / hy;
-    const double scale = ldexp(1.0, P.fixed_bits);
+    const R hxi = (R)(1.0 / hx), hyi = (R)(1.0 / hy);
+    const R scale = (R)ldexp(1.0, P.fixed_bits);
     const SoA S = C.beam[P.src_beam];
-    const double s = P.s;
-    const double xlo = sg.x0, xhi = sg.x0 + sg.w, ylo = sg.y0, yhi = sg.y0 + sg.h;
+    const R *X = col<R>(S, 0), *PX = col<R>(S, 1), *Y = col<R>(S, 2), *PY = col<R>(S, 3);
+    const R s = (R)P.s;
+    const R x0 = (R)sg.x0, y0 = (R)sg.y0;
+    const R xlo = x0, xhi = (R)(sg.x0 + sg.w), ylo = y0, yhi = (R)(sg.y0 + sg.h);
     int outside = 0;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < P.src_n; k += (long long)gridDim.x * blockDim.x) {
         const long long p = P.src_start + k;
-        const double xd = S.c[0][p] + S.c[1][p] * s;
-        const double yd = S.c[2][p] + S.c[3][p] * s;
+        const R xd = X[p] + PX[p] * s;
+        const R yd = Y[p] + PY[p] * s;
         if (P.count_dropped && !(isfinite(xd) && xlo <= xd && xd <= xhi && isfinite(yd) && ylo <= yd && yd <= yhi))
             ++outside;
-        deposit_taps<METHOD>((xd - sg.x0) * hxi, (yd - sg.y0) * hyi, nx, ny, scale, acc, nx);
+        deposit_taps<R, METHOD>((xd - x0) * hxi, (yd - y0) * hyi, nx, ny, scale, acc, nx);
     }
     if (P.count_dropped) {
         for (int o = 16; o; o >>= 1) outside += __shfl_xor_sync(0xffffffffu, outside, o);
@@ -460,9 +469,9 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
 
 // Luminosity planes: 2 per pair (side 0 = beam-1 slice i at sM1, side 1 = beam-2 slice j at sM2)
 // on the (lnx+1) x (lny+1) overlap mesh (pic_cpu.jl:2724-2735).
-template <int METHOD>
+template <class R, int METHOD>
 __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0) {
-    extern __shared__ long long sq[];
+    long long *sq = (long long *)g_smem;
     const int ql = blockIdx.y >> 1, side = blockIdx.y & 1;
     const LumJob &J = C.lumjobs[lj0 + ql];
     const LumGeom &L = C.lumgeom[J.pair];
@@ -472,15 +481,17 @@ __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0) {
     __syncthreads();
     long long *acc = generic_ptr(sq);
     const SoA S = C.beam[side];
+    const R *X = col<R>(S, 0), *PX = col<R>(S, 1), *Y = col<R>(S, 2), *PY = col<R>(S, 3);
     const long long st = side ? J.s2_start : J.s1_start, n = side ? J.s2_n : J.s1_n;
-    const double s = side ? J.sM2 : J.sM1;
-    const double scale = ldexp(1.0, side ? J.bits2 : J.bits1);
-    const double hxi = 1.0 / L.hx, hyi = 1.0 / L.hy;
+    const R s = (R)(side ? J.sM2 : J.sM1);
+    const R scale = (R)ldexp(1.0, side ? J.bits2 : J.bits1);
+    const R hxi = (R)(1.0 / L.hx), hyi = (R)(1.0 / L.hy);
+    const R x0 = (R)L.x0, y0 = (R)L.y0;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
         const long long p = st + k;
-        const double vx = S.c[0][p] + S.c[1][p] * s;
-        const double vy = S.c[2][p] + S.c[3][p] * s;
-        deposit_taps<METHOD>((vx - L.x0) * hxi, (vy - L.y0) * hyi, nw, nh, scale, acc, nw);
+        const R vx = X[p] + PX[p] * s;
+        const R vy = Y[p] + PY[p] * s;
+        deposit_taps<R, METHOD>((vx - x0) * hxi, (vy - y0) * hyi, nw, nh, scale, acc, nw);
     }
     __syncthreads();
     merge_grid(sq, C.lq + (long long)blockIdx.y * cells, cells);
@@ -535,17 +546,21 @@ __device__ __forceinline__ int plane_green(const Collide &C, const Plane &P) {
 }
 
 // Forward x-transform of the charge rows: two rows per warp packed as one complex line
-// (zero-padded to 2nx); the int64 grid is converted to FP64 and cleared as it is read.
+// (zero-padded to 2nx).  Plain form: the int64 grid is converted to FP64 and cleared as it is read.
+// Precision form: the plane's int64 value is the exact difference with its partner plane when it has
+// one (Plane::other_delta), and the host clears the front's grids after the launch.
+template <class R>
 __global__ void __launch_bounds__(128) k_conv_rows(Collide C, int plane0) {
-    extern __shared__ double2 sm[];
+    using C2 = typename RealT<R>::C2;
+    C2 *sm = (C2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx;
     const int lgx = 31 - __clz(NX);
     const int pl = blockIdx.y;
     const Plane &P = C.planes[plane0 + pl];
     if (plane_green(C, P) < 0) return;
-    double2 *tw = sm;
-    double2 *line = sm + NX / 2 + (threadIdx.x >> 5) * NX;
-    load_twiddles(tw, C.tw_x, NX);
+    C2 *tw = sm;
+    C2 *line = sm + NX / 2 + (threadIdx.x >> 5) * NX;
+    load_twiddles(tw, (const C2 *)C.twr_x, NX);
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -553,67 +568,113 @@ __global__ void __launch_bounds__(128) k_conv_rows(Collide C, int plane0) {
     if (j0 >= ny) return;
     const double inv = ldexp(1.0, -P.fixed_bits);
     long long *q = C.qgrid + (long long)pl * nx * ny;
+    constexpr bool kPrecision = sizeof(R) == 4;
+    const long long *qo = q + (long long)P.other_delta * nx * ny;
+    const bool diff = kPrecision && P.other_delta != 0;
+    const long long sgn = P.self_first ? 1 : -1;
     for (int i = lane; i < NX; i += 32) {
-        double a = 0.0, b = 0.0;
+        C2 v;
+        v.x = R(0);
+        v.y = R(0);
         if (i < nx) {
-            const long long qa = q[(long long)j0 * nx + i];
-            a = (double)qa * inv;
-            if (qa) q[(long long)j0 * nx + i] = 0;
+            long long qa = q[(long long)j0 * nx + i];
+            if (diff) qa = sgn * (qa - qo[(long long)j0 * nx + i]);
+            v.x = (R)((double)qa * inv);
+            if (!kPrecision && qa) q[(long long)j0 * nx + i] = 0;
             if (j1 < ny) {
-                const long long qb = q[(long long)j1 * nx + i];
-                b = (double)qb * inv;
-                if (qb) q[(long long)j1 * nx + i] = 0;
+                long long qb = q[(long long)j1 * nx + i];
+                if (diff) qb = sgn * (qb - qo[(long long)j1 * nx + i]);
+                v.y = (R)((double)qb * inv);
+                if (!kPrecision && qb) q[(long long)j1 * nx + i] = 0;
             }
         }
-        line[bitrev(i, lgx)] = make_double2(a, b);
+        line[bitrev(i, lgx)] = v;
     }
     warp_fft_passes(line, NX, tw, false);
-    double2 *H = C.spec + (long long)pl * (nx + 1) * ny;
+    C2 *H = (C2 *)C.spec + (long long)pl * (nx + 1) * ny;
     for (int k = lane; k <= nx; k += 32) {
-        double2 zk = line[k], zm = conjg(line[(NX - k) & (NX - 1)]);
-        double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y + zm.y));
-        double2 D = csub(zk, zm);
+        C2 zk = line[k], zm = conjg(line[(NX - k) & (NX - 1)]);
+        C2 A, B;
+        A.x = R(0.5) * (zk.x + zm.x);
+        A.y = R(0.5) * (zk.y + zm.y);
+        C2 D = csub(zk, zm);
+        B.x = R(0.5) * D.y;
+        B.y = R(-0.5) * D.x;
         H[(long long)k * ny + j0] = A;
-        if (j1 < ny) H[(long long)k * ny + j1] = make_double2(0.5 * D.y, -0.5 * D.x);
+        if (j1 < ny) H[(long long)k * ny + j1] = B;
     }
 }
 
-// y-transform, multiply by the Green spectrum, inverse y-transform; one frequency column per warp,
-// in place.  Only rows j < ny of the result are kept (the field quadrant).
+// y-transform, multiply by the (FP64) Green spectrum, inverse y-transform; one frequency column per
+// warp, in place.  Only rows j < ny of the result are kept (the field quadrant).
+template <class R>
 __global__ void __launch_bounds__(128) k_conv_cols(Collide C, int plane0) {
-    extern __shared__ double2 sm[];
+    using C2 = typename RealT<R>::C2;
+    C2 *sm = (C2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NY = 2 * ny;
     const int lgy = 31 - __clz(NY);
     const int pl = blockIdx.y;
     const Plane &P = C.planes[plane0 + pl];
     const int slot = plane_green(C, P);
     if (slot < 0) return;
-    double2 *tw = sm;
-    double2 *line = sm + NY / 2 + (threadIdx.x >> 5) * NY;
-    load_twiddles(tw, C.tw_y, NY);
+    C2 *tw = sm;
+    C2 *line = sm + NY / 2 + (threadIdx.x >> 5) * NY;
+    load_twiddles(tw, (const C2 *)C.twr_y, NY);
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (k > nx) return;
-    double2 *col = C.spec + ((long long)pl * (nx + 1) + k) * ny;
-    for (int j = lane; j < NY; j += 32) line[bitrev(j, lgy)] = j < ny ? col[j] : make_double2(0.0, 0.0);
+    C2 *col = (C2 *)C.spec + ((long long)pl * (nx + 1) + k) * ny;
+    C2 zero;
+    zero.x = R(0);
+    zero.y = R(0);
+    for (int j = lane; j < NY; j += 32) line[bitrev(j, lgy)] = j < ny ? col[j] : zero;
     warp_fft_passes(line, NY, tw, false);
     const double2 *g = C.ghat + (long long)slot * C.gstride + (long long)k * NY;
-    for (int j = lane; j < NY; j += 32) line[j] = cmul(line[j], g[j]);
+    for (int j = lane; j < NY; j += 32) {
+        const double2 gv = g[j];
+        C2 gg;
+        gg.x = (R)gv.x;
+        gg.y = (R)gv.y;
+        line[j] = cmul(line[j], gg);
+    }
     __syncwarp();
     for (int j = lane; j < NY; j += 32) {  // bit-reverse permutation in place
         int r = bitrev(j, lgy);
-        if (j < r) { double2 t = line[j]; line[j] = line[r]; line[r] = t; }
+        if (j < r) { C2 t = line[j]; line[j] = line[r]; line[r] = t; }
     }
     warp_fft_passes(line, NY, tw, true);
     for (int j = lane; j < ny; j += 32) col[j] = line[j];
 }
 
+// Field planes: a cell is (phi, Ex), (Ey, 0) as two double2 (plain form) or one float4 (precision
+// form), so one tap of one plane is one 32-byte or 16-byte access.
+__device__ __forceinline__ void store_cell(double2 *F, long long o, double phi, double ex, double ey) {
+    F[2 * o] = make_double2(phi, ex);
+    F[2 * o + 1] = make_double2(ey, 0.0);
+}
+__device__ __forceinline__ void store_cell(float4 *F, long long o, float phi, float ex, float ey) {
+    F[o] = make_float4(phi, ex, ey, 0.f);
+}
+__device__ __forceinline__ void load_cell(const double2 *F, long long c, double &phi, double &ex, double &ey) {
+    const double2 a = F[2 * c], b = F[2 * c + 1];
+    phi = a.x; ex = a.y; ey = b.x;
+}
+__device__ __forceinline__ void load_cell(const float4 *F, long long c, float &phi, float &ex, float &ey) {
+    const float4 v = F[c];
+    phi = v.x; ex = v.y; ey = v.z;
+}
+__device__ __forceinline__ double load_phi(const double2 *F, long long c) { return F[2 * c].x; }
+__device__ __forceinline__ float load_phi(const float4 *F, long long c) { return F[c].x; }
+
 // Inverse x-transform (two Hermitian rows per complex line) producing phi for a tile of rows plus a
 // two-row halo, then E = -grad(phi) on the tile (pic_cpu.jl:2531-2591).
 constexpr int kFieldTile = 8;
+template <class R>
 __global__ void __launch_bounds__(128) k_conv_field(Collide C, int plane0) {
-    extern __shared__ double2 sm[];
+    using C2 = typename RealT<R>::C2;
+    using FC = typename RealT<R>::FC;
+    C2 *sm = (C2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx, NY = 2 * ny;
     const int lgx = 31 - __clz(NX);
     const int pl = blockIdx.y;
@@ -622,32 +683,38 @@ __global__ void __launch_bounds__(128) k_conv_field(Collide C, int plane0) {
     Grid sg;
     if (P.geom >= 0) sg = C.nodes[P.geom].sg;
     else sg = C.geom[P.task].sg;
-    double2 *tw = sm;
-    double2 *lines = sm + NX / 2;
-    double *phi = (double *)(lines + 4 * NX);  // (kFieldTile + 4) rows x nx
-    load_twiddles(tw, C.tw_x, NX);
+    C2 *tw = sm;
+    C2 *lines = sm + NX / 2;
+    R *phi = (R *)(lines + 4 * NX);  // (kFieldTile + 4) rows x nx
+    load_twiddles(tw, (const C2 *)C.twr_x, NX);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int jt0 = blockIdx.x * kFieldTile;
     const int jt1 = min(jt0 + kFieldTile, ny);
     const int ja0 = max(jt0 - 2, 0), ja1 = min(jt1 + 2, ny);
     const int nrows = ja1 - ja0;
-    const double2 *H = C.spec + (long long)pl * (nx + 1) * ny;
-    const double scale = 1.0 / ((double)NX * (double)NY);
-    double2 *line = lines + warp * NX;
+    const C2 *H = (const C2 *)C.spec + (long long)pl * (nx + 1) * ny;
+    const R scale = (R)(1.0 / ((double)NX * (double)NY));
+    C2 *line = lines + warp * NX;
+    C2 zero;
+    zero.x = R(0);
+    zero.y = R(0);
     for (int rp = warp; 2 * rp < nrows; rp += 4) {
         const int ra = ja0 + 2 * rp, rb = ra + 1;
         const bool hb = rb < ja1;
         for (int k = lane; k < NX; k += 32) {
-            double2 ca, cb;
+            C2 ca, cb;
             if (k <= nx) {
                 ca = H[(long long)k * ny + ra];
-                cb = hb ? H[(long long)k * ny + rb] : make_double2(0.0, 0.0);
+                cb = hb ? H[(long long)k * ny + rb] : zero;
             } else {
                 ca = conjg(H[(long long)(NX - k) * ny + ra]);
-                cb = hb ? conjg(H[(long long)(NX - k) * ny + rb]) : make_double2(0.0, 0.0);
+                cb = hb ? conjg(H[(long long)(NX - k) * ny + rb]) : zero;
             }
-            line[bitrev(k, lgx)] = make_double2(ca.x - cb.y, ca.y + cb.x);
+            C2 v;
+            v.x = ca.x - cb.y;
+            v.y = ca.y + cb.x;
+            line[bitrev(k, lgx)] = v;
         }
         warp_fft_passes(line, NX, tw, true);
         for (int i = lane; i < nx; i += 32) {
@@ -658,46 +725,52 @@ __global__ void __launch_bounds__(128) k_conv_field(Collide C, int plane0) {
     }
     __syncthreads();
     const double hx = sg.w / (double)(nx - 1), hy = sg.h / (double)(ny - 1);
-    const double hxi = 1.0 / hx, hyi = 1.0 / hy;
-    const double c4 = 1.0 / 12.0;
+    const R hxi = (R)(1.0 / hx), hyi = (R)(1.0 / hy);
+    const R c4 = (R)(1.0 / 12.0);
     const bool fourth = C.o.fourth != 0;
-    double2 *F = C.fields + (long long)pl * 2 * nx * ny;
+    FC *F = (FC *)C.fields + (long long)pl * RealT<R>::kCellVec * nx * ny;
     auto Pv = [&](int i, int j) { return phi[(j - ja0) * nx + i]; };  // 0-based i, j
     for (int idx = threadIdx.x; idx < (jt1 - jt0) * nx; idx += blockDim.x) {
         const int j = jt0 + idx / nx, i = idx % nx;
-        double ey, ex;
+        R ey, ex;
         // Ey (pic_cpu.jl:2553-2572), 1-based j' = j+1
-        if (j == 0) ey = hyi * (1.5 * Pv(i, 0) - 2 * Pv(i, 1) + 0.5 * Pv(i, 2));
-        else if (j == ny - 1) ey = hyi * (-1.5 * Pv(i, ny - 1) + 2 * Pv(i, ny - 2) - 0.5 * Pv(i, ny - 3));
-        else if (fourth && (j == 1 || j == ny - 2)) ey = 0.5 * hyi * (Pv(i, j - 1) - Pv(i, j + 1));
-        else if (fourth) ey = c4 * hyi * ((Pv(i, j + 2) - Pv(i, j - 2)) + 8 * (Pv(i, j - 1) - Pv(i, j + 1)));
-        else ey = 0.5 * hyi * (Pv(i, j - 1) - Pv(i, j + 1));
+        if (j == 0) ey = hyi * (R(1.5) * Pv(i, 0) - R(2) * Pv(i, 1) + R(0.5) * Pv(i, 2));
+        else if (j == ny - 1) ey = hyi * (R(-1.5) * Pv(i, ny - 1) + R(2) * Pv(i, ny - 2) - R(0.5) * Pv(i, ny - 3));
+        else if (fourth && (j == 1 || j == ny - 2)) ey = R(0.5) * hyi * (Pv(i, j - 1) - Pv(i, j + 1));
+        else if (fourth) ey = c4 * hyi * ((Pv(i, j + 2) - Pv(i, j - 2)) + R(8) * (Pv(i, j - 1) - Pv(i, j + 1)));
+        else ey = R(0.5) * hyi * (Pv(i, j - 1) - Pv(i, j + 1));
         // Ex (pic_cpu.jl:2573-2590)
-        if (i == 0) ex = hxi * (1.5 * Pv(0, j) - 2 * Pv(1, j) + 0.5 * Pv(2, j));
-        else if (i == nx - 1) ex = hxi * (-1.5 * Pv(nx - 1, j) + 2 * Pv(nx - 2, j) - 0.5 * Pv(nx - 3, j));
-        else if (fourth && (i == 1 || i == nx - 2)) ex = 0.5 * hxi * (Pv(i - 1, j) - Pv(i + 1, j));
-        else if (fourth) ex = c4 * hxi * ((Pv(i + 2, j) - Pv(i - 2, j)) + 8 * (Pv(i - 1, j) - Pv(i + 1, j)));
-        else ex = 0.5 * hxi * (Pv(i - 1, j) - Pv(i + 1, j));
-        long long o = (long long)j * nx + i;
-        F[2 * o] = make_double2(Pv(i, j), ex);
-        F[2 * o + 1] = make_double2(ey, 0.0);
+        if (i == 0) ex = hxi * (R(1.5) * Pv(0, j) - R(2) * Pv(1, j) + R(0.5) * Pv(2, j));
+        else if (i == nx - 1) ex = hxi * (R(-1.5) * Pv(nx - 1, j) + R(2) * Pv(nx - 2, j) - R(0.5) * Pv(nx - 3, j));
+        else if (fourth && (i == 1 || i == nx - 2)) ex = R(0.5) * hxi * (Pv(i - 1, j) - Pv(i + 1, j));
+        else if (fourth) ex = c4 * hxi * ((Pv(i + 2, j) - Pv(i - 2, j)) + R(8) * (Pv(i - 1, j) - Pv(i + 1, j)));
+        else ex = R(0.5) * hxi * (Pv(i - 1, j) - Pv(i + 1, j));
+        store_cell(F, (long long)j * nx + i, Pv(i, j), ex, ey);
     }
 }
 
 // ------------------------------------------------------------------ kick
-// Field planes are interleaved per cell as (phi, Ex), (Ey, 0), so one tap of one plane is a single
-// 32-byte sector.  Weights and taps follow _pic_interpolate_kick (pic_cpu.jl:2596-2619), x-outer.
-template <int METHOD>
+// Weights and taps follow _pic_interpolate_kick (pic_cpu.jl:2596-2619), x-outer.
+template <class R>
+struct GridR {
+    R x0, y0, w, h;
+};
+template <class R>
+__device__ __forceinline__ GridR<R> grid_r(const Grid &g) {
+    return GridR<R>{(R)g.x0, (R)g.y0, (R)g.w, (R)g.h};
+}
+
+template <class R, int METHOD>
 struct Taps {
     static constexpr int NT = METHOD == 0 ? 2 : 3;
     int c0;          // first cell (x-outer, y-inner order follows from c0 + m + k*nx)
-    double w[NT * NT];
+    R w[NT * NT];
     // hxi, hyi: reciprocals of the mesh spacing g.w/(nx-1), g.h/(ny-1), computed once per block.  The
-    // reference divides by the spacing (pic_cpu.jl:2601-2602); the product differs from that quotient
-    // by at most 1.5 ulp of u, a ~1e-14 relative change of the interpolation weights.
-    __device__ __forceinline__ Taps(const DevOptions &o, const Grid &g, double hxi, double hyi, double x, double y) {
-        const double u = (x - g.x0) * hxi, v = (y - g.y0) * hyi;
-        int ix, iy; double wx[NT], wy[NT];
+    // reference divides by the spacing (pic_cpu.jl:2601-2602); in FP64 the product differs from that
+    // quotient by at most 1.5 ulp of u, a ~1e-14 relative change of the interpolation weights.
+    __device__ __forceinline__ Taps(const DevOptions &o, const GridR<R> &g, R hxi, R hyi, R x, R y) {
+        const R u = (x - g.x0) * hxi, v = (y - g.y0) * hyi;
+        int ix, iy; R wx[NT], wy[NT];
         if (METHOD == 0) { cic_weights(u, o.nx, ix, wx); cic_weights(v, o.ny, iy, wy); }
         else { tsc_weights(u, o.nx, ix, wx); tsc_weights(v, o.ny, iy, wy); }
         c0 = (iy - 1) * o.nx + (ix - 1);
@@ -709,75 +782,88 @@ struct Taps {
     __device__ __forceinline__ int cell(int t, int nx) const { return c0 + (t / NT) + (t % NT) * nx; }
 };
 
-__device__ __forceinline__ void load_cell(const double2 *F, long long c, double &phi, double &ex, double &ey) {
-    const double2 a = F[2 * c], b = F[2 * c + 1];
-    phi = a.x; ex = a.y; ey = b.x;
-}
-
 // Synchro-beam kick of every field particle of the front's tasks: drift in, interpolated kick,
 // drift out (pic_cpu.jl:1005-1017, 1218-1243, 1248-1273; :node form 1448-1538).
 // Blocks map to (task, chunk of kKickChunk particles) through `blockmap`; the block reads its task
 // and meshes once into shared memory, then each thread kicks kKickChunk / blockDim particles.
 constexpr int kKickThreads = 256;
 constexpr int kKickChunk = 2048;
+template <class R>
 struct KickJob {
-    Grid gL, gR;
-    double hxL, hyL, hxR, hyR;  // reciprocal spacings
-    double c_src, hzi, zbias, ks;
+    GridR<R> gL, gR;
+    R hxL, hyL, hxR, hyR;  // reciprocal spacings
+    R c_src, hzi, zbias, ks;
     long long fld_start, fld_n, plane_off;
     int fld_beam, ok;
 };
 
+template <class R>
 struct Coord6 {
-    double x, px, y, py, z, pz;
+    R x, px, y, py, z, pz;
 };
-__device__ __forceinline__ Coord6 load_coord(const SoA &S, long long p) {
-    return Coord6{S.c[0][p], S.c[1][p], S.c[2][p], S.c[3][p], S.c[4][p], S.c[5][p]};
+template <class R>
+__device__ __forceinline__ Coord6<R> load_coord(const SoA &S, long long p) {
+    return Coord6<R>{col<R>(S, 0)[p], col<R>(S, 1)[p], col<R>(S, 2)[p], col<R>(S, 3)[p], col<R>(S, 4)[p], col<R>(S, 5)[p]};
 }
 
-template <int METHOD>
-__device__ __forceinline__ void kick_particle(const Collide &C, const KickJob &J, long long p, const Coord6 &q) {
-    constexpr int NT2 = Taps<METHOD>::NT * Taps<METHOD>::NT;
+template <class R, int METHOD>
+__device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R> &J, long long p, const Coord6<R> &q) {
+    using FC = typename RealT<R>::FC;
+    constexpr int CV = RealT<R>::kCellVec;
+    constexpr int NT2 = Taps<R, METHOD>::NT * Taps<R, METHOD>::NT;
+    // Precision form: the planes hold exact charge differences (see k_conv_rows), so the kick uses the
+    // algebraically equal difference forms below; the plain form keeps the reference's expressions.
+    constexpr bool kPrecision = sizeof(R) == 4;
     const DevOptions &o = C.o;
     const long long pc = (long long)o.nx * o.ny;
-    const double2 *base = C.fields + J.plane_off * 2 * pc;
+    const FC *base = (const FC *)C.fields + J.plane_off * CV * pc;
     const SoA S = C.beam[J.fld_beam];
-    double x = q.x, px = q.px, y = q.y, py = q.py;
-    const double z = q.z;
-    double pz = q.pz;
+    R x = q.x, px = q.px, y = q.y, py = q.py;
+    const R z = q.z;
+    R pz = q.pz;
     const bool lk = o.longitudinal_kick != 0;
-    const double s = 0.5 * (z - J.c_src);
+    const R s = R(0.5) * (z - J.c_src);
+    // Precision form: the drift and kick increments of x, y and pz are summed in registers and added
+    // to the stored coordinate once, so each FP32 coordinate is rounded once per kick (the pz drift
+    // terms, ~1e-7, dwarf the pz kick, ~1e-9, and three roundings of pz would cost ~3 ulps of it).
+    const R px0 = px, py0 = py;
+    R dpz = R(0);
     x += s * px;
     y += s * py;
-    if (lk) pz -= 0.25 * (px * px + py * py);
-    const double zL = jclamp(-z * J.hzi + J.zbias, 0.0, 1.0);
-    const double zR = 1.0 - zL;
-    const double ks = J.ks;
+    if (kPrecision) {
+        if (lk) dpz = -(R(0.25) * (px * px + py * py));
+    } else if (lk) {
+        pz -= R(0.25) * (px * px + py * py);
+    }
+    const R zL = jclamp(-z * J.hzi + J.zbias, R(0), R(1));
+    const R zR = R(1) - zL;
+    const R ks = J.ks;
     if (o.node) {
         // L on gL, R on gR, Z (the R drift deposited on gL) on gL; with zL = 1, zR = 0 the reference's
         // single-plane interpolations reduce exactly to w * E (pic_cpu.jl:1517-1528).
-        const Grid &gL = J.gL, &gR = J.gR;
-        const double2 *FL = base, *FR = base + 2 * pc, *FZ = base + 4 * pc;
+        const GridR<R> &gL = J.gL, &gR = J.gR;
+        const FC *FL = base, *FR = base + CV * pc, *FZ = base + 2 * CV * pc;
         if (!(isfinite(x) && gL.x0 <= x && x <= gL.x0 + gL.w && isfinite(y) && gL.y0 <= y && y <= gL.y0 + gL.h))
             atomicAdd((unsigned long long *)&C.status->dropped, 1ull);
-        double KxL = 0, KyL = 0, Kz = 0, KxR = 0, KyR = 0;
+        R KxL = 0, KyL = 0, Kz = 0, KxR = 0, KyR = 0;
         {
-            const Taps<METHOD> tp(o, gL, J.hxL, J.hyL, x, y);
+            const Taps<R, METHOD> tp(o, gL, J.hxL, J.hyL, x, y);
 #pragma unroll
             for (int t = 0; t < NT2; ++t) {
-                double phl, exl, eyl;
+                R phl, exl, eyl;
                 load_cell(FL, tp.cell(t, o.nx), phl, exl, eyl);
-                const double phz = FZ[2 * tp.cell(t, o.nx)].x;
+                const R phz = load_phi(FZ, tp.cell(t, o.nx));
                 KxL += tp.w[t] * exl;
                 KyL += tp.w[t] * eyl;
-                Kz += tp.w[t] * (phl - phz);
+                if (kPrecision) Kz += tp.w[t] * phz;  // the Z plane holds phi_L - phi_Z
+                else Kz += tp.w[t] * (phl - phz);
             }
         }
         {
-            const Taps<METHOD> tp(o, gR, J.hxR, J.hyR, x, y);
+            const Taps<R, METHOD> tp(o, gR, J.hxR, J.hyR, x, y);
 #pragma unroll
             for (int t = 0; t < NT2; ++t) {
-                double ph, ex, ey;
+                R ph, ex, ey;
                 load_cell(FR, tp.cell(t, o.nx), ph, ex, ey);
                 KxR += tp.w[t] * ex;
                 KyR += tp.w[t] * ey;
@@ -785,73 +871,94 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob &J
         }
         px += ks * (zL * KxL + zR * KxR);
         py += ks * (zL * KyL + zR * KyR);
-        if (lk) pz += ks * Kz * J.hzi;
+        if (lk) { if (kPrecision) dpz += ks * Kz * J.hzi; else pz += ks * Kz * J.hzi; }
     } else if (o.quadratic) {
         // three nodes L, R, M (pic_cpu.jl:2648-2680) at t = 1 - zL
-        const double2 *FL = base, *FR = base + 2 * pc, *FM = base + 4 * pc;
-        const double t = 1.0 - zL;
-        const double t2 = t * t;
-        const double aL = 2.0 * t2 - 3.0 * t + 1.0, aM = 4.0 * t - 4.0 * t2, aR = 2.0 * t2 - t;
-        const double bL = 3.0 - 4.0 * t, bM = 8.0 * t - 4.0, bR = 1.0 - 4.0 * t;
-        const Taps<METHOD> tp(o, J.gL, J.hxL, J.hyL, x, y);
-        double Kx = 0, Ky = 0, Kz = 0;
+        const FC *FL = base, *FR = base + CV * pc, *FM = base + 2 * CV * pc;
+        const R t = R(1) - zL;
+        const R t2 = t * t;
+        const R aL = R(2) * t2 - R(3) * t + R(1), aM = R(4) * t - R(4) * t2, aR = R(2) * t2 - t;
+        const R bL = R(3) - R(4) * t, bM = R(8) * t - R(4), bR = R(1) - R(4) * t;
+        const Taps<R, METHOD> tp(o, J.gL, J.hxL, J.hyL, x, y);
+        R Kx = 0, Ky = 0, Kz = 0;
 #pragma unroll
         for (int q = 0; q < NT2; ++q) {
-            double pl, el, fl, pm, em, fm, pr, er, fr;
+            R pl, el, fl, pm, em, fm, pr, er, fr;
             load_cell(FL, tp.cell(q, o.nx), pl, el, fl);
             load_cell(FM, tp.cell(q, o.nx), pm, em, fm);
             load_cell(FR, tp.cell(q, o.nx), pr, er, fr);
-            Kx += tp.w[q] * (aL * el + aM * em + aR * er);
-            Ky += tp.w[q] * (aL * fl + aM * fm + aR * fr);
-            Kz += tp.w[q] * (bL * pl + bM * pm + bR * pr);
+            if (kPrecision) {  // L, R planes hold L - M, R - M; aL + aM + aR = 1, bL + bM + bR = 0
+                Kx += tp.w[q] * (em + aL * el + aR * er);
+                Ky += tp.w[q] * (fm + aL * fl + aR * fr);
+                Kz += tp.w[q] * (bL * pl + bR * pr);
+            } else {
+                Kx += tp.w[q] * (aL * el + aM * em + aR * er);
+                Ky += tp.w[q] * (aL * fl + aM * fm + aR * fr);
+                Kz += tp.w[q] * (bL * pl + bM * pm + bR * pr);
+            }
         }
         px += ks * Kx;
         py += ks * Ky;
-        if (lk) pz += ks * Kz * J.hzi;
+        if (lk) { if (kPrecision) dpz += ks * Kz * J.hzi; else pz += ks * Kz * J.hzi; }
     } else {
-        const double2 *FL = base, *FR = base + 2 * pc;
-        const Taps<METHOD> tp(o, J.gL, J.hxL, J.hyL, x, y);
-        double Kx = 0, Ky = 0, Kz = 0;
+        const FC *FL = base, *FR = base + CV * pc;
+        const Taps<R, METHOD> tp(o, J.gL, J.hxL, J.hyL, x, y);
+        R Kx = 0, Ky = 0, Kz = 0;
 #pragma unroll
         for (int q = 0; q < NT2; ++q) {
-            double pl, el, fl, pr, er, fr;
+            R pl, el, fl, pr, er, fr;
             load_cell(FL, tp.cell(q, o.nx), pl, el, fl);
             load_cell(FR, tp.cell(q, o.nx), pr, er, fr);
-            Kx += tp.w[q] * (zL * el + zR * er);
-            Ky += tp.w[q] * (zL * fl + zR * fr);
-            Kz += tp.w[q] * (pl - pr);
+            if (kPrecision) {  // the R plane holds L - R
+                Kx += tp.w[q] * (el - zR * er);
+                Ky += tp.w[q] * (fl - zR * fr);
+                Kz += tp.w[q] * pr;
+            } else {
+                Kx += tp.w[q] * (zL * el + zR * er);
+                Ky += tp.w[q] * (zL * fl + zR * fr);
+                Kz += tp.w[q] * (pl - pr);
+            }
         }
         px += ks * Kx;
         py += ks * Ky;
-        if (lk) pz += ks * Kz * J.hzi;
+        if (lk) { if (kPrecision) dpz += ks * Kz * J.hzi; else pz += ks * Kz * J.hzi; }
     }
-    const double s2 = 0.5 * (J.c_src - z);
-    x += s2 * px;
-    y += s2 * py;
-    if (lk) pz += 0.25 * (px * px + py * py);
-    S.c[0][p] = x; S.c[1][p] = px; S.c[2][p] = y; S.c[3][p] = py; S.c[5][p] = pz;
+    const R s2 = R(0.5) * (J.c_src - z);
+    if (kPrecision) {
+        x = q.x + (s * px0 + s2 * px);
+        y = q.y + (s * py0 + s2 * py);
+        if (lk) pz = q.pz + (dpz + R(0.25) * (px * px + py * py));
+    } else {
+        x += s2 * px;
+        y += s2 * py;
+        if (lk) pz += R(0.25) * (px * px + py * py);
+    }
+    col<R>(S, 0)[p] = x; col<R>(S, 1)[p] = px; col<R>(S, 2)[p] = y; col<R>(S, 3)[p] = py; col<R>(S, 5)[p] = pz;
 }
 
-template <int METHOD>
+template <class R, int METHOD>
 __global__ void __launch_bounds__(kKickThreads) k_kick(Collide C, int plane0_front, const int2 *blockmap) {
-    __shared__ KickJob J;
+    __shared__ KickJob<R> J;
     if (threadIdx.x == 0) {
         const int2 bm = blockmap[blockIdx.x];
         const Task &T = C.tasks[bm.x];
         J.ok = 1;
+        Grid gL, gR;
         if (C.o.node) {
             J.ok = C.nodes[T.nodeL].valid && C.nodes[T.nodeR].valid;
-            J.gL = C.nodes[T.nodeL].fg;
-            J.gR = C.nodes[T.nodeR].fg;
+            gL = C.nodes[T.nodeL].fg;
+            gR = C.nodes[T.nodeR].fg;
         } else {
             const TaskGeom &G = C.geom[bm.x];
             J.ok = G.green >= 0;
-            J.gL = G.fg;
-            J.gR = G.fg;
+            gL = G.fg;
+            gR = G.fg;
         }
-        J.hxL = 1.0 / (J.gL.w / (double)(C.o.nx - 1)); J.hyL = 1.0 / (J.gL.h / (double)(C.o.ny - 1));
-        J.hxR = 1.0 / (J.gR.w / (double)(C.o.nx - 1)); J.hyR = 1.0 / (J.gR.h / (double)(C.o.ny - 1));
-        J.c_src = T.c_src; J.hzi = T.hzi; J.zbias = T.zbias; J.ks = T.ks;
+        J.gL = grid_r<R>(gL);
+        J.gR = grid_r<R>(gR);
+        J.hxL = (R)(1.0 / (gL.w / (double)(C.o.nx - 1))); J.hyL = (R)(1.0 / (gL.h / (double)(C.o.ny - 1)));
+        J.hxR = (R)(1.0 / (gR.w / (double)(C.o.nx - 1))); J.hyR = (R)(1.0 / (gR.h / (double)(C.o.ny - 1)));
+        J.c_src = (R)T.c_src; J.hzi = (R)T.hzi; J.zbias = (R)T.zbias; J.ks = (R)T.ks;
         J.fld_start = T.fld_start + bm.y;
         const long long rest = T.fld_n - (long long)bm.y;
         J.fld_n = rest < (long long)kKickChunk ? rest : (long long)kKickChunk;
@@ -865,12 +972,12 @@ __global__ void __launch_bounds__(kKickThreads) k_kick(Collide C, int plane0_fro
     const SoA S = C.beam[J.fld_beam];
     int k = threadIdx.x;
     if (k >= J.fld_n) return;
-    Coord6 cur = load_coord(S, J.fld_start + k);
+    Coord6<R> cur = load_coord<R>(S, J.fld_start + k);
     for (;;) {
         const int kn = k + kKickThreads;
-        Coord6 nxt;
-        if (kn < J.fld_n) nxt = load_coord(S, J.fld_start + kn);
-        kick_particle<METHOD>(C, J, J.fld_start + k, cur);
+        Coord6<R> nxt;
+        if (kn < J.fld_n) nxt = load_coord<R>(S, J.fld_start + kn);
+        kick_particle<R, METHOD>(C, J, J.fld_start + k, cur);
         if (kn >= J.fld_n) break;
         cur = nxt;
         k = kn;
@@ -883,7 +990,7 @@ __global__ void __launch_bounds__(kKickThreads) k_kick(Collide C, int plane0_fro
 // Field mode: each field particle drifted to the collision point of every source-slice center,
 // sh = 0.5*(z - c_i) with c_i = ref[i].  boxes: [sl][ref][4] ordered (xmin, xmax, ymin, ymax).
 struct NodeBoxArgs {
-    const double *x, *px, *y, *py, *z;
+    const void *x, *px, *y, *py, *z;  // slice-sorted coordinates, element type R
     long long start[kMaxSlices], count[kMaxSlices];
     const double *ref;
     unsigned long long *boxes;
@@ -891,7 +998,10 @@ struct NodeBoxArgs {
     int nsl, nref, field_mode, pad;
 };
 
+template <class R>
 __global__ void __launch_bounds__(256) k_node_boxes(NodeBoxArgs A) {
+    const R *AX = (const R *)A.x, *APX = (const R *)A.px, *AY = (const R *)A.y, *APY = (const R *)A.py,
+            *AZ = (const R *)A.z;
     const int sl = blockIdx.y;
     const long long st = A.start[sl], n = A.count[sl];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -904,23 +1014,23 @@ __global__ void __launch_bounds__(256) k_node_boxes(NodeBoxArgs A) {
         bool nan = false;
         for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
             const long long p = st + k;
-            const double x = A.x[p], px = A.px[p], y = A.y[p], py = A.py[p];
-            const double z = A.field_mode ? A.z[p] : 0.0;
+            const R x = AX[p], px = APX[p], y = AY[p], py = APY[p];
+            const R z = A.field_mode ? AZ[p] : R(0);
 #pragma unroll
             for (int r = 0; r < 8; ++r) {
                 if (r < rn) {
-                    double xv, yv;
+                    R xv, yv;
                     if (A.field_mode) {
-                        double sh = 0.5 * (z - A.ref[r0 + r]);
+                        const R sh = R(0.5) * (z - (R)A.ref[r0 + r]);
                         xv = x + sh * px;
                         yv = y + sh * py;
                     } else {
-                        double d = A.ref[(long long)sl * A.nref + r0 + r];
+                        const R d = (R)A.ref[(long long)sl * A.nref + r0 + r];
                         xv = x + px * d;
                         yv = y + py * d;
                     }
                     nan |= (xv != xv) | (yv != yv);
-                    unsigned long long ex = ord_encode(xv), ey = ord_encode(yv);
+                    unsigned long long ex = ord_encode((double)xv), ey = ord_encode((double)yv);
                     mnx[r] = min(mnx[r], ex); mxx[r] = max(mxx[r], ex);
                     mny[r] = min(mny[r], ey); mxy[r] = max(mxy[r], ey);
                 }

@@ -1,6 +1,7 @@
 // Longitudinal slicing on the device (slicing.jl:51-75, 405-460, 523-559).
 //
-// Order-dependent statistics use the reference's canonical 4096-lane fold (slicing.jl:208-257):
+// The particle arrays have element type R (double, or float in the precision form); every statistic
+// is folded in FP64.  Order-dependent statistics use the reference's canonical 4096-lane fold (slicing.jl:208-257):
 // lane t folds elements t, t+4096, ... in order and the lanes are folded serially, so the
 // mean, sigma and slice centroids are bit-identical to the reference's.  Membership is a
 // stable partition: each slice's members keep ascending particle order, the order the
@@ -29,7 +30,8 @@ struct SliceInfo {          // device-resident, read back once per collide
 // keep enough loads in flight each block stages a tile of kTileIters iterations x 32 lanes in shared
 // memory with all its threads, then one thread per lane adds its column in order.
 constexpr int kTileIters = 64;
-__global__ void __launch_bounds__(256) k_lane_fold(const double *__restrict__ z, long long n, const SliceInfo *info,
+template <class R>
+__global__ void __launch_bounds__(256) k_lane_fold(const R *__restrict__ z, long long n, const SliceInfo *info,
                                                    int square, double *lane_sum, double *lane_min, double *lane_max) {
     __shared__ double tile[kTileIters][33];
     const int lane0 = blockIdx.x * 32;
@@ -41,7 +43,7 @@ __global__ void __launch_bounds__(256) k_lane_fold(const double *__restrict__ z,
         for (int e = t; e < kTileIters * 32; e += blockDim.x) {
             const int kk = e >> 5, l = e & 31;
             const long long i = (k0 + kk) * kFoldLanes + lane0 + l;
-            tile[kk][l] = i < n ? z[i] : 0.0;
+            tile[kk][l] = i < n ? (double)z[i] : 0.0;
         }
         __syncthreads();
         if (t < 32) {
@@ -142,7 +144,8 @@ __device__ __forceinline__ int slice_of(double z, const double *b, int ns, int z
 }
 
 // Per-block slice counts over contiguous chunks.
-__global__ void k_slice_count(const double *__restrict__ z, long long n, long long chunk, const SliceInfo *info,
+template <class R>
+__global__ void k_slice_count(const R *__restrict__ z, long long n, long long chunk, const SliceInfo *info,
                               int *counts) {
     __shared__ double b[kMaxSlices + 1];
     __shared__ int c[kMaxSlices];
@@ -152,7 +155,7 @@ __global__ void k_slice_count(const double *__restrict__ z, long long n, long lo
     __syncthreads();
     int zw = info->zero_width;
     long long lo = (long long)blockIdx.x * chunk, hi = min(n, lo + chunk);
-    for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) atomicAdd(&c[slice_of(z[i], b, ns, zw)], 1);
+    for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) atomicAdd(&c[slice_of((double)z[i], b, ns, zw)], 1);
     __syncthreads();
     for (int t = threadIdx.x; t < ns; t += blockDim.x) counts[(long long)blockIdx.x * ns + t] = c[t];
 }
@@ -187,11 +190,11 @@ __global__ void k_slice_offsets(const int *counts, int nblocks, int align, Slice
 
 // Stable scatter into slice-contiguous SoA buffers; perm[pos] = original index.
 // Each block walks its chunk in tiles of blockDim particles, ranking within warps by match_any.
-__global__ void k_slice_scatter(const double *__restrict__ x, const double *__restrict__ px,
-                                const double *__restrict__ y, const double *__restrict__ py,
-                                const double *__restrict__ z, const double *__restrict__ pz, long long n,
-                                long long chunk, const SliceInfo *info, const long long *blockoff, double *sx,
-                                double *spx, double *sy, double *spy, double *sz, double *spz, int *perm) {
+template <class R>
+__global__ void k_slice_scatter(const R *__restrict__ x, const R *__restrict__ px, const R *__restrict__ y,
+                                const R *__restrict__ py, const R *__restrict__ z, const R *__restrict__ pz, long long n,
+                                long long chunk, const SliceInfo *info, const long long *blockoff, R *sx, R *spx, R *sy,
+                                R *spy, R *sz, R *spz, int *perm) {
     __shared__ double b[kMaxSlices + 1];
     __shared__ long long run[kMaxSlices];
     __shared__ int wcount[32][kMaxSlices];
@@ -207,7 +210,7 @@ __global__ void k_slice_scatter(const double *__restrict__ x, const double *__re
         __syncthreads();
         long long i = base + threadIdx.x;
         bool live = i < hi;
-        int s = live ? slice_of(z[i], b, ns, zw) : -1;
+        int s = live ? slice_of((double)z[i], b, ns, zw) : -1;
         unsigned peers = __match_any_sync(0xffffffffu, s);
         int rank = __popc(peers & ((1u << lane) - 1u));
         if (live && rank == 0) wcount[warp][s] = __popc(peers);
@@ -230,13 +233,14 @@ __global__ void k_slice_scatter(const double *__restrict__ x, const double *__re
 }
 
 // Centroid lane sums per slice: lane t folds members t, t+4096, ... of the slice list (slicing.jl:240-257).
-__global__ void k_slice_lanes(const double *__restrict__ sz, const SliceInfo *info, double *lanes) {
+template <class R>
+__global__ void k_slice_lanes(const R *__restrict__ sz, const SliceInfo *info, double *lanes) {
     int s = blockIdx.y;
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= kFoldLanes || s >= info->ns) return;
     long long st = info->start[s], cnt = info->count[s];
     double acc = 0.0;
-    for (long long k = t; k < cnt; k += kFoldLanes) acc += sz[st + k];
+    for (long long k = t; k < cnt; k += kFoldLanes) acc += (double)sz[st + k];
     lanes[(long long)s * kFoldLanes + t] = acc;
 }
 
@@ -265,9 +269,10 @@ __global__ void __launch_bounds__(1024) k_slice_finish(const double *lanes, long
 }
 
 // Write the kicked slice-sorted coordinates back in caller order.
-__global__ void k_unsort(const int *__restrict__ perm, long long total, const double *sx, const double *spx,
-                         const double *sy, const double *spy, const double *sz, const double *spz, double *x,
-                         double *px, double *y, double *py, double *z, double *pz, const SliceInfo *info) {
+template <class R>
+__global__ void k_unsort(const int *__restrict__ perm, long long total, const R *sx, const R *spx, const R *sy,
+                         const R *spy, const R *sz, const R *spz, R *x, R *px, R *y, R *py, R *z, R *pz,
+                         const SliceInfo *info) {
     // total = padded length; padding positions carry perm = -1
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= total) return;

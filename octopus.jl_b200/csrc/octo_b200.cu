@@ -108,6 +108,13 @@ std::vector<std::vector<OrderEntry>> pair_batches(const std::vector<OrderEntry> 
     return batches;
 }
 
+// Run f with the particle real type of the context: double (plain form) or float (precision form).
+template <class F>
+void with_real(bool fp32, F f) {
+    if (fp32) f(float(0));
+    else f(double(0));
+}
+
 template <class T>
 struct DevBuf {
     T *p = nullptr;
@@ -150,7 +157,7 @@ constexpr int kAlign = 32;           // slice start alignment (elements)
 constexpr long long kChunk = 8192;   // particles per slicing block
 
 struct BeamWS {
-    DevBuf<double> s[6];  // slice-sorted coordinates
+    DevBuf<double> s[6];  // slice-sorted coordinates (sized in doubles; float elements in the precision form)
     DevBuf<int> perm;
     DevBuf<SliceInfo> info;
     DevBuf<double> lane_sum, lane_min, lane_max, lanes, q;
@@ -175,7 +182,9 @@ struct octo_ctx {
     std::string err;
     int ns[2] = {0, 0};
     BeamWS bw[2];
-    DevBuf<double2> tw_x, tw_y;
+    DevBuf<double2> tw_x, tw_y;  // FP64 twiddles (Green spectra; plain-form convolution)
+    DevBuf<float2> twf_x, twf_y; // FP32 twiddles (precision-form convolution)
+    int fp32 = 0;                // precision form: float particles, field planes and FFTs
     DevBuf<Task> tasks;
     DevBuf<Plane> planes;
     DevBuf<LumJob> lumjobs;
@@ -301,7 +310,10 @@ int validate_options(const octo_pic_options &o, std::string &msg) {
         const double *p = b == 0 ? o.positions1 : o.positions2;
         if (m == OCTO_SLICING_SPECIFIED && ns > 1 && !p) { msg = "specified slicing requires nslices-1 internal positions"; return OCTO_ERR_ARG; }
     }
-    if (o.precision != 0) { msg = "only the FP64 plain form (precision = 0) is available"; return OCTO_ERR_UNSUPPORTED; }
+    if (o.precision != 0 && o.precision != 1) {
+        msg = "precision must be 0 (FP64 plain form) or 1 (FP32 precision form)";
+        return OCTO_ERR_ARG;
+    }
     return OCTO_OK;
 }
 
@@ -313,6 +325,16 @@ void upload_twiddles(DevBuf<double2> &buf, int L) {
     }
     buf.ensure(L / 2);
     CK(cudaMemcpy(buf.p, h.data(), sizeof(double2) * (L / 2), cudaMemcpyHostToDevice));
+}
+// FP32 twiddles: the FP64 values rounded once.
+void upload_twiddles(DevBuf<float2> &buf, int L) {
+    std::vector<float2> h(L / 2);
+    for (int k = 0; k < L / 2; ++k) {
+        double a = 2.0 * 3.141592653589793238462643 * (double)k / (double)L;
+        h[k] = make_float2((float)std::cos(a), (float)-std::sin(a));
+    }
+    buf.ensure(L / 2);
+    CK(cudaMemcpy(buf.p, h.data(), sizeof(float2) * (L / 2), cudaMemcpyHostToDevice));
 }
 
 long long padded_total(long long n, int ns) { return n + (long long)ns * kAlign; }
@@ -354,45 +376,58 @@ void slice_beam(octo_ctx *c, int b, const octo_beam &beam, cudaStream_t st, long
     W.counts.ensure((size_t)nblocks * ns);
     W.blockoff.ensure((size_t)nblocks * ns);
     W.total = total;
-    const double *z = (const double *)beam.z;
     int method = b == 0 ? c->opt.slicing_method1 : c->opt.slicing_method2;
     int cpos = b == 0 ? c->opt.center_position1 : c->opt.center_position2;
-    k_lane_fold<<<kFoldLanes / 32, 256, 0, st>>>(z, n, W.info.p, 0, W.lane_sum.p, W.lane_min.p, W.lane_max.p);
-    k_fold_stats<<<1, 1024, 0, st>>>(W.lane_sum.p, W.lane_min.p, W.lane_max.p, n, 0, method, ns, W.q.p, W.info.p);
-    k_lane_fold<<<kFoldLanes / 32, 256, 0, st>>>(z, n, W.info.p, 1, W.lane_sum.p, W.lane_min.p, W.lane_max.p);
-    k_fold_stats<<<1, 1024, 0, st>>>(W.lane_sum.p, W.lane_min.p, W.lane_max.p, n, 1, method, ns, W.q.p, W.info.p);
-    k_slice_count<<<(unsigned)nblocks, 256, 0, st>>>(z, n, kChunk, W.info.p, W.counts.p);
-    k_slice_offsets<<<1, 64, 0, st>>>(W.counts.p, (int)nblocks, kAlign, W.info.p, W.blockoff.p);
-    CK(cudaMemsetAsync(W.perm.p, 0xff, sizeof(int) * total, st));
-    k_slice_scatter<<<(unsigned)nblocks, 256, 0, st>>>(
-        (const double *)beam.x, (const double *)beam.px, (const double *)beam.y, (const double *)beam.py, z,
-        (const double *)beam.pz, n, kChunk, W.info.p, W.blockoff.p, W.s[0].p, W.s[1].p, W.s[2].p, W.s[3].p, W.s[4].p,
-        W.s[5].p, W.perm.p);
-    k_slice_lanes<<<dim3(kFoldLanes / 256, ns), 256, 0, st>>>(W.s[4].p, W.info.p, W.lanes.p);
-    k_slice_finish<<<ns, 1024, 0, st>>>(W.lanes.p, n, cpos, W.info.p);
+    with_real(c->fp32, [&](auto r) {
+        using R = decltype(r);
+        const R *z = (const R *)beam.z;
+        R *ws[6];
+        for (int k = 0; k < 6; ++k) ws[k] = (R *)W.s[k].p;
+        k_lane_fold<R><<<kFoldLanes / 32, 256, 0, st>>>(z, n, W.info.p, 0, W.lane_sum.p, W.lane_min.p, W.lane_max.p);
+        k_fold_stats<<<1, 1024, 0, st>>>(W.lane_sum.p, W.lane_min.p, W.lane_max.p, n, 0, method, ns, W.q.p, W.info.p);
+        k_lane_fold<R><<<kFoldLanes / 32, 256, 0, st>>>(z, n, W.info.p, 1, W.lane_sum.p, W.lane_min.p, W.lane_max.p);
+        k_fold_stats<<<1, 1024, 0, st>>>(W.lane_sum.p, W.lane_min.p, W.lane_max.p, n, 1, method, ns, W.q.p, W.info.p);
+        k_slice_count<R><<<(unsigned)nblocks, 256, 0, st>>>(z, n, kChunk, W.info.p, W.counts.p);
+        k_slice_offsets<<<1, 64, 0, st>>>(W.counts.p, (int)nblocks, kAlign, W.info.p, W.blockoff.p);
+        CK(cudaMemsetAsync(W.perm.p, 0xff, sizeof(int) * total, st));
+        k_slice_scatter<R><<<(unsigned)nblocks, 256, 0, st>>>(
+            (const R *)beam.x, (const R *)beam.px, (const R *)beam.y, (const R *)beam.py, z, (const R *)beam.pz, n, kChunk,
+            W.info.p, W.blockoff.p, ws[0], ws[1], ws[2], ws[3], ws[4], ws[5], W.perm.p);
+        k_slice_lanes<R><<<dim3(kFoldLanes / 256, ns), 256, 0, st>>>(ws[4], W.info.p, W.lanes.p);
+        k_slice_finish<<<ns, 1024, 0, st>>>(W.lanes.p, n, cpos, W.info.p);
+    });
     launches += 10;
     CK(cudaGetLastError());
 }
 
 long long first_nonfinite_host(const octo_beam &beam, cudaStream_t st, bool z_only) {
-    std::vector<double> h(beam.n);
+    const size_t esz = beam.dtype == 1 ? sizeof(float) : sizeof(double);
+    std::vector<unsigned char> h((size_t)beam.n * esz);
     void *arr[6] = {beam.x, beam.px, beam.y, beam.py, beam.z, beam.pz};
     long long first = -1;
     for (int k = 0; k < 6; ++k) {
         if (z_only && k != 4) continue;
-        CK(cudaMemcpyAsync(h.data(), arr[k], sizeof(double) * beam.n, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(h.data(), arr[k], esz * beam.n, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        for (long long i = 0; i < beam.n; ++i)
-            if (!std::isfinite(h[i])) { if (first < 0 || i < first) first = i; break; }
+        for (long long i = 0; i < beam.n; ++i) {
+            const double v = beam.dtype == 1 ? (double)((const float *)h.data())[i] : ((const double *)h.data())[i];
+            if (!std::isfinite(v)) { if (first < 0 || i < first) first = i; break; }
+        }
     }
     return first;
 }
 
-int check_beam(const octo_beam *b, std::string &msg) {
+// dtype: the element type the call requires (0 float64, 1 float32), or -1 for either.
+int check_beam(const octo_beam *b, std::string &msg, int dtype = 0) {
     if (!b) { msg = "beam pointer is NULL"; return OCTO_ERR_ARG; }
     if (b->n <= 0) { msg = "longitudinal slicing requires at least one particle"; return OCTO_ERR_ARG; }
     if (b->n >= (1LL << 31) - 4096) { msg = "beam too large for 32-bit particle indices"; return OCTO_ERR_ARG; }
-    if (b->dtype != 0) { msg = "only float64 beams are supported"; return OCTO_ERR_UNSUPPORTED; }
+    if (b->dtype != 0 && b->dtype != 1) { msg = "beam dtype must be 0 (float64) or 1 (float32)"; return OCTO_ERR_ARG; }
+    if (dtype >= 0 && b->dtype != dtype) {
+        msg = dtype == 0 ? "this call needs float64 beams (the plain form's element type)"
+                         : "the precision form (precision = 1) needs float32 beams";
+        return OCTO_ERR_ARG;
+    }
     if (!b->x || !b->px || !b->y || !b->py || !b->z || !b->pz) { msg = "beam coordinate pointer is NULL"; return OCTO_ERR_ARG; }
     return OCTO_OK;
 }
@@ -404,12 +439,15 @@ void launch_method(int method, F f) {
 }
 
 
-// Dynamic shared memory of the FFT kernels for line lengths NX, NY (4 warps per block).
-size_t fft_smem(int L) { return sizeof(double2) * (size_t)(L / 2 + 4 * L); }
-// k_green_rows: twiddles + 4 lines + the (kGreenRows+1) x (NX+1) corner lattice of F.
+// Dynamic shared memory of the FFT kernels for line length L (4 warps per block), complex elements of
+// `real` bytes per component (8 FP64, 4 FP32).
+size_t fft_smem(int L, size_t real = sizeof(double)) { return 2 * real * (size_t)(L / 2 + 4 * L); }
+// k_green_rows (FP64): twiddles + 4 lines + the (kGreenRows+1) x (NX+1) corner lattice of F.
 size_t green_smem(int NX) { return fft_smem(NX) + sizeof(double) * (size_t)(kGreenRows + 1) * (NX + 1); }
 // k_conv_field: twiddles (NX/2) + 4 lines (4*NX) complex, plus a (tile+4) x nx phi tile; NX = 2*nx.
-size_t field_smem(int NX) { return sizeof(double2) * (size_t)(NX / 2 + 4 * NX) + sizeof(double) * (size_t)(kFieldTile + 4) * (NX / 2); }
+size_t field_smem(int NX, size_t real = sizeof(double)) {
+    return fft_smem(NX, real) + real * (size_t)(kFieldTile + 4) * (NX / 2);
+}
 constexpr size_t kSmemLimit = 227 * 1024;
 
 // Enqueue the node meshes of both directions (pic_cpu.jl:1404-1419) with no host synchronisation: the
@@ -460,7 +498,7 @@ void build_node_meshes(octo_ctx *c, Collide &C, const SliceInfo &S1, const Slice
         A.nanf = c->nodenan.p;
         A.nsl = nss; A.nref = nb; A.field_mode = 0;
         unsigned bx = (unsigned)std::min<long long>(64, (maxn + 4095) / 4096);
-        k_node_boxes<<<dim3(bx, nss), 256, 0, st>>>(A);
+        with_real(c->fp32, [&](auto r) { k_node_boxes<decltype(r)><<<dim3(bx, nss), 256, 0, st>>>(A); });
         NodeBoxArgs F{};
         F.x = WF.s[0].p; F.px = WF.s[1].p; F.y = WF.s[2].p; F.py = WF.s[3].p; F.z = WF.s[4].p;
         maxn = 1;
@@ -470,7 +508,7 @@ void build_node_meshes(octo_ctx *c, Collide &C, const SliceInfo &S1, const Slice
         F.nanf = c->nodenan.p;
         F.nsl = nsf; F.nref = nss; F.field_mode = 1;
         bx = (unsigned)std::min<long long>(64, (maxn + 4095) / 4096);
-        k_node_boxes<<<dim3(bx, nsf), 256, 0, st>>>(F);
+        with_real(c->fp32, [&](auto r) { k_node_boxes<decltype(r)><<<dim3(bx, nsf), 256, 0, st>>>(F); });
         k_node_plan<<<(nss * nb + 63) / 64, 64, 0, st>>>(c->dopt, sbox, fbox, nss, nb, dcnt, c->nodenan.p,
                                                          c->nodes.p + mesh0, c->status.p);
         launches += 5;
@@ -497,10 +535,12 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
     const octo_pic_options &o = c->opt;
     long long launches = 0;
     std::string msg;
-    int rc = check_beam(b1, msg);
-    if (rc == OCTO_OK) rc = check_beam(b2, msg);
+    int rc = check_beam(b1, msg, c->fp32);
+    if (rc == OCTO_OK) rc = check_beam(b2, msg, c->fp32);
     if (rc != OCTO_OK) throw OctoFail{rc, msg};
     if (!p1 || !p2) throw OctoFail{OCTO_ERR_ARG, "beam params pointer is NULL"};
+    const bool fp32 = c->fp32 != 0;
+    const size_t rsz = fp32 ? sizeof(float) : sizeof(double);
     CK(cudaSetDevice(c->device));
     // kbb and luminosity scale (slicing.jl:77-91, pic_cpu.jl:821-829)
     if (!o.has_kbb1 && !(std::isfinite(p1->E0) && p1->E0 != 0))
@@ -549,6 +589,8 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
         for (int k = 0; k < 6; ++k) C.beam[b].c[k] = c->bw[b].s[k].p;
     C.tw_x = c->tw_x.p;
     C.tw_y = c->tw_y.p;
+    C.twr_x = fp32 ? (const void *)c->twf_x.p : (const void *)c->tw_x.p;
+    C.twr_y = fp32 ? (const void *)c->twf_y.p : (const void *)c->tw_y.p;
     C.gstride = c->gstride;
 
     // ---- Green slots / cache / status
@@ -654,12 +696,15 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
                         P.geom = (k == 1) ? T.nodeR : T.nodeL;
                         P.green = P.geom;
                         P.count_dropped = k < 2 ? 1 : 0;
+                        if (fp32 && k == 2) { P.other_delta = -2; P.self_first = 0; }  // L - Z
                     } else {
                         P.kind = k == 0 ? 0 : (k == 1 ? 1 : 2);
                         P.s = k == 0 ? T.sL : (k == 1 ? T.sR : 0.5 * (T.sL + T.sR));
                         P.geom = -1;
                         P.green = -1;
                         P.count_dropped = 0;
+                        if (fp32 && !quad && k == 1) { P.other_delta = -1; P.self_first = 0; }  // L - R
+                        if (fp32 && quad && k < 2) { P.other_delta = 2 - k; P.self_first = 1; }  // L - M, R - M
                     }
                     planes.push_back(P);
                 }
@@ -709,7 +754,7 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
         CK(cudaMemsetAsync(c->qgrid.p, 0, sizeof(long long) * c->qgrid.n, st));
     }
     c->spec.ensure((size_t)max_planes * (nx + 1) * ny);
-    c->fields.ensure((size_t)max_planes * 2 * cells);
+    c->fields.ensure((size_t)max_planes * (fp32 ? 1 : 2) * cells);  // double2 units: 32 B (FP64) / 16 B (FP32) per cell
     c->lum_partial.ensure((size_t)max_lum * kLumSplit);
     if (c->lq.n < (size_t)2 * max_lum * lcells) {
         c->lq.ensure((size_t)2 * max_lum * lcells);
@@ -759,10 +804,13 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
         for (int t = F.t0; t < F.t0 + F.nt; t += 2) slice_bytes += (double)(tasks[t].src_n + tasks[t].fld_n);
         for (int t = F.t0; t < F.t0 + F.nt; ++t) { src_bytes += (double)tasks[t].src_n; fld_bytes += (double)tasks[t].fld_n; }
         if (!node || compute_lum) {
-            PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, 1, slice_bytes * 5 * sizeof(double));
+            PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, 1, slice_bytes * 5 * rsz);
             unsigned bps = (unsigned)std::max<long long>(1, std::min<long long>(128, (F.maxsrc + 2047) / 2048));
-            if (node) k_pair_bounds<true><<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
-            else k_pair_bounds<false><<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
+            with_real(fp32, [&](auto r) {
+                using R = decltype(r);
+                if (node) k_pair_bounds<R, true><<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
+                else k_pair_bounds<R, false><<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
+            });
             launches++;
         }
         if (!node) {
@@ -776,36 +824,49 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
             launches += 3;
         }
         if (compute_lum && F.nl) {
-            PhaseScope ps(c, OCTO_PHASE_LUMINOSITY, st, 4, slice_bytes * 4 * sizeof(double));
+            PhaseScope ps(c, OCTO_PHASE_LUMINOSITY, st, 4, slice_bytes * 4 * rsz);
             k_lum_plan<<<(F.nl + 63) / 64, 64, 0, st>>>(C, F.l0, F.nl, F.t0);
             unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(8, (F.maxlum + 32767) / 32768));
-            launch_method(lmethod, [&](auto M) {
-                k_lum_deposit<decltype(M)::value><<<dim3(bpp, 2 * F.nl), 1024, lum_bytes, st>>>(C, F.l0);
+            with_real(fp32, [&](auto r) {
+                launch_method(lmethod, [&](auto M) {
+                    k_lum_deposit<decltype(r), decltype(M)::value><<<dim3(bpp, 2 * F.nl), 1024, lum_bytes, st>>>(C, F.l0);
+                });
             });
             k_lum_overlap<<<dim3(kLumSplit, F.nl), 256, 0, st>>>(C, F.l0);
             k_lum_fold<<<(F.nl + 63) / 64, 64, 0, st>>>(C, F.l0, F.nl);
             launches += 4;
         }
         {
-            PhaseScope ps(c, OCTO_PHASE_DEPOSIT, st, 1, src_bytes * 4 * sizeof(double));
+            PhaseScope ps(c, OCTO_PHASE_DEPOSIT, st, 1, src_bytes * 4 * rsz);
             unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(8, (F.maxsrc + 32767) / 32768));
-            launch_method(method, [&](auto M) {
-                k_deposit<decltype(M)::value><<<dim3(bpp, F.np), 1024, dep_bytes, st>>>(C, F.p0);
+            with_real(fp32, [&](auto r) {
+                launch_method(method, [&](auto M) {
+                    k_deposit<decltype(r), decltype(M)::value><<<dim3(bpp, F.np), 1024, dep_bytes, st>>>(C, F.p0);
+                });
             });
         }
         {
             PhaseScope ps(c, OCTO_PHASE_FFT, st, 2);
-            k_conv_rows<<<dim3((ny / 2 + 3) / 4, F.np), 128, fft_smem(NX), st>>>(C, F.p0);
-            k_conv_cols<<<dim3((nx + 1 + 3) / 4, F.np), 128, fft_smem(NY), st>>>(C, F.p0);
+            with_real(fp32, [&](auto r) {
+                using R = decltype(r);
+                k_conv_rows<R><<<dim3((ny / 2 + 3) / 4, F.np), 128, fft_smem(NX, rsz), st>>>(C, F.p0);
+                if (fp32)  // the precision form reads partner grids, so the front's grids are cleared here
+                    CK(cudaMemsetAsync(c->qgrid.p, 0, sizeof(long long) * cells * F.np, st));
+                k_conv_cols<R><<<dim3((nx + 1 + 3) / 4, F.np), 128, fft_smem(NY, rsz), st>>>(C, F.p0);
+            });
         }
         {
             PhaseScope ps(c, OCTO_PHASE_FIELD, st, 1);
-            k_conv_field<<<dim3((ny + kFieldTile - 1) / kFieldTile, F.np), 128, field_smem(NX), st>>>(C, F.p0);
+            with_real(fp32, [&](auto r) {
+                k_conv_field<decltype(r)><<<dim3((ny + kFieldTile - 1) / kFieldTile, F.np), 128, field_smem(NX, rsz), st>>>(C, F.p0);
+            });
         }
         {
-            PhaseScope ps(c, OCTO_PHASE_KICK, st, 1, fld_bytes * 11 * sizeof(double));
-            launch_method(method, [&](auto M) {
-                k_kick<decltype(M)::value><<<F.nb, kKickThreads, 0, st>>>(C, F.p0, c->blockmap.p + F.b0);
+            PhaseScope ps(c, OCTO_PHASE_KICK, st, 1, fld_bytes * 11 * rsz);
+            with_real(fp32, [&](auto r) {
+                launch_method(method, [&](auto M) {
+                    k_kick<decltype(r), decltype(M)::value><<<F.nb, kKickThreads, 0, st>>>(C, F.p0, c->blockmap.p + F.b0);
+                });
             });
         }
         launches += 5;
@@ -814,13 +875,17 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
 
     // ---- back to caller order
     {
-        PhaseScope ps(c, OCTO_PHASE_UNSORT, st, 2, (double)(n1 + n2) * 12 * sizeof(double));
+        PhaseScope ps(c, OCTO_PHASE_UNSORT, st, 2, (double)(n1 + n2) * 12 * rsz);
         for (int b = 0; b < 2; ++b) {
             const BeamWS &W = c->bw[b];
             const octo_beam &B = b == 0 ? *b1 : *b2;
-            k_unsort<<<(unsigned)((W.total + 255) / 256), 256, 0, st>>>(
-                W.perm.p, W.total, W.s[0].p, W.s[1].p, W.s[2].p, W.s[3].p, W.s[4].p, W.s[5].p, (double *)B.x,
-                (double *)B.px, (double *)B.y, (double *)B.py, (double *)B.z, (double *)B.pz, W.info.p);
+            with_real(fp32, [&](auto r) {
+                using R = decltype(r);
+                k_unsort<R><<<(unsigned)((W.total + 255) / 256), 256, 0, st>>>(
+                    W.perm.p, W.total, (const R *)W.s[0].p, (const R *)W.s[1].p, (const R *)W.s[2].p,
+                    (const R *)W.s[3].p, (const R *)W.s[4].p, (const R *)W.s[5].p, (R *)B.x, (R *)B.px, (R *)B.y,
+                    (R *)B.py, (R *)B.z, (R *)B.pz, W.info.p);
+            });
             launches++;
         }
     }
@@ -939,8 +1004,13 @@ octo_ctx *octo_create(int32_t device, const octo_pic_options *options) {
     d.growth = options->green_growth;
     try {
         CK(cudaSetDevice(device));
+        c->fp32 = options->precision == 1;
         upload_twiddles(c->tw_x, 2 * options->nx);
         upload_twiddles(c->tw_y, 2 * options->ny);
+        if (c->fp32) {
+            upload_twiddles(c->twf_x, 2 * options->nx);
+            upload_twiddles(c->twf_y, 2 * options->ny);
+        }
         c->gstride = (long long)(options->nx + 1) * 2 * options->ny;
         for (int b = 0; b < 2; ++b) {
             int ns = c->ns[b];
@@ -957,16 +1027,19 @@ octo_ctx *octo_create(int32_t device, const octo_pic_options *options) {
         if (dep > kSmemLimit || lum > kSmemLimit)
             throw CudaFail{"grid too large for the shared-memory deposit (at most 168 x 168 cells on this backend)"};
         int dsm = (int)dep, lsm = (int)lum;
-        CK(cudaFuncSetAttribute(k_deposit<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
-        CK(cudaFuncSetAttribute(k_deposit<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
-        CK(cudaFuncSetAttribute(k_lum_deposit<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
-        CK(cudaFuncSetAttribute(k_lum_deposit<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
-        int fx = (int)fft_smem(2 * options->nx), fy = (int)fft_smem(2 * options->ny), ff = (int)field_smem(2 * options->nx);
         CK(cudaFuncSetAttribute(k_green_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)green_smem(2 * options->nx)));
-        CK(cudaFuncSetAttribute(k_green_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, fy));
-        CK(cudaFuncSetAttribute(k_conv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, fx));
-        CK(cudaFuncSetAttribute(k_conv_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, fy));
-        CK(cudaFuncSetAttribute(k_conv_field, cudaFuncAttributeMaxDynamicSharedMemorySize, ff));
+        CK(cudaFuncSetAttribute(k_green_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(2 * options->ny)));
+        with_real(c->fp32, [&](auto r) {
+            using R = decltype(r);
+            const size_t rs = sizeof(R);
+            CK(cudaFuncSetAttribute(k_deposit<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
+            CK(cudaFuncSetAttribute(k_deposit<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
+            CK(cudaFuncSetAttribute(k_lum_deposit<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
+            CK(cudaFuncSetAttribute(k_lum_deposit<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
+            CK(cudaFuncSetAttribute(k_conv_rows<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(2 * options->nx, rs)));
+            CK(cudaFuncSetAttribute(k_conv_cols<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(2 * options->ny, rs)));
+            CK(cudaFuncSetAttribute(k_conv_field<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)field_smem(2 * options->nx, rs)));
+        });
     } catch (CudaFail &e) {
         c->err = e.msg;
         c->opt.nx = 0;
@@ -979,7 +1052,7 @@ void octo_destroy(octo_ctx *c) {
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
     for (auto &b : c->bw) b.release();
-    c->tw_x.release(); c->tw_y.release(); c->tasks.release(); c->planes.release(); c->lumjobs.release();
+    c->tw_x.release(); c->tw_y.release(); c->twf_x.release(); c->twf_y.release(); c->tasks.release(); c->planes.release(); c->lumjobs.release();
     c->geom.release(); c->blockmap.release(); c->cache.release(); c->nodes.release(); c->lumgeom.release();
     c->bnd.release(); c->lumb.release(); c->nodebox_s.release(); c->nodebox_f.release(); c->nanflag.release();
     c->nodenan.release(); c->status.release(); c->ghat.release(); c->qgrid.release(); c->lq.release();
@@ -1038,15 +1111,17 @@ int64_t octo_pair_luminosity_trace(octo_ctx *c, int32_t *pi, int32_t *pj, double
 int32_t octo_linear6d(octo_ctx *c, octo_beam *beam, const double matrix[36], int32_t turns, void *stream) {
     if (!c || !beam || !matrix) return OCTO_ERR_ARG;
     std::string msg;
-    int rc = check_beam(beam, msg);
+    int rc = check_beam(beam, msg, -1);
     if (rc != OCTO_OK) return fail(c, rc, msg);
     try {
         CK(cudaSetDevice(c->device));
         Mat6 M;
         for (int k = 0; k < 36; ++k) M.m[k] = matrix[k];
-        k_linear6d<<<(unsigned)((beam->n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
-            (double *)beam->x, (double *)beam->px, (double *)beam->y, (double *)beam->py, (double *)beam->z,
-            (double *)beam->pz, beam->n, M, turns);
+        with_real(beam->dtype == 1, [&](auto r) {
+            using R = decltype(r);
+            k_linear6d<R><<<(unsigned)((beam->n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+                (R *)beam->x, (R *)beam->px, (R *)beam->y, (R *)beam->py, (R *)beam->z, (R *)beam->pz, beam->n, M, turns);
+        });
         CK(cudaGetLastError());
         return OCTO_OK;
     } catch (CudaFail &e) {

@@ -46,6 +46,10 @@ struct Plane {
     int32_t count_dropped;
     int32_t src_beam;
     int32_t pad;
+    // Precision form only: the plane is transformed as an exact int64 difference of charge grids,
+    // q[self] - q[self + other_delta] (self_first = 1) or q[self + other_delta] - q[self] (self_first = 0),
+    // so potentials that the kick subtracts are solved without FP32 cancellation.  other_delta = 0: none.
+    int32_t other_delta, self_first;
     int64_t src_start, src_n;
     double s;            // drift of the deposit
 };
@@ -128,43 +132,73 @@ __host__ __device__ inline double jmax(double a, double b) {
 __host__ __device__ inline double jclamp(double x, double lo, double hi) {
     return x > hi ? hi : (x < lo ? lo : x);
 }
+__host__ __device__ inline float jclamp(float x, float lo, float hi) {
+    return x > hi ? hi : (x < lo ? lo : x);
+}
+
+// ---------------------------------------------------------------- particle real type
+// R is the element type of the particle arrays and the arithmetic type of the particle kernels:
+// double for the plain form, float for the precision form (FP32 particles, field planes and FFTs;
+// FP64 Green function, slice statistics, grid geometry and luminosity sums; int64 charge grids).
+// Every expression is written once for both, so the R = double instantiation is the plain form.
+template <class R>
+struct RealT;
+template <>
+struct RealT<double> {
+    using C2 = double2;  // complex FFT element
+    using FC = double2;  // field-plane vector: a cell is two of them, (phi, Ex), (Ey, 0)
+    static constexpr int kCellVec = 2;
+};
+template <>
+struct RealT<float> {
+    using C2 = float2;
+    using FC = float4;   // a cell is one 16-byte vector (phi, Ex, Ey, 0)
+    static constexpr int kCellVec = 1;
+};
+
+__device__ __forceinline__ int floor_int(double u) { return __double2int_rd(u); }
+__device__ __forceinline__ int floor_int(float u) { return __float2int_rd(u); }
+__device__ __forceinline__ long long round_ll(double v) { return __double2ll_rn(v); }
+__device__ __forceinline__ long long round_ll(float v) { return __float2ll_rn(v); }
 
 // ---------------------------------------------------------------- weights
 // CIC (pic_cpu.jl:2182-2197): 1-based base, zero weights outside [0, n-1] or non-finite.
-__device__ __forceinline__ void cic_weights(double u, int n, int &base, double w[2]) {
-    if (!(0.0 <= u && u <= (double)(n - 1))) {
-        base = 1; w[0] = 0.0; w[1] = 0.0;
+template <class R>
+__device__ __forceinline__ void cic_weights(R u, int n, int &base, R w[2]) {
+    if (!(R(0) <= u && u <= (R)(n - 1))) {
+        base = 1; w[0] = R(0); w[1] = R(0);
         return;
     }
-    int b = __double2int_rd(u) + 1;  // floor(u) + 1; u is in [0, n-1] here
+    int b = floor_int(u) + 1;  // floor(u) + 1; u is in [0, n-1] here
     b = b < 1 ? 1 : (b > n - 1 ? n - 1 : b);
     base = b;
-    double f = jclamp(u - (double)(base - 1), 0.0, 1.0);
-    w[0] = 1.0 - f;
+    R f = jclamp(u - (R)(base - 1), R(0), R(1));
+    w[0] = R(1) - f;
     w[1] = f;
 }
 
 // TSC (pic_cpu.jl:2225-2252).
-__device__ __forceinline__ void tsc_weights(double u, int n, int &base, double w[3]) {
-    if (!(0.0 <= u && u <= (double)(n - 1))) {
-        base = 1; w[0] = 0.0; w[1] = 0.0; w[2] = 0.0;
+template <class R>
+__device__ __forceinline__ void tsc_weights(R u, int n, int &base, R w[3]) {
+    if (!(R(0) <= u && u <= (R)(n - 1))) {
+        base = 1; w[0] = R(0); w[1] = R(0); w[2] = R(0);
         return;
     }
-    const int ix = __double2int_rd(u);  // floor(u); u is in [0, n-1] here
-    double f = u - (double)ix;
+    const int ix = floor_int(u);  // floor(u); u is in [0, n-1] here
+    R f = u - (R)ix;
     int b;
-    if (f < 0.5) {
-        double t = f * f;
-        w[0] = 0.125 + 0.5 * (t - f);
-        w[1] = 0.75 - t;
-        w[2] = 0.125 + 0.5 * (t + f);
+    if (f < R(0.5)) {
+        R t = f * f;
+        w[0] = R(0.125) + R(0.5) * (t - f);
+        w[1] = R(0.75) - t;
+        w[2] = R(0.125) + R(0.5) * (t + f);
         b = ix;
     } else {
-        double fr = 1.0 - f;
-        double t = fr * fr;
-        w[0] = 0.125 + 0.5 * (t + fr);
-        w[1] = 0.75 - t;
-        w[2] = 0.125 + 0.5 * (t - fr);
+        R fr = R(1) - f;
+        R t = fr * fr;
+        w[0] = R(0.125) + R(0.5) * (t + fr);
+        w[1] = R(0.75) - t;
+        w[2] = R(0.125) + R(0.5) * (t - fr);
         b = ix + 1;
     }
     b = b < 1 ? 1 : (b > n - 2 ? n - 2 : b);

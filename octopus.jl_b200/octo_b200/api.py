@@ -43,10 +43,16 @@ class TrackingContext:
 class Context:
     """One libocto_b200 context: device workspaces plus the slice-pair Green cache."""
 
-    def __init__(self, solver: PICPoissonSolver, device: int = 0):
+    def __init__(self, solver: PICPoissonSolver, device: int = 0, dtype: torch.dtype = torch.float64):
+        """dtype is the beams' element type: float64 runs the plain form, float32 the precision form
+        (FP32 particles, field planes and FFTs; FP64 Green function, statistics and luminosity)."""
+        if dtype not in (torch.float64, torch.float32):
+            raise ArgumentError("beam element type must be Float64 or Float32")
         self.solver = solver
         self.device = device
+        self.dtype = dtype
         self._opts = solver.to_c()
+        self._opts.precision = 1 if dtype == torch.float32 else 0
         self._ptr = _lib.lib().octo_create(int(device), C.byref(self._opts))
         if not self._ptr:
             raise RuntimeError("octo_create failed")
@@ -105,16 +111,17 @@ class Context:
 
 
 class StrongStrongRuntime:
-    """Twin of task.runtime_cache: one persistent context per (label, solver)."""
+    """Twin of task.runtime_cache: one persistent context per (label, solver, element type), the key
+    of pic_cpu.jl:499-515."""
 
     def __init__(self):
         self._ctx: Dict[tuple, Context] = {}
 
-    def context(self, label: str, solver: PICPoissonSolver, device: int) -> Context:
-        key = (label, solver, device)
+    def context(self, label: str, solver: PICPoissonSolver, device: int, dtype: torch.dtype = torch.float64) -> Context:
+        key = (label, solver, device, dtype)
         ctx = self._ctx.get(key)
         if ctx is None:
-            ctx = Context(solver, device)
+            ctx = Context(solver, device, dtype)
             self._ctx[key] = ctx
         return ctx
 
@@ -143,16 +150,19 @@ def collide(solver: PICPoissonSolver, beam1: Beam, beam2: Beam, backend=CUDABack
         raise ArgumentError("this backend implements collide! for CUDABackend beams only")
     if beam1.coords.device != beam2.coords.device:
         raise ArgumentError("both beams must be on the same device (interface.jl:2461-2464)")
+    if beam1.dtype != beam2.dtype:
+        raise ArgumentError("both beams must have the same element type")
     device = beam1.coords.device.index or 0
     turn = -1 if ctx is None else int(ctx.turn)
     lum_on = compute_luminosity(solver, ctx)
     if runtime is None:
-        c = Context(solver, device)
+        c = Context(solver, device, beam1.dtype)
         try:
             return c.collide(beam1, beam2, turn=turn, compute_luminosity=lum_on)
         finally:
             c.close()
-    return runtime.context(label, solver, device).collide(beam1, beam2, turn=turn, compute_luminosity=lum_on)
+    return runtime.context(label, solver, device, beam1.dtype).collide(beam1, beam2, turn=turn,
+                                                                       compute_luminosity=lum_on)
 
 
 _scratch: Dict[int, int] = {}

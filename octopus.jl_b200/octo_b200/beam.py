@@ -1,5 +1,6 @@
 """Device-resident beams: ``Beam`` holds the six SoA coordinates (Phase6DRep, Beam.jl:45-55)
-as CUDA float64 tensors and the ``BeamParams`` (Beam.jl:29-35)."""
+as CUDA float64 tensors (or float32 for the precision form, the reference's Beam{CUDABackend, Float32})
+and the ``BeamParams`` (Beam.jl:29-35)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -32,16 +33,28 @@ class BeamParams:
         return _lib.OctoBeamParams(self.charge, self.mc2, self.E0, self.r0, self.npart)
 
 
+_DTYPE_CODE = {torch.float64: 0, torch.float32: 1}
+
+
 class Beam:
-    """A beam on one CUDA device: ``coords`` is a (6, n) float64 tensor, rows x, px, y, py, z, pz."""
+    """A beam on one CUDA device: ``coords`` is a (6, n) float64 (plain form) or float32 (precision
+    form) tensor, rows x, px, y, py, z, pz."""
 
     def __init__(self, coords: torch.Tensor, params: BeamParams):
         if coords.dim() != 2 or coords.shape[0] != 6:
             raise ValueError("coords must have shape (6, n)")
-        if coords.dtype != torch.float64 or not coords.is_cuda:
-            raise ValueError("coords must be a CUDA float64 tensor")
+        if coords.dtype not in _DTYPE_CODE or not coords.is_cuda:
+            raise ValueError("coords must be a CUDA float64 or float32 tensor")
         self.coords = coords.contiguous()
         self.params = params
+
+    @property
+    def dtype(self) -> torch.dtype:
+        return self.coords.dtype
+
+    def astype(self, dtype: torch.dtype) -> "Beam":
+        """A copy of the beam with coordinates of another element type (rounded once)."""
+        return Beam(self.coords.to(dtype), BeamParams(**vars(self.params)))
 
     @property
     def n(self) -> int:
@@ -51,8 +64,9 @@ class Beam:
         return self.n
 
     @classmethod
-    def from_numpy(cls, arr: np.ndarray, params: BeamParams, device="cuda:0") -> "Beam":
-        return cls(torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float64)).to(device), params)
+    def from_numpy(cls, arr: np.ndarray, params: BeamParams, device="cuda:0", dtype=torch.float64) -> "Beam":
+        np_dtype = np.float64 if dtype == torch.float64 else np.float32
+        return cls(torch.from_numpy(np.ascontiguousarray(arr, dtype=np_dtype)).to(device), params)
 
     def numpy(self) -> np.ndarray:
         return self.coords.cpu().numpy()
@@ -60,7 +74,7 @@ class Beam:
     def to_c(self) -> _lib.OctoBeam:
         b = _lib.OctoBeam()
         b.n = self.n
-        b.dtype = 0
+        b.dtype = _DTYPE_CODE[self.coords.dtype]
         for k, name in enumerate(COORDS):
             setattr(b, name, C.c_void_p(self.coords[k].data_ptr()))
         return b
@@ -68,9 +82,11 @@ class Beam:
     @classmethod
     def gaussian(cls, n: int, *, beta: Sequence[float], alpha: Sequence[float] = (0.0, 0.0, 0.0),
                  sigma: Sequence[float], cutoff: float = 5.0, rng_id: int, seed: int = 123456789,
-                 charge=0.0, mc2=0.0, E0=0.0, r0=None, npart=None, device="cuda:0") -> "Beam":
+                 charge=0.0, mc2=0.0, E0=0.0, r0=None, npart=None, device="cuda:0",
+                 dtype=torch.float64) -> "Beam":
         """Seeded counter-RNG Gaussian beam, built on the device like
-        Beam(n, backend, Float64; beta, alpha, sigma, cutoff, rng_id, charge, mc2, E0, r0, npart)."""
+        Beam(n, backend, Float64; beta, alpha, sigma, cutoff, rng_id, charge, mc2, E0, r0, npart).
+        dtype=torch.float32 builds the float64 beam and rounds it once to float32."""
         from .api import _scratch_ctx
         dev = torch.device(device)
         coords = torch.empty((6, int(n)), dtype=torch.float64, device=dev)
@@ -85,4 +101,4 @@ class Beam:
                                            d3(*sigma), float(cutoff), C.c_void_p(stream))
         if rc != _lib.OCTO_OK:
             raise RuntimeError(_lib.last_error(ctx))
-        return beam
+        return beam if dtype == torch.float64 else beam.astype(dtype)
