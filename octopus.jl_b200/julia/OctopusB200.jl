@@ -77,7 +77,7 @@ function _slicing_fields(s::LongitudinalSlicing)
             s.center_position === :centroid ? Int32(0) : Int32(1))
 end
 
-function _options(p::PICPoissonSolver, keep::Vector{Any})
+function _options(p::PICPoissonSolver, keep::Vector{Any}, precision::Integer=0)
     m1, n1, c1 = _slicing_fields(p.slicing1)
     m2, n2, c2 = _slicing_fields(p.slicing2)
     pos1 = Float64.(p.slicing1.positions); pos2 = Float64.(p.slicing2.positions)
@@ -99,15 +99,16 @@ function _options(p::PICPoissonSolver, keep::Vector{Any})
         isempty(pos1) ? Ptr{Float64}(C_NULL) : pointer(pos1), isempty(pos2) ? Ptr{Float64}(C_NULL) : pointer(pos2),
         Int32(p.kbb1 !== nothing), Int32(p.kbb2 !== nothing), Int32(p.luminosity_scale !== nothing),
         p.kbb1 === nothing ? 0.0 : Float64(p.kbb1), p.kbb2 === nothing ? 0.0 : Float64(p.kbb2),
-        p.luminosity_scale === nothing ? 0.0 : Float64(p.luminosity_scale), Int32(0), ntuple(_ -> Int32(0), 7))
+        p.luminosity_scale === nothing ? 0.0 : Float64(p.luminosity_scale), Int32(precision), ntuple(_ -> Int32(0), 7))
 end
 
 """Context: device workspaces and the slice-pair Green cache (the twin of task.runtime_cache)."""
 mutable struct Context
     ptr::Ptr{Cvoid}
-    function Context(p::PICPoissonSolver)
+    # T = Float64: the plain form; T = Float32: the precision form (FP32 particles, planes and FFTs)
+    function Context(p::PICPoissonSolver, ::Type{T}=Float64) where {T<:Union{Float32,Float64}}
         keep = Any[]
-        opts = Ref(_options(p, keep))
+        opts = Ref(_options(p, keep, T === Float32 ? 1 : 0))
         ptr = GC.@preserve keep ccall((:octo_create, LIB), Ptr{Cvoid}, (Int32, Ref{OctoPicOptions}),
                                       Int32(CUDA.device().handle), opts)
         ptr == C_NULL && error("octo_create failed")
@@ -126,14 +127,14 @@ function _last_error(ctx::Context)
     return unsafe_string(pointer(buf))
 end
 
-_octo_beam(b::Beam) = OctoBeam(Int64(length(b.rep.x)), Int32(0), Int32(0),
+_octo_beam(b::Beam) = OctoBeam(Int64(length(b.rep.x)), Int32(eltype(b.rep.x) === Float32 ? 1 : 0), Int32(0),
     pointer(b.rep.x), pointer(b.rep.px), pointer(b.rep.y), pointer(b.rep.py), pointer(b.rep.z), pointer(b.rep.pz))
 _octo_params(b::Beam) = OctoBeamParams(Float64(b.params.charge), Float64(b.params.mc2), Float64(b.params.E0),
                                        Float64(b.params.r0), Float64(b.params.npart))
 
 function _collide!(ctx::Context, solver::B200PICPoissonSolver, beam1::Beam, beam2::Beam, turn::Integer)
-    eltype(beam1.rep.x) === Float64 && eltype(beam2.rep.x) === Float64 || throw(ArgumentError(
-        "the B200 backend's plain form takes Float64 beams"))
+    eltype(beam1.rep.x) === eltype(beam2.rep.x) && eltype(beam1.rep.x) in (Float32, Float64) || throw(ArgumentError(
+        "the B200 backend takes two Float64 (plain form) or two Float32 (precision form) beams"))
     b1 = Ref(_octo_beam(beam1)); b2 = Ref(_octo_beam(beam2))
     p1 = Ref(_octo_params(beam1)); p2 = Ref(_octo_params(beam2))
     lum = Ref(NaN)
@@ -152,7 +153,7 @@ end
 as the reference's public collide! builds a fresh Green cache (pic_cuda.jl:94-126)."""
 function Octopus.collide!(solver::B200PICPoissonSolver, beam1::Beam, beam2::Beam, ::Type{CUDABackend},
                           ctx::Union{Nothing,TrackingContext}=nothing)
-    c = Context(solver.pic)
+    c = Context(solver.pic, eltype(beam1.rep.x))
     try
         return _collide!(c, solver, beam1, beam2, ctx === nothing ? -1 : ctx.turn)
     finally
@@ -164,8 +165,9 @@ end
 function Octopus._strong_strong_collide_backend!(task::StrongStrongTask, label::Symbol,
                                                  solver::B200PICPoissonSolver, beam1::Beam, beam2::Beam,
                                                  ::Type{CUDABackend}, ctx::TrackingContext)
-    key = (:octo_b200_context, label, solver.pic.grid, objectid(solver))
-    c = get!(() -> Context(solver.pic), task.runtime_cache, key)::Context
+    T = eltype(beam1.rep.x)
+    key = (:octo_b200_context, label, T, solver.pic.grid, objectid(solver))
+    c = get!(() -> Context(solver.pic, T), task.runtime_cache, key)::Context
     return _collide!(c, solver, beam1, beam2, ctx.turn)
 end
 
