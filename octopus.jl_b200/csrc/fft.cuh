@@ -1,8 +1,10 @@
-// Shared-memory radix-2 FFT building blocks for the zero-padded Hockney convolution.
+// Shared-memory FFT building blocks for the zero-padded Hockney convolution.
 //
-// One warp transforms one line of length L = 2^lg (L <= 1024) held in shared memory, in FP64
-// (double2) or FP32 (float2) complex arithmetic.
-// Twiddles tw[k] = exp(-2 pi i k / L), k < L/2, are staged in shared memory per block.
+// One warp transforms one line of length L = 2^a or 3 * 2^a (L <= 1024; padded grids of 2^a or 3 * 2^a
+// cells per axis) held in shared memory, in FP64 (double2) or FP32 (float2) complex arithmetic.
+// Twiddles tw[k] = exp(-2 pi i k / L), k < L/2, are staged in shared memory per block.  A line is loaded
+// at fft_pos(i) (bit-reversed; for 3 * 2^a the residue classes i mod 3 as three contiguous bit-reversed
+// sub-lines), and warp_fft() leaves it in natural order.
 // The convolution never materialises the padded (2nx x 2ny) complex plane: rows are
 // transformed two at a time as one complex line (real-input packing), only the nx+1
 // non-redundant x-frequencies are carried through the column pass, and the inverse
@@ -32,8 +34,9 @@ __device__ __forceinline__ int bitrev(int k, int lg) { return (int)(__brev((unsi
 // {i, i+h, i+2h, i+3h}: half the shared-memory round trips and warp syncs of plain radix-2, with the
 // same twiddles (the second-stage twiddle of the odd pair is -i times that of the even pair, applied
 // exactly by a swap and a sign change).  An odd log2(L) starts with one radix-2 pass.
+// tws: twiddle stride, 1 for a table of length L itself, 3 for a sub-line of length L of a 3L table.
 template <class C2>
-__device__ __forceinline__ void warp_fft_passes(C2 *a, int L, const C2 *tw, bool inv) {
+__device__ __forceinline__ void warp_fft_passes(C2 *a, int L, const C2 *tw, bool inv, int tws = 1) {
     const int lane = threadIdx.x & 31;
     __syncwarp();
     int half = 1, step = L >> 1;
@@ -55,8 +58,8 @@ __device__ __forceinline__ void warp_fft_passes(C2 *a, int L, const C2 *tw, bool
         for (int b = lane; b < quads; b += 32) {
             const int j = b & (half - 1);
             const int i0 = ((b & ~(half - 1)) << 2) | j;
-            C2 w1 = tw[j * step];          // W_{2h}^j
-            C2 w2 = tw[j * (step >> 1)];   // W_{4h}^j
+            C2 w1 = tw[j * step * tws];          // W_{2h}^j
+            C2 w2 = tw[j * (step >> 1) * tws];   // W_{4h}^j
             if (inv) { w1.y = -w1.y; w2.y = -w2.y; }
             const C2 x0 = a[i0], x1 = a[i0 + half], x2 = a[i0 + 2 * half], x3 = a[i0 + 3 * half];
             const C2 t1 = cmul(x1, w1), t3 = cmul(x3, w1);
@@ -72,6 +75,69 @@ __device__ __forceinline__ void warp_fft_passes(C2 *a, int L, const C2 *tw, bool
         }
         __syncwarp();
     }
+}
+
+// Line geometry: M = L (power of two) or L / 3.
+struct FftLen {
+    int L, M, lgM, three;
+};
+__device__ __forceinline__ FftLen fft_len(int L) {
+    FftLen f;
+    f.L = L;
+    f.three = (L % 3) == 0;
+    f.M = f.three ? L / 3 : L;
+    f.lgM = 31 - __clz(f.M);
+    return f;
+}
+__device__ __forceinline__ int fft_pos(const FftLen &f, int i) {
+    if (!f.three) return bitrev(i, f.lgM);
+    const int m = i / 3;
+    return (i - 3 * m) * f.M + bitrev(m, f.lgM);
+}
+// W_L^k for 0 <= k < L from the half table (W_L^k = -W_L^(k - L/2)), conjugated for the inverse.
+template <class C2>
+__device__ __forceinline__ C2 twiddle(const C2 *tw, int L, int k, bool inv) {
+    C2 w;
+    if (k < (L >> 1)) w = tw[k];
+    else { w = tw[k - (L >> 1)]; w.x = -w.x; w.y = -w.y; }
+    if (inv) w.y = -w.y;
+    return w;
+}
+
+// Whole-line transform in place: radix-2^2 passes for L = 2^a; for L = 3 * 2^a three length-L/3
+// transforms of the residue classes (decimation in time) and one radix-3 combine,
+// X[k + qM] = Y0[k] + W3^q W^k Y1[k] + W3^2q W^2k Y2[k].
+template <class C2>
+__device__ __forceinline__ void warp_fft(C2 *a, const FftLen &f, const C2 *tw, bool inv) {
+    if (!f.three) {
+        warp_fft_passes(a, f.L, tw, inv);
+        return;
+    }
+    const int M = f.M;
+    warp_fft_passes(a, M, tw, inv, 3);
+    warp_fft_passes(a + M, M, tw, inv, 3);
+    warp_fft_passes(a + 2 * M, M, tw, inv, 3);
+    __syncwarp();
+    using R = decltype(a[0].x);
+    const R h = R(0.5), s3 = R(0.86602540378443864676);  // sin(2 pi / 3)
+    for (int k = (threadIdx.x & 31); k < M; k += 32) {
+        const C2 y0 = a[k];
+        const C2 z1 = cmul(a[M + k], twiddle(tw, f.L, k, inv));
+        const C2 z2 = cmul(a[2 * M + k], twiddle(tw, f.L, 2 * k, inv));
+        const C2 t = cadd(z1, z2), d = csub(z1, z2);
+        C2 m, x0, x1, x2;
+        m.x = y0.x - h * t.x;
+        m.y = y0.y - h * t.y;
+        // forward: X1 = m - i s3 d, X2 = m + i s3 d (the inverse swaps them)
+        const R ux = s3 * d.y, uy = -(s3 * d.x);  // -i s3 d
+        x0 = cadd(y0, t);
+        x1.x = m.x + (inv ? -ux : ux); x1.y = m.y + (inv ? -uy : uy);
+        x2.x = m.x - (inv ? -ux : ux); x2.y = m.y - (inv ? -uy : uy);
+        a[k] = x0;
+        a[M + k] = x1;
+        a[2 * M + k] = x2;
+    }
+    __syncwarp();
 }
 
 // Stage the twiddle table of length L/2 into shared memory (block-wide).

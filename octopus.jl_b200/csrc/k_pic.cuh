@@ -285,7 +285,7 @@ constexpr int kGreenRows = 8;
 __global__ void __launch_bounds__(128) k_green_rows(Collide C, int mode, int base, int node_slot0) {
     double2 *sm = (double2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx, NY = 2 * ny;
-    const int lgx = 31 - __clz(NX);
+    const FftLen fx = fft_len(NX);
     double2 *tw = sm;
     double2 *lines = sm + NX / 2;
     double *corner = (double *)(lines + 4 * NX);  // (kGreenRows + 1) x (NX + 1)
@@ -341,12 +341,12 @@ __global__ void __launch_bounds__(128) k_green_rows(Collide C, int mode, int bas
                     g[q] = green_value(C.o.green_type, i, j0 + r, nx, ny, dx0, dy0, hx, hy);
                 }
             }
-            line[bitrev(i, lgx)] = make_double2(g[0], g[1]);
+            line[fft_pos(fx, i)] = make_double2(g[0], g[1]);
         }
-        warp_fft_passes(line, NX, tw, false);
+        warp_fft(line, fx, tw, false);
         const int ja = j0 + r0, jb = ja + 1;
         for (int k = lane; k <= nx; k += 32) {
-            double2 zk = line[k], zm = conjg(line[(NX - k) & (NX - 1)]);
+            double2 zk = line[k], zm = conjg(line[(NX - k) % NX]);
             double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y + zm.y));
             double2 D = csub(zk, zm);
             out[(long long)k * NY + ja] = A;
@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(128) k_green_rows(Collide C, int mode, int bas
 __global__ void __launch_bounds__(128) k_green_cols(Collide C, int mode, int base, int node_slot0) {
     double2 *sm = (double2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NY = 2 * ny;
-    int lgy = 31 - __clz(NY);
+    const FftLen fy = fft_len(NY);
     double2 *tw = sm;
     double2 *line = sm + NY / 2 + (threadIdx.x >> 5) * NY;
     int slot;
@@ -378,8 +378,8 @@ __global__ void __launch_bounds__(128) k_green_cols(Collide C, int mode, int bas
     const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (k > nx) return;
     double2 *col = C.ghat + (long long)slot * C.gstride + (long long)k * NY;
-    for (int j = lane; j < NY; j += 32) line[bitrev(j, lgy)] = col[j];
-    warp_fft_passes(line, NY, tw, false);
+    for (int j = lane; j < NY; j += 32) line[fft_pos(fy, j)] = col[j];
+    warp_fft(line, fy, tw, false);
     for (int j = lane; j < NY; j += 32) col[j] = line[j];
 }
 
@@ -439,9 +439,12 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
         if (G.green < 0) return;
         sg = G.sg;
     }
-    for (int c = threadIdx.x; c < cells; c += blockDim.x) sq[c] = 0;
+    // grids larger than shared memory (C.o.dep_global) accumulate straight into the plane's grid
+    const bool local = !C.o.dep_global;
+    if (local)
+        for (int c = threadIdx.x; c < cells; c += blockDim.x) sq[c] = 0;
     __syncthreads();
-    long long *acc = generic_ptr(sq);
+    long long *acc = local ? generic_ptr(sq) : C.qgrid + (long long)pl * cells;
     const double hx = sg.w / (double)(nx - 1), hy = sg.h / (double)(ny - 1);
     const R hxi = (R)(1.0 / hx), hyi = (R)(1.0 / hy);
     const R scale = (R)ldexp(1.0, P.fixed_bits);
@@ -463,8 +466,10 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
         for (int o = 16; o; o >>= 1) outside += __shfl_xor_sync(0xffffffffu, outside, o);
         if ((threadIdx.x & 31) == 0 && outside) atomicAdd((unsigned long long *)&C.status->dropped, (unsigned long long)outside);
     }
-    __syncthreads();
-    merge_grid(sq, C.qgrid + (long long)pl * cells, cells);
+    if (local) {
+        __syncthreads();
+        merge_grid(sq, C.qgrid + (long long)pl * cells, cells);
+    }
 }
 
 // Luminosity planes: 2 per pair (side 0 = beam-1 slice i at sM1, side 1 = beam-2 slice j at sM2)
@@ -477,9 +482,11 @@ __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0) {
     const LumGeom &L = C.lumgeom[J.pair];
     if (!L.ok) return;
     const int nw = C.o.lnx + 1, nh = C.o.lny + 1, cells = nw * nh;
-    for (int c = threadIdx.x; c < cells; c += blockDim.x) sq[c] = 0;
+    const bool local = !C.o.lum_global;
+    if (local)
+        for (int c = threadIdx.x; c < cells; c += blockDim.x) sq[c] = 0;
     __syncthreads();
-    long long *acc = generic_ptr(sq);
+    long long *acc = local ? generic_ptr(sq) : C.lq + (long long)blockIdx.y * cells;
     const SoA S = C.beam[side];
     const R *X = col<R>(S, 0), *PX = col<R>(S, 1), *Y = col<R>(S, 2), *PY = col<R>(S, 3);
     const long long st = side ? J.s2_start : J.s1_start, n = side ? J.s2_n : J.s1_n;
@@ -493,8 +500,10 @@ __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0) {
         const R vy = Y[p] + PY[p] * s;
         deposit_taps<R, METHOD>((vx - x0) * hxi, (vy - y0) * hyi, nw, nh, scale, acc, nw);
     }
-    __syncthreads();
-    merge_grid(sq, C.lq + (long long)blockIdx.y * cells, cells);
+    if (local) {
+        __syncthreads();
+        merge_grid(sq, C.lq + (long long)blockIdx.y * cells, cells);
+    }
 }
 
 // Overlap integral per pair: sum q1*q2 over the full (nx+1)(ny+1) extent (pic_cpu.jl:2725-2736),
@@ -554,7 +563,7 @@ __global__ void __launch_bounds__(128) k_conv_rows(Collide C, int plane0) {
     using C2 = typename RealT<R>::C2;
     C2 *sm = (C2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx;
-    const int lgx = 31 - __clz(NX);
+    const FftLen fx = fft_len(NX);
     const int pl = blockIdx.y;
     const Plane &P = C.planes[plane0 + pl];
     if (plane_green(C, P) < 0) return;
@@ -588,12 +597,12 @@ __global__ void __launch_bounds__(128) k_conv_rows(Collide C, int plane0) {
                 if (!kPrecision && qb) q[(long long)j1 * nx + i] = 0;
             }
         }
-        line[bitrev(i, lgx)] = v;
+        line[fft_pos(fx, i)] = v;
     }
-    warp_fft_passes(line, NX, tw, false);
+    warp_fft(line, fx, tw, false);
     C2 *H = (C2 *)C.spec + (long long)pl * (nx + 1) * ny;
     for (int k = lane; k <= nx; k += 32) {
-        C2 zk = line[k], zm = conjg(line[(NX - k) & (NX - 1)]);
+        C2 zk = line[k], zm = conjg(line[(NX - k) % NX]);
         C2 A, B;
         A.x = R(0.5) * (zk.x + zm.x);
         A.y = R(0.5) * (zk.y + zm.y);
@@ -606,19 +615,21 @@ __global__ void __launch_bounds__(128) k_conv_rows(Collide C, int plane0) {
 }
 
 // y-transform, multiply by the (FP64) Green spectrum, inverse y-transform; one frequency column per
-// warp, in place.  Only rows j < ny of the result are kept (the field quadrant).
+// warp.  Only rows j < ny of the result are kept (the field quadrant).  The inverse input is permuted in
+// place for NY = 2^a (bit reversal is an involution) and through a second line for NY = 3 * 2^a.
 template <class R>
 __global__ void __launch_bounds__(128) k_conv_cols(Collide C, int plane0) {
     using C2 = typename RealT<R>::C2;
     C2 *sm = (C2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NY = 2 * ny;
-    const int lgy = 31 - __clz(NY);
+    const FftLen fy = fft_len(NY);
     const int pl = blockIdx.y;
     const Plane &P = C.planes[plane0 + pl];
     const int slot = plane_green(C, P);
     if (slot < 0) return;
     C2 *tw = sm;
     C2 *line = sm + NY / 2 + (threadIdx.x >> 5) * NY;
+    C2 *line2 = sm + NY / 2 + (4 + (threadIdx.x >> 5)) * NY;  // NY = 3 * 2^a only
     load_twiddles(tw, (const C2 *)C.twr_y, NY);
     __syncthreads();
     const int lane = threadIdx.x & 31;
@@ -628,23 +639,28 @@ __global__ void __launch_bounds__(128) k_conv_cols(Collide C, int plane0) {
     C2 zero;
     zero.x = R(0);
     zero.y = R(0);
-    for (int j = lane; j < NY; j += 32) line[bitrev(j, lgy)] = j < ny ? col[j] : zero;
-    warp_fft_passes(line, NY, tw, false);
+    for (int j = lane; j < NY; j += 32) line[fft_pos(fy, j)] = j < ny ? col[j] : zero;
+    warp_fft(line, fy, tw, false);
     const double2 *g = C.ghat + (long long)slot * C.gstride + (long long)k * NY;
+    C2 *dst = fy.three ? line2 : line;
     for (int j = lane; j < NY; j += 32) {
         const double2 gv = g[j];
         C2 gg;
         gg.x = (R)gv.x;
         gg.y = (R)gv.y;
-        line[j] = cmul(line[j], gg);
+        const C2 v = cmul(line[j], gg);
+        if (fy.three) dst[fft_pos(fy, j)] = v;
+        else line[j] = v;
     }
     __syncwarp();
-    for (int j = lane; j < NY; j += 32) {  // bit-reverse permutation in place
-        int r = bitrev(j, lgy);
-        if (j < r) { C2 t = line[j]; line[j] = line[r]; line[r] = t; }
+    if (!fy.three) {
+        for (int j = lane; j < NY; j += 32) {  // bit-reverse permutation in place
+            int r = bitrev(j, fy.lgM);
+            if (j < r) { C2 t = line[j]; line[j] = line[r]; line[r] = t; }
+        }
     }
-    warp_fft_passes(line, NY, tw, true);
-    for (int j = lane; j < ny; j += 32) col[j] = line[j];
+    warp_fft(dst, fy, tw, true);
+    for (int j = lane; j < ny; j += 32) col[j] = dst[j];
 }
 
 // Field planes: a cell is (phi, Ex), (Ey, 0) as two double2 (plain form) or one float4 (precision
@@ -676,7 +692,7 @@ __global__ void __launch_bounds__(128) k_conv_field(Collide C, int plane0) {
     using FC = typename RealT<R>::FC;
     C2 *sm = (C2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx, NY = 2 * ny;
-    const int lgx = 31 - __clz(NX);
+    const FftLen fx = fft_len(NX);
     const int pl = blockIdx.y;
     const Plane &P = C.planes[plane0 + pl];
     if (plane_green(C, P) < 0) return;
@@ -714,9 +730,9 @@ __global__ void __launch_bounds__(128) k_conv_field(Collide C, int plane0) {
             C2 v;
             v.x = ca.x - cb.y;
             v.y = ca.y + cb.x;
-            line[bitrev(k, lgx)] = v;
+            line[fft_pos(fx, k)] = v;
         }
-        warp_fft_passes(line, NX, tw, true);
+        warp_fft(line, fx, tw, true);
         for (int i = lane; i < nx; i += 32) {
             phi[(ra - ja0) * nx + i] = line[i].x * scale;
             if (hb) phi[(rb - ja0) * nx + i] = line[i].y * scale;
@@ -937,7 +953,7 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
 }
 
 template <class R, int METHOD>
-__global__ void __launch_bounds__(kKickThreads) k_kick(Collide C, int plane0_front, const int2 *blockmap) {
+__global__ void __launch_bounds__(kKickThreads, sizeof(R) == 8 ? 1 : 4) k_kick(Collide C, int plane0_front, const int2 *blockmap) {
     __shared__ KickJob<R> J;
     if (threadIdx.x == 0) {
         const int2 bm = blockmap[blockIdx.x];

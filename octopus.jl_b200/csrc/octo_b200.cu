@@ -265,11 +265,13 @@ void harvest_timing(octo_ctx *c) {
 void set_error(octo_ctx *c, const std::string &m) { c->err = m; }
 
 bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+// Grid sizes the shared-memory FFTs take: 2^a or 3 * 2^a cells per axis (padded lines 2^(a+1), 3 * 2^(a+1)).
+bool fft_size_ok(int v) { return is_pow2(v) || (v % 3 == 0 && is_pow2(v / 3)); }
 
 int validate_options(const octo_pic_options &o, std::string &msg) {
     if (o.nx < 5 || o.ny < 5) { msg = "PICPoissonSolver grid must be at least (5, 5)"; return OCTO_ERR_ARG; }
-    if (!is_pow2(o.nx) || !is_pow2(o.ny) || o.nx > 512 || o.ny > 512) {
-        msg = "this backend's FFT needs power-of-two grid dimensions <= 512";
+    if (!fft_size_ok(o.nx) || !fft_size_ok(o.ny) || o.nx < 8 || o.ny % 8 != 0 || o.nx > 512 || o.ny > 512) {
+        msg = "this backend's FFT needs grid dimensions of the form 2^a or 3*2^a in 8..512, ny a multiple of 8";
         return OCTO_ERR_UNSUPPORTED;
     }
     if (o.deposit_method != OCTO_CIC && o.deposit_method != OCTO_TSC) { msg = "deposit_method must be :CIC or :TSC"; return OCTO_ERR_ARG; }
@@ -441,7 +443,9 @@ void launch_method(int method, F f) {
 
 // Dynamic shared memory of the FFT kernels for line length L (4 warps per block), complex elements of
 // `real` bytes per component (8 FP64, 4 FP32).
-size_t fft_smem(int L, size_t real = sizeof(double)) { return 2 * real * (size_t)(L / 2 + 4 * L); }
+size_t fft_smem(int L, size_t real = sizeof(double), int lines = 4) { return 2 * real * (size_t)(L / 2 + lines * L); }
+// k_conv_cols: a second line per warp when the padded column length is 3 * 2^a.
+size_t cols_smem(int L, size_t real) { return fft_smem(L, real, L % 3 == 0 ? 8 : 4); }
 // k_green_rows (FP64): twiddles + 4 lines + the (kGreenRows+1) x (NX+1) corner lattice of F.
 size_t green_smem(int NX) { return fft_smem(NX) + sizeof(double) * (size_t)(kGreenRows + 1) * (NX + 1); }
 // k_conv_field: twiddles (NX/2) + 4 lines (4*NX) complex, plus a (tile+4) x nx phi tile; NX = 2*nx.
@@ -794,8 +798,8 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
     C.lum_partial = c->lum_partial.p;
     C.nodes = c->nodes.p;
 
-    const size_t dep_bytes = cells * sizeof(long long);
-    const size_t lum_bytes = lcells * sizeof(long long);
+    const size_t dep_bytes = c->dopt.dep_global ? 0 : cells * sizeof(long long);
+    const size_t lum_bytes = c->dopt.lum_global ? 0 : lcells * sizeof(long long);
 
     // ---- wavefronts
     for (const Front &F : fronts) {
@@ -852,7 +856,7 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
                 k_conv_rows<R><<<dim3((ny / 2 + 3) / 4, F.np), 128, fft_smem(NX, rsz), st>>>(C, F.p0);
                 if (fp32)  // the precision form reads partner grids, so the front's grids are cleared here
                     CK(cudaMemsetAsync(c->qgrid.p, 0, sizeof(long long) * cells * F.np, st));
-                k_conv_cols<R><<<dim3((nx + 1 + 3) / 4, F.np), 128, fft_smem(NY, rsz), st>>>(C, F.p0);
+                k_conv_cols<R><<<dim3((nx + 1 + 3) / 4, F.np), 128, cols_smem(NY, rsz), st>>>(C, F.p0);
             });
         }
         {
@@ -1022,11 +1026,13 @@ octo_ctx *octo_create(int32_t device, const octo_pic_options *options) {
             c->bw[b].q.ensure(kMaxSlices + 1);
             CK(cudaMemcpy(c->bw[b].q.p, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice));
         }
+        // Charge grids up to 227 KB (168 x 168 int64 cells) accumulate in shared memory; larger ones go
+        // straight to the plane's grid with global atomics.
         size_t dep = (size_t)options->nx * options->ny * sizeof(long long);
         size_t lum = (size_t)(d.lnx + 1) * (d.lny + 1) * sizeof(long long);
-        if (dep > kSmemLimit || lum > kSmemLimit)
-            throw CudaFail{"grid too large for the shared-memory deposit (at most 168 x 168 cells on this backend)"};
-        int dsm = (int)dep, lsm = (int)lum;
+        d.dep_global = dep > kSmemLimit;
+        d.lum_global = lum > kSmemLimit;
+        int dsm = d.dep_global ? 0 : (int)dep, lsm = d.lum_global ? 0 : (int)lum;
         CK(cudaFuncSetAttribute(k_green_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)green_smem(2 * options->nx)));
         CK(cudaFuncSetAttribute(k_green_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(2 * options->ny)));
         with_real(c->fp32, [&](auto r) {
@@ -1037,7 +1043,7 @@ octo_ctx *octo_create(int32_t device, const octo_pic_options *options) {
             CK(cudaFuncSetAttribute(k_lum_deposit<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
             CK(cudaFuncSetAttribute(k_lum_deposit<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
             CK(cudaFuncSetAttribute(k_conv_rows<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(2 * options->nx, rs)));
-            CK(cudaFuncSetAttribute(k_conv_cols<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(2 * options->ny, rs)));
+            CK(cudaFuncSetAttribute(k_conv_cols<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cols_smem(2 * options->ny, rs)));
             CK(cudaFuncSetAttribute(k_conv_field<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)field_smem(2 * options->nx, rs)));
         });
     } catch (CudaFail &e) {

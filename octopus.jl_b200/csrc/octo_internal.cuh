@@ -219,6 +219,7 @@ inline int fixed_bits_for(int64_t n) {
 struct DevOptions {
     int nx, ny, method, lum_method, lnx, lny;
     int green_type, green_cache, fourth, quadratic, node, longitudinal_kick;
+    int dep_global, lum_global;  // charge / luminosity grid larger than shared memory: global atomics
     double min_ex, min_ey, quantize, min_ratio, growth;
 };
 

@@ -202,6 +202,9 @@ def _require_gpu_options(s: PICPoissonSolver):
                                 ":normal_quantile (the production method) or :specified.")
         if sl.nslices > 64:
             raise ArgumentError("the GPU PIC backend supports at most 64 slices per beam")
-    for n in s.grid:
-        if n & (n - 1) or n > 512:
-            raise ArgumentError(f"the GPU PIC backend's FFT needs power-of-two grid dimensions <= 512; got {s.grid}")
+    def fft_ok(n):
+        m = n // 3 if n % 3 == 0 else n
+        return m & (m - 1) == 0 and 8 <= n <= 512
+    if not all(fft_ok(n) for n in s.grid) or s.grid[1] % 8:
+        raise ArgumentError("the GPU PIC backend's FFT needs grid dimensions of the form 2^a or 3*2^a in 8..512, "
+                            f"ny a multiple of 8; got {s.grid}")

@@ -134,3 +134,19 @@ def test_nonfinite_input_reports_location(grid_mode, row, role):
     be2, bp2 = _device_beams(ob, e2, p2)
     assert np.isfinite(ctx.collide(be2, bp2, turn=8))
     rt.close()
+
+
+@pytest.mark.parametrize("grid", [(48, 48), (96, 64), (64, 96), (192, 192), (256, 256)])
+def test_grid_sizes(grid):
+    """Grids of the batched scan and the hybrid: 3*2^a sizes (mixed radix-3 FFT lines of 96, 192, 384) and
+    grids whose int64 plane exceeds shared memory (192^2, 256^2: global-memory deposition)."""
+    ob = _gpu()
+    s = ob.PICPoissonSolver(grid=grid, slicing=ob.LongitudinalSlicing(nslices=4, method="normal_quantile"))
+    check(run_both(s, 8000, 6000, turns=2))
+
+
+def test_node_mode_96():
+    ob = _gpu()
+    s = ob.PICPoissonSolver(grid=(96, 96), interaction_grid="node", deposit_method="TSC",
+                            slicing=ob.LongitudinalSlicing(nslices=5, method="normal_quantile"))
+    check(run_both(s, 12000, 8000, turns=2, e_sigma=(95e-6, 8.5e-6, 0.7e-2), p_sigma=(95e-6, 8.5e-6, 6e-2)))
