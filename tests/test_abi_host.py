@@ -95,10 +95,12 @@ def test_solver_defaults_and_validation():
 def test_gpu_backend_rejects_what_it_does_not_implement():
     sl = ob.LongitudinalSlicing(nslices=3, method="normal_quantile")
     for kw in (dict(interaction_grid="source_slice"), dict(grid_extent="sigma"), dict(green_type="lattice"),
-               dict(grid=(96, 96))):
+               dict(grid=(80, 80)), dict(grid=(96, 36)), dict(grid=(1024, 64))):
         with pytest.raises(ob.ArgumentError):
             ob.PICPoissonSolver(slicing=sl, **kw).to_c()
     with pytest.raises(ob.ArgumentError):
         ob.PICPoissonSolver(slicing=ob.LongitudinalSlicing(nslices=3, method="equal_area")).to_c()
+    for g in ((48, 48), (96, 64), (384, 192), (512, 512)):  # 2^a and 3*2^a FFT lines
+        assert ob.PICPoissonSolver(slicing=sl, grid=g).to_c().nx == g[0]
     o = ob.PICPoissonSolver(slicing=sl, deposit_method="TSC", field_derivative="fourth").to_c()
     assert (o.nx, o.deposit_method, o.field_derivative, o.nslices1) == (128, 1, 4, 3)
