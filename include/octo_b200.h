@@ -118,6 +118,18 @@ int32_t octo_pic_collide(octo_ctx *ctx, octo_beam *beam1, octo_beam *beam2, cons
                          const octo_beam_params *p2, int64_t turn, int32_t compute_luminosity,
                          double *luminosity, octo_collide_report *report, void *stream);
 
+/* A batch of independent collides (one per context, e.g. the collision points of a lattice or the cases
+ * of a parameter scan), each on its own stream: the slicing of every collide is enqueued first, then each
+ * collide's schedule is built and its wavefronts enqueued while the earlier ones run, then all are
+ * finished.  Same results as `count` octo_pic_collide calls (the reference runs its collision points
+ * one after another in the turn loop, interface.jl:2499-2501).  status[k] receives each collide's
+ * code; the return value is OCTO_OK or the first failing code.  Contexts must be distinct; streams
+ * should be distinct for the collides to overlap.  luminosity, reports and status may be NULL. */
+int32_t octo_pic_collide_batch(int32_t count, octo_ctx *const *ctx, octo_beam *const *beam1, octo_beam *const *beam2,
+                               const octo_beam_params *const *p1, const octo_beam_params *const *p2, int64_t turn,
+                               int32_t compute_luminosity, double *luminosity, octo_collide_report *reports,
+                               int32_t *status, void *const *streams);
+
 /* Green-cache counters (the contract of Contracts.jl:947-960). */
 int32_t octo_green_cache_stats(octo_ctx *ctx, int64_t *hits, int64_t *misses, int64_t *rebuilds);
 

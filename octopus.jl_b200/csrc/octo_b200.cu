@@ -163,7 +163,6 @@ struct BeamWS {
     DevBuf<double> lane_sum, lane_min, lane_max, lanes, q;
     DevBuf<int> counts;
     DevBuf<long long> blockoff;
-    SliceInfo host;
     long long total = 0;
     void release() {
         for (auto &b : s) b.release();
@@ -206,6 +205,7 @@ struct octo_ctx {
     PinBuf<double> h_lum;
     PinBuf<DevStatus> h_status;
     PinBuf<double> h_noderef;
+    PinBuf<SliceInfo> h_slices;
     long long gstride = 0;
     int nslots = 0;
     int cache_ready = 0;
@@ -454,6 +454,26 @@ size_t field_smem(int NX, size_t real = sizeof(double)) {
 }
 constexpr size_t kSmemLimit = 227 * 1024;
 
+// Raise the dynamic shared-memory limit of every kernel launched with more than 48 KB to the B200 opt-in
+// maximum (the attribute only permits; occupancy follows the size each launch asks for).
+void set_smem_limits() {
+    const int lim = (int)kSmemLimit;
+    CK(cudaFuncSetAttribute(k_green_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    CK(cudaFuncSetAttribute(k_green_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    auto per_real = [&](auto r) {
+        using R = decltype(r);
+        CK(cudaFuncSetAttribute(k_deposit<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(k_deposit<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(k_lum_deposit<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(k_lum_deposit<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(k_conv_rows<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(k_conv_cols<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(k_conv_field<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    };
+    per_real(double(0));
+    per_real(float(0));
+}
+
 // Enqueue the node meshes of both directions (pic_cpu.jl:1404-1419) with no host synchronisation: the
 // per-direction drift tables and slice counts are staged in pinned memory owned by the context, and
 // mesh validity is known on the host from the slice counts (node_mesh_valid).
@@ -534,40 +554,73 @@ bool node_mesh_valid(const SliceInfo &SS, const SliceInfo &SF, int nsf, int src0
     return false;
 }
 
-double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_params *p1, const octo_beam_params *p2,
-                    int64_t turn, int compute_lum, octo_collide_report *rep, cudaStream_t st) {
-    const octo_pic_options &o = c->opt;
+// One collide as three stages, so a batch of independent collides can interleave them:
+// begin() validates and enqueues the slicing and the copy of the slice tables to pinned memory; run()
+// waits for those tables, builds the schedule and enqueues every wavefront, the write-back and the copy
+// of the results; finish() waits for the results, reports errors and folds the luminosity.
+struct CollideJob {
+    octo_ctx *c;
+    octo_beam *b1, *b2;
+    const octo_beam_params *p1, *p2;
+    int64_t turn;
+    int compute_lum;
+    octo_collide_report *rep;
+    cudaStream_t st;
     long long launches = 0;
+    bool fp32 = false;
+    size_t rsz = sizeof(double);
+    long long n1 = 0, n2 = 0;
+    double kbb1 = 0, kbb2 = 0, klum = 0;
+    std::vector<OrderEntry> order;
+    std::vector<std::vector<OrderEntry>> batches;
+    std::vector<char> ran;
+    std::vector<Task> tasks;
+    int ntasks = 0, npairs_total = 0;
+    void begin();
+    void run();
+    double finish();
+};
+
+void CollideJob::begin() {
+    const octo_pic_options &o = c->opt;
     std::string msg;
     int rc = check_beam(b1, msg, c->fp32);
     if (rc == OCTO_OK) rc = check_beam(b2, msg, c->fp32);
     if (rc != OCTO_OK) throw OctoFail{rc, msg};
     if (!p1 || !p2) throw OctoFail{OCTO_ERR_ARG, "beam params pointer is NULL"};
-    const bool fp32 = c->fp32 != 0;
-    const size_t rsz = fp32 ? sizeof(float) : sizeof(double);
+    fp32 = c->fp32 != 0;
+    rsz = fp32 ? sizeof(float) : sizeof(double);
     CK(cudaSetDevice(c->device));
     // kbb and luminosity scale (slicing.jl:77-91, pic_cpu.jl:821-829)
     if (!o.has_kbb1 && !(std::isfinite(p1->E0) && p1->E0 != 0))
         throw OctoFail{OCTO_ERR_ARG, "beam1 E0 must be finite and nonzero when kbb1 is not specified"};
     if (!o.has_kbb2 && !(std::isfinite(p2->E0) && p2->E0 != 0))
         throw OctoFail{OCTO_ERR_ARG, "beam2 E0 must be finite and nonzero when kbb2 is not specified"};
-    const long long n1 = b1->n, n2 = b2->n;
+    n1 = b1->n;
+    n2 = b2->n;
     const double kbb1p = o.has_kbb1 ? o.kbb1 : p1->charge * p2->charge * p1->r0 * p2->npart * p1->mc2 / p1->E0;
     const double kbb2p = o.has_kbb2 ? o.kbb2 : p1->charge * p2->charge * p2->r0 * p1->npart * p2->mc2 / p2->E0;
-    const double kbb1 = kbb1p / (double)n2, kbb2 = kbb2p / (double)n1;
-    const double klum = o.has_lum_scale ? o.lum_scale : p1->npart * p2->npart / (double)(n1 * n2);
+    kbb1 = kbb1p / (double)n2;
+    kbb2 = kbb2p / (double)n1;
+    klum = o.has_lum_scale ? o.lum_scale : p1->npart * p2->npart / (double)(n1 * n2);
 
-    // ---- slicing (one readback of the slice tables)
+    // ---- slicing (one readback of the slice tables, into pinned memory so the copy is asynchronous)
     {
         PhaseScope ps(c, OCTO_PHASE_SLICING, st, 20);
         slice_beam(c, 0, *b1, st, launches);
         slice_beam(c, 1, *b2, st, launches);
     }
-    CK(cudaMemcpyAsync(&c->bw[0].host, c->bw[0].info.p, sizeof(SliceInfo), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&c->bw[1].host, c->bw[1].info.p, sizeof(SliceInfo), cudaMemcpyDeviceToHost, st));
+    c->h_slices.ensure(2);
+    CK(cudaMemcpyAsync(c->h_slices.p + 0, c->bw[0].info.p, sizeof(SliceInfo), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(c->h_slices.p + 1, c->bw[1].info.p, sizeof(SliceInfo), cudaMemcpyDeviceToHost, st));
+}
+
+void CollideJob::run() {
+    const octo_pic_options &o = c->opt;
+    CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(st));
     for (int b = 0; b < 2; ++b) {
-        if (c->bw[b].host.nonfinite) {
+        if (c->h_slices.p[b].nonfinite) {
             long long first = first_nonfinite_host(b == 0 ? *b1 : *b2, st, true);
             if (rep) { rep->role = 3; rep->first_index = first + 1; }
             char m[192];
@@ -576,7 +629,7 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
             throw OctoFail{OCTO_ERR_NONFINITE, m};
         }
     }
-    const SliceInfo S1 = c->bw[0].host, S2 = c->bw[1].host;
+    const SliceInfo S1 = c->h_slices.p[0], S2 = c->h_slices.p[1];
     const int ns1 = c->ns[0], ns2 = c->ns[1];
     const int nx = o.nx, ny = o.ny, NX = 2 * nx, NY = 2 * ny;
     const int lnx = c->dopt.lnx, lny = c->dopt.lny;
@@ -619,8 +672,8 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
     C.ghat = c->ghat.p;
 
     // ---- schedule (slicing.jl:561-647), skipping pairs with an empty slice (pic_cpu.jl:302)
-    auto order = collision_order(S1.center, ns1, S2.center, ns2);
-    auto batches = pair_batches(order, ns1, ns2);
+    order = collision_order(S1.center, ns1, S2.center, ns2);
+    batches = pair_batches(order, ns1, ns2);
     std::vector<int> pos_of((size_t)ns1 * ns2);
     for (size_t p = 0; p < order.size(); ++p) pos_of[(size_t)(order[p].i - 1) * ns2 + (order[p].j - 1)] = (int)p;
 
@@ -637,14 +690,13 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
         return dir == 1 ? src_slice0 * (ns2 + 1) + (node1 - 1) : ns1 * (ns2 + 1) + src_slice0 * (ns1 + 1) + (node1 - 1);
     };
 
-    std::vector<Task> tasks;
     std::vector<Plane> planes;
     std::vector<LumJob> lumjobs;
     std::vector<int2> blockmap;
     struct Front { int t0, nt, p0, np, l0, nl, b0, nb; long long maxsrc, maxlum; };
     std::vector<Front> fronts;
     const int nplanes_task = node ? (lk ? 3 : 2) : (quad ? 3 : 2);
-    std::vector<char> ran(order.size(), 0);
+    ran.assign(order.size(), 0);
     for (size_t f = 0; f < batches.size(); ++f) {
         Front F{(int)tasks.size(), 0, (int)planes.size(), 0, (int)lumjobs.size(), 0, (int)blockmap.size(), 0, 1, 1};
         for (const OrderEntry &pr : batches[f]) {
@@ -735,8 +787,8 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
         F.nb = (int)blockmap.size() - F.b0;
         if (F.nt) fronts.push_back(F);
     }
-    const int ntasks = (int)tasks.size();
-    const int npairs_total = (int)order.size();
+    ntasks = (int)tasks.size();
+    npairs_total = (int)order.size();
     int max_planes = 1, max_lum = 1;
     for (auto &F : fronts) { max_planes = std::max(max_planes, F.np); max_lum = std::max(max_lum, F.nl); }
 
@@ -897,6 +949,10 @@ double collide_impl(octo_ctx *c, octo_beam *b1, octo_beam *b2, const octo_beam_p
     c->h_status.ensure(1);
     CK(cudaMemcpyAsync(c->h_lum.p, c->lum_parts.p, sizeof(double) * npairs_total, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(c->h_status.p, c->status.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+}
+
+double CollideJob::finish() {
+    CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(st));
     CK(cudaGetLastError());
     harvest_timing(c);
@@ -1032,20 +1088,10 @@ octo_ctx *octo_create(int32_t device, const octo_pic_options *options) {
         size_t lum = (size_t)(d.lnx + 1) * (d.lny + 1) * sizeof(long long);
         d.dep_global = dep > kSmemLimit;
         d.lum_global = lum > kSmemLimit;
-        int dsm = d.dep_global ? 0 : (int)dep, lsm = d.lum_global ? 0 : (int)lum;
-        CK(cudaFuncSetAttribute(k_green_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)green_smem(2 * options->nx)));
-        CK(cudaFuncSetAttribute(k_green_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(2 * options->ny)));
-        with_real(c->fp32, [&](auto r) {
-            using R = decltype(r);
-            const size_t rs = sizeof(R);
-            CK(cudaFuncSetAttribute(k_deposit<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
-            CK(cudaFuncSetAttribute(k_deposit<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm));
-            CK(cudaFuncSetAttribute(k_lum_deposit<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
-            CK(cudaFuncSetAttribute(k_lum_deposit<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lsm));
-            CK(cudaFuncSetAttribute(k_conv_rows<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(2 * options->nx, rs)));
-            CK(cudaFuncSetAttribute(k_conv_cols<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cols_smem(2 * options->ny, rs)));
-            CK(cudaFuncSetAttribute(k_conv_field<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)field_smem(2 * options->nx, rs)));
-        });
+        // The dynamic shared-memory limit is a per-kernel attribute shared by every context in the
+        // process, so it is raised to the opt-in maximum once rather than to this context's sizes (a later
+        // context with smaller grids must not cap an earlier one's launches).
+        set_smem_limits();
     } catch (CudaFail &e) {
         c->err = e.msg;
         c->opt.nx = 0;
@@ -1064,7 +1110,7 @@ void octo_destroy(octo_ctx *c) {
     c->nodenan.release(); c->status.release(); c->ghat.release(); c->qgrid.release(); c->lq.release();
     c->spec.release(); c->fields.release(); c->lum_parts.release(); c->lum_partial.release(); c->node_ref.release(); c->stats.release();
     c->partial.release(); c->soa_ptrs.release();
-    c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_noderef.release();
+    c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_noderef.release(); c->h_slices.release();
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     delete c;
 }
@@ -1076,7 +1122,10 @@ int32_t octo_pic_collide(octo_ctx *c, octo_beam *beam1, octo_beam *beam2, const 
     if (report) { std::memset(report, 0, sizeof(*report)); report->turn = turn; }
     if (c->opt.nx == 0) return fail(c, OCTO_ERR_UNSUPPORTED, c->err.empty() ? "invalid context" : c->err);
     try {
-        double lum = collide_impl(c, beam1, beam2, p1, p2, turn, compute_luminosity, report, (cudaStream_t)stream);
+        CollideJob job{c, beam1, beam2, p1, p2, turn, compute_luminosity, report, (cudaStream_t)stream};
+        job.begin();
+        job.run();
+        double lum = job.finish();
         if (luminosity) *luminosity = lum;
         c->err.clear();
         if (report) report->status = OCTO_OK;
@@ -1088,6 +1137,56 @@ int32_t octo_pic_collide(octo_ctx *c, octo_beam *beam1, octo_beam *beam2, const 
         if (report) report->status = OCTO_ERR_CUDA;
         return fail(c, OCTO_ERR_CUDA, e.msg);
     }
+}
+
+int32_t octo_pic_collide_batch(int32_t count, octo_ctx *const *ctxs, octo_beam *const *beam1, octo_beam *const *beam2,
+                               const octo_beam_params *const *p1, const octo_beam_params *const *p2, int64_t turn,
+                               int32_t compute_luminosity, double *luminosity, octo_collide_report *reports,
+                               int32_t *status, void *const *streams) {
+    if (count < 0 || (count > 0 && (!ctxs || !beam1 || !beam2 || !p1 || !p2))) return OCTO_ERR_ARG;
+    for (int k = 0; k < count; ++k) {
+        if (!ctxs[k]) return OCTO_ERR_ARG;
+        for (int m = 0; m < k; ++m)
+            if (ctxs[m] == ctxs[k]) return fail(ctxs[k], OCTO_ERR_ARG, "a batch needs a distinct context per collide");
+    }
+    std::vector<CollideJob> jobs;
+    std::vector<int32_t> rc(count, OCTO_OK);
+    jobs.reserve(count);
+    for (int k = 0; k < count; ++k) {
+        octo_collide_report *r = reports ? reports + k : nullptr;
+        if (r) { std::memset(r, 0, sizeof(*r)); r->turn = turn; }
+        jobs.push_back(CollideJob{ctxs[k], beam1[k], beam2[k], p1[k], p2[k], turn, compute_luminosity, r,
+                                  streams ? (cudaStream_t)streams[k] : (cudaStream_t)0});
+        if (luminosity) luminosity[k] = NAN;
+        if (ctxs[k]->opt.nx == 0) rc[k] = fail(ctxs[k], OCTO_ERR_UNSUPPORTED, ctxs[k]->err.empty() ? "invalid context" : ctxs[k]->err);
+    }
+    // Each stage of each collide runs under its own error handler, so one failing collide leaves the
+    // others of the batch to complete.
+    auto stage = [&](int k, int which) {
+        if (rc[k] != OCTO_OK) return;
+        try {
+            if (which == 0) jobs[k].begin();
+            else if (which == 1) jobs[k].run();
+            else {
+                const double lum = jobs[k].finish();
+                if (luminosity) luminosity[k] = lum;
+                jobs[k].c->err.clear();
+            }
+        } catch (OctoFail &e) {
+            rc[k] = fail(jobs[k].c, e.code, e.msg);
+        } catch (CudaFail &e) {
+            rc[k] = fail(jobs[k].c, OCTO_ERR_CUDA, e.msg);
+        }
+    };
+    for (int which = 0; which < 3; ++which)
+        for (int k = 0; k < count; ++k) stage(k, which);
+    int32_t first = OCTO_OK;
+    for (int k = 0; k < count; ++k) {
+        if (reports) reports[k].status = rc[k];
+        if (status) status[k] = rc[k];
+        if (first == OCTO_OK) first = rc[k];
+    }
+    return first;
 }
 
 int32_t octo_green_cache_stats(octo_ctx *c, int64_t *hits, int64_t *misses, int64_t *rebuilds) {

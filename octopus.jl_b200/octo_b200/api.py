@@ -165,6 +165,46 @@ def collide(solver: PICPoissonSolver, beam1: Beam, beam2: Beam, backend=CUDABack
                                                                        compute_luminosity=lum_on)
 
 
+def collide_batch(contexts, beams1, beams2, turn: int = -1, compute_luminosity: bool = True, streams=None):
+    """Independent collides, one per context, overlapped on their own streams (octo_pic_collide_batch):
+    the parameter-scan and multi-collision-point form of collide!.  Returns the luminosities; raises
+    CollisionError for the first failing collide after all of them have run."""
+    n = len(contexts)
+    if not (len(beams1) == len(beams2) == n):
+        raise ArgumentError("collide_batch needs one beam pair per context")
+    if streams is None:
+        streams = [torch.cuda.Stream(device=b.coords.device) for b in beams1]
+    cb1 = [b.to_c() for b in beams1]
+    cb2 = [b.to_c() for b in beams2]
+    cp1 = [b.params.to_c() for b in beams1]
+    cp2 = [b.params.to_c() for b in beams2]
+    P = C.POINTER
+    arr = lambda T, items: (T * max(n, 1))(*items)
+    ctxs = arr(C.c_void_p, [c.ptr for c in contexts])
+    a1 = arr(P(_lib.OctoBeam), [C.pointer(b) for b in cb1])
+    a2 = arr(P(_lib.OctoBeam), [C.pointer(b) for b in cb2])
+    q1 = arr(P(_lib.OctoBeamParams), [C.pointer(p) for p in cp1])
+    q2 = arr(P(_lib.OctoBeamParams), [C.pointer(p) for p in cp2])
+    lum = (C.c_double * max(n, 1))()
+    reps = (_lib.OctoCollideReport * max(n, 1))()
+    status = (C.c_int32 * max(n, 1))()
+    sts = arr(C.c_void_p, [s.cuda_stream for s in streams])
+    # the caller's current stream work on the beams precedes the batch's streams
+    for s, b in zip(streams, beams1):
+        s.wait_stream(torch.cuda.current_stream(b.coords.device))
+    rc = _lib.lib().octo_pic_collide_batch(n, ctxs, a1, a2, q1, q2, int(turn), int(bool(compute_luminosity)), lum, reps,
+                                           status, sts)
+    for c, r in zip(contexts, reps):
+        c.last_report = r
+    for b, s in zip(beams1, streams):
+        torch.cuda.current_stream(b.coords.device).wait_stream(s)
+    if rc != _lib.OCTO_OK:
+        k = next(i for i in range(n) if status[i] != _lib.OCTO_OK)
+        raise CollisionError(rc, f"collide {k}: {_lib.ERROR_NAMES.get(rc, rc)}: {_lib.last_error(contexts[k].ptr)}",
+                             reps[k])
+    return [lum[k] for k in range(n)]
+
+
 _scratch: Dict[int, int] = {}
 
 
