@@ -11,6 +11,7 @@
 // FFT is this file's own (the reference calls FFTW 3.3.12), so field values
 // agree with the reference to rounding, not bitwise.
 #include "oracle.h"
+#include "oracle_be.hpp"
 
 #include <algorithm>
 #include <array>
@@ -999,6 +1000,219 @@ void interaction(Ctx &C, Workspace &ws, const Coords &source, const SliceParam &
 }
 
 // pic_cpu.jl:1448-1538
+// ---------------------------------------------------------------- Gaussian-subtracted hybrid
+// GaussianPICPoissonSolver (gaussian_pic.jl), default uncoupled subtraction (coupling_tol = Inf).
+
+// Node-centred erf-integrated profile of a unit 1D Gaussian against the CIC / TSC assignment function
+// (gaussian_pic.jl:206-237); node i sits at x0 + i h.
+void gaussian_profile(int method, double x0, double h, double mu, double s, int n, double *g) {
+    const double invroot = 1.0 / (s * std::sqrt(2.0));
+    const double norm = 1.0 / (s * std::sqrt(2.0 * be::kPi));
+    auto pdf = [&](double x) { return norm * std::exp(-((x - mu) * (x - mu)) / (2.0 * s * s)); };
+    auto m0 = [&](double A, double B) { return 0.5 * (std::erf((B - mu) * invroot) - std::erf((A - mu) * invroot)); };
+    auto m1 = [&](double A, double B, double xi) { return (mu - xi) * m0(A, B) - s * s * (pdf(B) - pdf(A)); };
+    auto m2 = [&](double A, double B, double xi) {
+        return (s * s + (mu - xi) * (mu - xi)) * m0(A, B) - s * s * ((B - mu) * pdf(B) - (A - mu) * pdf(A)) -
+               2.0 * (mu - xi) * s * s * (pdf(B) - pdf(A));
+    };
+    const double half = h / 2.0;
+    for (int i = 0; i < n; ++i) {
+        const double xi = x0 + (double)i * h;
+        if (method == 0) {
+            g[i] = m0(xi - h, xi + h) + (m1(xi - h, xi, xi) - m1(xi, xi + h, xi)) / h;
+        } else {
+            const double cL = xi - half, cR = xi + half;
+            const double lL = xi - 3.0 * half, lR = xi - half, rL = xi + half, rR = xi + 3.0 * half;
+            g[i] = 0.75 * m0(cL, cR) - m2(cL, cR, xi) / (h * h) + 1.125 * (m0(lL, lR) + m0(rL, rR)) +
+                   1.5 * (m1(lL, lR, xi) - m1(rL, rR, xi)) / h + 0.5 * (m2(lL, lR, xi) + m2(rL, rR, xi)) / (h * h);
+        }
+    }
+}
+
+// Transverse moments of the source slice from sums relative to its first particle (gaussian_pic.jl:432-486).
+struct SourceMoments {
+    int64_t n;
+    double mx, mpx, varx, cxpx, varpx, my, mpy, vary, cypy, varpy;
+};
+SourceMoments source_moments(const Coords &s) {
+    SourceMoments m{};
+    const size_t n = s.size();
+    m.n = (int64_t)n;
+    const double x0 = s.x[0], px0 = s.px[0], y0 = s.y[0], py0 = s.py[0];
+    double sx = 0, spx = 0, sy = 0, spy = 0, sxx = 0, spxpx = 0, syy = 0, spypy = 0, sxpx = 0, sypy = 0;
+    for (size_t i = 0; i < n; ++i) {
+        const double dx = s.x[i] - x0, dpx = s.px[i] - px0, dy = s.y[i] - y0, dpy = s.py[i] - py0;
+        sx += dx; spx += dpx; sy += dy; spy += dpy;
+        sxx += dx * dx; spxpx += dpx * dpx;
+        syy += dy * dy; spypy += dpy * dpy;
+        sxpx += dx * dpx; sypy += dy * dpy;
+    }
+    const double invn = 1.0 / (double)n;
+    const double dmx = sx * invn, dmpx = spx * invn, dmy = sy * invn, dmpy = spy * invn;
+    m.mx = x0 + dmx; m.mpx = px0 + dmpx; m.my = y0 + dmy; m.mpy = py0 + dmpy;
+    // muladd(-a, b, c) of slicing.jl:664-668, fused on FMA hosts
+    m.varx = jmax(std::fma(-dmx, dmx, sxx * invn), 0.0);
+    m.vary = jmax(std::fma(-dmy, dmy, syy * invn), 0.0);
+    m.cxpx = std::fma(-dmx, dmpx, sxpx * invn);
+    m.varpx = jmax(std::fma(-dmpx, dmpx, spxpx * invn), 0.0);
+    m.cypy = std::fma(-dmy, dmpy, sypy * invn);
+    m.varpy = jmax(std::fma(-dmpy, dmpy, spypy * invn), 0.0);
+    return m;
+}
+
+// Drifted reference Gaussian at a slice boundary (gaussian_pic.jl:496-540, uncoupled).
+struct Boundary {
+    double mux, muy, sigx, sigy, rx, ry, s;
+};
+Boundary boundary(const SourceMoments &m, double s) {
+    Boundary b{};
+    b.s = s;
+    b.mux = m.mx + m.mpx * s;
+    b.muy = m.my + m.mpy * s;
+    const double varx = m.varx + 2.0 * s * m.cxpx + s * s * m.varpx;
+    const double vary = m.vary + 2.0 * s * m.cypy + s * s * m.varpy;
+    b.sigx = std::sqrt(jmax(varx, 0.0));
+    b.sigy = std::sqrt(jmax(vary, 0.0));
+    b.rx = 2.0 * (m.cxpx + s * m.varpx);
+    b.ry = 2.0 * (m.cypy + s * m.varpy);
+    return b;
+}
+
+bool boundary_resolved(int64_t n, const Boundary &L, const Boundary &R) {  // gaussian_pic.jl:542-553
+    return n >= 2 && std::isfinite(L.sigx) && std::isfinite(L.sigy) && std::isfinite(R.sigx) &&
+           std::isfinite(R.sigy) && L.sigx > 0 && L.sigy > 0 && R.sigx > 0 && R.sigy > 0;
+}
+
+// Deposit, subtract the (neutralised) erf-integrated reference Gaussian, solve (gaussian_pic.jl:559-597).
+void solve_drifted_gaussian(const Options &O, Workspace &ws, FieldPlanes &fp, const Coords &src, double s,
+                            const Grid &sg, const std::vector<cplx> &gfft, const Boundary &b) {
+    const int nx = O.o.nx, ny = O.o.ny;
+    const double hx = sg.width / (double)(nx - 1), hy = sg.height / (double)(ny - 1);
+    std::fill(ws.charge.begin(), ws.charge.end(), 0.0);
+    deposit_grid(ws.charge.data(), 2 * nx, O.o.deposit_method, src.x.data(), src.px.data(), src.y.data(),
+                 src.py.data(), (int64_t)src.size(), true, s, sg.x0, sg.y0, hx, hy, nx, ny,
+                 O.o.fixed_point_deposit != 0, nullptr);
+    std::vector<double> gx(nx), gy(ny);
+    gaussian_profile(O.o.deposit_method, sg.x0, hx, b.mux, b.sigx, nx, gx.data());
+    gaussian_profile(O.o.deposit_method, sg.y0, hy, b.muy, b.sigy, ny, gy.data());
+    double sgx = 0, sgy = 0;
+    for (double v : gx) sgx += v;
+    for (double v : gy) sgy += v;
+    double qsum = 0;
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) qsum += ws.charge[i + (size_t)j * 2 * nx];
+    double amp = (double)src.size();
+    if (O.o.neutralize && sgx * sgy > 0.0) amp = qsum / (sgx * sgy);
+    for (int j = 0; j < ny; ++j) {
+        const double gj = amp * gy[j];
+        for (int i = 0; i < nx; ++i) ws.charge[i + (size_t)j * 2 * nx] -= gx[i] * gj;
+    }
+    for (size_t k = 0; k < ws.charge.size(); ++k) ws.spectral[k] = cplx(ws.charge[k], 0.0);
+    ws.fft.run(ws.spectral.data(), false);
+    for (size_t k = 0; k < ws.spectral.size(); ++k) ws.spectral[k] *= gfft[k];
+    ws.fft.run(ws.spectral.data(), true);
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) fp.phi[i + (size_t)j * nx] = ws.spectral[i + (size_t)j * 2 * nx].real();
+    field_from_phi(fp.phi.data(), nx, ny, hx, hy, O.o.field_derivative == 4, fp.Ex.data(), fp.Ey.data());
+}
+
+// One directed Gaussian-subtracted interaction (gaussian_pic.jl:604-810); falls back to plain PIC when
+// the drifted source moments are degenerate (gaussian_pic.jl:542-553, 634-637).
+void interaction_gaussian(Ctx &C, Workspace &ws, const Coords &source, const SliceParam &ps, Coords &field,
+                          const SliceParam &pf, double kbb, int i, int j, int dir, int vslot, int64_t counters[3]) {
+    const Options &O = C.O;
+    const int nsource = (int)source.size(), nfield = (int)field.size();
+    const double sL = 0.5 * (ps.center - pf.lb);
+    const double sR = 0.5 * (ps.center - pf.rb);
+    const SourceMoments mom = source_moments(source);
+    const Boundary bL = boundary(mom, sL), bR = boundary(mom, sR);
+    if (!boundary_resolved(mom.n, bL, bR)) {
+        interaction(C, ws, source, ps, field, pf, kbb, i, j, dir, vslot, counters);
+        return;
+    }
+    const double margin = O.o.margin_sigma;
+    double sxl = source.x[0] + source.px[0] * sL, syl = source.y[0] + source.py[0] * sL;
+    double sxr = source.x[0] + source.px[0] * sR, syr = source.y[0] + source.py[0] * sR;
+    double sxmin = jmin(sxl, sxr), sxmax = jmax(sxl, sxr), symin = jmin(syl, syr), symax = jmax(syl, syr);
+    for (int k = 1; k < nsource; ++k) {
+        const double xl = source.x[k] + source.px[k] * sL, yl = source.y[k] + source.py[k] * sL;
+        const double xr = source.x[k] + source.px[k] * sR, yr = source.y[k] + source.py[k] * sR;
+        sxmin = jmin(jmin(sxmin, xl), xr); sxmax = jmax(jmax(sxmax, xl), xr);
+        symin = jmin(jmin(symin, yl), yr); symax = jmax(jmax(symax, yl), yr);
+    }
+    if (margin > 0) {
+        const double gxlo = jmin(bL.mux - margin * bL.sigx, bR.mux - margin * bR.sigx);
+        const double gxhi = jmax(bL.mux + margin * bL.sigx, bR.mux + margin * bR.sigx);
+        const double gylo = jmin(bL.muy - margin * bL.sigy, bR.muy - margin * bR.sigy);
+        const double gyhi = jmax(bL.muy + margin * bL.sigy, bR.muy + margin * bR.sigy);
+        sxmin = jmin(sxmin, gxlo); sxmax = jmax(sxmax, gxhi);
+        symin = jmin(symin, gylo); symax = jmax(symax, gyhi);
+    }
+    if (!(std::isfinite(sxmin) && std::isfinite(sxmax) && std::isfinite(symin) && std::isfinite(symax)))
+        nonfinite("source", source, pair_ctx(i, j, dir));
+    double fxmin = field.x[0] + 0.5 * (field.z[0] - ps.center) * field.px[0];
+    double fxmax = fxmin;
+    double fymin = field.y[0] + 0.5 * (field.z[0] - ps.center) * field.py[0];
+    double fymax = fymin;
+    const bool lk = O.o.longitudinal_kick != 0;
+    for (int k = 0; k < nfield; ++k) {
+        const double s = 0.5 * (field.z[k] - ps.center);
+        field.x[k] += s * field.px[k];
+        field.y[k] += s * field.py[k];
+        if (lk) field.pz[k] -= 0.25 * (field.px[k] * field.px[k] + field.py[k] * field.py[k]);
+        fxmin = jmin(fxmin, field.x[k]); fxmax = jmax(fxmax, field.x[k]);
+        fymin = jmin(fymin, field.y[k]); fymax = jmax(fymax, field.y[k]);
+    }
+    if (!(std::isfinite(fxmin) && std::isfinite(fxmax) && std::isfinite(fymin) && std::isfinite(fymax)))
+        nonfinite("field", field, pair_ctx(i, j, dir));
+    Grid sg, fg;
+    interaction_grids(O, sxmin, sxmax, symin, symax, fxmin, fxmax, fymin, fymax, sg, fg);
+    Bounds sb{sxmin, sxmax, symin, symax}, fb{fxmin, fxmax, fymin, fymax};
+    std::vector<cplx> own;
+    const std::vector<cplx> &gfft = slice_pair_green(C, ws, i, j, dir, sg, fg, sb, fb, own, counters);
+    solve_drifted_gaussian(O, ws, ws.left, source, sL, sg, gfft, bL);
+    solve_drifted_gaussian(O, ws, ws.right, source, sR, sg, gfft, bR);
+
+    const double ks = 2.0 * kbb;
+    const double half_ns = 0.5 * (double)nsource;
+    const double kbb_eff = ks * half_ns;
+    double hzi, zbias;
+    slice_interp_params(pf.lb, pf.rb, hzi, zbias);
+    for (int k = 0; k < nfield; ++k) {
+        const double x = field.x[k], y = field.y[k];
+        const double zL = jclamp(-field.z[k] * hzi + zbias, 0.0, 1.0);
+        const double zR = 1.0 - zL;
+        double Kxd, Kyd, Kzd;
+        interpolate_kick(O, fg, x, y, ws.left, ws.right, zL, zR, Kxd, Kyd, Kzd);
+        double bLx, bLy, HxL = 0, HyL = 0, bRx, bRy, HxR = 0, HyR = 0;
+        if (lk) {
+            be::response(kbb_eff, bL.sigx, bL.sigy, x - bL.mux, y - bL.muy, bLx, bLy, HxL, HyL);
+            be::response(kbb_eff, bR.sigx, bR.sigy, x - bR.mux, y - bR.muy, bRx, bRy, HxR, HyR);
+        } else {
+            be::kick(bL.sigx, bL.sigy, x - bL.mux, y - bL.muy, bLx, bLy);
+            be::kick(bR.sigx, bR.sigy, x - bR.mux, y - bR.muy, bRx, bRy);
+        }
+        const double Kxa = half_ns * (zL * bLx + zR * bRx);
+        const double Kya = half_ns * (zL * bLy + zR * bRy);
+        const double dpxa = ks * Kxa, dpya = ks * Kya;
+        field.px[k] += ks * Kxd + dpxa;
+        field.py[k] += ks * Kyd + dpya;
+        if (lk) {
+            const double covL = (HxL * bL.rx + HyL * bL.ry) / 4.0;
+            const double covR = (HxR * bR.rx + HyR * bR.ry) / 4.0;
+            field.pz[k] += ks * Kzd * hzi;
+            field.pz[k] += zL * covL + zR * covR;
+            field.pz[k] += 0.5 * (dpxa * mom.mpx + dpya * mom.mpy);
+        }
+        const double s = 0.5 * (ps.center - field.z[k]);
+        field.x[k] += s * field.px[k];
+        field.y[k] += s * field.py[k];
+        if (lk) field.pz[k] += 0.25 * (field.px[k] * field.px[k] + field.py[k] * field.py[k]);
+    }
+    const double sM = 0.5 * (ps.center - pf.center);
+    virtual_positions(source, sM, ws.vx[vslot], ws.vy[vslot]);
+}
+
 void interaction_node(Ctx &C, Workspace &ws, const Coords &source, const SliceParam &ps, Coords &field,
                       const SliceParam &pf, double kbb, const NodeMesh &gL, const NodeMesh &gR, int vslot) {
     const Options &O = C.O;
@@ -1155,6 +1369,10 @@ void validate(const Options &O) {
         throw OracleError(OO_ERR_UNSUPPORTED, "grid_extent != :extrema with interaction_grid != :slice_pair");
     if (o.interaction_grid == 2 && o.slice_interpolation != 0)
         throw OracleError(OO_ERR_UNSUPPORTED, "slice_interpolation = :quadratic with interaction_grid = :node");
+    if (o.gaussian && (o.slice_interpolation != 0 || o.interaction_grid != 0 || o.grid_extent != 0))
+        throw OracleError(OO_ERR_UNSUPPORTED, "GaussianPICPoissonSolver needs linear slice interpolation on the "
+                                              ":slice_pair grid with grid_extent = :extrema");
+    if (o.gaussian && !(o.margin_sigma >= 0)) throw OracleError(OO_ERR_ARG, "margin_sigma must be non-negative");
 }
 
 int nslices_of(const oo_options &o, int which) {
@@ -1260,6 +1478,9 @@ double collide(Ctx &C, double *b1[6], int64_t n1, double *b2[6], int64_t n2, con
                     if (!gL1.valid || !gR1.valid || !gL2.valid || !gR2.valid) continue;
                     interaction_node(C, ws, coord1, pa1, field2, pa2, kbb2, gL1, gR1, 0);
                     interaction_node(C, ws, coord2, pa2, coord1, pa1, kbb1, gL2, gR2, 1);
+                } else if (O.o.gaussian) {
+                    interaction_gaussian(C, ws, coord1, pa1, field2, pa2, kbb2, i, j, 1, 0, counters[p].data());
+                    interaction_gaussian(C, ws, coord2, pa2, coord1, pa1, kbb1, i, j, 2, 1, counters[p].data());
                 } else {
                     interaction(C, ws, coord1, pa1, field2, pa2, kbb2, i, j, 1, 0, counters[p].data());
                     interaction(C, ws, coord2, pa2, coord1, pa1, kbb1, i, j, 2, 1, counters[p].data());
@@ -1355,6 +1576,13 @@ void oo_beam_gaussian(int64_t n, uint64_t seed, uint64_t rng_id, const double be
 }
 
 double oo_erfinv(double x) { return erfinv_impl(x); }
+void oo_faddeeva(double zr, double zi, double out[2]) { be::faddeeva(zr, zi, out[0], out[1]); }
+void oo_be_response(double kbb, double sigx, double sigy, double x, double y, double out[4]) {
+    be::response(kbb, sigx, sigy, x, y, out[0], out[1], out[2], out[3]);
+}
+void oo_gaussian_profile(int32_t method, double x0, double h, double mu, double sigma, int32_t n, double *g) {
+    gaussian_profile(method, x0, h, mu, sigma, n, g);
+}
 double oo_kernel_integral(double x, double y) { return kernel_integral(x, y); }
 double oo_atan_ratio(double num, double den) { return atan_ratio(num, den); }
 void oo_cic_weights(double u, int32_t n, int32_t *base, double w[2]) { int b; cic_weights(u, n, b, w); *base = b; }

@@ -50,9 +50,19 @@ typedef struct {
     double kbb1, kbb2, lum_scale;
     int32_t fixed_point_deposit;       /* 1: int64 fixed-point charge grid (see oo_fixed_scale_bits) */
     int32_t nthreads;                  /* OpenMP threads for the pair batches (results do not depend on it) */
+    int32_t gaussian;                  /* 1: GaussianPICPoissonSolver (Gaussian-subtracted hybrid) */
+    int32_t neutralize;                /* hybrid: rescale the subtracted Gaussian to the deposited charge */
+    double margin_sigma;               /* hybrid: adaptive-box half-width in beam sigmas */
 } oo_options;
 
 typedef struct { double charge, mc2, E0, r0, npart; } oo_beam_params;
+
+/* Gaussian-subtracted hybrid pieces (gaussian_pic.jl, strong_beam.jl, SpecialMath.jl). */
+void oo_faddeeva(double zr, double zi, double out[2]);
+/* kick (Kx, Ky) and kbb-scaled potential Hessians (Hxx, Hyy) of a (sigx, sigy) Gaussian at (x, y) */
+void oo_be_response(double kbb, double sigx, double sigy, double x, double y, double out[4]);
+/* erf-integrated CIC (0) / TSC (1) node profile of a 1D Gaussian on nodes x0 + i h, i < n */
+void oo_gaussian_profile(int32_t method, double x0, double h, double mu, double sigma, int32_t n, double *g);
 
 /* Counter RNG and beam construction (counter_rng.jl, Beam.jl). */
 void oo_philox4x32_block(const uint32_t c[4], const uint32_t k[2], uint32_t out[4]);

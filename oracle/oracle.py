@@ -53,6 +53,8 @@ class OOOptions(C.Structure):
         ("kbb1", C.c_double), ("kbb2", C.c_double), ("lum_scale", C.c_double),
         ("fixed_point_deposit", C.c_int32),
         ("nthreads", C.c_int32),
+        ("gaussian", C.c_int32), ("neutralize", C.c_int32),
+        ("margin_sigma", C.c_double),
     ]
 
 
@@ -79,6 +81,9 @@ def lib():
         L.oo_beam_gaussian.argtypes = [i64, u64, u64, P(d), P(d), P(d), d] + [P(d)] * 6
         L.oo_erfinv.restype = d
         L.oo_erfinv.argtypes = [d]
+        L.oo_faddeeva.argtypes = [d, d, P(d)]
+        L.oo_be_response.argtypes = [d, d, d, d, d, P(d)]
+        L.oo_gaussian_profile.argtypes = [i32, d, d, d, d, i32, P(d)]
         L.oo_kernel_integral.restype = d
         L.oo_kernel_integral.argtypes = [d, d]
         L.oo_atan_ratio.restype = d
@@ -168,6 +173,9 @@ class OracleOptions:
     luminosity_scale: Optional[float] = None
     fixed_point_deposit: bool = False
     nthreads: int = 1
+    gaussian: bool = False          # GaussianPICPoissonSolver (the Gaussian-subtracted hybrid)
+    neutralize: bool = True
+    margin_sigma: float = 5.0
 
     def to_c(self) -> OOOptions:
         o = OOOptions()
@@ -206,7 +214,30 @@ class OracleOptions:
         o.lum_scale = self.luminosity_scale or 0.0
         o.fixed_point_deposit = int(bool(self.fixed_point_deposit))
         o.nthreads = int(self.nthreads)
+        o.gaussian = int(bool(self.gaussian))
+        o.neutralize = int(bool(self.neutralize))
+        o.margin_sigma = float(self.margin_sigma)
         return o
+
+
+def faddeeva(z: complex) -> complex:
+    out = (C.c_double * 2)()
+    lib().oo_faddeeva(C.c_double(z.real), C.c_double(z.imag), out)
+    return complex(out[0], out[1])
+
+
+def be_response(kbb, sigx, sigy, x, y):
+    """(Kx, Ky, Hxx, Hyy): Bassetti-Erskine kick and kbb-scaled potential Hessians of a (sigx, sigy) Gaussian."""
+    out = (C.c_double * 4)()
+    lib().oo_be_response(C.c_double(kbb), C.c_double(sigx), C.c_double(sigy), C.c_double(x), C.c_double(y), out)
+    return tuple(out)
+
+
+def gaussian_profile(method, x0, h, mu, sigma, n):
+    g = np.zeros(n)
+    lib().oo_gaussian_profile(int(_SYM["deposit_method"][method]), C.c_double(x0), C.c_double(h), C.c_double(mu),
+                              C.c_double(sigma), int(n), _dp(g))
+    return g
 
 
 def philox4x32_block(c, k):
