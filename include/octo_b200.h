@@ -85,8 +85,13 @@ typedef struct {
     const double *positions1, *positions2;      /* :specified internal positions (nslices-1 each) */
     int32_t has_kbb1, has_kbb2, has_lum_scale;
     double kbb1, kbb2, lum_scale;
-    int32_t precision;                 /* 0 = FP64 plain form */
-    int32_t reserved[7];
+    int32_t precision;                 /* 0 = FP64 plain form, 1 = FP32 precision form (float32 beams) */
+    /* GaussianPICPoissonSolver (gaussian_pic.jl:87-112): 1 = subtract the drifted reference Gaussian of
+     * each source slice before the solve and add its Bassetti-Erskine kick back analytically */
+    int32_t gaussian;
+    double margin_sigma;               /* hybrid: Gaussian containment half-width in sigmas (default 5) */
+    int32_t neutralize;                /* hybrid: rescale the subtracted Gaussian to the deposited charge */
+    int32_t reserved[3];
 } octo_pic_options;
 
 /* What a collide reports besides the luminosity. */

@@ -2,6 +2,7 @@
 // or pair of one collision-time wavefront (slicing.jl:601-647), so the S1*S2 pairs of a turn run
 // as 2S-1 batched launch sequences instead of one launch chain per pair.
 #pragma once
+#include "be_device.cuh"
 #include "fft.cuh"
 #include "geometry.cuh"
 #include "octo_internal.cuh"
@@ -43,6 +44,12 @@ struct Collide {           // device pointers for one collide (passed by value)
     const void *twr_x, *twr_y;   // the same in RealT<R>::C2 (charge convolution)
     SoA beam[2];
     double klum;
+    // Gaussian-subtracted hybrid (C.o.gaussian)
+    HybridTask *hyb;             // [task]
+    double *hmom;                // [task][kMaxBoundBlocks][kMomentSums] block partial moment sums
+    unsigned long long *qtot;    // [plane-in-front] total fixed-point charge of the plane (two's complement)
+    double *hprof;               // [plane-in-front][nx + ny] reference-Gaussian node profiles
+    double *hsum;                // [plane-in-front][2] profile sums
 };
 
 // ------------------------------------------------------------------ bounds
@@ -133,13 +140,67 @@ __global__ void __launch_bounds__(256) k_pair_bounds(Collide C, int task0) {
     }
 }
 
+// Hybrid: transverse moment sums of each task's source slice relative to its first particle
+// (gaussian_pic.jl:432-486), as per-block partials folded in block order by k_plan.  grid: (blocks per
+// side, 2 * pairs in front), the mapping of k_pair_bounds.
+__global__ void __launch_bounds__(256) k_hyb_moments(Collide C, int task0) {
+    const int q = blockIdx.y >> 1, side = blockIdx.y & 1;
+    const int t = task0 + 2 * q + side;  // side 0: direction-1 task (source beam 1), side 1: direction 2
+    const Task &T = C.tasks[t];
+    const SoA S = C.beam[T.src_beam];
+    const long long st = T.src_start, n = T.src_n;
+    const double *X = col<double>(S, 0) + st, *PX = col<double>(S, 1) + st, *Y = col<double>(S, 2) + st,
+                 *PY = col<double>(S, 3) + st;
+    double a[kMomentSums];
+#pragma unroll
+    for (int k = 0; k < kMomentSums; ++k) a[k] = 0.0;
+    if (n > 0) {
+        const double x0 = X[0], px0 = PX[0], y0 = Y[0], py0 = PY[0];
+        for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+            const double dx = X[k] - x0, dpx = PX[k] - px0, dy = Y[k] - y0, dpy = PY[k] - py0;
+            a[0] += dx; a[1] += dpx; a[2] += dy; a[3] += dpy;
+            a[4] += dx * dx; a[5] += dpx * dpx; a[6] += dy * dy; a[7] += dpy * dpy;
+            a[8] += dx * dpx; a[9] += dy * dpy;
+        }
+    }
+    __shared__ double red[8][kMomentSums];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < kMomentSums; ++k) {
+        double v = a[k];
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kMomentSums) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][threadIdx.x];
+        C.hmom[((long long)t * kMaxBoundBlocks + blockIdx.x) * kMomentSums + threadIdx.x] = v;
+    }
+}
+
+// Drifted reference Gaussian of the source at drift s (gaussian_pic.jl:496-540, uncoupled).
+__device__ __forceinline__ void hyb_boundary(const double m[10], double s, HybridTask &H, int side) {
+    // m: mx, mpx, varx, cxpx, varpx, my, mpy, vary, cypy, varpy
+    H.mux[side] = m[0] + m[1] * s;
+    H.muy[side] = m[5] + m[6] * s;
+    const double varx = m[2] + 2.0 * s * m[3] + s * s * m[4];
+    const double vary = m[7] + 2.0 * s * m[8] + s * s * m[9];
+    H.sigx[side] = sqrt(jmax(varx, 0.0));
+    H.sigy[side] = sqrt(jmax(vary, 0.0));
+    H.rx[side] = 2.0 * (m[3] + s * m[4]);
+    H.ry[side] = 2.0 * (m[8] + s * m[9]);
+}
+
 __device__ inline void record_error(DevStatus *st, int task, int code, int role) {
     unsigned long long key = ((unsigned long long)task << 16) | ((unsigned long long)code << 8) | (unsigned)role;
     atomicMin(&st->first_bad, key);
 }
 
-// Grid geometry and Green-cache decision per task (pic_cpu.jl:954-1064, 1729-1821).
-__global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0) {
+// Grid geometry and Green-cache decision per task (pic_cpu.jl:954-1064, 1729-1821).  Hybrid: the source
+// moments (nblk block partials), the reference Gaussians at both boundaries, the plain-PIC fallback test and
+// the margin box around the Gaussians joined to the source extent (gaussian_pic.jl:604-660).
+__global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0, int nblk) {
     int tl = blockIdx.x * blockDim.x + threadIdx.x;
     if (tl >= ntasks) return;
     int t = task0 + tl;
@@ -158,6 +219,49 @@ __global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0) {
     if ((nf & 2) || !(isfinite(fxmin) && isfinite(fxmax) && isfinite(fymin) && isfinite(fymax))) {
         record_error(C.status, t, 1, 2);
         return;
+    }
+    if (C.o.gaussian) {
+        HybridTask &H = C.hyb[t];
+        H.mode = 0;
+        double sum[kMomentSums];
+        for (int k = 0; k < kMomentSums; ++k) sum[k] = 0.0;
+        for (int b = 0; b < nblk; ++b)
+            for (int k = 0; k < kMomentSums; ++k) sum[k] += C.hmom[((long long)t * kMaxBoundBlocks + b) * kMomentSums + k];
+        const SoA S = C.beam[T.src_beam];
+        const long long st = T.src_start, n = T.src_n;
+        const double x0 = col<double>(S, 0)[st], px0 = col<double>(S, 1)[st], y0 = col<double>(S, 2)[st],
+                     py0 = col<double>(S, 3)[st];
+        const double invn = 1.0 / (double)n;
+        const double dmx = sum[0] * invn, dmpx = sum[1] * invn, dmy = sum[2] * invn, dmpy = sum[3] * invn;
+        double m[10];
+        m[0] = x0 + dmx; m[1] = px0 + dmpx; m[5] = y0 + dmy; m[6] = py0 + dmpy;
+        // muladd(-a, b, c) of slicing.jl:664-668, fused on FMA hosts
+        m[2] = jmax(fma(-dmx, dmx, sum[4] * invn), 0.0);
+        m[7] = jmax(fma(-dmy, dmy, sum[6] * invn), 0.0);
+        m[3] = fma(-dmx, dmpx, sum[8] * invn);
+        m[4] = jmax(fma(-dmpx, dmpx, sum[5] * invn), 0.0);
+        m[8] = fma(-dmy, dmpy, sum[9] * invn);
+        m[9] = jmax(fma(-dmpy, dmpy, sum[7] * invn), 0.0);
+        hyb_boundary(m, T.sL, H, 0);
+        hyb_boundary(m, T.sR, H, 1);
+        H.half_ns = 0.5 * (double)n;
+        H.mpx = m[1];
+        H.mpy = m[6];
+        bool ok = n >= 2;
+        for (int sd = 0; sd < 2; ++sd)
+            ok = ok && isfinite(H.sigx[sd]) && isfinite(H.sigy[sd]) && H.sigx[sd] > 0 && H.sigy[sd] > 0;
+        H.mode = ok ? 1 : 0;
+        if (ok && C.o.margin > 0) {
+            const double mg = C.o.margin;
+            sxmin = jmin(sxmin, jmin(H.mux[0] - mg * H.sigx[0], H.mux[1] - mg * H.sigx[1]));
+            sxmax = jmax(sxmax, jmax(H.mux[0] + mg * H.sigx[0], H.mux[1] + mg * H.sigx[1]));
+            symin = jmin(symin, jmin(H.muy[0] - mg * H.sigy[0], H.muy[1] - mg * H.sigy[1]));
+            symax = jmax(symax, jmax(H.muy[0] + mg * H.sigy[0], H.muy[1] + mg * H.sigy[1]));
+            if (!(isfinite(sxmin) && isfinite(sxmax) && isfinite(symin) && isfinite(symax))) {
+                record_error(C.status, t, 1, 1);
+                return;
+            }
+        }
     }
     Grid sg, fg;
     if (!interaction_grids(C.o, sxmin, sxmax, symin, symax, fxmin, fxmax, fymin, fymax, sg, fg)) {
@@ -397,9 +501,10 @@ __device__ __forceinline__ T *generic_ptr(T *p) {
     return p;
 }
 template <class R, int METHOD>
-__device__ __forceinline__ void deposit_taps(R u, R v, int nw, int nh, R scale, long long *grid, int ld) {
+__device__ __forceinline__ long long deposit_taps(R u, R v, int nw, int nh, R scale, long long *grid, int ld) {
     constexpr int NT = METHOD == 0 ? 2 : 3;
     int ix, iy;
+    long long total = 0;
     R wx[NT], wy[NT];
     if (METHOD == 0) { cic_weights(u, nw, ix, wx); cic_weights(v, nh, iy, wy); }
     else { tsc_weights(u, nw, ix, wx); tsc_weights(v, nh, iy, wy); }
@@ -409,8 +514,10 @@ __device__ __forceinline__ void deposit_taps(R u, R v, int nw, int nh, R scale, 
 #pragma unroll
         for (int k = 0; k < NT; ++k) {
             const long long qv = round_ll(wx[m] * wy[k] * scale);
+            total += qv;
             if (qv) atomicAdd((unsigned long long *)&grid[c0 + k * ld + m], (unsigned long long)qv);
         }
+    return total;
 }
 
 // Merge a block's shared-memory grid into the plane's int64 grid.
@@ -454,13 +561,18 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
     const R x0 = (R)sg.x0, y0 = (R)sg.y0;
     const R xlo = x0, xhi = (R)(sg.x0 + sg.w), ylo = y0, yhi = (R)(sg.y0 + sg.h);
     int outside = 0;
+    long long total = 0;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < P.src_n; k += (long long)gridDim.x * blockDim.x) {
         const long long p = P.src_start + k;
         const R xd = X[p] + PX[p] * s;
         const R yd = Y[p] + PY[p] * s;
         if (P.count_dropped && !(isfinite(xd) && xlo <= xd && xd <= xhi && isfinite(yd) && ylo <= yd && yd <= yhi))
             ++outside;
-        deposit_taps<R, METHOD>((xd - x0) * hxi, (yd - y0) * hyi, nx, ny, scale, acc, nx);
+        total += deposit_taps<R, METHOD>((xd - x0) * hxi, (yd - y0) * hyi, nx, ny, scale, acc, nx);
+    }
+    if (C.o.gaussian) {  // the plane's exact total charge, for the neutralised subtraction
+        for (int o = 16; o; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+        if ((threadIdx.x & 31) == 0 && total) atomicAdd(&C.qtot[pl], (unsigned long long)total);
     }
     if (P.count_dropped) {
         for (int o = 16; o; o >>= 1) outside += __shfl_xor_sync(0xffffffffu, outside, o);
@@ -548,6 +660,51 @@ __global__ void k_lum_fold(Collide C, int lj0, int nl) {
     C.lum_parts[J.pair] = s * C.klum * hxi * hyi;
 }
 
+// Hybrid: erf-integrated CIC/TSC node profiles of the reference Gaussian of each field-solve plane
+// (gaussian_pic.jl:206-237) on its source grid, and their sums (the neutralisation denominator).
+// One block per plane of the front.
+__device__ __forceinline__ double gauss_node_weight(int method, double xi, double h, double mu, double s) {
+    const double invroot = 1.0 / (s * 1.4142135623730951);
+    const double norm = 1.0 / (s * 2.5066282746310002);  // s * sqrt(2 pi)
+    auto pdf = [&](double x) { return norm * exp(-((x - mu) * (x - mu)) / (2.0 * s * s)); };
+    auto m0 = [&](double A, double B) { return 0.5 * (erf((B - mu) * invroot) - erf((A - mu) * invroot)); };
+    auto m1 = [&](double A, double B) { return (mu - xi) * m0(A, B) - s * s * (pdf(B) - pdf(A)); };
+    auto m2 = [&](double A, double B) {
+        return (s * s + (mu - xi) * (mu - xi)) * m0(A, B) - s * s * ((B - mu) * pdf(B) - (A - mu) * pdf(A)) -
+               2.0 * (mu - xi) * s * s * (pdf(B) - pdf(A));
+    };
+    if (method == 0) return m0(xi - h, xi + h) + (m1(xi - h, xi) - m1(xi, xi + h)) / h;
+    const double half = h / 2.0;
+    const double cL = xi - half, cR = xi + half, lL = xi - 3.0 * half, lR = xi - half, rL = xi + half,
+                 rR = xi + 3.0 * half;
+    return 0.75 * m0(cL, cR) - m2(cL, cR) / (h * h) + 1.125 * (m0(lL, lR) + m0(rL, rR)) +
+           1.5 * (m1(lL, lR) - m1(rL, rR)) / h + 0.5 * (m2(lL, lR) + m2(rL, rR)) / (h * h);
+}
+
+__global__ void __launch_bounds__(256) k_hyb_profiles(Collide C, int plane0) {
+    const int pl = blockIdx.x;
+    const Plane &P = C.planes[plane0 + pl];
+    const TaskGeom &G = C.geom[P.task];
+    const HybridTask &H = C.hyb[P.task];
+    if (G.green < 0 || !H.mode) return;
+    const int nx = C.o.nx, ny = C.o.ny, side = P.kind == 0 ? 0 : 1;
+    const Grid sg = G.sg;
+    const double hx = sg.w / (double)(nx - 1), hy = sg.h / (double)(ny - 1);
+    double *g = C.hprof + (long long)pl * (nx + ny);
+    for (int i = threadIdx.x; i < nx + ny; i += blockDim.x) {
+        if (i < nx) g[i] = gauss_node_weight(C.o.method, sg.x0 + (double)i * hx, hx, H.mux[side], H.sigx[side]);
+        else g[i] = gauss_node_weight(C.o.method, sg.y0 + (double)(i - nx) * hy, hy, H.muy[side], H.sigy[side]);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {  // sequential sums, node order
+        double sx = 0.0, sy = 0.0;
+        for (int i = 0; i < nx; ++i) sx += g[i];
+        for (int j = 0; j < ny; ++j) sy += g[nx + j];
+        C.hsum[2 * pl] = sx;
+        C.hsum[2 * pl + 1] = sy;
+    }
+}
+
 // ------------------------------------------------------------------ FFT convolution
 __device__ __forceinline__ int plane_green(const Collide &C, const Plane &P) {
     if (P.green >= 0) return P.green;
@@ -581,6 +738,18 @@ __global__ void __launch_bounds__(128) k_conv_rows(Collide C, int plane0) {
     const long long *qo = q + (long long)P.other_delta * nx * ny;
     const bool diff = kPrecision && P.other_delta != 0;
     const long long sgn = P.self_first ? 1 : -1;
+    // Hybrid: subtract amp * gx[i] * gy[j] (gaussian_pic.jl:580-589); amp neutralises the subtracted
+    // Gaussian to the deposited charge, else it carries the slice's particle count.
+    const bool hyb = C.o.gaussian && C.hyb[P.task].mode;
+    const double *gx = C.hprof + (long long)pl * (nx + ny), *gy = gx + nx;
+    double gj0 = 0.0, gj1 = 0.0;
+    if (hyb) {
+        const double sgx = C.hsum[2 * pl], sgy = C.hsum[2 * pl + 1];
+        double amp = (double)P.src_n;
+        if (C.o.neutralize && sgx * sgy > 0.0) amp = ((double)(long long)C.qtot[pl] * inv) / (sgx * sgy);
+        gj0 = amp * gy[j0];
+        if (j1 < ny) gj1 = amp * gy[j1];
+    }
     for (int i = lane; i < NX; i += 32) {
         C2 v;
         v.x = R(0);
@@ -588,12 +757,12 @@ __global__ void __launch_bounds__(128) k_conv_rows(Collide C, int plane0) {
         if (i < nx) {
             long long qa = q[(long long)j0 * nx + i];
             if (diff) qa = sgn * (qa - qo[(long long)j0 * nx + i]);
-            v.x = (R)((double)qa * inv);
+            v.x = hyb ? (R)((double)qa * inv - gx[i] * gj0) : (R)((double)qa * inv);
             if (!kPrecision && qa) q[(long long)j0 * nx + i] = 0;
             if (j1 < ny) {
                 long long qb = q[(long long)j1 * nx + i];
                 if (diff) qb = sgn * (qb - qo[(long long)j1 * nx + i]);
-                v.y = (R)((double)qb * inv);
+                v.y = hyb ? (R)((double)qb * inv - gx[i] * gj1) : (R)((double)qb * inv);
                 if (!kPrecision && qb) q[(long long)j1 * nx + i] = 0;
             }
         }
@@ -811,6 +980,8 @@ struct KickJob {
     R c_src, hzi, zbias, ks;
     long long fld_start, fld_n, plane_off;
     int fld_beam, ok;
+    int hyb;               // Gaussian-subtracted hybrid active for this task (FP64 only)
+    HybridTask H;
 };
 
 template <class R>
@@ -920,6 +1091,7 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
         const FC *FL = base, *FR = base + CV * pc;
         const Taps<R, METHOD> tp(o, J.gL, J.hxL, J.hyL, x, y);
         R Kx = 0, Ky = 0, Kz = 0;
+        // (hybrid: K is the field of the residual charge; the analytic Gaussian kick is added below)
 #pragma unroll
         for (int q = 0; q < NT2; ++q) {
             R pl, el, fl, pr, er, fr;
@@ -935,9 +1107,33 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
                 Kz += tp.w[q] * (pl - pr);
             }
         }
-        px += ks * Kx;
-        py += ks * Ky;
-        if (lk) { if (kPrecision) dpz += ks * Kz * J.hzi; else pz += ks * Kz * J.hzi; }
+        if (!kPrecision && J.hyb) {
+            // Analytic add-back of the subtracted Gaussian (gaussian_pic.jl:851-884): half the slice population
+            // times the Bassetti-Erskine kick at both boundaries, blended in z, and its longitudinal terms.
+            const HybridTask &H = J.H;
+            const double kbb_eff = (double)ks * H.half_ns;
+            double bLx, bLy, HxL = 0, HyL = 0, bRx, bRy, HxR = 0, HyR = 0;
+            be_response(lk ? kbb_eff : 0.0, H.sigx[0], H.sigy[0], (double)x - H.mux[0], (double)y - H.muy[0], bLx, bLy,
+                        HxL, HyL);
+            be_response(lk ? kbb_eff : 0.0, H.sigx[1], H.sigy[1], (double)x - H.mux[1], (double)y - H.muy[1], bRx, bRy,
+                        HxR, HyR);
+            const double Kxa = H.half_ns * ((double)zL * bLx + (double)zR * bRx);
+            const double Kya = H.half_ns * ((double)zL * bLy + (double)zR * bRy);
+            const double dpxa = (double)ks * Kxa, dpya = (double)ks * Kya;
+            px += (R)((double)ks * (double)Kx + dpxa);
+            py += (R)((double)ks * (double)Ky + dpya);
+            if (lk) {
+                const double covL = (HxL * H.rx[0] + HyL * H.ry[0]) / 4.0;
+                const double covR = (HxR * H.rx[1] + HyR * H.ry[1]) / 4.0;
+                pz += ks * Kz * J.hzi;
+                pz += (R)((double)zL * covL + (double)zR * covR);
+                pz += (R)(0.5 * (dpxa * H.mpx + dpya * H.mpy));
+            }
+        } else {
+            px += ks * Kx;
+            py += ks * Ky;
+            if (lk) { if (kPrecision) dpz += ks * Kz * J.hzi; else pz += ks * Kz * J.hzi; }
+        }
     }
     const R s2 = R(0.5) * (J.c_src - z);
     if (kPrecision) {
@@ -969,6 +1165,11 @@ __global__ void __launch_bounds__(kKickThreads, sizeof(R) == 8 ? 1 : 4) k_kick(C
             J.ok = G.green >= 0;
             gL = G.fg;
             gR = G.fg;
+        }
+        J.hyb = 0;
+        if (C.o.gaussian && J.ok) {
+            J.H = C.hyb[bm.x];
+            J.hyb = J.H.mode;
         }
         J.gL = grid_r<R>(gL);
         J.gR = grid_r<R>(gR);

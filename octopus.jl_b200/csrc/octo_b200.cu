@@ -200,6 +200,9 @@ struct octo_ctx {
     DevBuf<double2> spec;
     DevBuf<double2> fields;
     DevBuf<double> lum_parts, lum_partial, node_ref, stats, partial;
+    DevBuf<HybridTask> hyb;            // Gaussian-subtracted hybrid state per task
+    DevBuf<double> hmom, hprof, hsum;  // its moment partials, node profiles and profile sums
+    DevBuf<unsigned long long> qtot;   // per-plane total fixed-point charge
     DevBuf<double *> soa_ptrs;
     PinBuf<char> stage;
     PinBuf<double> h_lum;
@@ -312,6 +315,18 @@ int validate_options(const octo_pic_options &o, std::string &msg) {
         const double *p = b == 0 ? o.positions1 : o.positions2;
         if (m == OCTO_SLICING_SPECIFIED && ns > 1 && !p) { msg = "specified slicing requires nslices-1 internal positions"; return OCTO_ERR_ARG; }
     }
+    if (o.gaussian) {  // GaussianPICPoissonSolver (gaussian_pic.jl:94-110, 140-151)
+        if (o.interaction_grid != OCTO_GRID_SLICE_PAIR || o.slice_interpolation != 0) {
+            msg = "GaussianPICPoissonSolver uses linear slice interpolation on the :slice_pair grid; "
+                  "interaction_grid and slice_interpolation must keep their defaults";
+            return OCTO_ERR_UNSUPPORTED;
+        }
+        if (!(o.margin_sigma >= 0.0)) { msg = "margin_sigma must be non-negative"; return OCTO_ERR_ARG; }
+        if (o.precision != 0) {
+            msg = "the Gaussian-subtracted hybrid runs in the FP64 plain form on this backend (float64 beams)";
+            return OCTO_ERR_UNSUPPORTED;
+        }
+    }
     if (o.precision != 0 && o.precision != 1) {
         msg = "precision must be 0 (FP64 plain form) or 1 (FP32 precision form)";
         return OCTO_ERR_ARG;
@@ -337,6 +352,29 @@ void upload_twiddles(DevBuf<float2> &buf, int L) {
     }
     buf.ensure(L / 2);
     CK(cudaMemcpy(buf.p, h.data(), sizeof(float2) * (L / 2), cudaMemcpyHostToDevice));
+}
+
+// Coefficients of Weideman's N = 32 rational approximation of w(z) (SIAM J. Numer. Anal. 31, 1994), from the
+// paper's construction: a_m = Re(DFT of f(t_k) = exp(-t_k^2)(L^2 + t_k^2) on t_k = L tan(k pi / 2M))_m / 2M.
+void upload_weideman() {
+    constexpr int N = kWeidemanN, M = 2 * N, M2 = 2 * M;
+    const double pi = 3.141592653589793238462643;
+    double h[N + 1];
+    const double L = std::sqrt((double)N / std::sqrt(2.0));
+    h[0] = L;
+    double f[M2];
+    for (int idx = 0; idx < M2; ++idx) {
+        const int k = idx - M;
+        if (k == -M) { f[idx] = 0.0; continue; }
+        const double t = L * std::tan(0.5 * (double)k * pi / (double)M);
+        f[idx] = std::exp(-t * t) * (L * L + t * t);
+    }
+    for (int m = 1; m <= N; ++m) {
+        double re = 0.0;
+        for (int n = 0; n < M2; ++n) re += f[(n + M) % M2] * std::cos(2.0 * pi * (double)((long)m * n % M2) / (double)M2);
+        h[1 + N - m] = re / (double)M2;
+    }
+    CK(cudaMemcpyToSymbol(c_weideman, h, sizeof h));
 }
 
 long long padded_total(long long n, int ns) { return n + (long long)ns * kAlign; }
@@ -849,6 +887,19 @@ void CollideJob::run() {
     C.lum_parts = c->lum_parts.p;
     C.lum_partial = c->lum_partial.p;
     C.nodes = c->nodes.p;
+    const bool gaussian = c->dopt.gaussian != 0;
+    if (gaussian) {
+        c->hyb.ensure(std::max(ntasks, 1));
+        c->hmom.ensure((size_t)std::max(ntasks, 1) * kMaxBoundBlocks * kMomentSums);
+        c->qtot.ensure(max_planes);
+        c->hprof.ensure((size_t)max_planes * (nx + ny));
+        c->hsum.ensure((size_t)max_planes * 2);
+        C.hyb = c->hyb.p;
+        C.hmom = c->hmom.p;
+        C.qtot = c->qtot.p;
+        C.hprof = c->hprof.p;
+        C.hsum = c->hsum.p;
+    }
 
     const size_t dep_bytes = c->dopt.dep_global ? 0 : cells * sizeof(long long);
     const size_t lum_bytes = c->dopt.lum_global ? 0 : lcells * sizeof(long long);
@@ -859,25 +910,30 @@ void CollideJob::run() {
         double slice_bytes = 0.0, src_bytes = 0.0, fld_bytes = 0.0;
         for (int t = F.t0; t < F.t0 + F.nt; t += 2) slice_bytes += (double)(tasks[t].src_n + tasks[t].fld_n);
         for (int t = F.t0; t < F.t0 + F.nt; ++t) { src_bytes += (double)tasks[t].src_n; fld_bytes += (double)tasks[t].fld_n; }
+        const unsigned bps = (unsigned)std::max<long long>(1, std::min<long long>(kMaxBoundBlocks, (F.maxsrc + 2047) / 2048));
         if (!node || compute_lum) {
-            PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, 1, slice_bytes * 5 * rsz);
-            unsigned bps = (unsigned)std::max<long long>(1, std::min<long long>(128, (F.maxsrc + 2047) / 2048));
+            PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, gaussian ? 2 : 1, slice_bytes * 5 * rsz);
             with_real(fp32, [&](auto r) {
                 using R = decltype(r);
                 if (node) k_pair_bounds<R, true><<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
                 else k_pair_bounds<R, false><<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
             });
-            launches++;
+            if (gaussian) k_hyb_moments<<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
+            launches += gaussian ? 2 : 1;
         }
         if (!node) {
             {
                 PhaseScope ps(c, OCTO_PHASE_PLAN, st, 1);
-                k_plan<<<(F.nt + 63) / 64, 64, 0, st>>>(C, F.t0, F.nt, 0);
+                k_plan<<<(F.nt + 63) / 64, 64, 0, st>>>(C, F.t0, F.nt, 0, (int)bps);
             }
-            PhaseScope ps(c, OCTO_PHASE_GREEN, st, 2);
+            PhaseScope ps(c, OCTO_PHASE_GREEN, st, gaussian ? 3 : 2);
             k_green_rows<<<dim3(NY / kGreenRows, F.nt), 128, green_smem(NX), st>>>(C, 0, F.t0, 0);
             k_green_cols<<<dim3((nx + 1 + 3) / 4, F.nt), 128, fft_smem(NY), st>>>(C, 0, F.t0, 0);
-            launches += 3;
+            if (gaussian) {
+                k_hyb_profiles<<<F.np, 256, 0, st>>>(C, F.p0);
+                CK(cudaMemsetAsync(c->qtot.p, 0, sizeof(unsigned long long) * F.np, st));
+            }
+            launches += gaussian ? 4 : 3;
         }
         if (compute_lum && F.nl) {
             PhaseScope ps(c, OCTO_PHASE_LUMINOSITY, st, 4, slice_bytes * 4 * rsz);
@@ -1062,9 +1118,13 @@ octo_ctx *octo_create(int32_t device, const octo_pic_options *options) {
     d.quantize = options->grid_quantize;
     d.min_ratio = options->green_min_ratio;
     d.growth = options->green_growth;
+    d.gaussian = options->gaussian != 0;
+    d.neutralize = options->neutralize != 0;
+    d.margin = options->margin_sigma;
     try {
         CK(cudaSetDevice(device));
         c->fp32 = options->precision == 1;
+        if (d.gaussian) upload_weideman();
         upload_twiddles(c->tw_x, 2 * options->nx);
         upload_twiddles(c->tw_y, 2 * options->ny);
         if (c->fp32) {
@@ -1110,6 +1170,7 @@ void octo_destroy(octo_ctx *c) {
     c->nodenan.release(); c->status.release(); c->ghat.release(); c->qgrid.release(); c->lq.release();
     c->spec.release(); c->fields.release(); c->lum_parts.release(); c->lum_partial.release(); c->node_ref.release(); c->stats.release();
     c->partial.release(); c->soa_ptrs.release();
+    c->hyb.release(); c->hmom.release(); c->hprof.release(); c->hsum.release(); c->qtot.release();
     c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_noderef.release(); c->h_slices.release();
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     delete c;

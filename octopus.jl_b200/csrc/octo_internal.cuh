@@ -220,7 +220,20 @@ struct DevOptions {
     int nx, ny, method, lum_method, lnx, lny;
     int green_type, green_cache, fourth, quadratic, node, longitudinal_kick;
     int dep_global, lum_global;  // charge / luminosity grid larger than shared memory: global atomics
+    int gaussian, neutralize;    // GaussianPICPoissonSolver (Gaussian-subtracted hybrid)
     double min_ex, min_ey, quantize, min_ratio, growth;
+    double margin;               // hybrid: Gaussian containment half-width in sigmas
 };
+
+// Gaussian-subtracted hybrid state of one directed task (gaussian_pic.jl:604-705): the drifted reference
+// Gaussian of the source slice at the two boundaries of the field slice ([0]: sL, [1]: sR).
+struct HybridTask {
+    int32_t mode;  // 1: subtraction and analytic add-back; 0: plain PIC (degenerate moments)
+    int32_t pad;
+    double half_ns, mpx, mpy;
+    double mux[2], muy[2], sigx[2], sigy[2], rx[2], ry[2];
+};
+constexpr int kMomentSums = 10;     // sums of dx, dpx, dy, dpy, dx^2, dpx^2, dy^2, dpy^2, dx dpx, dy dpy
+constexpr int kMaxBoundBlocks = 128;  // blocks per slice of the bounds / moments passes
 
 }  // namespace octo

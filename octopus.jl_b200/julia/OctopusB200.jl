@@ -47,7 +47,7 @@ struct OctoPicOptions
     positions1::Ptr{Float64}; positions2::Ptr{Float64}
     has_kbb1::Int32; has_kbb2::Int32; has_lum_scale::Int32
     kbb1::Float64; kbb2::Float64; lum_scale::Float64
-    precision::Int32; reserved::NTuple{7,Int32}
+    precision::Int32; gaussian::Int32; margin_sigma::Float64; neutralize::Int32; reserved::NTuple{3,Int32}
 end
 
 # include/octo_b200.h: octo_collide_report
@@ -77,7 +77,7 @@ function _slicing_fields(s::LongitudinalSlicing)
             s.center_position === :centroid ? Int32(0) : Int32(1))
 end
 
-function _options(p::PICPoissonSolver, keep::Vector{Any}, precision::Integer=0)
+function _options(p::PICPoissonSolver, keep::Vector{Any}, precision::Integer=0, gaussian=nothing)
     m1, n1, c1 = _slicing_fields(p.slicing1)
     m2, n2, c2 = _slicing_fields(p.slicing2)
     pos1 = Float64.(p.slicing1.positions); pos2 = Float64.(p.slicing2.positions)
@@ -99,7 +99,9 @@ function _options(p::PICPoissonSolver, keep::Vector{Any}, precision::Integer=0)
         isempty(pos1) ? Ptr{Float64}(C_NULL) : pointer(pos1), isempty(pos2) ? Ptr{Float64}(C_NULL) : pointer(pos2),
         Int32(p.kbb1 !== nothing), Int32(p.kbb2 !== nothing), Int32(p.luminosity_scale !== nothing),
         p.kbb1 === nothing ? 0.0 : Float64(p.kbb1), p.kbb2 === nothing ? 0.0 : Float64(p.kbb2),
-        p.luminosity_scale === nothing ? 0.0 : Float64(p.luminosity_scale), Int32(precision), ntuple(_ -> Int32(0), 7))
+        p.luminosity_scale === nothing ? 0.0 : Float64(p.luminosity_scale), Int32(precision),
+        Int32(gaussian !== nothing), gaussian === nothing ? 5.0 : Float64(gaussian.margin_sigma),
+        Int32(gaussian === nothing ? 1 : gaussian.neutralize), ntuple(_ -> Int32(0), 3))
 end
 
 """Context: device workspaces and the slice-pair Green cache (the twin of task.runtime_cache)."""

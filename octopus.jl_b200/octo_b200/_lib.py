@@ -61,7 +61,10 @@ class OctoPicOptions(C.Structure):
         ("has_kbb1", C.c_int32), ("has_kbb2", C.c_int32), ("has_lum_scale", C.c_int32),
         ("kbb1", C.c_double), ("kbb2", C.c_double), ("lum_scale", C.c_double),
         ("precision", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("gaussian", C.c_int32),
+        ("margin_sigma", C.c_double),
+        ("neutralize", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 

@@ -9,6 +9,7 @@ implement are rejected when the solver is bound to the backend (the reference's
 from __future__ import annotations
 
 import ctypes as C
+import math
 from dataclasses import dataclass, field
 from typing import Optional, Sequence, Tuple
 
@@ -208,3 +209,58 @@ def _require_gpu_options(s: PICPoissonSolver):
     if not all(fft_ok(n) for n in s.grid) or s.grid[1] % 8:
         raise ArgumentError("the GPU PIC backend's FFT needs grid dimensions of the form 2^a or 3*2^a in 8..512, "
                             f"ny a multiple of 8; got {s.grid}")
+
+
+class GaussianPICPoissonSolver:
+    """GaussianPICPoissonSolver(; margin_sigma=5.0, neutralize=true, coupling_tol=Inf, kwargs...)
+    (gaussian_pic.jl:87-112): a PICPoissonSolver built from the remaining keywords, whose slice-pair
+    interactions subtract the drifted reference Gaussian of each source slice before the solve and add its
+    Bassetti-Erskine kick back analytically.  The PIC options the hybrid does not read must keep their
+    defaults (gaussian_pic.jl:162-164); this backend implements the default uncoupled subtraction
+    (coupling_tol = Inf)."""
+
+    def __init__(self, margin_sigma: float = 5.0, neutralize: bool = True, coupling_tol: float = math.inf,
+                 **kwargs):
+        pic = kwargs.pop("pic", None) or PICPoissonSolver(**kwargs)
+        if not float(margin_sigma) >= 0.0:
+            raise ArgumentError(f"margin_sigma must be non-negative; got {margin_sigma}.")
+        if not float(coupling_tol) >= 0.0:
+            raise ArgumentError(f"coupling_tol must be non-negative; got {coupling_tol}.")
+        self.pic = pic
+        self.margin_sigma = float(margin_sigma)
+        self.neutralize = bool(neutralize)
+        self.coupling_tol = float(coupling_tol)
+
+    def __getattr__(self, name):  # the embedded PIC solver's options
+        if name == "pic":
+            raise AttributeError(name)
+        return getattr(self.pic, name)
+
+    def _key(self):
+        return (self.pic, self.margin_sigma, self.neutralize, self.coupling_tol)
+
+    def __eq__(self, other):
+        return isinstance(other, GaussianPICPoissonSolver) and self._key() == other._key()
+
+    def __hash__(self):
+        return hash(("GaussianPICPoissonSolver",) + self._key())
+
+    def replace(self, **pic_changes) -> "GaussianPICPoissonSolver":
+        from dataclasses import replace
+        return GaussianPICPoissonSolver(self.margin_sigma, self.neutralize, self.coupling_tol,
+                                        pic=replace(self.pic, **pic_changes))
+
+    def to_c(self) -> "_lib.OctoPicOptions":
+        p = self.pic
+        if p.slice_interpolation != "linear" or p.interaction_grid != "slice_pair" or p.grid_extent != "extrema":
+            raise ArgumentError(
+                "GaussianPICPoissonSolver does not read slice_interpolation, interaction_grid or grid_extent: it "
+                "interpolates linearly on its own :slice_pair box (gaussian_pic.jl:162-164); keep their defaults.")
+        if math.isfinite(self.coupling_tol):
+            raise ArgumentError("coupling_tol < Inf (the coupled, rotated subtraction) is not implemented by this "
+                                "backend; use the default uncoupled subtraction.")
+        o = p.to_c()
+        o.gaussian = 1
+        o.margin_sigma = self.margin_sigma
+        o.neutralize = int(self.neutralize)
+        return o

@@ -46,7 +46,9 @@ def oracle_options(solver, nthreads=8, fixed=False):
         center_position1=s1.center_position, center_position2=s2.center_position,
         positions1=list(s1.positions), positions2=list(s2.positions),
         kbb1=solver.kbb1, kbb2=solver.kbb2, luminosity_scale=solver.luminosity_scale,
-        fixed_point_deposit=fixed, nthreads=nthreads)
+        fixed_point_deposit=fixed, nthreads=nthreads,
+        gaussian=hasattr(solver, "margin_sigma"), neutralize=getattr(solver, "neutralize", True),
+        margin_sigma=getattr(solver, "margin_sigma", 5.0))
 
 
 def within(a, b, atol, rtol):

@@ -150,3 +150,49 @@ def test_node_mode_96():
     s = ob.PICPoissonSolver(grid=(96, 96), interaction_grid="node", deposit_method="TSC",
                             slicing=ob.LongitudinalSlicing(nslices=5, method="normal_quantile"))
     check(run_both(s, 12000, 8000, turns=2, e_sigma=(95e-6, 8.5e-6, 0.7e-2), p_sigma=(95e-6, 8.5e-6, 6e-2)))
+
+
+@pytest.mark.parametrize("opts", [
+    dict(),
+    dict(deposit_method="TSC", field_derivative="fourth"),
+    dict(neutralize=False, margin_sigma=0.0),
+    dict(longitudinal_kick=False),
+    dict(green_cache="none", grid=(48, 48)),
+])
+def test_gaussian_hybrid(opts):
+    """GaussianPICPoissonSolver (gaussian_pic.jl) against the oracle's hybrid at the contract tolerance."""
+    ob = _gpu()
+    kw = dict(grid=(64, 64), slicing=ob.LongitudinalSlicing(nslices=4, method="normal_quantile"))
+    kw.update(opts)
+    s = ob.GaussianPICPoissonSolver(**kw)
+    check(run_both(s, 6000, 4000, turns=2, e_sigma=(95e-6, 8.5e-6, 7e-3), p_sigma=(95e-6, 8.5e-6, 6e-2)))
+
+
+def test_gaussian_hybrid_round_beams():
+    """Near-round drifted slices exercise the round, near-round-series and blend regimes of the add-back."""
+    ob = _gpu()
+    s = ob.GaussianPICPoissonSolver(grid=(48, 48), slicing=ob.LongitudinalSlicing(nslices=3, method="normal_quantile"))
+    check(run_both(s, 8000, 8000, turns=2, e_sigma=(50e-6, 50e-6, 7e-3), p_sigma=(50e-6, 50e-6, 6e-2)))
+
+
+@pytest.mark.parametrize("c", [1.0, 1.0 + 1e-4, 1.0 + 3e-4])
+def test_gaussian_hybrid_near_round_regimes(c):
+    """Source slices with y = c x, py = c px have sigma_y / sigma_x = c exactly at every drift, so the add-back
+    runs the round closed form (c = 1), the near-round series (eta ~ 1e-4) and the blend (eta ~ 3e-4)."""
+    from oracle import oracle as orc
+    ob = _gpu()
+    e, p = beams(6000, 5000, (60e-6, 60e-6, 7e-3), (60e-6, 60e-6, 6e-2))
+    for b in (e, p):
+        b[2] = c * b[0]
+        b[3] = c * b[1]
+    be, bp = _device_beams(ob, e, p)
+    s = ob.GaussianPICPoissonSolver(grid=(48, 48), slicing=ob.LongitudinalSlicing(nslices=2, method="normal_quantile"))
+    rt = ob.StrongStrongRuntime()
+    ctx = rt.context("ip", s, 0)
+    oracle = orc.Oracle(oracle_options(s))
+    pe, pp = oracle_params()
+    lum_g = ctx.collide(be, bp, turn=1)
+    lum_o = oracle.collide(e, p, pe, pp)
+    assert abs(lum_g / lum_o - 1) <= 1e-10
+    assert within(be.numpy(), e, ATOL, RTOL) <= 1.0 and within(bp.numpy(), p, ATOL, RTOL) <= 1.0
+    rt.close()
