@@ -68,6 +68,25 @@ struct B200PICPoissonSolver{T<:Real} <: AbstractPoissonSolver
 end
 B200PICPoissonSolver(; kwargs...) = B200PICPoissonSolver(PICPoissonSolver(; kwargs...))
 
+"""
+    B200GaussianPICPoissonSolver(; margin_sigma=5.0, neutralize=true, coupling_tol=Inf, kwargs...)
+
+`GaussianPICPoissonSolver(; ...)` (gaussian_pic.jl:87-112) run on libocto_b200 (the uncoupled subtraction).
+"""
+struct B200GaussianPICPoissonSolver{T<:Real} <: AbstractPoissonSolver
+    gpic::GaussianPICPoissonSolver{T}
+    pic::PICPoissonSolver{T}
+end
+function B200GaussianPICPoissonSolver(; kwargs...)
+    g = GaussianPICPoissonSolver(; kwargs...)
+    isfinite(g.coupling_tol) && throw(ArgumentError(
+        "coupling_tol < Inf (the coupled subtraction) is not implemented by the B200 backend"))
+    return B200GaussianPICPoissonSolver(g, g.pic)
+end
+const B200Solver = Union{B200PICPoissonSolver,B200GaussianPICPoissonSolver}
+_gaussian_of(::B200PICPoissonSolver) = nothing
+_gaussian_of(s::B200GaussianPICPoissonSolver) = s.gpic
+
 _sym(v, table) = Int32(table[Symbol(v)])
 
 function _slicing_fields(s::LongitudinalSlicing)
@@ -108,9 +127,9 @@ end
 mutable struct Context
     ptr::Ptr{Cvoid}
     # T = Float64: the plain form; T = Float32: the precision form (FP32 particles, planes and FFTs)
-    function Context(p::PICPoissonSolver, ::Type{T}=Float64) where {T<:Union{Float32,Float64}}
+    function Context(p::PICPoissonSolver, ::Type{T}=Float64, gaussian=nothing) where {T<:Union{Float32,Float64}}
         keep = Any[]
-        opts = Ref(_options(p, keep, T === Float32 ? 1 : 0))
+        opts = Ref(_options(p, keep, T === Float32 ? 1 : 0, gaussian))
         ptr = GC.@preserve keep ccall((:octo_create, LIB), Ptr{Cvoid}, (Int32, Ref{OctoPicOptions}),
                                       Int32(CUDA.device().handle), opts)
         ptr == C_NULL && error("octo_create failed")
@@ -134,7 +153,7 @@ _octo_beam(b::Beam) = OctoBeam(Int64(length(b.rep.x)), Int32(eltype(b.rep.x) ===
 _octo_params(b::Beam) = OctoBeamParams(Float64(b.params.charge), Float64(b.params.mc2), Float64(b.params.E0),
                                        Float64(b.params.r0), Float64(b.params.npart))
 
-function _collide!(ctx::Context, solver::B200PICPoissonSolver, beam1::Beam, beam2::Beam, turn::Integer)
+function _collide!(ctx::Context, solver::B200Solver, beam1::Beam, beam2::Beam, turn::Integer)
     eltype(beam1.rep.x) === eltype(beam2.rep.x) && eltype(beam1.rep.x) in (Float32, Float64) || throw(ArgumentError(
         "the B200 backend takes two Float64 (plain form) or two Float32 (precision form) beams"))
     b1 = Ref(_octo_beam(beam1)); b2 = Ref(_octo_beam(beam2))
@@ -153,9 +172,9 @@ end
 
 """collide!(solver, beam1, beam2, CUDABackend[, ctx]) on libocto_b200: a fresh (cold) context per call,
 as the reference's public collide! builds a fresh Green cache (pic_cuda.jl:94-126)."""
-function Octopus.collide!(solver::B200PICPoissonSolver, beam1::Beam, beam2::Beam, ::Type{CUDABackend},
+function Octopus.collide!(solver::B200Solver, beam1::Beam, beam2::Beam, ::Type{CUDABackend},
                           ctx::Union{Nothing,TrackingContext}=nothing)
-    c = Context(solver.pic, eltype(beam1.rep.x))
+    c = Context(solver.pic, eltype(beam1.rep.x), _gaussian_of(solver))
     try
         return _collide!(c, solver, beam1, beam2, ctx === nothing ? -1 : ctx.turn)
     finally
@@ -165,14 +184,14 @@ end
 
 # Task path: one persistent context per (label, solver) in task.runtime_cache (pic_cuda.jl:127-137).
 function Octopus._strong_strong_collide_backend!(task::StrongStrongTask, label::Symbol,
-                                                 solver::B200PICPoissonSolver, beam1::Beam, beam2::Beam,
+                                                 solver::B200Solver, beam1::Beam, beam2::Beam,
                                                  ::Type{CUDABackend}, ctx::TrackingContext)
     T = eltype(beam1.rep.x)
     key = (:octo_b200_context, label, T, solver.pic.grid, objectid(solver))
-    c = get!(() -> Context(solver.pic, T), task.runtime_cache, key)::Context
+    c = get!(() -> Context(solver.pic, T, _gaussian_of(solver)), task.runtime_cache, key)::Context
     return _collide!(c, solver, beam1, beam2, ctx.turn)
 end
 
-Octopus._pic_compute_luminosity(solver::B200PICPoissonSolver, ctx) = Octopus._pic_compute_luminosity(solver.pic, ctx)
+Octopus._pic_compute_luminosity(solver::B200Solver, ctx) = Octopus._pic_compute_luminosity(solver.pic, ctx)
 
 end # module
