@@ -16,7 +16,7 @@ module OctopusB200
 
 using CUDA
 import Octopus
-using Octopus: Beam, CUDABackend, TrackingContext, PICPoissonSolver, LongitudinalSlicing,
+using Octopus: Beam, CUDABackend, TrackingContext, PICPoissonSolver, GaussianPICPoissonSolver, LongitudinalSlicing,
                AbstractPoissonSolver, StrongStrongTask
 
 const LIB = get(ENV, "OCTO_B200_LIB", joinpath(@__DIR__, "..", "build", "libocto_b200.so"))
