@@ -179,6 +179,17 @@ __global__ void __launch_bounds__(256) k_hyb_moments(Collide C, int task0) {
     }
 }
 
+// Fold the per-block moment partials of each task, in block order, into slot 0 (one warp per task: lane k
+// sums quantity k over the blocks).
+__global__ void k_hyb_fold(Collide C, int task0, int ntasks, int nblk) {
+    const int tl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (tl >= ntasks || lane >= kMomentSums) return;
+    double *m = C.hmom + (long long)(task0 + tl) * kMaxBoundBlocks * kMomentSums;
+    double v = 0.0;
+    for (int b = 0; b < nblk; ++b) v += m[b * kMomentSums + lane];
+    m[lane] = v;
+}
+
 // Drifted reference Gaussian of the source at drift s (gaussian_pic.jl:496-540, uncoupled).
 __device__ __forceinline__ void hyb_boundary(const double m[10], double s, HybridTask &H, int side) {
     // m: mx, mpx, varx, cxpx, varpx, my, mpy, vary, cypy, varpy
@@ -198,9 +209,9 @@ __device__ inline void record_error(DevStatus *st, int task, int code, int role)
 }
 
 // Grid geometry and Green-cache decision per task (pic_cpu.jl:954-1064, 1729-1821).  Hybrid: the source
-// moments (nblk block partials), the reference Gaussians at both boundaries, the plain-PIC fallback test and
-// the margin box around the Gaussians joined to the source extent (gaussian_pic.jl:604-660).
-__global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0, int nblk) {
+// moments (folded by k_hyb_fold), the reference Gaussians at both boundaries, the plain-PIC fallback test
+// and the margin box around the Gaussians joined to the source extent (gaussian_pic.jl:604-660).
+__global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0) {
     int tl = blockIdx.x * blockDim.x + threadIdx.x;
     if (tl >= ntasks) return;
     int t = task0 + tl;
@@ -223,10 +234,8 @@ __global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0, int 
     if (C.o.gaussian) {
         HybridTask &H = C.hyb[t];
         H.mode = 0;
-        double sum[kMomentSums];
-        for (int k = 0; k < kMomentSums; ++k) sum[k] = 0.0;
-        for (int b = 0; b < nblk; ++b)
-            for (int k = 0; k < kMomentSums; ++k) sum[k] += C.hmom[((long long)t * kMaxBoundBlocks + b) * kMomentSums + k];
+        double sum[kMomentSums];  // folded by k_hyb_fold
+        for (int k = 0; k < kMomentSums; ++k) sum[k] = C.hmom[(long long)t * kMaxBoundBlocks * kMomentSums + k];
         const SoA S = C.beam[T.src_beam];
         const long long st = T.src_start, n = T.src_n;
         const double x0 = col<double>(S, 0)[st], px0 = col<double>(S, 1)[st], y0 = col<double>(S, 2)[st],
@@ -832,14 +841,27 @@ __global__ void __launch_bounds__(128) k_conv_cols(Collide C, int plane0) {
     for (int j = lane; j < ny; j += 32) col[j] = dst[j];
 }
 
-// Field planes: a cell is (phi, Ex), (Ey, 0) as two double2 (plain form) or one float4 (precision
-// form), so one tap of one plane is one 32-byte or 16-byte access.
+// Field planes: a cell is (phi, Ex, Ey, w) as two double2 (plain form) or one float4 (precision form), so
+// one tap of one plane is one 32-byte or 16-byte access.  The fourth word w of an L plane in :node mode
+// carries phi of the task's Z plane (written by the Z plane's own k_conv_field block), so the L-mesh taps
+// of the kick read phi_L, Ex_L, Ey_L and phi_Z in that one access.
 __device__ __forceinline__ void store_cell(double2 *F, long long o, double phi, double ex, double ey) {
     F[2 * o] = make_double2(phi, ex);
-    F[2 * o + 1] = make_double2(ey, 0.0);
+    reinterpret_cast<double *>(F)[4 * o + 2] = ey;
 }
 __device__ __forceinline__ void store_cell(float4 *F, long long o, float phi, float ex, float ey) {
-    F[o] = make_float4(phi, ex, ey, 0.f);
+    reinterpret_cast<float2 *>(F)[2 * o] = make_float2(phi, ex);
+    reinterpret_cast<float *>(F)[4 * o + 2] = ey;
+}
+__device__ __forceinline__ void store_w(double2 *F, long long o, double w) { reinterpret_cast<double *>(F)[4 * o + 3] = w; }
+__device__ __forceinline__ void store_w(float4 *F, long long o, float w) { reinterpret_cast<float *>(F)[4 * o + 3] = w; }
+__device__ __forceinline__ void load_cell4(const double2 *F, long long c, double &phi, double &ex, double &ey, double &w) {
+    const double2 a = F[2 * c], b = F[2 * c + 1];
+    phi = a.x; ex = a.y; ey = b.x; w = b.y;
+}
+__device__ __forceinline__ void load_cell4(const float4 *F, long long c, float &phi, float &ex, float &ey, float &w) {
+    const float4 v = F[c];
+    phi = v.x; ex = v.y; ey = v.z; w = v.w;
 }
 __device__ __forceinline__ void load_cell(const double2 *F, long long c, double &phi, double &ex, double &ey) {
     const double2 a = F[2 * c], b = F[2 * c + 1];
@@ -849,8 +871,6 @@ __device__ __forceinline__ void load_cell(const float4 *F, long long c, float &p
     const float4 v = F[c];
     phi = v.x; ex = v.y; ey = v.z;
 }
-__device__ __forceinline__ double load_phi(const double2 *F, long long c) { return F[2 * c].x; }
-__device__ __forceinline__ float load_phi(const float4 *F, long long c) { return F[c].x; }
 
 // Inverse x-transform (two Hermitian rows per complex line) producing phi for a tile of rows plus a
 // two-row halo, then E = -grad(phi) on the tile (pic_cpu.jl:2531-2591).
@@ -913,10 +933,15 @@ __global__ void __launch_bounds__(128) k_conv_field(Collide C, int plane0) {
     const R hxi = (R)(1.0 / hx), hyi = (R)(1.0 / hy);
     const R c4 = (R)(1.0 / 12.0);
     const bool fourth = C.o.fourth != 0;
-    FC *F = (FC *)C.fields + (long long)pl * RealT<R>::kCellVec * nx * ny;
+    const bool zplane = P.kind == 3;  // :node Z plane: only its phi is used, stored in its L plane's w word
+    FC *F = (FC *)C.fields + (long long)(zplane ? pl - 2 : pl) * RealT<R>::kCellVec * nx * ny;
     auto Pv = [&](int i, int j) { return phi[(j - ja0) * nx + i]; };  // 0-based i, j
     for (int idx = threadIdx.x; idx < (jt1 - jt0) * nx; idx += blockDim.x) {
         const int j = jt0 + idx / nx, i = idx % nx;
+        if (zplane) {
+            store_w(F, (long long)j * nx + i, Pv(i, j));
+            continue;
+        }
         R ey, ex;
         // Ey (pic_cpu.jl:2553-2572), 1-based j' = j+1
         if (j == 0) ey = hyi * (R(1.5) * Pv(i, 0) - R(2) * Pv(i, 1) + R(0.5) * Pv(i, 2));
@@ -1029,7 +1054,7 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
         // L on gL, R on gR, Z (the R drift deposited on gL) on gL; with zL = 1, zR = 0 the reference's
         // single-plane interpolations reduce exactly to w * E (pic_cpu.jl:1517-1528).
         const GridR<R> &gL = J.gL, &gR = J.gR;
-        const FC *FL = base, *FR = base + CV * pc, *FZ = base + 2 * CV * pc;
+        const FC *FL = base, *FR = base + CV * pc;  // the L plane's w word holds phi_Z (k_conv_field)
         if (!(isfinite(x) && gL.x0 <= x && x <= gL.x0 + gL.w && isfinite(y) && gL.y0 <= y && y <= gL.y0 + gL.h))
             atomicAdd((unsigned long long *)&C.status->dropped, 1ull);
         R KxL = 0, KyL = 0, Kz = 0, KxR = 0, KyR = 0;
@@ -1037,9 +1062,8 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
             const Taps<R, METHOD> tp(o, gL, J.hxL, J.hyL, x, y);
 #pragma unroll
             for (int t = 0; t < NT2; ++t) {
-                R phl, exl, eyl;
-                load_cell(FL, tp.cell(t, o.nx), phl, exl, eyl);
-                const R phz = load_phi(FZ, tp.cell(t, o.nx));
+                R phl, exl, eyl, phz;
+                load_cell4(FL, tp.cell(t, o.nx), phl, exl, eyl, phz);
                 KxL += tp.w[t] * exl;
                 KyL += tp.w[t] * eyl;
                 if (kPrecision) Kz += tp.w[t] * phz;  // the Z plane holds phi_L - phi_Z

@@ -918,13 +918,16 @@ void CollideJob::run() {
                 if (node) k_pair_bounds<R, true><<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
                 else k_pair_bounds<R, false><<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
             });
-            if (gaussian) k_hyb_moments<<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
-            launches += gaussian ? 2 : 1;
+            if (gaussian) {
+                k_hyb_moments<<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
+                k_hyb_fold<<<(F.nt * 32 + 127) / 128, 128, 0, st>>>(C, F.t0, F.nt, (int)bps);
+            }
+            launches += gaussian ? 3 : 1;
         }
         if (!node) {
             {
                 PhaseScope ps(c, OCTO_PHASE_PLAN, st, 1);
-                k_plan<<<(F.nt + 63) / 64, 64, 0, st>>>(C, F.t0, F.nt, 0, (int)bps);
+                k_plan<<<(F.nt + 63) / 64, 64, 0, st>>>(C, F.t0, F.nt, 0);
             }
             PhaseScope ps(c, OCTO_PHASE_GREEN, st, gaussian ? 3 : 2);
             k_green_rows<<<dim3(NY / kGreenRows, F.nt), 128, green_smem(NX), st>>>(C, 0, F.t0, 0);

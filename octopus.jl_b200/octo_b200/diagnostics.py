@@ -64,8 +64,9 @@ def field_error(solver, sx: float, sy: float, dtype: torch.dtype = torch.float64
     from .beam import Beam, BeamParams
     from .solver import LongitudinalSlicing
 
-    s = replace(solver, kbb1=1.0, kbb2=1.0, luminosity_scale=1.0,
-                slicing=LongitudinalSlicing(nslices=1, method="normal_quantile"), slicing1=None, slicing2=None)
+    changes = dict(kbb1=1.0, kbb2=1.0, luminosity_scale=1.0,
+                   slicing=LongitudinalSlicing(nslices=1, method="normal_quantile"), slicing1=None, slicing2=None)
+    s = solver.replace(**changes) if hasattr(solver, "margin_sigma") else replace(solver, **changes)
     xs, ys = quantile_lattice(n_source, sx, sy)
     g = np.linspace(-extent, extent, n_probe)
     px_, py_ = np.meshgrid(g * sx, g * sy, indexing="ij")
