@@ -140,6 +140,48 @@ __global__ void __launch_bounds__(256) k_pair_bounds(Collide C, int task0) {
     }
 }
 
+// Block-wide reduction of a thread's virtual-position extrema into a pair's luminosity box (ordered
+// atomics) and the non-finite flag of its direction-1 task.
+template <class R>
+__device__ __forceinline__ void reduce_lum_box(Collide &C, R mnx, R mxx, R mny, R mxy, bool nan, int pair, int task) {
+    __shared__ unsigned long long red[8][4];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned long long a = shfl_min_u64(mnx == R(INFINITY) ? kOrdMinInit : ord_encode((double)mnx));
+    unsigned long long b = shfl_max_u64(mxx == R(-INFINITY) ? kOrdMaxInit : ord_encode((double)mxx));
+    unsigned long long c = shfl_min_u64(mny == R(INFINITY) ? kOrdMinInit : ord_encode((double)mny));
+    unsigned long long d = shfl_max_u64(mxy == R(-INFINITY) ? kOrdMaxInit : ord_encode((double)mxy));
+    if (lane == 0) { red[warp][0] = a; red[warp][1] = b; red[warp][2] = c; red[warp][3] = d; }
+    const int any_nan = __syncthreads_or(nan);
+    if (threadIdx.x < 4) {
+        unsigned long long r = red[0][threadIdx.x];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) r = (threadIdx.x & 1) ? max(r, red[w][threadIdx.x]) : min(r, red[w][threadIdx.x]);
+        unsigned long long *dst = C.lumb + (long long)pair * 4 + threadIdx.x;
+        if (threadIdx.x & 1) atomicMax(dst, r); else atomicMin(dst, r);
+    }
+    if (threadIdx.x == 0 && any_nan) atomicOr(&C.nanflag[task], 4);
+}
+
+// :node with luminosity, turn start: every slice's virtual positions at the drift of its first pair
+// (pic_cpu.jl:1279-1287, 2706-2712); later pairs get theirs from the kick of the slice's previous pair.
+// grid: (blocks per slice, slices of both beams).
+template <class R>
+__global__ void __launch_bounds__(256) k_first_lum_bounds(Collide C, const FirstLum *first) {
+    const FirstLum F = first[blockIdx.y];
+    const SoA S = C.beam[F.beam];
+    const R *X = col<R>(S, 0) + F.start, *PX = col<R>(S, 1) + F.start, *Y = col<R>(S, 2) + F.start,
+            *PY = col<R>(S, 3) + F.start;
+    const R s = (R)F.sM;
+    R mnx = R(INFINITY), mxx = R(-INFINITY), mny = R(INFINITY), mxy = R(-INFINITY);
+    bool nan = false;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < F.count; k += (long long)gridDim.x * blockDim.x) {
+        const R vx = X[k] + PX[k] * s, vy = Y[k] + PY[k] * s;
+        nan |= (vx != vx) | (vy != vy);
+        mnx = fmin(mnx, vx); mxx = fmax(mxx, vx);
+        mny = fmin(mny, vy); mxy = fmax(mxy, vy);
+    }
+    reduce_lum_box(C, mnx, mxx, mny, mxy, nan, F.pair, F.task);
+}
+
 // Hybrid: transverse moment sums of each task's source slice relative to its first particle
 // (gaussian_pic.jl:432-486), as per-block partials folded in block order by k_plan.  grid: (blocks per
 // side, 2 * pairs in front), the mapping of k_pair_bounds.
@@ -1007,6 +1049,8 @@ struct KickJob {
     int fld_beam, ok;
     int hyb;               // Gaussian-subtracted hybrid active for this task (FP64 only)
     HybridTask H;
+    int next_pair, next_task;  // luminosity box of the field slice's next pair (:node), or -1
+    R next_sM;
 };
 
 template <class R>
@@ -1019,7 +1063,8 @@ __device__ __forceinline__ Coord6<R> load_coord(const SoA &S, long long p) {
 }
 
 template <class R, int METHOD>
-__device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R> &J, long long p, const Coord6<R> &q) {
+__device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R> &J, long long p, const Coord6<R> &q,
+                                              R &xo, R &pxo, R &yo, R &pyo) {
     using FC = typename RealT<R>::FC;
     constexpr int CV = RealT<R>::kCellVec;
     constexpr int NT2 = Taps<R, METHOD>::NT * Taps<R, METHOD>::NT;
@@ -1170,6 +1215,7 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
         if (lk) pz += R(0.25) * (px * px + py * py);
     }
     col<R>(S, 0)[p] = x; col<R>(S, 1)[p] = px; col<R>(S, 2)[p] = y; col<R>(S, 3)[p] = py; col<R>(S, 5)[p] = pz;
+    xo = x; pxo = px; yo = y; pyo = py;
 }
 
 template <class R, int METHOD>
@@ -1205,24 +1251,40 @@ __global__ void __launch_bounds__(kKickThreads, sizeof(R) == 8 ? 1 : 4) k_kick(C
         J.fld_n = rest < (long long)kKickChunk ? rest : (long long)kKickChunk;
         J.plane_off = T.plane0 - plane0_front;
         J.fld_beam = T.fld_beam;
+        J.next_pair = C.o.node ? T.next_pair : -1;
+        J.next_task = T.next_task;
+        J.next_sM = (R)T.next_sM;
     }
     __syncthreads();
     if (!J.ok) return;
     // The next particle's coordinates are loaded before the current one is kicked, so two
-    // particles' HBM loads are in flight per thread.
+    // particles' HBM loads are in flight per thread.  In :node mode with luminosity the kicked slice's
+    // virtual positions for its next pair are reduced on the way (pic_cpu.jl:1279-1287).
     const SoA S = C.beam[J.fld_beam];
+    const bool lum_next = J.next_pair >= 0;
+    R mnx = R(INFINITY), mxx = R(-INFINITY), mny = R(INFINITY), mxy = R(-INFINITY);
+    bool nan = false;
     int k = threadIdx.x;
-    if (k >= J.fld_n) return;
-    Coord6<R> cur = load_coord<R>(S, J.fld_start + k);
-    for (;;) {
-        const int kn = k + kKickThreads;
-        Coord6<R> nxt;
-        if (kn < J.fld_n) nxt = load_coord<R>(S, J.fld_start + kn);
-        kick_particle<R, METHOD>(C, J, J.fld_start + k, cur);
-        if (kn >= J.fld_n) break;
-        cur = nxt;
-        k = kn;
+    if (k < J.fld_n) {
+        Coord6<R> cur = load_coord<R>(S, J.fld_start + k);
+        for (;;) {
+            const int kn = k + kKickThreads;
+            Coord6<R> nxt;
+            if (kn < J.fld_n) nxt = load_coord<R>(S, J.fld_start + kn);
+            R x, px, y, py;
+            kick_particle<R, METHOD>(C, J, J.fld_start + k, cur, x, px, y, py);
+            if (lum_next) {
+                const R vx = x + px * J.next_sM, vy = y + py * J.next_sM;
+                nan |= (vx != vx) | (vy != vy);
+                mnx = fmin(mnx, vx); mxx = fmax(mxx, vx);
+                mny = fmin(mny, vy); mxy = fmax(mxy, vy);
+            }
+            if (kn >= J.fld_n) break;
+            cur = nxt;
+            k = kn;
+        }
     }
+    if (lum_next) reduce_lum_box(C, mnx, mxx, mny, mxy, nan, J.next_pair, J.next_task);
 }
 
 // ------------------------------------------------------------------ node meshes

@@ -189,6 +189,7 @@ struct octo_ctx {
     DevBuf<LumJob> lumjobs;
     DevBuf<TaskGeom> geom;
     DevBuf<int2> blockmap;
+    DevBuf<FirstLum> first_lum;
     DevBuf<CacheEntry> cache;
     DevBuf<NodeMesh> nodes;
     DevBuf<LumGeom> lumgeom;
@@ -827,6 +828,45 @@ void CollideJob::run() {
     }
     ntasks = (int)tasks.size();
     npairs_total = (int)order.size();
+    // :node with luminosity: each kick reduces its field slice's virtual positions for that slice's next pair,
+    // and one turn-start pass covers every slice's first pair (no per-front bounds pass).
+    for (auto &T : tasks) { T.next_pair = -1; T.next_task = -1; T.next_sM = 0.0; }
+    std::vector<FirstLum> first_lum;
+    const bool fused_lum_bounds = node && compute_lum;
+    if (fused_lum_bounds) {
+        // lumjob k belongs to tasks 2k (direction 1) and 2k + 1
+        std::vector<std::vector<int>> lj_of[2];
+        lj_of[0].resize(ns1);
+        lj_of[1].resize(ns2);
+        for (int k = 0; k < (int)lumjobs.size(); ++k) {
+            lj_of[0][tasks[2 * k].i - 1].push_back(k);
+            lj_of[1][tasks[2 * k].j - 1].push_back(k);
+        }
+        for (int t = 0; t < ntasks; ++t) {
+            Task &T = tasks[t];
+            const int fb = T.fld_beam, sl = fb == 0 ? T.i - 1 : T.j - 1;
+            const std::vector<int> &L = lj_of[fb][sl];
+            const auto it = std::upper_bound(L.begin(), L.end(), t / 2);
+            if (it == L.end()) continue;
+            const LumJob &J = lumjobs[*it];
+            T.next_pair = J.pair;
+            T.next_task = 2 * *it;
+            T.next_sM = fb == 0 ? J.sM1 : J.sM2;
+        }
+        for (int b = 0; b < 2; ++b)
+            for (int sl = 0; sl < (b == 0 ? ns1 : ns2); ++sl) {
+                if (lj_of[b][sl].empty()) continue;
+                const LumJob &J = lumjobs[lj_of[b][sl][0]];
+                FirstLum F{};
+                F.start = b == 0 ? J.s1_start : J.s2_start;
+                F.count = b == 0 ? J.s1_n : J.s2_n;
+                F.sM = b == 0 ? J.sM1 : J.sM2;
+                F.beam = b;
+                F.pair = J.pair;
+                F.task = 2 * lj_of[b][sl][0];
+                first_lum.push_back(F);
+            }
+    }
     int max_planes = 1, max_lum = 1;
     for (auto &F : fronts) { max_planes = std::max(max_planes, F.np); max_lum = std::max(max_lum, F.nl); }
 
@@ -854,8 +894,9 @@ void CollideJob::run() {
         c->lq.ensure((size_t)2 * max_lum * lcells);
         CK(cudaMemsetAsync(c->lq.p, 0, sizeof(long long) * c->lq.n, st));
     }
+    c->first_lum.ensure(std::max<size_t>(first_lum.size(), 1));
     const size_t bytes = sizeof(Task) * tasks.size() + sizeof(Plane) * planes.size() + sizeof(LumJob) * lumjobs.size() +
-                         sizeof(int2) * blockmap.size() + 64;
+                         sizeof(int2) * blockmap.size() + sizeof(FirstLum) * first_lum.size() + 64;
     c->stage.ensure(bytes);
     char *h = c->stage.p;
     auto put = [&](void *dst, const void *src, size_t nbytes) {
@@ -868,6 +909,7 @@ void CollideJob::run() {
     put(c->planes.p, planes.data(), sizeof(Plane) * planes.size());
     put(c->lumjobs.p, lumjobs.data(), sizeof(LumJob) * lumjobs.size());
     put(c->blockmap.p, blockmap.data(), sizeof(int2) * blockmap.size());
+    put(c->first_lum.p, first_lum.data(), sizeof(FirstLum) * first_lum.size());
     CK(cudaMemsetAsync(c->lum_parts.p, 0, sizeof(double) * npairs_total, st));
     k_init_bounds<<<(std::max(ntasks, npairs_total) + 255) / 256, 256, 0, st>>>(c->bnd.p, ntasks, c->lumb.p, npairs_total,
                                                                                 c->nanflag.p, c->status.p, 0);
@@ -901,6 +943,17 @@ void CollideJob::run() {
         C.hsum = c->hsum.p;
     }
 
+    if (!first_lum.empty()) {
+        PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, 1, (double)(n1 + n2) * 4 * rsz);
+        long long maxn = 1;
+        for (auto &F : first_lum) maxn = std::max<long long>(maxn, F.count);
+        const unsigned bx = (unsigned)std::max<long long>(1, std::min<long long>(kMaxBoundBlocks, (maxn + 2047) / 2048));
+        with_real(fp32, [&](auto r) {
+            k_first_lum_bounds<decltype(r)><<<dim3(bx, (unsigned)first_lum.size()), 256, 0, st>>>(C, c->first_lum.p);
+        });
+        launches += 1;
+    }
+
     const size_t dep_bytes = c->dopt.dep_global ? 0 : cells * sizeof(long long);
     const size_t lum_bytes = c->dopt.lum_global ? 0 : lcells * sizeof(long long);
 
@@ -911,13 +964,9 @@ void CollideJob::run() {
         for (int t = F.t0; t < F.t0 + F.nt; t += 2) slice_bytes += (double)(tasks[t].src_n + tasks[t].fld_n);
         for (int t = F.t0; t < F.t0 + F.nt; ++t) { src_bytes += (double)tasks[t].src_n; fld_bytes += (double)tasks[t].fld_n; }
         const unsigned bps = (unsigned)std::max<long long>(1, std::min<long long>(kMaxBoundBlocks, (F.maxsrc + 2047) / 2048));
-        if (!node || compute_lum) {
+        if (!node) {
             PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, gaussian ? 2 : 1, slice_bytes * 5 * rsz);
-            with_real(fp32, [&](auto r) {
-                using R = decltype(r);
-                if (node) k_pair_bounds<R, true><<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
-                else k_pair_bounds<R, false><<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
-            });
+            with_real(fp32, [&](auto r) { k_pair_bounds<decltype(r), false><<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0); });
             if (gaussian) {
                 k_hyb_moments<<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
                 k_hyb_fold<<<(F.nt * 32 + 127) / 128, 128, 0, st>>>(C, F.t0, F.nt, (int)bps);
@@ -1173,6 +1222,7 @@ void octo_destroy(octo_ctx *c) {
     c->nodenan.release(); c->status.release(); c->ghat.release(); c->qgrid.release(); c->lq.release();
     c->spec.release(); c->fields.release(); c->lum_parts.release(); c->lum_partial.release(); c->node_ref.release(); c->stats.release();
     c->partial.release(); c->soa_ptrs.release();
+    c->first_lum.release();
     c->hyb.release(); c->hmom.release(); c->hprof.release(); c->hsum.release(); c->qtot.release();
     c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_noderef.release(); c->h_slices.release();
     for (auto e : c->ev_pool) cudaEventDestroy(e);

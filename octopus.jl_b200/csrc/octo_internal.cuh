@@ -35,6 +35,18 @@ struct Task {
     int64_t src_start, src_n, fld_start, fld_n;  // ranges in the slice-sorted arrays
     double c_src, c_fld, lb_fld, rb_fld;
     double sL, sR, sM, ks, hzi, zbias;
+    // :node with luminosity: the kick of this task's field slice also reduces that slice's virtual positions
+    // for its next pair in the schedule (collision-order index next_pair, whose direction-1 task is
+    // next_task, drift next_sM); -1 when the slice has no later pair.
+    int32_t next_pair, next_task;
+    double next_sM;
+};
+
+// :node with luminosity: virtual-position extrema of each slice for its first pair of the collide.
+struct FirstLum {
+    int64_t start, count;
+    double sM;
+    int32_t beam, pair, task, pad;
 };
 
 // One deposit+solve plane.  kind: 0 = L (sL), 1 = R (sR), 2 = M (midpoint), 3 = Z (:node, sR on gL).
