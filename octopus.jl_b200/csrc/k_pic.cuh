@@ -1062,7 +1062,9 @@ __device__ __forceinline__ Coord6<R> load_coord(const SoA &S, long long p) {
     return Coord6<R>{col<R>(S, 0)[p], col<R>(S, 1)[p], col<R>(S, 2)[p], col<R>(S, 3)[p], col<R>(S, 4)[p], col<R>(S, 5)[p]};
 }
 
-template <class R, int METHOD>
+// HYB: the Gaussian-subtracted hybrid's add-back is compiled in (FP64 only), a separate instantiation so
+// the plain kernels keep their register budget.
+template <class R, int METHOD, bool HYB>
 __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R> &J, long long p, const Coord6<R> &q,
                                               R &xo, R &pxo, R &yo, R &pyo) {
     using FC = typename RealT<R>::FC;
@@ -1176,7 +1178,7 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
                 Kz += tp.w[q] * (pl - pr);
             }
         }
-        if (!kPrecision && J.hyb) {
+        if (HYB && !kPrecision && J.hyb) {
             // Analytic add-back of the subtracted Gaussian (gaussian_pic.jl:851-884): half the slice population
             // times the Bassetti-Erskine kick at both boundaries, blended in z, and its longitudinal terms.
             const HybridTask &H = J.H;
@@ -1218,8 +1220,8 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
     xo = x; pxo = px; yo = y; pyo = py;
 }
 
-template <class R, int METHOD>
-__global__ void __launch_bounds__(kKickThreads, sizeof(R) == 8 ? 1 : 4) k_kick(Collide C, int plane0_front, const int2 *blockmap) {
+template <class R, int METHOD, bool HYB>
+__global__ void __launch_bounds__(kKickThreads, sizeof(R) == 8 ? 2 : 4) k_kick(Collide C, int plane0_front, const int2 *blockmap) {
     __shared__ KickJob<R> J;
     if (threadIdx.x == 0) {
         const int2 bm = blockmap[blockIdx.x];
@@ -1272,7 +1274,7 @@ __global__ void __launch_bounds__(kKickThreads, sizeof(R) == 8 ? 1 : 4) k_kick(C
             Coord6<R> nxt;
             if (kn < J.fld_n) nxt = load_coord<R>(S, J.fld_start + kn);
             R x, px, y, py;
-            kick_particle<R, METHOD>(C, J, J.fld_start + k, cur, x, px, y, py);
+            kick_particle<R, METHOD, HYB>(C, J, J.fld_start + k, cur, x, px, y, py);
             if (lum_next) {
                 const R vx = x + px * J.next_sM, vy = y + py * J.next_sM;
                 nan |= (vx != vx) | (vy != vy);

@@ -1029,7 +1029,10 @@ void CollideJob::run() {
             PhaseScope ps(c, OCTO_PHASE_KICK, st, 1, fld_bytes * 11 * rsz);
             with_real(fp32, [&](auto r) {
                 launch_method(method, [&](auto M) {
-                    k_kick<decltype(r), decltype(M)::value><<<F.nb, kKickThreads, 0, st>>>(C, F.p0, c->blockmap.p + F.b0);
+                    using R = decltype(r);
+                    constexpr int MM = decltype(M)::value;
+                    if (gaussian) k_kick<R, MM, true><<<F.nb, kKickThreads, 0, st>>>(C, F.p0, c->blockmap.p + F.b0);
+                    else k_kick<R, MM, false><<<F.nb, kKickThreads, 0, st>>>(C, F.p0, c->blockmap.p + F.b0);
                 });
             });
         }
