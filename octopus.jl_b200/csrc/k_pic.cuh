@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(128) k_green_rows(Collide C, int mode, int bas
         warp_fft(line, fx, tw, false);
         const int ja = j0 + r0, jb = ja + 1;
         for (int k = lane; k <= nx; k += 32) {
-            double2 zk = line[k], zm = conjg(line[(NX - k) % NX]);
+            double2 zk = line[fft_out(fx, k)], zm = conjg(line[fft_out(fx, (NX - k) % NX)]);
             double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y + zm.y));
             double2 D = csub(zk, zm);
             out[(long long)k * NY + ja] = A;
@@ -535,7 +535,7 @@ __global__ void __launch_bounds__(128) k_green_cols(Collide C, int mode, int bas
     double2 *col = C.ghat + (long long)slot * C.gstride + (long long)k * NY;
     for (int j = lane; j < NY; j += 32) line[fft_pos(fy, j)] = col[j];
     warp_fft(line, fy, tw, false);
-    for (int j = lane; j < NY; j += 32) col[j] = line[j];
+    for (int j = lane; j < NY; j += 32) col[j] = line[fft_out(fy, j)];
 }
 
 // ------------------------------------------------------------------ deposition
@@ -822,7 +822,7 @@ __global__ void __launch_bounds__(128) k_conv_rows(Collide C, int plane0) {
     warp_fft(line, fx, tw, false);
     C2 *H = (C2 *)C.spec + (long long)pl * (nx + 1) * ny;
     for (int k = lane; k <= nx; k += 32) {
-        C2 zk = line[k], zm = conjg(line[(NX - k) % NX]);
+        C2 zk = line[fft_out(fx, k)], zm = conjg(line[fft_out(fx, (NX - k) % NX)]);
         C2 A, B;
         A.x = R(0.5) * (zk.x + zm.x);
         A.y = R(0.5) * (zk.y + zm.y);
@@ -868,19 +868,19 @@ __global__ void __launch_bounds__(128) k_conv_cols(Collide C, int plane0) {
         C2 gg;
         gg.x = (R)gv.x;
         gg.y = (R)gv.y;
-        const C2 v = cmul(line[j], gg);
+        const C2 v = cmul(line[fft_out(fy, j)], gg);
         if (fy.three) dst[fft_pos(fy, j)] = v;
-        else line[j] = v;
+        else line[fft_out(fy, j)] = v;
     }
     __syncwarp();
     if (!fy.three) {
         for (int j = lane; j < NY; j += 32) {  // bit-reverse permutation in place
             int r = bitrev(j, fy.lgM);
-            if (j < r) { C2 t = line[j]; line[j] = line[r]; line[r] = t; }
+            if (j < r) { const int pj = sw(j), pr = sw(r); C2 t = line[pj]; line[pj] = line[pr]; line[pr] = t; }
         }
     }
     warp_fft(dst, fy, tw, true);
-    for (int j = lane; j < ny; j += 32) col[j] = dst[j];
+    for (int j = lane; j < ny; j += 32) col[j] = dst[fft_out(fy, j)];
 }
 
 // Field planes: a cell is (phi, Ex, Ey, w) as two double2 (plain form) or one float4 (precision form), so
@@ -965,8 +965,9 @@ __global__ void __launch_bounds__(128) k_conv_field(Collide C, int plane0) {
         }
         warp_fft(line, fx, tw, true);
         for (int i = lane; i < nx; i += 32) {
-            phi[(ra - ja0) * nx + i] = line[i].x * scale;
-            if (hb) phi[(rb - ja0) * nx + i] = line[i].y * scale;
+            const C2 v = line[fft_out(fx, i)];
+            phi[(ra - ja0) * nx + i] = v.x * scale;
+            if (hb) phi[(rb - ja0) * nx + i] = v.y * scale;
         }
         __syncwarp();
     }
