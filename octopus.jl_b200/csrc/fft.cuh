@@ -35,14 +35,22 @@ __device__ __forceinline__ int bitrev(int k, int lg) { return (int)(__brev((unsi
 // (L = 256) and from 4x to 1.6x for 8-byte elements.
 __device__ __forceinline__ int sw(int i) { return i ^ ((i >> 4) & 15); }
 
+// Twiddle-table swizzle: entry k sits at k ^ (((k >> 3) ^ (k >> 5)) & m), m = 15 when the table length L/2 is a
+// multiple of 16 (a bijection inside each aligned block of 16), else 0.  The passes read W^(j * step) with
+// power-of-two steps, which without it fall into one bank (simulated: 200 -> 64 wavefronts per 256-point
+// FP64 line).
+__device__ __forceinline__ int tsw(int k, int m) { return k ^ (((k >> 3) ^ (k >> 5)) & m); }
+__device__ __forceinline__ int tw_mask(int L) { return ((L >> 1) & 15) ? 0 : 15; }
+
 // Butterfly passes on a buffer already loaded in bit-reversed order.  Pairs of radix-2 DIT stages
 // (half-sizes h and 2h) are merged into one radix-2^2 pass over groups of four elements
 // {i, i+h, i+2h, i+3h}: half the shared-memory round trips and warp syncs of plain radix-2, with the
 // same twiddles (the second-stage twiddle of the odd pair is -i times that of the even pair, applied
 // exactly by a swap and a sign change).  An odd log2(L) starts with one radix-2 pass.
-// tws: twiddle stride, 1 for a table of length L itself, 3 for a sub-line of length L of a 3L table.
+// tws: twiddle stride, 1 for a table of length L itself, 3 for a sub-line of length L of a 3L table;
+// tm: the table's swizzle mask (tw_mask of its own length).
 template <class C2>
-__device__ __forceinline__ void warp_fft_passes(C2 *a, int L, const C2 *tw, bool inv, int tws = 1) {
+__device__ __forceinline__ void warp_fft_passes(C2 *a, int L, const C2 *tw, bool inv, int tws, int tm) {
     const int lane = threadIdx.x & 31;
     __syncwarp();
     int half = 1, step = L >> 1;
@@ -64,8 +72,8 @@ __device__ __forceinline__ void warp_fft_passes(C2 *a, int L, const C2 *tw, bool
         for (int b = lane; b < quads; b += 32) {
             const int j = b & (half - 1);
             const int i0 = ((b & ~(half - 1)) << 2) | j;
-            C2 w1 = tw[j * step * tws];          // W_{2h}^j
-            C2 w2 = tw[j * (step >> 1) * tws];   // W_{4h}^j
+            C2 w1 = tw[tsw(j * step * tws, tm)];          // W_{2h}^j
+            C2 w2 = tw[tsw(j * (step >> 1) * tws, tm)];   // W_{4h}^j
             if (inv) { w1.y = -w1.y; w2.y = -w2.y; }
             const C2 x0 = a[sw(i0)], x1 = a[sw(i0 + half)], x2 = a[sw(i0 + 2 * half)], x3 = a[sw(i0 + 3 * half)];
             const C2 t1 = cmul(x1, w1), t3 = cmul(x3, w1);
@@ -85,11 +93,12 @@ __device__ __forceinline__ void warp_fft_passes(C2 *a, int L, const C2 *tw, bool
 
 // Line geometry: M = L (power of two) or L / 3.
 struct FftLen {
-    int L, M, lgM, three;
+    int L, M, lgM, three, tm;
 };
 __device__ __forceinline__ FftLen fft_len(int L) {
     FftLen f;
     f.L = L;
+    f.tm = tw_mask(L);
     f.three = (L % 3) == 0;
     f.M = f.three ? L / 3 : L;
     f.lgM = 31 - __clz(f.M);
@@ -105,10 +114,10 @@ __device__ __forceinline__ int fft_pos(const FftLen &f, int i) {
 __device__ __forceinline__ int fft_out(const FftLen &f, int k) { return (k & ~(f.M - 1)) | sw(k & (f.M - 1)); }
 // W_L^k for 0 <= k < L from the half table (W_L^k = -W_L^(k - L/2)), conjugated for the inverse.
 template <class C2>
-__device__ __forceinline__ C2 twiddle(const C2 *tw, int L, int k, bool inv) {
+__device__ __forceinline__ C2 twiddle(const C2 *tw, int L, int k, bool inv, int tm) {
     C2 w;
-    if (k < (L >> 1)) w = tw[k];
-    else { w = tw[k - (L >> 1)]; w.x = -w.x; w.y = -w.y; }
+    if (k < (L >> 1)) w = tw[tsw(k, tm)];
+    else { w = tw[tsw(k - (L >> 1), tm)]; w.x = -w.x; w.y = -w.y; }
     if (inv) w.y = -w.y;
     return w;
 }
@@ -119,21 +128,21 @@ __device__ __forceinline__ C2 twiddle(const C2 *tw, int L, int k, bool inv) {
 template <class C2>
 __device__ __forceinline__ void warp_fft(C2 *a, const FftLen &f, const C2 *tw, bool inv) {
     if (!f.three) {
-        warp_fft_passes(a, f.L, tw, inv);
+        warp_fft_passes(a, f.L, tw, inv, 1, f.tm);
         return;
     }
     const int M = f.M;
-    warp_fft_passes(a, M, tw, inv, 3);
-    warp_fft_passes(a + M, M, tw, inv, 3);
-    warp_fft_passes(a + 2 * M, M, tw, inv, 3);
+    warp_fft_passes(a, M, tw, inv, 3, f.tm);
+    warp_fft_passes(a + M, M, tw, inv, 3, f.tm);
+    warp_fft_passes(a + 2 * M, M, tw, inv, 3, f.tm);
     __syncwarp();
     using R = decltype(a[0].x);
     const R h = R(0.5), s3 = R(0.86602540378443864676);  // sin(2 pi / 3)
     for (int k = (threadIdx.x & 31); k < M; k += 32) {
         const int ks = sw(k);
         const C2 y0 = a[ks];
-        const C2 z1 = cmul(a[M + ks], twiddle(tw, f.L, k, inv));
-        const C2 z2 = cmul(a[2 * M + ks], twiddle(tw, f.L, 2 * k, inv));
+        const C2 z1 = cmul(a[M + ks], twiddle(tw, f.L, k, inv, f.tm));
+        const C2 z2 = cmul(a[2 * M + ks], twiddle(tw, f.L, 2 * k, inv, f.tm));
         const C2 t = cadd(z1, z2), d = csub(z1, z2);
         C2 m, x0, x1, x2;
         m.x = y0.x - h * t.x;
@@ -153,7 +162,8 @@ __device__ __forceinline__ void warp_fft(C2 *a, const FftLen &f, const C2 *tw, b
 // Stage the twiddle table of length L/2 into shared memory (block-wide).
 template <class C2>
 __device__ __forceinline__ void load_twiddles(C2 *s_tw, const C2 *g_tw, int L) {
-    for (int k = threadIdx.x; k < (L >> 1); k += blockDim.x) s_tw[k] = g_tw[k];
+    const int tm = tw_mask(L);
+    for (int k = threadIdx.x; k < (L >> 1); k += blockDim.x) s_tw[tsw(k, tm)] = g_tw[k];
 }
 
 }  // namespace octo
