@@ -613,13 +613,23 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
     const R xlo = x0, xhi = (R)(sg.x0 + sg.w), ylo = y0, yhi = (R)(sg.y0 + sg.h);
     int outside = 0;
     long long total = 0;
-    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < P.src_n; k += (long long)gridDim.x * blockDim.x) {
-        const long long p = P.src_start + k;
-        const R xd = X[p] + PX[p] * s;
-        const R yd = Y[p] + PY[p] * s;
+    // the next particle's coordinates are loaded before the current one's taps, two loads in flight
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    R cx = 0, cpx = 0, cy = 0, cpy = 0;
+    if (k < P.src_n) { const long long p = P.src_start + k; cx = X[p]; cpx = PX[p]; cy = Y[p]; cpy = PY[p]; }
+    for (; k < P.src_n; k += stride) {
+        R nx_ = 0, npx = 0, ny_ = 0, npy = 0;
+        if (k + stride < P.src_n) {
+            const long long q = P.src_start + k + stride;
+            nx_ = X[q]; npx = PX[q]; ny_ = Y[q]; npy = PY[q];
+        }
+        const R xd = cx + cpx * s;
+        const R yd = cy + cpy * s;
         if (P.count_dropped && !(isfinite(xd) && xlo <= xd && xd <= xhi && isfinite(yd) && ylo <= yd && yd <= yhi))
             ++outside;
         total += deposit_taps<R, METHOD>((xd - x0) * hxi, (yd - y0) * hyi, nx, ny, scale, acc, nx);
+        cx = nx_; cpx = npx; cy = ny_; cpy = npy;
     }
     if (C.o.gaussian) {  // the plane's exact total charge, for the neutralised subtraction
         for (int o = 16; o; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
@@ -657,11 +667,20 @@ __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0) {
     const R scale = (R)ldexp(1.0, side ? J.bits2 : J.bits1);
     const R hxi = (R)(1.0 / L.hx), hyi = (R)(1.0 / L.hy);
     const R x0 = (R)L.x0, y0 = (R)L.y0;
-    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-        const long long p = st + k;
-        const R vx = X[p] + PX[p] * s;
-        const R vy = Y[p] + PY[p] * s;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    R cx = 0, cpx = 0, cy = 0, cpy = 0;
+    if (k < n) { cx = X[st + k]; cpx = PX[st + k]; cy = Y[st + k]; cpy = PY[st + k]; }
+    for (; k < n; k += stride) {  // next particle prefetched, as in k_deposit
+        R nx_ = 0, npx = 0, ny_ = 0, npy = 0;
+        if (k + stride < n) {
+            const long long q = st + k + stride;
+            nx_ = X[q]; npx = PX[q]; ny_ = Y[q]; npy = PY[q];
+        }
+        const R vx = cx + cpx * s;
+        const R vy = cy + cpy * s;
         deposit_taps<R, METHOD>((vx - x0) * hxi, (vy - y0) * hyi, nw, nh, scale, acc, nw);
+        cx = nx_; cpx = npx; cy = ny_; cpy = npy;
     }
     if (local) {
         __syncthreads();
