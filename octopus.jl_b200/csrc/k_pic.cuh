@@ -40,6 +40,7 @@ struct Collide {           // device pointers for one collide (passed by value)
     long long *lq;             // luminosity grids: (pair-in-front*2 + side) * (lnx+1)*(lny+1)
     double *lum_parts;         // [pair position]
     double *lum_partial;       // [pair-in-front][kLumSplit] overlap partial sums
+    unsigned *lum_tick;        // [pair-in-front] blocks of k_lum_overlap done (reset by the last)
     const double2 *tw_x, *tw_y;  // FP64 twiddles for 2nx and 2ny (Green spectra)
     const void *twr_x, *twr_y;   // the same in RealT<R>::C2 (charge convolution)
     SoA beam[2];
@@ -362,28 +363,19 @@ __global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0) {
     G.rebuild = 1;
 }
 
-// Luminosity mesh per pair (pic_cpu.jl:2706-2723).
-__global__ void k_lum_plan(Collide C, int lj0, int npairs, int task0) {
-    int ql = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ql >= npairs) return;
-    const LumJob &J = C.lumjobs[lj0 + ql];
-    LumGeom &L = C.lumgeom[J.pair];
+// Luminosity mesh of a pair from its virtual-position box (pic_cpu.jl:2706-2723); false with err = 1
+// (non-finite position) or 3 (degenerate extent).  t1: the pair's direction-1 task.
+__device__ __forceinline__ bool lum_geometry(const Collide &C, const LumJob &J, int t1, LumGeom &L, int &err) {
     L.ok = 0;
+    err = 0;
     const unsigned long long *b = C.lumb + (long long)J.pair * 4;
     double xmin = ord_decode(b[0]), xmax = ord_decode(b[1]), ymin = ord_decode(b[2]), ymax = ord_decode(b[3]);
-    int t1 = task0 + 2 * ql;
-    if ((C.nanflag[t1] & 4) || (C.nanflag[t1 + 1] & 4)) {
-        record_error(C.status, t1, 1, 1);
-        return;
-    }
+    if ((C.nanflag[t1] & 4) || (C.nanflag[t1 + 1] & 4)) { err = 1; return false; }
     double width, height;
-    if (!resolve_extent(C.o, xmax - xmin, ymax - ymin, width, height)) {
-        record_error(C.status, t1, 3, 0);
-        return;
-    }
-    int nx = C.o.lnx, ny = C.o.lny;
-    double tx = width / ((double)nx - 1.1);
-    double ty = height / ((double)ny - 1.1);
+    if (!resolve_extent(C.o, xmax - xmin, ymax - ymin, width, height)) { err = 3; return false; }
+    const int nx = C.o.lnx, ny = C.o.lny;
+    const double tx = width / ((double)nx - 1.1);
+    const double ty = height / ((double)ny - 1.1);
     width += 0.1 * tx;
     height += 0.1 * ty;
     xmin -= 0.05 * tx;
@@ -393,6 +385,7 @@ __global__ void k_lum_plan(Collide C, int lj0, int npairs, int task0) {
     L.hx = width / (double)(nx - 1);
     L.hy = height / (double)(ny - 1);
     L.ok = 1;
+    return true;
 }
 
 // ------------------------------------------------------------------ Green function
@@ -647,13 +640,20 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
 
 // Luminosity planes: 2 per pair (side 0 = beam-1 slice i at sM1, side 1 = beam-2 slice j at sM2)
 // on the (lnx+1) x (lny+1) overlap mesh (pic_cpu.jl:2724-2735).
+// Every block derives its pair's mesh (lum_geometry); block (0, side 0) publishes it and reports errors.
 template <class R, int METHOD>
-__global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0) {
+__global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0, int task0) {
     long long *sq = (long long *)g_smem;
     const int ql = blockIdx.y >> 1, side = blockIdx.y & 1;
     const LumJob &J = C.lumjobs[lj0 + ql];
-    const LumGeom &L = C.lumgeom[J.pair];
-    if (!L.ok) return;
+    LumGeom L;
+    int err;
+    const bool ok = lum_geometry(C, J, task0 + 2 * ql, L, err);
+    if (blockIdx.x == 0 && side == 0 && threadIdx.x == 0) {
+        C.lumgeom[J.pair] = L;
+        if (!ok) record_error(C.status, task0 + 2 * ql, err, err == 1 ? 1 : 0);
+    }
+    if (!ok) return;
     const int nw = C.o.lnx + 1, nh = C.o.lny + 1, cells = nw * nh;
     const bool local = !C.o.lum_global;
     if (local)
@@ -690,7 +690,7 @@ __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0) {
 
 // Overlap integral per pair: sum q1*q2 over the full (nx+1)(ny+1) extent (pic_cpu.jl:2725-2736),
 // split over kLumSplit blocks per pair into fixed partial sums (deterministic), clearing both grids for
-// the next front.  k_lum_fold adds the partials in order and applies klum/(hx hy).
+// the next front.
 constexpr int kLumSplit = 16;
 __global__ void __launch_bounds__(256) k_lum_overlap(Collide C, int lj0) {
     const int ql = blockIdx.y, part = blockIdx.x;
@@ -715,19 +715,23 @@ __global__ void __launch_bounds__(256) k_lum_overlap(Collide C, int lj0) {
         if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
         __syncthreads();
     }
-    if (threadIdx.x == 0) C.lum_partial[(long long)ql * kLumSplit + part] = red[0];
-}
-
-__global__ void k_lum_fold(Collide C, int lj0, int nl) {
-    const int ql = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ql >= nl) return;
-    const LumJob &J = C.lumjobs[lj0 + ql];
-    const LumGeom &L = C.lumgeom[J.pair];
-    if (!L.ok) return;
-    double s = 0.0;
-    for (int k = 0; k < kLumSplit; ++k) s += C.lum_partial[(long long)ql * kLumSplit + k];
-    const double hxi = 1.0 / L.hx, hyi = 1.0 / L.hy;
-    C.lum_parts[J.pair] = s * C.klum * hxi * hyi;
+    if (threadIdx.x == 0) {
+        // the pair's last block to finish adds the kLumSplit partials in order and applies klum/(hx hy)
+        C.lum_partial[(long long)ql * kLumSplit + part] = red[0];
+        __threadfence();
+        const unsigned ticket = atomicAdd(&C.lum_tick[ql], 1u);
+        if (ticket == kLumSplit - 1) {
+            __threadfence();
+            const LumGeom &L = C.lumgeom[J.pair];
+            if (L.ok) {
+                double sum = 0.0;
+                for (int k = 0; k < kLumSplit; ++k) sum += __ldcg(&C.lum_partial[(long long)ql * kLumSplit + k]);
+                const double hxi = 1.0 / L.hx, hyi = 1.0 / L.hy;
+                C.lum_parts[J.pair] = sum * C.klum * hxi * hyi;
+            }
+            C.lum_tick[ql] = 0u;  // ready for the next front
+        }
+    }
 }
 
 // Hybrid: erf-integrated CIC/TSC node profiles of the reference Gaussian of each field-solve plane

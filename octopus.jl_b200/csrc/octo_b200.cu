@@ -190,6 +190,7 @@ struct octo_ctx {
     DevBuf<TaskGeom> geom;
     DevBuf<int2> blockmap;
     DevBuf<FirstLum> first_lum;
+    DevBuf<unsigned> lum_tick;
     DevBuf<CacheEntry> cache;
     DevBuf<NodeMesh> nodes;
     DevBuf<LumGeom> lumgeom;
@@ -890,6 +891,10 @@ void CollideJob::run() {
     c->spec.ensure((size_t)max_planes * (nx + 1) * ny);
     c->fields.ensure((size_t)max_planes * (fp32 ? 1 : 2) * cells);  // double2 units: 32 B (FP64) / 16 B (FP32) per cell
     c->lum_partial.ensure((size_t)max_lum * kLumSplit);
+    if (c->lum_tick.n < (size_t)max_lum) {
+        c->lum_tick.ensure((size_t)max_lum);
+        CK(cudaMemsetAsync(c->lum_tick.p, 0, sizeof(unsigned) * c->lum_tick.n, st));
+    }
     if (c->lq.n < (size_t)2 * max_lum * lcells) {
         c->lq.ensure((size_t)2 * max_lum * lcells);
         CK(cudaMemsetAsync(c->lq.p, 0, sizeof(long long) * c->lq.n, st));
@@ -928,6 +933,7 @@ void CollideJob::run() {
     C.lq = c->lq.p;
     C.lum_parts = c->lum_parts.p;
     C.lum_partial = c->lum_partial.p;
+    C.lum_tick = c->lum_tick.p;
     C.nodes = c->nodes.p;
     const bool gaussian = c->dopt.gaussian != 0;
     if (gaussian) {
@@ -988,17 +994,15 @@ void CollideJob::run() {
             launches += gaussian ? 4 : 3;
         }
         if (compute_lum && F.nl) {
-            PhaseScope ps(c, OCTO_PHASE_LUMINOSITY, st, 4, slice_bytes * 4 * rsz);
-            k_lum_plan<<<(F.nl + 63) / 64, 64, 0, st>>>(C, F.l0, F.nl, F.t0);
+            PhaseScope ps(c, OCTO_PHASE_LUMINOSITY, st, 2, slice_bytes * 4 * rsz);
             unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(8, (F.maxlum + 32767) / 32768));
             with_real(fp32, [&](auto r) {
                 launch_method(lmethod, [&](auto M) {
-                    k_lum_deposit<decltype(r), decltype(M)::value><<<dim3(bpp, 2 * F.nl), 1024, lum_bytes, st>>>(C, F.l0);
+                    k_lum_deposit<decltype(r), decltype(M)::value><<<dim3(bpp, 2 * F.nl), 1024, lum_bytes, st>>>(C, F.l0, F.t0);
                 });
             });
             k_lum_overlap<<<dim3(kLumSplit, F.nl), 256, 0, st>>>(C, F.l0);
-            k_lum_fold<<<(F.nl + 63) / 64, 64, 0, st>>>(C, F.l0, F.nl);
-            launches += 4;
+            launches += 2;
         }
         {
             PhaseScope ps(c, OCTO_PHASE_DEPOSIT, st, 1, src_bytes * 4 * rsz);
@@ -1225,7 +1229,7 @@ void octo_destroy(octo_ctx *c) {
     c->nodenan.release(); c->status.release(); c->ghat.release(); c->qgrid.release(); c->lq.release();
     c->spec.release(); c->fields.release(); c->lum_parts.release(); c->lum_partial.release(); c->node_ref.release(); c->stats.release();
     c->partial.release(); c->soa_ptrs.release();
-    c->first_lum.release();
+    c->first_lum.release(); c->lum_tick.release();
     c->hyb.release(); c->hmom.release(); c->hprof.release(); c->hsum.release(); c->qtot.release();
     c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_noderef.release(); c->h_slices.release();
     for (auto e : c->ev_pool) cudaEventDestroy(e);
