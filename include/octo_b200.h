@@ -171,6 +171,9 @@ int32_t octo_last_error(octo_ctx *ctx, char *buf, int64_t len);
 #define OCTO_PHASE_NODE 10
 #define OCTO_NPHASES 11
 int32_t octo_set_timing(octo_ctx *ctx, int32_t enable); /* enabling also clears the accumulators */
+/* Restrict the timing to the phases whose bit (1 << OCTO_PHASE_*) is set in mask (default: all).  Each
+ * timed launch group records two events; timing one phase keeps that overhead off the others. */
+int32_t octo_set_timing_phases(octo_ctx *ctx, uint32_t mask);
 int32_t octo_timing_report(octo_ctx *ctx, double ms[OCTO_NPHASES], int64_t launches[OCTO_NPHASES],
                            double bytes[OCTO_NPHASES]);
 

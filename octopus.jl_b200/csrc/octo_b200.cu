@@ -219,6 +219,7 @@ struct octo_ctx {
     long long last_launches = 0;
     // per-phase device timing (octo_set_timing): event pairs recorded around each launch group
     int timing = 0;
+    unsigned timing_mask = ~0u;  // phases timed when timing is on (octo_set_timing_phases)
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_marks;
@@ -246,7 +247,7 @@ struct PhaseScope {
     int nlaunch;
     double bytes;
     PhaseScope(octo_ctx *c_, int ph, cudaStream_t s, int nl = 1, double b = 0.0) : c(c_), phase(ph), st(s), nlaunch(nl), bytes(b) {
-        if (c->timing) { a = take_event(c); CK(cudaEventRecord(a, st)); }
+        if (c->timing && ((c->timing_mask >> phase) & 1u)) { a = take_event(c); CK(cudaEventRecord(a, st)); }
     }
     ~PhaseScope() {
         if (c->timing && a) {
@@ -1386,6 +1387,12 @@ int32_t octo_beam_gaussian(octo_ctx *c, octo_beam *beam, uint64_t seed, uint64_t
     } catch (CudaFail &e) {
         return fail(c, OCTO_ERR_CUDA, e.msg);
     }
+}
+
+int32_t octo_set_timing_phases(octo_ctx *c, uint32_t mask) {
+    if (!c) return OCTO_ERR_ARG;
+    c->timing_mask = mask;
+    return OCTO_OK;
 }
 
 int32_t octo_set_timing(octo_ctx *c, int32_t enable) {

@@ -92,8 +92,11 @@ class Context:
         _lib.lib().octo_green_cache_stats(self._ptr, C.byref(h), C.byref(m), C.byref(r))
         return h.value, m.value, r.value
 
-    def set_timing(self, enable: bool = True):
-        """Per-phase device timing (the reference's pic_timing diagnostics); enabling clears it."""
+    def set_timing(self, enable: bool = True, phases=None):
+        """Per-phase device timing (the reference's pic_timing diagnostics); enabling clears it.  phases: the
+        names of the phases to time (default all); each timed launch group records two CUDA events."""
+        mask = 0xFFFFFFFF if phases is None else sum(1 << _lib.PHASES.index(p) for p in phases)
+        _lib.lib().octo_set_timing_phases(self._ptr, mask)
         _lib.lib().octo_set_timing(self._ptr, int(bool(enable)))
 
     def timing_report(self):
