@@ -906,35 +906,44 @@ __global__ void __launch_bounds__(128) k_conv_cols(Collide C, int plane0) {
     for (int j = lane; j < ny; j += 32) col[j] = dst[fft_out(fy, j)];
 }
 
-// Field planes: a cell is (phi, Ex, Ey, w) as two double2 (plain form) or one float4 (precision form), so
-// one tap of one plane is one 32-byte or 16-byte access.  The fourth word w of an L plane in :node mode
-// carries phi of the task's Z plane (written by the Z plane's own k_conv_field block), so the L-mesh taps
-// of the kick read phi_L, Ex_L, Ey_L and phi_Z in that one access.
+// Field planes: a cell is (Ex, Ey, phi, w) as two double2 (plain form) or one float4 (precision form), so
+// one tap of one plane is one 32-byte or 16-byte access, and a tap that needs only the field (the R mesh
+// in :node mode) one 16-byte or 8-byte access.  The fourth word w of an L plane in :node mode carries phi of
+// the task's Z plane (written by the Z plane's own k_conv_field block), so the L-mesh taps of the kick read
+// Ex_L, Ey_L, phi_L and phi_Z in that one access.
 __device__ __forceinline__ void store_cell(double2 *F, long long o, double phi, double ex, double ey) {
-    F[2 * o] = make_double2(phi, ex);
-    reinterpret_cast<double *>(F)[4 * o + 2] = ey;
+    F[2 * o] = make_double2(ex, ey);
+    reinterpret_cast<double *>(F)[4 * o + 2] = phi;
 }
 __device__ __forceinline__ void store_cell(float4 *F, long long o, float phi, float ex, float ey) {
-    reinterpret_cast<float2 *>(F)[2 * o] = make_float2(phi, ex);
-    reinterpret_cast<float *>(F)[4 * o + 2] = ey;
+    reinterpret_cast<float2 *>(F)[2 * o] = make_float2(ex, ey);
+    reinterpret_cast<float *>(F)[4 * o + 2] = phi;
 }
 __device__ __forceinline__ void store_w(double2 *F, long long o, double w) { reinterpret_cast<double *>(F)[4 * o + 3] = w; }
 __device__ __forceinline__ void store_w(float4 *F, long long o, float w) { reinterpret_cast<float *>(F)[4 * o + 3] = w; }
 __device__ __forceinline__ void load_cell4(const double2 *F, long long c, double &phi, double &ex, double &ey, double &w) {
     const double2 a = F[2 * c], b = F[2 * c + 1];
-    phi = a.x; ex = a.y; ey = b.x; w = b.y;
+    ex = a.x; ey = a.y; phi = b.x; w = b.y;
 }
 __device__ __forceinline__ void load_cell4(const float4 *F, long long c, float &phi, float &ex, float &ey, float &w) {
     const float4 v = F[c];
-    phi = v.x; ex = v.y; ey = v.z; w = v.w;
+    ex = v.x; ey = v.y; phi = v.z; w = v.w;
+}
+__device__ __forceinline__ void load_field(const double2 *F, long long c, double &ex, double &ey) {
+    const double2 a = F[2 * c];
+    ex = a.x; ey = a.y;
+}
+__device__ __forceinline__ void load_field(const float4 *F, long long c, float &ex, float &ey) {
+    const float2 a = reinterpret_cast<const float2 *>(F)[2 * c];
+    ex = a.x; ey = a.y;
 }
 __device__ __forceinline__ void load_cell(const double2 *F, long long c, double &phi, double &ex, double &ey) {
     const double2 a = F[2 * c], b = F[2 * c + 1];
-    phi = a.x; ex = a.y; ey = b.x;
+    ex = a.x; ey = a.y; phi = b.x;
 }
 __device__ __forceinline__ void load_cell(const float4 *F, long long c, float &phi, float &ex, float &ey) {
     const float4 v = F[c];
-    phi = v.x; ex = v.y; ey = v.z;
+    ex = v.x; ey = v.y; phi = v.z;
 }
 
 // Inverse x-transform (two Hermitian rows per complex line) producing phi for a tile of rows plus a
@@ -1145,8 +1154,8 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
             const Taps<R, METHOD> tp(o, gR, J.hxR, J.hyR, x, y);
 #pragma unroll
             for (int t = 0; t < NT2; ++t) {
-                R ph, ex, ey;
-                load_cell(FR, tp.cell(t, o.nx), ph, ex, ey);
+                R ex, ey;
+                load_field(FR, tp.cell(t, o.nx), ex, ey);
                 KxR += tp.w[t] * ex;
                 KyR += tp.w[t] * ey;
             }
