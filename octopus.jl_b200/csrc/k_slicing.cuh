@@ -25,14 +25,34 @@ struct SliceInfo {          // device-resident, read back once per collide
     int pad;
 };
 
+// Both beams are sliced by the same launches: blockIdx.z (or blockIdx.x for the one-block kernels)
+// selects the beam, so the two serial lane folds run side by side.
+template <class R>
+struct SliceArgs {
+    const R *c[2][6];        // caller-order coordinates x, px, y, py, z, pz
+    R *s[2][6];              // slice-sorted copies
+    int *perm[2];
+    SliceInfo *info[2];
+    double *lane_sum[2], *lane_min[2], *lane_max[2], *lanes[2];
+    const double *q[2];      // quantile table (see k_fold_stats)
+    int *counts[2];
+    long long *blockoff[2];
+    long long n[2], nblocks[2];
+    int method[2], ns[2], cpos[2];
+};
+
 // Lane partial sums / extrema over all particles.  square != 0 folds (z - mu)^2.
 // Lane t must add elements t, t+4096, ... strictly in order, so the parallelism is across lanes; to
 // keep enough loads in flight each block stages a tile of kTileIters iterations x 32 lanes in shared
-// memory with all its threads, then one thread per lane adds its column in order.
+// memory with all its threads, then one thread per lane adds its column in order.  grid (128, 1, 2).
 constexpr int kTileIters = 64;
 template <class R>
-__global__ void __launch_bounds__(256) k_lane_fold(const R *__restrict__ z, long long n, const SliceInfo *info,
-                                                   int square, double *lane_sum, double *lane_min, double *lane_max) {
+__global__ void __launch_bounds__(256) k_lane_fold(const SliceArgs<R> A, int square) {
+    const int bm = blockIdx.z;
+    const R *__restrict__ z = A.c[bm][4];
+    const long long n = A.n[bm];
+    const SliceInfo *info = A.info[bm];
+    double *lane_sum = A.lane_sum[bm], *lane_min = A.lane_min[bm], *lane_max = A.lane_max[bm];
     __shared__ double tile[kTileIters][33];
     const int lane0 = blockIdx.x * 32;
     const double mu = square ? info->mu : 0.0;
@@ -73,9 +93,15 @@ __global__ void __launch_bounds__(256) k_lane_fold(const R *__restrict__ z, long
 // Serial fold of the lanes (slicing.jl:254-257), staged through shared memory so the single adding
 // thread reads at shared-memory latency.  stage 0: mean and extrema; stage 1: sigma and boundaries.
 // q[s] for s = 1..ns-1 holds sqrt(2)*erfinv(2s/ns - 1) (:normal_quantile) or the :specified positions.
-__global__ void __launch_bounds__(1024) k_fold_stats(const double *lane_sum, const double *lane_min,
-                                                     const double *lane_max, long long n, int stage, int method,
-                                                     int ns, const double *q, SliceInfo *info) {
+// grid (2): one block per beam.
+template <class R>
+__global__ void __launch_bounds__(1024) k_fold_stats(const SliceArgs<R> A, int stage) {
+    const int bm = blockIdx.x;
+    const double *lane_sum = A.lane_sum[bm], *lane_min = A.lane_min[bm], *lane_max = A.lane_max[bm];
+    const long long n = A.n[bm];
+    const int method = A.method[bm], ns = A.ns[bm];
+    const double *q = A.q[bm];
+    SliceInfo *info = A.info[bm];
     __shared__ double sl[kFoldLanes];
     __shared__ double rlo[32], rhi[32];
     for (int t = threadIdx.x; t < kFoldLanes; t += blockDim.x) sl[t] = lane_sum[t];
@@ -143,10 +169,14 @@ __device__ __forceinline__ int slice_of(double z, const double *b, int ns, int z
     return k - 1;
 }
 
-// Per-block slice counts over contiguous chunks.
+// Per-block slice counts over contiguous chunks.  grid (max blocks, 1, 2).
 template <class R>
-__global__ void k_slice_count(const R *__restrict__ z, long long n, long long chunk, const SliceInfo *info,
-                              int *counts) {
+__global__ void k_slice_count(const SliceArgs<R> A, long long chunk) {
+    const int bm = blockIdx.z;
+    if (blockIdx.x >= A.nblocks[bm]) return;
+    const R *__restrict__ z = A.c[bm][4];
+    const long long n = A.n[bm];
+    const SliceInfo *info = A.info[bm];
     __shared__ double b[kMaxSlices + 1];
     __shared__ int c[kMaxSlices];
     int ns = info->ns;
@@ -157,11 +187,17 @@ __global__ void k_slice_count(const R *__restrict__ z, long long n, long long ch
     long long lo = (long long)blockIdx.x * chunk, hi = min(n, lo + chunk);
     for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) atomicAdd(&c[slice_of((double)z[i], b, ns, zw)], 1);
     __syncthreads();
-    for (int t = threadIdx.x; t < ns; t += blockDim.x) counts[(long long)blockIdx.x * ns + t] = c[t];
+    for (int t = threadIdx.x; t < ns; t += blockDim.x) A.counts[bm][(long long)blockIdx.x * ns + t] = c[t];
 }
 
-// Slice starts (aligned to `align` elements) and per-block write offsets.  One block.
-__global__ void k_slice_offsets(const int *counts, int nblocks, int align, SliceInfo *info, long long *blockoff) {
+// Slice starts (aligned to `align` elements) and per-block write offsets.  grid (2): one block per beam.
+template <class R>
+__global__ void k_slice_offsets(const SliceArgs<R> A, int align) {
+    const int bm = blockIdx.x;
+    const int *counts = A.counts[bm];
+    const int nblocks = (int)A.nblocks[bm];
+    SliceInfo *info = A.info[bm];
+    long long *blockoff = A.blockoff[bm];
     int ns = info->ns;
     __shared__ long long tot[kMaxSlices];
     for (int s = threadIdx.x; s < ns; s += blockDim.x) {
@@ -190,11 +226,15 @@ __global__ void k_slice_offsets(const int *counts, int nblocks, int align, Slice
 
 // Stable scatter into slice-contiguous SoA buffers; perm[pos] = original index.
 // Each block walks its chunk in tiles of blockDim particles, ranking within warps by match_any.
+// grid (max blocks, 1, 2).
 template <class R>
-__global__ void k_slice_scatter(const R *__restrict__ x, const R *__restrict__ px, const R *__restrict__ y,
-                                const R *__restrict__ py, const R *__restrict__ z, const R *__restrict__ pz, long long n,
-                                long long chunk, const SliceInfo *info, const long long *blockoff, R *sx, R *spx, R *sy,
-                                R *spy, R *sz, R *spz, int *perm) {
+__global__ void k_slice_scatter(const SliceArgs<R> A, long long chunk) {
+    const int bm = blockIdx.z;
+    if (blockIdx.x >= A.nblocks[bm]) return;
+    const long long n = A.n[bm];
+    const SliceInfo *info = A.info[bm];
+    const long long *blockoff = A.blockoff[bm];
+    int *perm = A.perm[bm];
     __shared__ double b[kMaxSlices + 1];
     __shared__ long long run[kMaxSlices];
     __shared__ int wcount[32][kMaxSlices];
@@ -210,7 +250,7 @@ __global__ void k_slice_scatter(const R *__restrict__ x, const R *__restrict__ p
         __syncthreads();
         long long i = base + threadIdx.x;
         bool live = i < hi;
-        int s = live ? slice_of((double)z[i], b, ns, zw) : -1;
+        int s = live ? slice_of((double)A.c[bm][4][i], b, ns, zw) : -1;
         unsigned peers = __match_any_sync(0xffffffffu, s);
         int rank = __popc(peers & ((1u << lane) - 1u));
         if (live && rank == 0) wcount[warp][s] = __popc(peers);
@@ -219,8 +259,8 @@ __global__ void k_slice_scatter(const R *__restrict__ x, const R *__restrict__ p
             long long pos = run[s] + rank;
             for (int w = 0; w < warp; ++w) pos += wcount[w][s];
             perm[pos] = (int)i;
-            sx[pos] = x[i]; spx[pos] = px[i]; sy[pos] = y[i];
-            spy[pos] = py[i]; sz[pos] = z[i]; spz[pos] = pz[i];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) A.s[bm][k][pos] = A.c[bm][k][i];
         }
         __syncthreads();
         for (int t = threadIdx.x; t < ns; t += blockDim.x) {
@@ -233,21 +273,30 @@ __global__ void k_slice_scatter(const R *__restrict__ x, const R *__restrict__ p
 }
 
 // Centroid lane sums per slice: lane t folds members t, t+4096, ... of the slice list (slicing.jl:240-257).
+// grid (kFoldLanes / 256, max slices, 2).
 template <class R>
-__global__ void k_slice_lanes(const R *__restrict__ sz, const SliceInfo *info, double *lanes) {
+__global__ void k_slice_lanes(const SliceArgs<R> A) {
+    const int bm = blockIdx.z;
+    const SliceInfo *info = A.info[bm];
     int s = blockIdx.y;
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= kFoldLanes || s >= info->ns) return;
+    const R *__restrict__ sz = A.s[bm][4];
     long long st = info->start[s], cnt = info->count[s];
     double acc = 0.0;
     for (long long k = t; k < cnt; k += kFoldLanes) acc += (double)sz[st + k];
-    lanes[(long long)s * kFoldLanes + t] = acc;
+    A.lanes[bm][(long long)s * kFoldLanes + t] = acc;
 }
 
 // Serial lane fold per slice (one block per slice, lanes staged in shared memory); centers and
-// weights (slicing.jl:523-559).
-__global__ void __launch_bounds__(1024) k_slice_finish(const double *lanes, long long n, int center_position,
-                                                       SliceInfo *info) {
+// weights (slicing.jl:523-559).  grid (max slices, 2).
+template <class R>
+__global__ void __launch_bounds__(1024) k_slice_finish(const SliceArgs<R> A) {
+    const int bm = blockIdx.y;
+    SliceInfo *info = A.info[bm];
+    const double *lanes = A.lanes[bm];
+    const long long n = A.n[bm];
+    const int center_position = A.cpos[bm];
     __shared__ double sl[kFoldLanes];
     const int s = blockIdx.x;
     if (s >= info->ns) return;

@@ -404,42 +404,61 @@ __global__ void k_init_boxes(unsigned long long *box, long long n4) {
     if (t < n4) box[t] = (t & 1) ? kOrdMaxInit : kOrdMinInit;
 }
 
-// Device slicing of one beam; returns after enqueueing (the slice table is read back by the caller).
-void slice_beam(octo_ctx *c, int b, const octo_beam &beam, cudaStream_t st, long long &launches) {
-    BeamWS &W = c->bw[b];
-    const long long n = beam.n;
-    const int ns = c->ns[b];
-    const long long total = padded_total(n, ns);
-    for (auto &a : W.s) a.ensure(total);
-    W.perm.ensure(total);
-    W.info.ensure(1);
-    W.lane_sum.ensure(kFoldLanes); W.lane_min.ensure(kFoldLanes); W.lane_max.ensure(kFoldLanes);
-    W.lanes.ensure((size_t)kFoldLanes * ns);
-    const long long nblocks = (n + kChunk - 1) / kChunk;
-    W.counts.ensure((size_t)nblocks * ns);
-    W.blockoff.ensure((size_t)nblocks * ns);
-    W.total = total;
-    int method = b == 0 ? c->opt.slicing_method1 : c->opt.slicing_method2;
-    int cpos = b == 0 ? c->opt.center_position1 : c->opt.center_position2;
+// Device slicing of both beams in shared launches; returns after enqueueing (the slice tables are read
+// back by the caller).
+void slice_beams(octo_ctx *c, const octo_beam &b1, const octo_beam &b2, cudaStream_t st, long long &launches) {
+    long long nblk_max = 1;
+    int ns_max = 1;
+    for (int b = 0; b < 2; ++b) {
+        BeamWS &W = c->bw[b];
+        const long long n = (b == 0 ? b1 : b2).n;
+        const int ns = c->ns[b];
+        const long long total = padded_total(n, ns);
+        for (auto &a : W.s) a.ensure(total);
+        W.perm.ensure(total);
+        W.info.ensure(1);
+        W.lane_sum.ensure(kFoldLanes); W.lane_min.ensure(kFoldLanes); W.lane_max.ensure(kFoldLanes);
+        W.lanes.ensure((size_t)kFoldLanes * ns);
+        const long long nblocks = (n + kChunk - 1) / kChunk;
+        W.counts.ensure((size_t)nblocks * ns);
+        W.blockoff.ensure((size_t)nblocks * ns);
+        W.total = total;
+        CK(cudaMemsetAsync(W.perm.p, 0xff, sizeof(int) * total, st));
+        nblk_max = std::max(nblk_max, nblocks);
+        ns_max = std::max(ns_max, ns);
+    }
     with_real(c->fp32, [&](auto r) {
         using R = decltype(r);
-        const R *z = (const R *)beam.z;
-        R *ws[6];
-        for (int k = 0; k < 6; ++k) ws[k] = (R *)W.s[k].p;
-        k_lane_fold<R><<<kFoldLanes / 32, 256, 0, st>>>(z, n, W.info.p, 0, W.lane_sum.p, W.lane_min.p, W.lane_max.p);
-        k_fold_stats<<<1, 1024, 0, st>>>(W.lane_sum.p, W.lane_min.p, W.lane_max.p, n, 0, method, ns, W.q.p, W.info.p);
-        k_lane_fold<R><<<kFoldLanes / 32, 256, 0, st>>>(z, n, W.info.p, 1, W.lane_sum.p, W.lane_min.p, W.lane_max.p);
-        k_fold_stats<<<1, 1024, 0, st>>>(W.lane_sum.p, W.lane_min.p, W.lane_max.p, n, 1, method, ns, W.q.p, W.info.p);
-        k_slice_count<R><<<(unsigned)nblocks, 256, 0, st>>>(z, n, kChunk, W.info.p, W.counts.p);
-        k_slice_offsets<<<1, 64, 0, st>>>(W.counts.p, (int)nblocks, kAlign, W.info.p, W.blockoff.p);
-        CK(cudaMemsetAsync(W.perm.p, 0xff, sizeof(int) * total, st));
-        k_slice_scatter<R><<<(unsigned)nblocks, 256, 0, st>>>(
-            (const R *)beam.x, (const R *)beam.px, (const R *)beam.y, (const R *)beam.py, z, (const R *)beam.pz, n, kChunk,
-            W.info.p, W.blockoff.p, ws[0], ws[1], ws[2], ws[3], ws[4], ws[5], W.perm.p);
-        k_slice_lanes<R><<<dim3(kFoldLanes / 256, ns), 256, 0, st>>>(ws[4], W.info.p, W.lanes.p);
-        k_slice_finish<<<ns, 1024, 0, st>>>(W.lanes.p, n, cpos, W.info.p);
+        SliceArgs<R> A{};
+        for (int b = 0; b < 2; ++b) {
+            BeamWS &W = c->bw[b];
+            const octo_beam &B = b == 0 ? b1 : b2;
+            const void *cc[6] = {B.x, B.px, B.y, B.py, B.z, B.pz};
+            for (int k = 0; k < 6; ++k) { A.c[b][k] = (const R *)cc[k]; A.s[b][k] = (R *)W.s[k].p; }
+            A.perm[b] = W.perm.p;
+            A.info[b] = W.info.p;
+            A.lane_sum[b] = W.lane_sum.p; A.lane_min[b] = W.lane_min.p; A.lane_max[b] = W.lane_max.p;
+            A.lanes[b] = W.lanes.p;
+            A.q[b] = W.q.p;
+            A.counts[b] = W.counts.p;
+            A.blockoff[b] = W.blockoff.p;
+            A.n[b] = B.n;
+            A.nblocks[b] = (B.n + kChunk - 1) / kChunk;
+            A.method[b] = b == 0 ? c->opt.slicing_method1 : c->opt.slicing_method2;
+            A.ns[b] = c->ns[b];
+            A.cpos[b] = b == 0 ? c->opt.center_position1 : c->opt.center_position2;
+        }
+        k_lane_fold<R><<<dim3(kFoldLanes / 32, 1, 2), 256, 0, st>>>(A, 0);
+        k_fold_stats<R><<<2, 1024, 0, st>>>(A, 0);
+        k_lane_fold<R><<<dim3(kFoldLanes / 32, 1, 2), 256, 0, st>>>(A, 1);
+        k_fold_stats<R><<<2, 1024, 0, st>>>(A, 1);
+        k_slice_count<R><<<dim3((unsigned)nblk_max, 1, 2), 256, 0, st>>>(A, kChunk);
+        k_slice_offsets<R><<<2, 64, 0, st>>>(A, kAlign);
+        k_slice_scatter<R><<<dim3((unsigned)nblk_max, 1, 2), 256, 0, st>>>(A, kChunk);
+        k_slice_lanes<R><<<dim3(kFoldLanes / 256, ns_max, 2), 256, 0, st>>>(A);
+        k_slice_finish<R><<<dim3(ns_max, 2), 1024, 0, st>>>(A);
     });
-    launches += 10;
+    launches += 9;
     CK(cudaGetLastError());
 }
 
@@ -647,9 +666,8 @@ void CollideJob::begin() {
 
     // ---- slicing (one readback of the slice tables, into pinned memory so the copy is asynchronous)
     {
-        PhaseScope ps(c, OCTO_PHASE_SLICING, st, 20);
-        slice_beam(c, 0, *b1, st, launches);
-        slice_beam(c, 1, *b2, st, launches);
+        PhaseScope ps(c, OCTO_PHASE_SLICING, st, 9);
+        slice_beams(c, *b1, *b2, st, launches);
     }
     c->h_slices.ensure(2);
     CK(cudaMemcpyAsync(c->h_slices.p + 0, c->bw[0].info.p, sizeof(SliceInfo), cudaMemcpyDeviceToHost, st));
