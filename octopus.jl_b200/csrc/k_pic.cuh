@@ -1344,11 +1344,18 @@ __global__ void __launch_bounds__(256) k_node_boxes(NodeBoxArgs A) {
     const long long st = A.start[sl], n = A.count[sl];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     __shared__ unsigned long long red[8][4];
+    // Per-thread extrema with the native min/max (NaN is flagged separately; a +-0 tie cannot change a
+    // mesh built from them), encoded to ordered integers once per block for the atomics.
     for (int r0 = 0; r0 < A.nref; r0 += 8) {
         const int rn = min(8, A.nref - r0);
-        unsigned long long mnx[8], mxx[8], mny[8], mxy[8];
+        R mnx[8], mxx[8], mny[8], mxy[8];
+        R ref[8];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) { mnx[r] = mny[r] = kOrdMinInit; mxx[r] = mxy[r] = kOrdMaxInit; }
+        for (int r = 0; r < 8; ++r) {
+            mnx[r] = mny[r] = R(INFINITY);
+            mxx[r] = mxy[r] = R(-INFINITY);
+            ref[r] = r < rn ? (R)(A.field_mode ? A.ref[r0 + r] : A.ref[(long long)sl * A.nref + r0 + r]) : R(0);
+        }
         bool nan = false;
         for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
             const long long p = st + k;
@@ -1359,26 +1366,26 @@ __global__ void __launch_bounds__(256) k_node_boxes(NodeBoxArgs A) {
                 if (r < rn) {
                     R xv, yv;
                     if (A.field_mode) {
-                        const R sh = R(0.5) * (z - (R)A.ref[r0 + r]);
+                        const R sh = R(0.5) * (z - ref[r]);
                         xv = x + sh * px;
                         yv = y + sh * py;
                     } else {
-                        const R d = (R)A.ref[(long long)sl * A.nref + r0 + r];
-                        xv = x + px * d;
-                        yv = y + py * d;
+                        xv = x + px * ref[r];
+                        yv = y + py * ref[r];
                     }
                     nan |= (xv != xv) | (yv != yv);
-                    unsigned long long ex = ord_encode((double)xv), ey = ord_encode((double)yv);
-                    mnx[r] = min(mnx[r], ex); mxx[r] = max(mxx[r], ex);
-                    mny[r] = min(mny[r], ey); mxy[r] = max(mxy[r], ey);
+                    mnx[r] = fmin(mnx[r], xv); mxx[r] = fmax(mxx[r], xv);
+                    mny[r] = fmin(mny[r], yv); mxy[r] = fmax(mxy[r], yv);
                 }
             }
         }
         int anynan = __syncthreads_or(nan);
         if (anynan && threadIdx.x == 0) atomicOr(A.nanf, 1);
         for (int r = 0; r < rn; ++r) {
-            unsigned long long a = shfl_min_u64(mnx[r]), b = shfl_max_u64(mxx[r]);
-            unsigned long long c = shfl_min_u64(mny[r]), d = shfl_max_u64(mxy[r]);
+            unsigned long long a = shfl_min_u64(mnx[r] == R(INFINITY) ? kOrdMinInit : ord_encode((double)mnx[r]));
+            unsigned long long b = shfl_max_u64(mxx[r] == R(-INFINITY) ? kOrdMaxInit : ord_encode((double)mxx[r]));
+            unsigned long long c = shfl_min_u64(mny[r] == R(INFINITY) ? kOrdMinInit : ord_encode((double)mny[r]));
+            unsigned long long d = shfl_max_u64(mxy[r] == R(-INFINITY) ? kOrdMaxInit : ord_encode((double)mxy[r]));
             if (lane == 0) { red[warp][0] = a; red[warp][1] = b; red[warp][2] = c; red[warp][3] = d; }
             __syncthreads();
             if (threadIdx.x < 4) {
