@@ -43,8 +43,8 @@ CONFIG = {
     "l2": "inputs larger than L2 (172 MB of particle coordinates per turn)",
 }
 # DRAM bytes (read + write) per field particle of one kick launch, from one `ncu --set full` capture of
-# the 15-pair front of this workload (285.4 MB for 3.584M field particles; profiles/kick_node_production.md).
-KICK_TRAFFIC_BYTES_PER_PARTICLE = 79.6
+# the 15-pair front of this workload (275.6 MB for 3.584M field particles).
+KICK_TRAFFIC_BYTES_PER_PARTICLE = 76.9
 
 
 def _dist():
