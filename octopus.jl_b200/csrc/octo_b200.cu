@@ -218,6 +218,10 @@ struct octo_ctx {
     std::vector<double> trace_lum;
     long long last_launches = 0;
     // per-phase device timing (octo_set_timing): event pairs recorded around each launch group
+    // second stream of the collide: each front's luminosity work overlaps its field solve (forked after the
+    // front's bounds, joined before its kick)
+    cudaStream_t lum_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int timing = 0;
     unsigned timing_mask = ~0u;  // phases timed when timing is on (octo_set_timing_phases)
     std::vector<cudaEvent_t> ev_pool;
@@ -955,6 +959,14 @@ void CollideJob::run() {
     C.lum_tick = c->lum_tick.p;
     C.nodes = c->nodes.p;
     const bool gaussian = c->dopt.gaussian != 0;
+    if (!c->lum_stream) {
+        CK(cudaStreamCreateWithFlags(&c->lum_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+    }
+    // nothing an earlier (failed) collide left on the luminosity stream may overlap this one
+    CK(cudaEventRecord(c->ev_join, c->lum_stream));
+    CK(cudaStreamWaitEvent(st, c->ev_join, 0));
     if (gaussian) {
         c->hyb.ensure(std::max(ntasks, 1));
         c->hmom.ensure((size_t)std::max(ntasks, 1) * kMaxBoundBlocks * kMomentSums);
@@ -998,6 +1010,25 @@ void CollideJob::run() {
             }
             launches += gaussian ? 3 : 1;
         }
+        bool lum_forked = false;
+        if (compute_lum && F.nl) {
+            CK(cudaEventRecord(c->ev_fork, st));
+            CK(cudaStreamWaitEvent(c->lum_stream, c->ev_fork, 0));
+            {
+                PhaseScope ps(c, OCTO_PHASE_LUMINOSITY, c->lum_stream, 2, slice_bytes * 4 * rsz);
+                unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(8, (F.maxlum + 32767) / 32768));
+                with_real(fp32, [&](auto r) {
+                    launch_method(lmethod, [&](auto M) {
+                        k_lum_deposit<decltype(r), decltype(M)::value><<<dim3(bpp, 2 * F.nl), 1024, lum_bytes, c->lum_stream>>>(
+                            C, F.l0, F.t0);
+                    });
+                });
+                k_lum_overlap<<<dim3(kLumSplit, F.nl), 256, 0, c->lum_stream>>>(C, F.l0);
+            }
+            CK(cudaEventRecord(c->ev_join, c->lum_stream));
+            lum_forked = true;
+            launches += 2;
+        }
         if (!node) {
             {
                 PhaseScope ps(c, OCTO_PHASE_PLAN, st, 1);
@@ -1011,17 +1042,6 @@ void CollideJob::run() {
                 CK(cudaMemsetAsync(c->qtot.p, 0, sizeof(unsigned long long) * F.np, st));
             }
             launches += gaussian ? 4 : 3;
-        }
-        if (compute_lum && F.nl) {
-            PhaseScope ps(c, OCTO_PHASE_LUMINOSITY, st, 2, slice_bytes * 4 * rsz);
-            unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(8, (F.maxlum + 32767) / 32768));
-            with_real(fp32, [&](auto r) {
-                launch_method(lmethod, [&](auto M) {
-                    k_lum_deposit<decltype(r), decltype(M)::value><<<dim3(bpp, 2 * F.nl), 1024, lum_bytes, st>>>(C, F.l0, F.t0);
-                });
-            });
-            k_lum_overlap<<<dim3(kLumSplit, F.nl), 256, 0, st>>>(C, F.l0);
-            launches += 2;
         }
         {
             PhaseScope ps(c, OCTO_PHASE_DEPOSIT, st, 1, src_bytes * 4 * rsz);
@@ -1048,6 +1068,7 @@ void CollideJob::run() {
                 k_conv_field<decltype(r)><<<dim3((ny + kFieldTile - 1) / kFieldTile, F.np), 128, field_smem(NX, rsz), st>>>(C, F.p0);
             });
         }
+        if (lum_forked) CK(cudaStreamWaitEvent(st, c->ev_join, 0));  // the kick changes what the luminosity read
         {
             PhaseScope ps(c, OCTO_PHASE_KICK, st, 1, fld_bytes * 11 * rsz);
             with_real(fp32, [&](auto r) {
@@ -1252,6 +1273,9 @@ void octo_destroy(octo_ctx *c) {
     c->hyb.release(); c->hmom.release(); c->hprof.release(); c->hsum.release(); c->qtot.release();
     c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_noderef.release(); c->h_slices.release();
     for (auto e : c->ev_pool) cudaEventDestroy(e);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->lum_stream) cudaStreamDestroy(c->lum_stream);
     delete c;
 }
 
