@@ -270,6 +270,29 @@ def run_ours(args, rank, world, local_rank):
         fast = {"ms": ms32, "lum": lum32, "phases": {k: v[0] / n_phase for k, v in ph32.items()}, "kick": kick32}
     clk = clocks.stop()
 
+    # long-term tracking of both forms from the same beams (outside every timed region, one GPU only):
+    # the relative emittance growth of each plane after --emittance-turns turns
+    emit = None
+    if world == 1 and args.emittance_turns > 0:
+        from octo_b200.diagnostics import emittances
+        emit = {"turns": args.emittance_turns}
+        for name, dt in (("plain", torch.float64), ("fast", torch.float32)):
+            if name == "fast" and args.no_fast:
+                continue
+            ee, pp = e.astype(dt), p.astype(dt)
+            ee.coords.copy_(e0.to(dt))
+            pp.coords.copy_(p0.to(dt))
+            cx = rt.context("ip", solver, local_rank, dt)
+            start = (emittances(ee), emittances(pp))
+            for t in range(args.emittance_turns):
+                cx.collide(ee, pp, turn=20_000 + t, stream=stream)
+                me.track(ee, stream=stream)
+                mp.track(pp, stream=stream)
+            torch.cuda.synchronize()
+            end = (emittances(ee), emittances(pp))
+            emit[name] = {beam: [end[k][q] / start[k][q] - 1.0 for q in range(3)]
+                          for k, beam in enumerate(("electron", "proton"))}
+
     if world > 1:
         import torch.distributed as dist
         tt = torch.tensor([ms, e2e_ms, fast["ms"] if fast else 0.0], device=dev, dtype=torch.float64)
@@ -337,6 +360,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roof,
         "cpu_baseline": cpu,
         "fast_form": fast_line,
+        "emittance_growth": emit,
         "clocks": clk,
         "luminosity": lum,
         "dominant_phase": dom[0],
@@ -357,6 +381,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
     ap.add_argument("--no-fast", action="store_true", help="skip the precision-form (float32) pass")
+    ap.add_argument("--emittance-turns", type=int, default=1000,
+                    help="turns of the emittance-growth comparison of both forms (0 skips it; one GPU only)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -93,3 +93,16 @@ def field_error(solver, sx: float, sy: float, dtype: torch.dtype = torch.float64
     norm = float(np.max(np.hypot(bx, by)))
     return {"rms": float(np.sqrt(np.mean(err * err)) / norm), "max": float(err.max() / norm),
             "aspect": sx / sy, "points": int(xp.size)}
+
+
+def emittances(beam) -> Tuple[float, float, float]:
+    """RMS emittances sqrt(<u^2><u'^2> - <u u'>^2) of the (x, px), (y, py), (z, pz) planes with population
+    moments, as beam_statistics reports them (Beam.jl:650-734); reduced in FP64 on the beam's device."""
+    c = beam.coords.to(torch.float64)
+    c = c - c.mean(dim=1, keepdim=True)
+    out = []
+    for k in range(3):
+        u, v = c[2 * k], c[2 * k + 1]
+        a, b, d = (u * u).mean(), (v * v).mean(), (u * v).mean()
+        out.append(float(torch.sqrt(torch.clamp(a * b - d * d, min=0.0))))
+    return tuple(out)
