@@ -372,6 +372,84 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+def scan_cases(n_cases=64, seed=SEED):
+    """Seeded batched-scan cases: N per beam log-uniform in [64k, 2.56M], slices uniform in 5..31, grid in
+    {64, 96, 128, 256}^2, sigma_x / sigma_y log-uniform in [1, 25] with sigma_y = 8.5 um."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    cases = []
+    for _ in range(n_cases):
+        n1, n2 = (int(np.exp(rng.uniform(np.log(64_000), np.log(2_560_000)))) for _ in range(2))
+        s1, s2 = (int(rng.integers(5, 32)) for _ in range(2))
+        g = int(rng.choice([64, 96, 128, 256]))
+        aspect = float(np.exp(rng.uniform(0.0, np.log(25.0))))
+        cases.append(dict(n1=n1, n2=n2, s1=s1, s2=s2, grid=g, aspect=aspect, rng=int(rng.integers(1, 2**31))))
+    return cases
+
+
+def run_scan(args, local_rank):
+    """The batched scan: independent collisions in the precision form, in batches of --scan-batch collides
+    overlapped on their own streams (octo_pic_collide_batch), against the same collides one by one."""
+    import torch
+    import octo_b200 as ob
+    dev = torch.device(f"cuda:{local_rank}")
+    torch.cuda.set_device(dev)
+    cases = scan_cases(args.scan_cases)
+    turns = args.scan_turns
+    sy = 8.5e-6
+
+    def make(case):
+        sol = ob.PICPoissonSolver(grid=(case["grid"], case["grid"]),
+                                  slicing1=ob.LongitudinalSlicing(nslices=case["s1"], method="normal_quantile"),
+                                  slicing2=ob.LongitudinalSlicing(nslices=case["s2"], method="normal_quantile"))
+        sx = case["aspect"] * sy
+        e = ob.Beam.gaussian(case["n1"], seed=case["rng"], charge=-1.0, mc2=ob.EMASS_EV, E0=10e9, npart=1.7e11,
+                             device=dev, dtype=torch.float32, beta=E_BEAM["beta"], sigma=(sx, sy, 7e-3), rng_id=1)
+        p = ob.Beam.gaussian(case["n2"], seed=case["rng"], charge=1.0, mc2=ob.PMASS_EV, E0=275e9, npart=6.9e10,
+                             device=dev, dtype=torch.float32, beta=P_BEAM["beta"], sigma=(sx, sy, 6e-2), rng_id=2)
+        return sol, e, p
+
+    times = {}
+    for mode in ("batched", "sequential"):
+        total_ms = 0.0
+        for g0 in range(0, len(cases), args.scan_batch):
+            group = [make(c) for c in cases[g0:g0 + args.scan_batch]]
+            ctxs = [ob.Context(sol, local_rank, torch.float32) for sol, _, _ in group]
+            streams = [torch.cuda.Stream(device=dev) for _ in group]
+            for t in range(2):  # warm-up turns (workspaces, Green caches)
+                ob.collide_batch(ctxs, [g[1] for g in group], [g[2] for g in group], turn=t, streams=streams)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for t in range(turns):
+                if mode == "batched":
+                    ob.collide_batch(ctxs, [g[1] for g in group], [g[2] for g in group], turn=2 + t, streams=streams)
+                else:
+                    for k, (sol, e, p) in enumerate(group):
+                        ctxs[k].collide(e, p, turn=2 + t)
+            torch.cuda.synchronize()
+            total_ms += (time.perf_counter() - t0) * 1e3
+            for c in ctxs:
+                c.close()
+            del group
+            torch.cuda.empty_cache()
+        times[mode] = total_ms
+    collide_turns = len(cases) * turns
+    line = {
+        "metric": "batched scan: s per collision-turn", "value": times["batched"] / 1e3 / collide_turns,
+        "unit": "s/collision-turn", "n_gpus": 1, "higher_is_better": False, "impl": "ours",
+        "sequential_value": times["sequential"] / 1e3 / collide_turns,
+        "batching_speedup": times["sequential"] / times["batched"],
+        "config": {"workload": "independent collisions, precision form (float32 beams), default PICPoissonSolver "
+                               "options (:slice_pair grid, slice-pair Green cache, CIC); N log-uniform 64k-2.56M per "
+                               "beam, slices 5..31, grids 64/96/128/256, aspect 1-25",
+                   "cases": len(cases), "turns": turns, "batch": args.scan_batch,
+                   "timing": "host wall clock around each group's turns after 2 warm-up turns, synchronized"},
+        "particles": sum(c["n1"] + c["n2"] for c in cases),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -381,6 +459,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
     ap.add_argument("--no-fast", action="store_true", help="skip the precision-form (float32) pass")
+    ap.add_argument("--scan", action="store_true", help="time the batched scan of independent collisions instead")
+    ap.add_argument("--scan-cases", type=int, default=64)
+    ap.add_argument("--scan-turns", type=int, default=20)
+    ap.add_argument("--scan-batch", type=int, default=8)
     ap.add_argument("--emittance-turns", type=int, default=1000,
                     help="turns of the emittance-growth comparison of both forms (0 skips it; one GPU only)")
     args = ap.parse_args()
@@ -390,6 +472,8 @@ def main():
     try:
         if args.impl == "reference":
             return run_reference(args, rank)
+        if args.scan:
+            return run_scan(args, local_rank) if rank == 0 else 0
         return run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
