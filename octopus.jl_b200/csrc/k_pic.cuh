@@ -402,6 +402,16 @@ __device__ __forceinline__ double kernel_integral(double x, double y) {
     if (r2 == 0.0) return 0.0;
     return (log(r2) - 3) * x * y + atan_ratio(y, x) * x * x + atan_ratio(x, y) * y * y;
 }
+// The same F with one arctangent: atan(x/y) = sign(xy) pi/2 - atan(y/x) off the axes; on an axis every term
+// vanishes (x = 0 or y = 0 gives F = 0 exactly, as atan_ratio does).  The second arctangent's rounding
+// changes F by an ulp of its magnitude, the level the Green table's second differences already carry.
+__device__ __forceinline__ double kernel_integral_1atan(double x, double y) {
+    if (x == 0.0 || y == 0.0) return 0.0;
+    const double r2 = x * x + y * y;
+    const double a = atan(y / x);
+    const double b = ((x > 0.0) == (y > 0.0) ? 1.5707963267948966 : -1.5707963267948966) - a;
+    return (log(r2) - 3) * x * y + a * x * x + b * y * y;
+}
 // One cell of the wrapped (2nx x 2ny) Green table (pic_cpu.jl:2478-2509).
 __device__ __forceinline__ double green_value(int green_type, int i, int j, int nx, int ny, double dx0, double dy0,
                                               double hx, double hy) {
@@ -461,7 +471,7 @@ __global__ void __launch_bounds__(128) k_green_rows(Collide C, int mode, int bas
             const int b = jj0 + rb, a = ca - nx;           // corner indices: cell b-1 "+" corner
             const double X = a > -nx ? (dx0 + (double)(a - 1) * hx) + half_hx : (dx0 + (double)a * hx) - half_hx;
             const double Y = b > -ny ? (dy0 + (double)(b - 1) * hy) + half_hy : (dy0 + (double)b * hy) - half_hy;
-            corner[e] = kernel_integral(X, Y);
+            corner[e] = kernel_integral_1atan(X, Y);
         }
     }
     __syncthreads();

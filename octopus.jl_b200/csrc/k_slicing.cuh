@@ -317,18 +317,18 @@ __global__ void __launch_bounds__(1024) k_slice_finish(const SliceArgs<R> A) {
     }
 }
 
-// Write the kicked slice-sorted coordinates back in caller order.
+// Write the kicked slice-sorted coordinates back in caller order.  z is left alone: a collide never
+// changes it, so the caller's z array already holds the final values.
 template <class R>
 __global__ void k_unsort(const int *__restrict__ perm, long long total, const R *sx, const R *spx, const R *sy,
-                         const R *spy, const R *sz, const R *spz, R *x, R *px, R *y, R *py, R *z, R *pz,
-                         const SliceInfo *info) {
+                         const R *spy, const R *spz, R *x, R *px, R *y, R *py, R *pz) {
     // total = padded length; padding positions carry perm = -1
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= total) return;
     int i = perm[p];
     if (i < 0) return;
     x[i] = sx[p]; px[i] = spx[p]; y[i] = sy[p];
-    py[i] = spy[p]; z[i] = sz[p]; pz[i] = spz[p];
+    py[i] = spy[p]; pz[i] = spz[p];
 }
 
 }  // namespace octo

@@ -1086,7 +1086,7 @@ void CollideJob::run() {
 
     // ---- back to caller order
     {
-        PhaseScope ps(c, OCTO_PHASE_UNSORT, st, 2, (double)(n1 + n2) * 12 * rsz);
+        PhaseScope ps(c, OCTO_PHASE_UNSORT, st, 2, (double)(n1 + n2) * 10 * rsz);
         for (int b = 0; b < 2; ++b) {
             const BeamWS &W = c->bw[b];
             const octo_beam &B = b == 0 ? *b1 : *b2;
@@ -1094,8 +1094,7 @@ void CollideJob::run() {
                 using R = decltype(r);
                 k_unsort<R><<<(unsigned)((W.total + 255) / 256), 256, 0, st>>>(
                     W.perm.p, W.total, (const R *)W.s[0].p, (const R *)W.s[1].p, (const R *)W.s[2].p,
-                    (const R *)W.s[3].p, (const R *)W.s[4].p, (const R *)W.s[5].p, (R *)B.x, (R *)B.px, (R *)B.y,
-                    (R *)B.py, (R *)B.z, (R *)B.pz, W.info.p);
+                    (const R *)W.s[3].p, (const R *)W.s[5].p, (R *)B.x, (R *)B.px, (R *)B.y, (R *)B.py, (R *)B.pz);
             });
             launches++;
         }
