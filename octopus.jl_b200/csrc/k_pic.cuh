@@ -1333,79 +1333,106 @@ __global__ void __launch_bounds__(kKickThreads, sizeof(R) == 8 ? 2 : 4) k_kick(C
 }
 
 // ------------------------------------------------------------------ node meshes
-// Per-slice boxes of the turn-start state (pic_cpu.jl:1317-1358).  Source mode: the source
-// slice drifted to every partner node, d = 0.5*(c_i - boundary_b) from `ref[sl*nref + b]`.
-// Field mode: each field particle drifted to the collision point of every source-slice center,
-// sh = 0.5*(z - c_i) with c_i = ref[i].  boxes: [sl][ref][4] ordered (xmin, xmax, ymin, ymax).
+// Per-slice boxes of the turn-start state (pic_cpu.jl:1317-1358), both beams and both roles in one
+// pass.  Row (beam bm, slice sl) has nref = 2*o + 1 drift references, o = the other beam's slice count:
+//   k <  o + 1: source role, the slice drifted to node k, x + px*d with d = 0.5*(c_sl - boundary_k);
+//   k >= o + 1: field role, the slice drifted to the collision point of the other beam's slice
+//               i = k - (o + 1), x + sh*px with sh = 0.5*(z - c_i).
+// ref[bm][sl*nref + k] holds d or c_i.  Source boxes go to sbox[bm] ([sl][node][4]), field boxes to
+// fbox[bm] ([field slice][source slice][4]), each ordered (xmin, xmax, ymin, ymax).
+// A block stages a tile of particles in shared memory once; its 16-lane rows of threads each take one
+// reference (4 groups of 16 references per block), so every particle is read from HBM once per turn.
+constexpr int kBoxTile = 512, kBoxLanes = 16, kBoxGroups = 4, kBoxThreads = 256;
 struct NodeBoxArgs {
-    const void *x, *px, *y, *py, *z;  // slice-sorted coordinates, element type R
-    long long start[kMaxSlices], count[kMaxSlices];
-    const double *ref;
-    unsigned long long *boxes;
+    const void *x[2], *px[2], *y[2], *py[2], *z[2];  // slice-sorted coordinates, element type R
+    long long start[2][kMaxSlices], count[2][kMaxSlices];
+    const double *ref[2];
+    unsigned long long *sbox[2], *fbox[2];
     int *nanf;
-    int nsl, nref, field_mode, pad;
+    int ns[2];
+    long long chunk;  // particles per block
 };
 
 template <class R>
-__global__ void __launch_bounds__(256) k_node_boxes(NodeBoxArgs A) {
-    const R *AX = (const R *)A.x, *APX = (const R *)A.px, *AY = (const R *)A.y, *APY = (const R *)A.py,
-            *AZ = (const R *)A.z;
-    const int sl = blockIdx.y;
-    const long long st = A.start[sl], n = A.count[sl];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    __shared__ unsigned long long red[8][4];
-    // Per-thread extrema with the native min/max (NaN is flagged separately; a +-0 tie cannot change a
-    // mesh built from them), encoded to ordered integers once per block for the atomics.
-    for (int r0 = 0; r0 < A.nref; r0 += 8) {
-        const int rn = min(8, A.nref - r0);
-        R mnx[8], mxx[8], mny[8], mxy[8];
-        R ref[8];
+__global__ void __launch_bounds__(kBoxThreads) k_node_boxes(NodeBoxArgs A) {
+    __shared__ R tile[5][kBoxTile];
+    __shared__ unsigned long long red[kBoxThreads / 32][kBoxLanes][4];
+    const int bm = (int)blockIdx.y < A.ns[0] ? 0 : 1;
+    const int sl = bm ? (int)blockIdx.y - A.ns[0] : (int)blockIdx.y;
+    const int o = A.ns[1 - bm], nb = o + 1, nref = nb + o;
+    const int g0 = blockIdx.z * kBoxGroups;
+    const long long n = A.count[bm][sl], k0 = (long long)blockIdx.x * A.chunk;
+    if (k0 >= n || g0 * kBoxLanes >= nref) return;  // block-uniform
+    const long long k1 = min(n, k0 + A.chunk), st = A.start[bm][sl];
+    const int ng = min(kBoxGroups, (nref - g0 * kBoxLanes + kBoxLanes - 1) / kBoxLanes);
+    const R *X = (const R *)A.x[bm], *PX = (const R *)A.px[bm], *Y = (const R *)A.y[bm],
+            *PY = (const R *)A.py[bm], *Z = (const R *)A.z[bm];
+    const int lane16 = threadIdx.x & (kBoxLanes - 1), prow = threadIdx.x / kBoxLanes;
+    constexpr int kRows = kBoxThreads / kBoxLanes;
+    R sref[kBoxGroups], mnx[kBoxGroups], mxx[kBoxGroups], mny[kBoxGroups], mxy[kBoxGroups];
+    bool fld[kBoxGroups], live[kBoxGroups];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            mnx[r] = mny[r] = R(INFINITY);
-            mxx[r] = mxy[r] = R(-INFINITY);
-            ref[r] = r < rn ? (R)(A.field_mode ? A.ref[r0 + r] : A.ref[(long long)sl * A.nref + r0 + r]) : R(0);
+    for (int g = 0; g < kBoxGroups; ++g) {
+        const int k = (g0 + g) * kBoxLanes + lane16;
+        live[g] = g < ng && k < nref;
+        fld[g] = k >= nb;
+        sref[g] = live[g] ? (R)A.ref[bm][(long long)sl * nref + k] : R(0);
+        mnx[g] = mny[g] = R(INFINITY);
+        mxx[g] = mxy[g] = R(-INFINITY);
+    }
+    bool nan = false;
+    for (long long t0 = k0; t0 < k1; t0 += kBoxTile) {
+        const int tn = (int)min((long long)kBoxTile, k1 - t0);
+        __syncthreads();  // the previous tile is consumed
+        for (int j = threadIdx.x; j < tn; j += kBoxThreads) {
+            const long long p = st + t0 + j;
+            tile[0][j] = X[p]; tile[1][j] = PX[p]; tile[2][j] = Y[p]; tile[3][j] = PY[p]; tile[4][j] = Z[p];
         }
-        bool nan = false;
-        for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-            const long long p = st + k;
-            const R x = AX[p], px = APX[p], y = AY[p], py = APY[p];
-            const R z = A.field_mode ? AZ[p] : R(0);
+        __syncthreads();
+        for (int j = prow; j < tn; j += kRows) {
+            const R x = tile[0][j], px = tile[1][j], y = tile[2][j], py = tile[3][j], z = tile[4][j];
 #pragma unroll
-            for (int r = 0; r < 8; ++r) {
-                if (r < rn) {
-                    R xv, yv;
-                    if (A.field_mode) {
-                        const R sh = R(0.5) * (z - ref[r]);
-                        xv = x + sh * px;
-                        yv = y + sh * py;
-                    } else {
-                        xv = x + px * ref[r];
-                        yv = y + py * ref[r];
-                    }
+            for (int g = 0; g < kBoxGroups; ++g) {
+                if (g < ng && live[g]) {
+                    const R s = fld[g] ? R(0.5) * (z - sref[g]) : sref[g];
+                    const R xv = x + s * px, yv = y + s * py;
                     nan |= (xv != xv) | (yv != yv);
-                    mnx[r] = fmin(mnx[r], xv); mxx[r] = fmax(mxx[r], xv);
-                    mny[r] = fmin(mny[r], yv); mxy[r] = fmax(mxy[r], yv);
+                    mnx[g] = fmin(mnx[g], xv); mxx[g] = fmax(mxx[g], xv);
+                    mny[g] = fmin(mny[g], yv); mxy[g] = fmax(mxy[g], yv);
                 }
             }
         }
-        int anynan = __syncthreads_or(nan);
-        if (anynan && threadIdx.x == 0) atomicOr(A.nanf, 1);
-        for (int r = 0; r < rn; ++r) {
-            unsigned long long a = shfl_min_u64(mnx[r] == R(INFINITY) ? kOrdMinInit : ord_encode((double)mnx[r]));
-            unsigned long long b = shfl_max_u64(mxx[r] == R(-INFINITY) ? kOrdMaxInit : ord_encode((double)mxx[r]));
-            unsigned long long c = shfl_min_u64(mny[r] == R(INFINITY) ? kOrdMinInit : ord_encode((double)mny[r]));
-            unsigned long long d = shfl_max_u64(mxy[r] == R(-INFINITY) ? kOrdMaxInit : ord_encode((double)mxy[r]));
-            if (lane == 0) { red[warp][0] = a; red[warp][1] = b; red[warp][2] = c; red[warp][3] = d; }
-            __syncthreads();
-            if (threadIdx.x < 4) {
-                unsigned long long v = red[0][threadIdx.x];
-                for (int w = 1; w < nw; ++w) v = (threadIdx.x & 1) ? max(v, red[w][threadIdx.x]) : min(v, red[w][threadIdx.x]);
-                unsigned long long *dst = A.boxes + ((long long)sl * A.nref + r0 + r) * 4 + threadIdx.x;
-                if (threadIdx.x & 1) atomicMax(dst, v); else atomicMin(dst, v);
-            }
-            __syncthreads();
+    }
+    if (__syncthreads_or(nan) && threadIdx.x == 0) atomicOr(A.nanf, 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int g = 0; g < ng; ++g) {
+        // lanes l and l + 16 of a warp hold the same reference
+        unsigned long long v[4] = {mnx[g] == R(INFINITY) ? kOrdMinInit : ord_encode((double)mnx[g]),
+                                   mxx[g] == R(-INFINITY) ? kOrdMaxInit : ord_encode((double)mxx[g]),
+                                   mny[g] == R(INFINITY) ? kOrdMinInit : ord_encode((double)mny[g]),
+                                   mxy[g] == R(-INFINITY) ? kOrdMaxInit : ord_encode((double)mxy[g])};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const unsigned long long w = __shfl_xor_sync(0xffffffffu, v[q], kBoxLanes);
+            v[q] = (q & 1) ? max(v[q], w) : min(v[q], w);
         }
+        if (lane < kBoxLanes) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) red[warp][lane][q] = v[q];
+        }
+        __syncthreads();
+        if (threadIdx.x < kBoxLanes * 4) {
+            const int r = threadIdx.x >> 2, q = threadIdx.x & 3;
+            unsigned long long a = red[0][r][q];
+            for (int w = 1; w < kBoxThreads / 32; ++w) a = (q & 1) ? max(a, red[w][r][q]) : min(a, red[w][r][q]);
+            const int k = (g0 + g) * kBoxLanes + r;
+            if (k < nref) {
+                unsigned long long *dst = k < nb ? A.sbox[bm] + ((long long)sl * nb + k) * 4 + q
+                                                 : A.fbox[bm] + ((long long)sl * o + (k - nb)) * 4 + q;
+                if (q & 1) atomicMax(dst, a); else atomicMin(dst, a);
+            }
+        }
+        __syncthreads();
     }
 }
 

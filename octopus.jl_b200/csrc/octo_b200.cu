@@ -403,9 +403,10 @@ __global__ void k_init_bounds(unsigned long long *bnd, int ntasks, unsigned long
     }
 }
 
-__global__ void k_init_boxes(unsigned long long *box, long long n4) {
+__global__ void k_init_boxes(unsigned long long *a, long long na, unsigned long long *b, long long nb) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n4) box[t] = (t & 1) ? kOrdMaxInit : kOrdMinInit;
+    if (t < na) a[t] = (t & 1) ? kOrdMaxInit : kOrdMinInit;
+    else if (t < na + nb) b[t - na] = (t & 1) ? kOrdMaxInit : kOrdMinInit;
 }
 
 // Device slicing of both beams in shared launches; returns after enqueueing (the slice tables are read
@@ -548,59 +549,64 @@ void build_node_meshes(octo_ctx *c, Collide &C, const SliceInfo &S1, const Slice
     c->nodes.ensure(nnode);
     c->nodenan.ensure(1);
     CK(cudaMemsetAsync(c->nodenan.p, 0, sizeof(int), st));
-    // staging per direction: ref [nss*nb + nss] doubles, then nss counts
-    const size_t per_dir = (size_t)kMaxSlices * (kMaxSlices + 2) + kMaxSlices;
-    c->h_noderef.ensure(2 * per_dir);
-    c->node_ref.ensure(2 * per_dir);
+    // staging: the drift references of each beam's rows ([slice][2*o + 1], o = the other beam's slice
+    // count: o + 1 node drifts, then the o field-role centres), then both beams' slice counts
+    const int nref1 = 2 * ns2 + 1, nref2 = 2 * ns1 + 1;
+    const size_t off2 = (size_t)ns1 * nref1, offc = off2 + (size_t)ns2 * nref2;
+    const size_t cap = 2 * (size_t)kMaxSlices * (2 * kMaxSlices + 1) + 2 * kMaxSlices;
+    c->h_noderef.ensure(cap);
+    c->node_ref.ensure(cap);
+    double *href = c->h_noderef.p;
+    for (int bm = 0; bm < 2; ++bm) {
+        const SliceInfo &SS = bm == 0 ? S1 : S2, &SO = bm == 0 ? S2 : S1;
+        const int ns = bm ? ns2 : ns1, o = bm ? ns1 : ns2, nref = 2 * o + 1;
+        double *r = href + (bm ? off2 : 0);
+        for (int sl = 0; sl < ns; ++sl) {
+            for (int b = 0; b <= o; ++b) r[(size_t)sl * nref + b] = 0.5 * (SS.center[sl] - SO.boundary[b]);
+            for (int i = 0; i < o; ++i) r[(size_t)sl * nref + o + 1 + i] = SO.center[i];
+        }
+    }
+    long long *hcnt = (long long *)(href + offc);
+    for (int s = 0; s < ns1; ++s) hcnt[s] = S1.count[s];
+    for (int s = 0; s < ns2; ++s) hcnt[ns1 + s] = S2.count[s];
+    CK(cudaMemcpyAsync(c->node_ref.p, href, sizeof(double) * (offc + ns1 + ns2), cudaMemcpyHostToDevice, st));
+    const long long *dcnt = (const long long *)(c->node_ref.p + offc);
     const int nbox_s = std::max(ns1 * (ns2 + 1), ns2 * (ns1 + 1)), nbox_f = ns1 * ns2;
     c->nodebox_s.ensure((size_t)2 * nbox_s * 4);
     c->nodebox_f.ensure((size_t)2 * nbox_f * 4);
-    for (int dir = 1; dir <= 2; ++dir) {
-        const SliceInfo &SS = dir == 1 ? S1 : S2;
-        const SliceInfo &SF = dir == 1 ? S2 : S1;
-        const int nss = dir == 1 ? ns1 : ns2, nsf = dir == 1 ? ns2 : ns1, nb = nsf + 1;
-        const int sbeam = dir - 1, fbeam = 2 - dir;
-        const int mesh0 = dir == 1 ? 0 : ns1 * (ns2 + 1);
-        double *href = c->h_noderef.p + (dir - 1) * per_dir;
-        double *dref = c->node_ref.p + (dir - 1) * per_dir;
-        for (int i = 0; i < nss; ++i) {
-            for (int b = 0; b < nb; ++b) href[(size_t)i * nb + b] = 0.5 * (SS.center[i] - SF.boundary[b]);
-            href[(size_t)nss * nb + i] = SS.center[i];
+    unsigned long long *sbox1 = c->nodebox_s.p, *sbox2 = c->nodebox_s.p + (size_t)nbox_s * 4;
+    unsigned long long *fbox1 = c->nodebox_f.p, *fbox2 = c->nodebox_f.p + (size_t)nbox_f * 4;
+    const long long ns8 = 8ll * nbox_s, nf8 = 8ll * nbox_f;
+    k_init_boxes<<<(unsigned)((ns8 + nf8 + 255) / 256), 256, 0, st>>>(c->nodebox_s.p, ns8, c->nodebox_f.p, nf8);
+    // one pass over both beams: beam 0's source role is direction 1, its field role direction 2
+    NodeBoxArgs A{};
+    long long maxn = 1;
+    for (int bm = 0; bm < 2; ++bm) {
+        const BeamWS &W = c->bw[bm];
+        const SliceInfo &SS = bm == 0 ? S1 : S2;
+        A.x[bm] = W.s[0].p; A.px[bm] = W.s[1].p; A.y[bm] = W.s[2].p; A.py[bm] = W.s[3].p; A.z[bm] = W.s[4].p;
+        for (int s = 0; s < c->ns[bm]; ++s) {
+            A.start[bm][s] = SS.start[s];
+            A.count[bm][s] = SS.count[s];
+            maxn = std::max(maxn, SS.count[s]);
         }
-        long long *hcnt = (long long *)(href + (size_t)nss * nb + nss);
-        long long *dcnt = (long long *)(dref + (size_t)nss * nb + nss);
-        for (int s = 0; s < nss; ++s) hcnt[s] = SS.count[s];
-        CK(cudaMemcpyAsync(dref, href, sizeof(double) * ((size_t)nss * nb + 2 * nss), cudaMemcpyHostToDevice, st));
-        unsigned long long *sbox = c->nodebox_s.p + (size_t)(dir - 1) * nbox_s * 4;
-        unsigned long long *fbox = c->nodebox_f.p + (size_t)(dir - 1) * nbox_f * 4;
-        long long ns4 = (long long)nss * nb * 4, nf4 = (long long)nsf * nss * 4;
-        k_init_boxes<<<(unsigned)((ns4 + 255) / 256), 256, 0, st>>>(sbox, ns4);
-        k_init_boxes<<<(unsigned)((nf4 + 255) / 256), 256, 0, st>>>(fbox, nf4);
-        NodeBoxArgs A{};
-        const BeamWS &WS = c->bw[sbeam], &WF = c->bw[fbeam];
-        A.x = WS.s[0].p; A.px = WS.s[1].p; A.y = WS.s[2].p; A.py = WS.s[3].p; A.z = WS.s[4].p;
-        long long maxn = 1;
-        for (int s = 0; s < nss; ++s) { A.start[s] = SS.start[s]; A.count[s] = SS.count[s]; maxn = std::max(maxn, SS.count[s]); }
-        A.ref = dref;
-        A.boxes = sbox;
-        A.nanf = c->nodenan.p;
-        A.nsl = nss; A.nref = nb; A.field_mode = 0;
-        unsigned bx = (unsigned)std::min<long long>(64, (maxn + 4095) / 4096);
-        with_real(c->fp32, [&](auto r) { k_node_boxes<decltype(r)><<<dim3(bx, nss), 256, 0, st>>>(A); });
-        NodeBoxArgs F{};
-        F.x = WF.s[0].p; F.px = WF.s[1].p; F.y = WF.s[2].p; F.py = WF.s[3].p; F.z = WF.s[4].p;
-        maxn = 1;
-        for (int s = 0; s < nsf; ++s) { F.start[s] = SF.start[s]; F.count[s] = SF.count[s]; maxn = std::max(maxn, SF.count[s]); }
-        F.ref = dref + (size_t)nss * nb;
-        F.boxes = fbox;
-        F.nanf = c->nodenan.p;
-        F.nsl = nsf; F.nref = nss; F.field_mode = 1;
-        bx = (unsigned)std::min<long long>(64, (maxn + 4095) / 4096);
-        with_real(c->fp32, [&](auto r) { k_node_boxes<decltype(r)><<<dim3(bx, nsf), 256, 0, st>>>(F); });
-        k_node_plan<<<(nss * nb + 63) / 64, 64, 0, st>>>(c->dopt, sbox, fbox, nss, nb, dcnt, c->nodenan.p,
-                                                         c->nodes.p + mesh0, c->status.p);
-        launches += 5;
+        A.ns[bm] = c->ns[bm];
     }
+    A.ref[0] = c->node_ref.p; A.ref[1] = c->node_ref.p + off2;
+    A.sbox[0] = sbox1; A.sbox[1] = sbox2;
+    A.fbox[0] = fbox2; A.fbox[1] = fbox1;
+    A.nanf = c->nodenan.p;
+    const long long bx = std::min<long long>(256, (maxn + 4095) / 4096);
+    A.chunk = ((maxn + bx - 1) / bx + kBoxTile - 1) / kBoxTile * kBoxTile;
+    const int gz = (std::max(nref1, nref2) + kBoxLanes * kBoxGroups - 1) / (kBoxLanes * kBoxGroups);
+    with_real(c->fp32, [&](auto r) {
+        k_node_boxes<decltype(r)><<<dim3((unsigned)bx, ns1 + ns2, gz), kBoxThreads, 0, st>>>(A);
+    });
+    k_node_plan<<<(ns1 * (ns2 + 1) + 63) / 64, 64, 0, st>>>(c->dopt, sbox1, fbox1, ns1, ns2 + 1, dcnt, c->nodenan.p,
+                                                           c->nodes.p, c->status.p);
+    k_node_plan<<<(ns2 * (ns1 + 1) + 63) / 64, 64, 0, st>>>(c->dopt, sbox2, fbox2, ns2, ns1 + 1, dcnt + ns1,
+                                                           c->nodenan.p, c->nodes.p + ns1 * (ns2 + 1), c->status.p);
+    launches += 4;
     // Green spectra of every valid node mesh
     const int NX = 2 * c->opt.nx, NY = 2 * c->opt.ny;
     C.nodes = c->nodes.p;
