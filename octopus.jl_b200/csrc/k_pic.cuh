@@ -4,6 +4,7 @@
 #pragma once
 #include "be_device.cuh"
 #include "fft.cuh"
+#include "rfft.cuh"
 #include "geometry.cuh"
 #include "octo_internal.cuh"
 
@@ -541,6 +542,119 @@ __global__ void __launch_bounds__(128) k_green_cols(Collide C, int mode, int bas
     for (int j = lane; j < NY; j += 32) col[j] = line[fft_out(fy, j)];
 }
 
+// Register-FFT forms of the two Green kernels (rfft.cuh) for NX = 8 Gx and NY = 8 Gy.  Rows: the block
+// covers 8 * (32 / G) table rows, two per line, and the spectrum leaves in the same natural layout as
+// k_green_rows'.  Columns: each line is one x-frequency column, stored back in register order
+// (entry r * G + l holds frequency rf_spec(l, r)), the order k_conv_cols_r multiplies in.
+template <int G>
+__global__ void __launch_bounds__(128) k_green_rows_r(Collide C, int mode, int base, int node_slot0) {
+    using RG = RfGeom<G>;
+    constexpr int LPW = 32 / G, ROWS = 8 * LPW;
+    double2 *sm = (double2 *)g_smem;
+    const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx, NY = 2 * ny;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, line = lane / G, l = lane & (G - 1);
+    double2 *T = sm, *S = sm + RG::kTables + warp * RG::kWarpScratch;
+    double *corner = (double *)(sm + RG::kTables + 4 * RG::kWarpScratch);  // (ROWS + 1) x (NX + 1)
+    Grid sg, fg;
+    int slot;
+    if (mode == 0) {
+        const TaskGeom &Gm = C.geom[base + blockIdx.y];
+        if (!Gm.rebuild) return;
+        sg = Gm.sg; fg = Gm.fg; slot = Gm.green;
+    } else {
+        const NodeMesh &M = C.nodes[base + blockIdx.y];
+        if (!M.valid) return;
+        sg = M.sg; fg = M.fg; slot = node_slot0 + base + blockIdx.y;
+    }
+    rf_tables<G>(T, C.tw_x);
+    const double hx = sg.w / (double)(nx - 1), hy = sg.h / (double)(ny - 1);
+    const double dx0 = fg.x0 - sg.x0, dy0 = fg.y0 - sg.y0;
+    const double half_hx = hx / 2, half_hy = hy / 2;
+    const int j0 = blockIdx.x * ROWS;      // rows j0 .. j0 + ROWS - 1 (ROWS divides ny)
+    const int jj0 = j0 < ny ? j0 : j0 - NY;
+    const bool integrated = C.o.green_type == 0;
+    if (integrated) {
+        for (int e = threadIdx.x; e < (ROWS + 1) * (NX + 1); e += blockDim.x) {
+            const int rb = e / (NX + 1), ca = e % (NX + 1);
+            const int b = jj0 + rb, a = ca - nx;
+            const double X = a > -nx ? (dx0 + (double)(a - 1) * hx) + half_hx : (dx0 + (double)a * hx) - half_hx;
+            const double Y = b > -ny ? (dy0 + (double)(b - 1) * hy) + half_hy : (dy0 + (double)b * hy) - half_hy;
+            corner[e] = kernel_integral_1atan(X, Y);
+        }
+    }
+    __syncthreads();
+    const double hxihyi = -0.5 / (hx * hy);
+    const int r0 = 2 * (warp * LPW + line);
+    double2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int i = l + G * m, ii = i < nx ? i : i - NX;
+        double g[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int r = r0 + q;
+            if (integrated) {
+                const double *lo = corner + r * (NX + 1), *hi = corner + (r + 1) * (NX + 1);
+                const int a = ii + nx;
+                double val = hi[a + 1];
+                val += lo[a];
+                val -= lo[a + 1];
+                val -= hi[a];
+                g[q] = hxihyi * val;
+            } else {
+                g[q] = green_value(C.o.green_type, i, j0 + r, nx, ny, dx0, dy0, hx, hy);
+            }
+        }
+        v[m] = make_double2(g[0], g[1]);
+    }
+    rf_fwd<G>(v, S, T);
+    double2 *Sl = S + line * 8 * G;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) Sl[rf_nat(rf_spec<G>(l, r))] = v[r];
+    __syncwarp();
+    const int ja = j0 + r0, jb = ja + 1;
+    double2 *out = C.ghat + (long long)slot * C.gstride;
+    for (int k = l; k <= nx; k += G) {
+        const double2 zk = Sl[rf_nat(k)], zm = conjg(Sl[rf_nat((NX - k) % NX)]);
+        const double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y + zm.y));
+        const double2 D = csub(zk, zm);
+        out[(long long)k * NY + ja] = A;
+        out[(long long)k * NY + jb] = make_double2(0.5 * D.y, -0.5 * D.x);
+    }
+}
+
+template <int G>
+__global__ void __launch_bounds__(128) k_green_cols_r(Collide C, int mode, int base, int node_slot0) {
+    using RG = RfGeom<G>;
+    constexpr int LPW = 32 / G;
+    double2 *sm = (double2 *)g_smem;
+    const int nx = C.o.nx, NY = 2 * C.o.ny;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, line = lane / G, l = lane & (G - 1);
+    double2 *T = sm, *S = sm + RG::kTables + warp * RG::kWarpScratch;
+    int slot;
+    if (mode == 0) {
+        const TaskGeom &Gm = C.geom[base + blockIdx.y];
+        if (!Gm.rebuild) return;
+        slot = Gm.green;
+    } else {
+        if (!C.nodes[base + blockIdx.y].valid) return;
+        slot = node_slot0 + base + blockIdx.y;
+    }
+    rf_tables<G>(T, C.tw_y);
+    __syncthreads();
+    const int k = (blockIdx.x * 4 + warp) * LPW + line;
+    const bool ok = k <= nx;
+    double2 *col = C.ghat + (long long)slot * C.gstride + (long long)k * NY;
+    double2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) v[m] = ok ? col[l + G * m] : make_double2(0.0, 0.0);
+    rf_fwd<G>(v, S, T);
+    if (ok) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) col[r * G + l] = v[r];
+    }
+}
+
 // ------------------------------------------------------------------ deposition
 // Fixed-point CIC/TSC taps of one particle (pic_cpu.jl:2129-2146): q = round(w * 2^bits) added to an int64
 // grid (a block-private shared-memory copy, merged into the plane's grid at the end of the block).
@@ -956,13 +1070,49 @@ __device__ __forceinline__ void load_cell(const float4 *F, long long c, float &p
     ex = v.x; ey = v.y; phi = v.z;
 }
 
+// E = -grad(phi) on rows [jt0, jt1) of a plane (pic_cpu.jl:2531-2591) from the phi rows [ja0, ja1) held in
+// shared memory, stored as field cells; the :node Z plane stores only its phi, into its L plane's w word.
+template <class R>
+__device__ __forceinline__ void field_cells(const Collide &C, const Plane &P, int pl, const Grid &sg, const R *phi,
+                                            int ja0, int jt0, int jt1) {
+    using FC = typename RealT<R>::FC;
+    const int nx = C.o.nx, ny = C.o.ny;
+    const double hx = sg.w / (double)(nx - 1), hy = sg.h / (double)(ny - 1);
+    const R hxi = (R)(1.0 / hx), hyi = (R)(1.0 / hy);
+    const R c4 = (R)(1.0 / 12.0);
+    const bool fourth = C.o.fourth != 0;
+    const bool zplane = P.kind == 3;  // :node Z plane: only its phi is used, stored in its L plane's w word
+    FC *F = (FC *)C.fields + (long long)(zplane ? pl - 2 : pl) * RealT<R>::kCellVec * nx * ny;
+    auto Pv = [&](int i, int j) { return phi[(j - ja0) * nx + i]; };  // 0-based i, j
+    for (int idx = threadIdx.x; idx < (jt1 - jt0) * nx; idx += blockDim.x) {
+        const int j = jt0 + idx / nx, i = idx % nx;
+        if (zplane) {
+            store_w(F, (long long)j * nx + i, Pv(i, j));
+            continue;
+        }
+        R ey, ex;
+        // Ey (pic_cpu.jl:2553-2572), 1-based j' = j+1
+        if (j == 0) ey = hyi * (R(1.5) * Pv(i, 0) - R(2) * Pv(i, 1) + R(0.5) * Pv(i, 2));
+        else if (j == ny - 1) ey = hyi * (R(-1.5) * Pv(i, ny - 1) + R(2) * Pv(i, ny - 2) - R(0.5) * Pv(i, ny - 3));
+        else if (fourth && (j == 1 || j == ny - 2)) ey = R(0.5) * hyi * (Pv(i, j - 1) - Pv(i, j + 1));
+        else if (fourth) ey = c4 * hyi * ((Pv(i, j + 2) - Pv(i, j - 2)) + R(8) * (Pv(i, j - 1) - Pv(i, j + 1)));
+        else ey = R(0.5) * hyi * (Pv(i, j - 1) - Pv(i, j + 1));
+        // Ex (pic_cpu.jl:2573-2590)
+        if (i == 0) ex = hxi * (R(1.5) * Pv(0, j) - R(2) * Pv(1, j) + R(0.5) * Pv(2, j));
+        else if (i == nx - 1) ex = hxi * (R(-1.5) * Pv(nx - 1, j) + R(2) * Pv(nx - 2, j) - R(0.5) * Pv(nx - 3, j));
+        else if (fourth && (i == 1 || i == nx - 2)) ex = R(0.5) * hxi * (Pv(i - 1, j) - Pv(i + 1, j));
+        else if (fourth) ex = c4 * hxi * ((Pv(i + 2, j) - Pv(i - 2, j)) + R(8) * (Pv(i - 1, j) - Pv(i + 1, j)));
+        else ex = R(0.5) * hxi * (Pv(i - 1, j) - Pv(i + 1, j));
+        store_cell(F, (long long)j * nx + i, Pv(i, j), ex, ey);
+    }
+}
+
 // Inverse x-transform (two Hermitian rows per complex line) producing phi for a tile of rows plus a
 // two-row halo, then E = -grad(phi) on the tile (pic_cpu.jl:2531-2591).
 constexpr int kFieldTile = 8;
 template <class R>
 __global__ void __launch_bounds__(128) k_conv_field(Collide C, int plane0) {
     using C2 = typename RealT<R>::C2;
-    using FC = typename RealT<R>::FC;
     C2 *sm = (C2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx, NY = 2 * ny;
     const FftLen fx = fft_len(NX);
@@ -1014,34 +1164,184 @@ __global__ void __launch_bounds__(128) k_conv_field(Collide C, int plane0) {
         __syncwarp();
     }
     __syncthreads();
-    const double hx = sg.w / (double)(nx - 1), hy = sg.h / (double)(ny - 1);
-    const R hxi = (R)(1.0 / hx), hyi = (R)(1.0 / hy);
-    const R c4 = (R)(1.0 / 12.0);
-    const bool fourth = C.o.fourth != 0;
-    const bool zplane = P.kind == 3;  // :node Z plane: only its phi is used, stored in its L plane's w word
-    FC *F = (FC *)C.fields + (long long)(zplane ? pl - 2 : pl) * RealT<R>::kCellVec * nx * ny;
-    auto Pv = [&](int i, int j) { return phi[(j - ja0) * nx + i]; };  // 0-based i, j
-    for (int idx = threadIdx.x; idx < (jt1 - jt0) * nx; idx += blockDim.x) {
-        const int j = jt0 + idx / nx, i = idx % nx;
-        if (zplane) {
-            store_w(F, (long long)j * nx + i, Pv(i, j));
-            continue;
-        }
-        R ey, ex;
-        // Ey (pic_cpu.jl:2553-2572), 1-based j' = j+1
-        if (j == 0) ey = hyi * (R(1.5) * Pv(i, 0) - R(2) * Pv(i, 1) + R(0.5) * Pv(i, 2));
-        else if (j == ny - 1) ey = hyi * (R(-1.5) * Pv(i, ny - 1) + R(2) * Pv(i, ny - 2) - R(0.5) * Pv(i, ny - 3));
-        else if (fourth && (j == 1 || j == ny - 2)) ey = R(0.5) * hyi * (Pv(i, j - 1) - Pv(i, j + 1));
-        else if (fourth) ey = c4 * hyi * ((Pv(i, j + 2) - Pv(i, j - 2)) + R(8) * (Pv(i, j - 1) - Pv(i, j + 1)));
-        else ey = R(0.5) * hyi * (Pv(i, j - 1) - Pv(i, j + 1));
-        // Ex (pic_cpu.jl:2573-2590)
-        if (i == 0) ex = hxi * (R(1.5) * Pv(0, j) - R(2) * Pv(1, j) + R(0.5) * Pv(2, j));
-        else if (i == nx - 1) ex = hxi * (R(-1.5) * Pv(nx - 1, j) + R(2) * Pv(nx - 2, j) - R(0.5) * Pv(nx - 3, j));
-        else if (fourth && (i == 1 || i == nx - 2)) ex = R(0.5) * hxi * (Pv(i - 1, j) - Pv(i + 1, j));
-        else if (fourth) ex = c4 * hxi * ((Pv(i + 2, j) - Pv(i - 2, j)) + R(8) * (Pv(i - 1, j) - Pv(i + 1, j)));
-        else ex = R(0.5) * hxi * (Pv(i - 1, j) - Pv(i + 1, j));
-        store_cell(F, (long long)j * nx + i, Pv(i, j), ex, ey);
+    field_cells<R>(C, P, pl, sg, phi, ja0, jt0, jt1);
+}
+
+// Register-FFT forms of the three convolution kernels (rfft.cuh) for NX = 8 Gx (rows, field) and
+// NY = 8 Gy (columns); the arithmetic around the transforms is that of k_conv_rows, k_conv_cols and
+// k_conv_field.  Lines that fall outside the plane (ok == false) still take part in the warp's
+// transforms, on zeros, and store nothing.
+template <class R, int G>
+__global__ void __launch_bounds__(128) k_conv_rows_r(Collide C, int plane0) {
+    using C2 = typename RealT<R>::C2;
+    using RG = RfGeom<G>;
+    constexpr int LPW = 32 / G;
+    C2 *sm = (C2 *)g_smem;
+    const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx;
+    const int pl = blockIdx.y;
+    const Plane &P = C.planes[plane0 + pl];
+    if (plane_green(C, P) < 0) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, line = lane / G, l = lane & (G - 1);
+    C2 *T = sm, *S = sm + RG::kTables + warp * RG::kWarpScratch;
+    rf_tables<G>(T, (const C2 *)C.twr_x);
+    __syncthreads();
+    const int j0 = 2 * ((blockIdx.x * 4 + warp) * LPW + line), j1 = j0 + 1;
+    const bool ok = j0 < ny;
+    const double inv = ldexp(1.0, -P.fixed_bits);
+    long long *q = C.qgrid + (long long)pl * nx * ny;
+    constexpr bool kPrecision = sizeof(R) == 4;
+    const long long *qo = q + (long long)P.other_delta * nx * ny;
+    const bool diff = kPrecision && P.other_delta != 0;
+    const long long sgn = P.self_first ? 1 : -1;
+    const bool hyb = C.o.gaussian && C.hyb[P.task].mode;
+    const double *gx = C.hprof + (long long)pl * (nx + ny), *gy = gx + nx;
+    double gj0 = 0.0, gj1 = 0.0;
+    if (hyb && ok) {
+        const double sgx = C.hsum[2 * pl], sgy = C.hsum[2 * pl + 1];
+        double amp = (double)P.src_n;
+        if (C.o.neutralize && sgx * sgy > 0.0) amp = ((double)(long long)C.qtot[pl] * inv) / (sgx * sgy);
+        gj0 = amp * gy[j0];
+        if (j1 < ny) gj1 = amp * gy[j1];
     }
+    C2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        v[m].x = R(0);
+        v[m].y = R(0);
+        const int i = l + G * m;
+        if (m < 4 && ok) {  // i < nx = 4 G
+            long long qa = q[(long long)j0 * nx + i];
+            if (diff) qa = sgn * (qa - qo[(long long)j0 * nx + i]);
+            v[m].x = hyb ? (R)((double)qa * inv - gx[i] * gj0) : (R)((double)qa * inv);
+            if (!kPrecision && qa) q[(long long)j0 * nx + i] = 0;
+            if (j1 < ny) {
+                long long qb = q[(long long)j1 * nx + i];
+                if (diff) qb = sgn * (qb - qo[(long long)j1 * nx + i]);
+                v[m].y = hyb ? (R)((double)qb * inv - gx[i] * gj1) : (R)((double)qb * inv);
+                if (!kPrecision && qb) q[(long long)j1 * nx + i] = 0;
+            }
+        }
+    }
+    rf_fwd<G>(v, S, T);
+    C2 *Sl = S + line * 8 * G;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) Sl[rf_nat(rf_spec<G>(l, r))] = v[r];
+    __syncwarp();
+    if (!ok) return;
+    C2 *H = (C2 *)C.spec + (long long)pl * (nx + 1) * ny;
+    for (int k = l; k <= nx; k += G) {
+        const C2 zk = Sl[rf_nat(k)], zm = conjg(Sl[rf_nat((NX - k) % NX)]);
+        C2 A, B;
+        A.x = R(0.5) * (zk.x + zm.x);
+        A.y = R(0.5) * (zk.y + zm.y);
+        const C2 D = csub(zk, zm);
+        B.x = R(0.5) * D.y;
+        B.y = R(-0.5) * D.x;
+        H[(long long)k * ny + j0] = A;
+        if (j1 < ny) H[(long long)k * ny + j1] = B;
+    }
+}
+
+template <class R, int G>
+__global__ void __launch_bounds__(128) k_conv_cols_r(Collide C, int plane0) {
+    using C2 = typename RealT<R>::C2;
+    using RG = RfGeom<G>;
+    constexpr int LPW = 32 / G;
+    C2 *sm = (C2 *)g_smem;
+    const int nx = C.o.nx, ny = C.o.ny, NY = 2 * ny;
+    const int pl = blockIdx.y;
+    const Plane &P = C.planes[plane0 + pl];
+    const int slot = plane_green(C, P);
+    if (slot < 0) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, line = lane / G, l = lane & (G - 1);
+    C2 *T = sm, *S = sm + RG::kTables + warp * RG::kWarpScratch;
+    rf_tables<G>(T, (const C2 *)C.twr_y);
+    __syncthreads();
+    const int k = (blockIdx.x * 4 + warp) * LPW + line;
+    const bool ok = k <= nx;
+    C2 *col = (C2 *)C.spec + ((long long)pl * (nx + 1) + k) * ny;
+    C2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        v[m].x = R(0);
+        v[m].y = R(0);
+        if (m < 4 && ok) v[m] = col[l + G * m];  // rows j < ny = 4 G; the zero padding above
+    }
+    rf_fwd<G>(v, S, T);
+    const double2 *g = C.ghat + (long long)slot * C.gstride + (long long)k * NY;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const double2 gv = ok ? g[r * G + l] : make_double2(0.0, 0.0);
+        C2 gg;
+        gg.x = (R)gv.x;
+        gg.y = (R)gv.y;
+        v[r] = cmul(v[r], gg);
+    }
+    rf_inv<G>(v, S, T);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 4; ++m) col[l + G * m] = v[m];
+    }
+}
+
+// Tile of 12 rows: with the two-row halo, 16 rows = 8 lines, two per warp (G = 32).
+constexpr int kFieldTileR = 12;
+template <class R, int G>
+__global__ void __launch_bounds__(128) k_conv_field_r(Collide C, int plane0) {
+    using C2 = typename RealT<R>::C2;
+    using RG = RfGeom<G>;
+    constexpr int LPW = 32 / G;
+    C2 *sm = (C2 *)g_smem;
+    const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx, NY = 2 * ny;
+    const int pl = blockIdx.y;
+    const Plane &P = C.planes[plane0 + pl];
+    if (plane_green(C, P) < 0) return;
+    Grid sg;
+    if (P.geom >= 0) sg = C.nodes[P.geom].sg;
+    else sg = C.geom[P.task].sg;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, line = lane / G, l = lane & (G - 1);
+    C2 *T = sm, *S = sm + RG::kTables + warp * RG::kWarpScratch;
+    R *phi = (R *)(sm + RG::kTables + 4 * RG::kWarpScratch);  // (kFieldTileR + 4) rows x nx
+    rf_tables<G>(T, (const C2 *)C.twr_x);
+    __syncthreads();
+    const int jt0 = blockIdx.x * kFieldTileR;
+    const int jt1 = min(jt0 + kFieldTileR, ny);
+    const int ja0 = max(jt0 - 2, 0), ja1 = min(jt1 + 2, ny);
+    const int nrows = ja1 - ja0;
+    const C2 *H = (const C2 *)C.spec + (long long)pl * (nx + 1) * ny;
+    const R scale = (R)(1.0 / ((double)NX * (double)NY));
+    for (int rp0 = warp * LPW; 2 * rp0 < nrows; rp0 += 4 * LPW) {  // warp-uniform trip count
+        const int ra = ja0 + 2 * (rp0 + line), rb = ra + 1;
+        const bool ha = ra < ja1, hb = rb < ja1;
+        C2 v[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int k = rf_spec<G>(l, r);
+            C2 ca, cb;
+            ca.x = ca.y = cb.x = cb.y = R(0);
+            if (ha) {
+                if (k <= nx) {
+                    ca = H[(long long)k * ny + ra];
+                    if (hb) cb = H[(long long)k * ny + rb];
+                } else {
+                    ca = conjg(H[(long long)(NX - k) * ny + ra]);
+                    if (hb) cb = conjg(H[(long long)(NX - k) * ny + rb]);
+                }
+            }
+            v[r].x = ca.x - cb.y;
+            v[r].y = ca.y + cb.x;
+        }
+        rf_inv<G>(v, S, T);
+        if (ha) {
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {  // i = l + G m < nx
+                phi[(ra - ja0) * nx + l + G * m] = v[m].x * scale;
+                if (hb) phi[(rb - ja0) * nx + l + G * m] = v[m].y * scale;
+            }
+        }
+    }
+    __syncthreads();
+    field_cells<R>(C, P, pl, sg, phi, ja0, jt0, jt1);
 }
 
 // ------------------------------------------------------------------ kick

@@ -517,6 +517,22 @@ size_t green_smem(int NX) { return fft_smem(NX) + sizeof(double) * (size_t)(kGre
 size_t field_smem(int NX, size_t real = sizeof(double)) {
     return fft_smem(NX, real) + real * (size_t)(kFieldTile + 4) * (NX / 2);
 }
+// Register-FFT kernels (rfft.cuh): twiddle tables + one 256-element scratch per warp.
+size_t rf_smem(int G, size_t real) {
+    const int tables = G == 32 ? RfGeom<32>::kTables : G == 16 ? RfGeom<16>::kTables : RfGeom<8>::kTables;
+    return 2 * real * (size_t)(tables + 4 * RfGeom<8>::kWarpScratch);
+}
+template <class F>
+void with_rf(int G, F f) {
+    if (G == 32) f(std::integral_constant<int, 32>());
+    else if (G == 16) f(std::integral_constant<int, 16>());
+    else f(std::integral_constant<int, 8>());
+}
+// Lanes per line of the register FFT for the x-lines (rows, field) and y-lines (columns), 0 where the
+// shared-memory FFT of fft.cuh runs.  The Green spectra are stored in the column transform's order, so
+// k_green_cols* and k_conv_cols* always take the same path (both decide from NY alone).
+int rf_rows(int nx) { return rf_lanes(2 * nx); }
+int rf_cols(int ny) { return rf_lanes(2 * ny); }
 constexpr size_t kSmemLimit = 227 * 1024;
 
 // Raise the dynamic shared-memory limit of every kernel launched with more than 48 KB to the B200 opt-in
@@ -537,6 +553,45 @@ void set_smem_limits() {
     };
     per_real(double(0));
     per_real(float(0));
+    auto per_g = [&](auto g) {
+        constexpr int G = decltype(g)::value;
+        CK(cudaFuncSetAttribute(k_green_rows_r<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(k_green_cols_r<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        auto per_r = [&](auto r) {
+            using R = decltype(r);
+            CK(cudaFuncSetAttribute(k_conv_rows_r<R, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            CK(cudaFuncSetAttribute(k_conv_cols_r<R, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            CK(cudaFuncSetAttribute(k_conv_field_r<R, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        };
+        per_r(double(0));
+        per_r(float(0));
+    };
+    per_g(std::integral_constant<int, 8>());
+    per_g(std::integral_constant<int, 16>());
+    per_g(std::integral_constant<int, 32>());
+}
+
+// Green spectra of `count` meshes (mode 0: the front's tasks from `base`; mode 1: node meshes).
+void launch_green(const octo_ctx *c, const Collide &C, int mode, int base, int count, cudaStream_t st) {
+    const int nx = c->opt.nx, ny = c->opt.ny, NX = 2 * nx, NY = 2 * ny;
+    const int gx = rf_rows(nx), gy = rf_cols(ny);
+    if (gx && ny % (8 * (32 / gx)) == 0) {  // a block's rows never straddle the wrap at row ny
+        with_rf(gx, [&](auto g) {
+            constexpr int G = decltype(g)::value, ROWS = 8 * (32 / G);
+            const size_t sm = rf_smem(G, sizeof(double)) + sizeof(double) * (size_t)(ROWS + 1) * (NX + 1);
+            k_green_rows_r<G><<<dim3(NY / ROWS, count), 128, sm, st>>>(C, mode, base, 0);
+        });
+    } else {
+        k_green_rows<<<dim3(NY / kGreenRows, count), 128, green_smem(NX), st>>>(C, mode, base, 0);
+    }
+    if (gy) {
+        with_rf(gy, [&](auto g) {
+            constexpr int G = decltype(g)::value, PER = 4 * (32 / G);
+            k_green_cols_r<G><<<dim3((nx + 1 + PER - 1) / PER, count), 128, rf_smem(G, sizeof(double)), st>>>(C, mode, base, 0);
+        });
+    } else {
+        k_green_cols<<<dim3((nx + 1 + 3) / 4, count), 128, fft_smem(NY), st>>>(C, mode, base, 0);
+    }
 }
 
 // Enqueue the node meshes of both directions (pic_cpu.jl:1404-1419) with no host synchronisation: the
@@ -608,10 +663,8 @@ void build_node_meshes(octo_ctx *c, Collide &C, const SliceInfo &S1, const Slice
                                                            c->nodenan.p, c->nodes.p + ns1 * (ns2 + 1), c->status.p);
     launches += 4;
     // Green spectra of every valid node mesh
-    const int NX = 2 * c->opt.nx, NY = 2 * c->opt.ny;
     C.nodes = c->nodes.p;
-    k_green_rows<<<dim3(NY / kGreenRows, nnode), 128, green_smem(NX), st>>>(C, 1, 0, 0);
-    k_green_cols<<<dim3((c->opt.nx + 1 + 3) / 4, nnode), 128, fft_smem(NY), st>>>(C, 1, 0, 0);
+    launch_green(c, C, 1, 0, nnode, st);
     launches += 2;
 }
 
@@ -701,6 +754,7 @@ void CollideJob::run() {
     const SliceInfo S1 = c->h_slices.p[0], S2 = c->h_slices.p[1];
     const int ns1 = c->ns[0], ns2 = c->ns[1];
     const int nx = o.nx, ny = o.ny, NX = 2 * nx, NY = 2 * ny;
+    const int gx = rf_rows(nx), gy = rf_cols(ny);
     const int lnx = c->dopt.lnx, lny = c->dopt.lny;
     const bool node = o.interaction_grid == OCTO_GRID_NODE;
     const bool lk = o.longitudinal_kick != 0;
@@ -1041,8 +1095,7 @@ void CollideJob::run() {
                 k_plan<<<(F.nt + 63) / 64, 64, 0, st>>>(C, F.t0, F.nt, 0);
             }
             PhaseScope ps(c, OCTO_PHASE_GREEN, st, gaussian ? 3 : 2);
-            k_green_rows<<<dim3(NY / kGreenRows, F.nt), 128, green_smem(NX), st>>>(C, 0, F.t0, 0);
-            k_green_cols<<<dim3((nx + 1 + 3) / 4, F.nt), 128, fft_smem(NY), st>>>(C, 0, F.t0, 0);
+            launch_green(c, C, 0, F.t0, F.nt, st);
             if (gaussian) {
                 k_hyb_profiles<<<F.np, 256, 0, st>>>(C, F.p0);
                 CK(cudaMemsetAsync(c->qtot.p, 0, sizeof(unsigned long long) * F.np, st));
@@ -1062,16 +1115,39 @@ void CollideJob::run() {
             PhaseScope ps(c, OCTO_PHASE_FFT, st, 2);
             with_real(fp32, [&](auto r) {
                 using R = decltype(r);
-                k_conv_rows<R><<<dim3((ny / 2 + 3) / 4, F.np), 128, fft_smem(NX, rsz), st>>>(C, F.p0);
+                if (gx) {
+                    with_rf(gx, [&](auto g) {
+                        constexpr int G = decltype(g)::value, PER = 4 * (32 / G);
+                        k_conv_rows_r<R, G><<<dim3((ny / 2 + PER - 1) / PER, F.np), 128, rf_smem(G, rsz), st>>>(C, F.p0);
+                    });
+                } else {
+                    k_conv_rows<R><<<dim3((ny / 2 + 3) / 4, F.np), 128, fft_smem(NX, rsz), st>>>(C, F.p0);
+                }
                 if (fp32)  // the precision form reads partner grids, so the front's grids are cleared here
                     CK(cudaMemsetAsync(c->qgrid.p, 0, sizeof(long long) * cells * F.np, st));
-                k_conv_cols<R><<<dim3((nx + 1 + 3) / 4, F.np), 128, cols_smem(NY, rsz), st>>>(C, F.p0);
+                if (gy) {
+                    with_rf(gy, [&](auto g) {
+                        constexpr int G = decltype(g)::value, PER = 4 * (32 / G);
+                        k_conv_cols_r<R, G><<<dim3((nx + 1 + PER - 1) / PER, F.np), 128, rf_smem(G, rsz), st>>>(C, F.p0);
+                    });
+                } else {
+                    k_conv_cols<R><<<dim3((nx + 1 + 3) / 4, F.np), 128, cols_smem(NY, rsz), st>>>(C, F.p0);
+                }
             });
         }
         {
             PhaseScope ps(c, OCTO_PHASE_FIELD, st, 1);
             with_real(fp32, [&](auto r) {
-                k_conv_field<decltype(r)><<<dim3((ny + kFieldTile - 1) / kFieldTile, F.np), 128, field_smem(NX, rsz), st>>>(C, F.p0);
+                using R = decltype(r);
+                if (gx) {
+                    with_rf(gx, [&](auto g) {
+                        constexpr int G = decltype(g)::value;
+                        const size_t sm = rf_smem(G, rsz) + rsz * (size_t)(kFieldTileR + 4) * nx;
+                        k_conv_field_r<R, G><<<dim3((ny + kFieldTileR - 1) / kFieldTileR, F.np), 128, sm, st>>>(C, F.p0);
+                    });
+                } else {
+                    k_conv_field<R><<<dim3((ny + kFieldTile - 1) / kFieldTile, F.np), 128, field_smem(NX, rsz), st>>>(C, F.p0);
+                }
             });
         }
         if (lum_forked) CK(cudaStreamWaitEvent(st, c->ev_join, 0));  // the kick changes what the luminosity read

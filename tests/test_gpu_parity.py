@@ -136,10 +136,12 @@ def test_nonfinite_input_reports_location(grid_mode, row, role):
     rt.close()
 
 
-@pytest.mark.parametrize("grid", [(48, 48), (96, 64), (64, 96), (192, 192), (256, 256)])
+@pytest.mark.parametrize("grid", [(48, 48), (96, 64), (64, 96), (192, 192), (256, 256), (128, 128), (128, 32),
+                                  (32, 128)])
 def test_grid_sizes(grid):
-    """Grids of the batched scan and the hybrid: 3*2^a sizes (mixed radix-3 FFT lines of 96, 192, 384) and
-    grids whose int64 plane exceeds shared memory (192^2, 256^2: global-memory deposition)."""
+    """Grids of the batched scan and the hybrid: 3*2^a sizes (mixed radix-3 FFT lines of 96, 192, 384),
+    grids whose int64 plane exceeds shared memory (192^2, 256^2: global-memory deposition), and lines of
+    64, 128 and 256 (register-resident FFT) on either axis next to the shared-memory FFT on the other."""
     ob = _gpu()
     s = ob.PICPoissonSolver(grid=grid, slicing=ob.LongitudinalSlicing(nslices=4, method="normal_quantile"))
     check(run_both(s, 8000, 6000, turns=2))
