@@ -668,7 +668,8 @@ __device__ __forceinline__ T *generic_ptr(T *p) {
     asm("" : "+l"(p));  // hide the address space from the compiler
     return p;
 }
-template <class R, int METHOD>
+// TOTAL: also return the sum of the quanta (the hybrid's neutralisation needs the plane's exact charge).
+template <class R, int METHOD, bool TOTAL = false>
 __device__ __forceinline__ long long deposit_taps(R u, R v, int nw, int nh, R scale, long long *grid, int ld) {
     constexpr int NT = METHOD == 0 ? 2 : 3;
     int ix, iy;
@@ -682,7 +683,7 @@ __device__ __forceinline__ long long deposit_taps(R u, R v, int nw, int nh, R sc
 #pragma unroll
         for (int k = 0; k < NT; ++k) {
             const long long qv = round_ll(wx[m] * wy[k] * scale);
-            total += qv;
+            if (TOTAL) total += qv;
             if (qv) atomicAdd((unsigned long long *)&grid[c0 + k * ld + m], (unsigned long long)qv);
         }
     return total;
@@ -732,22 +733,27 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
     long long total = 0;
     // the next particle's coordinates are loaded before the current one's taps, two loads in flight
     const long long stride = (long long)gridDim.x * blockDim.x;
-    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    R cx = 0, cpx = 0, cy = 0, cpy = 0;
-    if (k < P.src_n) { const long long p = P.src_start + k; cx = X[p]; cpx = PX[p]; cy = Y[p]; cpy = PY[p]; }
-    for (; k < P.src_n; k += stride) {
-        R nx_ = 0, npx = 0, ny_ = 0, npy = 0;
-        if (k + stride < P.src_n) {
-            const long long q = P.src_start + k + stride;
-            nx_ = X[q]; npx = PX[q]; ny_ = Y[q]; npy = PY[q];
+    auto sweep = [&](auto with_total) {
+        constexpr bool TOT = decltype(with_total)::value;
+        long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        R cx = 0, cpx = 0, cy = 0, cpy = 0;
+        if (k < P.src_n) { const long long p = P.src_start + k; cx = X[p]; cpx = PX[p]; cy = Y[p]; cpy = PY[p]; }
+        for (; k < P.src_n; k += stride) {
+            R nx_ = 0, npx = 0, ny_ = 0, npy = 0;
+            if (k + stride < P.src_n) {
+                const long long q = P.src_start + k + stride;
+                nx_ = X[q]; npx = PX[q]; ny_ = Y[q]; npy = PY[q];
+            }
+            const R xd = cx + cpx * s;
+            const R yd = cy + cpy * s;
+            if (P.count_dropped && !(isfinite(xd) && xlo <= xd && xd <= xhi && isfinite(yd) && ylo <= yd && yd <= yhi))
+                ++outside;
+            total += deposit_taps<R, METHOD, TOT>((xd - x0) * hxi, (yd - y0) * hyi, nx, ny, scale, acc, nx);
+            cx = nx_; cpx = npx; cy = ny_; cpy = npy;
         }
-        const R xd = cx + cpx * s;
-        const R yd = cy + cpy * s;
-        if (P.count_dropped && !(isfinite(xd) && xlo <= xd && xd <= xhi && isfinite(yd) && ylo <= yd && yd <= yhi))
-            ++outside;
-        total += deposit_taps<R, METHOD>((xd - x0) * hxi, (yd - y0) * hyi, nx, ny, scale, acc, nx);
-        cx = nx_; cpx = npx; cy = ny_; cpy = npy;
-    }
+    };
+    if (C.o.gaussian) sweep(std::true_type());
+    else sweep(std::false_type());
     if (C.o.gaussian) {  // the plane's exact total charge, for the neutralised subtraction
         for (int o = 16; o; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
         if ((threadIdx.x & 31) == 0 && total) atomicAdd(&C.qtot[pl], (unsigned long long)total);
@@ -1267,11 +1273,14 @@ __global__ void __launch_bounds__(128) k_conv_cols_r(Collide C, int plane0) {
         v[m].y = R(0);
         if (m < 4 && ok) v[m] = col[l + G * m];  // rows j < ny = 4 G; the zero padding above
     }
-    rf_fwd<G>(v, S, T);
     const double2 *g = C.ghat + (long long)slot * C.gstride + (long long)k * NY;
+    double2 gpre[8];  // the Green spectrum's loads are in flight during the forward transform
+#pragma unroll
+    for (int r = 0; r < 8; ++r) gpre[r] = ok ? g[r * G + l] : make_double2(0.0, 0.0);
+    rf_fwd<G>(v, S, T);
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
-        const double2 gv = ok ? g[r * G + l] : make_double2(0.0, 0.0);
+        const double2 gv = gpre[r];
         C2 gg;
         gg.x = (R)gv.x;
         gg.y = (R)gv.y;
@@ -1284,10 +1293,10 @@ __global__ void __launch_bounds__(128) k_conv_cols_r(Collide C, int plane0) {
     }
 }
 
-// Tile of 12 rows: with the two-row halo, 16 rows = 8 lines, two per warp (G = 32).
-constexpr int kFieldTileR = 12;
+// Tile of 12 rows: with the two-row halo, 16 rows = 8 lines, one per warp of 8 (G = 32).
+constexpr int kFieldTileR = 12, kFieldWarpsR = 8;
 template <class R, int G>
-__global__ void __launch_bounds__(128) k_conv_field_r(Collide C, int plane0) {
+__global__ void __launch_bounds__(32 * kFieldWarpsR) k_conv_field_r(Collide C, int plane0) {
     using C2 = typename RealT<R>::C2;
     using RG = RfGeom<G>;
     constexpr int LPW = 32 / G;
@@ -1301,7 +1310,7 @@ __global__ void __launch_bounds__(128) k_conv_field_r(Collide C, int plane0) {
     else sg = C.geom[P.task].sg;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, line = lane / G, l = lane & (G - 1);
     C2 *T = sm, *S = sm + RG::kTables + warp * RG::kWarpScratch;
-    R *phi = (R *)(sm + RG::kTables + 4 * RG::kWarpScratch);  // (kFieldTileR + 4) rows x nx
+    R *phi = (R *)(sm + RG::kTables + kFieldWarpsR * RG::kWarpScratch);  // (kFieldTileR + 4) rows x nx
     rf_tables<G>(T, (const C2 *)C.twr_x);
     __syncthreads();
     const int jt0 = blockIdx.x * kFieldTileR;
@@ -1310,23 +1319,22 @@ __global__ void __launch_bounds__(128) k_conv_field_r(Collide C, int plane0) {
     const int nrows = ja1 - ja0;
     const C2 *H = (const C2 *)C.spec + (long long)pl * (nx + 1) * ny;
     const R scale = (R)(1.0 / ((double)NX * (double)NY));
-    for (int rp0 = warp * LPW; 2 * rp0 < nrows; rp0 += 4 * LPW) {  // warp-uniform trip count
+    for (int rp0 = warp * LPW; 2 * rp0 < nrows; rp0 += kFieldWarpsR * LPW) {  // warp-uniform trip count
         const int ra = ja0 + 2 * (rp0 + line), rb = ra + 1;
         const bool ha = ra < ja1, hb = rb < ja1;
         C2 v[8];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
+        for (int r = 0; r < 8; ++r) {  // x-frequency k; above nx from the conjugate of NX - k
             const int k = rf_spec<G>(l, r);
+            const bool mir = k > nx;
+            const C2 *h = H + (long long)(mir ? NX - k : k) * ny;
             C2 ca, cb;
             ca.x = ca.y = cb.x = cb.y = R(0);
-            if (ha) {
-                if (k <= nx) {
-                    ca = H[(long long)k * ny + ra];
-                    if (hb) cb = H[(long long)k * ny + rb];
-                } else {
-                    ca = conjg(H[(long long)(NX - k) * ny + ra]);
-                    if (hb) cb = conjg(H[(long long)(NX - k) * ny + rb]);
-                }
+            if (ha) ca = h[ra];
+            if (hb) cb = h[rb];
+            if (mir) {
+                ca.y = -ca.y;
+                cb.y = -cb.y;
             }
             v[r].x = ca.x - cb.y;
             v[r].y = ca.y + cb.x;

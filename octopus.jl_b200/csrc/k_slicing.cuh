@@ -31,7 +31,7 @@ template <class R>
 struct SliceArgs {
     const R *c[2][6];        // caller-order coordinates x, px, y, py, z, pz
     R *s[2][6];              // slice-sorted copies
-    int *perm[2];
+    int *dest[2];            // caller index -> slice-sorted position
     SliceInfo *info[2];
     double *lane_sum[2], *lane_min[2], *lane_max[2], *lanes[2];
     const double *q[2];      // quantile table (see k_fold_stats)
@@ -224,7 +224,7 @@ __global__ void k_slice_offsets(const SliceArgs<R> A, int align) {
     }
 }
 
-// Stable scatter into slice-contiguous SoA buffers; perm[pos] = original index.
+// Stable scatter into slice-contiguous SoA buffers; dest[original index] = pos.
 // Each block walks its chunk in tiles of blockDim particles, ranking within warps by match_any.
 // grid (max blocks, 1, 2).
 template <class R>
@@ -234,7 +234,7 @@ __global__ void k_slice_scatter(const SliceArgs<R> A, long long chunk) {
     const long long n = A.n[bm];
     const SliceInfo *info = A.info[bm];
     const long long *blockoff = A.blockoff[bm];
-    int *perm = A.perm[bm];
+    int *dest = A.dest[bm];
     __shared__ double b[kMaxSlices + 1];
     __shared__ long long run[kMaxSlices];
     __shared__ int wcount[32][kMaxSlices];
@@ -258,7 +258,7 @@ __global__ void k_slice_scatter(const SliceArgs<R> A, long long chunk) {
         if (live) {
             long long pos = run[s] + rank;
             for (int w = 0; w < warp; ++w) pos += wcount[w][s];
-            perm[pos] = (int)i;
+            dest[i] = (int)pos;
 #pragma unroll
             for (int k = 0; k < 6; ++k) A.s[bm][k][pos] = A.c[bm][k][i];
         }
@@ -317,18 +317,25 @@ __global__ void __launch_bounds__(1024) k_slice_finish(const SliceArgs<R> A) {
     }
 }
 
-// Write the kicked slice-sorted coordinates back in caller order.  z is left alone: a collide never
-// changes it, so the caller's z array already holds the final values.
+// Write the kicked slice-sorted coordinates back in caller order, both beams (blockIdx.y), as a gather
+// over caller indices: the stores are coalesced and the loads follow the slices' ascending runs (the
+// slice scatter is stable).  z is left alone: a collide never changes it, so the caller's z array
+// already holds the final values.
 template <class R>
-__global__ void k_unsort(const int *__restrict__ perm, long long total, const R *sx, const R *spx, const R *sy,
-                         const R *spy, const R *spz, R *x, R *px, R *y, R *py, R *pz) {
-    // total = padded length; padding positions carry perm = -1
-    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= total) return;
-    int i = perm[p];
-    if (i < 0) return;
-    x[i] = sx[p]; px[i] = spx[p]; y[i] = sy[p];
-    py[i] = spy[p]; pz[i] = spz[p];
+struct UnsortArgs {
+    const int *dest[2];
+    const R *s[2][5];  // sorted x, px, y, py, pz
+    R *c[2][5];        // caller-order x, px, y, py, pz
+    long long n[2];
+};
+template <class R>
+__global__ void k_unsort(const UnsortArgs<R> A) {
+    const int b = blockIdx.y;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n[b]) return;
+    const int p = A.dest[b][i];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) A.c[b][k][i] = A.s[b][k][p];
 }
 
 }  // namespace octo

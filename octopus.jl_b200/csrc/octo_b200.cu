@@ -158,7 +158,7 @@ constexpr long long kChunk = 8192;   // particles per slicing block
 
 struct BeamWS {
     DevBuf<double> s[6];  // slice-sorted coordinates (sized in doubles; float elements in the precision form)
-    DevBuf<int> perm;
+    DevBuf<int> dest;  // caller index -> slice-sorted position
     DevBuf<SliceInfo> info;
     DevBuf<double> lane_sum, lane_min, lane_max, lanes, q;
     DevBuf<int> counts;
@@ -166,7 +166,7 @@ struct BeamWS {
     long long total = 0;
     void release() {
         for (auto &b : s) b.release();
-        perm.release(); info.release(); lane_sum.release(); lane_min.release(); lane_max.release();
+        dest.release(); info.release(); lane_sum.release(); lane_min.release(); lane_max.release();
         lanes.release(); q.release(); counts.release(); blockoff.release();
     }
 };
@@ -420,7 +420,7 @@ void slice_beams(octo_ctx *c, const octo_beam &b1, const octo_beam &b2, cudaStre
         const int ns = c->ns[b];
         const long long total = padded_total(n, ns);
         for (auto &a : W.s) a.ensure(total);
-        W.perm.ensure(total);
+        W.dest.ensure(n);
         W.info.ensure(1);
         W.lane_sum.ensure(kFoldLanes); W.lane_min.ensure(kFoldLanes); W.lane_max.ensure(kFoldLanes);
         W.lanes.ensure((size_t)kFoldLanes * ns);
@@ -428,7 +428,6 @@ void slice_beams(octo_ctx *c, const octo_beam &b1, const octo_beam &b2, cudaStre
         W.counts.ensure((size_t)nblocks * ns);
         W.blockoff.ensure((size_t)nblocks * ns);
         W.total = total;
-        CK(cudaMemsetAsync(W.perm.p, 0xff, sizeof(int) * total, st));
         nblk_max = std::max(nblk_max, nblocks);
         ns_max = std::max(ns_max, ns);
     }
@@ -440,7 +439,7 @@ void slice_beams(octo_ctx *c, const octo_beam &b1, const octo_beam &b2, cudaStre
             const octo_beam &B = b == 0 ? b1 : b2;
             const void *cc[6] = {B.x, B.px, B.y, B.py, B.z, B.pz};
             for (int k = 0; k < 6; ++k) { A.c[b][k] = (const R *)cc[k]; A.s[b][k] = (R *)W.s[k].p; }
-            A.perm[b] = W.perm.p;
+            A.dest[b] = W.dest.p;
             A.info[b] = W.info.p;
             A.lane_sum[b] = W.lane_sum.p; A.lane_min[b] = W.lane_min.p; A.lane_max[b] = W.lane_max.p;
             A.lanes[b] = W.lanes.p;
@@ -518,9 +517,9 @@ size_t field_smem(int NX, size_t real = sizeof(double)) {
     return fft_smem(NX, real) + real * (size_t)(kFieldTile + 4) * (NX / 2);
 }
 // Register-FFT kernels (rfft.cuh): twiddle tables + one 256-element scratch per warp.
-size_t rf_smem(int G, size_t real) {
+size_t rf_smem(int G, size_t real, int warps = 4) {
     const int tables = G == 32 ? RfGeom<32>::kTables : G == 16 ? RfGeom<16>::kTables : RfGeom<8>::kTables;
-    return 2 * real * (size_t)(tables + 4 * RfGeom<8>::kWarpScratch);
+    return 2 * real * (size_t)(tables + warps * RfGeom<8>::kWarpScratch);
 }
 template <class F>
 void with_rf(int G, F f) {
@@ -1142,8 +1141,9 @@ void CollideJob::run() {
                 if (gx) {
                     with_rf(gx, [&](auto g) {
                         constexpr int G = decltype(g)::value;
-                        const size_t sm = rf_smem(G, rsz) + rsz * (size_t)(kFieldTileR + 4) * nx;
-                        k_conv_field_r<R, G><<<dim3((ny + kFieldTileR - 1) / kFieldTileR, F.np), 128, sm, st>>>(C, F.p0);
+                        const size_t sm = rf_smem(G, rsz, kFieldWarpsR) + rsz * (size_t)(kFieldTileR + 4) * nx;
+                        k_conv_field_r<R, G><<<dim3((ny + kFieldTileR - 1) / kFieldTileR, F.np), 32 * kFieldWarpsR, sm,
+                                               st>>>(C, F.p0);
                     });
                 } else {
                     k_conv_field<R><<<dim3((ny + kFieldTile - 1) / kFieldTile, F.np), 128, field_smem(NX, rsz), st>>>(C, F.p0);
@@ -1168,18 +1168,23 @@ void CollideJob::run() {
 
     // ---- back to caller order
     {
-        PhaseScope ps(c, OCTO_PHASE_UNSORT, st, 2, (double)(n1 + n2) * 10 * rsz);
-        for (int b = 0; b < 2; ++b) {
-            const BeamWS &W = c->bw[b];
-            const octo_beam &B = b == 0 ? *b1 : *b2;
-            with_real(fp32, [&](auto r) {
-                using R = decltype(r);
-                k_unsort<R><<<(unsigned)((W.total + 255) / 256), 256, 0, st>>>(
-                    W.perm.p, W.total, (const R *)W.s[0].p, (const R *)W.s[1].p, (const R *)W.s[2].p,
-                    (const R *)W.s[3].p, (const R *)W.s[5].p, (R *)B.x, (R *)B.px, (R *)B.y, (R *)B.py, (R *)B.pz);
-            });
-            launches++;
-        }
+        PhaseScope ps(c, OCTO_PHASE_UNSORT, st, 1, (double)(n1 + n2) * 10 * rsz);
+        with_real(fp32, [&](auto r) {
+            using R = decltype(r);
+            UnsortArgs<R> A{};
+            for (int b = 0; b < 2; ++b) {
+                const BeamWS &W = c->bw[b];
+                const octo_beam &B = b == 0 ? *b1 : *b2;
+                void *cc[5] = {B.x, B.px, B.y, B.py, B.pz};
+                const int sk[5] = {0, 1, 2, 3, 5};
+                A.dest[b] = W.dest.p;
+                for (int k = 0; k < 5; ++k) { A.s[b][k] = (const R *)W.s[sk[k]].p; A.c[b][k] = (R *)cc[k]; }
+                A.n[b] = B.n;
+            }
+            const long long nmax = std::max(n1, n2);
+            k_unsort<R><<<dim3((unsigned)((nmax + 255) / 256), 2), 256, 0, st>>>(A);
+        });
+        launches++;
     }
     c->h_lum.ensure(std::max(npairs_total, 1));
     c->h_status.ensure(1);
