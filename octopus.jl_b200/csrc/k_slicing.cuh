@@ -44,10 +44,11 @@ struct SliceArgs {
 // Lane partial sums / extrema over all particles.  square != 0 folds (z - mu)^2.
 // Lane t must add elements t, t+4096, ... strictly in order, so the parallelism is across lanes; to
 // keep enough loads in flight each block stages a tile of kTileIters iterations x 32 lanes in shared
-// memory with all its threads, then one thread per lane adds its column in order.  grid (128, 1, 2).
-constexpr int kTileIters = 64;
+// memory with all its threads (ten loads each in flight), then one thread per lane adds its column in
+// order.  grid (128, 1, 2).
+constexpr int kTileIters = 160, kLaneFoldThreads = 512;
 template <class R>
-__global__ void __launch_bounds__(256) k_lane_fold(const SliceArgs<R> A, int square) {
+__global__ void __launch_bounds__(kLaneFoldThreads) k_lane_fold(const SliceArgs<R> A, int square) {
     const int bm = blockIdx.z;
     const R *__restrict__ z = A.c[bm][4];
     const long long n = A.n[bm];
@@ -190,20 +191,32 @@ __global__ void k_slice_count(const SliceArgs<R> A, long long chunk) {
     for (int t = threadIdx.x; t < ns; t += blockDim.x) A.counts[bm][(long long)blockIdx.x * ns + t] = c[t];
 }
 
-// Slice starts (aligned to `align` elements) and per-block write offsets.  grid (2): one block per beam.
+// Slice starts (aligned to `align` elements) and per-block write offsets: one warp per slice sums its
+// per-block counts and scans them in chunks of 32 blocks (integer sums: any order is exact).
+// grid (2): one block per beam, 1024 threads.
+__device__ __forceinline__ long long warp_incl_scan(long long v) {
+    const int lane = threadIdx.x & 31;
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long w = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += w;
+    }
+    return v;
+}
 template <class R>
-__global__ void k_slice_offsets(const SliceArgs<R> A, int align) {
+__global__ void __launch_bounds__(1024) k_slice_offsets(const SliceArgs<R> A, int align) {
     const int bm = blockIdx.x;
     const int *counts = A.counts[bm];
     const int nblocks = (int)A.nblocks[bm];
     SliceInfo *info = A.info[bm];
     long long *blockoff = A.blockoff[bm];
-    int ns = info->ns;
+    const int ns = info->ns;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     __shared__ long long tot[kMaxSlices];
-    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+    for (int s = warp; s < ns; s += nw) {
         long long acc = 0;
-        for (int b = 0; b < nblocks; ++b) acc += counts[(long long)b * ns + s];
-        tot[s] = acc;
+        for (int b = lane; b < nblocks; b += 32) acc += counts[(long long)b * ns + s];
+        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) tot[s] = acc;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -215,20 +228,25 @@ __global__ void k_slice_offsets(const SliceArgs<R> A, int align) {
         }
     }
     __syncthreads();
-    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
-        long long acc = info->start[s];
-        for (int b = 0; b < nblocks; ++b) {
-            blockoff[(long long)b * ns + s] = acc;
-            acc += counts[(long long)b * ns + s];
+    for (int s = warp; s < ns; s += nw) {
+        long long base = info->start[s];
+        for (int b0 = 0; b0 < nblocks; b0 += 32) {
+            const int b = b0 + lane;
+            const long long v = b < nblocks ? counts[(long long)b * ns + s] : 0;
+            const long long incl = warp_incl_scan(v);
+            if (b < nblocks) blockoff[(long long)b * ns + s] = base + incl - v;
+            base += __shfl_sync(0xffffffffu, incl, 31);
         }
     }
 }
 
 // Stable scatter into slice-contiguous SoA buffers; dest[original index] = pos.
-// Each block walks its chunk in tiles of blockDim particles, ranking within warps by match_any.
-// grid (max blocks, 1, 2).
+// Each block walks its chunk in rounds of blockDim (1024) particles: warps rank their particles per slice
+// with match_any, one warp per slice scans the per-warp counts into write positions, and every particle
+// writes its six coordinates.  grid (max blocks, 1, 2).
+constexpr int kScatterThreads = 1024;
 template <class R>
-__global__ void k_slice_scatter(const SliceArgs<R> A, long long chunk) {
+__global__ void __launch_bounds__(kScatterThreads) k_slice_scatter(const SliceArgs<R> A, long long chunk) {
     const int bm = blockIdx.z;
     if (blockIdx.x >= A.nblocks[bm]) return;
     const long long n = A.n[bm];
@@ -237,36 +255,36 @@ __global__ void k_slice_scatter(const SliceArgs<R> A, long long chunk) {
     int *dest = A.dest[bm];
     __shared__ double b[kMaxSlices + 1];
     __shared__ long long run[kMaxSlices];
-    __shared__ int wcount[32][kMaxSlices];
-    int ns = info->ns;
-    int zw = info->zero_width;
+    __shared__ long long wpos[kScatterThreads / 32][kMaxSlices];  // per-warp count, then write base
+    const int ns = info->ns;
+    const int zw = info->zero_width;
     for (int t = threadIdx.x; t <= ns; t += blockDim.x) b[t] = info->boundary[t];
     for (int t = threadIdx.x; t < ns; t += blockDim.x) run[t] = blockoff[(long long)blockIdx.x * ns + t];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    long long lo = (long long)blockIdx.x * chunk, hi = min(n, lo + chunk);
-    __syncthreads();
+    const long long lo = (long long)blockIdx.x * chunk, hi = min(n, lo + chunk);
     for (long long base = lo; base < hi; base += blockDim.x) {
-        for (int t = threadIdx.x; t < 32 * ns; t += blockDim.x) wcount[t / ns][t % ns] = 0;
+        for (int t = threadIdx.x; t < nwarps * ns; t += blockDim.x) wpos[t / ns][t % ns] = 0;
+        __syncthreads();  // the previous round's reads of wpos are done (its closing barrier) and b, run are loaded
+        const long long i = base + threadIdx.x;
+        const bool live = i < hi;
+        const int s = live ? slice_of((double)A.c[bm][4][i], b, ns, zw) : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, s);
+        const int rank = __popc(peers & ((1u << lane) - 1u));
+        if (live && rank == 0) wpos[warp][s] = __popc(peers);
         __syncthreads();
-        long long i = base + threadIdx.x;
-        bool live = i < hi;
-        int s = live ? slice_of((double)A.c[bm][4][i], b, ns, zw) : -1;
-        unsigned peers = __match_any_sync(0xffffffffu, s);
-        int rank = __popc(peers & ((1u << lane) - 1u));
-        if (live && rank == 0) wcount[warp][s] = __popc(peers);
+        for (int sl = warp; sl < ns; sl += nwarps) {  // exclusive scan over warps, one warp per slice
+            const long long v = lane < nwarps ? wpos[lane][sl] : 0;
+            const long long incl = warp_incl_scan(v);
+            if (lane < nwarps) wpos[lane][sl] = run[sl] + incl - v;
+            __syncwarp();
+            if (lane == 31) run[sl] += incl;
+        }
         __syncthreads();
         if (live) {
-            long long pos = run[s] + rank;
-            for (int w = 0; w < warp; ++w) pos += wcount[w][s];
+            const long long pos = wpos[warp][s] + rank;
             dest[i] = (int)pos;
 #pragma unroll
             for (int k = 0; k < 6; ++k) A.s[bm][k][pos] = A.c[bm][k][i];
-        }
-        __syncthreads();
-        for (int t = threadIdx.x; t < ns; t += blockDim.x) {
-            int add = 0;
-            for (int w = 0; w < nwarps; ++w) add += wcount[w][t];
-            run[t] += add;
         }
         __syncthreads();
     }

@@ -452,13 +452,13 @@ void slice_beams(octo_ctx *c, const octo_beam &b1, const octo_beam &b2, cudaStre
             A.ns[b] = c->ns[b];
             A.cpos[b] = b == 0 ? c->opt.center_position1 : c->opt.center_position2;
         }
-        k_lane_fold<R><<<dim3(kFoldLanes / 32, 1, 2), 256, 0, st>>>(A, 0);
+        k_lane_fold<R><<<dim3(kFoldLanes / 32, 1, 2), kLaneFoldThreads, 0, st>>>(A, 0);
         k_fold_stats<R><<<2, 1024, 0, st>>>(A, 0);
-        k_lane_fold<R><<<dim3(kFoldLanes / 32, 1, 2), 256, 0, st>>>(A, 1);
+        k_lane_fold<R><<<dim3(kFoldLanes / 32, 1, 2), kLaneFoldThreads, 0, st>>>(A, 1);
         k_fold_stats<R><<<2, 1024, 0, st>>>(A, 1);
         k_slice_count<R><<<dim3((unsigned)nblk_max, 1, 2), 256, 0, st>>>(A, kChunk);
-        k_slice_offsets<R><<<2, 64, 0, st>>>(A, kAlign);
-        k_slice_scatter<R><<<dim3((unsigned)nblk_max, 1, 2), 256, 0, st>>>(A, kChunk);
+        k_slice_offsets<R><<<2, 1024, 0, st>>>(A, kAlign);
+        k_slice_scatter<R><<<dim3((unsigned)nblk_max, 1, 2), kScatterThreads, 0, st>>>(A, kChunk);
         k_slice_lanes<R><<<dim3(kFoldLanes / 256, ns_max, 2), 256, 0, st>>>(A);
         k_slice_finish<R><<<dim3(ns_max, 2), 1024, 0, st>>>(A);
     });
