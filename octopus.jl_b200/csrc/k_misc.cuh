@@ -11,6 +11,8 @@ struct Mat6 {
 // Linear 6D map (linear6d.jl:110-121), applied `turns` times in FP64 to coordinates of element type R.
 template <class R>
 __global__ void __launch_bounds__(256) k_linear6d(R *x, R *px, R *y, R *py, R *z, R *pz, long long n, Mat6 M, int turns) {
+    pdl_wait();
+    pdl_release();
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double a = x[i], b = px[i], c = y[i], d = py[i], e = z[i], f = pz[i];
@@ -61,6 +63,8 @@ __device__ __forceinline__ double d_uniform_open01(unsigned long long v) {
 // octopus_normal (counter_rng.jl:168-173): Box-Muller pair, odd component -> cos branch.
 __global__ void k_beam_normals(double *out, long long n, unsigned long long seed, unsigned long long rng_id, int comp,
                                double cutoff) {
+    pdl_wait();
+    pdl_release();
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     unsigned long long particle = (unsigned long long)(i + 1);
@@ -77,6 +81,8 @@ __global__ void k_beam_normals(double *out, long long n, unsigned long long seed
 // Deterministic block partial sums of v (pow = 1) or (v - mu)^2 (pow = 2).
 __global__ void __launch_bounds__(256) k_partial_sum(const double *v, long long n, const double *mu, int pow2,
                                                      double *partial) {
+    pdl_wait();
+    pdl_release();
     __shared__ double red[256];
     double m = pow2 ? *mu : 0.0;
     double acc = 0.0;
@@ -94,6 +100,8 @@ __global__ void __launch_bounds__(256) k_partial_sum(const double *v, long long 
 }
 
 __global__ void k_fold_partials(const double *partial, int nb, long long n, int stage, double *stats) {
+    pdl_wait();
+    pdl_release();
     if (threadIdx.x != 0) return;
     double s = 0.0;
     for (int b = 0; b < nb; ++b) s += partial[b];
@@ -103,6 +111,8 @@ __global__ void k_fold_partials(const double *partial, int nb, long long n, int 
 
 // Beam.jl:148-160 (standardise) followed by the sigma/Twiss normalisation of Beam.jl:545-553.
 __global__ void k_standardize(double *v, long long n, const double *stats) {
+    pdl_wait();
+    pdl_release();
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double mu = stats[0], s = stats[1];
@@ -111,6 +121,8 @@ __global__ void k_standardize(double *v, long long n, const double *stats) {
 }
 
 __global__ void k_twiss(double *q, double *p, long long n, double sigma, double beta, double alpha) {
+    pdl_wait();
+    pdl_release();
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double f = sigma / beta;

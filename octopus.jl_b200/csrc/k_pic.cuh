@@ -79,6 +79,8 @@ __device__ __forceinline__ unsigned long long shfl_max_u64(unsigned long long v)
 // grid: (blocks per side, 2 * pairs in front).
 template <class R, bool LUM_ONLY>
 __global__ void __launch_bounds__(256) k_pair_bounds(Collide C, int task0) {
+    pdl_wait();
+    pdl_release();
     const int q = blockIdx.y >> 1, side = blockIdx.y & 1;
     const int t1 = task0 + 2 * q, t2 = t1 + 1;
     const Task &A = C.tasks[t1];  // dir 1: source beam-1 slice i, field beam-2 slice j
@@ -168,6 +170,8 @@ __device__ __forceinline__ void reduce_lum_box(Collide &C, R mnx, R mxx, R mny, 
 // grid: (blocks per slice, slices of both beams).
 template <class R>
 __global__ void __launch_bounds__(256) k_first_lum_bounds(Collide C, const FirstLum *first) {
+    pdl_wait();
+    pdl_release();
     const FirstLum F = first[blockIdx.y];
     const SoA S = C.beam[F.beam];
     const R *X = col<R>(S, 0) + F.start, *PX = col<R>(S, 1) + F.start, *Y = col<R>(S, 2) + F.start,
@@ -188,6 +192,8 @@ __global__ void __launch_bounds__(256) k_first_lum_bounds(Collide C, const First
 // (gaussian_pic.jl:432-486), as per-block partials folded in block order by k_plan.  grid: (blocks per
 // side, 2 * pairs in front), the mapping of k_pair_bounds.
 __global__ void __launch_bounds__(256) k_hyb_moments(Collide C, int task0) {
+    pdl_wait();
+    pdl_release();
     const int q = blockIdx.y >> 1, side = blockIdx.y & 1;
     const int t = task0 + 2 * q + side;  // side 0: direction-1 task (source beam 1), side 1: direction 2
     const Task &T = C.tasks[t];
@@ -226,6 +232,8 @@ __global__ void __launch_bounds__(256) k_hyb_moments(Collide C, int task0) {
 // Fold the per-block moment partials of each task, in block order, into slot 0 (one warp per task: lane k
 // sums quantity k over the blocks).
 __global__ void k_hyb_fold(Collide C, int task0, int ntasks, int nblk) {
+    pdl_wait();
+    pdl_release();
     const int tl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (tl >= ntasks || lane >= kMomentSums) return;
     double *m = C.hmom + (long long)(task0 + tl) * kMaxBoundBlocks * kMomentSums;
@@ -256,6 +264,8 @@ __device__ inline void record_error(DevStatus *st, int task, int code, int role)
 // moments (folded by k_hyb_fold), the reference Gaussians at both boundaries, the plain-PIC fallback test
 // and the margin box around the Gaussians joined to the source extent (gaussian_pic.jl:604-660).
 __global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0) {
+    pdl_wait();
+    pdl_release();
     int tl = blockIdx.x * blockDim.x + threadIdx.x;
     if (tl >= ntasks) return;
     int t = task0 + tl;
@@ -442,6 +452,8 @@ __device__ __forceinline__ double green_value(int green_type, int i, int j, int 
 // mode 0: blockIdx.y = task of the front (only tasks that rebuild); mode 1: blockIdx.y = node mesh.
 constexpr int kGreenRows = 8;
 __global__ void __launch_bounds__(128) k_green_rows(Collide C, int mode, int base, int node_slot0) {
+    pdl_wait();
+    pdl_release();
     double2 *sm = (double2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx, NY = 2 * ny;
     const FftLen fx = fft_len(NX);
@@ -517,6 +529,8 @@ __global__ void __launch_bounds__(128) k_green_rows(Collide C, int mode, int bas
 
 // Column transforms of the Green slots (length 2ny, in place, natural-order output).
 __global__ void __launch_bounds__(128) k_green_cols(Collide C, int mode, int base, int node_slot0) {
+    pdl_wait();
+    pdl_release();
     double2 *sm = (double2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NY = 2 * ny;
     const FftLen fy = fft_len(NY);
@@ -548,6 +562,8 @@ __global__ void __launch_bounds__(128) k_green_cols(Collide C, int mode, int bas
 // (entry r * G + l holds frequency rf_spec(l, r)), the order k_conv_cols_r multiplies in.
 template <int G>
 __global__ void __launch_bounds__(128) k_green_rows_r(Collide C, int mode, int base, int node_slot0) {
+    pdl_wait();
+    pdl_release();
     using RG = RfGeom<G>;
     constexpr int LPW = 32 / G, ROWS = 8 * LPW;
     double2 *sm = (double2 *)g_smem;
@@ -625,6 +641,8 @@ __global__ void __launch_bounds__(128) k_green_rows_r(Collide C, int mode, int b
 
 template <int G>
 __global__ void __launch_bounds__(128) k_green_cols_r(Collide C, int mode, int base, int node_slot0) {
+    pdl_wait();
+    pdl_release();
     using RG = RfGeom<G>;
     constexpr int LPW = 32 / G;
     double2 *sm = (double2 *)g_smem;
@@ -702,6 +720,8 @@ __device__ __forceinline__ void merge_grid(const long long *sq, long long *g, in
 // memory, then merges it with global atomics (the consumer, k_conv_rows, clears the grid it reads).
 template <class R, int METHOD>
 __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
+    pdl_wait();
+    pdl_release();
     long long *sq = (long long *)g_smem;
     const int pl = blockIdx.y;
     const Plane &P = C.planes[plane0 + pl];
@@ -773,6 +793,8 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
 // Every block derives its pair's mesh (lum_geometry); block (0, side 0) publishes it and reports errors.
 template <class R, int METHOD>
 __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0, int task0) {
+    pdl_wait();
+    pdl_release();
     long long *sq = (long long *)g_smem;
     const int ql = blockIdx.y >> 1, side = blockIdx.y & 1;
     const LumJob &J = C.lumjobs[lj0 + ql];
@@ -823,6 +845,8 @@ __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0, int
 // the next front.
 constexpr int kLumSplit = 16;
 __global__ void __launch_bounds__(256) k_lum_overlap(Collide C, int lj0) {
+    pdl_wait();
+    pdl_release();
     const int ql = blockIdx.y, part = blockIdx.x;
     const LumJob &J = C.lumjobs[lj0 + ql];
     const int cells = (C.o.lnx + 1) * (C.o.lny + 1);
@@ -886,6 +910,8 @@ __device__ __forceinline__ double gauss_node_weight(int method, double xi, doubl
 }
 
 __global__ void __launch_bounds__(256) k_hyb_profiles(Collide C, int plane0) {
+    pdl_wait();
+    pdl_release();
     const int pl = blockIdx.x;
     const Plane &P = C.planes[plane0 + pl];
     const TaskGeom &G = C.geom[P.task];
@@ -921,6 +947,8 @@ __device__ __forceinline__ int plane_green(const Collide &C, const Plane &P) {
 // one (Plane::other_delta), and the host clears the front's grids after the launch.
 template <class R>
 __global__ void __launch_bounds__(128) k_conv_rows(Collide C, int plane0) {
+    pdl_wait();
+    pdl_release();
     using C2 = typename RealT<R>::C2;
     C2 *sm = (C2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx;
@@ -992,6 +1020,8 @@ __global__ void __launch_bounds__(128) k_conv_rows(Collide C, int plane0) {
 // place for NY = 2^a (bit reversal is an involution) and through a second line for NY = 3 * 2^a.
 template <class R>
 __global__ void __launch_bounds__(128) k_conv_cols(Collide C, int plane0) {
+    pdl_wait();
+    pdl_release();
     using C2 = typename RealT<R>::C2;
     C2 *sm = (C2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NY = 2 * ny;
@@ -1118,6 +1148,8 @@ __device__ __forceinline__ void field_cells(const Collide &C, const Plane &P, in
 constexpr int kFieldTile = 8;
 template <class R>
 __global__ void __launch_bounds__(128) k_conv_field(Collide C, int plane0) {
+    pdl_wait();
+    pdl_release();
     using C2 = typename RealT<R>::C2;
     C2 *sm = (C2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx, NY = 2 * ny;
@@ -1179,6 +1211,8 @@ __global__ void __launch_bounds__(128) k_conv_field(Collide C, int plane0) {
 // transforms, on zeros, and store nothing.
 template <class R, int G>
 __global__ void __launch_bounds__(128) k_conv_rows_r(Collide C, int plane0) {
+    pdl_wait();
+    pdl_release();
     using C2 = typename RealT<R>::C2;
     using RG = RfGeom<G>;
     constexpr int LPW = 32 / G;
@@ -1250,6 +1284,8 @@ __global__ void __launch_bounds__(128) k_conv_rows_r(Collide C, int plane0) {
 
 template <class R, int G>
 __global__ void __launch_bounds__(128) k_conv_cols_r(Collide C, int plane0) {
+    pdl_wait();
+    pdl_release();
     using C2 = typename RealT<R>::C2;
     using RG = RfGeom<G>;
     constexpr int LPW = 32 / G;
@@ -1297,6 +1333,8 @@ __global__ void __launch_bounds__(128) k_conv_cols_r(Collide C, int plane0) {
 constexpr int kFieldTileR = 12, kFieldWarpsR = 8;
 template <class R, int G>
 __global__ void __launch_bounds__(32 * kFieldWarpsR) k_conv_field_r(Collide C, int plane0) {
+    pdl_wait();
+    pdl_release();
     using C2 = typename RealT<R>::C2;
     using RG = RfGeom<G>;
     constexpr int LPW = 32 / G;
@@ -1573,6 +1611,8 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
 
 template <class R, int METHOD, bool HYB>
 __global__ void __launch_bounds__(kKickThreads, sizeof(R) == 8 ? 2 : 4) k_kick(Collide C, int plane0_front, const int2 *blockmap) {
+    pdl_wait();
+    pdl_release();
     __shared__ KickJob<R> J;
     if (threadIdx.x == 0) {
         const int2 bm = blockmap[blockIdx.x];
@@ -1663,6 +1703,8 @@ struct NodeBoxArgs {
 
 template <class R>
 __global__ void __launch_bounds__(kBoxThreads) k_node_boxes(NodeBoxArgs A) {
+    pdl_wait();
+    pdl_release();
     __shared__ R tile[5][kBoxTile];
     __shared__ unsigned long long red[kBoxThreads / 32][kBoxLanes][4];
     const int bm = (int)blockIdx.y < A.ns[0] ? 0 : 1;
@@ -1752,6 +1794,8 @@ __global__ void __launch_bounds__(kBoxThreads) k_node_boxes(NodeBoxArgs A) {
 // role 4 = node-mesh build): the reference fails at the turn-start mesh build, before any pair.
 __global__ void k_node_plan(DevOptions o, const unsigned long long *sbox, const unsigned long long *fbox, int ns_src,
                             int nb, const long long *src_count, const int *nanf, NodeMesh *meshes, DevStatus *st) {
+    pdl_wait();
+    pdl_release();
     int id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= ns_src * nb) return;
     const int i = id / nb, b = id % nb + 1;  // b is 1-based

@@ -49,6 +49,8 @@ struct SliceArgs {
 constexpr int kTileIters = 160, kLaneFoldThreads = 512;
 template <class R>
 __global__ void __launch_bounds__(kLaneFoldThreads) k_lane_fold(const SliceArgs<R> A, int square) {
+    pdl_wait();
+    pdl_release();
     const int bm = blockIdx.z;
     const R *__restrict__ z = A.c[bm][4];
     const long long n = A.n[bm];
@@ -97,6 +99,8 @@ __global__ void __launch_bounds__(kLaneFoldThreads) k_lane_fold(const SliceArgs<
 // grid (2): one block per beam.
 template <class R>
 __global__ void __launch_bounds__(1024) k_fold_stats(const SliceArgs<R> A, int stage) {
+    pdl_wait();
+    pdl_release();
     const int bm = blockIdx.x;
     const double *lane_sum = A.lane_sum[bm], *lane_min = A.lane_min[bm], *lane_max = A.lane_max[bm];
     const long long n = A.n[bm];
@@ -173,6 +177,8 @@ __device__ __forceinline__ int slice_of(double z, const double *b, int ns, int z
 // Per-block slice counts over contiguous chunks.  grid (max blocks, 1, 2).
 template <class R>
 __global__ void k_slice_count(const SliceArgs<R> A, long long chunk) {
+    pdl_wait();
+    pdl_release();
     const int bm = blockIdx.z;
     if (blockIdx.x >= A.nblocks[bm]) return;
     const R *__restrict__ z = A.c[bm][4];
@@ -204,6 +210,8 @@ __device__ __forceinline__ long long warp_incl_scan(long long v) {
 }
 template <class R>
 __global__ void __launch_bounds__(1024) k_slice_offsets(const SliceArgs<R> A, int align) {
+    pdl_wait();
+    pdl_release();
     const int bm = blockIdx.x;
     const int *counts = A.counts[bm];
     const int nblocks = (int)A.nblocks[bm];
@@ -247,6 +255,8 @@ __global__ void __launch_bounds__(1024) k_slice_offsets(const SliceArgs<R> A, in
 constexpr int kScatterThreads = 1024;
 template <class R>
 __global__ void __launch_bounds__(kScatterThreads) k_slice_scatter(const SliceArgs<R> A, long long chunk) {
+    pdl_wait();
+    pdl_release();
     const int bm = blockIdx.z;
     if (blockIdx.x >= A.nblocks[bm]) return;
     const long long n = A.n[bm];
@@ -294,6 +304,8 @@ __global__ void __launch_bounds__(kScatterThreads) k_slice_scatter(const SliceAr
 // grid (kFoldLanes / 256, max slices, 2).
 template <class R>
 __global__ void k_slice_lanes(const SliceArgs<R> A) {
+    pdl_wait();
+    pdl_release();
     const int bm = blockIdx.z;
     const SliceInfo *info = A.info[bm];
     int s = blockIdx.y;
@@ -310,6 +322,8 @@ __global__ void k_slice_lanes(const SliceArgs<R> A) {
 // weights (slicing.jl:523-559).  grid (max slices, 2).
 template <class R>
 __global__ void __launch_bounds__(1024) k_slice_finish(const SliceArgs<R> A) {
+    pdl_wait();
+    pdl_release();
     const int bm = blockIdx.y;
     SliceInfo *info = A.info[bm];
     const double *lanes = A.lanes[bm];
@@ -348,6 +362,8 @@ struct UnsortArgs {
 };
 template <class R>
 __global__ void k_unsort(const UnsortArgs<R> A) {
+    pdl_wait();
+    pdl_release();
     const int b = blockIdx.y;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n[b]) return;

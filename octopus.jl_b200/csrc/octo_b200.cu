@@ -39,6 +39,24 @@ struct OctoFail {
         if (e_ != cudaSuccess) throw CudaFail{std::string(#call) + ": " + cudaGetErrorString(e_)};         \
     } while (0)
 
+// Launch a kernel of the collide path with programmatic stream serialization: it may begin launching
+// while its predecessor in the stream drains, and its first statement (pdl_wait) holds it until that
+// grid has completed.  A predecessor that is a copy, a memset or an event wait stays a full dependency.
+template <class... P, class... A>
+void launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A &&...args) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...));
+}
+
 // Inverse error function: Winitzki start, Halley steps on erf / erfc.  Used only for the
 // :normal_quantile slice quantiles sqrt(2)*erfinv(2s/ns-1) (slicing.jl:425).
 double erfinv_host(double x) {
@@ -388,6 +406,8 @@ long long padded_total(long long n, int ns) { return n + (long long)ns * kAlign;
 
 __global__ void k_init_bounds(unsigned long long *bnd, int ntasks, unsigned long long *lumb, int npairs, int *nanflag,
                               DevStatus *st, int reset_status) {
+    pdl_wait();
+    pdl_release();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < ntasks) {
         for (int k = 0; k < 8; ++k) bnd[(long long)t * 8 + k] = (k & 1) ? kOrdMaxInit : kOrdMinInit;
@@ -404,6 +424,8 @@ __global__ void k_init_bounds(unsigned long long *bnd, int ntasks, unsigned long
 }
 
 __global__ void k_init_boxes(unsigned long long *a, long long na, unsigned long long *b, long long nb) {
+    pdl_wait();
+    pdl_release();
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t < na) a[t] = (t & 1) ? kOrdMaxInit : kOrdMinInit;
     else if (t < na + nb) b[t - na] = (t & 1) ? kOrdMaxInit : kOrdMinInit;
@@ -452,15 +474,15 @@ void slice_beams(octo_ctx *c, const octo_beam &b1, const octo_beam &b2, cudaStre
             A.ns[b] = c->ns[b];
             A.cpos[b] = b == 0 ? c->opt.center_position1 : c->opt.center_position2;
         }
-        k_lane_fold<R><<<dim3(kFoldLanes / 32, 1, 2), kLaneFoldThreads, 0, st>>>(A, 0);
-        k_fold_stats<R><<<2, 1024, 0, st>>>(A, 0);
-        k_lane_fold<R><<<dim3(kFoldLanes / 32, 1, 2), kLaneFoldThreads, 0, st>>>(A, 1);
-        k_fold_stats<R><<<2, 1024, 0, st>>>(A, 1);
-        k_slice_count<R><<<dim3((unsigned)nblk_max, 1, 2), 256, 0, st>>>(A, kChunk);
-        k_slice_offsets<R><<<2, 1024, 0, st>>>(A, kAlign);
-        k_slice_scatter<R><<<dim3((unsigned)nblk_max, 1, 2), kScatterThreads, 0, st>>>(A, kChunk);
-        k_slice_lanes<R><<<dim3(kFoldLanes / 256, ns_max, 2), 256, 0, st>>>(A);
-        k_slice_finish<R><<<dim3(ns_max, 2), 1024, 0, st>>>(A);
+        launch_pdl(k_lane_fold<R>, dim3(kFoldLanes / 32, 1, 2), kLaneFoldThreads, 0, st, A, 0);
+        launch_pdl(k_fold_stats<R>, 2, 1024, 0, st, A, 0);
+        launch_pdl(k_lane_fold<R>, dim3(kFoldLanes / 32, 1, 2), kLaneFoldThreads, 0, st, A, 1);
+        launch_pdl(k_fold_stats<R>, 2, 1024, 0, st, A, 1);
+        launch_pdl(k_slice_count<R>, dim3((unsigned)nblk_max, 1, 2), 256, 0, st, A, kChunk);
+        launch_pdl(k_slice_offsets<R>, 2, 1024, 0, st, A, kAlign);
+        launch_pdl(k_slice_scatter<R>, dim3((unsigned)nblk_max, 1, 2), kScatterThreads, 0, st, A, kChunk);
+        launch_pdl(k_slice_lanes<R>, dim3(kFoldLanes / 256, ns_max, 2), 256, 0, st, A);
+        launch_pdl(k_slice_finish<R>, dim3(ns_max, 2), 1024, 0, st, A);
     });
     launches += 9;
     CK(cudaGetLastError());
@@ -578,18 +600,18 @@ void launch_green(const octo_ctx *c, const Collide &C, int mode, int base, int c
         with_rf(gx, [&](auto g) {
             constexpr int G = decltype(g)::value, ROWS = 8 * (32 / G);
             const size_t sm = rf_smem(G, sizeof(double)) + sizeof(double) * (size_t)(ROWS + 1) * (NX + 1);
-            k_green_rows_r<G><<<dim3(NY / ROWS, count), 128, sm, st>>>(C, mode, base, 0);
+            launch_pdl(k_green_rows_r<G>, dim3(NY / ROWS, count), 128, sm, st, C, mode, base, 0);
         });
     } else {
-        k_green_rows<<<dim3(NY / kGreenRows, count), 128, green_smem(NX), st>>>(C, mode, base, 0);
+        launch_pdl(k_green_rows, dim3(NY / kGreenRows, count), 128, green_smem(NX), st, C, mode, base, 0);
     }
     if (gy) {
         with_rf(gy, [&](auto g) {
             constexpr int G = decltype(g)::value, PER = 4 * (32 / G);
-            k_green_cols_r<G><<<dim3((nx + 1 + PER - 1) / PER, count), 128, rf_smem(G, sizeof(double)), st>>>(C, mode, base, 0);
+            launch_pdl(k_green_cols_r<G>, dim3((nx + 1 + PER - 1) / PER, count), 128, rf_smem(G, sizeof(double)), st, C, mode, base, 0);
         });
     } else {
-        k_green_cols<<<dim3((nx + 1 + 3) / 4, count), 128, fft_smem(NY), st>>>(C, mode, base, 0);
+        launch_pdl(k_green_cols, dim3((nx + 1 + 3) / 4, count), 128, fft_smem(NY), st, C, mode, base, 0);
     }
 }
 
@@ -631,7 +653,7 @@ void build_node_meshes(octo_ctx *c, Collide &C, const SliceInfo &S1, const Slice
     unsigned long long *sbox1 = c->nodebox_s.p, *sbox2 = c->nodebox_s.p + (size_t)nbox_s * 4;
     unsigned long long *fbox1 = c->nodebox_f.p, *fbox2 = c->nodebox_f.p + (size_t)nbox_f * 4;
     const long long ns8 = 8ll * nbox_s, nf8 = 8ll * nbox_f;
-    k_init_boxes<<<(unsigned)((ns8 + nf8 + 255) / 256), 256, 0, st>>>(c->nodebox_s.p, ns8, c->nodebox_f.p, nf8);
+    launch_pdl(k_init_boxes, (unsigned)((ns8 + nf8 + 255) / 256), 256, 0, st, c->nodebox_s.p, ns8, c->nodebox_f.p, nf8);
     // one pass over both beams: beam 0's source role is direction 1, its field role direction 2
     NodeBoxArgs A{};
     long long maxn = 1;
@@ -654,11 +676,11 @@ void build_node_meshes(octo_ctx *c, Collide &C, const SliceInfo &S1, const Slice
     A.chunk = ((maxn + bx - 1) / bx + kBoxTile - 1) / kBoxTile * kBoxTile;
     const int gz = (std::max(nref1, nref2) + kBoxLanes * kBoxGroups - 1) / (kBoxLanes * kBoxGroups);
     with_real(c->fp32, [&](auto r) {
-        k_node_boxes<decltype(r)><<<dim3((unsigned)bx, ns1 + ns2, gz), kBoxThreads, 0, st>>>(A);
+        launch_pdl(k_node_boxes<decltype(r)>, dim3((unsigned)bx, ns1 + ns2, gz), kBoxThreads, 0, st, A);
     });
-    k_node_plan<<<(ns1 * (ns2 + 1) + 63) / 64, 64, 0, st>>>(c->dopt, sbox1, fbox1, ns1, ns2 + 1, dcnt, c->nodenan.p,
+    launch_pdl(k_node_plan, (ns1 * (ns2 + 1) + 63) / 64, 64, 0, st, c->dopt, sbox1, fbox1, ns1, ns2 + 1, dcnt, c->nodenan.p,
                                                            c->nodes.p, c->status.p);
-    k_node_plan<<<(ns2 * (ns1 + 1) + 63) / 64, 64, 0, st>>>(c->dopt, sbox2, fbox2, ns2, ns1 + 1, dcnt + ns1,
+    launch_pdl(k_node_plan, (ns2 * (ns1 + 1) + 63) / 64, 64, 0, st, c->dopt, sbox2, fbox2, ns2, ns1 + 1, dcnt + ns1,
                                                            c->nodenan.p, c->nodes.p + ns1 * (ns2 + 1), c->status.p);
     launches += 4;
     // Green spectra of every valid node mesh
@@ -800,7 +822,7 @@ void CollideJob::run() {
     for (size_t p = 0; p < order.size(); ++p) pos_of[(size_t)(order[p].i - 1) * ns2 + (order[p].j - 1)] = (int)p;
 
     // ---- status reset for this call (cache counters stay cumulative)
-    k_init_bounds<<<1, 1, 0, st>>>(nullptr, 0, nullptr, 0, nullptr, c->status.p, 1);
+    launch_pdl(k_init_bounds, 1, 1, 0, st, nullptr, 0, nullptr, 0, nullptr, c->status.p, 1);
     launches += 1;
 
     // ---- node meshes at turn start
@@ -998,7 +1020,7 @@ void CollideJob::run() {
     put(c->blockmap.p, blockmap.data(), sizeof(int2) * blockmap.size());
     put(c->first_lum.p, first_lum.data(), sizeof(FirstLum) * first_lum.size());
     CK(cudaMemsetAsync(c->lum_parts.p, 0, sizeof(double) * npairs_total, st));
-    k_init_bounds<<<(std::max(ntasks, npairs_total) + 255) / 256, 256, 0, st>>>(c->bnd.p, ntasks, c->lumb.p, npairs_total,
+    launch_pdl(k_init_bounds, (std::max(ntasks, npairs_total) + 255) / 256, 256, 0, st, c->bnd.p, ntasks, c->lumb.p, npairs_total,
                                                                                 c->nanflag.p, c->status.p, 0);
     launches += 1;
     C.tasks = c->tasks.p;
@@ -1045,7 +1067,7 @@ void CollideJob::run() {
         for (auto &F : first_lum) maxn = std::max<long long>(maxn, F.count);
         const unsigned bx = (unsigned)std::max<long long>(1, std::min<long long>(kMaxBoundBlocks, (maxn + 2047) / 2048));
         with_real(fp32, [&](auto r) {
-            k_first_lum_bounds<decltype(r)><<<dim3(bx, (unsigned)first_lum.size()), 256, 0, st>>>(C, c->first_lum.p);
+            launch_pdl(k_first_lum_bounds<decltype(r)>, dim3(bx, (unsigned)first_lum.size()), 256, 0, st, C, c->first_lum.p);
         });
         launches += 1;
     }
@@ -1062,10 +1084,10 @@ void CollideJob::run() {
         const unsigned bps = (unsigned)std::max<long long>(1, std::min<long long>(kMaxBoundBlocks, (F.maxsrc + 2047) / 2048));
         if (!node) {
             PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, gaussian ? 2 : 1, slice_bytes * 5 * rsz);
-            with_real(fp32, [&](auto r) { k_pair_bounds<decltype(r), false><<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0); });
+            with_real(fp32, [&](auto r) { launch_pdl(k_pair_bounds<decltype(r), false>, dim3(bps, 2 * npf), 256, 0, st, C, F.t0); });
             if (gaussian) {
-                k_hyb_moments<<<dim3(bps, 2 * npf), 256, 0, st>>>(C, F.t0);
-                k_hyb_fold<<<(F.nt * 32 + 127) / 128, 128, 0, st>>>(C, F.t0, F.nt, (int)bps);
+                launch_pdl(k_hyb_moments, dim3(bps, 2 * npf), 256, 0, st, C, F.t0);
+                launch_pdl(k_hyb_fold, (F.nt * 32 + 127) / 128, 128, 0, st, C, F.t0, F.nt, (int)bps);
             }
             launches += gaussian ? 3 : 1;
         }
@@ -1078,11 +1100,11 @@ void CollideJob::run() {
                 unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(8, (F.maxlum + 32767) / 32768));
                 with_real(fp32, [&](auto r) {
                     launch_method(lmethod, [&](auto M) {
-                        k_lum_deposit<decltype(r), decltype(M)::value><<<dim3(bpp, 2 * F.nl), 1024, lum_bytes, c->lum_stream>>>(
+                        launch_pdl(k_lum_deposit<decltype(r), decltype(M)::value>, dim3(bpp, 2 * F.nl), 1024, lum_bytes, c->lum_stream, 
                             C, F.l0, F.t0);
                     });
                 });
-                k_lum_overlap<<<dim3(kLumSplit, F.nl), 256, 0, c->lum_stream>>>(C, F.l0);
+                launch_pdl(k_lum_overlap, dim3(kLumSplit, F.nl), 256, 0, c->lum_stream, C, F.l0);
             }
             CK(cudaEventRecord(c->ev_join, c->lum_stream));
             lum_forked = true;
@@ -1091,12 +1113,12 @@ void CollideJob::run() {
         if (!node) {
             {
                 PhaseScope ps(c, OCTO_PHASE_PLAN, st, 1);
-                k_plan<<<(F.nt + 63) / 64, 64, 0, st>>>(C, F.t0, F.nt, 0);
+                launch_pdl(k_plan, (F.nt + 63) / 64, 64, 0, st, C, F.t0, F.nt, 0);
             }
             PhaseScope ps(c, OCTO_PHASE_GREEN, st, gaussian ? 3 : 2);
             launch_green(c, C, 0, F.t0, F.nt, st);
             if (gaussian) {
-                k_hyb_profiles<<<F.np, 256, 0, st>>>(C, F.p0);
+                launch_pdl(k_hyb_profiles, F.np, 256, 0, st, C, F.p0);
                 CK(cudaMemsetAsync(c->qtot.p, 0, sizeof(unsigned long long) * F.np, st));
             }
             launches += gaussian ? 4 : 3;
@@ -1106,7 +1128,7 @@ void CollideJob::run() {
             unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(8, (F.maxsrc + 32767) / 32768));
             with_real(fp32, [&](auto r) {
                 launch_method(method, [&](auto M) {
-                    k_deposit<decltype(r), decltype(M)::value><<<dim3(bpp, F.np), 1024, dep_bytes, st>>>(C, F.p0);
+                    launch_pdl(k_deposit<decltype(r), decltype(M)::value>, dim3(bpp, F.np), 1024, dep_bytes, st, C, F.p0);
                 });
             });
         }
@@ -1117,20 +1139,20 @@ void CollideJob::run() {
                 if (gx) {
                     with_rf(gx, [&](auto g) {
                         constexpr int G = decltype(g)::value, PER = 4 * (32 / G);
-                        k_conv_rows_r<R, G><<<dim3((ny / 2 + PER - 1) / PER, F.np), 128, rf_smem(G, rsz), st>>>(C, F.p0);
+                        launch_pdl(k_conv_rows_r<R, G>, dim3((ny / 2 + PER - 1) / PER, F.np), 128, rf_smem(G, rsz), st, C, F.p0);
                     });
                 } else {
-                    k_conv_rows<R><<<dim3((ny / 2 + 3) / 4, F.np), 128, fft_smem(NX, rsz), st>>>(C, F.p0);
+                    launch_pdl(k_conv_rows<R>, dim3((ny / 2 + 3) / 4, F.np), 128, fft_smem(NX, rsz), st, C, F.p0);
                 }
                 if (fp32)  // the precision form reads partner grids, so the front's grids are cleared here
                     CK(cudaMemsetAsync(c->qgrid.p, 0, sizeof(long long) * cells * F.np, st));
                 if (gy) {
                     with_rf(gy, [&](auto g) {
                         constexpr int G = decltype(g)::value, PER = 4 * (32 / G);
-                        k_conv_cols_r<R, G><<<dim3((nx + 1 + PER - 1) / PER, F.np), 128, rf_smem(G, rsz), st>>>(C, F.p0);
+                        launch_pdl(k_conv_cols_r<R, G>, dim3((nx + 1 + PER - 1) / PER, F.np), 128, rf_smem(G, rsz), st, C, F.p0);
                     });
                 } else {
-                    k_conv_cols<R><<<dim3((nx + 1 + 3) / 4, F.np), 128, cols_smem(NY, rsz), st>>>(C, F.p0);
+                    launch_pdl(k_conv_cols<R>, dim3((nx + 1 + 3) / 4, F.np), 128, cols_smem(NY, rsz), st, C, F.p0);
                 }
             });
         }
@@ -1142,11 +1164,11 @@ void CollideJob::run() {
                     with_rf(gx, [&](auto g) {
                         constexpr int G = decltype(g)::value;
                         const size_t sm = rf_smem(G, rsz, kFieldWarpsR) + rsz * (size_t)(kFieldTileR + 4) * nx;
-                        k_conv_field_r<R, G><<<dim3((ny + kFieldTileR - 1) / kFieldTileR, F.np), 32 * kFieldWarpsR, sm,
-                                               st>>>(C, F.p0);
+                        launch_pdl(k_conv_field_r<R, G>, dim3((ny + kFieldTileR - 1) / kFieldTileR, F.np), 32 * kFieldWarpsR, sm,
+                                               st, C, F.p0);
                     });
                 } else {
-                    k_conv_field<R><<<dim3((ny + kFieldTile - 1) / kFieldTile, F.np), 128, field_smem(NX, rsz), st>>>(C, F.p0);
+                    launch_pdl(k_conv_field<R>, dim3((ny + kFieldTile - 1) / kFieldTile, F.np), 128, field_smem(NX, rsz), st, C, F.p0);
                 }
             });
         }
@@ -1157,8 +1179,8 @@ void CollideJob::run() {
                 launch_method(method, [&](auto M) {
                     using R = decltype(r);
                     constexpr int MM = decltype(M)::value;
-                    if (gaussian) k_kick<R, MM, true><<<F.nb, kKickThreads, 0, st>>>(C, F.p0, c->blockmap.p + F.b0);
-                    else k_kick<R, MM, false><<<F.nb, kKickThreads, 0, st>>>(C, F.p0, c->blockmap.p + F.b0);
+                    if (gaussian) launch_pdl(k_kick<R, MM, true>, F.nb, kKickThreads, 0, st, C, F.p0, c->blockmap.p + F.b0);
+                    else launch_pdl(k_kick<R, MM, false>, F.nb, kKickThreads, 0, st, C, F.p0, c->blockmap.p + F.b0);
                 });
             });
         }
@@ -1182,7 +1204,7 @@ void CollideJob::run() {
                 A.n[b] = B.n;
             }
             const long long nmax = std::max(n1, n2);
-            k_unsort<R><<<dim3((unsigned)((nmax + 255) / 256), 2), 256, 0, st>>>(A);
+            launch_pdl(k_unsort<R>, dim3((unsigned)((nmax + 255) / 256), 2), 256, 0, st, A);
         });
         launches++;
     }

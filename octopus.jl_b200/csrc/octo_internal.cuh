@@ -110,6 +110,16 @@ struct DevStatus {
     long long dropped;
 };
 
+// ---------------------------------------------------------------- programmatic dependent launch
+// Every kernel of the library begins with pdl_wait(); pdl_release().  A kernel launched with programmatic
+// stream serialization (launch_pdl) may then begin launching while its predecessor in the stream drains:
+// pdl_wait() blocks until the predecessor grid has completed and its memory operations are visible, and
+// pdl_release() lets the successor's blocks launch once every block of this grid has executed it.  For a
+// kernel launched normally both are no-ops.  Because the wait comes before any memory access and before
+// any early return, a grid's completion still implies the completion of everything before it in the stream.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // ---------------------------------------------------------------- ordered doubles
 // Monotone map double -> uint64 so integer atomicMin/atomicMax order doubles the way
 // Julia's min/max do (-0.0 < +0.0).  NaN never enters: callers flag it separately.
