@@ -193,6 +193,7 @@ struct BeamWS {
 
 struct octo_ctx {
     int device = 0;
+    int num_sms = 148;  // the device's SM count (block-count policies)
     octo_pic_options opt{};
     std::vector<double> pos[2];
     DevOptions dopt{};
@@ -1125,7 +1126,10 @@ void CollideJob::run() {
         }
         {
             PhaseScope ps(c, OCTO_PHASE_DEPOSIT, st, 1, src_bytes * 4 * rsz);
-            unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(8, (F.maxsrc + 32767) / 32768));
+            // blocks per plane: 32768-particle shares, and at least one full wave of the GPU's SMs for the
+            // narrow fronts (one block per SM: a block holds its plane's whole int64 grid)
+            const long long wave = (c->num_sms + F.np - 1) / F.np;
+            unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(32, std::max<long long>((F.maxsrc + 32767) / 32768, wave)));
             with_real(fp32, [&](auto r) {
                 launch_method(method, [&](auto M) {
                     launch_pdl(k_deposit<decltype(r), decltype(M)::value>, dim3(bpp, F.np), 1024, dep_bytes, st, C, F.p0);
@@ -1330,6 +1334,7 @@ octo_ctx *octo_create(int32_t device, const octo_pic_options *options) {
     d.margin = options->margin_sigma;
     try {
         CK(cudaSetDevice(device));
+        CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
         c->fp32 = options->precision == 1;
         if (d.gaussian) upload_weideman();
         upload_twiddles(c->tw_x, 2 * options->nx);
