@@ -1427,8 +1427,8 @@ struct Taps {
 
 // Synchro-beam kick of every field particle of the front's tasks: drift in, interpolated kick,
 // drift out (pic_cpu.jl:1005-1017, 1218-1243, 1248-1273; :node form 1448-1538).
-// Blocks map to (task, chunk of kKickChunk particles) through `blockmap`; the block reads its task
-// and meshes once into shared memory, then each thread kicks kKickChunk / blockDim particles.
+// Blocks map to (task, chunk of `chunk` <= kKickChunk particles) through `blockmap`; the block reads its
+// task and meshes once into shared memory, then each thread kicks chunk / blockDim particles.
 constexpr int kKickThreads = 256;
 constexpr int kKickChunk = 2048;
 template <class R>
@@ -1612,7 +1612,8 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
 }
 
 template <class R, int METHOD, bool HYB>
-__global__ void __launch_bounds__(kKickThreads, sizeof(R) == 8 ? 2 : 4) k_kick(Collide C, int plane0_front, const int2 *blockmap) {
+__global__ void __launch_bounds__(kKickThreads, sizeof(R) == 8 ? 2 : 4)
+    k_kick(Collide C, int plane0_front, const int2 *blockmap, int chunk) {
     pdl_wait();
     pdl_release();
     __shared__ KickJob<R> J;
@@ -1643,7 +1644,7 @@ __global__ void __launch_bounds__(kKickThreads, sizeof(R) == 8 ? 2 : 4) k_kick(C
         J.c_src = (R)T.c_src; J.hzi = (R)T.hzi; J.zbias = (R)T.zbias; J.ks = (R)T.ks;
         J.fld_start = T.fld_start + bm.y;
         const long long rest = T.fld_n - (long long)bm.y;
-        J.fld_n = rest < (long long)kKickChunk ? rest : (long long)kKickChunk;
+        J.fld_n = rest < (long long)chunk ? rest : (long long)chunk;
         J.plane_off = T.plane0 - plane0_front;
         J.fld_beam = T.fld_beam;
         J.next_pair = C.o.node ? T.next_pair : -1;

@@ -838,12 +838,13 @@ void CollideJob::run() {
     std::vector<Plane> planes;
     std::vector<LumJob> lumjobs;
     std::vector<int2> blockmap;
-    struct Front { int t0, nt, p0, np, l0, nl, b0, nb; long long maxsrc, maxlum; };
+    struct Front { int t0, nt, p0, np, l0, nl, b0, nb; long long maxsrc, maxlum; int kchunk; };
     std::vector<Front> fronts;
     const int nplanes_task = node ? (lk ? 3 : 2) : (quad ? 3 : 2);
     ran.assign(order.size(), 0);
     for (size_t f = 0; f < batches.size(); ++f) {
-        Front F{(int)tasks.size(), 0, (int)planes.size(), 0, (int)lumjobs.size(), 0, (int)blockmap.size(), 0, 1, 1};
+        Front F{(int)tasks.size(), 0, (int)planes.size(), 0, (int)lumjobs.size(), 0, (int)blockmap.size(), 0, 1, 1,
+                kKickChunk};
         for (const OrderEntry &pr : batches[f]) {
             const int i = pr.i, j = pr.j;
             if (S1.count[i - 1] == 0 || S2.count[j - 1] == 0) continue;
@@ -909,7 +910,6 @@ void CollideJob::run() {
                     }
                     planes.push_back(P);
                 }
-                for (long long off = 0; off < T.fld_n; off += kKickChunk) blockmap.push_back(make_int2(tid, (int)off));
                 F.maxsrc = std::max<long long>(F.maxsrc, T.src_n);
                 tasks.push_back(T);
             }
@@ -927,6 +927,16 @@ void CollideJob::run() {
             }
         }
         F.nt = (int)tasks.size() - F.t0;
+        // kick blocks of kchunk field particles: 2048, or fewer where the front would not fill the GPU's
+        // resident block slots (two per SM in FP64, four in FP32)
+        long long nfld = 0;
+        for (int t = F.t0; t < F.t0 + F.nt; ++t) nfld += tasks[t].fld_n;
+        const long long slots = (long long)c->num_sms * (fp32 ? 4 : 2);
+        const long long want = (nfld + slots - 1) / slots;
+        F.kchunk = (int)std::min<long long>(kKickChunk, std::max<long long>(kKickThreads, (want + kKickThreads - 1) /
+                                                                                           kKickThreads * kKickThreads));
+        for (int t = F.t0; t < F.t0 + F.nt; ++t)
+            for (long long off = 0; off < tasks[t].fld_n; off += F.kchunk) blockmap.push_back(make_int2(t, (int)off));
         F.np = (int)planes.size() - F.p0;
         F.nl = (int)lumjobs.size() - F.l0;
         F.nb = (int)blockmap.size() - F.b0;
@@ -1183,8 +1193,8 @@ void CollideJob::run() {
                 launch_method(method, [&](auto M) {
                     using R = decltype(r);
                     constexpr int MM = decltype(M)::value;
-                    if (gaussian) launch_pdl(k_kick<R, MM, true>, F.nb, kKickThreads, 0, st, C, F.p0, c->blockmap.p + F.b0);
-                    else launch_pdl(k_kick<R, MM, false>, F.nb, kKickThreads, 0, st, C, F.p0, c->blockmap.p + F.b0);
+                    if (gaussian) launch_pdl(k_kick<R, MM, true>, F.nb, kKickThreads, 0, st, C, F.p0, c->blockmap.p + F.b0, F.kchunk);
+                    else launch_pdl(k_kick<R, MM, false>, F.nb, kKickThreads, 0, st, C, F.p0, c->blockmap.p + F.b0, F.kchunk);
                 });
             });
         }
