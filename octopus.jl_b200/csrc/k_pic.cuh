@@ -562,8 +562,6 @@ __global__ void __launch_bounds__(128) k_green_cols(Collide C, int mode, int bas
 // (entry r * G + l holds frequency rf_spec(l, r)), the order k_conv_cols_r multiplies in.
 template <int G>
 __global__ void __launch_bounds__(128) k_green_rows_r(Collide C, int mode, int base, int node_slot0) {
-    pdl_wait();
-    pdl_release();
     using RG = RfGeom<G>;
     constexpr int LPW = 32 / G, ROWS = 8 * LPW;
     double2 *sm = (double2 *)g_smem;
@@ -571,6 +569,9 @@ __global__ void __launch_bounds__(128) k_green_rows_r(Collide C, int mode, int b
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, line = lane / G, l = lane & (G - 1);
     double2 *T = sm, *S = sm + RG::kTables + warp * RG::kWarpScratch;
     double *corner = (double *)(sm + RG::kTables + 4 * RG::kWarpScratch);  // (ROWS + 1) x (NX + 1)
+    rf_tables<G>(T, C.tw_x);  // twiddles written once at context creation: built before the wait
+    pdl_wait();
+    pdl_release();
     Grid sg, fg;
     int slot;
     if (mode == 0) {
@@ -582,7 +583,6 @@ __global__ void __launch_bounds__(128) k_green_rows_r(Collide C, int mode, int b
         if (!M.valid) return;
         sg = M.sg; fg = M.fg; slot = node_slot0 + base + blockIdx.y;
     }
-    rf_tables<G>(T, C.tw_x);
     const double hx = sg.w / (double)(nx - 1), hy = sg.h / (double)(ny - 1);
     const double dx0 = fg.x0 - sg.x0, dy0 = fg.y0 - sg.y0;
     const double half_hx = hx / 2, half_hy = hy / 2;
@@ -641,14 +641,15 @@ __global__ void __launch_bounds__(128) k_green_rows_r(Collide C, int mode, int b
 
 template <int G>
 __global__ void __launch_bounds__(128) k_green_cols_r(Collide C, int mode, int base, int node_slot0) {
-    pdl_wait();
-    pdl_release();
     using RG = RfGeom<G>;
     constexpr int LPW = 32 / G;
     double2 *sm = (double2 *)g_smem;
     const int nx = C.o.nx, NY = 2 * C.o.ny;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, line = lane / G, l = lane & (G - 1);
     double2 *T = sm, *S = sm + RG::kTables + warp * RG::kWarpScratch;
+    rf_tables<G>(T, C.tw_y);  // before the wait (constant twiddles)
+    pdl_wait();
+    pdl_release();
     int slot;
     if (mode == 0) {
         const TaskGeom &Gm = C.geom[base + blockIdx.y];
@@ -658,14 +659,13 @@ __global__ void __launch_bounds__(128) k_green_cols_r(Collide C, int mode, int b
         if (!C.nodes[base + blockIdx.y].valid) return;
         slot = node_slot0 + base + blockIdx.y;
     }
-    rf_tables<G>(T, C.tw_y);
-    __syncthreads();
     const int k = (blockIdx.x * 4 + warp) * LPW + line;
     const bool ok = k <= nx;
     double2 *col = C.ghat + (long long)slot * C.gstride + (long long)k * NY;
     double2 v[8];
 #pragma unroll
     for (int m = 0; m < 8; ++m) v[m] = ok ? col[l + G * m] : make_double2(0.0, 0.0);
+    __syncthreads();  // tables ready (the column's loads are already in flight)
     rf_fwd<G>(v, S, T);
     if (ok) {
 #pragma unroll
@@ -722,12 +722,17 @@ __device__ __forceinline__ void merge_grid(const long long *sq, long long *g, in
 // memory, then merges it with global atomics (the consumer, k_conv_rows, clears the grid it reads).
 template <class R, int METHOD>
 __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
+    long long *sq = (long long *)g_smem;
+    const int nx = C.o.nx, ny = C.o.ny, cells = nx * ny;
+    // grids larger than shared memory (C.o.dep_global) accumulate straight into the plane's grid; the
+    // block's shared grid is cleared before the wait (shared memory only)
+    const bool local = !C.o.dep_global;
+    if (local)
+        for (int c = threadIdx.x; c < cells; c += blockDim.x) sq[c] = 0;
     pdl_wait();
     pdl_release();
-    long long *sq = (long long *)g_smem;
     const int pl = blockIdx.y;
     const Plane &P = C.planes[plane0 + pl];
-    const int nx = C.o.nx, ny = C.o.ny, cells = nx * ny;
     Grid sg;
     if (P.geom >= 0) {
         if (!C.nodes[P.geom].valid) return;
@@ -737,10 +742,6 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
         if (G.green < 0) return;
         sg = G.sg;
     }
-    // grids larger than shared memory (C.o.dep_global) accumulate straight into the plane's grid
-    const bool local = !C.o.dep_global;
-    if (local)
-        for (int c = threadIdx.x; c < cells; c += blockDim.x) sq[c] = 0;
     __syncthreads();
     long long *acc = local ? generic_ptr(sq) : C.qgrid + (long long)pl * cells;
     const double hx = sg.w / (double)(nx - 1), hy = sg.h / (double)(ny - 1);
@@ -1213,20 +1214,19 @@ __global__ void __launch_bounds__(128) k_conv_field(Collide C, int plane0) {
 // transforms, on zeros, and store nothing.
 template <class R, int G>
 __global__ void __launch_bounds__(128) k_conv_rows_r(Collide C, int plane0) {
-    pdl_wait();
-    pdl_release();
     using C2 = typename RealT<R>::C2;
     using RG = RfGeom<G>;
     constexpr int LPW = 32 / G;
     C2 *sm = (C2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, line = lane / G, l = lane & (G - 1);
+    C2 *T = sm, *S = sm + RG::kTables + warp * RG::kWarpScratch;
+    rf_tables<G>(T, (const C2 *)C.twr_x);  // before the wait (constant twiddles)
+    pdl_wait();
+    pdl_release();
     const int pl = blockIdx.y;
     const Plane &P = C.planes[plane0 + pl];
     if (plane_green(C, P) < 0) return;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, line = lane / G, l = lane & (G - 1);
-    C2 *T = sm, *S = sm + RG::kTables + warp * RG::kWarpScratch;
-    rf_tables<G>(T, (const C2 *)C.twr_x);
-    __syncthreads();
     const int j0 = 2 * ((blockIdx.x * 4 + warp) * LPW + line), j1 = j0 + 1;
     const bool ok = j0 < ny;
     const double inv = ldexp(1.0, -P.fixed_bits);
@@ -1264,6 +1264,7 @@ __global__ void __launch_bounds__(128) k_conv_rows_r(Collide C, int plane0) {
             }
         }
     }
+    __syncthreads();  // tables ready (the rows' loads are already in flight)
     rf_fwd<G>(v, S, T);
     C2 *Sl = S + line * 8 * G;
 #pragma unroll
@@ -1286,21 +1287,20 @@ __global__ void __launch_bounds__(128) k_conv_rows_r(Collide C, int plane0) {
 
 template <class R, int G>
 __global__ void __launch_bounds__(128) k_conv_cols_r(Collide C, int plane0) {
-    pdl_wait();
-    pdl_release();
     using C2 = typename RealT<R>::C2;
     using RG = RfGeom<G>;
     constexpr int LPW = 32 / G;
     C2 *sm = (C2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NY = 2 * ny;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, line = lane / G, l = lane & (G - 1);
+    C2 *T = sm, *S = sm + RG::kTables + warp * RG::kWarpScratch;
+    rf_tables<G>(T, (const C2 *)C.twr_y);  // before the wait (constant twiddles)
+    pdl_wait();
+    pdl_release();
     const int pl = blockIdx.y;
     const Plane &P = C.planes[plane0 + pl];
     const int slot = plane_green(C, P);
     if (slot < 0) return;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, line = lane / G, l = lane & (G - 1);
-    C2 *T = sm, *S = sm + RG::kTables + warp * RG::kWarpScratch;
-    rf_tables<G>(T, (const C2 *)C.twr_y);
-    __syncthreads();
     const int k = (blockIdx.x * 4 + warp) * LPW + line;
     const bool ok = k <= nx;
     C2 *col = (C2 *)C.spec + ((long long)pl * (nx + 1) + k) * ny;
@@ -1315,6 +1315,7 @@ __global__ void __launch_bounds__(128) k_conv_cols_r(Collide C, int plane0) {
     double2 gpre[8];  // the Green spectrum's loads are in flight during the forward transform
 #pragma unroll
     for (int r = 0; r < 8; ++r) gpre[r] = ok ? g[r * G + l] : make_double2(0.0, 0.0);
+    __syncthreads();  // tables ready (the column's and the Green spectrum's loads are in flight)
     rf_fwd<G>(v, S, T);
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
@@ -1335,23 +1336,23 @@ __global__ void __launch_bounds__(128) k_conv_cols_r(Collide C, int plane0) {
 constexpr int kFieldTileR = 12, kFieldWarpsR = 8;
 template <class R, int G>
 __global__ void __launch_bounds__(32 * kFieldWarpsR) k_conv_field_r(Collide C, int plane0) {
-    pdl_wait();
-    pdl_release();
     using C2 = typename RealT<R>::C2;
     using RG = RfGeom<G>;
     constexpr int LPW = 32 / G;
     C2 *sm = (C2 *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, NX = 2 * nx, NY = 2 * ny;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, line = lane / G, l = lane & (G - 1);
+    C2 *T = sm, *S = sm + RG::kTables + warp * RG::kWarpScratch;
+    R *phi = (R *)(sm + RG::kTables + kFieldWarpsR * RG::kWarpScratch);  // (kFieldTileR + 4) rows x nx
+    rf_tables<G>(T, (const C2 *)C.twr_x);  // before the wait (constant twiddles)
+    pdl_wait();
+    pdl_release();
     const int pl = blockIdx.y;
     const Plane &P = C.planes[plane0 + pl];
     if (plane_green(C, P) < 0) return;
     Grid sg;
     if (P.geom >= 0) sg = C.nodes[P.geom].sg;
     else sg = C.geom[P.task].sg;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, line = lane / G, l = lane & (G - 1);
-    C2 *T = sm, *S = sm + RG::kTables + warp * RG::kWarpScratch;
-    R *phi = (R *)(sm + RG::kTables + kFieldWarpsR * RG::kWarpScratch);  // (kFieldTileR + 4) rows x nx
-    rf_tables<G>(T, (const C2 *)C.twr_x);
     __syncthreads();
     const int jt0 = blockIdx.x * kFieldTileR;
     const int jt1 = min(jt0 + kFieldTileR, ny);

@@ -115,8 +115,10 @@ struct DevStatus {
 // stream serialization (launch_pdl) may then begin launching while its predecessor in the stream drains:
 // pdl_wait() blocks until the predecessor grid has completed and its memory operations are visible, and
 // pdl_release() lets the successor's blocks launch once every block of this grid has executed it.  For a
-// kernel launched normally both are no-ops.  Because the wait comes before any memory access and before
-// any early return, a grid's completion still implies the completion of everything before it in the stream.
+// kernel launched normally both are no-ops.  Only work that touches no memory another kernel of the
+// stream writes comes before the wait (twiddle tables uploaded at context creation, clearing shared
+// memory); the wait precedes every other access and every early return, so a grid's completion still
+// implies the completion of everything before it in the stream.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
