@@ -556,6 +556,15 @@ __global__ void __launch_bounds__(128) k_green_cols(Collide C, int mode, int bas
     for (int j = lane; j < NY; j += 32) col[j] = line[fft_out(fy, j)];
 }
 
+// Two consecutive complex values, 2-element aligned, in one vector store (the row pairs of the forward
+// x-transforms; measured: FFT phase 1.10 -> 1.07 ms per production turn).
+__device__ __forceinline__ void store_pair(double2 *p, double2 a, double2 b) {
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a.x), "d"(a.y), "d"(b.x), "d"(b.y) : "memory");
+}
+__device__ __forceinline__ void store_pair(float2 *p, float2 a, float2 b) {
+    *reinterpret_cast<float4 *>(p) = make_float4(a.x, a.y, b.x, b.y);
+}
+
 // Register-FFT forms of the two Green kernels (rfft.cuh) for NX = 8 Gx and NY = 8 Gy.  Rows: the block
 // covers 8 * (32 / G) table rows, two per line, and the spectrum leaves in the same natural layout as
 // k_green_rows'.  Columns: each line is one x-frequency column, stored back in register order
@@ -634,8 +643,7 @@ __global__ void __launch_bounds__(128) k_green_rows_r(Collide C, int mode, int b
         const double2 zk = Sl[rf_nat(k)], zm = conjg(Sl[rf_nat((NX - k) % NX)]);
         const double2 A = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y + zm.y));
         const double2 D = csub(zk, zm);
-        out[(long long)k * NY + ja] = A;
-        out[(long long)k * NY + jb] = make_double2(0.5 * D.y, -0.5 * D.x);
+        store_pair(out + (long long)k * NY + ja, A, make_double2(0.5 * D.y, -0.5 * D.x));  // ja even
     }
 }
 
@@ -1013,8 +1021,7 @@ __global__ void __launch_bounds__(128) k_conv_rows(Collide C, int plane0) {
         C2 D = csub(zk, zm);
         B.x = R(0.5) * D.y;
         B.y = R(-0.5) * D.x;
-        H[(long long)k * ny + j0] = A;
-        if (j1 < ny) H[(long long)k * ny + j1] = B;
+        store_pair(H + (long long)k * ny + j0, A, B);  // rows j0, j0 + 1 (j0 even, ny even)
     }
 }
 
@@ -1296,8 +1303,7 @@ __global__ void __launch_bounds__(128) k_conv_rows_r(Collide C, int plane0) {
         const C2 D = csub(zk, zm);
         B.x = R(0.5) * D.y;
         B.y = R(-0.5) * D.x;
-        H[(long long)k * ny + j0] = A;
-        if (j1 < ny) H[(long long)k * ny + j1] = B;
+        store_pair(H + (long long)k * ny + j0, A, B);  // rows j0, j0 + 1 (j0 even, ny even)
     }
 }
 
