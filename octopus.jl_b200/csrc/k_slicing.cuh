@@ -42,13 +42,15 @@ struct SliceArgs {
 };
 
 // Lane partial sums / extrema over all particles.  square != 0 folds (z - mu)^2.
-// Lane t must add elements t, t+4096, ... strictly in order, so the parallelism is across lanes; to
-// keep enough loads in flight each block stages a tile of kTileIters iterations x 32 lanes in shared
-// memory with all its threads (ten loads each in flight), then one thread per lane adds its column in
-// order.  grid (128, 1, 2).
-constexpr int kTileIters = 160, kLaneFoldThreads = 512;
+// Lane t must add elements t, t+4096, ... strictly in order, so the parallelism is across lanes.  A block
+// owns 32 lanes: all its threads stage up to kLaneFoldRows rows of the 32 lane columns in shared memory
+// (one tile covers the production beams), then one thread per lane adds its column in order from shared
+// memory, eight loads ahead.  The extrema do not depend on order (min and max with Julia's signed-zero
+// and NaN rules), so the staging threads fold them and a final pass combines the 16 threads of each lane.
+// grid (128, 1, 2); dynamic shared memory rows x 33 doubles.
+constexpr int kLaneFoldThreads = 512, kLaneFoldRows = 640;
 template <class R>
-__global__ void __launch_bounds__(kLaneFoldThreads) k_lane_fold(const SliceArgs<R> A, int square) {
+__global__ void __launch_bounds__(kLaneFoldThreads) k_lane_fold(const SliceArgs<R> A, int square, int rows) {
     pdl_wait();
     pdl_release();
     const int bm = blockIdx.z;
@@ -56,41 +58,88 @@ __global__ void __launch_bounds__(kLaneFoldThreads) k_lane_fold(const SliceArgs<
     const long long n = A.n[bm];
     const SliceInfo *info = A.info[bm];
     double *lane_sum = A.lane_sum[bm], *lane_min = A.lane_min[bm], *lane_max = A.lane_max[bm];
-    __shared__ double tile[kTileIters][33];
-    const int lane0 = blockIdx.x * 32;
+    double *tile = (double *)g_smem;  // [rows][33]
+    __shared__ double red_lo[kLaneFoldThreads], red_hi[kLaneFoldThreads];
+    const int lane0 = blockIdx.x * 32, t = threadIdx.x, l = t & 31;  // every element a thread stages is lane l's
     const double mu = square ? info->mu : 0.0;
+    const long long first = lane0 + l;
+    const long long cnt = first < n ? (n - first + kFoldLanes - 1) / kFoldLanes : 0;  // elements of lane l
     const long long iters = (n + kFoldLanes - 1) / kFoldLanes;
     double s = 0.0, lo = INFINITY, hi = -INFINITY;
-    const int t = threadIdx.x;
-    for (long long k0 = 0; k0 < iters; k0 += kTileIters) {
-        for (int e = t; e < kTileIters * 32; e += blockDim.x) {
-            const int kk = e >> 5, l = e & 31;
-            const long long i = (k0 + kk) * kFoldLanes + lane0 + l;
-            tile[kk][l] = i < n ? (double)z[i] : 0.0;
+    for (long long k0 = 0; k0 < iters; k0 += rows) {
+        const int nr = (int)min((long long)rows, iters - k0);
+        for (int e = t; e < nr * 32; e += blockDim.x) {
+            const int kk = e >> 5;
+            const long long k = k0 + kk;
+            double v = 0.0;
+            if (k < cnt) {
+                v = (double)z[k * kFoldLanes + first];
+                if (!square) {
+                    lo = jmin(lo, v);
+                    hi = jmax(hi, v);
+                }
+            }
+            tile[kk * 33 + l] = v;
         }
         __syncthreads();
         if (t < 32) {
-            const long long kmax = min((long long)kTileIters, iters - k0);
-            for (int kk = 0; kk < kmax; ++kk) {
-                const long long i = (k0 + kk) * kFoldLanes + lane0 + t;
-                if (i >= n) break;
-                const double v = tile[kk][t];
+            const int m = (int)max(0LL, min((long long)nr, cnt - k0));  // lane t's rows in this tile
+            int kk = 0;
+            for (; kk + 8 <= m; kk += 8) {
+                double v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) v[u] = tile[(kk + u) * 33 + t];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (square) {
+                        const double d = v[u] - mu;
+                        s += d * d;
+                    } else {
+                        s += v[u];
+                    }
+                }
+            }
+            for (; kk < m; ++kk) {
+                const double v = tile[kk * 33 + t];
                 if (square) {
                     const double d = v - mu;
                     s += d * d;
                 } else {
                     s += v;
-                    lo = jmin(lo, v);
-                    hi = jmax(hi, v);
                 }
             }
         }
         __syncthreads();
     }
-    if (t < 32) {
-        lane_sum[lane0 + t] = s;
-        if (!square) { lane_min[lane0 + t] = lo; lane_max[lane0 + t] = hi; }
+    if (!square) {
+        red_lo[t] = lo;
+        red_hi[t] = hi;
+        __syncthreads();
+        if (t < 32) {
+            for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+                lo = jmin(lo, red_lo[t + 32 * w]);
+                hi = jmax(hi, red_hi[t + 32 * w]);
+            }
+            lane_min[lane0 + t] = lo;
+            lane_max[lane0 + t] = hi;
+        }
     }
+    if (t < 32) lane_sum[lane0 + t] = s;
+}
+
+// In-order sum of n shared-memory values, sixteen loads ahead of the adds (the order of a plain loop).
+__device__ __forceinline__ double serial_sum(const double *v, int n) {
+    double s = 0.0;
+    int t = 0;
+    for (; t + 16 <= n; t += 16) {
+        double w[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) w[u] = v[t + u];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) s += w[u];
+    }
+    for (; t < n; ++t) s += v[t];
+    return s;
 }
 
 // Serial fold of the lanes (slicing.jl:254-257), staged through shared memory so the single adding
@@ -121,8 +170,7 @@ __global__ void __launch_bounds__(1024) k_fold_stats(const SliceArgs<R> A, int s
     }
     __syncthreads();
     if (threadIdx.x != 0) return;
-    double s = 0.0;
-    for (int t = 0; t < kFoldLanes; ++t) s += sl[t];
+    const double s = serial_sum(sl, kFoldLanes);
     if (stage == 0) {
         double lo = INFINITY, hi = -INFINITY;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { lo = jmin(lo, rlo[w]); hi = jmax(hi, rhi[w]); }
@@ -341,9 +389,7 @@ __global__ void __launch_bounds__(1024) k_slice_finish(const SliceArgs<R> A) {
     info->weight[s] = (double)cnt / (double)n;
     const double *b = info->boundary;
     if (fold) {
-        double acc = 0.0;
-        for (int t = 0; t < kFoldLanes; ++t) acc += sl[t];
-        info->center[s] = acc / (double)cnt;
+        info->center[s] = serial_sum(sl, kFoldLanes) / (double)cnt;
     } else {
         info->center[s] = (b[s] + b[s + 1]) / 2;
     }

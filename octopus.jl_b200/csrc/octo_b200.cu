@@ -475,9 +475,12 @@ void slice_beams(octo_ctx *c, const octo_beam &b1, const octo_beam &b2, cudaStre
             A.ns[b] = c->ns[b];
             A.cpos[b] = b == 0 ? c->opt.center_position1 : c->opt.center_position2;
         }
-        launch_pdl(k_lane_fold<R>, dim3(kFoldLanes / 32, 1, 2), kLaneFoldThreads, 0, st, A, 0);
+        const long long iters = (std::max(b1.n, b2.n) + kFoldLanes - 1) / kFoldLanes;
+        const int rows = (int)std::min<long long>(kLaneFoldRows, std::max<long long>(1, iters));
+        const size_t fold_smem = sizeof(double) * 33 * (size_t)rows;
+        launch_pdl(k_lane_fold<R>, dim3(kFoldLanes / 32, 1, 2), kLaneFoldThreads, fold_smem, st, A, 0, rows);
         launch_pdl(k_fold_stats<R>, 2, 1024, 0, st, A, 0);
-        launch_pdl(k_lane_fold<R>, dim3(kFoldLanes / 32, 1, 2), kLaneFoldThreads, 0, st, A, 1);
+        launch_pdl(k_lane_fold<R>, dim3(kFoldLanes / 32, 1, 2), kLaneFoldThreads, fold_smem, st, A, 1, rows);
         launch_pdl(k_fold_stats<R>, 2, 1024, 0, st, A, 1);
         launch_pdl(k_slice_count<R>, dim3((unsigned)nblk_max, 1, 2), 256, 0, st, A, kChunk);
         launch_pdl(k_slice_offsets<R>, 2, 1024, 0, st, A, kAlign);
@@ -572,6 +575,8 @@ void set_smem_limits() {
         CK(cudaFuncSetAttribute(k_conv_rows<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
         CK(cudaFuncSetAttribute(k_conv_cols<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
         CK(cudaFuncSetAttribute(k_conv_field<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(k_lane_fold<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                lim - (int)(2 * kLaneFoldThreads * sizeof(double))));
     };
     per_real(double(0));
     per_real(float(0));
