@@ -1119,6 +1119,29 @@ __device__ __forceinline__ void load_cell(const float4 *F, long long c, float &p
     ex = v.x; ey = v.y; phi = v.z;
 }
 
+// :node R planes with CIC taps are "pair cells": the kick reads only the field of an R plane, so the second
+// half of cell (i, j) holds the field of cell (i + 1, j) instead of phi and w, and the two x-taps of a row
+// are one 32-byte (16-byte) load.  The CIC base is clamped to i <= nx - 2, so the last cell's second half
+// is never read.
+__device__ __forceinline__ void store_field_pair(double2 *F, long long o, int i, double ex, double ey) {
+    F[2 * o] = make_double2(ex, ey);
+    if (i > 0) F[2 * o - 1] = make_double2(ex, ey);
+}
+__device__ __forceinline__ void store_field_pair(float4 *F, long long o, int i, float ex, float ey) {
+    float2 *f = reinterpret_cast<float2 *>(F);
+    f[2 * o] = make_float2(ex, ey);
+    if (i > 0) f[2 * o - 1] = make_float2(ex, ey);
+}
+__device__ __forceinline__ void load_field_pair(const double2 *F, long long c, double &ex0, double &ey0, double &ex1,
+                                                double &ey1) {
+    asm("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(ex0), "=d"(ey0), "=d"(ex1), "=d"(ey1) : "l"(F + 2 * c));
+}
+__device__ __forceinline__ void load_field_pair(const float4 *F, long long c, float &ex0, float &ey0, float &ex1,
+                                                float &ey1) {
+    const float4 v = F[c];
+    ex0 = v.x; ey0 = v.y; ex1 = v.z; ey1 = v.w;
+}
+
 // E = -grad(phi) on rows [jt0, jt1) of a plane (pic_cpu.jl:2531-2591) from the phi rows [ja0, ja1) held in
 // shared memory, stored as field cells; the :node Z plane stores only its phi, into its L plane's w word.
 template <class R>
@@ -1131,6 +1154,7 @@ __device__ __forceinline__ void field_cells(const Collide &C, const Plane &P, in
     const R c4 = (R)(1.0 / 12.0);
     const bool fourth = C.o.fourth != 0;
     const bool zplane = P.kind == 3;  // :node Z plane: only its phi is used, stored in its L plane's w word
+    const bool rpair = C.o.node && P.kind == 1 && C.o.method == 0;  // :node R plane, CIC: pair cells
     FC *F = (FC *)C.fields + (long long)(zplane ? pl - 2 : pl) * RealT<R>::kCellVec * nx * ny;
     auto Pv = [&](int i, int j) { return phi[(j - ja0) * nx + i]; };  // 0-based i, j
     for (int idx = threadIdx.x; idx < (jt1 - jt0) * nx; idx += blockDim.x) {
@@ -1152,7 +1176,8 @@ __device__ __forceinline__ void field_cells(const Collide &C, const Plane &P, in
         else if (fourth && (i == 1 || i == nx - 2)) ex = R(0.5) * hxi * (Pv(i - 1, j) - Pv(i + 1, j));
         else if (fourth) ex = c4 * hxi * ((Pv(i + 2, j) - Pv(i - 2, j)) + R(8) * (Pv(i - 1, j) - Pv(i + 1, j)));
         else ex = R(0.5) * hxi * (Pv(i - 1, j) - Pv(i + 1, j));
-        store_cell(F, (long long)j * nx + i, Pv(i, j), ex, ey);
+        if (rpair) store_field_pair(F, (long long)j * nx + i, i, ex, ey);
+        else store_cell(F, (long long)j * nx + i, Pv(i, j), ex, ey);
     }
 }
 
@@ -1533,12 +1558,24 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
         }
         {
             const Taps<R, METHOD> tp(o, gR, J.hxR, J.hyR, x, y);
+            if constexpr (METHOD == 0) {
+                // pair cells: row iy - 1 holds taps (0, 0) and (1, 0), row iy taps (0, 1) and (1, 1); summed in
+                // the x-outer tap order t = 0..3 = (0, 0), (0, 1), (1, 0), (1, 1)
+                R ex00, ey00, ex10, ey10, ex01, ey01, ex11, ey11;
+                load_field_pair(FR, tp.c0, ex00, ey00, ex10, ey10);
+                load_field_pair(FR, tp.c0 + o.nx, ex01, ey01, ex11, ey11);
+                KxR += tp.w[0] * ex00; KyR += tp.w[0] * ey00;
+                KxR += tp.w[1] * ex01; KyR += tp.w[1] * ey01;
+                KxR += tp.w[2] * ex10; KyR += tp.w[2] * ey10;
+                KxR += tp.w[3] * ex11; KyR += tp.w[3] * ey11;
+            } else {
 #pragma unroll
-            for (int t = 0; t < NT2; ++t) {
-                R ex, ey;
-                load_field(FR, tp.cell(t, o.nx), ex, ey);
-                KxR += tp.w[t] * ex;
-                KyR += tp.w[t] * ey;
+                for (int t = 0; t < NT2; ++t) {
+                    R ex, ey;
+                    load_field(FR, tp.cell(t, o.nx), ex, ey);
+                    KxR += tp.w[t] * ex;
+                    KyR += tp.w[t] * ey;
+                }
             }
         }
         px += ks * (zL * KxL + zR * KxR);
