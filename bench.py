@@ -43,8 +43,8 @@ CONFIG = {
     "l2": "inputs larger than L2 (172 MB of particle coordinates per turn)",
 }
 # DRAM bytes (read + write) per field particle of one kick launch, from one `ncu --set full` capture of
-# the 15-pair front of this workload (275.6 MB for 3.584M field particles).
-KICK_TRAFFIC_BYTES_PER_PARTICLE = 76.9
+# the 15-pair front of this workload (276.9 MB for 3.584M field particles).
+KICK_TRAFFIC_BYTES_PER_PARTICLE = 77.3
 
 
 def _dist():
@@ -139,13 +139,13 @@ def run_reference(args, rank):
         return 0
     budget = 180.0
     t0 = time.perf_counter()
-    one, threads, _ = _cpu_baseline(1)  # also serves as warm-up
-    per = one
+    n_warm = max(1, args.warmup)
+    per, threads, _ = _cpu_baseline(n_warm)  # the requested warm-up turns (median turn time sizes the sample)
     n_time = max(1, min(args.steps, int(max(1.0, (budget - (time.perf_counter() - t0)) / max(per, 1e-3)))))
     val, threads, sample = _cpu_baseline(n_time)
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": n_time,
-        "warmup": 1, "ms_per_step": val * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "warmup": n_warm, "ms_per_step": val * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded counter-RNG Gaussian beams)", "config": CONFIG,
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
