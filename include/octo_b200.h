@@ -135,6 +135,15 @@ int32_t octo_pic_collide_batch(int32_t count, octo_ctx *const *ctx, octo_beam *c
                                int32_t compute_luminosity, double *luminosity, octo_collide_report *reports,
                                int32_t *status, void *const *streams);
 
+/* Launch-shape autotuner (no reference counterpart; the extras' tile autotuner): times `rounds` collides
+ * of beam1/beam2 with each of four launch shapes -- charge-deposit blocks of at least one or two waves of
+ * the GPU's SMs per wavefront, kick blocks sized to fill one or two times the resident block slots -- after
+ * one untimed collide, and keeps the fastest shape for this context's later collides (*choice: 0..3).
+ * The shape changes only the time, never a result: charge sums are exact integers and every particle's
+ * kick is its own.  The collides update beam1 and beam2 in place, so pass scratch copies.  rounds: 1..16. */
+int32_t octo_pic_autotune(octo_ctx *ctx, octo_beam *beam1, octo_beam *beam2, const octo_beam_params *p1,
+                          const octo_beam_params *p2, int32_t rounds, int32_t *choice, void *stream);
+
 /* Green-cache counters (the contract of Contracts.jl:947-960). */
 int32_t octo_green_cache_stats(octo_ctx *ctx, int64_t *hits, int64_t *misses, int64_t *rebuilds);
 

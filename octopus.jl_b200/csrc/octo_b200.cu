@@ -194,6 +194,9 @@ struct BeamWS {
 struct octo_ctx {
     int device = 0;
     int num_sms = 148;  // the device's SM count (block-count policies)
+    // launch shape (octo_pic_autotune): the deposit launches at least dep_waves waves of the SMs per front,
+    // the kick sizes its blocks to fill kick_slots times the resident block slots
+    int dep_waves = 1, kick_slots = 1;
     octo_pic_options opt{};
     std::vector<double> pos[2];
     DevOptions dopt{};
@@ -936,7 +939,7 @@ void CollideJob::run() {
         // resident block slots (two per SM in FP64, four in FP32)
         long long nfld = 0;
         for (int t = F.t0; t < F.t0 + F.nt; ++t) nfld += tasks[t].fld_n;
-        const long long slots = (long long)c->num_sms * (fp32 ? 4 : 2);
+        const long long slots = (long long)c->num_sms * (fp32 ? 4 : 2) * c->kick_slots;
         const long long want = (nfld + slots - 1) / slots;
         F.kchunk = (int)std::min<long long>(kKickChunk, std::max<long long>(kKickThreads, (want + kKickThreads - 1) /
                                                                                            kKickThreads * kKickThreads));
@@ -1143,7 +1146,7 @@ void CollideJob::run() {
             PhaseScope ps(c, OCTO_PHASE_DEPOSIT, st, 1, src_bytes * 4 * rsz);
             // blocks per plane: 32768-particle shares, and at least one full wave of the GPU's SMs for the
             // narrow fronts (one block per SM: a block holds its plane's whole int64 grid)
-            const long long wave = (c->num_sms + F.np - 1) / F.np;
+            const long long wave = ((long long)c->num_sms * c->dep_waves + F.np - 1) / F.np;
             unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(32, std::max<long long>((F.maxsrc + 32767) / 32768, wave)));
             with_real(fp32, [&](auto r) {
                 launch_method(method, [&](auto M) {
@@ -1429,6 +1432,51 @@ int32_t octo_pic_collide(octo_ctx *c, octo_beam *beam1, octo_beam *beam2, const 
         if (report) report->status = OCTO_ERR_CUDA;
         return fail(c, OCTO_ERR_CUDA, e.msg);
     }
+}
+
+int32_t octo_pic_autotune(octo_ctx *c, octo_beam *beam1, octo_beam *beam2, const octo_beam_params *p1,
+                          const octo_beam_params *p2, int32_t rounds, int32_t *choice, void *stream) {
+    if (!c) return OCTO_ERR_ARG;
+    if (rounds < 1 || rounds > 16) return fail(c, OCTO_ERR_ARG, "autotune rounds must be 1..16");
+    static const int kShapes[4][2] = {{1, 1}, {2, 1}, {1, 2}, {2, 2}};  // (dep_waves, kick_slots)
+    const cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    double best[4];
+    for (double &b : best) b = 1e300;
+    int32_t rc = OCTO_OK;
+    try {
+        CK(cudaSetDevice(c->device));
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        // one collide first (Green cache, workspaces), then every shape once per round
+        for (int r = -1; r < rounds && rc == OCTO_OK; ++r) {
+            for (int k = 0; k < 4 && rc == OCTO_OK; ++k) {
+                if (r < 0 && k > 0) break;
+                c->dep_waves = kShapes[k][0];
+                c->kick_slots = kShapes[k][1];
+                CK(cudaEventRecord(e0, st));
+                double lum;
+                rc = octo_pic_collide(c, beam1, beam2, p1, p2, -1, 1, &lum, nullptr, stream);
+                CK(cudaEventRecord(e1, st));
+                CK(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                if (r >= 0) best[k] = std::min(best[k], (double)ms);
+            }
+        }
+    } catch (CudaFail &e) {
+        rc = fail(c, OCTO_ERR_CUDA, e.msg);
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    int pick = 0;
+    for (int k = 1; k < 4; ++k)
+        if (best[k] < best[pick]) pick = k;
+    if (rc != OCTO_OK) pick = 0;  // a failed collide leaves the default shape
+    c->dep_waves = kShapes[pick][0];
+    c->kick_slots = kShapes[pick][1];
+    if (choice) *choice = pick;
+    return rc;
 }
 
 int32_t octo_pic_collide_batch(int32_t count, octo_ctx *const *ctxs, octo_beam *const *beam1, octo_beam *const *beam2,

@@ -170,6 +170,21 @@ function _collide!(ctx::Context, solver::B200Solver, beam1::Beam, beam2::Beam, t
     return Float64(lum[])
 end
 
+"""autotune!(ctx, beam1, beam2; rounds=2) -> shape index: times collides of copies of the beams in each
+launch shape (octo_pic_autotune) and keeps the fastest for this context; results do not depend on it."""
+function autotune!(ctx::Context, beam1::Beam, beam2::Beam; rounds::Integer=2)
+    c1 = deepcopy(beam1); c2 = deepcopy(beam2)
+    b1 = Ref(_octo_beam(c1)); b2 = Ref(_octo_beam(c2))
+    p1 = Ref(_octo_params(c1)); p2 = Ref(_octo_params(c2))
+    choice = Ref(Int32(-1))
+    rc = GC.@preserve c1 c2 ccall((:octo_pic_autotune, LIB), Int32,
+               (Ptr{Cvoid}, Ref{OctoBeam}, Ref{OctoBeam}, Ref{OctoBeamParams}, Ref{OctoBeamParams}, Int32,
+                Ref{Int32}, Ptr{Cvoid}),
+               ctx.ptr, b1, b2, p1, p2, Int32(rounds), choice, CUDA.stream().handle)
+    rc == 0 || throw(ArgumentError(_last_error(ctx)))
+    return Int(choice[])
+end
+
 """collide!(solver, beam1, beam2, CUDABackend[, ctx]) on libocto_b200: a fresh (cold) context per call,
 as the reference's public collide! builds a fresh Green cache (pic_cuda.jl:94-126)."""
 function Octopus.collide!(solver::B200Solver, beam1::Beam, beam2::Beam, ::Type{CUDABackend},

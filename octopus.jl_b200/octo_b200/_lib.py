@@ -24,7 +24,7 @@ EXPORTS = (
     "octo_create", "octo_destroy", "octo_pic_collide", "octo_green_cache_stats",
     "octo_pair_luminosity_trace", "octo_linear6d", "octo_beam_gaussian", "octo_last_error",
     "octo_normal_quantile", "octo_erfinv", "octo_version", "octo_set_timing", "octo_timing_report",
-    "octo_beam_gaussian_noalloc", "octo_pic_collide_batch", "octo_set_timing_phases",
+    "octo_beam_gaussian_noalloc", "octo_pic_collide_batch", "octo_set_timing_phases", "octo_pic_autotune",
 )
 
 PHASES = ("slicing", "bounds", "plan", "green", "luminosity", "deposit", "fft", "field", "kick", "unsort", "node")
@@ -102,6 +102,8 @@ def lib():
     L.octo_pic_collide_batch.restype = i32
     L.octo_pic_collide_batch.argtypes = [i32, P(vp), P(P(OctoBeam)), P(P(OctoBeam)), P(P(OctoBeamParams)),
                                          P(P(OctoBeamParams)), i64, i32, P(d), P(OctoCollideReport), P(i32), P(vp)]
+    L.octo_pic_autotune.restype = i32
+    L.octo_pic_autotune.argtypes = [vp, P(OctoBeam), P(OctoBeam), P(OctoBeamParams), P(OctoBeamParams), i32, P(i32), vp]
     L.octo_green_cache_stats.restype = i32
     L.octo_green_cache_stats.argtypes = [vp, P(i64), P(i64), P(i64)]
     L.octo_pair_luminosity_trace.restype = i64

@@ -87,6 +87,25 @@ class Context:
             raise CollisionError(rc, f"{_lib.ERROR_NAMES.get(rc, rc)}: {_lib.last_error(self._ptr)}", rep)
         return lum.value
 
+    AUTOTUNE_SHAPES = ((1, 1), (2, 1), (1, 2), (2, 2))  # (deposit waves, kick block-slot multiple)
+
+    def autotune(self, beam1: Beam, beam2: Beam, rounds: int = 2,
+                 stream: Optional[torch.cuda.Stream] = None) -> int:
+        """Pick this context's launch shape by timing collides of copies of beam1 and beam2 (the beams
+        themselves are untouched); later collides give the same results in any shape, only faster.
+        Returns the chosen shape's index into AUTOTUNE_SHAPES."""
+        c1 = Beam(beam1.coords.clone(), beam1.params)
+        c2 = Beam(beam2.coords.clone(), beam2.params)
+        b1, b2 = c1.to_c(), c2.to_c()
+        p1, p2 = c1.params.to_c(), c2.params.to_c()
+        choice = C.c_int32(-1)
+        st = (stream or torch.cuda.current_stream(beam1.coords.device)).cuda_stream
+        rc = _lib.lib().octo_pic_autotune(self._ptr, C.byref(b1), C.byref(b2), C.byref(p1), C.byref(p2), int(rounds),
+                                          C.byref(choice), C.c_void_p(st))
+        if rc != _lib.OCTO_OK:
+            raise CollisionError(rc, f"{_lib.ERROR_NAMES.get(rc, rc)}: {_lib.last_error(self._ptr)}", None)
+        return choice.value
+
     def green_cache_stats(self) -> Tuple[int, int, int]:
         h, m, r = C.c_int64(), C.c_int64(), C.c_int64()
         _lib.lib().octo_green_cache_stats(self._ptr, C.byref(h), C.byref(m), C.byref(r))
