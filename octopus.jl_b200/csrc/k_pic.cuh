@@ -73,11 +73,10 @@ __device__ __forceinline__ unsigned long long shfl_max_u64(unsigned long long v)
 // Extremes of one slice of a pair in all three roles it plays: source of one direction
 // (drifted to sL and sR, pic_cpu.jl:961-1003), field of the other (drifted to its collision
 // point, pic_cpu.jl:1005-1035) and luminosity source (drifted to sM, pic_cpu.jl:1279-1287).
-// LUM_ONLY (interaction_grid = :node, whose meshes are prebuilt) keeps only the luminosity role.
 // Per-thread extrema use the native min/max (NaN is flagged separately; a +-0 tie cannot change any
 // geometry built from them), encoded to ordered integers once per block for the atomics.
 // grid: (blocks per side, 2 * pairs in front).
-template <class R, bool LUM_ONLY>
+template <class R>
 __global__ void __launch_bounds__(256) k_pair_bounds(Collide C, int task0) {
     pdl_wait();
     pdl_release();
@@ -103,30 +102,27 @@ __global__ void __launch_bounds__(256) k_pair_bounds(Collide C, int task0) {
         nan_l |= (lx != lx) | (ly != ly);
         mn[4] = fmin(mn[4], lx); mx[4] = fmax(mx[4], lx);
         mn[5] = fmin(mn[5], ly); mx[5] = fmax(mx[5], ly);
-        if (!LUM_ONLY) {
-            const R z = Z[k];
-            const R a = x + px * sL, b = x + px * sR, c = y + py * sL, d = y + py * sR;
-            const R s = R(0.5) * (z - cf);
-            const R fx = x + s * px, fy = y + s * py;
-            nan_s |= (a != a) | (b != b) | (c != c) | (d != d);
-            nan_f |= (fx != fx) | (fy != fy);
-            mn[0] = fmin(mn[0], fmin(a, b)); mx[0] = fmax(mx[0], fmax(a, b));
-            mn[1] = fmin(mn[1], fmin(c, d)); mx[1] = fmax(mx[1], fmax(c, d));
-            mn[2] = fmin(mn[2], fx); mx[2] = fmax(mx[2], fx);
-            mn[3] = fmin(mn[3], fy); mx[3] = fmax(mx[3], fy);
-        }
+        const R z = Z[k];
+        const R a = x + px * sL, b = x + px * sR, c = y + py * sL, d = y + py * sR;
+        const R s = R(0.5) * (z - cf);
+        const R fx = x + s * px, fy = y + s * py;
+        nan_s |= (a != a) | (b != b) | (c != c) | (d != d);
+        nan_f |= (fx != fx) | (fy != fy);
+        mn[0] = fmin(mn[0], fmin(a, b)); mx[0] = fmax(mx[0], fmax(a, b));
+        mn[1] = fmin(mn[1], fmin(c, d)); mx[1] = fmax(mx[1], fmax(c, d));
+        mn[2] = fmin(mn[2], fx); mx[2] = fmax(mx[2], fx);
+        mn[3] = fmin(mn[3], fy); mx[3] = fmax(mx[3], fy);
     }
     __shared__ unsigned long long red[8][12];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-        if (LUM_ONLY && k < 4) continue;
         unsigned long long a = shfl_min_u64(mn[k] == R(INFINITY) ? kOrdMinInit : ord_encode((double)mn[k]));
         unsigned long long b = shfl_max_u64(mx[k] == R(-INFINITY) ? kOrdMaxInit : ord_encode((double)mx[k]));
         if (lane == 0) { red[warp][2 * k] = a; red[warp][2 * k + 1] = b; }
     }
     int any_s = __syncthreads_or(nan_s), any_f = __syncthreads_or(nan_f), any_l = __syncthreads_or(nan_l);
-    if (threadIdx.x < 12 && !(LUM_ONLY && threadIdx.x < 8)) {
+    if (threadIdx.x < 12) {
         int k = threadIdx.x;
         unsigned long long r = red[0][k];
         for (int w = 1; w < (int)(blockDim.x >> 5); ++w) r = (k & 1) ? max(r, red[w][k]) : min(r, red[w][k]);

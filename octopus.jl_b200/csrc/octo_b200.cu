@@ -1103,7 +1103,7 @@ void CollideJob::run() {
         const unsigned bps = (unsigned)std::max<long long>(1, std::min<long long>(kMaxBoundBlocks, (F.maxsrc + 2047) / 2048));
         if (!node) {
             PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, gaussian ? 2 : 1, slice_bytes * 5 * rsz);
-            with_real(fp32, [&](auto r) { launch_pdl(k_pair_bounds<decltype(r), false>, dim3(bps, 2 * npf), 256, 0, st, C, F.t0); });
+            with_real(fp32, [&](auto r) { launch_pdl(k_pair_bounds<decltype(r)>, dim3(bps, 2 * npf), 256, 0, st, C, F.t0); });
             if (gaussian) {
                 launch_pdl(k_hyb_moments, dim3(bps, 2 * npf), 256, 0, st, C, F.t0);
                 launch_pdl(k_hyb_fold, (F.nt * 32 + 127) / 128, 128, 0, st, C, F.t0, F.nt, (int)bps);
