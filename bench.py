@@ -15,6 +15,7 @@ shard); `value` is the whole-job seconds per turn (max-over-ranks step time / tu
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -78,7 +79,7 @@ class Clocks:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-lms", "100", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -201,12 +202,17 @@ def run_ours(args, rank, world, local_rank):
     barrier()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # every turn waits on the host for its luminosity, so a host pause is GPU idle time: no Python garbage
+    # collection inside the timed loops
+    gc.collect()
+    gc.disable()
     ev0.record(stream)
     for t in range(args.steps):
         lum = turn(args.warmup + t)
         launches += ctx.last_report.kernel_launches + 2
     ev1.record(stream)
     torch.cuda.synchronize()
+    gc.enable()
     barrier()
     ms = ev0.elapsed_time(ev1) / args.steps
     n_kick = max(3, min(args.steps, 20))
@@ -230,6 +236,8 @@ def run_ours(args, rank, world, local_rank):
     e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, 20))
     torch.cuda.synchronize()
     barrier()
+    gc.collect()
+    gc.disable()
     w0 = time.perf_counter()
     ev0.record(stream)
     for t in range(e2e_steps):
@@ -240,6 +248,7 @@ def run_ours(args, rank, world, local_rank):
         hp.copy_(p.coords, non_blocking=True)
     ev1.record(stream)
     torch.cuda.synchronize()
+    gc.enable()
     wall = (time.perf_counter() - w0) / max(e2e_steps, 1)
     barrier()
     e2e_ms = ev0.elapsed_time(ev1) / e2e_steps if e2e_steps else float("nan")
@@ -266,11 +275,14 @@ def run_ours(args, rank, world, local_rank):
         cX.set_timing(False)
         barrier()
         torch.cuda.synchronize()
+        gc.collect()
+        gc.disable()
         ev0.record(stream)
         for t in range(args.steps):
             lumX = turnX(args.warmup + t)
         ev1.record(stream)
         torch.cuda.synchronize()
+        gc.enable()
         barrier()
         msX = ev0.elapsed_time(ev1) / args.steps
         cX.set_timing(True, phases=["kick"])
