@@ -154,6 +154,51 @@ int64_t octo_pair_luminosity_trace(octo_ctx *ctx, int32_t *pair_i, int32_t *pair
 /* Linear 6D one-turn map (linear6d.jl:110-121), row-major 6x6, applied `turns` times in place. */
 int32_t octo_linear6d(octo_ctx *ctx, octo_beam *beam, const double matrix[36], int32_t turns, void *stream);
 
+/* Line tracking between collisions: a sequence of zero-length elements applied to every particle in one
+ * fused pass (one read and one write of the six coordinates per particle and call), the twin of
+ * track!(rep, elems, turns; context) with fusedTrack (src/track/phase6d_track.jl:25-35, 197-212;
+ * src/track/fused_track.jl:53-77) for the elements the production strong-strong lines place around the
+ * collision (examples/strong_strong_tracking.jl:206-262).  Element parameters (p[]) per kind: */
+#define OCTO_ELEM_LINEAR6D 1             /* p[0..35] row-major 6x6 matrix (linear6d.jl:110-121) */
+#define OCTO_ELEM_THIN_CRAB_CAVITY 2     /* p[0] frequency [Hz], finite and nonzero; harmonic h < nharm:
+                                            p[1+h] strengthX, p[9+h] strengthY, p[17+h] phase [rad]
+                                            (crab_cavity.jl:87-144) */
+#define OCTO_ELEM_LORENTZ_BOOST 3        /* p[0] half crossing angle [rad] (lorentz_boost.jl:128-143) */
+#define OCTO_ELEM_REV_LORENTZ_BOOST 4    /* p[0] half crossing angle [rad] (lorentz_boost.jl:148-161) */
+#define OCTO_ELEM_CHROMATICITY_KICK 5    /* p[0..1] xi, p[2..3] beta, p[4..5] alpha, p[6..9] zeta,
+                                            p[10..13] eta, p[14..17] R (chromaticity_kick.jl:74-136) */
+#define OCTO_ELEM_LUMPED_RAD 6           /* p[0..2] damping_turns, p[3..5] beta, p[6..8] alpha,
+                                            p[9..11] sigma (all >= 0 enables excitation, all < 0 disables it),
+                                            p[12..15] zeta, p[16..19] eta, p[20..23] R; mode = OCTO_RAD_*,
+                                            is_damping, is_excitation, rng_id (radiation.jl:83-232) */
+#define OCTO_ELEM_CRAB_DISPERSION 7      /* p[0..3] zeta1..zeta4 (linear_maps.jl:125-132) */
+#define OCTO_ELEM_MOMENTUM_DISPERSION 8  /* p[0..3] eta1..eta4 (linear_maps.jl:213-220) */
+#define OCTO_ELEM_XY_COUPLING 9          /* p[0..3] r1..r4, 1 + r1 r4 - r2 r3 > 0; mode 0 identity, 1 A, 2 B
+                                            (linear_maps.jl:296-310, 355-373) */
+#define OCTO_RAD_RADIATION 0 /* Radiation6DMap: damping and excitation as flagged */
+#define OCTO_RAD_DAMPING 1   /* Damping6DMap: damping only */
+#define OCTO_RAD_DIFFUSION 2 /* Diffusion6DMap: excitation only */
+#define OCTO_RNG_PHILOX 1    /* RNG_PHILOX (counter_rng.jl:10) */
+#define OCTO_RNG_SPLITMIX 2  /* RNG_SPLITMIX (counter_rng.jl:13) */
+#define OCTO_CRAB_MAX_HARMONICS 8
+#define OCTO_LINE_MAX_ELEMENTS 32
+typedef struct {
+    int32_t kind;          /* OCTO_ELEM_* */
+    int32_t nharm;         /* thin crab cavity: harmonic count N, 1..OCTO_CRAB_MAX_HARMONICS */
+    int32_t mode;          /* lumped radiation: OCTO_RAD_*; xy coupling: 0, 1, 2 */
+    int32_t is_damping;    /* lumped radiation flags */
+    int32_t is_excitation;
+    int32_t reserved;
+    uint64_t rng_id;       /* lumped radiation counter-RNG stream id */
+    double p[40];
+} octo_element;
+/* Applies elems[0..n_elems) to every particle of beam, `turns` times.  Turn t (0-based) of the call draws
+ * the radiation noise of TrackingContext turn `turn + t` (seed, rng_method: OCTO_RNG_*), particle i
+ * (0-based) as particle_id i + 1, so a run split into several calls is bit-identical to one call.
+ * Parameters are validated as the reference's constructors do (OCTO_ERR_ARG with the message). */
+int32_t octo_track_line(octo_ctx *ctx, octo_beam *beam, const octo_element *elems, int32_t n_elems, int64_t turn,
+                        int32_t turns, uint64_t seed, int32_t rng_method, void *stream);
+
 /* Seeded Gaussian beam on the device as Beam(n, backend, Float64; beta, alpha, sigma, cutoff, rng_id)
  * builds it (Beam.jl:475-515; counter RNG counter_rng.jl:154-233). */
 int32_t octo_beam_gaussian(octo_ctx *ctx, octo_beam *beam, uint64_t seed, uint64_t rng_id, const double beta[3],

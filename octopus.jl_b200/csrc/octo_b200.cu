@@ -12,11 +12,13 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/octo_b200.h"
+#include "k_line.cuh"
 #include "k_misc.cuh"
 #include "k_pic.cuh"
 #include "k_slicing.cuh"
@@ -1300,6 +1302,215 @@ int fail(octo_ctx *c, int code, const std::string &m) {
     return code;
 }
 
+// ---------------------------------------------------------------- line elements
+uint64_t splitmix64_host(uint64_t x) {
+    uint64_t z = x + 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+// _linear6d_symplectic_error (linear6d.jl:147-204): the worst row of M^T J M - J against a componentwise
+// forward-error bound, 64 eps max(1, row scale).  Returns the ratio (> 1 rejects; non-finite entries: inf).
+double linear6d_symplectic_ratio(const double *m) {
+    const double inf = std::numeric_limits<double>::infinity();
+    for (int k = 0; k < 36; ++k)
+        if (!std::isfinite(m[k])) return inf;
+    double worst = 0.0;
+    for (int i = 0; i < 6; ++i) {
+        double row_res = 0.0, row_scale = 0.0;
+        for (int j = 0; j < 6; ++j) {
+            double value = 0.0, pscale = 0.0;
+            for (int q = 0; q < 6; q += 2) {
+                const double pos = m[q * 6 + i] * m[(q + 1) * 6 + j];
+                const double neg = m[(q + 1) * 6 + i] * m[q * 6 + j];
+                if (!std::isfinite(pos) || !std::isfinite(neg)) return inf;
+                value = (value + pos) - neg;
+                pscale += std::fabs(pos) + std::fabs(neg);
+            }
+            const double target = (i % 2 == 0 && j == i + 1) ? 1.0 : (i % 2 == 1 && j == i - 1) ? -1.0 : 0.0;
+            row_res += std::fabs(value - target);
+            row_scale += std::max(std::fabs(target), pscale);
+        }
+        const double tol = 64.0 * std::numeric_limits<double>::epsilon() * std::max(1.0, row_scale);
+        if (!std::isfinite(row_res) || !std::isfinite(tol)) return inf;
+        const double ratio = tol > 0.0 ? row_res / tol : (row_res == 0.0 ? 0.0 : inf);
+        worst = std::max(worst, ratio);
+    }
+    return worst;
+}
+
+bool all_finite(const double *v, int n) {
+    for (int k = 0; k < n; ++k)
+        if (!std::isfinite(v[k])) return false;
+    return true;
+}
+
+// 1 / sqrt(1 + r1 r4 - r2 r3) of a coupling block, with the XYCoupling constructor's check
+// (linear_maps.jl:296-310).
+bool coupling_scale(const double *r, double &g, std::string &msg, const char *who) {
+    const double det = 1.0 + r[0] * r[3] - r[1] * r[2];
+    if (std::isfinite(det) && det <= 0.0) {
+        char b[256];
+        snprintf(b, sizeof b, "%s: XYCoupling is not invertible: 1 + r1*r4 - r2*r3 = %.17g must be positive", who, det);
+        msg = b;
+        return false;
+    }
+    g = 1.0 / std::sqrt(det);
+    return true;
+}
+
+// kZeroZeta / kZeroEta / kZeroR for a frame's zeta[4], eta[4], R[4] (contiguous).
+int zero_frame_flags(const double *zer) {
+    auto zero4 = [](const double *v) { return v[0] == 0.0 && v[1] == 0.0 && v[2] == 0.0 && v[3] == 0.0; };
+    return (zero4(zer) ? kZeroZeta : 0) | (zero4(zer + 4) ? kZeroEta : 0) | (zero4(zer + 8) ? kZeroR : 0);
+}
+
+// Compiles one element into its constant form (the compile_runtime step of each element's constructor),
+// validating as those constructors do.
+int compile_line_op(const octo_element &e, int rng, uint64_t seed, LineOp &op, std::string &msg) {
+    std::memset(&op, 0, sizeof op);
+    op.kind = e.kind;
+    const double *p = e.p;
+    char b[320];
+    switch (e.kind) {
+        case OCTO_ELEM_LINEAR6D: {
+            const double ratio = linear6d_symplectic_ratio(p);
+            if (!(ratio <= 1.0)) {
+                snprintf(b, sizeof b,
+                         "Linear6D runtime matrix must be finite and canonical symplectic in (x, px, y, py, z, pz) "
+                         "order: ratio=%.6g",
+                         ratio);
+                msg = b;
+                return OCTO_ERR_ARG;
+            }
+            for (int k = 0; k < 36; ++k) op.a[k] = p[k];
+            return OCTO_OK;
+        }
+        case OCTO_ELEM_THIN_CRAB_CAVITY: {
+            if (!std::isfinite(p[0]) || p[0] == 0.0) {
+                snprintf(b, sizeof b, "thin crab-cavity frequency must be finite and nonzero; got %.17g", p[0]);
+                msg = b;
+                return OCTO_ERR_ARG;
+            }
+            if (e.nharm < 1 || e.nharm > OCTO_CRAB_MAX_HARMONICS) {
+                msg = "thin crab-cavity harmonic count must be 1.." + std::to_string(OCTO_CRAB_MAX_HARMONICS);
+                return OCTO_ERR_ARG;
+            }
+            // kcc = 2 pi f / c (crab_cavity.jl:93), i kcc per harmonic (:133); harmonics with both strengths
+            // zero are dropped (their terms are zeros for finite particles; the kernel keeps their NaN spread)
+            const double kcc = 2.0 * 3.14159265358979323846 * p[0] / 299792458.0;
+            op.n = 0;
+            for (int h = 0; h < e.nharm; ++h) {
+                if (p[1 + h] == 0.0 && p[9 + h] == 0.0) {
+                    op.flags |= kCrabDropped;
+                    continue;
+                }
+                op.a[op.n] = (double)(h + 1) * kcc;
+                op.a[8 + op.n] = p[1 + h];
+                op.a[16 + op.n] = p[9 + h];
+                op.a[24 + op.n] = p[17 + h];
+                ++op.n;
+            }
+            return OCTO_OK;
+        }
+        case OCTO_ELEM_LORENTZ_BOOST:
+        case OCTO_ELEM_REV_LORENTZ_BOOST: {
+            if (!std::isfinite(p[0])) { msg = "Lorentz boost angle must be finite"; return OCTO_ERR_ARG; }
+            // _lorentz_boost (lorentz_boost.jl:168-174)
+            const double c = std::cos(p[0]), s = std::sin(p[0]);
+            op.a[0] = c;
+            op.a[1] = s;
+            op.a[2] = s / c;
+            return OCTO_OK;
+        }
+        case OCTO_ELEM_CHROMATICITY_KICK: {
+            if (!all_finite(p, 18)) { msg = "chromaticity kick parameters must be finite"; return OCTO_ERR_ARG; }
+            // ChromaticityKick(spec) (chromaticity_kick.jl:74-96)
+            for (int k = 0; k < 6; ++k) op.a[k] = p[k];
+            op.a[6] = (1.0 + p[4] * p[4]) / p[2];
+            op.a[7] = (1.0 + p[5] * p[5]) / p[3];
+            for (int k = 0; k < 12; ++k) op.a[8 + k] = p[6 + k];
+            op.flags = zero_frame_flags(p + 6);
+            return coupling_scale(p + 14, op.a[20], msg, "chromaticity kick") ? OCTO_OK : OCTO_ERR_ARG;
+        }
+        case OCTO_ELEM_LUMPED_RAD: {
+            // LumpedRad(spec) and _validate_lumped_rad_parameters (radiation.jl:83-160)
+            for (int i = 0; i < 3; ++i)
+                if (!(p[i] > 0.0)) {
+                    snprintf(b, sizeof b, "damping_turns[%d] must be positive, got %.17g", i + 1, p[i]);
+                    msg = b;
+                    return OCTO_ERR_ARG;
+                }
+            static const char *names[6] = {"beta", "alpha", "sigma", "zeta", "eta", "R"};
+            static const int off[6] = {3, 6, 9, 12, 16, 20}, len[6] = {3, 3, 3, 4, 4, 4};
+            for (int g = 0; g < 6; ++g)
+                for (int i = 0; i < len[g]; ++i)
+                    if (!std::isfinite(p[off[g] + i])) {
+                        snprintf(b, sizeof b, "%s[%d] must be finite, got %.17g", names[g], i + 1, p[off[g] + i]);
+                        msg = b;
+                        return OCTO_ERR_ARG;
+                    }
+            for (int i = 0; i < 3; ++i)
+                if (!(p[3 + i] > 0.0)) {
+                    snprintf(b, sizeof b, "beta[%d] must be positive, got %.17g", i + 1, p[3 + i]);
+                    msg = b;
+                    return OCTO_ERR_ARG;
+                }
+            const bool enabled = p[9] >= 0.0 && p[10] >= 0.0 && p[11] >= 0.0;
+            const bool disabled = p[9] < 0.0 && p[10] < 0.0 && p[11] < 0.0;
+            if (!enabled && !disabled) {
+                msg = "sigma must be nonnegative in all three planes to enable excitation or negative in all three "
+                      "planes to disable it";
+                return OCTO_ERR_ARG;
+            }
+            if (e.mode < OCTO_RAD_RADIATION || e.mode > OCTO_RAD_DIFFUSION) {
+                msg = "LumpedRad supports Radiation6DMap, Damping6DMap, or Diffusion6DMap";
+                return OCTO_ERR_ARG;
+            }
+            // _lumped_rad_effective_components (radiation.jl:162-171)
+            const bool damp = e.is_damping != 0 && e.mode != OCTO_RAD_DIFFUSION;
+            const bool exc = e.is_excitation != 0 && enabled && e.mode != OCTO_RAD_DAMPING;
+            op.flags = (damp ? kRadDamping : 0) | (exc ? kRadExcitation : 0) | zero_frame_flags(p + 12);
+            for (int i = 0; i < 3; ++i) {
+                op.a[i] = std::exp(-1.0 / p[i]);
+                // _radiation_excitation (radiation.jl:286-299) with scale sqrt(-expm1(-2/tau)) (:110-113)
+                const double scale = std::sqrt(-std::expm1(-2.0 / p[i]));
+                const double sigma = p[9 + i];
+                const double amp = sigma < 0.0 ? 0.0 : sigma * scale;
+                const double slope = sigma < 0.0 ? 0.0 : amp / p[3 + i];
+                op.a[3 + 3 * i] = amp;
+                op.a[4 + 3 * i] = slope;
+                op.a[5 + 3 * i] = sigma < 0.0 ? 0.0 : -slope * p[6 + i];
+            }
+            for (int k = 0; k < 12; ++k) op.a[12 + k] = p[12 + k];
+            if (!coupling_scale(p + 20, op.a[24], msg, "lumped radiation")) return OCTO_ERR_ARG;
+            // component keys (counter_rng.jl:187-205 for Philox, :284-291 for SplitMix)
+            for (int c = 1; c <= 6; ++c)
+                op.key[c - 1] = rng == OCTO_RNG_PHILOX
+                                    ? splitmix64_host(seed) ^ splitmix64_host(e.rng_id + 0x9e3779b97f4a7c15ull) ^
+                                          splitmix64_host((uint64_t)c + 0xbf58476d1ce4e5b9ull)
+                                    : seed ^ splitmix64_host(e.rng_id + 0xbf58476d1ce4e5b9ull) ^
+                                          splitmix64_host((uint64_t)c + 0xD2B74407B1CE6E93ull);
+            return OCTO_OK;
+        }
+        case OCTO_ELEM_CRAB_DISPERSION:
+        case OCTO_ELEM_MOMENTUM_DISPERSION:
+            if (!all_finite(p, 4)) { msg = "dispersion coefficients must be finite"; return OCTO_ERR_ARG; }
+            for (int k = 0; k < 4; ++k) op.a[k] = p[k];
+            return OCTO_OK;
+        case OCTO_ELEM_XY_COUPLING:
+            if (e.mode < 0 || e.mode > 2) { msg = "XYCoupling mode must be 0 (undefined), 1 (A) or 2 (B)"; return OCTO_ERR_ARG; }
+            for (int k = 0; k < 4; ++k) op.a[k] = p[k];
+            op.n = e.mode;
+            if (e.mode == 0) return OCTO_OK;
+            return coupling_scale(p, op.a[4], msg, "xy coupling") ? OCTO_OK : OCTO_ERR_ARG;
+        default:
+            msg = "unknown line element kind " + std::to_string(e.kind);
+            return OCTO_ERR_ARG;
+    }
+}
+
 }  // namespace
 
 // ====================================================================== C ABI
@@ -1567,6 +1778,56 @@ int32_t octo_linear6d(octo_ctx *c, octo_beam *beam, const double matrix[36], int
             k_linear6d<R><<<(unsigned)((beam->n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
                 (R *)beam->x, (R *)beam->px, (R *)beam->y, (R *)beam->py, (R *)beam->z, (R *)beam->pz, beam->n, M, turns);
         });
+        CK(cudaGetLastError());
+        return OCTO_OK;
+    } catch (CudaFail &e) {
+        return fail(c, OCTO_ERR_CUDA, e.msg);
+    }
+}
+
+int32_t octo_track_line(octo_ctx *c, octo_beam *beam, const octo_element *elems, int32_t n_elems, int64_t turn,
+                        int32_t turns, uint64_t seed, int32_t rng_method, void *stream) {
+    if (!c || !beam || (n_elems > 0 && !elems)) return OCTO_ERR_ARG;
+    if (n_elems < 0 || n_elems > OCTO_LINE_MAX_ELEMENTS)
+        return fail(c, OCTO_ERR_ARG, "a line holds 0.." + std::to_string(OCTO_LINE_MAX_ELEMENTS) + " elements");
+    if (turns < 0) return fail(c, OCTO_ERR_ARG, "turns must be non-negative");
+    if (turn < 0) return fail(c, OCTO_ERR_ARG, "turn must be non-negative");
+    if (rng_method != OCTO_RNG_PHILOX && rng_method != OCTO_RNG_SPLITMIX)
+        return fail(c, OCTO_ERR_ARG, "unknown RNG method code; use RNG_PHILOX or RNG_SPLITMIX");
+    if (beam->n < 0 || beam->n >= (1LL << 40)) return fail(c, OCTO_ERR_ARG, "beam size out of range");
+    if (beam->dtype != 0 && beam->dtype != 1) return fail(c, OCTO_ERR_ARG, "beam dtype must be 0 (float64) or 1 (float32)");
+    if (beam->n > 0 && (!beam->x || !beam->px || !beam->y || !beam->py || !beam->z || !beam->pz))
+        return fail(c, OCTO_ERR_ARG, "beam coordinate pointer is NULL");
+    std::vector<LineOp> ops((size_t)std::max(n_elems, 1));
+    for (int k = 0; k < n_elems; ++k) {
+        std::string msg;
+        const int rc = compile_line_op(elems[k], rng_method, seed, ops[k], msg);
+        if (rc != OCTO_OK) return fail(c, rc, "line element " + std::to_string(k + 1) + ": " + msg);
+    }
+    if (beam->n == 0 || turns == 0 || n_elems == 0) return OCTO_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    try {
+        CK(cudaSetDevice(c->device));
+        const unsigned blocks = (unsigned)((beam->n + 255) / 256);
+        // One launch runs every turn when the line fits one program; a longer line runs turn by turn, its
+        // programs in element order (the same per-particle sequence).
+        const int nprog = (n_elems + kLineOpsPerLaunch - 1) / kLineOpsPerLaunch;
+        const int outer = nprog == 1 ? 1 : turns;
+        for (int t = 0; t < outer; ++t)
+            for (int g = 0; g < nprog; ++g) {
+                LineProgram P;
+                std::memset(&P, 0, sizeof P);
+                P.nops = std::min(kLineOpsPerLaunch, n_elems - g * kLineOpsPerLaunch);
+                P.rng = rng_method;
+                P.turns = nprog == 1 ? turns : 1;
+                P.turn0 = turn + t;
+                for (int k = 0; k < P.nops; ++k) P.op[k] = ops[g * kLineOpsPerLaunch + k];
+                with_real(beam->dtype == 1, [&](auto r) {
+                    using R = decltype(r);
+                    launch_pdl(k_track_line<R>, blocks, 256, 0, st, (R *)beam->x, (R *)beam->px, (R *)beam->y,
+                               (R *)beam->py, (R *)beam->z, (R *)beam->pz, (long long)beam->n, P);
+                });
+            }
         CK(cudaGetLastError());
         return OCTO_OK;
     } catch (CudaFail &e) {

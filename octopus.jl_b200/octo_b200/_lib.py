@@ -25,6 +25,7 @@ EXPORTS = (
     "octo_pair_luminosity_trace", "octo_linear6d", "octo_beam_gaussian", "octo_last_error",
     "octo_normal_quantile", "octo_erfinv", "octo_version", "octo_set_timing", "octo_timing_report",
     "octo_beam_gaussian_noalloc", "octo_pic_collide_batch", "octo_set_timing_phases", "octo_pic_autotune",
+    "octo_track_line",
 )
 
 PHASES = ("slicing", "bounds", "plan", "green", "luminosity", "deposit", "fft", "field", "kick", "unsort", "node")
@@ -34,6 +35,21 @@ class OctoBeam(C.Structure):
     _fields_ = [("n", C.c_int64), ("dtype", C.c_int32), ("reserved", C.c_int32),
                 ("x", C.c_void_p), ("px", C.c_void_p), ("y", C.c_void_p),
                 ("py", C.c_void_p), ("z", C.c_void_p), ("pz", C.c_void_p)]
+
+
+# Line elements (OCTO_ELEM_* kinds of include/octo_b200.h).
+ELEM_LINEAR6D, ELEM_THIN_CRAB_CAVITY, ELEM_LORENTZ_BOOST, ELEM_REV_LORENTZ_BOOST, ELEM_CHROMATICITY_KICK, \
+    ELEM_LUMPED_RAD, ELEM_CRAB_DISPERSION, ELEM_MOMENTUM_DISPERSION, ELEM_XY_COUPLING = range(1, 10)
+RAD_RADIATION, RAD_DAMPING, RAD_DIFFUSION = range(3)
+RNG_PHILOX, RNG_SPLITMIX = 1, 2
+CRAB_MAX_HARMONICS = 8
+LINE_MAX_ELEMENTS = 32
+
+
+class OctoElement(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("nharm", C.c_int32), ("mode", C.c_int32), ("is_damping", C.c_int32),
+                ("is_excitation", C.c_int32), ("reserved", C.c_int32), ("rng_id", C.c_uint64),
+                ("p", C.c_double * 40)]
 
 
 class OctoBeamParams(C.Structure):
@@ -108,6 +124,8 @@ def lib():
     L.octo_green_cache_stats.argtypes = [vp, P(i64), P(i64), P(i64)]
     L.octo_pair_luminosity_trace.restype = i64
     L.octo_pair_luminosity_trace.argtypes = [vp, P(i32), P(i32), P(d), i64]
+    L.octo_track_line.restype = i32
+    L.octo_track_line.argtypes = [vp, P(OctoBeam), P(OctoElement), i32, i64, i32, u64, i32, vp]
     L.octo_linear6d.restype = i32
     L.octo_linear6d.argtypes = [vp, P(OctoBeam), P(d), i32, vp]
     L.octo_beam_gaussian.restype = i32

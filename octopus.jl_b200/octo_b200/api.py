@@ -10,13 +10,14 @@ from __future__ import annotations
 
 import ctypes as C
 import math
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 from typing import Dict, Optional, Tuple
 
 import numpy as np
 import torch
 
 from . import _lib
+from . import line as _line
 from .beam import Beam
 from .solver import ArgumentError, LongitudinalSlicing, PICPoissonSolver
 
@@ -36,8 +37,17 @@ class CollisionError(ArgumentError):
 
 @dataclass
 class TrackingContext:
-    """The subset of TrackingContext the collision reads: the turn (for messages and schedules)."""
+    """TrackingContext (src/track/Track.jl:3-22): the turn (collision messages and schedules; the turn of
+    the counter-RNG draws of line tracking) and the seed and method of the global counter RNG, taken when
+    the context is made.  turn = -1 marks a collide outside a turn loop."""
     turn: int = -1
+    seed: int = field(default_factory=_line.global_rng_seed)
+    rng_method: str = field(default_factory=_line.global_rng_method)
+
+
+def with_turn(ctx: TrackingContext, turn: int) -> TrackingContext:
+    """with_turn (src/track/Track.jl:24-32)."""
+    return TrackingContext(turn=int(turn), seed=ctx.seed, rng_method=ctx.rng_method)
 
 
 class Context:
@@ -265,3 +275,25 @@ class Linear6D:
         if rc != _lib.OCTO_OK:
             raise RuntimeError(_lib.last_error(ctx))
         return beam
+
+
+def track(beam: Beam, elems, turns: int = 1, context: Optional[TrackingContext] = None, stream=None) -> Beam:
+    """track!(rep, elems, turns; context) (src/track/phase6d_track.jl:10-35, 197-212) for a line of zero-length
+    element specs (octo_b200.line), nested tuples expanded as fusedTrack does: one fused device pass applies
+    every element to every particle, `turns` times.  Turn t of the call draws the radiation noise of
+    context turn ``context.turn + t`` for particle i as id i + 1, so chunked runs equal one run bit for bit.
+    The default context is TrackingContext(turn=0) with the global seed and method."""
+    ctx = context if context is not None else TrackingContext(turn=0)
+    if ctx.turn < 0:
+        raise ArgumentError("line tracking needs a context turn >= 0")
+    if int(turns) < 0:
+        raise ArgumentError("turns must be non-negative")
+    arr, n = _line.compile_line(elems)
+    b = beam.to_c()
+    st = (stream or torch.cuda.current_stream(beam.coords.device)).cuda_stream
+    cptr = _scratch_ctx(beam.coords.device.index or 0)
+    rc = _lib.lib().octo_track_line(cptr, C.byref(b), arr, n, int(ctx.turn), int(turns), int(ctx.seed),
+                                    _line.rng_method_code(ctx.rng_method), C.c_void_p(st))
+    if rc != _lib.OCTO_OK:
+        raise ArgumentError(_lib.last_error(cptr))
+    return beam

@@ -1760,4 +1760,224 @@ void oo_linear6d_matrix(const double beta[3], const double alpha[3], const doubl
     }
 }
 
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- line elements
+// Each element restated per particle as the reference evaluates it, constructor constants included.
+namespace {
+
+// splitmix_uint64 (counter_rng.jl:284-291)
+uint64_t splitmix_u64(uint64_t seed, uint64_t turn, uint64_t rng_id, uint64_t particle, uint64_t comp) {
+    uint64_t x = seed;
+    x ^= splitmix64(turn + 0x9e3779b97f4a7c15ULL);
+    x ^= splitmix64(rng_id + 0xbf58476d1ce4e5b9ULL);
+    x ^= splitmix64(particle + 0x94d049bb133111ebULL);
+    x ^= splitmix64(comp + 0xD2B74407B1CE6E93ULL);
+    return splitmix64(x);
+}
+
+// octopus_normal (counter_rng.jl:103-176): method-selected uniform pair, Box-Muller, odd component -> cos.
+double octopus_normal(uint64_t seed, int method, uint64_t turn, uint64_t rng_id, uint64_t particle, uint64_t comp) {
+    const uint64_t pair = (comp + 1) / 2;
+    auto u64 = [&](uint64_t c) {
+        return method == 1 ? counter_u64(seed, turn, rng_id, particle, c) : splitmix_u64(seed, turn, rng_id, particle, c);
+    };
+    const double u1 = uniform_open01(u64(2 * pair - 1));
+    const double u2 = uniform_open01(u64(2 * pair));
+    const double r = std::sqrt(-2.0 * std::log(u1));
+    const double theta = 6.283185307179586476925286766559 * u2;
+    return (comp & 1) ? r * std::cos(theta) : r * std::sin(theta);
+}
+
+typedef std::array<double, 6> Phase;
+
+// CrabDispersion / MomentumDispersion forward (linear_maps.jl:125-132, 213-220) and inverse
+// (chromaticity_kick.jl:151-167).
+Phase zeta_fwd(const double *zt, Phase v) {
+    const double x0 = v[0], px0 = v[1], y0 = v[2], py0 = v[3], z0 = v[4], pz0 = v[5];
+    const double pz1 = pz0 + zt[1] * x0 - zt[0] * px0 + zt[3] * y0 - zt[2] * py0;
+    return {x0 + zt[0] * z0, px0 + zt[1] * z0, y0 + zt[2] * z0, py0 + zt[3] * z0, z0, pz1};
+}
+Phase zeta_inv(const double *zt, Phase v) {
+    const double x0 = v[0], px0 = v[1], y0 = v[2], py0 = v[3], z0 = v[4], pz0 = v[5];
+    const double pz1 = pz0 - zt[1] * x0 + zt[0] * px0 - zt[3] * y0 + zt[2] * py0;
+    return {x0 - zt[0] * z0, px0 - zt[1] * z0, y0 - zt[2] * z0, py0 - zt[3] * z0, z0, pz1};
+}
+Phase eta_fwd(const double *et, Phase v) {
+    const double x0 = v[0], px0 = v[1], y0 = v[2], py0 = v[3], z0 = v[4], pz0 = v[5];
+    const double z1 = z0 - et[1] * x0 + et[0] * px0 - et[3] * y0 + et[2] * py0;
+    return {x0 + et[0] * pz0, px0 + et[1] * pz0, y0 + et[2] * pz0, py0 + et[3] * pz0, z1, pz0};
+}
+Phase eta_inv(const double *et, Phase v) {
+    const double x0 = v[0], px0 = v[1], y0 = v[2], py0 = v[3], z0 = v[4], pz0 = v[5];
+    const double z1 = z0 + et[1] * x0 - et[0] * px0 + et[3] * y0 - et[2] * py0;
+    return {x0 - et[0] * pz0, px0 - et[1] * pz0, y0 - et[2] * pz0, py0 - et[3] * pz0, z1, pz0};
+}
+// XYCoupling (linear_maps.jl:353-372) and its mode-A inverse (chromaticity_kick.jl:179-186).
+Phase xy_fwd(const double *r, int mode, Phase v) {
+    if (mode == 0) return v;
+    const double g = 1.0 / std::sqrt(1 + r[0] * r[3] - r[1] * r[2]);
+    const double x0 = v[0], px0 = v[1], y0 = v[2], py0 = v[3];
+    if (mode == 1)
+        return {g * (x0 + r[3] * y0 - r[1] * py0), g * (px0 - r[2] * y0 + r[0] * py0),
+                g * (-r[0] * x0 - r[1] * px0 + y0), g * (-r[2] * x0 - r[3] * px0 + py0), v[4], v[5]};
+    return {g * (r[3] * x0 - r[1] * px0 + y0), g * (-r[2] * x0 + r[0] * px0 + py0), g * (x0 - r[0] * y0 - r[1] * py0),
+            g * (px0 - r[2] * y0 - r[3] * py0), v[4], v[5]};
+}
+Phase xy_inv_a(const double *r, Phase v) {
+    const double g = 1.0 / std::sqrt(1 + r[0] * r[3] - r[1] * r[2]);
+    const double x0 = v[0], px0 = v[1], y0 = v[2], py0 = v[3];
+    return {g * (x0 - r[3] * y0 + r[1] * py0), g * (px0 + r[2] * y0 - r[0] * py0), g * (r[0] * x0 + r[1] * px0 + y0),
+            g * (r[2] * x0 + r[3] * px0 + py0), v[4], v[5]};
+}
+
+Phase track_element(const oo_element &e, Phase v, uint64_t seed, int method, uint64_t turn, uint64_t particle) {
+    const double *p = e.p;
+    switch (e.kind) {
+        case 1: {  // Linear6D (linear6d.jl:110-121)
+            Phase o;
+            for (int r = 0; r < 6; ++r) {
+                const double *m = p + 6 * r;
+                o[r] = m[0] * v[0] + m[1] * v[1] + m[2] * v[2] + m[3] * v[3] + m[4] * v[4] + m[5] * v[5];
+            }
+            return o;
+        }
+        case 2: {  // ThinCrabCavity (crab_cavity.jl:87-101, 128-144)
+            const double kcc = 2.0 * 3.14159265358979323846 * p[0] / 299792458.0;
+            double dpx = 0.0, dpy = 0.0, dpz = 0.0;
+            for (int i = 1; i <= e.nharm; ++i) {
+                const double ikcc = (double)i * kcc;
+                const double th = ikcc * v[4] + p[17 + i - 1];
+                const double s = std::sin(th), c = std::cos(th);
+                const double sx = p[1 + i - 1], sy = p[9 + i - 1];
+                dpx -= sx * s / ikcc;
+                dpy -= sy * s / ikcc;
+                dpz -= (sx * v[0] + sy * v[2]) * c;
+            }
+            return {v[0], v[1] + dpx, v[2], v[3] + dpy, v[4], v[5] + dpz};
+        }
+        case 3: {  // LorentzBoost (lorentz_boost.jl:128-143, constants :168-174)
+            const double ca = std::cos(p[0]), sa = std::sin(p[0]), ta = sa / ca;
+            const double x0 = v[0], px0 = v[1], y0 = v[2], py0 = v[3], z0 = v[4], pz0 = v[5];
+            const double ps0 = std::sqrt((1.0 + pz0) * (1.0 + pz0) - px0 * px0 - py0 * py0);
+            const double h0 = 1.0 + pz0 - ps0;
+            const double py1 = py0 / ca;
+            const double h1 = h0 / (ca * ca);
+            const double px1 = px0 / ca - h1 * sa;
+            const double pz1 = pz0 - px1 * sa;
+            const double ps1 = 1.0 + pz1 - h1;
+            const double ds = x0 * sa;
+            return {x0 + z0 * ta + px1 / ps1 * ds, px1, y0 + py1 / ps1 * ds, py1, z0 / ca - h1 / ps1 * ds, pz1};
+        }
+        case 4: {  // RevLorentzBoost (lorentz_boost.jl:148-161)
+            const double ca = std::cos(p[0]), sa = std::sin(p[0]);
+            const double x0 = v[0], px0 = v[1], y0 = v[2], py0 = v[3], z0 = v[4], pz0 = v[5];
+            const double ps0 = std::sqrt((1.0 + pz0) * (1.0 + pz0) - px0 * px0 - py0 * py0);
+            const double h0 = 1.0 + pz0 - ps0;
+            double x1 = x0 - z0 * sa;
+            x1 = x1 / (1.0 + (px0 + h0 * sa) * sa / ps0);
+            const double z1 = (z0 + h0 / ps0 * x1 * sa) * ca;
+            const double y1 = y0 - py0 / ps0 * x1 * sa;
+            return {x1, (px0 + h0 * sa) * ca, y1, py0 * ca, z1, pz0 + px0 * sa};
+        }
+        case 5: {  // ChromaticityKick (chromaticity_kick.jl:74-136)
+            const double xix = p[0], xiy = p[1], betx = p[2], bety = p[3], alfx = p[4], alfy = p[5];
+            const double gamx = (1.0 + alfx * alfx) / betx, gamy = (1.0 + alfy * alfy) / bety;
+            const double *zt = p + 6, *et = p + 10, *r = p + 14;
+            v = zeta_inv(zt, v);
+            v = eta_inv(et, v);
+            v = xy_inv_a(r, v);
+            const double x0 = v[0], px0 = v[1], y0 = v[2], py0 = v[3];
+            const double twopi = 6.283185307179586476925286766559005768394338;
+            const double mux = twopi * xix * v[5];
+            const double cx = std::cos(mux), sx = std::sin(mux);
+            v[0] = x0 * (cx + alfx * sx) + px0 * betx * sx;
+            v[1] = -x0 * sx * gamx + px0 * (cx - alfx * sx);
+            const double muy = twopi * xiy * v[5];
+            const double cy = std::cos(muy), sy = std::sin(muy);
+            v[2] = y0 * (cy + alfy * sy) + py0 * bety * sy;
+            v[3] = -y0 * sy * gamy + py0 * (cy - alfy * sy);
+            const double jx = 0.5 * (gamx * x0 * x0 + 2 * alfx * x0 * px0 + betx * px0 * px0);
+            const double jy = 0.5 * (gamy * y0 * y0 + 2 * alfy * y0 * py0 + bety * py0 * py0);
+            v[4] += twopi * (xix * jx + xiy * jy);
+            v = xy_fwd(r, 1, v);
+            v = eta_fwd(et, v);
+            return zeta_fwd(zt, v);
+        }
+        case 6: {  // LumpedRad (radiation.jl:83-131, 162-171, 196-279, 286-299)
+            const bool enabled = p[9] >= 0.0 && p[10] >= 0.0 && p[11] >= 0.0;
+            const bool damp = e.is_damping != 0 && e.mode != 2;
+            const bool exc = e.is_excitation != 0 && enabled && e.mode != 1;
+            if (!damp && !exc) return v;
+            double damping[3], excitation[9];
+            for (int i = 0; i < 3; ++i) {
+                damping[i] = std::exp(-1.0 / p[i]);
+                const double scale = std::sqrt(-std::expm1(-2.0 / p[i]));
+                for (int k = 0; k < 3; ++k) {
+                    const double sigma = p[9 + i];
+                    double val;
+                    if (sigma < 0.0) val = 0.0;
+                    else {
+                        const double amp = sigma * scale, slope = amp / p[3 + i];
+                        val = k == 0 ? amp : k == 1 ? slope : -slope * p[6 + i];
+                    }
+                    excitation[3 * i + k] = val;
+                }
+            }
+            double nrm[6] = {0, 0, 0, 0, 0, 0};
+            if (exc)
+                for (int c = 1; c <= 6; ++c) nrm[c - 1] = octopus_normal(seed, method, turn, e.rng_id, particle, c);
+            const double *zt = p + 12, *et = p + 16, *r = p + 20;
+            v = zeta_inv(zt, v);
+            v = eta_inv(et, v);
+            v = xy_inv_a(r, v);
+            if (damp) {
+                v[0] *= damping[0]; v[1] *= damping[0];
+                v[2] *= damping[1]; v[3] *= damping[1];
+                v[4] *= damping[2]; v[5] *= damping[2];
+            }
+            if (exc) {
+                v[0] += excitation[0] * nrm[0];
+                v[1] += excitation[1] * nrm[1] + excitation[2] * nrm[0];
+                v[2] += excitation[3] * nrm[2];
+                v[3] += excitation[4] * nrm[3] + excitation[5] * nrm[2];
+                v[4] += excitation[6] * nrm[4];
+                v[5] += excitation[7] * nrm[5] + excitation[8] * nrm[4];
+            }
+            v = xy_fwd(r, 1, v);
+            v = eta_fwd(et, v);
+            return zeta_fwd(zt, v);
+        }
+        case 7: return zeta_fwd(p, v);
+        case 8: return eta_fwd(p, v);
+        case 9: return xy_fwd(p, e.mode, v);
+        default: return v;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+double oo_octopus_normal(uint64_t seed, int32_t rng_method, uint64_t turn, uint64_t rng_id, uint64_t particle,
+                         uint64_t component) {
+    return octopus_normal(seed, rng_method, turn, rng_id, particle, component);
+}
+
+// track!(rep, elems, turns, policy, ctx) (src/track/phase6d_track.jl:25-35): turn-major, particle i as id i + 1.
+void oo_track_line(const oo_element *elems, int32_t n_elems, int64_t turn, int32_t turns, uint64_t seed,
+                   int32_t rng_method, double *x, double *px, double *y, double *py, double *z, double *pz,
+                   int64_t n) {
+    for (int32_t t = 0; t < turns; ++t) {
+        const uint64_t tt = (uint64_t)(turn + t);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; ++i) {
+            Phase v = {x[i], px[i], y[i], py[i], z[i], pz[i]};
+            for (int32_t k = 0; k < n_elems; ++k) v = track_element(elems[k], v, seed, rng_method, tt, (uint64_t)(i + 1));
+            x[i] = v[0]; px[i] = v[1]; y[i] = v[2]; py[i] = v[3]; z[i] = v[4]; pz[i] = v[5];
+        }
+    }
+}
+
 }  // extern "C"

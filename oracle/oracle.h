@@ -123,6 +123,22 @@ int64_t oo_dropped(void *ctx);
 /* Per-pair luminosity of the last collide in collision order (i, j 1-based); returns count. */
 int64_t oo_pair_trace(void *ctx, int32_t *pi, int32_t *pj, double *lum, int64_t cap);
 const char *oo_last_error(void *ctx);
+/* Line elements (the layout of octo_element in the product header; kinds 1..9: Linear6D, thin crab
+   cavity, Lorentz boost, reverse boost, chromaticity kick, lumped radiation, crab dispersion, momentum
+   dispersion, xy coupling).  oo_track_line applies elems to each particle `turns` times, turn t drawing
+   the counter-RNG noise of turn `turn + t` (rng_method 1 Philox, 2 SplitMix), particle i as id i + 1
+   (src/track/phase6d_track.jl:25-35 with fusedTrack, src/track/fused_track.jl:53-77). */
+typedef struct {
+    int32_t kind, nharm, mode, is_damping, is_excitation, reserved;
+    uint64_t rng_id;
+    double p[40];
+} oo_element;
+void oo_track_line(const oo_element *elems, int32_t n_elems, int64_t turn, int32_t turns, uint64_t seed,
+                   int32_t rng_method, double *x, double *px, double *y, double *py, double *z, double *pz,
+                   int64_t n);
+/* octopus_normal (counter_rng.jl:168-176) for either method. */
+double oo_octopus_normal(uint64_t seed, int32_t rng_method, uint64_t turn, uint64_t rng_id, uint64_t particle,
+                         uint64_t component);
 /* Linear 6D one-turn map (linear6d.jl:110-121) with a row-major 6x6 matrix. */
 void oo_linear6d(const double m[36], double *x, double *px, double *y, double *py, double *z, double *pz, int64_t n);
 void oo_linear6d_matrix(const double beta[3], const double alpha[3], const double tune[3], double m[36]);

@@ -25,6 +25,13 @@ ME0 = EMASS_EV
 PMASS_EV = 938.27208943e6
 
 
+class OOElement(C.Structure):
+    """oo_element: the layout of the product's octo_element."""
+    _fields_ = [("kind", C.c_int32), ("nharm", C.c_int32), ("mode", C.c_int32), ("is_damping", C.c_int32),
+                ("is_excitation", C.c_int32), ("reserved", C.c_int32), ("rng_id", C.c_uint64),
+                ("p", C.c_double * 40)]
+
+
 def build() -> str:
     src = os.path.join(HERE, "octo_oracle.cpp")
     if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
@@ -120,6 +127,10 @@ def lib():
         L.oo_last_error.argtypes = [vp]
         L.oo_linear6d.argtypes = [P(d)] + [P(d)] * 6 + [i64]
         L.oo_linear6d_matrix.argtypes = [P(d), P(d), P(d), P(d)]
+        L.oo_track_line.argtypes = [P(OOElement), i32, i64, i32, C.c_uint64, i32] + [P(d)] * 6 + [i64]
+        L.oo_track_line.restype = None
+        L.oo_octopus_normal.argtypes = [C.c_uint64, i32, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]
+        L.oo_octopus_normal.restype = d
     return _lib
 
 
@@ -393,3 +404,24 @@ def luminosity(options: OracleOptions, x1, y1, x2, y2, klum):
                               float(klum), _dp(q1), _dp(q2))
     f = lambda q: q.reshape(ny + 1, nx + 1).T.copy()
     return lum, f(q1), f(q2)
+
+
+def as_oo_elements(elems):
+    """Copies C element structs of the same layout (the product's octo_element) into oo_element."""
+    arr = (OOElement * max(len(elems), 1))()
+    for k, e in enumerate(elems):
+        C.memmove(C.byref(arr[k]), C.byref(e), C.sizeof(OOElement))
+    return arr
+
+
+def track_line(elems, beam, turn=0, turns=1, seed=0, rng_method=1):
+    """oo_track_line on a (6, n) float64 array (copied); elems: octo_element / oo_element structs."""
+    b = np.ascontiguousarray(beam, dtype=np.float64).copy()
+    arr = as_oo_elements(list(elems))
+    lib().oo_track_line(arr, len(elems), int(turn), int(turns), C.c_uint64(seed), int(rng_method),
+                        *[_dp(b[k]) for k in range(6)], b.shape[1])
+    return b
+
+
+def octopus_normal(seed, rng_method, turn, rng_id, particle, component):
+    return lib().oo_octopus_normal(seed, rng_method, turn, rng_id, particle, component)
