@@ -209,4 +209,83 @@ end
 
 Octopus._pic_compute_luminosity(solver::B200Solver, ctx) = Octopus._pic_compute_luminosity(solver.pic, ctx)
 
+# ---------------------------------------------------------------- line tracking between collisions
+# include/octo_b200.h: octo_element
+struct OctoElement
+    kind::Int32; nharm::Int32; mode::Int32; is_damping::Int32; is_excitation::Int32; reserved::Int32
+    rng_id::UInt64
+    p::NTuple{40,Float64}
+end
+
+function _elem(kind, p::Vector{Float64}; nharm=0, mode=0, is_damping=0, is_excitation=0, rng_id=0)
+    q = zeros(40); q[1:length(p)] .= p
+    return OctoElement(Int32(kind), Int32(nharm), Int32(mode), Int32(is_damping), Int32(is_excitation), Int32(0),
+                       UInt64(rng_id), Tuple(q))
+end
+_f(v) = Float64[Float64(x) for x in v]
+_par(spec, k) = Octopus.param(spec, k)
+
+# One element spec -> octo_element (the OCTO_ELEM_* layouts of include/octo_b200.h).
+_octo_element(s::Octopus.ElementSpec{:linear6d}) = _elem(1, _f(Octopus.compile_runtime(s).matrix))
+function _octo_element(s::Octopus.ElementSpec{:thin_crab_cavity})
+    N = _par(s, :N); p = zeros(25); p[1] = Float64(_par(s, :frequency))
+    for h in 1:N
+        p[1 + h] = _par(s, :strengthX)[h]; p[9 + h] = _par(s, :strengthY)[h]; p[17 + h] = _par(s, :phase)[h]
+    end
+    return _elem(2, p; nharm=N)
+end
+_octo_element(s::Octopus.ElementSpec{:lorentz_boost}) = _elem(3, [Float64(_par(s, :angle))])
+_octo_element(s::Octopus.ElementSpec{:rev_lorentz_boost}) = _elem(4, [Float64(_par(s, :angle))])
+_octo_element(s::Octopus.ElementSpec{:chromaticity_kick}) =
+    _elem(5, vcat(_f(_par(s, :xi)), _f(_par(s, :beta))[1:2], _f(_par(s, :alpha))[1:2],
+                  _f(_par(s, :zeta)), _f(_par(s, :eta)), _f(_par(s, :R))))
+function _octo_element(s::Octopus.ElementSpec{:lumped_radiation})
+    m = Octopus.tracking_method(s)
+    mode = m isa Octopus.Damping6DMap ? 1 : m isa Octopus.Diffusion6DMap ? 2 : 0
+    p = vcat(_f(_par(s, :damping_turns)), _f(_par(s, :beta)), _f(_par(s, :alpha)), _f(_par(s, :sigma)),
+             _f(_par(s, :zeta)), _f(_par(s, :eta)), _f(_par(s, :R)))
+    return _elem(6, p; mode=mode, is_damping=Int(Octopus.getparam(s, :is_damping, true)),
+                 is_excitation=Int(Octopus.getparam(s, :is_excitation, true)), rng_id=_par(s, :rng_id))
+end
+_octo_element(s::Octopus.ElementSpec{:crab_dispersion}) = _elem(7, [Float64(_par(s, k)) for k in (:zeta1, :zeta2, :zeta3, :zeta4)])
+_octo_element(s::Octopus.ElementSpec{:momentum_dispersion}) = _elem(8, [Float64(_par(s, k)) for k in (:eta1, :eta2, :eta3, :eta4)])
+_octo_element(s::Octopus.ElementSpec{:xy_coupling}) =
+    _elem(9, [Float64(_par(s, k)) for k in (:r1, :r2, :r3, :r4)]; mode=Int(Octopus.getparam(s, :mode, Octopus.XY_MODEA)))
+
+_flatten(e) = (e,)
+_flatten(t::Tuple) = Tuple(Iterators.flatten(map(_flatten, t)))
+
+const _SCRATCH = Ref{Union{Nothing,Context}}(nothing)
+function _scratch_context()
+    if _SCRATCH[] === nothing
+        _SCRATCH[] = Context(PICPoissonSolver(grid=(8, 8), slicing=LongitudinalSlicing(nslices=1, method=:normal_quantile)))
+    end
+    return _SCRATCH[]::Context
+end
+
+_octo_rep(r) = OctoBeam(Int64(length(r.x)), Int32(eltype(r.x) === Float32 ? 1 : 0), Int32(0),
+    pointer(r.x), pointer(r.px), pointer(r.y), pointer(r.py), pointer(r.z), pointer(r.pz))
+
+"""
+    track_line!(rep, specs, turns=1; context=TrackingContext())
+
+track!(rep, elems, turns; context) (src/track/phase6d_track.jl:10-35) on libocto_b200 for a line of the
+zero-length elements around the collision (Linear6D, thin crab cavity, Lorentz boost pair, chromaticity kick,
+lumped radiation, crab/momentum dispersion, xy coupling), given as their `ElementSpec`s, nested tuples
+expanded as fusedTrack does: one fused device pass on the task's stream.  The radiation draws use
+`context.seed`, `context.rng_method` and turn `context.turn + t - 1` for particle index i, as the
+reference's fused CUDA kernel does, so results match it to the ulps of the device's libm.
+"""
+function track_line!(rep, specs::Tuple, turns::Integer=1; context::TrackingContext=TrackingContext())
+    elems = OctoElement[_octo_element(s) for s in _flatten(specs)]
+    c = _scratch_context()
+    b = Ref(_octo_rep(rep))
+    rc = GC.@preserve rep elems ccall((:octo_track_line, LIB), Int32,
+               (Ptr{Cvoid}, Ref{OctoBeam}, Ptr{OctoElement}, Int32, Int64, Int32, UInt64, Int32, Ptr{Cvoid}),
+               c.ptr, b, elems, Int32(length(elems)), Int64(context.turn), Int32(turns), UInt64(context.seed),
+               Int32(context.rng_method), CUDA.stream().handle)
+    rc == 0 || throw(ArgumentError(_last_error(c)))
+    return rep
+end
+
 end # module
