@@ -199,6 +199,17 @@ typedef struct {
 int32_t octo_track_line(octo_ctx *ctx, octo_beam *beam, const octo_element *elems, int32_t n_elems, int64_t turn,
                         int32_t turns, uint64_t seed, int32_t rng_method, void *stream);
 
+/* One moment row of a beam as MomentObserver records it (src/tasks/BeamObservers.jl:630-720, 1000-1060,
+ * 1254-1271): row[0] = turn; row[1 + k] = moment k of powers[6k .. 6k+5] (exponents of x, px, y, py, z, pz),
+ * the mean of its coordinate for order 1, else the central moment mean(prod (c_d - <c_d>)^p_d).  With
+ * mask_lost != 0 (allow_lost_particles) only particles whose six coordinates are finite count, and a beam
+ * without such particles gets NaN moments; otherwise a non-finite particle makes the row NaN.  `row` is a
+ * DEVICE pointer (a slot of the caller's record buffer): the call never synchronises the host.  Up to
+ * OCTO_MOMENTS_MAX moments, each order-1 moment at most once, exponents 0..32. */
+#define OCTO_MOMENTS_MAX 256
+int32_t octo_beam_moments(octo_ctx *ctx, const octo_beam *beam, const int32_t *powers, int32_t n_moments,
+                          int32_t mask_lost, int64_t turn, double *row, void *stream);
+
 /* Seeded Gaussian beam on the device as Beam(n, backend, Float64; beta, alpha, sigma, cutoff, rng_id)
  * builds it (Beam.jl:475-515; counter RNG counter_rng.jl:154-233). */
 int32_t octo_beam_gaussian(octo_ctx *ctx, octo_beam *beam, uint64_t seed, uint64_t rng_id, const double beta[3],

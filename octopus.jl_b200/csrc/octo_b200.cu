@@ -19,6 +19,7 @@
 
 #include "../../include/octo_b200.h"
 #include "k_line.cuh"
+#include "k_moments.cuh"
 #include "k_misc.cuh"
 #include "k_pic.cuh"
 #include "k_slicing.cuh"
@@ -228,6 +229,7 @@ struct octo_ctx {
     DevBuf<double> lum_parts, lum_partial, node_ref, stats, partial;
     DevBuf<HybridTask> hyb;            // Gaussian-subtracted hybrid state per task
     DevBuf<double> hmom, hprof, hsum;  // its moment partials, node profiles and profile sums
+    DevBuf<double> mom_partial, mom_means;  // beam moment rows: block partials and the means
     DevBuf<unsigned long long> qtot;   // per-plane total fixed-point charge
     DevBuf<double *> soa_ptrs;
     PinBuf<char> stage;
@@ -1828,6 +1830,92 @@ int32_t octo_track_line(octo_ctx *c, octo_beam *beam, const octo_element *elems,
                                (R *)beam->py, (R *)beam->z, (R *)beam->pz, (long long)beam->n, P);
                 });
             }
+        CK(cudaGetLastError());
+        return OCTO_OK;
+    } catch (CudaFail &e) {
+        return fail(c, OCTO_ERR_CUDA, e.msg);
+    }
+}
+
+int32_t octo_beam_moments(octo_ctx *c, const octo_beam *beam, const int32_t *powers, int32_t n_moments,
+                          int32_t mask_lost, int64_t turn, double *row, void *stream) {
+    if (!c || !beam || !row || (n_moments > 0 && !powers)) return OCTO_ERR_ARG;
+    if (n_moments < 0 || n_moments > kMomentsMax)
+        return fail(c, OCTO_ERR_ARG, "a moment row holds 0.." + std::to_string(kMomentsMax) + " moments");
+    if (beam->n < 0 || beam->n >= (1LL << 40)) return fail(c, OCTO_ERR_ARG, "beam size out of range");
+    if (beam->dtype != 0 && beam->dtype != 1) return fail(c, OCTO_ERR_ARG, "beam dtype must be 0 (float64) or 1 (float32)");
+    if (beam->n > 0 && (!beam->x || !beam->px || !beam->y || !beam->py || !beam->z || !beam->pz))
+        return fail(c, OCTO_ERR_ARG, "beam coordinate pointer is NULL");
+    MomentHead head{};
+    MomentPairRows pairs{};
+    std::vector<int> general;  // rows of order >= 3
+    unsigned mean_seen = 0, pair_seen = 0;
+    for (int k = 0; k < n_moments; ++k) {
+        int order = 0, coord = -1, second = -1;
+        for (int d = 0; d < 6; ++d) {
+            const int p = powers[6 * k + d];
+            if (p < 0 || p > 32) return fail(c, OCTO_ERR_ARG, "moment powers must be integers in 0..32");
+            order += p;
+            if (p && coord < 0) coord = d;
+            if (p == 2) second = d;
+            else if (p == 1 && coord != d) second = d;
+        }
+        if (order == 0) return fail(c, OCTO_ERR_ARG, "a moment needs a positive order");
+        if (order == 1) {
+            if (mean_seen & (1u << coord)) return fail(c, OCTO_ERR_ARG, "a moment row holds each mean once");
+            mean_seen |= 1u << coord;
+            head.slot[head.n] = (unsigned char)k;
+            head.coord[head.n] = (unsigned char)coord;
+            ++head.n;
+        } else if (order == 2) {
+            // (coord, second) with coord <= second; pair index over the upper triangle, row-major
+            const int a = coord, b = second;
+            const int pidx = a * 6 - a * (a - 1) / 2 + (b - a);
+            if (pair_seen & (1u << pidx)) return fail(c, OCTO_ERR_ARG, "a moment row holds each second moment once");
+            pair_seen |= 1u << pidx;
+            pairs.pair[pairs.n] = (unsigned char)pidx;
+            pairs.slot[pairs.n] = (unsigned char)k;
+            ++pairs.n;
+        } else {
+            general.push_back(k);
+        }
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    try {
+        CK(cudaSetDevice(c->device));
+        c->mom_partial.ensure((size_t)kMomentBlocks * kMomentPairs);
+        c->mom_means.ensure(16);
+        const long long n = beam->n;
+        const int mask = mask_lost != 0;
+        with_real(beam->dtype == 1, [&](auto r) {
+            using R = decltype(r);
+            R *b[6] = {(R *)beam->x, (R *)beam->px, (R *)beam->y, (R *)beam->py, (R *)beam->z, (R *)beam->pz};
+            const double *means = c->mom_means.p;
+            launch_pdl(k_moment_sums<R>, kMomentBlocks, kMomentThreads, 0, st, b[0], b[1], b[2], b[3], b[4], b[5], n,
+                       mask, c->mom_partial.p);
+            launch_pdl(k_moment_means, 7, kMomentThreads, 0, st, (const double *)c->mom_partial.p, (int)kMomentBlocks,
+                       c->mom_means.p);
+            launch_pdl(k_moment_divide, 1, 32, 0, st, c->mom_means.p);
+            launch_pdl(k_moment_row_head, 1, 32, 0, st, means, (double)turn, head, row);
+            if (pairs.n) {
+                launch_pdl(k_moment_pairs<R>, kMomentBlocks, kMomentThreads, 0, st, b[0], b[1], b[2], b[3], b[4],
+                           b[5], n, mask, means, c->mom_partial.p);
+                launch_pdl(k_moment_fold_pairs, pairs.n, kMomentThreads, 0, st, (const double *)c->mom_partial.p,
+                           (int)kMomentBlocks, means, pairs, row);
+            }
+            for (size_t g0 = 0; g0 < general.size(); g0 += kMomentChunk) {
+                MomentPowers P{};
+                P.n = (int)std::min<size_t>(kMomentChunk, general.size() - g0);
+                for (int k = 0; k < P.n; ++k) {
+                    for (int d = 0; d < 6; ++d) P.p[k][d] = (unsigned char)powers[6 * general[g0 + k] + d];
+                    P.slot[k] = (unsigned char)general[g0 + k];
+                }
+                launch_pdl(k_moment_general<R>, kMomentBlocks, kMomentThreads, 0, st, b[0], b[1], b[2], b[3], b[4],
+                           b[5], n, mask, means, P, c->mom_partial.p);
+                launch_pdl(k_moment_fold, P.n, kMomentThreads, 0, st, (const double *)c->mom_partial.p,
+                           (int)kMomentBlocks, means, P, row);
+            }
+        });
         CK(cudaGetLastError());
         return OCTO_OK;
     } catch (CudaFail &e) {

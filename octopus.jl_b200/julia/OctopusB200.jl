@@ -288,4 +288,26 @@ function track_line!(rep, specs::Tuple, turns::Integer=1; context::TrackingConte
     return rep
 end
 
+# ---------------------------------------------------------------- moment rows on the device
+"""
+    moment_row!(row, rep, moments; turn, mask_lost=Octopus.allow_lost_particles())
+
+One MomentObserver row (src/tasks/BeamObservers.jl:1013-1040, 1254-1271) of `rep` computed on the device into
+`row::CuVector{Float64}` of length `1 + length(moments)` (typically a row view of the observer's device record
+matrix): `row[1] = turn`, then each `Moment`'s mean (order 1) or central moment.  No host synchronisation; the
+caller copies the record matrix to the host when it flushes.
+"""
+function moment_row!(row::CuArray{Float64}, rep, moments; turn::Integer,
+                     mask_lost::Bool=Octopus.allow_lost_particles())
+    powers = Int32[p for m in moments for p in m.powers]
+    c = _scratch_context()
+    b = Ref(_octo_rep(rep))
+    rc = GC.@preserve rep row powers ccall((:octo_beam_moments, LIB), Int32,
+               (Ptr{Cvoid}, Ref{OctoBeam}, Ptr{Int32}, Int32, Int32, Int64, CuPtr{Float64}, Ptr{Cvoid}),
+               c.ptr, b, powers, Int32(length(moments)), Int32(mask_lost), Int64(turn), pointer(row),
+               CUDA.stream().handle)
+    rc == 0 || throw(ArgumentError(_last_error(c)))
+    return row
+end
+
 end # module

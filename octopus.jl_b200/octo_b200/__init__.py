@@ -12,6 +12,7 @@ from .line import (ChromaticityKickSpec, CrabDispersionSpec, Linear6DSpec, Loren
                    LumpedRadSpec, MomentumDispersionSpec, RevLorentzBoostSpec, ThinCrabCavitySpec,
                    XYCouplingSpec, claim_rng_id, global_rng_method, global_rng_seed, next_rng_id,
                    reset_rng_id_counter, set_global_rng)
+from .observers import MomentObserver, moment, moment_name, selected_moments  # noqa: F401
 from .beam import EMASS_EV, ME0, PMASS_EV, RE, Beam, BeamParams  # noqa: F401
 from .solver import ArgumentError, GaussianPICPoissonSolver, LongitudinalSlicing, PICPoissonSolver  # noqa: F401
 
@@ -21,4 +22,4 @@ __all__ = ["PICPoissonSolver", "GaussianPICPoissonSolver", "LongitudinalSlicing"
            "ThinCrabCavitySpec", "LorentzBoostSpec", "RevLorentzBoostSpec", "ChromaticityKickSpec",
            "LumpedRadSpec", "CrabDispersionSpec", "MomentumDispersionSpec", "XYCouplingSpec",
            "set_global_rng", "global_rng_seed", "global_rng_method", "next_rng_id", "claim_rng_id",
-           "reset_rng_id_counter"]
+           "reset_rng_id_counter", "MomentObserver", "moment", "moment_name", "selected_moments"]

@@ -25,7 +25,7 @@ EXPORTS = (
     "octo_pair_luminosity_trace", "octo_linear6d", "octo_beam_gaussian", "octo_last_error",
     "octo_normal_quantile", "octo_erfinv", "octo_version", "octo_set_timing", "octo_timing_report",
     "octo_beam_gaussian_noalloc", "octo_pic_collide_batch", "octo_set_timing_phases", "octo_pic_autotune",
-    "octo_track_line",
+    "octo_track_line", "octo_beam_moments",
 )
 
 PHASES = ("slicing", "bounds", "plan", "green", "luminosity", "deposit", "fft", "field", "kick", "unsort", "node")
@@ -43,6 +43,7 @@ ELEM_LINEAR6D, ELEM_THIN_CRAB_CAVITY, ELEM_LORENTZ_BOOST, ELEM_REV_LORENTZ_BOOST
 RAD_RADIATION, RAD_DAMPING, RAD_DIFFUSION = range(3)
 RNG_PHILOX, RNG_SPLITMIX = 1, 2
 CRAB_MAX_HARMONICS = 8
+MOMENTS_MAX = 256
 LINE_MAX_ELEMENTS = 32
 
 
@@ -124,6 +125,8 @@ def lib():
     L.octo_green_cache_stats.argtypes = [vp, P(i64), P(i64), P(i64)]
     L.octo_pair_luminosity_trace.restype = i64
     L.octo_pair_luminosity_trace.argtypes = [vp, P(i32), P(i32), P(d), i64]
+    L.octo_beam_moments.restype = i32
+    L.octo_beam_moments.argtypes = [vp, P(OctoBeam), P(i32), i32, i32, i64, vp, vp]
     L.octo_track_line.restype = i32
     L.octo_track_line.argtypes = [vp, P(OctoBeam), P(OctoElement), i32, i64, i32, u64, i32, vp]
     L.octo_linear6d.restype = i32

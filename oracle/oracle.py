@@ -6,6 +6,7 @@ this module, as the checker.  The product library never imports it.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 from dataclasses import dataclass, field
@@ -425,3 +426,40 @@ def track_line(elems, beam, turn=0, turns=1, seed=0, rng_method=1):
 
 def octopus_normal(seed, rng_method, turn, rng_id, particle, component):
     return lib().oo_octopus_normal(seed, rng_method, turn, rng_id, particle, component)
+
+
+def moment_row(beam, moments, turn, mask_lost=False):
+    """_moment_observer_row (src/tasks/BeamObservers.jl:1013-1040, 1254-1271) on a (6, n) float64 array:
+    [turn, moments...]; order 1 the mean of its coordinate, higher orders the central moment with term
+    1.0 * prod_d (c_d - mean_d)^p_d, summed in particle order.  mask_lost: only particles whose six
+    coordinates are finite count; a beam without them gives NaN moments."""
+    b = np.asarray(beam, dtype=np.float64)
+    if mask_lost:
+        b = b[:, np.all(np.isfinite(b), axis=0)]
+    n = b.shape[1]
+    row = [float(turn)]
+    if n == 0:
+        return np.array(row + [np.nan] * len(moments))
+    means = [_seq_sum(b[d]) / n for d in range(6)]
+    for m in moments:
+        if sum(m) == 1:
+            row.append(means[m.index(1)])
+            continue
+        term = np.ones(n)
+        for d in range(6):
+            if m[d]:
+                dv = b[d] - means[d]
+                t = dv.copy()
+                for _ in range(1, m[d]):
+                    t = t * dv
+                term = term * t
+        row.append(_seq_sum(term) / n)
+    return np.array(row)
+
+
+def _seq_sum(v):
+    """Sequential left-to-right sum (the reference's CPU loop)."""
+    s = 0.0
+    for a in np.asarray(v, dtype=np.float64).tolist():
+        s += a
+    return s
