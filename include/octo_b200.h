@@ -91,8 +91,19 @@ typedef struct {
     int32_t gaussian;
     double margin_sigma;               /* hybrid: Gaussian containment half-width in sigmas (default 5) */
     int32_t neutralize;                /* hybrid: rescale the subtracted Gaussian to the deposited charge */
-    int32_t reserved[3];
+    /* GaussianPoissonSolver, the soft-Gaussian strong-strong solver (src/tasks/strongstrong/gaussian.jl,
+     * options interface.jl:949-1020): solver = OCTO_SOLVER_SOFT_GAUSSIAN runs it instead of the PIC solve
+     * (the grid, deposit, Green and interaction-grid fields are then unused; kbb1/kbb2/lum_scale overrides,
+     * the slicings and longitudinal_kick keep their meaning).  FP64 beams only. */
+    int32_t solver;                    /* OCTO_SOLVER_PIC / OCTO_SOLVER_SOFT_GAUSSIAN */
+    int32_t gaussian_when_luminosity;  /* 1 or 2: the beam whose slice is the Gaussian the luminosity samples */
+    int32_t ignore_centroid1, ignore_centroid2;
+    int32_t virtual_drift;             /* 0 = :hirata (the one built; :chromatic / :exact: OCTO_ERR_UNSUPPORTED) */
+    int32_t include_sigma_xy;          /* coupled slice covariance: not built (OCTO_ERR_UNSUPPORTED) */
+    double min_sigma;                  /* transverse RMS floor, finite and >= 0 */
 } octo_pic_options;
+#define OCTO_SOLVER_PIC 0
+#define OCTO_SOLVER_SOFT_GAUSSIAN 1
 
 /* What a collide reports besides the luminosity. */
 typedef struct {

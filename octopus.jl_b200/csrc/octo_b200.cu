@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/octo_b200.h"
+#include "k_gauss.cuh"
 #include "k_line.cuh"
 #include "k_moments.cuh"
 #include "k_misc.cuh"
@@ -230,6 +231,13 @@ struct octo_ctx {
     DevBuf<HybridTask> hyb;            // Gaussian-subtracted hybrid state per task
     DevBuf<double> hmom, hprof, hsum;  // its moment partials, node profiles and profile sums
     DevBuf<double> mom_partial, mom_means;  // beam moment rows: block partials and the means
+    // soft-Gaussian solver: slices, their moments, kick tasks, block maps, partial sums
+    DevBuf<GSlice> g_slices;
+    DevBuf<GMoments> g_mom;
+    DevBuf<GTask> g_tasks;
+    DevBuf<int2> g_bmap;
+    DevBuf<int> g_index;
+    DevBuf<double> g_partial, g_lum_partial;
     DevBuf<unsigned long long> qtot;   // per-plane total fixed-point charge
     DevBuf<double *> soa_ptrs;
     PinBuf<char> stage;
@@ -363,6 +371,29 @@ int validate_options(const octo_pic_options &o, std::string &msg) {
     if (o.precision != 0 && o.precision != 1) {
         msg = "precision must be 0 (FP64 plain form) or 1 (FP32 precision form)";
         return OCTO_ERR_ARG;
+    }
+    if (o.solver != OCTO_SOLVER_PIC && o.solver != OCTO_SOLVER_SOFT_GAUSSIAN) {
+        msg = "solver must be OCTO_SOLVER_PIC or OCTO_SOLVER_SOFT_GAUSSIAN";
+        return OCTO_ERR_ARG;
+    }
+    if (o.solver == OCTO_SOLVER_SOFT_GAUSSIAN) {  // GaussianPoissonSolver{T} (interface.jl:976-1000)
+        if (!(std::isfinite(o.min_sigma) && o.min_sigma >= 0.0)) { msg = "min_sigma must be finite and nonnegative"; return OCTO_ERR_ARG; }
+        if (o.gaussian_when_luminosity != 1 && o.gaussian_when_luminosity != 2) {
+            msg = "gaussian_when_luminosity must be 1 or 2";
+            return OCTO_ERR_ARG;
+        }
+        if (o.virtual_drift != 0) {
+            msg = "the soft-Gaussian solver on this backend implements virtual_drift = :hirata only";
+            return OCTO_ERR_UNSUPPORTED;
+        }
+        if (o.include_sigma_xy) {
+            msg = "include_sigma_xy = true (coupled slice covariance) is not implemented by this backend";
+            return OCTO_ERR_UNSUPPORTED;
+        }
+        if (o.precision != 0 || o.gaussian) {
+            msg = "the soft-Gaussian solver runs on float64 beams, without the PIC hybrid";
+            return OCTO_ERR_UNSUPPORTED;
+        }
     }
     return OCTO_OK;
 }
@@ -728,6 +759,7 @@ struct CollideJob {
     size_t rsz = sizeof(double);
     long long n1 = 0, n2 = 0;
     double kbb1 = 0, kbb2 = 0, klum = 0;
+    double kbb1p = 0, kbb2p = 0;  // per beam, before the division by the other beam's macroparticles
     std::vector<OrderEntry> order;
     std::vector<std::vector<OrderEntry>> batches;
     std::vector<char> ran;
@@ -735,6 +767,8 @@ struct CollideJob {
     int ntasks = 0, npairs_total = 0;
     void begin();
     void run();
+    void run_gaussian(const SliceInfo &S1, const SliceInfo &S2);
+    void write_back();
     double finish();
 };
 
@@ -759,6 +793,8 @@ void CollideJob::begin() {
     const double kbb2p = o.has_kbb2 ? o.kbb2 : p1->charge * p2->charge * p2->r0 * p1->npart * p2->mc2 / p2->E0;
     kbb1 = kbb1p / (double)n2;
     kbb2 = kbb2p / (double)n1;
+    this->kbb1p = kbb1p;
+    this->kbb2p = kbb2p;
     klum = o.has_lum_scale ? o.lum_scale : p1->npart * p2->npart / (double)(n1 * n2);
 
     // ---- slicing (one readback of the slice tables, into pinned memory so the copy is asynchronous)
@@ -786,6 +822,11 @@ void CollideJob::run() {
         }
     }
     const SliceInfo S1 = c->h_slices.p[0], S2 = c->h_slices.p[1];
+    if (o.solver == OCTO_SOLVER_SOFT_GAUSSIAN) {
+        run_gaussian(S1, S2);
+        write_back();
+        return;
+    }
     const int ns1 = c->ns[0], ns2 = c->ns[1];
     const int nx = o.nx, ny = o.ny, NX = 2 * nx, NY = 2 * ny;
     const int gx = rf_rows(nx), gy = rf_cols(ny);
@@ -1213,7 +1254,11 @@ void CollideJob::run() {
         launches += 5;
     }
     CK(cudaGetLastError());
+    write_back();
+}
 
+// Slice-sorted coordinates back to caller order, and the copies of the pair luminosities and the status.
+void CollideJob::write_back() {
     // ---- back to caller order
     {
         PhaseScope ps(c, OCTO_PHASE_UNSORT, st, 1, (double)(n1 + n2) * 10 * rsz);
@@ -1238,6 +1283,158 @@ void CollideJob::run() {
     c->h_status.ensure(1);
     CK(cudaMemcpyAsync(c->h_lum.p, c->lum_parts.p, sizeof(double) * npairs_total, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(c->h_status.p, c->status.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+}
+
+// The soft-Gaussian solver (gaussian.jl:7-57): every slice pair in collision order -- all pairs, empty slices
+// included, as the reference runs them -- one wavefront of conflict-free pairs at a time.  Task 2k kicks the
+// beam-2 slice of pair k with the Gaussian of its beam-1 slice (the reference's lum1 direction), task 2k + 1
+// the beam-1 slice with the Gaussian of the beam-2 slice (lum2).
+void CollideJob::run_gaussian(const SliceInfo &S1, const SliceInfo &S2) {
+    const octo_pic_options &o = c->opt;
+    const int ns1 = c->ns[0], ns2 = c->ns[1];
+    // luminosity scales (slicing.jl:93-102)
+    const double klum1 = o.has_lum_scale ? o.lum_scale : p1->npart * p2->npart / (double)n1;
+    const double klum2 = o.has_lum_scale ? o.lum_scale : p1->npart * p2->npart / (double)n2;
+    const bool sample_beam1 = o.gaussian_when_luminosity == 1;
+    order = collision_order(S1.center, ns1, S2.center, ns2);
+    batches = pair_batches(order, ns1, ns2);
+    std::vector<int> pos_of((size_t)ns1 * ns2);
+    for (size_t p = 0; p < order.size(); ++p) pos_of[(size_t)(order[p].i - 1) * ns2 + (order[p].j - 1)] = (int)p;
+    ran.assign(order.size(), 1);
+    npairs_total = (int)order.size();
+
+    std::vector<GSlice> gs;
+    std::vector<GTask> gt;
+    std::vector<int2> smap, kmap;             // sums blocks, kick blocks
+    std::vector<int> sfirst, scount;          // per slice: its sums blocks
+    std::vector<int> ltask, lfirst, lcount;   // per sampling task: its kick blocks
+    struct Front { int s0, ns, sb0, nsb, t0, nt, kb0, nkb, l0, nl; };
+    std::vector<Front> fronts;
+    tasks.clear();
+    for (size_t f = 0; f < batches.size(); ++f) {
+        Front F{(int)gs.size(), 0, (int)smap.size(), 0, (int)gt.size(), 0, (int)kmap.size(), 0, (int)ltask.size(), 0};
+        for (const OrderEntry &pr : batches[f]) {
+            const int i = pr.i, j = pr.j, p = pos_of[(size_t)(i - 1) * ns2 + (j - 1)];
+            const int t0 = (int)gt.size();
+            // the two slices (moments 2p' and 2p' + 1 of this front: beam 1 slice i, beam 2 slice j)
+            for (int b = 0; b < 2; ++b) {
+                const SliceInfo &SI = b == 0 ? S1 : S2;
+                const int sl = b == 0 ? i - 1 : j - 1;
+                GSlice G{SI.start[sl], SI.count[sl], b, t0 + b};
+                sfirst.push_back((int)smap.size());
+                for (long long off = 0; off < G.n; off += kGaussChunk) smap.push_back(make_int2((int)gs.size(), (int)off));
+                scount.push_back((int)smap.size() - sfirst.back());
+                gs.push_back(G);
+            }
+            const int m1 = (int)gs.size() - 2, m2 = (int)gs.size() - 1;
+            for (int dir = 1; dir <= 2; ++dir) {
+                GTask T{};
+                const bool fld2 = dir == 1;  // direction 1: beam-1 source kicks the beam-2 slice
+                const SliceInfo &SF = fld2 ? S2 : S1, &SS = fld2 ? S1 : S2;
+                const int sf = fld2 ? j - 1 : i - 1, ss = fld2 ? i - 1 : j - 1;
+                T.fld_start = SF.start[sf];
+                T.fld_n = SF.count[sf];
+                T.fld_beam = fld2 ? 1 : 0;
+                T.mom = fld2 ? m1 : m2;
+                T.pair = p;
+                T.lum = compute_lum && (fld2 ? sample_beam1 : !sample_beam1);
+                T.center = SS.center[ss];
+                T.kbb = SS.weight[ss] * (fld2 ? kbb2p : kbb1p);
+                T.klum = SS.weight[ss] * (fld2 ? klum2 : klum1);
+                const int tid = (int)gt.size();
+                if (T.lum) {
+                    ltask.push_back(tid);
+                    lfirst.push_back((int)kmap.size());
+                }
+                for (long long off = 0; off < T.fld_n; off += kGaussChunk) kmap.push_back(make_int2(tid, (int)off));
+                if (T.lum) lcount.push_back((int)kmap.size() - lfirst.back());
+                gt.push_back(T);
+                Task PT{};  // for error reports
+                PT.dir = dir; PT.i = i; PT.j = j; PT.src_beam = fld2 ? 0 : 1; PT.fld_beam = T.fld_beam; PT.pair = p;
+                tasks.push_back(PT);
+            }
+        }
+        F.ns = (int)gs.size() - F.s0;
+        F.nsb = (int)smap.size() - F.sb0;
+        F.nt = (int)gt.size() - F.t0;
+        F.nkb = (int)kmap.size() - F.kb0;
+        F.nl = (int)ltask.size() - F.l0;
+        if (F.ns) fronts.push_back(F);
+    }
+    ntasks = (int)tasks.size();
+    // device copies: slices, tasks, block maps, and the index arrays [sfirst | scount | ltask | lfirst | lcount]
+    c->g_slices.ensure(std::max<size_t>(gs.size(), 1));
+    c->g_mom.ensure(std::max<size_t>(gs.size(), 1));
+    c->g_tasks.ensure(std::max<size_t>(gt.size(), 1));
+    c->g_bmap.ensure(std::max<size_t>(smap.size() + kmap.size(), 1));
+    std::vector<int> idx;
+    idx.insert(idx.end(), sfirst.begin(), sfirst.end());
+    idx.insert(idx.end(), scount.begin(), scount.end());
+    idx.insert(idx.end(), ltask.begin(), ltask.end());
+    idx.insert(idx.end(), lfirst.begin(), lfirst.end());
+    idx.insert(idx.end(), lcount.begin(), lcount.end());
+    c->g_index.ensure(std::max<size_t>(idx.size(), 1));
+    c->g_partial.ensure(std::max<size_t>(smap.size(), 1) * kGaussSums);
+    c->g_lum_partial.ensure(std::max<size_t>(kmap.size(), 1));
+    c->lum_parts.ensure(std::max(npairs_total, 1));
+    c->status.ensure(1);
+    if (!gs.empty()) CK(cudaMemcpyAsync(c->g_slices.p, gs.data(), sizeof(GSlice) * gs.size(), cudaMemcpyHostToDevice, st));
+    if (!gt.empty()) CK(cudaMemcpyAsync(c->g_tasks.p, gt.data(), sizeof(GTask) * gt.size(), cudaMemcpyHostToDevice, st));
+    if (!smap.empty()) CK(cudaMemcpyAsync(c->g_bmap.p, smap.data(), sizeof(int2) * smap.size(), cudaMemcpyHostToDevice, st));
+    if (!kmap.empty())
+        CK(cudaMemcpyAsync(c->g_bmap.p + smap.size(), kmap.data(), sizeof(int2) * kmap.size(), cudaMemcpyHostToDevice, st));
+    if (!idx.empty()) CK(cudaMemcpyAsync(c->g_index.p, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(c->lum_parts.p, 0, sizeof(double) * std::max(npairs_total, 1), st));
+    {
+        DevStatus z{};
+        z.first_bad = ~0ull;
+        c->h_status.ensure(1);
+        *c->h_status.p = z;
+        CK(cudaMemcpyAsync(c->status.p, c->h_status.p, sizeof z, cudaMemcpyHostToDevice, st));
+    }
+    const int *d_sfirst = c->g_index.p, *d_scount = d_sfirst + sfirst.size();
+    const int *d_ltask = d_scount + scount.size(), *d_lfirst = d_ltask + ltask.size(), *d_lcount = d_lfirst + lfirst.size();
+    GaussArgs A{};
+    for (int b = 0; b < 2; ++b)
+        for (int k = 0; k < 6; ++k) A.c[b][k] = (double *)c->bw[b].s[k].p;
+    A.slices = c->g_slices.p;
+    A.mom = c->g_mom.p;
+    A.tasks = c->g_tasks.p;
+    A.partial = c->g_partial.p;
+    A.lum_partial = c->g_lum_partial.p;
+    A.lum_parts = c->lum_parts.p;
+    A.status = c->status.p;
+    A.min_sigma = o.min_sigma;
+    A.ignore_centroid[0] = o.ignore_centroid1 != 0;
+    A.ignore_centroid[1] = o.ignore_centroid2 != 0;
+    A.longitudinal = o.longitudinal_kick != 0;
+    for (const Front &F : fronts) {
+        {
+            PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, 2);
+            GaussArgs As = A;
+            As.blockmap = c->g_bmap.p + F.sb0;
+            As.partial = c->g_partial.p + (size_t)F.sb0 * kGaussSums;
+            if (F.nsb) launch_pdl(k_gauss_sums, F.nsb, kGaussThreads, 0, st, As);
+            // moments: first[] is relative to the front's first sums block
+            GaussArgs Am = A;
+            Am.slices = c->g_slices.p + F.s0;
+            Am.mom = c->g_mom.p + F.s0;
+            launch_pdl(k_gauss_moments, F.ns, 32, 0, st, Am, d_sfirst + F.s0, d_scount + F.s0);
+            launches += (F.nsb ? 1 : 0) + 1;
+        }
+        {
+            PhaseScope ps(c, OCTO_PHASE_KICK, st, 2);
+            GaussArgs Ak = A;
+            Ak.blockmap = c->g_bmap.p + smap.size() + F.kb0;
+            Ak.lum_partial = c->g_lum_partial.p + F.kb0;
+            if (F.nkb) launch_pdl(k_gauss_kick, F.nkb, kGaussThreads, 0, st, Ak);
+            // the fold reads the kick partials by their index over all fronts (lfirst)
+            if (F.nl) launch_pdl(k_gauss_lum, (F.nl + 31) / 32, 32, 0, st, A, d_ltask + F.l0, d_lfirst + F.l0,
+                                 d_lcount + F.l0, F.nl);
+            launches += (F.nkb ? 1 : 0) + (F.nl ? 1 : 0);
+        }
+    }
+    CK(cudaGetLastError());
 }
 
 double CollideJob::finish() {
@@ -1567,7 +1764,8 @@ octo_ctx *octo_create(int32_t device, const octo_pic_options *options) {
         CK(cudaSetDevice(device));
         CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
         c->fp32 = options->precision == 1;
-        if (d.gaussian) upload_weideman();
+        // the Faddeeva coefficients of the Bassetti-Erskine field: the hybrid's add-back and the soft-Gaussian kick
+        if (d.gaussian || options->solver == OCTO_SOLVER_SOFT_GAUSSIAN) upload_weideman();
         upload_twiddles(c->tw_x, 2 * options->nx);
         upload_twiddles(c->tw_y, 2 * options->ny);
         if (c->fp32) {

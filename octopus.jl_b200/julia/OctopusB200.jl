@@ -47,7 +47,9 @@ struct OctoPicOptions
     positions1::Ptr{Float64}; positions2::Ptr{Float64}
     has_kbb1::Int32; has_kbb2::Int32; has_lum_scale::Int32
     kbb1::Float64; kbb2::Float64; lum_scale::Float64
-    precision::Int32; gaussian::Int32; margin_sigma::Float64; neutralize::Int32; reserved::NTuple{3,Int32}
+    precision::Int32; gaussian::Int32; margin_sigma::Float64; neutralize::Int32
+    solver::Int32; gaussian_when_luminosity::Int32; ignore_centroid1::Int32; ignore_centroid2::Int32
+    virtual_drift::Int32; include_sigma_xy::Int32; min_sigma::Float64
 end
 
 # include/octo_b200.h: octo_collide_report
@@ -120,7 +122,8 @@ function _options(p::PICPoissonSolver, keep::Vector{Any}, precision::Integer=0, 
         p.kbb1 === nothing ? 0.0 : Float64(p.kbb1), p.kbb2 === nothing ? 0.0 : Float64(p.kbb2),
         p.luminosity_scale === nothing ? 0.0 : Float64(p.luminosity_scale), Int32(precision),
         Int32(gaussian !== nothing), gaussian === nothing ? 5.0 : Float64(gaussian.margin_sigma),
-        Int32(gaussian === nothing ? 1 : gaussian.neutralize), ntuple(_ -> Int32(0), 3))
+        Int32(gaussian === nothing ? 1 : gaussian.neutralize), Int32(0), Int32(2), Int32(0), Int32(0), Int32(0),
+        Int32(0), 0.0)
 end
 
 """Context: device workspaces and the slice-pair Green cache (the twin of task.runtime_cache)."""

@@ -14,7 +14,8 @@ from .line import (ChromaticityKickSpec, CrabDispersionSpec, Linear6DSpec, Loren
                    reset_rng_id_counter, set_global_rng)
 from .observers import MomentObserver, moment, moment_name, selected_moments  # noqa: F401
 from .beam import EMASS_EV, ME0, PMASS_EV, RE, Beam, BeamParams  # noqa: F401
-from .solver import ArgumentError, GaussianPICPoissonSolver, LongitudinalSlicing, PICPoissonSolver  # noqa: F401
+from .solver import (ArgumentError, GaussianPICPoissonSolver, GaussianPoissonSolver,  # noqa: F401
+                     LongitudinalSlicing, PICPoissonSolver)
 
 __all__ = ["PICPoissonSolver", "GaussianPICPoissonSolver", "LongitudinalSlicing", "Beam", "BeamParams", "collide", "collide_batch", "Context",
            "StrongStrongRuntime", "TrackingContext", "CUDABackend", "Linear6D", "ArgumentError",
@@ -22,4 +23,4 @@ __all__ = ["PICPoissonSolver", "GaussianPICPoissonSolver", "LongitudinalSlicing"
            "ThinCrabCavitySpec", "LorentzBoostSpec", "RevLorentzBoostSpec", "ChromaticityKickSpec",
            "LumpedRadSpec", "CrabDispersionSpec", "MomentumDispersionSpec", "XYCouplingSpec",
            "set_global_rng", "global_rng_seed", "global_rng_method", "next_rng_id", "claim_rng_id",
-           "reset_rng_id_counter", "MomentObserver", "moment", "moment_name", "selected_moments"]
+           "reset_rng_id_counter", "GaussianPoissonSolver", "MomentObserver", "moment", "moment_name", "selected_moments"]

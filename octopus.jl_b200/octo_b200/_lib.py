@@ -81,8 +81,14 @@ class OctoPicOptions(C.Structure):
         ("gaussian", C.c_int32),
         ("margin_sigma", C.c_double),
         ("neutralize", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("solver", C.c_int32), ("gaussian_when_luminosity", C.c_int32),
+        ("ignore_centroid1", C.c_int32), ("ignore_centroid2", C.c_int32),
+        ("virtual_drift", C.c_int32), ("include_sigma_xy", C.c_int32),
+        ("min_sigma", C.c_double),
     ]
+
+
+SOLVER_PIC, SOLVER_SOFT_GAUSSIAN = 0, 1
 
 
 class OctoCollideReport(C.Structure):

@@ -264,3 +264,61 @@ class GaussianPICPoissonSolver:
         o.margin_sigma = self.margin_sigma
         o.neutralize = int(self.neutralize)
         return o
+
+
+@dataclass(frozen=True)
+class GaussianPoissonSolver:
+    """GaussianPoissonSolver(; ...) -- the soft-Gaussian strong-strong solver (interface.jl:949-1020,
+    src/tasks/strongstrong/gaussian.jl): each slice pair kicks each slice with the Bassetti-Erskine field of a
+    Gaussian carrying the other slice's transverse moments.  This backend implements the uncoupled form
+    (include_sigma_xy = false) with the Hirata virtual drift on float64 beams."""
+    kbb1: Optional[float] = None
+    kbb2: Optional[float] = None
+    luminosity_scale: Optional[float] = None
+    slicing: LongitudinalSlicing = field(default_factory=LongitudinalSlicing)
+    slicing1: Optional[LongitudinalSlicing] = None
+    slicing2: Optional[LongitudinalSlicing] = None
+    min_sigma: float = 0.0
+    gaussian_when_luminosity: int = 2
+    ignore_centroid1: bool = False
+    ignore_centroid2: bool = False
+    longitudinal_kick: bool = True
+    virtual_drift: str = "hirata"
+    include_sigma_xy: bool = False
+    batch_mode: str = "wavefront"
+    luminosity_schedule: Optional[object] = None
+
+    def __post_init__(self):
+        ms = float(self.min_sigma)
+        if not (math.isfinite(ms) and ms >= 0):
+            raise ArgumentError(f"min_sigma must be finite and nonnegative; got {self.min_sigma}.")
+        if self.gaussian_when_luminosity not in (1, 2):
+            raise ArgumentError("gaussian_when_luminosity must be 1 or 2")
+        _choice("batch_mode", self.batch_mode, ("sequential", "wavefront"))
+        _choice("virtual_drift", self.virtual_drift, ("hirata", "chromatic", "exact"))
+
+    @property
+    def resolved_slicing1(self) -> LongitudinalSlicing:
+        return self.slicing1 if self.slicing1 is not None else self.slicing
+
+    @property
+    def resolved_slicing2(self) -> LongitudinalSlicing:
+        return self.slicing2 if self.slicing2 is not None else self.slicing
+
+    def to_c(self) -> "_lib.OctoPicOptions":
+        if self.include_sigma_xy:
+            raise ArgumentError("include_sigma_xy = true (coupled slice covariance) is not implemented by this backend")
+        if self.virtual_drift != "hirata":
+            raise ArgumentError(f"virtual_drift = :{self.virtual_drift} is not implemented by this backend (:hirata)")
+        # the PIC fields are unused by this solver; a valid small grid keeps the context's setup cheap
+        o = PICPoissonSolver(grid=(8, 8), kbb1=self.kbb1, kbb2=self.kbb2, luminosity_scale=self.luminosity_scale,
+                             slicing=self.slicing, slicing1=self.slicing1, slicing2=self.slicing2,
+                             longitudinal_kick=self.longitudinal_kick).to_c()
+        o.solver = _lib.SOLVER_SOFT_GAUSSIAN
+        o.gaussian_when_luminosity = int(self.gaussian_when_luminosity)
+        o.ignore_centroid1 = int(bool(self.ignore_centroid1))
+        o.ignore_centroid2 = int(bool(self.ignore_centroid2))
+        o.virtual_drift = 0
+        o.include_sigma_xy = 0
+        o.min_sigma = float(self.min_sigma)
+        return o

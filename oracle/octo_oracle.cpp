@@ -1980,4 +1980,197 @@ void oo_track_line(const oo_element *elems, int32_t n_elems, int64_t turn, int32
     }
 }
 
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- the soft-Gaussian solver (gaussian.jl)
+namespace {
+std::string g_gauss_error;
+
+const int REDUCTION_CHUNKS = 64;          // interface.jl:664
+const int64_t PARALLEL_MOMENT_MIN = 4096; // interface.jl:609
+const int64_t PARALLEL_KICK_MIN = 4096;   // interface.jl:610
+
+// _chunk_bounds (slicing.jl:517-521), 0-based half-open
+inline void chunk_bounds(int64_t n, int nchunks, int chunk1, int64_t &lo, int64_t &hi) {
+    lo = ((int64_t)(chunk1 - 1) * n) / nchunks;
+    hi = ((int64_t)chunk1 * n) / nchunks;
+}
+
+struct SoftMoments {
+    double mx, mpx, my, mpy;                  // after ignore_centroid
+    double a0, d0, bxx, bypy, qxx, qyy;       // StrongTransverseMoments{T,false}
+    double sx, sy, spx, spy, covxpx, covypy;  // for the finiteness check
+};
+
+// _slice_transverse_moments (slicing.jl:670-770), uncoupled
+SoftMoments slice_moments(double *const b[6], const std::vector<int64_t> &idx, bool ignore_centroid, double min_sigma) {
+    SoftMoments M{};
+    const int64_t n = (int64_t)idx.size();
+    const double floor2 = min_sigma * min_sigma;
+    if (n == 0) {
+        M.a0 = floor2; M.d0 = floor2;
+        M.sx = min_sigma; M.sy = min_sigma;
+        return M;
+    }
+    const int64_t f = idx[0];
+    const double x0 = b[0][f], px0 = b[1][f], y0 = b[2][f], py0 = b[3][f];
+    double s[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    auto acc = [&](double *t, int64_t lo, int64_t hi) {
+        for (int64_t p = lo; p < hi; ++p) {
+            const int64_t i = idx[p];
+            const double dx = b[0][i] - x0, dpx = b[1][i] - px0, dy = b[2][i] - y0, dpy = b[3][i] - py0;
+            t[0] += dx; t[1] += dpx; t[2] += dy; t[3] += dpy;
+            t[4] += dx * dx; t[5] += dpx * dpx; t[6] += dy * dy; t[7] += dpy * dpy;
+            t[8] += dx * dpx; t[9] += dy * dpy;
+        }
+    };
+    if (n < PARALLEL_MOMENT_MIN) {
+        acc(s, 0, n);
+    } else {
+        for (int ch = 1; ch <= REDUCTION_CHUNKS; ++ch) {
+            double t[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+            int64_t lo, hi;
+            chunk_bounds(n, REDUCTION_CHUNKS, ch, lo, hi);
+            acc(t, lo, hi);
+            for (int q = 0; q < 10; ++q) s[q] += t[q];
+        }
+    }
+    const double invn = 1.0 / (double)n;
+    const double dmx = s[0] * invn, dmpx = s[1] * invn, dmy = s[2] * invn, dmpy = s[3] * invn;
+    double mx = x0 + dmx, mpx = px0 + dmpx, my = y0 + dmy, mpy = py0 + dmpy;
+    const double sx2 = std::fma(-dmx, dmx, s[4] * invn), spx2 = std::fma(-dmpx, dmpx, s[5] * invn);
+    const double sy2 = std::fma(-dmy, dmy, s[6] * invn), spy2 = std::fma(-dmpy, dmpy, s[7] * invn);
+    const double covxpx = std::fma(-dmx, dmpx, s[8] * invn), covypy = std::fma(-dmy, dmpy, s[9] * invn);
+    const double varx = jmax(sx2, floor2), vary = jmax(sy2, floor2);
+    M.a0 = varx; M.d0 = vary; M.bxx = covxpx; M.bypy = covypy;
+    M.qxx = jmax(spx2, 0.0); M.qyy = jmax(spy2, 0.0);
+    if (ignore_centroid) { mx = 0; mpx = 0; my = 0; mpy = 0; }
+    M.mx = mx; M.mpx = mpx; M.my = my; M.mpy = mpy;
+    M.sx = std::sqrt(varx); M.sy = std::sqrt(vary);
+    M.spx = std::sqrt(jmax(spx2, 0.0)); M.spy = std::sqrt(jmax(spy2, 0.0));
+    M.covxpx = covxpx; M.covypy = covypy;
+    return M;
+}
+
+// _gaussian_moments_finite (gaussian.jl:126-130)
+bool moments_finite(const SoftMoments &m) {
+    return std::isfinite(m.mx) && std::isfinite(m.mpx) && std::isfinite(m.my) && std::isfinite(m.mpy) &&
+           std::isfinite(m.sx) && std::isfinite(m.sy) && std::isfinite(m.spx) && std::isfinite(m.spy) &&
+           std::isfinite(m.covxpx) && std::isfinite(m.covypy);
+}
+
+// _apply_slice_kick_one! (gaussian.jl:152-185): Hirata paraxial drift (strong_beam.jl:559-577) or, without the
+// longitudinal kick, the frozen-longitudinal paraxial drift (:517-531); _cp_covariance_kick (:619-632)
+double apply_one(double *const b[6], int64_t i, const SoftMoments &m, double center, double kbb, bool lk,
+                 bool compute_lum) {
+    double x = b[0][i], px = b[1][i], y = b[2][i], py = b[3][i], z = b[4][i], pz = b[5][i];
+    double S = 0.5 * (z - center);
+    x += S * px;
+    y += S * py;
+    if (lk) pz -= 0.25 * (px * px + py * py);
+    const double xx = x - m.mx + m.mpx * S;
+    const double yy = y - m.my + m.mpy * S;
+    const double px0 = px, py0 = py, pz0 = pz;
+    const double a = m.a0 - 2 * S * m.bxx + S * S * m.qxx;
+    const double d = m.d0 - 2 * S * m.bypy + S * S * m.qyy;
+    const double au = 2 * (m.bxx - S * m.qxx);
+    const double du = 2 * (m.bypy - S * m.qyy);
+    const double twopi = 6.283185307179586476925286766559005768394338;
+    double density = 0.0;
+    if (!(a <= 0 || d <= 0)) {
+        const double sigx = std::sqrt(a), sigy = std::sqrt(d);
+        double Kx, Ky, Hxx, Hyy;
+        be::response(kbb, sigx, sigy, xx, yy, Kx, Ky, Hxx, Hyy);
+        const double expterm = std::exp(-0.5 * (xx * xx / (sigx * sigx) + yy * yy / (sigy * sigy)));
+        px += Kx * kbb;
+        py += Ky * kbb;
+        pz += 0.25 * (Hxx * au + Hyy * du);
+        density = expterm / twopi / sigx / sigy;
+    }
+    if (lk) pz += 0.5 * ((px - px0) * m.mpx + (py - py0) * m.mpy);
+    else pz = pz0;
+    S = 0.5 * (z - center);
+    x -= S * px;
+    y -= S * py;
+    if (lk) pz += 0.25 * (px * px + py * py);
+    b[0][i] = x; b[1][i] = px; b[2][i] = y; b[3][i] = py; b[4][i] = z; b[5][i] = pz;
+    return compute_lum ? density * twopi : 0.0;
+}
+
+// _slice_slice_gaussian_kick! (gaussian.jl:59-108)
+double slice_kick(double *const b[6], const std::vector<int64_t> &idx, const SoftMoments &m2, double center2,
+                  double kbb_slice, double klum_slice, bool lk, bool compute_lum) {
+    const int64_t n = (int64_t)idx.size();
+    if (n == 0) return 0.0;
+    const double twopi = 6.283185307179586476925286766559005768394338;
+    if (n < PARALLEL_KICK_MIN) {
+        double lum = 0.0;
+        for (int64_t p = 0; p < n; ++p) lum += apply_one(b, idx[p], m2, center2, kbb_slice, lk, compute_lum);
+        return lum / twopi * klum_slice;
+    }
+    double local[REDUCTION_CHUNKS];
+#pragma omp parallel for schedule(static)
+    for (int ch = 1; ch <= REDUCTION_CHUNKS; ++ch) {
+        int64_t lo, hi;
+        chunk_bounds(n, REDUCTION_CHUNKS, ch, lo, hi);
+        double t = 0.0;
+        for (int64_t p = lo; p < hi; ++p) t += apply_one(b, idx[p], m2, center2, kbb_slice, lk, compute_lum);
+        local[ch - 1] = t;
+    }
+    double sum = 0.0;
+    for (int ch = 0; ch < REDUCTION_CHUNKS; ++ch) sum += local[ch];
+    return sum / twopi * klum_slice;
+}
+
+}  // namespace
+
+extern "C" {
+
+// collide!(::GaussianPoissonSolver, beam1, beam2, ::CPUThreadsBackend) (gaussian.jl:7-57), uncoupled with the
+// Hirata drift; opt supplies the slicings, kbb / luminosity-scale overrides and longitudinal_kick.
+int oo_gaussian_collide(const oo_options *opt, double min_sigma, int32_t gaussian_when_luminosity,
+                        int32_t ignore_centroid1, int32_t ignore_centroid2, double *b1[6], int64_t n1, double *b2[6],
+                        int64_t n2, const oo_beam_params *p1, const oo_beam_params *p2, double *luminosity) {
+    try {
+        std::vector<double> pos1, pos2;
+        if (opt->slicing_method1 == 1 && opt->positions1) pos1.assign(opt->positions1, opt->positions1 + opt->nslices1 - 1);
+        if (opt->slicing_method2 == 1 && opt->positions2) pos2.assign(opt->positions2, opt->positions2 + opt->nslices2 - 1);
+        Slices s1 = make_slices(opt->slicing_method1, opt->nslices1, opt->center_position1, pos1, b1[4], n1);
+        Slices s2 = make_slices(opt->slicing_method2, opt->nslices2, opt->center_position2, pos2, b2[4], n2);
+        if (!opt->has_kbb1 && !(std::isfinite(p1->E0) && p1->E0 != 0))
+            throw OracleError(OO_ERR_ARG, "beam1 E0 must be finite and nonzero when kbb1 is not specified");
+        if (!opt->has_kbb2 && !(std::isfinite(p2->E0) && p2->E0 != 0))
+            throw OracleError(OO_ERR_ARG, "beam2 E0 must be finite and nonzero when kbb2 is not specified");
+        const double kbb1 = opt->has_kbb1 ? opt->kbb1 : p1->charge * p2->charge * p1->r0 * p2->npart * p1->mc2 / p1->E0;
+        const double kbb2 = opt->has_kbb2 ? opt->kbb2 : p1->charge * p2->charge * p2->r0 * p1->npart * p2->mc2 / p2->E0;
+        const double klum1 = opt->has_lum_scale ? opt->lum_scale : p1->npart * p2->npart / (double)n1;
+        const double klum2 = opt->has_lum_scale ? opt->lum_scale : p1->npart * p2->npart / (double)n2;
+        const bool lk = opt->longitudinal_kick != 0;
+        const bool sample_beam1 = gaussian_when_luminosity == 1;
+        double lum = 0.0;
+        for (const OrderEntry &pr : collision_order(s1.center, s2.center)) {
+            const int i = pr.i - 1, j = pr.j - 1;
+            const SoftMoments m1 = slice_moments(b1, s1.indices[i], ignore_centroid1 != 0, min_sigma);
+            const SoftMoments m2 = slice_moments(b2, s2.indices[j], ignore_centroid2 != 0, min_sigma);
+            if (!moments_finite(m1))
+                throw OracleError(OO_ERR_NONFINITE, "non-finite source coordinate (beam 1, slice " + std::to_string(i + 1) + ")");
+            if (!moments_finite(m2))
+                throw OracleError(OO_ERR_NONFINITE, "non-finite source coordinate (beam 2, slice " + std::to_string(j + 1) + ")");
+            const double lum2 = slice_kick(b1, s1.indices[i], m2, s2.center[j], s2.weight[j] * kbb1, s2.weight[j] * klum1,
+                                           lk, !sample_beam1);
+            const double lum1 = slice_kick(b2, s2.indices[j], m1, s1.center[i], s1.weight[i] * kbb2, s1.weight[i] * klum2,
+                                           lk, sample_beam1);
+            lum += sample_beam1 ? lum1 : lum2;
+        }
+        if (luminosity) *luminosity = lum;
+        return OO_OK;
+    } catch (OracleError &e) {
+        g_gauss_error = e.what();
+        return e.code;
+    }
+}
+
+const char *oo_gaussian_last_error(void) { return g_gauss_error.c_str(); }
+
 }  // extern "C"

@@ -128,6 +128,10 @@ def lib():
         L.oo_last_error.argtypes = [vp]
         L.oo_linear6d.argtypes = [P(d)] + [P(d)] * 6 + [i64]
         L.oo_linear6d_matrix.argtypes = [P(d), P(d), P(d), P(d)]
+        L.oo_gaussian_collide.argtypes = [P(OOOptions), d, i32, i32, i32, P(P(d)), i64, P(P(d)), i64,
+                                          P(OOBeamParams), P(OOBeamParams), P(d)]
+        L.oo_gaussian_collide.restype = C.c_int
+        L.oo_gaussian_last_error.restype = C.c_char_p
         L.oo_track_line.argtypes = [P(OOElement), i32, i64, i32, C.c_uint64, i32] + [P(d)] * 6 + [i64]
         L.oo_track_line.restype = None
         L.oo_octopus_normal.argtypes = [C.c_uint64, i32, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]
@@ -463,3 +467,20 @@ def _seq_sum(v):
     for a in np.asarray(v, dtype=np.float64).tolist():
         s += a
     return s
+
+
+def gaussian_collide(options: "OracleOptions", beam1: np.ndarray, beam2: np.ndarray, p1, p2, min_sigma=0.0,
+                     gaussian_when_luminosity=2, ignore_centroid1=False, ignore_centroid2=False) -> float:
+    """collide!(::GaussianPoissonSolver, ...) (src/tasks/strongstrong/gaussian.jl) in place on (6, n) float64
+    beams; options gives the slicings, kbb / luminosity-scale overrides and longitudinal_kick."""
+    P = C.POINTER(C.c_double)
+    a1 = (P * 6)(*[_dp(beam1[k]) for k in range(6)])
+    a2 = (P * 6)(*[_dp(beam2[k]) for k in range(6)])
+    copt = options.to_c()
+    lum = C.c_double(np.nan)
+    rc = lib().oo_gaussian_collide(C.byref(copt), float(min_sigma), int(gaussian_when_luminosity),
+                                   int(bool(ignore_centroid1)), int(bool(ignore_centroid2)), a1, beam1.shape[1], a2,
+                                   beam2.shape[1], C.byref(p1), C.byref(p2), C.byref(lum))
+    if rc != OK:
+        raise OracleErrorPy(rc, lib().oo_gaussian_last_error().decode())
+    return lum.value

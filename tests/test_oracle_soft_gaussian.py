@@ -1,0 +1,48 @@
+"""The oracle's soft-Gaussian solver (gaussian.jl restated) against physics it must reproduce: one slice
+each, long bunches made short (no hourglass), the luminosity of two Gaussian beams
+N1 N2 / (2 pi sqrt(sx1^2 + sx2^2) sqrt(sy1^2 + sy2^2)) to sampling accuracy, whichever beam is sampled; and
+the kick of a particle far outside the other beam approaches the point-charge kick 2 kbb / r."""
+import numpy as np
+
+from oracle import oracle as orc
+
+
+def test_luminosity_of_two_gaussians():
+    rng = np.random.default_rng(1)
+    n1, n2 = 200_000, 150_000
+    s1, s2 = (20e-6, 4e-6), (16e-6, 3e-6)
+
+    def beam(n, s):
+        b = np.zeros((6, n))
+        b[0] = rng.normal(size=n) * s[0]
+        b[2] = rng.normal(size=n) * s[1]
+        b[4] = rng.normal(size=n) * 1e-9   # short bunches: no hourglass over the drift
+        return b
+
+    N1, N2 = 1e11, 7e10
+    p1 = orc.beam_params(-1.0, orc.EMASS_EV, 10e9, N1)
+    p2 = orc.beam_params(1.0, orc.PMASS_EV, 275e9, N2)
+    opt = orc.OracleOptions(nslices1=1, nslices2=1, kbb1=0.0, kbb2=0.0)
+    want = N1 * N2 / (2 * np.pi * np.hypot(s1[0], s2[0]) * np.hypot(s1[1], s2[1]))
+    for g in (1, 2):
+        b1, b2 = beam(n1, s1), beam(n2, s2)
+        lum = orc.gaussian_collide(opt, b1, b2, p1, p2, gaussian_when_luminosity=g)
+        assert abs(lum / want - 1) < 0.01, (g, lum, want)
+
+
+def test_far_kick_is_point_charge():
+    rng = np.random.default_rng(2)
+    n2 = 100_000
+    b2 = np.zeros((6, n2))
+    b2[0] = rng.normal(size=n2) * 10e-6
+    b2[2] = rng.normal(size=n2) * 10e-6
+    b1 = np.zeros((6, 1))
+    b1[0, 0] = 2e-3  # 200 sigma away
+    kbb = 1e-4
+    opt = orc.OracleOptions(nslices1=1, nslices2=1, kbb1=kbb, kbb2=0.0, longitudinal_kick=False)
+    p = orc.beam_params(1.0, orc.PMASS_EV, 275e9, 1e11)
+    orc.gaussian_collide(opt, b1, b2, p, p)
+    # Kx -> 2 x / r^2 for a unit-normalised Gaussian; the slice weight is 1
+    assert abs(b1[1, 0] / (kbb * 2 / 2e-3) - 1) < 1e-4
+    # the y kick is the sampled centroid's offset (~1e-8 in y) seen from 2 mm
+    assert abs(b1[3, 0]) < 1e-4 * abs(b1[1, 0])
