@@ -306,6 +306,7 @@ def run_ours(args, rank, world, local_rank):
         shape32 = fast["shape"]
     lines = None if args.no_line else time_lines(ob, e0, p0, args, stream, barrier)
     observer = None if args.no_line else time_observer(ob, e0, p0, args, stream)
+    soft = None if args.no_line else time_soft_gaussian(ob, e0, p0, me, mp, rt, local_rank, args, stream)
     clk = clocks.stop()
 
     # long-term tracking of both forms from the same beams (outside every timed region, one GPU only):
@@ -423,6 +424,7 @@ def run_ours(args, rank, world, local_rank):
         "emittance_growth": emit,
         "line_tracking": lines,
         "moment_observer": observer,
+        "soft_gaussian": soft,
         "clocks": clk,
         "luminosity": lum,
         "dominant_phase": dom[0],
@@ -502,6 +504,61 @@ def time_lines(ob, e0, p0, args, stream, barrier):
             "note": "each launch reads and writes the six FP64 coordinates once; a segment of maps alone runs "
                     "at the HBM bound, the radiation's six Philox draws and three Box-Muller transforms per "
                     "particle make the electron's after-collision segment instruction-issue bound"}
+
+
+def time_soft_gaussian(ob, e0, p0, me, mp, rt, local_rank, args, stream):
+    """The soft-Gaussian solver (GaussianPoissonSolver, 15 slices) on the same beams and maps: s/turn, the
+    phase split (moments, kick), the kick's achieved bytes per second (11 FP64 values per field particle per
+    pair) and the oracle's time per turn on a 10 % sample."""
+    import torch
+    solver = ob.GaussianPoissonSolver(slicing=ob.LongitudinalSlicing(nslices=SLICES, method="normal_quantile"))
+    e = ob.Beam(e0.clone(), ob.BeamParams(-1.0, ob.EMASS_EV, 10e9, ob.RE, 1.7e11))
+    p = ob.Beam(p0.clone(), ob.BeamParams(1.0, ob.PMASS_EV, 275e9, ob.RE * ob.ME0 / ob.PMASS_EV, 6.9e10))
+    ctx = rt.context("soft", solver, local_rank)
+
+    def turn(t):
+        lum = ctx.collide(e, p, turn=t, stream=stream)
+        me.track(e, stream=stream)
+        mp.track(p, stream=stream)
+        return lum
+
+    for t in range(args.warmup):
+        turn(t)
+    torch.cuda.synchronize()
+    K = max(5, min(args.steps, 30))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    gc.collect()
+    gc.disable()
+    ev0.record(stream)
+    for t in range(K):
+        lum = turn(args.warmup + t)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    gc.enable()
+    ms = ev0.elapsed_time(ev1) / K
+    ctx.set_timing(True)
+    nph = 5
+    for t in range(nph):
+        turn(args.warmup + K + t)
+    torch.cuda.synchronize()
+    ph = ctx.timing_report()
+    ctx.set_timing(False)
+    kick_ms, _, _ = ph["kick"]
+    kick_bytes = (N_E + N_P) * SLICES * 11 * 8 * nph
+    out = {"value": ms / 1e3, "unit": UNIT, "ms_per_step": ms, "luminosity": lum, "nslices": SLICES,
+           "phases_ms_per_turn": {"slicing": ph["slicing"][0] / nph, "moments": ph["bounds"][0] / nph,
+                                  "kick": kick_ms / nph, "unsort": ph["unsort"][0] / nph},
+           "kick_achieved_gbs": kick_bytes / (kick_ms / 1e3) / 1e9 if kick_ms > 0 else None}
+    # the oracle on a 10 % sample of both beams (same slicing), all host threads
+    from oracle import oracle as orc
+    se, sp = e0[:, : N_E // 10].cpu().numpy().copy(), p0[:, : N_P // 10].cpu().numpy().copy()
+    opt = orc.OracleOptions(nslices1=SLICES, nslices2=SLICES)
+    t0 = time.perf_counter()
+    orc.gaussian_collide(opt, se, sp, orc.beam_params(-1.0, orc.EMASS_EV, 10e9, 1.7e11),
+                         orc.beam_params(1.0, orc.PMASS_EV, 275e9, 6.9e10))
+    out["cpu_oracle_s_per_turn"] = (time.perf_counter() - t0) * 10
+    out["cpu_sample"] = "10 % of each beam, one collide, scaled by 10"
+    return out
 
 
 def time_observer(ob, e0, p0, args, stream):
