@@ -21,6 +21,7 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -75,6 +76,8 @@ class Clocks:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
+        self.lines = []
+        self.first = threading.Event()
 
     def start(self):
         try:
@@ -83,19 +86,33 @@ class Clocks:
                                          stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+            return
+        self.reader = threading.Thread(target=self._read, daemon=True)
+        self.reader.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line)
+            self.first.set()
+
+    def wait_first(self, timeout: float = 10.0):
+        """Returns once the sampler has written its first sample: its start-up (driver and NVML
+        initialisation) then lies before the timed region rather than inside it."""
+        if self.proc is not None:
+            self.first.wait(timeout)
 
     def stop(self):
         if self.proc is None:
             return None
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=10)
+            self.proc.wait(timeout=10)
         except Exception:
             self.proc.kill()
-            out, _ = self.proc.communicate()
+        self.reader.join(timeout=10)
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.splitlines():
+        for line in list(self.lines):
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -192,6 +209,7 @@ def run_ours(args, rank, world, local_rank):
 
     clocks = Clocks(local_rank)
     clocks.start()
+    clocks.wait_first()
     time.sleep(0.3)
     # the timed region carries no instrumentation: an event recorded between two kernels of the collide
     # stream costs time and breaks their programmatic launch overlap (~0.3 ms per turn for the kicks'
