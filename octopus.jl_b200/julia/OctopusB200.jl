@@ -85,9 +85,34 @@ function B200GaussianPICPoissonSolver(; kwargs...)
         "coupling_tol < Inf (the coupled subtraction) is not implemented by the B200 backend"))
     return B200GaussianPICPoissonSolver(g, g.pic)
 end
-const B200Solver = Union{B200PICPoissonSolver,B200GaussianPICPoissonSolver}
-_gaussian_of(::B200PICPoissonSolver) = nothing
+"""
+    B200GaussianPoissonSolver(; kwargs...)
+
+`GaussianPoissonSolver(; kwargs...)`, the soft-Gaussian strong-strong solver (interface.jl:949-1020,
+gaussian.jl), run on libocto_b200: the uncoupled covariance (`include_sigma_xy = false`) with the Hirata
+virtual drift, on Float64 beams.  `pic` only carries the slicings, kbb and luminosity-scale overrides and
+`longitudinal_kick` into the shared options struct.
+"""
+struct B200GaussianPoissonSolver{T<:Real} <: AbstractPoissonSolver
+    soft::Octopus.GaussianPoissonSolver
+    pic::PICPoissonSolver{T}
+end
+function B200GaussianPoissonSolver(; kwargs...)
+    g = Octopus.GaussianPoissonSolver(; kwargs...)
+    g.include_sigma_xy && throw(ArgumentError(
+        "include_sigma_xy = true (the coupled slice covariance) is not implemented by the B200 backend"))
+    g.virtual_drift isa Octopus.HirataParaxialDrift || throw(ArgumentError(
+        "the B200 backend's soft-Gaussian solver implements virtual_drift = :hirata only"))
+    pic = PICPoissonSolver(; grid=(8, 8), kbb1=g.kbb1, kbb2=g.kbb2, luminosity_scale=g.luminosity_scale,
+                           slicing1=g.slicing1, slicing2=g.slicing2, longitudinal_kick=g.longitudinal_kick,
+                           luminosity_schedule=g.luminosity_schedule)
+    return B200GaussianPoissonSolver(g, pic)
+end
+const B200Solver = Union{B200PICPoissonSolver,B200GaussianPICPoissonSolver,B200GaussianPoissonSolver}
+_gaussian_of(::Union{B200PICPoissonSolver,B200GaussianPoissonSolver}) = nothing
 _gaussian_of(s::B200GaussianPICPoissonSolver) = s.gpic
+_soft_of(::Union{B200PICPoissonSolver,B200GaussianPICPoissonSolver}) = nothing
+_soft_of(s::B200GaussianPoissonSolver) = s.soft
 
 _sym(v, table) = Int32(table[Symbol(v)])
 
@@ -98,7 +123,7 @@ function _slicing_fields(s::LongitudinalSlicing)
             s.center_position === :centroid ? Int32(0) : Int32(1))
 end
 
-function _options(p::PICPoissonSolver, keep::Vector{Any}, precision::Integer=0, gaussian=nothing)
+function _options(p::PICPoissonSolver, keep::Vector{Any}, precision::Integer=0, gaussian=nothing; soft=nothing)
     m1, n1, c1 = _slicing_fields(p.slicing1)
     m2, n2, c2 = _slicing_fields(p.slicing2)
     pos1 = Float64.(p.slicing1.positions); pos2 = Float64.(p.slicing2.positions)
@@ -122,17 +147,21 @@ function _options(p::PICPoissonSolver, keep::Vector{Any}, precision::Integer=0, 
         p.kbb1 === nothing ? 0.0 : Float64(p.kbb1), p.kbb2 === nothing ? 0.0 : Float64(p.kbb2),
         p.luminosity_scale === nothing ? 0.0 : Float64(p.luminosity_scale), Int32(precision),
         Int32(gaussian !== nothing), gaussian === nothing ? 5.0 : Float64(gaussian.margin_sigma),
-        Int32(gaussian === nothing ? 1 : gaussian.neutralize), Int32(0), Int32(2), Int32(0), Int32(0), Int32(0),
-        Int32(0), 0.0)
+        Int32(gaussian === nothing ? 1 : gaussian.neutralize),
+        # soft-Gaussian solver fields (solver, gaussian_when_luminosity, ignore_centroid1/2, virtual_drift,
+        # include_sigma_xy, min_sigma)
+        Int32(soft === nothing ? 0 : 1), Int32(soft === nothing ? 2 : soft.gaussian_when_luminosity),
+        Int32(soft === nothing ? 0 : soft.ignore_centroid1), Int32(soft === nothing ? 0 : soft.ignore_centroid2),
+        Int32(0), Int32(0), soft === nothing ? 0.0 : Float64(soft.min_sigma))
 end
 
 """Context: device workspaces and the slice-pair Green cache (the twin of task.runtime_cache)."""
 mutable struct Context
     ptr::Ptr{Cvoid}
     # T = Float64: the plain form; T = Float32: the precision form (FP32 particles, planes and FFTs)
-    function Context(p::PICPoissonSolver, ::Type{T}=Float64, gaussian=nothing) where {T<:Union{Float32,Float64}}
+    function Context(p::PICPoissonSolver, ::Type{T}=Float64, gaussian=nothing; soft=nothing) where {T<:Union{Float32,Float64}}
         keep = Any[]
-        opts = Ref(_options(p, keep, T === Float32 ? 1 : 0, gaussian))
+        opts = Ref(_options(p, keep, T === Float32 ? 1 : 0, gaussian; soft=soft))
         ptr = GC.@preserve keep ccall((:octo_create, LIB), Ptr{Cvoid}, (Int32, Ref{OctoPicOptions}),
                                       Int32(CUDA.device().handle), opts)
         ptr == C_NULL && error("octo_create failed")
@@ -192,7 +221,7 @@ end
 as the reference's public collide! builds a fresh Green cache (pic_cuda.jl:94-126)."""
 function Octopus.collide!(solver::B200Solver, beam1::Beam, beam2::Beam, ::Type{CUDABackend},
                           ctx::Union{Nothing,TrackingContext}=nothing)
-    c = Context(solver.pic, eltype(beam1.rep.x), _gaussian_of(solver))
+    c = Context(solver.pic, eltype(beam1.rep.x), _gaussian_of(solver); soft=_soft_of(solver))
     try
         return _collide!(c, solver, beam1, beam2, ctx === nothing ? -1 : ctx.turn)
     finally
@@ -206,7 +235,7 @@ function Octopus._strong_strong_collide_backend!(task::StrongStrongTask, label::
                                                  ::Type{CUDABackend}, ctx::TrackingContext)
     T = eltype(beam1.rep.x)
     key = (:octo_b200_context, label, T, solver.pic.grid, objectid(solver))
-    c = get!(() -> Context(solver.pic, T, _gaussian_of(solver)), task.runtime_cache, key)::Context
+    c = get!(() -> Context(solver.pic, T, _gaussian_of(solver); soft=_soft_of(solver)), task.runtime_cache, key)::Context
     return _collide!(c, solver, beam1, beam2, ctx.turn)
 end
 
