@@ -52,7 +52,65 @@ struct GaussArgs {
     double min_sigma;
     int ignore_centroid[2];
     int longitudinal;
+    int drift;              // virtual drift with the longitudinal kick: 0 Hirata, 1 chromatic, 2 exact
 };
+
+// The virtual drifts to and from the collision point (strong_beam.jl:517-606): forward returns S.  Without the
+// longitudinal kick the solver uses the frozen-longitudinal paraxial drift (gaussian.jl:148-150).
+__device__ __forceinline__ double drift_forward(int kind, bool lk, double &x, double px, double &y, double py,
+                                                double &z, double &pz, double zo) {
+    if (!lk || kind == 0) {
+        const double S = 0.5 * (z - zo);
+        x += S * px;
+        y += S * py;
+        if (lk) pz -= 0.25 * (px * px + py * py);
+        return S;
+    }
+    if (kind == 1) {  // ChromaticDrift
+        const double S = 0.5 * (z - zo);
+        const double phi = sqrt(1 - 0.5 * (px * px + py * py) / ((1 + pz) * (1 + pz))) - 1;
+        x += S * px / (1 + pz);
+        y += S * py / (1 + pz);
+        z += 2 * S * phi;
+        pz += (1 + pz) * phi;
+        return S;
+    }
+    // ExactHamiltonianDrift
+    const double ps = sqrt((1 + pz) * (1 + pz) - px * px - py * py);
+    const double H = 1 + pz - ps;
+    const double rr = 0.5 * H / ps;
+    const double z2 = (z + rr * zo) / (1 + rr);
+    const double S = 0.5 * (z2 - zo);
+    z -= H / ps * S;
+    pz -= 0.5 * H;
+    x += px / ps * S;
+    y += py / ps * S;
+    return S;
+}
+__device__ __forceinline__ void drift_reverse(int kind, bool lk, double &x, double px, double &y, double py, double &z,
+                                              double &pz, double zo) {
+    const double S = 0.5 * (z - zo);
+    if (!lk || kind == 0) {
+        x -= S * px;
+        y -= S * py;
+        if (lk) pz += 0.25 * (px * px + py * py);
+        return;
+    }
+    if (kind == 1) {
+        const double psi = sqrt(1 + 0.5 * (px * px + py * py) / ((1 + pz) * (1 + pz))) - 1;
+        x -= S * px / (1 + pz);
+        y -= S * py / (1 + pz);
+        z += 2 * S * psi;
+        pz += (1 + pz) * psi;
+        return;
+    }
+    const double H0 = 0.5 * (px * px + py * py) / (1 + pz);
+    const double ps0 = 1 + pz - 0.5 * H0;
+    pz += 0.5 * H0;
+    x -= px / ps0 * S;
+    y -= py / ps0 * S;
+    z += H0 / ps0 * S;
+}
 
 __global__ void __launch_bounds__(kGaussThreads) k_gauss_sums(GaussArgs A) {
     pdl_wait();
@@ -135,8 +193,7 @@ __global__ void k_gauss_moments(GaussArgs A, const int *first, const int *count)
 }
 
 // _apply_slice_kick_one! (gaussian.jl:152-185) with the uncoupled _cp_covariance_kick (strong_beam.jl:619-632)
-// and the Hirata paraxial drift (strong_beam.jl:559-577), or the frozen-longitudinal paraxial drift without
-// the longitudinal kick (gaussian.jl:148-150, strong_beam.jl:517-531).
+// between the virtual drifts above.
 // Three blocks per SM (at most 85 registers): the Bassetti-Erskine response is an FP64 latency chain, and
 // occupancy hides it better than registers do (measured: 10.6 ms per production collide at one block per
 // SM, 9.4 at two, 9.0 at three).
@@ -153,13 +210,8 @@ __global__ void __launch_bounds__(kGaussThreads, 3) k_gauss_kick(GaussArgs A) {
     const long long end = min(T.fld_n, (long long)bm.y + kGaussChunk);
     for (long long k = bm.y + threadIdx.x; k < end; k += kGaussThreads) {
         const long long i = T.fld_start + k;
-        double x = c[0][i], px = c[1][i], y = c[2][i], py = c[3][i], pz = c[5][i];
-        const double z = c[4][i];
-        // forward virtual drift
-        const double S = 0.5 * (z - T.center);
-        x += S * px;
-        y += S * py;
-        if (lk) pz -= 0.25 * (px * px + py * py);
+        double x = c[0][i], px = c[1][i], y = c[2][i], py = c[3][i], z = c[4][i], pz = c[5][i];
+        const double S = drift_forward(A.drift, lk, x, px, y, py, z, pz, T.center);
         const double xx = x - M.mx + M.mpx * S;
         const double yy = y - M.my + M.mpy * S;
         const double px0 = px, py0 = py, pz0 = pz;
@@ -181,14 +233,12 @@ __global__ void __launch_bounds__(kGaussThreads, 3) k_gauss_kick(GaussArgs A) {
         }
         if (lk) pz += 0.5 * ((px - px0) * M.mpx + (py - py0) * M.mpy);
         else pz = pz0;
-        // reverse virtual drift (S from the unchanged z)
-        x -= S * px;
-        y -= S * py;
-        if (lk) pz += 0.25 * (px * px + py * py);
+        drift_reverse(A.drift, lk, x, px, y, py, z, pz, T.center);
         c[0][i] = x;
         c[1][i] = px;
         c[2][i] = y;
         c[3][i] = py;
+        c[4][i] = z;
         c[5][i] = pz;
         dens += density * twopi;
     }

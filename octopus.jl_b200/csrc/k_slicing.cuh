@@ -404,6 +404,8 @@ struct UnsortArgs {
     const int *dest[2];
     const R *s[2][5];  // sorted x, px, y, py, pz
     R *c[2][5];        // caller-order x, px, y, py, pz
+    const R *sz[2];    // sorted z, when the collide moved z (a z-moving virtual drift), else NULL
+    R *cz[2];
     long long n[2];
 };
 template <class R>
@@ -416,6 +418,7 @@ __global__ void k_unsort(const UnsortArgs<R> A) {
     const int p = A.dest[b][i];
 #pragma unroll
     for (int k = 0; k < 5; ++k) A.c[b][k][i] = A.s[b][k][p];
+    if (A.sz[b]) A.cz[b][i] = A.sz[b][p];
 }
 
 }  // namespace octo

@@ -382,9 +382,9 @@ int validate_options(const octo_pic_options &o, std::string &msg) {
             msg = "gaussian_when_luminosity must be 1 or 2";
             return OCTO_ERR_ARG;
         }
-        if (o.virtual_drift != 0) {
-            msg = "the soft-Gaussian solver on this backend implements virtual_drift = :hirata only";
-            return OCTO_ERR_UNSUPPORTED;
+        if (o.virtual_drift < 0 || o.virtual_drift > 2) {
+            msg = "virtual_drift must be 0 (:hirata), 1 (:chromatic) or 2 (:exact)";
+            return OCTO_ERR_ARG;
         }
         if (o.include_sigma_xy) {
             msg = "include_sigma_xy = true (coupled slice covariance) is not implemented by this backend";
@@ -1272,6 +1272,11 @@ void CollideJob::write_back() {
                 const int sk[5] = {0, 1, 2, 3, 5};
                 A.dest[b] = W.dest.p;
                 for (int k = 0; k < 5; ++k) { A.s[b][k] = (const R *)W.s[sk[k]].p; A.c[b][k] = (R *)cc[k]; }
+                // the soft-Gaussian solver's chromatic and exact virtual drifts move z
+                const bool moves_z = c->opt.solver == OCTO_SOLVER_SOFT_GAUSSIAN && c->opt.virtual_drift != 0 &&
+                                     c->opt.longitudinal_kick;
+                A.sz[b] = moves_z ? (const R *)W.s[4].p : nullptr;
+                A.cz[b] = moves_z ? (R *)B.z : nullptr;
                 A.n[b] = B.n;
             }
             const long long nmax = std::max(n1, n2);
@@ -1408,6 +1413,7 @@ void CollideJob::run_gaussian(const SliceInfo &S1, const SliceInfo &S2) {
     A.ignore_centroid[0] = o.ignore_centroid1 != 0;
     A.ignore_centroid[1] = o.ignore_centroid2 != 0;
     A.longitudinal = o.longitudinal_kick != 0;
+    A.drift = o.virtual_drift;
     for (const Front &F : fronts) {
         {
             PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, 2);

@@ -271,7 +271,7 @@ class GaussianPoissonSolver:
     """GaussianPoissonSolver(; ...) -- the soft-Gaussian strong-strong solver (interface.jl:949-1020,
     src/tasks/strongstrong/gaussian.jl): each slice pair kicks each slice with the Bassetti-Erskine field of a
     Gaussian carrying the other slice's transverse moments.  This backend implements the uncoupled form
-    (include_sigma_xy = false) with the Hirata virtual drift on float64 beams."""
+    (include_sigma_xy = false) with the :hirata, :chromatic and :exact virtual drifts on float64 beams."""
     kbb1: Optional[float] = None
     kbb2: Optional[float] = None
     luminosity_scale: Optional[float] = None
@@ -308,8 +308,6 @@ class GaussianPoissonSolver:
     def to_c(self) -> "_lib.OctoPicOptions":
         if self.include_sigma_xy:
             raise ArgumentError("include_sigma_xy = true (coupled slice covariance) is not implemented by this backend")
-        if self.virtual_drift != "hirata":
-            raise ArgumentError(f"virtual_drift = :{self.virtual_drift} is not implemented by this backend (:hirata)")
         # the PIC fields are unused by this solver; a valid small grid keeps the context's setup cheap
         o = PICPoissonSolver(grid=(8, 8), kbb1=self.kbb1, kbb2=self.kbb2, luminosity_scale=self.luminosity_scale,
                              slicing=self.slicing, slicing1=self.slicing1, slicing2=self.slicing2,
@@ -318,7 +316,7 @@ class GaussianPoissonSolver:
         o.gaussian_when_luminosity = int(self.gaussian_when_luminosity)
         o.ignore_centroid1 = int(bool(self.ignore_centroid1))
         o.ignore_centroid2 = int(bool(self.ignore_centroid2))
-        o.virtual_drift = 0
+        o.virtual_drift = {"hirata": 0, "chromatic": 1, "exact": 2}[self.virtual_drift]
         o.include_sigma_xy = 0
         o.min_sigma = float(self.min_sigma)
         return o

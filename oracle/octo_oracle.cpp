@@ -2062,13 +2062,65 @@ bool moments_finite(const SoftMoments &m) {
 
 // _apply_slice_kick_one! (gaussian.jl:152-185): Hirata paraxial drift (strong_beam.jl:559-577) or, without the
 // longitudinal kick, the frozen-longitudinal paraxial drift (:517-531); _cp_covariance_kick (:619-632)
+// The virtual drifts (strong_beam.jl:517-606); without the longitudinal kick the frozen paraxial drift.
+double forward_drift(int kind, bool lk, double &x, double px, double &y, double py, double &z, double &pz, double zo) {
+    if (!lk || kind == 0) {
+        const double S = 0.5 * (z - zo);
+        x += S * px;
+        y += S * py;
+        if (lk) pz -= 0.25 * (px * px + py * py);
+        return S;
+    }
+    if (kind == 1) {
+        const double S = 0.5 * (z - zo);
+        const double phi = std::sqrt(1 - 0.5 * (px * px + py * py) / ((1 + pz) * (1 + pz))) - 1;
+        x += S * px / (1 + pz);
+        y += S * py / (1 + pz);
+        z += 2 * S * phi;
+        pz += (1 + pz) * phi;
+        return S;
+    }
+    const double ps = std::sqrt((1 + pz) * (1 + pz) - px * px - py * py);
+    const double H = 1 + pz - ps;
+    const double rr = 0.5 * H / ps;
+    const double z2 = (z + rr * zo) / (1 + rr);
+    const double S = 0.5 * (z2 - zo);
+    z -= H / ps * S;
+    pz -= 0.5 * H;
+    x += px / ps * S;
+    y += py / ps * S;
+    return S;
+}
+void reverse_drift(int kind, bool lk, double &x, double px, double &y, double py, double &z, double &pz, double zo) {
+    const double S = 0.5 * (z - zo);
+    if (!lk || kind == 0) {
+        x -= S * px;
+        y -= S * py;
+        if (lk) pz += 0.25 * (px * px + py * py);
+        return;
+    }
+    if (kind == 1) {
+        const double psi = std::sqrt(1 + 0.5 * (px * px + py * py) / ((1 + pz) * (1 + pz))) - 1;
+        x -= S * px / (1 + pz);
+        y -= S * py / (1 + pz);
+        z += 2 * S * psi;
+        pz += (1 + pz) * psi;
+        return;
+    }
+    const double H0 = 0.5 * (px * px + py * py) / (1 + pz);
+    const double ps0 = 1 + pz - 0.5 * H0;
+    pz += 0.5 * H0;
+    x -= px / ps0 * S;
+    y -= py / ps0 * S;
+    z += H0 / ps0 * S;
+}
+
+int g_drift_kind = 0;
+
 double apply_one(double *const b[6], int64_t i, const SoftMoments &m, double center, double kbb, bool lk,
                  bool compute_lum) {
     double x = b[0][i], px = b[1][i], y = b[2][i], py = b[3][i], z = b[4][i], pz = b[5][i];
-    double S = 0.5 * (z - center);
-    x += S * px;
-    y += S * py;
-    if (lk) pz -= 0.25 * (px * px + py * py);
+    const double S = forward_drift(g_drift_kind, lk, x, px, y, py, z, pz, center);
     const double xx = x - m.mx + m.mpx * S;
     const double yy = y - m.my + m.mpy * S;
     const double px0 = px, py0 = py, pz0 = pz;
@@ -2090,10 +2142,7 @@ double apply_one(double *const b[6], int64_t i, const SoftMoments &m, double cen
     }
     if (lk) pz += 0.5 * ((px - px0) * m.mpx + (py - py0) * m.mpy);
     else pz = pz0;
-    S = 0.5 * (z - center);
-    x -= S * px;
-    y -= S * py;
-    if (lk) pz += 0.25 * (px * px + py * py);
+    reverse_drift(g_drift_kind, lk, x, px, y, py, z, pz, center);
     b[0][i] = x; b[1][i] = px; b[2][i] = y; b[3][i] = py; b[4][i] = z; b[5][i] = pz;
     return compute_lum ? density * twopi : 0.0;
 }
@@ -2127,12 +2176,15 @@ double slice_kick(double *const b[6], const std::vector<int64_t> &idx, const Sof
 
 extern "C" {
 
-// collide!(::GaussianPoissonSolver, beam1, beam2, ::CPUThreadsBackend) (gaussian.jl:7-57), uncoupled with the
-// Hirata drift; opt supplies the slicings, kbb / luminosity-scale overrides and longitudinal_kick.
+// collide!(::GaussianPoissonSolver, beam1, beam2, ::CPUThreadsBackend) (gaussian.jl:7-57), uncoupled; virtual_drift
+// 0 :hirata, 1 :chromatic, 2 :exact; opt supplies the slicings, kbb / luminosity-scale overrides and
+// longitudinal_kick.
 int oo_gaussian_collide(const oo_options *opt, double min_sigma, int32_t gaussian_when_luminosity,
-                        int32_t ignore_centroid1, int32_t ignore_centroid2, double *b1[6], int64_t n1, double *b2[6],
-                        int64_t n2, const oo_beam_params *p1, const oo_beam_params *p2, double *luminosity) {
+                        int32_t ignore_centroid1, int32_t ignore_centroid2, int32_t virtual_drift, double *b1[6],
+                        int64_t n1, double *b2[6], int64_t n2, const oo_beam_params *p1, const oo_beam_params *p2,
+                        double *luminosity) {
     try {
+        g_drift_kind = virtual_drift;
         std::vector<double> pos1, pos2;
         if (opt->slicing_method1 == 1 && opt->positions1) pos1.assign(opt->positions1, opt->positions1 + opt->nslices1 - 1);
         if (opt->slicing_method2 == 1 && opt->positions2) pos2.assign(opt->positions2, opt->positions2 + opt->nslices2 - 1);

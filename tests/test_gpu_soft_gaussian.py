@@ -32,7 +32,7 @@ def run_both(solver, e, p, turns=1):
     for t in range(turns):
         lum = ob.collide(solver, be, bp, ob.CUDABackend, ob.TrackingContext(turn=t), runtime=rt)
         lum_ref = orc.gaussian_collide(opt, oe, op, pe, pp, solver.min_sigma, solver.gaussian_when_luminosity,
-                                       solver.ignore_centroid1, solver.ignore_centroid2)
+                                       solver.ignore_centroid1, solver.ignore_centroid2, solver.virtual_drift)
         lums.append((lum, lum_ref))
     rt.close()
     return be.numpy(), bp.numpy(), oe, op, lums
@@ -44,6 +44,9 @@ def run_both(solver, e, p, turns=1):
     dict(longitudinal_kick=False),
     dict(ignore_centroid1=True, min_sigma=2e-6),
     dict(kbb1=-3e-4, kbb2=2e-4, luminosity_scale=1.5e20),
+    dict(virtual_drift="chromatic"),
+    dict(virtual_drift="exact"),
+    dict(virtual_drift="exact", longitudinal_kick=False),
 ])
 def test_matches_oracle(kw):
     import octo_b200 as ob
@@ -89,4 +92,4 @@ def test_nonfinite_and_unsupported():
     with pytest.raises(ob.ArgumentError):
         ob.GaussianPoissonSolver(include_sigma_xy=True).to_c()
     with pytest.raises(ob.ArgumentError):
-        ob.GaussianPoissonSolver(virtual_drift="exact").to_c()
+        ob.GaussianPoissonSolver(virtual_drift="paraxial")
