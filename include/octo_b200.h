@@ -99,7 +99,7 @@ typedef struct {
     int32_t gaussian_when_luminosity;  /* 1 or 2: the beam whose slice is the Gaussian the luminosity samples */
     int32_t ignore_centroid1, ignore_centroid2;
     int32_t virtual_drift;             /* 0 = :hirata, 1 = :chromatic, 2 = :exact (strong_beam.jl:20-30, 517-606) */
-    int32_t include_sigma_xy;          /* coupled slice covariance: not built (OCTO_ERR_UNSUPPORTED) */
+    int32_t include_sigma_xy;          /* 1: the full (coupled) transverse slice covariance */
     double min_sigma;                  /* transverse RMS floor, finite and >= 0 */
 } octo_pic_options;
 #define OCTO_SOLVER_PIC 0

@@ -108,8 +108,10 @@ __device__ __forceinline__ void be_moments(double q, int k0, double *m) {
     }
 }
 
+// L (optional): L / D of the rotation term, -x y / v^2 (m1 + eta dr m3 + eta^2 (1.5 m3 - q m4 + dr^2 m5 / 2))
+// (strong_beam.jl:930-932).
 __device__ __noinline__ void be_near_round(double kbb, double v, double eta, double x, double y, double &Kx, double &Ky,
-                                           double &H1, double &H2) {
+                                           double &H1, double &H2, double *L = nullptr) {
     const double q = (x * x + y * y) / (2.0 * v);
     const double dr = (x * x - y * y) / (2.0 * v);
     double m[7];
@@ -133,6 +135,7 @@ __device__ __noinline__ void be_near_round(double kbb, double v, double eta, dou
     const double ueta = u1 + 2.0 * eta * u2 + 3.0 * eta2 * u3;
     H1 = kbb / v * (uv + (1.0 - eta) * ueta);
     H2 = kbb / v * (uv - (1.0 + eta) * ueta);
+    if (L) *L = -x * y / (v * v) * (m[1] + eta * dr * m[3] + eta2 * (1.5 * m[3] - q * m[4] + dr * dr / 2.0 * m[5]));
 }
 
 __device__ __noinline__ double be_near_round_residual(double v, double eta, double x, double y) {
@@ -195,12 +198,18 @@ __device__ __noinline__ void be_elliptic(double s1, double s2, double x, double 
 }
 
 // Principal-axis response (s1 >= s2): kick and kbb-scaled potential Hessians.
+// L (optional): L / D, the rotation term's response (strong_beam.jl:1061-1116).
 __device__ __noinline__ void be_response_principal(double kbb, double s1, double s2, double x, double y, double &Kx,
-                                                   double &Ky, double &H1, double &H2) {
+                                                   double &Ky, double &H1, double &H2, double *L = nullptr) {
     const double v = (s1 * s1 + s2 * s2) / 2.0;
     const double eta = (s1 * s1 - s2 * s2) / (2.0 * v);
     if (eta == 0.0) {
         const double r2 = x * x + y * y;
+        if (L) {  // the eta -> 0 limit, -x y m1(q) / v^2
+            double mm[2];
+            be_moments<2>(r2 / (2.0 * v), 0, mm);
+            *L = -x * y / (v * v) * mm[1];
+        }
         const double u0 = r2 / (2.0 * v);
         const double phi0 = u0 == 0.0 ? 1.0 : -expm1(-u0) / u0;
         Kx = phi0 / v * x;
@@ -231,11 +240,12 @@ __device__ __noinline__ void be_response_principal(double kbb, double s1, double
     double inner, outer;
     be_eta_bounds(inner, outer);
     if (eta <= inner) {
-        be_near_round(kbb, v, eta, x, y, Kx, Ky, H1, H2);
+        be_near_round(kbb, v, eta, x, y, Kx, Ky, H1, H2, L);
         return;
     }
     double Kex, Key, He1, He2;
     be_elliptic(s1, s2, x, y, eta, Kex, Key);
+    const double Le = (Kex * y - Key * x) / (2.0 * v * eta);
     const double expterm = exp(-0.5 * (x * x / (s1 * s1) + y * y / (s2 * s2)));
     if (be_near_axis(s1, s2, x, y, eta)) {
         double k;
@@ -248,18 +258,57 @@ __device__ __noinline__ void be_response_principal(double kbb, double s1, double
     }
     if (eta >= outer) {
         Kx = Kex; Ky = Key; H1 = He1; H2 = He2;
+        if (L) *L = Le;
         return;
     }
     const double invw = 1.0 / (outer - inner), t = (eta - inner) * invw;
     const double w = t * t * t * (10.0 + t * (-15.0 + 6.0 * t));
     const double dw = 30.0 * t * t * (t - 1.0) * (t - 1.0) * invw;
-    double Ksx, Ksy, Hs1, Hs2;
-    be_near_round(kbb, v, eta, x, y, Ksx, Ksy, Hs1, Hs2);
+    double Ksx, Ksy, Hs1, Hs2, Ls;
+    be_near_round(kbb, v, eta, x, y, Ksx, Ksy, Hs1, Hs2, &Ls);
     const double chain = kbb * dw * be_near_round_residual(v, eta, x, y) / v;
     Kx = Ksx + w * (Kex - Ksx);
     Ky = Ksy + w * (Key - Ksy);
     H1 = Hs1 + w * (He1 - Hs1) + (1.0 - eta) * chain;
     H2 = Hs2 + w * (He2 - Hs2) - (1.0 + eta) * chain;
+    if (L) *L = Ls + w * (Le - Ls);
+}
+
+// Round Gaussian of size sigma: the kick (gaussian_beambeam_kick, strong_beam.jl:1139-1146 with eta = 0) and the
+// full potential Hessian (_round_gaussian_hessian, :711-763), for the coupled kick's D = 0 case.
+__device__ __noinline__ void be_round(double kbb, double sigma, double x, double y, double expterm, double &Kx,
+                                      double &Ky, double &Hxx, double &Hxy, double &Hyy) {
+    Kx = Ky = 0.0;
+    if (sigma != 0.0) {
+        const double v = (sigma * sigma + sigma * sigma) / 2.0;
+        const double r2 = x * x + y * y;
+        const double u0 = r2 / (2.0 * v);
+        const double phi0 = u0 == 0.0 ? 1.0 : -expm1(-u0) / u0;
+        Kx = phi0 / v * x;
+        Ky = phi0 / v * y;
+    }
+    const double r2 = x * x + y * y, sigma2 = sigma * sigma;
+    if (r2 == 0.0) {
+        Hxx = Hyy = -kbb / sigma2;
+        Hxy = 0.0;
+        return;
+    }
+    const double u = r2 / (2.0 * sigma2);
+    double f, fp;
+    if (u < 1.0e-2) {
+        const double ph = 1.0 + u * (-1.0 / 2 + u * (1.0 / 6 + u * (-1.0 / 24 + u * (1.0 / 120 + u * (-1.0 / 720 + u * (1.0 / 5040))))));
+        const double dph = -1.0 / 2 + u * (1.0 / 3 + u * (-1.0 / 8 + u * (1.0 / 30 + u * (-1.0 / 144 + u * (1.0 / 840 - u * (1.0 / 5760))))));
+        const double inv = 1.0 / sigma2;
+        f = ph * inv;
+        fp = dph * inv * inv / 2;
+    } else {
+        const double ome = 1 - expterm;
+        f = 2 * ome / r2;
+        fp = 2 * (expterm * u - ome) / (r2 * r2);
+    }
+    Hxx = -kbb * (f + 2 * x * x * fp);
+    Hxy = -kbb * (2 * x * y * fp);
+    Hyy = -kbb * (f + 2 * y * y * fp);
 }
 
 __device__ __forceinline__ void be_response(double kbb, double sigx, double sigy, double x, double y, double &Kx,

@@ -17,7 +17,8 @@ namespace octo {
 
 constexpr int kGaussChunk = 8192;    // particles per partial-sum / kick block
 constexpr int kGaussThreads = 256;
-constexpr int kGaussSums = 10;        // dx, dpx, dy, dpy, dx^2, dpx^2, dy^2, dpy^2, dx dpx, dy dpy
+constexpr int kGaussSums = 14;        // dx, dpx, dy, dpy, dx^2, dpx^2, dy^2, dpy^2, dx dpx, dy dpy, and the
+                                      // coupled dx dy, dx dpy, dpx dy, dpx dpy
 
 // One slice of one beam whose moments a front needs.
 struct GSlice {
@@ -29,6 +30,7 @@ struct GSlice {
 struct GMoments {
     double mx, mpx, my, mpy;            // zero when the beam's centroid is ignored
     double a0, d0, bxx, bypy, qxx, qyy; // var x, var y, cov(x, px), cov(y, py), var px, var py
+    double b0, bxpy, bypx, qxy;         // coupled: cov(x, y), cov(x, py), cov(px, y), cov(px, py); else zero
 };
 // One direction of one pair: the field slice kicked by the Gaussian of the source slice.
 struct GTask {
@@ -53,6 +55,7 @@ struct GaussArgs {
     int ignore_centroid[2];
     int longitudinal;
     int drift;              // virtual drift with the longitudinal kick: 0 Hirata, 1 chromatic, 2 exact
+    int coupled;            // include_sigma_xy: the full transverse covariance
 };
 
 // The virtual drifts to and from the collision point (strong_beam.jl:517-606): forward returns S.  Without the
@@ -119,7 +122,7 @@ __global__ void __launch_bounds__(kGaussThreads) k_gauss_sums(GaussArgs A) {
     const GSlice S = A.slices[bm.x];
     const double *const *c = A.c[S.beam];
     const double x0 = c[0][S.start], px0 = c[1][S.start], y0 = c[2][S.start], py0 = c[3][S.start];
-    double s[kGaussSums] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double s[kGaussSums] = {};
     const long long end = min(S.n, (long long)bm.y + kGaussChunk);
     for (long long k = bm.y + threadIdx.x; k < end; k += kGaussThreads) {
         const long long i = S.start + k;
@@ -127,6 +130,7 @@ __global__ void __launch_bounds__(kGaussThreads) k_gauss_sums(GaussArgs A) {
         s[0] += dx; s[1] += dpx; s[2] += dy; s[3] += dpy;
         s[4] += dx * dx; s[5] += dpx * dpx; s[6] += dy * dy; s[7] += dpy * dpy;
         s[8] += dx * dpx; s[9] += dy * dpy;
+        if (A.coupled) { s[10] += dx * dy; s[11] += dx * dpy; s[12] += dpx * dy; s[13] += dpx * dpy; }
     }
     __shared__ double red[kGaussSums][kGaussThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -162,7 +166,7 @@ __global__ void k_gauss_moments(GaussArgs A, const int *first, const int *count)
         A.mom[si] = M;
         return;
     }
-    double s[kGaussSums] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double s[kGaussSums] = {};
     for (int b = first[si]; b < first[si] + count[si]; ++b)
 #pragma unroll
         for (int q = 0; q < kGaussSums; ++q) s[q] += A.partial[(size_t)b * kGaussSums + q];
@@ -180,6 +184,12 @@ __global__ void k_gauss_moments(GaussArgs A, const int *first, const int *count)
     M.bypy = covypy;
     M.qxx = fmax(spx2, 0.0);
     M.qyy = fmax(spy2, 0.0);
+    if (A.coupled) {
+        M.b0 = fma(-dmx, dmy, s[10] * invn);
+        M.bxpy = fma(-dmx, dmpy, s[11] * invn);
+        M.bypx = fma(-dmpx, dmy, s[12] * invn);
+        M.qxy = fma(-dmpx, dmpy, s[13] * invn);
+    }
     if (!A.ignore_centroid[S.beam]) {
         M.mx = x0 + dmx;
         M.mpx = px0 + dmpx;
@@ -190,6 +200,58 @@ __global__ void k_gauss_moments(GaussArgs A, const int *first, const int *count)
     const double chk = M.mx + M.mpx + M.my + M.mpy + sx2 + sy2 + spx2 + spy2 + covxpx + covypy + (x0 + px0 + y0 + py0);
     if (!isfinite(chk)) record_error(A.status, S.task, OCTO_ERR_NONFINITE, 1);
     A.mom[si] = M;
+}
+
+// The coupled _cp_covariance_kick (strong_beam.jl:634-682): the transported covariance's principal axes, the
+// rotated kick and potential Hessians, the covariance pz term and the rotation term L / D.
+__device__ __noinline__ void coupled_kick(const GMoments &M, double kbb, double S, double xx, double yy, double &px,
+                                          double &py, double &pz, double &density) {
+    const double a = M.a0 - 2 * S * M.bxx + S * S * M.qxx;
+    const double b = M.b0 - S * (M.bxpy + M.bypx) + S * S * M.qxy;
+    const double d = M.d0 - 2 * S * M.bypy + S * S * M.qyy;
+    const double au = 2 * (M.bxx - S * M.qxx);
+    const double bu = M.bxpy + M.bypx - 2 * S * M.qxy;
+    const double du = 2 * (M.bypy - S * M.qyy);
+    const double detA = a * d - b * b;
+    const double twopi = 6.283185307179586476925286766559005768394338;
+    density = 0.0;
+    if (a <= 0 || d <= 0 || detA <= 0) return;
+    const double adiff = a - d;
+    const double D = hypot(adiff, 2 * b);
+    if (D == 0.0) {
+        const double sigma = sqrt((a + d) / 2);
+        const double expterm = exp(-0.5 * (xx * xx + yy * yy) / (sigma * sigma));
+        double Kx, Ky, Hxx, Hxy, Hyy;
+        be_round(kbb, sigma, xx, yy, expterm, Kx, Ky, Hxx, Hxy, Hyy);
+        px += kbb * Kx;
+        py += kbb * Ky;
+        pz += 0.25 * (Hxx * au + 2 * Hxy * bu + Hyy * du);
+        density = expterm / (twopi * sigma * sigma);
+        return;
+    }
+    const double theta = 0.5 * atan2(2 * b, a - d);
+    double sn, cs;
+    sincos(theta, &sn, &cs);
+    const double lambda1 = (a + d + D) / 2, lambda2 = (a + d - D) / 2;
+    const double sig1 = sqrt(lambda1), sig2 = sqrt(lambda2);
+    const double xh = cs * xx + sn * yy;
+    const double yh = -sn * xx + cs * yy;
+    const double eta = D / (a + d);
+    double inner, outer;
+    be_eta_bounds(inner, outer);
+    double Kxh, Kyh, H11, H22, LoD;
+    if (eta <= inner) be_near_round(kbb, (a + d) / 2, eta, xh, yh, Kxh, Kyh, H11, H22, &LoD);
+    else be_response_principal(kbb, sig1, sig2, xh, yh, Kxh, Kyh, H11, H22, &LoD);
+    const double expterm = exp(-0.5 * (xh * xh / lambda1 + yh * yh / lambda2));
+    const double Fxh = kbb * Kxh, Fyh = kbb * Kyh;
+    px += cs * Fxh - sn * Fyh;
+    py += sn * Fxh + cs * Fyh;
+    const double Du = (adiff * (au - du) + 4 * b * bu) / D;
+    const double traceu = au + du;
+    pz += 0.125 * ((H11 + H22) * traceu + (H11 - H22) * Du);
+    const double rotation_projection = (adiff * bu - b * (au - du)) / D;
+    pz -= 0.5 * kbb * rotation_projection * LoD;
+    density = expterm / (twopi * sig1 * sig2);
 }
 
 // _apply_slice_kick_one! (gaussian.jl:152-185) with the uncoupled _cp_covariance_kick (strong_beam.jl:619-632)
@@ -221,7 +283,8 @@ __global__ void __launch_bounds__(kGaussThreads, 3) k_gauss_kick(GaussArgs A) {
         const double au = 2 * (M.bxx - S * M.qxx);
         const double du = 2 * (M.bypy - S * M.qyy);
         double density = 0.0;
-        if (!(a <= 0 || d <= 0)) {
+        if (A.coupled) coupled_kick(M, T.kbb, S, xx, yy, px, py, pz, density);
+        else if (!(a <= 0 || d <= 0)) {
             const double sigx = sqrt(a), sigy = sqrt(d);
             double Kx, Ky, Hxx, Hyy;
             be_response(T.kbb, sigx, sigy, xx, yy, Kx, Ky, Hxx, Hyy);

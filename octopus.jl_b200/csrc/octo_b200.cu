@@ -386,9 +386,9 @@ int validate_options(const octo_pic_options &o, std::string &msg) {
             msg = "virtual_drift must be 0 (:hirata), 1 (:chromatic) or 2 (:exact)";
             return OCTO_ERR_ARG;
         }
-        if (o.include_sigma_xy) {
-            msg = "include_sigma_xy = true (coupled slice covariance) is not implemented by this backend";
-            return OCTO_ERR_UNSUPPORTED;
+        if (o.include_sigma_xy != 0 && o.include_sigma_xy != 1) {
+            msg = "include_sigma_xy must be 0 or 1";
+            return OCTO_ERR_ARG;
         }
         if (o.precision != 0 || o.gaussian) {
             msg = "the soft-Gaussian solver runs on float64 beams, without the PIC hybrid";
@@ -1414,6 +1414,7 @@ void CollideJob::run_gaussian(const SliceInfo &S1, const SliceInfo &S2) {
     A.ignore_centroid[1] = o.ignore_centroid2 != 0;
     A.longitudinal = o.longitudinal_kick != 0;
     A.drift = o.virtual_drift;
+    A.coupled = o.include_sigma_xy;
     for (const Front &F : fronts) {
         {
             PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, 2);

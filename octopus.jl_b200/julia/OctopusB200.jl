@@ -89,8 +89,8 @@ end
     B200GaussianPoissonSolver(; kwargs...)
 
 `GaussianPoissonSolver(; kwargs...)`, the soft-Gaussian strong-strong solver (interface.jl:949-1020,
-gaussian.jl), run on libocto_b200: the uncoupled covariance (`include_sigma_xy = false`) with the :hirata,
-:chromatic or :exact virtual drift, on Float64 beams.  `pic` only carries the slicings, kbb and luminosity-scale overrides and
+gaussian.jl), run on libocto_b200: the uncoupled or coupled (`include_sigma_xy`) covariance with the
+:hirata, :chromatic or :exact virtual drift, on Float64 beams.  `pic` only carries the slicings, kbb and luminosity-scale overrides and
 `longitudinal_kick` into the shared options struct.
 """
 struct B200GaussianPoissonSolver{T<:Real} <: AbstractPoissonSolver
@@ -99,8 +99,6 @@ struct B200GaussianPoissonSolver{T<:Real} <: AbstractPoissonSolver
 end
 function B200GaussianPoissonSolver(; kwargs...)
     g = Octopus.GaussianPoissonSolver(; kwargs...)
-    g.include_sigma_xy && throw(ArgumentError(
-        "include_sigma_xy = true (the coupled slice covariance) is not implemented by the B200 backend"))
     g.virtual_drift isa Union{Octopus.HirataParaxialDrift,Octopus.ChromaticDrift,Octopus.ExactHamiltonianDrift} ||
         throw(ArgumentError("the B200 backend's soft-Gaussian solver implements the :hirata, :chromatic and :exact drifts"))
     pic = PICPoissonSolver(; grid=(8, 8), kbb1=g.kbb1, kbb2=g.kbb2, luminosity_scale=g.luminosity_scale,
@@ -154,7 +152,7 @@ function _options(p::PICPoissonSolver, keep::Vector{Any}, precision::Integer=0, 
         Int32(soft === nothing ? 0 : soft.ignore_centroid1), Int32(soft === nothing ? 0 : soft.ignore_centroid2),
         Int32(soft === nothing ? 0 : soft.virtual_drift isa Octopus.ChromaticDrift ? 1 :
               soft.virtual_drift isa Octopus.ExactHamiltonianDrift ? 2 : 0),
-        Int32(0), soft === nothing ? 0.0 : Float64(soft.min_sigma))
+        Int32(soft === nothing ? 0 : soft.include_sigma_xy), soft === nothing ? 0.0 : Float64(soft.min_sigma))
 end
 
 """Context: device workspaces and the slice-pair Green cache (the twin of task.runtime_cache)."""

@@ -270,8 +270,8 @@ class GaussianPICPoissonSolver:
 class GaussianPoissonSolver:
     """GaussianPoissonSolver(; ...) -- the soft-Gaussian strong-strong solver (interface.jl:949-1020,
     src/tasks/strongstrong/gaussian.jl): each slice pair kicks each slice with the Bassetti-Erskine field of a
-    Gaussian carrying the other slice's transverse moments.  This backend implements the uncoupled form
-    (include_sigma_xy = false) with the :hirata, :chromatic and :exact virtual drifts on float64 beams."""
+    Gaussian carrying the other slice's transverse moments, uncoupled or with the full transverse covariance
+    (include_sigma_xy), with the :hirata, :chromatic and :exact virtual drifts, on float64 beams."""
     kbb1: Optional[float] = None
     kbb2: Optional[float] = None
     luminosity_scale: Optional[float] = None
@@ -306,8 +306,6 @@ class GaussianPoissonSolver:
         return self.slicing2 if self.slicing2 is not None else self.slicing
 
     def to_c(self) -> "_lib.OctoPicOptions":
-        if self.include_sigma_xy:
-            raise ArgumentError("include_sigma_xy = true (coupled slice covariance) is not implemented by this backend")
         # the PIC fields are unused by this solver; a valid small grid keeps the context's setup cheap
         o = PICPoissonSolver(grid=(8, 8), kbb1=self.kbb1, kbb2=self.kbb2, luminosity_scale=self.luminosity_scale,
                              slicing=self.slicing, slicing1=self.slicing1, slicing2=self.slicing2,
@@ -317,6 +315,6 @@ class GaussianPoissonSolver:
         o.ignore_centroid1 = int(bool(self.ignore_centroid1))
         o.ignore_centroid2 = int(bool(self.ignore_centroid2))
         o.virtual_drift = {"hirata": 0, "chromatic": 1, "exact": 2}[self.virtual_drift]
-        o.include_sigma_xy = 0
+        o.include_sigma_xy = int(bool(self.include_sigma_xy))
         o.min_sigma = float(self.min_sigma)
         return o

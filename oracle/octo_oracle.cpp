@@ -1999,9 +1999,11 @@ inline void chunk_bounds(int64_t n, int nchunks, int chunk1, int64_t &lo, int64_
 
 struct SoftMoments {
     double mx, mpx, my, mpy;                  // after ignore_centroid
-    double a0, d0, bxx, bypy, qxx, qyy;       // StrongTransverseMoments{T,false}
+    double a0, d0, bxx, bypy, qxx, qyy;       // StrongTransverseMoments
+    double b0, bxpy, bypx, qxy;               // its coupled entries (zero when uncoupled)
     double sx, sy, spx, spy, covxpx, covypy;  // for the finiteness check
 };
+bool g_coupled = false;
 
 // _slice_transverse_moments (slicing.jl:670-770), uncoupled
 SoftMoments slice_moments(double *const b[6], const std::vector<int64_t> &idx, bool ignore_centroid, double min_sigma) {
@@ -2015,7 +2017,7 @@ SoftMoments slice_moments(double *const b[6], const std::vector<int64_t> &idx, b
     }
     const int64_t f = idx[0];
     const double x0 = b[0][f], px0 = b[1][f], y0 = b[2][f], py0 = b[3][f];
-    double s[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double s[14] = {};
     auto acc = [&](double *t, int64_t lo, int64_t hi) {
         for (int64_t p = lo; p < hi; ++p) {
             const int64_t i = idx[p];
@@ -2023,17 +2025,18 @@ SoftMoments slice_moments(double *const b[6], const std::vector<int64_t> &idx, b
             t[0] += dx; t[1] += dpx; t[2] += dy; t[3] += dpy;
             t[4] += dx * dx; t[5] += dpx * dpx; t[6] += dy * dy; t[7] += dpy * dpy;
             t[8] += dx * dpx; t[9] += dy * dpy;
+            if (g_coupled) { t[10] += dx * dy; t[11] += dx * dpy; t[12] += dpx * dy; t[13] += dpx * dpy; }
         }
     };
     if (n < PARALLEL_MOMENT_MIN) {
         acc(s, 0, n);
     } else {
         for (int ch = 1; ch <= REDUCTION_CHUNKS; ++ch) {
-            double t[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+            double t[14] = {};
             int64_t lo, hi;
             chunk_bounds(n, REDUCTION_CHUNKS, ch, lo, hi);
             acc(t, lo, hi);
-            for (int q = 0; q < 10; ++q) s[q] += t[q];
+            for (int q = 0; q < 14; ++q) s[q] += t[q];
         }
     }
     const double invn = 1.0 / (double)n;
@@ -2045,6 +2048,12 @@ SoftMoments slice_moments(double *const b[6], const std::vector<int64_t> &idx, b
     const double varx = jmax(sx2, floor2), vary = jmax(sy2, floor2);
     M.a0 = varx; M.d0 = vary; M.bxx = covxpx; M.bypy = covypy;
     M.qxx = jmax(spx2, 0.0); M.qyy = jmax(spy2, 0.0);
+    if (g_coupled) {
+        M.b0 = std::fma(-dmx, dmy, s[10] * invn);
+        M.bxpy = std::fma(-dmx, dmpy, s[11] * invn);
+        M.bypx = std::fma(-dmpx, dmy, s[12] * invn);
+        M.qxy = std::fma(-dmpx, dmpy, s[13] * invn);
+    }
     if (ignore_centroid) { mx = 0; mpx = 0; my = 0; mpy = 0; }
     M.mx = mx; M.mpx = mpx; M.my = my; M.mpy = mpy;
     M.sx = std::sqrt(varx); M.sy = std::sqrt(vary);
@@ -2124,6 +2133,58 @@ double apply_one(double *const b[6], int64_t i, const SoftMoments &m, double cen
     const double xx = x - m.mx + m.mpx * S;
     const double yy = y - m.my + m.mpy * S;
     const double px0 = px, py0 = py, pz0 = pz;
+    const double twopi_c = 6.283185307179586476925286766559005768394338;
+    if (g_coupled) {  // _cp_covariance_kick, coupled (strong_beam.jl:634-682)
+        double density = 0.0;
+        const double a = m.a0 - 2 * S * m.bxx + S * S * m.qxx;
+        const double bb = m.b0 - S * (m.bxpy + m.bypx) + S * S * m.qxy;
+        const double d = m.d0 - 2 * S * m.bypy + S * S * m.qyy;
+        const double au = 2 * (m.bxx - S * m.qxx);
+        const double bu = m.bxpy + m.bypx - 2 * S * m.qxy;
+        const double du = 2 * (m.bypy - S * m.qyy);
+        const double detA = a * d - bb * bb;
+        if (!(a <= 0 || d <= 0 || detA <= 0)) {
+            const double adiff = a - d;
+            const double D = std::hypot(adiff, 2 * bb);
+            if (D == 0.0) {
+                const double sigma = std::sqrt((a + d) / 2);
+                const double expterm = std::exp(-0.5 * (xx * xx + yy * yy) / (sigma * sigma));
+                double Kx, Ky, Hxx, Hxy, Hyy;
+                be::round_kick_hessian(kbb, sigma, xx, yy, expterm, Kx, Ky, Hxx, Hxy, Hyy);
+                px += kbb * Kx;
+                py += kbb * Ky;
+                pz += 0.25 * (Hxx * au + 2 * Hxy * bu + Hyy * du);
+                density = expterm / (twopi_c * sigma * sigma);
+            } else {
+                const double theta = 0.5 * std::atan2(2 * bb, a - d);
+                const double c = std::cos(theta), sn = std::sin(theta);
+                const double lambda1 = (a + d + D) / 2, lambda2 = (a + d - D) / 2;
+                const double sig1 = std::sqrt(lambda1), sig2 = std::sqrt(lambda2);
+                const double xh = c * xx + sn * yy, yh = -sn * xx + c * yy;
+                const double eta = D / (a + d);
+                double inner, outer;
+                be::eta_bounds(inner, outer);
+                double Kxh, Kyh, H11, H22, LoD;
+                if (eta <= inner) be::near_round_series(kbb, (a + d) / 2, eta, xh, yh, Kxh, Kyh, H11, H22, &LoD);
+                else be::response_principal(kbb, sig1, sig2, xh, yh, Kxh, Kyh, H11, H22, &LoD);
+                const double expterm = std::exp(-0.5 * (xh * xh / lambda1 + yh * yh / lambda2));
+                const double Fxh = kbb * Kxh, Fyh = kbb * Kyh;
+                px += c * Fxh - sn * Fyh;
+                py += sn * Fxh + c * Fyh;
+                const double Du = (adiff * (au - du) + 4 * bb * bu) / D;
+                const double traceu = au + du;
+                pz += 0.125 * ((H11 + H22) * traceu + (H11 - H22) * Du);
+                const double rotation_projection = (adiff * bu - bb * (au - du)) / D;
+                pz -= 0.5 * kbb * rotation_projection * LoD;
+                density = expterm / (twopi_c * sig1 * sig2);
+            }
+        }
+        if (lk) pz += 0.5 * ((px - px0) * m.mpx + (py - py0) * m.mpy);
+        else pz = pz0;
+        reverse_drift(g_drift_kind, lk, x, px, y, py, z, pz, center);
+        b[0][i] = x; b[1][i] = px; b[2][i] = y; b[3][i] = py; b[4][i] = z; b[5][i] = pz;
+        return compute_lum ? density * twopi_c : 0.0;
+    }
     const double a = m.a0 - 2 * S * m.bxx + S * S * m.qxx;
     const double d = m.d0 - 2 * S * m.bypy + S * S * m.qyy;
     const double au = 2 * (m.bxx - S * m.qxx);
@@ -2176,15 +2237,16 @@ double slice_kick(double *const b[6], const std::vector<int64_t> &idx, const Sof
 
 extern "C" {
 
-// collide!(::GaussianPoissonSolver, beam1, beam2, ::CPUThreadsBackend) (gaussian.jl:7-57), uncoupled; virtual_drift
-// 0 :hirata, 1 :chromatic, 2 :exact; opt supplies the slicings, kbb / luminosity-scale overrides and
+// collide!(::GaussianPoissonSolver, beam1, beam2, ::CPUThreadsBackend) (gaussian.jl:7-57); include_sigma_xy selects
+// the coupled covariance; virtual_drift 0 :hirata, 1 :chromatic, 2 :exact; opt supplies the slicings, kbb / luminosity-scale overrides and
 // longitudinal_kick.
 int oo_gaussian_collide(const oo_options *opt, double min_sigma, int32_t gaussian_when_luminosity,
-                        int32_t ignore_centroid1, int32_t ignore_centroid2, int32_t virtual_drift, double *b1[6],
-                        int64_t n1, double *b2[6], int64_t n2, const oo_beam_params *p1, const oo_beam_params *p2,
-                        double *luminosity) {
+                        int32_t ignore_centroid1, int32_t ignore_centroid2, int32_t virtual_drift,
+                        int32_t include_sigma_xy, double *b1[6], int64_t n1, double *b2[6], int64_t n2,
+                        const oo_beam_params *p1, const oo_beam_params *p2, double *luminosity) {
     try {
         g_drift_kind = virtual_drift;
+        g_coupled = include_sigma_xy != 0;
         std::vector<double> pos1, pos2;
         if (opt->slicing_method1 == 1 && opt->positions1) pos1.assign(opt->positions1, opt->positions1 + opt->nslices1 - 1);
         if (opt->slicing_method2 == 1 && opt->positions2) pos2.assign(opt->positions2, opt->positions2 + opt->nslices2 - 1);

@@ -124,11 +124,11 @@ int64_t oo_dropped(void *ctx);
 int64_t oo_pair_trace(void *ctx, int32_t *pi, int32_t *pj, double *lum, int64_t cap);
 const char *oo_last_error(void *ctx);
 /* collide!(::GaussianPoissonSolver, ...) (src/tasks/strongstrong/gaussian.jl:7-185): the soft-Gaussian solver,
-   uncoupled; virtual_drift 0 :hirata, 1 :chromatic, 2 :exact; opt gives the slicings, kbb / luminosity-scale overrides and longitudinal_kick. */
+   include_sigma_xy: the coupled covariance; virtual_drift 0 :hirata, 1 :chromatic, 2 :exact; opt gives the slicings, kbb / luminosity-scale overrides and longitudinal_kick. */
 int oo_gaussian_collide(const oo_options *opt, double min_sigma, int32_t gaussian_when_luminosity,
-                        int32_t ignore_centroid1, int32_t ignore_centroid2, int32_t virtual_drift, double *b1[6],
-                        int64_t n1, double *b2[6], int64_t n2, const oo_beam_params *p1, const oo_beam_params *p2,
-                        double *luminosity);
+                        int32_t ignore_centroid1, int32_t ignore_centroid2, int32_t virtual_drift,
+                        int32_t include_sigma_xy, double *b1[6], int64_t n1, double *b2[6], int64_t n2,
+                        const oo_beam_params *p1, const oo_beam_params *p2, double *luminosity);
 const char *oo_gaussian_last_error(void);
 /* Line elements (the layout of octo_element in the product header; kinds 1..9: Linear6D, thin crab
    cavity, Lorentz boost, reverse boost, chromaticity kick, lumped radiation, crab dispersion, momentum

@@ -128,7 +128,7 @@ def lib():
         L.oo_last_error.argtypes = [vp]
         L.oo_linear6d.argtypes = [P(d)] + [P(d)] * 6 + [i64]
         L.oo_linear6d_matrix.argtypes = [P(d), P(d), P(d), P(d)]
-        L.oo_gaussian_collide.argtypes = [P(OOOptions), d, i32, i32, i32, i32, P(P(d)), i64, P(P(d)), i64,
+        L.oo_gaussian_collide.argtypes = [P(OOOptions), d, i32, i32, i32, i32, i32, P(P(d)), i64, P(P(d)), i64,
                                           P(OOBeamParams), P(OOBeamParams), P(d)]
         L.oo_gaussian_collide.restype = C.c_int
         L.oo_gaussian_last_error.restype = C.c_char_p
@@ -471,7 +471,7 @@ def _seq_sum(v):
 
 def gaussian_collide(options: "OracleOptions", beam1: np.ndarray, beam2: np.ndarray, p1, p2, min_sigma=0.0,
                      gaussian_when_luminosity=2, ignore_centroid1=False, ignore_centroid2=False,
-                     virtual_drift="hirata") -> float:
+                     virtual_drift="hirata", include_sigma_xy=False) -> float:
     """collide!(::GaussianPoissonSolver, ...) (src/tasks/strongstrong/gaussian.jl) in place on (6, n) float64
     beams; options gives the slicings, kbb / luminosity-scale overrides and longitudinal_kick."""
     P = C.POINTER(C.c_double)
@@ -481,7 +481,8 @@ def gaussian_collide(options: "OracleOptions", beam1: np.ndarray, beam2: np.ndar
     lum = C.c_double(np.nan)
     rc = lib().oo_gaussian_collide(C.byref(copt), float(min_sigma), int(gaussian_when_luminosity),
                                    int(bool(ignore_centroid1)), int(bool(ignore_centroid2)),
-                                   {"hirata": 0, "chromatic": 1, "exact": 2}[virtual_drift], a1, beam1.shape[1], a2,
+                                   {"hirata": 0, "chromatic": 1, "exact": 2}[virtual_drift], int(bool(include_sigma_xy)),
+                                   a1, beam1.shape[1], a2,
                                    beam2.shape[1], C.byref(p1), C.byref(p2), C.byref(lum))
     if rc != OK:
         raise OracleErrorPy(rc, lib().oo_gaussian_last_error().decode())

@@ -173,7 +173,7 @@ inline void moments(double q, int k0, int cnt, double *m) {
 
 // Near-round series: kick (Kx, Ky) and Hessians (H1, H2) of the potential, kbb-scaled.
 inline void near_round_series(double kbb, double v, double eta, double x, double y, double &Kx, double &Ky,
-                              double &H1, double &H2) {
+                              double &H1, double &H2, double *L = nullptr) {
     const double q = (x * x + y * y) / (2.0 * v);
     const double dr = (x * x - y * y) / (2.0 * v);
     double m[7];
@@ -197,6 +197,8 @@ inline void near_round_series(double kbb, double v, double eta, double x, double
     const double ueta = u1 + 2.0 * eta * u2 + 3.0 * eta2 * u3;
     H1 = kbb / v * (uv + (1.0 - eta) * ueta);
     H2 = kbb / v * (uv - (1.0 + eta) * ueta);
+    // L / D of the coupled kick's rotation term (strong_beam.jl:930-932)
+    if (L) *L = -x * y / (v * v) * (m[1] + eta * dr * m[3] + eta2 * (1.5 * m[3] - q * m[4] + dr * dr / 2.0 * m[5]));
 }
 
 // Exact-minus-series potential through eta^6 (the blend's chain-rule term).
@@ -262,11 +264,16 @@ inline void elliptic_kick(double s1, double s2, double x, double y, double eta, 
 
 // Principal-axis response (sig1 >= sig2): kick (Kx, Ky) and kbb-scaled potential Hessians (H1, H2).
 inline void response_principal(double kbb, double s1, double s2, double x, double y, double &Kx, double &Ky,
-                               double &H1, double &H2) {
+                               double &H1, double &H2, double *L = nullptr) {
     const double v = (s1 * s1 + s2 * s2) / 2.0;
     const double eta = (s1 * s1 - s2 * s2) / (2.0 * v);
     if (eta == 0.0) {
         const double r2 = x * x + y * y;
+        if (L) {  // strong_beam.jl:1091-1102: the eta -> 0 limit of L / D
+            double mm[2];
+            moments(r2 / (2.0 * v), 0, 2, mm);
+            *L = -x * y / (v * v) * mm[1];
+        }
         const double u0 = r2 / (2.0 * v);
         const double phi0 = u0 == 0.0 ? 1.0 : -std::expm1(-u0) / u0;
         const double scale = phi0 / v;
@@ -299,11 +306,12 @@ inline void response_principal(double kbb, double s1, double s2, double x, doubl
     double inner, outer;
     eta_bounds(inner, outer);
     if (eta <= inner) {
-        near_round_series(kbb, v, eta, x, y, Kx, Ky, H1, H2);
+        near_round_series(kbb, v, eta, x, y, Kx, Ky, H1, H2, L);
         return;
     }
     double Kex, Key, He1, He2;
     elliptic_kick(s1, s2, x, y, eta, Kex, Key);
+    const double Le = (Kex * y - Key * x) / (2.0 * v * eta);
     const double expterm = std::exp(-0.5 * (x * x / (s1 * s1) + y * y / (s2 * s2)));
     if (near_axis(s1, s2, x, y, eta)) {
         double k;
@@ -316,17 +324,56 @@ inline void response_principal(double kbb, double s1, double s2, double x, doubl
     }
     if (eta >= outer) {
         Kx = Kex; Ky = Key; H1 = He1; H2 = He2;
+        if (L) *L = Le;
         return;
     }
     double w, dw;
     blend(eta, w, dw);
-    double Ksx, Ksy, Hs1, Hs2;
-    near_round_series(kbb, v, eta, x, y, Ksx, Ksy, Hs1, Hs2);
+    double Ksx, Ksy, Hs1, Hs2, Ls;
+    near_round_series(kbb, v, eta, x, y, Ksx, Ksy, Hs1, Hs2, &Ls);
     const double chain = kbb * dw * near_round_residual(v, eta, x, y) / v;
     Kx = Ksx + w * (Kex - Ksx);
     Ky = Ksy + w * (Key - Ksy);
     H1 = Hs1 + w * (He1 - Hs1) + (1.0 - eta) * chain;
     H2 = Hs2 + w * (He2 - Hs2) - (1.0 + eta) * chain;
+    if (L) *L = Ls + w * (Le - Ls);
+}
+
+// Round Gaussian kick (gaussian_beambeam_kick with equal sizes) and full Hessian (_round_gaussian_hessian,
+// strong_beam.jl:711-763).
+inline void round_kick_hessian(double kbb, double sigma, double x, double y, double expterm, double &Kx, double &Ky,
+                               double &Hxx, double &Hxy, double &Hyy) {
+    Kx = Ky = 0.0;
+    if (sigma != 0.0) {
+        const double v = (sigma * sigma + sigma * sigma) / 2.0;
+        const double r2 = x * x + y * y;
+        const double u0 = r2 / (2.0 * v);
+        const double phi0 = u0 == 0.0 ? 1.0 : -std::expm1(-u0) / u0;
+        Kx = phi0 / v * x;
+        Ky = phi0 / v * y;
+    }
+    const double r2 = x * x + y * y, sigma2 = sigma * sigma;
+    if (r2 == 0.0) {
+        Hxx = Hyy = -kbb / sigma2;
+        Hxy = 0.0;
+        return;
+    }
+    const double u = r2 / (2.0 * sigma2);
+    double f, fp;
+    if (u < 1.0e-2) {
+        const double ph = 1.0 + u * (-1.0 / 2 + u * (1.0 / 6 + u * (-1.0 / 24 + u * (1.0 / 120 + u * (-1.0 / 720 + u * (1.0 / 5040))))));
+        const double dph = -1.0 / 2 + u * (1.0 / 3 + u * (-1.0 / 8 + u * (1.0 / 30 + u * (-1.0 / 144 + u * (1.0 / 840 - u * (1.0 / 5760))))));
+        const double inv = 1.0 / sigma2;
+        f = ph * inv;
+        fp = dph * inv * inv / 2;
+    } else {
+        const double ome = 1 - expterm;
+        f = 2 * ome / r2;
+        fp = 2 * (expterm * u - ome) / (r2 * r2);
+    }
+    Hxx = -kbb * (f + 2 * x * x * fp);
+    Hxy = -kbb * (2 * x * y * fp);
+    Hyy = -kbb * (f + 2 * y * y * fp);
 }
 
 // Kick and Hessians of a (sigx, sigy) Gaussian at (x, y): the larger sigma is the principal axis.

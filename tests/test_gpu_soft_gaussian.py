@@ -32,7 +32,8 @@ def run_both(solver, e, p, turns=1):
     for t in range(turns):
         lum = ob.collide(solver, be, bp, ob.CUDABackend, ob.TrackingContext(turn=t), runtime=rt)
         lum_ref = orc.gaussian_collide(opt, oe, op, pe, pp, solver.min_sigma, solver.gaussian_when_luminosity,
-                                       solver.ignore_centroid1, solver.ignore_centroid2, solver.virtual_drift)
+                                       solver.ignore_centroid1, solver.ignore_centroid2, solver.virtual_drift,
+                                       solver.include_sigma_xy)
         lums.append((lum, lum_ref))
     rt.close()
     return be.numpy(), bp.numpy(), oe, op, lums
@@ -47,6 +48,8 @@ def run_both(solver, e, p, turns=1):
     dict(virtual_drift="chromatic"),
     dict(virtual_drift="exact"),
     dict(virtual_drift="exact", longitudinal_kick=False),
+    dict(include_sigma_xy=True),
+    dict(include_sigma_xy=True, virtual_drift="chromatic", min_sigma=2e-6),
 ])
 def test_matches_oracle(kw):
     import octo_b200 as ob
@@ -89,7 +92,5 @@ def test_nonfinite_and_unsupported():
     with pytest.raises(ob.CollisionError) as err:
         ob.collide(solver, be, bp)
     assert err.value.code == 1 and "source" in str(err.value)
-    with pytest.raises(ob.ArgumentError):
-        ob.GaussianPoissonSolver(include_sigma_xy=True).to_c()
     with pytest.raises(ob.ArgumentError):
         ob.GaussianPoissonSolver(virtual_drift="paraxial")

@@ -46,3 +46,44 @@ def test_far_kick_is_point_charge():
     assert abs(b1[1, 0] / (kbb * 2 / 2e-3) - 1) < 1e-4
     # the y kick is the sampled centroid's offset (~1e-8 in y) seen from 2 mm
     assert abs(b1[3, 0]) < 1e-4 * abs(b1[1, 0])
+
+
+def test_coupled_kick_is_rotated_bassetti_erskine():
+    """include_sigma_xy: a Gaussian tilted in x-y kicks as the principal-axis Bassetti-Erskine field of its
+    covariance's eigenframe, rotated back (strong_beam.jl:634-682 at S = 0)."""
+    rng = np.random.default_rng(4)
+    n2 = 200_000
+    phi = 0.35
+    u, v = rng.normal(size=n2) * 30e-6, rng.normal(size=n2) * 8e-6
+    b2 = np.zeros((6, n2))
+    b2[0] = np.cos(phi) * u - np.sin(phi) * v
+    b2[2] = np.sin(phi) * u + np.cos(phi) * v
+    pts = [(12e-6, -5e-6), (-40e-6, 30e-6), (3e-6, 2e-6)]
+    b1 = np.zeros((6, len(pts)))
+    for k, (x, y) in enumerate(pts):
+        b1[0, k], b1[2, k] = x, y
+    kbb = 1e-4
+    opt = orc.OracleOptions(nslices1=1, nslices2=1, kbb1=kbb, kbb2=0.0, longitudinal_kick=False)
+    p = orc.beam_params(1.0, orc.PMASS_EV, 275e9, 1e11)
+    got = b1.copy()
+    orc.gaussian_collide(opt, got, b2.copy(), p, p, include_sigma_xy=True)
+    mx, my = b2[0].mean(), b2[2].mean()
+    C = np.cov(np.stack([b2[0], b2[2]]), bias=True)
+    w, V = np.linalg.eigh(C)
+    s1, s2 = np.sqrt(w[1]), np.sqrt(w[0])
+    e1 = V[:, 1]
+    for k, (x, y) in enumerate(pts):
+        dx, dy = x - mx, y - my
+        xh, yh = e1[0] * dx + e1[1] * dy, -e1[1] * dx + e1[0] * dy
+        kx, ky, _, _ = orc.be_response(0.0, s1, s2, xh, yh)
+        fx = kbb * (e1[0] * kx - e1[1] * ky)
+        fy = kbb * (e1[1] * kx + e1[0] * ky)
+        assert abs(got[1, k] - fx) < 1e-9 * abs(fx) + 1e-15 and abs(got[3, k] - fy) < 1e-9 * abs(fy) + 1e-15, \
+            (k, got[1, k], fx, got[3, k], fy)
+    # with no tilt the coupled and uncoupled kicks agree
+    b2r = np.zeros((6, n2))
+    b2r[0], b2r[2] = u, v
+    g1, g2 = b1.copy(), b1.copy()
+    orc.gaussian_collide(opt, g1, b2r.copy(), p, p, include_sigma_xy=True)
+    orc.gaussian_collide(opt, g2, b2r.copy(), p, p)
+    np.testing.assert_allclose(g1[1], g2[1], rtol=2e-3)
