@@ -36,9 +36,12 @@ int main(void) {
   printf("octo_pic_options size %zu\n", sizeof(octo_pic_options));
   printf("octo_beam size %zu\n", sizeof(octo_beam));
   printf("octo_collide_report size %zu\n", sizeof(octo_collide_report));
+  printf("octo_element size %zu\n", sizeof(octo_element));
   F(octo_pic_options, grid_extent_sigma) F(octo_pic_options, longitudinal_kick) F(octo_pic_options, positions1)
   F(octo_pic_options, kbb1) F(octo_pic_options, precision) F(octo_beam, x) F(octo_beam, pz)
+  F(octo_pic_options, solver) F(octo_pic_options, include_sigma_xy) F(octo_pic_options, min_sigma)
   F(octo_collide_report, turn) F(octo_collide_report, kernel_launches)
+  F(octo_element, rng_id) F(octo_element, p)
   return 0;
 }
 """
@@ -57,11 +60,12 @@ def test_ctypes_structures_match_header_layout():
     assert lay[("octo_pic_options", "size")] == C.sizeof(_lib.OctoPicOptions)
     assert lay[("octo_beam", "size")] == C.sizeof(_lib.OctoBeam)
     assert lay[("octo_collide_report", "size")] == C.sizeof(_lib.OctoCollideReport)
+    assert lay[("octo_element", "size")] == C.sizeof(_lib.OctoElement)
     for (t, m), v in lay.items():
         if m == "size":
             continue
         cls = {"octo_pic_options": _lib.OctoPicOptions, "octo_beam": _lib.OctoBeam,
-               "octo_collide_report": _lib.OctoCollideReport}[t]
+               "octo_collide_report": _lib.OctoCollideReport, "octo_element": _lib.OctoElement}[t]
         assert getattr(cls, m).offset == v, (t, m)
 
 
@@ -104,3 +108,21 @@ def test_gpu_backend_rejects_what_it_does_not_implement():
         assert ob.PICPoissonSolver(slicing=sl, grid=g).to_c().nx == g[0]
     o = ob.PICPoissonSolver(slicing=sl, deposit_method="TSC", field_derivative="fourth").to_c()
     assert (o.nx, o.deposit_method, o.field_derivative, o.nslices1) == (128, 1, 4, 3)
+
+
+def test_soft_gaussian_solver_options():
+    """GaussianPoissonSolver's keyword validation (interface.jl:976-1000) and its C options."""
+    import math
+    import octo_b200 as ob
+    for kw in (dict(min_sigma=-1.0), dict(min_sigma=math.inf), dict(gaussian_when_luminosity=3),
+               dict(batch_mode="parallel"), dict(virtual_drift="paraxial")):
+        with pytest.raises(ob.ArgumentError):
+            ob.GaussianPoissonSolver(**kw)
+    s = ob.GaussianPoissonSolver(slicing1=ob.LongitudinalSlicing(nslices=3, method="normal_quantile"),
+                                 slicing2=ob.LongitudinalSlicing(nslices=5, method="normal_quantile"),
+                                 min_sigma=2e-6, gaussian_when_luminosity=1, ignore_centroid2=True,
+                                 virtual_drift="exact", include_sigma_xy=True, kbb1=1e-4)
+    o = s.to_c()
+    assert (o.solver, o.nslices1, o.nslices2, o.gaussian_when_luminosity) == (_lib.SOLVER_SOFT_GAUSSIAN, 3, 5, 1)
+    assert (o.ignore_centroid1, o.ignore_centroid2, o.virtual_drift, o.include_sigma_xy) == (0, 1, 2, 1)
+    assert o.min_sigma == 2e-6 and o.has_kbb1 == 1 and o.kbb1 == 1e-4 and o.has_kbb2 == 0
