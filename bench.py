@@ -322,9 +322,11 @@ def run_ours(args, rank, world, local_rank):
         fast = time_form(solver)
         fast_coarse = time_form(solver_coarse)
         shape32 = fast["shape"]
-    lines = None if args.no_line else time_lines(ob, e0, p0, args, stream, barrier)
+    # the oracle's CPU timings of these passes run once, on a single-GPU run
+    cpu_side = world == 1 and not args.no_cpu_baseline
+    lines = None if args.no_line else time_lines(ob, e0, p0, args, stream, barrier, cpu_side)
     observer = None if args.no_line else time_observer(ob, e0, p0, args, stream)
-    soft = None if args.no_line else time_soft_gaussian(ob, e0, p0, me, mp, rt, local_rank, args, stream)
+    soft = None if args.no_line else time_soft_gaussian(ob, e0, p0, me, mp, rt, local_rank, args, stream, cpu_side)
     clk = clocks.stop()
 
     # long-term tracking of both forms from the same beams (outside every timed region, one GPU only):
@@ -455,7 +457,7 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
-def time_lines(ob, e0, p0, args, stream, barrier):
+def time_lines(ob, e0, p0, args, stream, barrier, cpu_side=True):
     """Line tracking between collisions on the same beams: both rings of the strong-strong example's lattice
     (before the collision: inverse crab transport, crab cavity, crab-to-IP transport, Lorentz boost; after
     it: reverse boost, IP-to-crab transport, crab cavity, inverse transport, one-turn map, chromaticity kick
@@ -508,14 +510,16 @@ def time_lines(ob, e0, p0, args, stream, barrier):
             gbs = n * 96 / (ms / 1e3) / 1e9
             per[f"{b}.{name}"] = {"elements": len(seg), "ms": ms, "achieved_gbs": gbs, "frac_of_hbm": gbs / hbm}
     # the oracle on a bounded sample, all host threads, scaled to the full beams
-    from oracle import oracle as orc
+    cpu_s = None
     sample = 100_000
-    t0 = time.perf_counter()
-    for b in beams:
-        src = (e0 if b == "electron" else p0)[:, :sample].cpu().numpy()
-        elems = [el.to_c() for el in ln.flatten(segs[b])]
-        orc.track_line(elems, src, turn=0, turns=1, seed=0, rng_method=1)
-    cpu_s = (time.perf_counter() - t0) * (N_E + N_P) / (2 * sample)
+    if cpu_side:
+        from oracle import oracle as orc
+        t0 = time.perf_counter()
+        for b in beams:
+            src = (e0 if b == "electron" else p0)[:, :sample].cpu().numpy()
+            elems = [el.to_c() for el in ln.flatten(segs[b])]
+            orc.track_line(elems, src, turn=0, turns=1, seed=0, rng_method=1)
+        cpu_s = (time.perf_counter() - t0) * (N_E + N_P) / (2 * sample)
     return {"ms_per_turn": turn_ms, "launches_per_turn": 4, "segments": per, "hbm_peak_gbs": hbm,
             "bytes_per_particle_per_launch": 96,
             "cpu_oracle_s_per_turn": cpu_s, "cpu_sample": f"{sample} particles of each beam, scaled",
@@ -524,7 +528,7 @@ def time_lines(ob, e0, p0, args, stream, barrier):
                     "particle make the electron's after-collision segment instruction-issue bound"}
 
 
-def time_soft_gaussian(ob, e0, p0, me, mp, rt, local_rank, args, stream):
+def time_soft_gaussian(ob, e0, p0, me, mp, rt, local_rank, args, stream, cpu_side=True):
     """The soft-Gaussian solver (GaussianPoissonSolver, 15 slices) on the same beams and maps: s/turn, the
     phase split (moments, kick), the kick's achieved bytes per second (11 FP64 values per field particle per
     pair) and the oracle's time per turn on a 10 % sample."""
@@ -568,14 +572,15 @@ def time_soft_gaussian(ob, e0, p0, me, mp, rt, local_rank, args, stream):
                                   "kick": kick_ms / nph, "unsort": ph["unsort"][0] / nph},
            "kick_achieved_gbs": kick_bytes / (kick_ms / 1e3) / 1e9 if kick_ms > 0 else None}
     # the oracle on a 10 % sample of both beams (same slicing), all host threads
-    from oracle import oracle as orc
-    se, sp = e0[:, : N_E // 10].cpu().numpy().copy(), p0[:, : N_P // 10].cpu().numpy().copy()
-    opt = orc.OracleOptions(nslices1=SLICES, nslices2=SLICES)
-    t0 = time.perf_counter()
-    orc.gaussian_collide(opt, se, sp, orc.beam_params(-1.0, orc.EMASS_EV, 10e9, 1.7e11),
-                         orc.beam_params(1.0, orc.PMASS_EV, 275e9, 6.9e10))
-    out["cpu_oracle_s_per_turn"] = (time.perf_counter() - t0) * 10
-    out["cpu_sample"] = "10 % of each beam, one collide, scaled by 10"
+    if cpu_side:
+        from oracle import oracle as orc
+        se, sp = e0[:, : N_E // 10].cpu().numpy().copy(), p0[:, : N_P // 10].cpu().numpy().copy()
+        opt = orc.OracleOptions(nslices1=SLICES, nslices2=SLICES)
+        t0 = time.perf_counter()
+        orc.gaussian_collide(opt, se, sp, orc.beam_params(-1.0, orc.EMASS_EV, 10e9, 1.7e11),
+                             orc.beam_params(1.0, orc.PMASS_EV, 275e9, 6.9e10))
+        out["cpu_oracle_s_per_turn"] = (time.perf_counter() - t0) * 10
+        out["cpu_sample"] = "10 % of each beam, one collide, scaled by 10"
     return out
 
 
