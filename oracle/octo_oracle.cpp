@@ -2287,4 +2287,17 @@ int oo_gaussian_collide(const oo_options *opt, double min_sigma, int32_t gaussia
 
 const char *oo_gaussian_last_error(void) { return g_gauss_error.c_str(); }
 
+// Pieces of the coupled kick's rotation term for the pins: the near-round series (strong_beam.jl:897-933) and
+// the principal-axis response (:1061-1116), each with L / D; and the elliptic kick alone (:1139-1146 regime).
+void oo_be_near_round_L(double kbb, double v, double eta, double x, double y, double out[5]) {
+    be::near_round_series(kbb, v, eta, x, y, out[0], out[1], out[2], out[3], &out[4]);
+}
+void oo_be_principal_L(double kbb, double s1, double s2, double x, double y, double out[5]) {
+    be::response_principal(kbb, s1, s2, x, y, out[0], out[1], out[2], out[3], &out[4]);
+}
+void oo_be_elliptic(double s1, double s2, double x, double y, double out[2]) {
+    const double eta = (s1 * s1 - s2 * s2) / (s1 * s1 + s2 * s2);
+    be::elliptic_kick(s1, s2, x, y, eta, out[0], out[1]);
+}
+
 }  // extern "C"

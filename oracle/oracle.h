@@ -130,6 +130,10 @@ int oo_gaussian_collide(const oo_options *opt, double min_sigma, int32_t gaussia
                         int32_t include_sigma_xy, double *b1[6], int64_t n1, double *b2[6], int64_t n2,
                         const oo_beam_params *p1, const oo_beam_params *p2, double *luminosity);
 const char *oo_gaussian_last_error(void);
+/* Rotation-term pins: out = Kx, Ky, H1, H2, L/D; the elliptic kick alone (s1 > s2). */
+void oo_be_near_round_L(double kbb, double v, double eta, double x, double y, double out[5]);
+void oo_be_principal_L(double kbb, double s1, double s2, double x, double y, double out[5]);
+void oo_be_elliptic(double s1, double s2, double x, double y, double out[2]);
 /* Line elements (the layout of octo_element in the product header; kinds 1..9: Linear6D, thin crab
    cavity, Lorentz boost, reverse boost, chromaticity kick, lumped radiation, crab dispersion, momentum
    dispersion, xy coupling).  oo_track_line applies elems to each particle `turns` times, turn t drawing

@@ -132,6 +132,9 @@ def lib():
                                           P(OOBeamParams), P(OOBeamParams), P(d)]
         L.oo_gaussian_collide.restype = C.c_int
         L.oo_gaussian_last_error.restype = C.c_char_p
+        L.oo_be_near_round_L.argtypes = [d, d, d, d, d, P(d)]
+        L.oo_be_principal_L.argtypes = [d, d, d, d, d, P(d)]
+        L.oo_be_elliptic.argtypes = [d, d, d, d, P(d)]
         L.oo_track_line.argtypes = [P(OOElement), i32, i64, i32, C.c_uint64, i32] + [P(d)] * 6 + [i64]
         L.oo_track_line.restype = None
         L.oo_octopus_normal.argtypes = [C.c_uint64, i32, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]
@@ -487,3 +490,21 @@ def gaussian_collide(options: "OracleOptions", beam1: np.ndarray, beam2: np.ndar
     if rc != OK:
         raise OracleErrorPy(rc, lib().oo_gaussian_last_error().decode())
     return lum.value
+
+
+def be_near_round_L(kbb, v, eta, x, y):
+    out = (C.c_double * 5)()
+    lib().oo_be_near_round_L(kbb, v, eta, x, y, out)
+    return tuple(out)
+
+
+def be_principal_L(kbb, s1, s2, x, y):
+    out = (C.c_double * 5)()
+    lib().oo_be_principal_L(kbb, s1, s2, x, y, out)
+    return tuple(out)
+
+
+def be_elliptic(s1, s2, x, y):
+    out = (C.c_double * 2)()
+    lib().oo_be_elliptic(s1, s2, x, y, out)
+    return tuple(out)

@@ -108,3 +108,25 @@ def test_agrees_with_pic_on_gaussian_beams():
             d1, d2 = b1[k] - b0[k], b2[k] - b0[k]
             assert np.corrcoef(d1, d2)[0, 1] > 0.999
             assert np.sqrt(np.mean((d1 - d2) ** 2)) < 0.06 * np.sqrt(np.mean(d1 ** 2))
+
+
+def test_rotation_term_series_matches_elliptic():
+    """The coupled kick's rotation term L / D has two independent forms: the near-round series
+    (strong_beam.jl:930-932) and (Kx y - Ky x) / D of the elliptic kick (:1107-1108).  Around the blend region
+    eta in [inner, outer] (:779-797) they agree to the series' truncation error, and the principal-axis
+    response takes the series below inner and the elliptic form above outer."""
+    import math
+    inner = math.sqrt(math.sqrt((8 / 3) * 64 * 2.220446049250313e-16)) / 2
+    outer = 2 * inner
+    v = 1e-8
+    for eta in (0.5 * inner, inner, 1.5 * inner, outer, 1.5 * outer):
+        s1, s2 = math.sqrt(v * (1 + eta)), math.sqrt(v * (1 - eta))
+        for x, y in ((1.3e-4, 0.7e-4), (-2e-5, 3e-5), (0.5e-4, -1.2e-4)):
+            series = orc.be_near_round_L(1.0, v, eta, x, y)[4]
+            kx, ky = orc.be_elliptic(s1, s2, x, y)
+            exact = (kx * y - ky * x) / (s1 * s1 - s2 * s2)
+            principal = orc.be_principal_L(1.0, s1, s2, x, y)[4]
+            assert abs(series - exact) < 2e-10 * abs(exact), (eta, series, exact)
+            assert abs(principal - exact) < 2e-10 * abs(exact)
+            if eta >= outer:  # the elliptic form itself (its denominator rounds as 2 v eta there)
+                assert abs(principal - exact) <= 1e-14 * abs(exact)
