@@ -250,3 +250,17 @@ def test_example_lines_compile():
         assert kinds[3] == 3 and kinds[4] == 4  # the boost pair frames the collision
     with pytest.raises(ArgumentError):
         ln.compile_line([object()])
+
+
+def test_linear6d_full_optics_case_is_symplectic():
+    """runtests.jl:250-268: optics with different ends and every dispersion / coupling tuple compiles, i.e.
+    its composed matrix passes the symplectic check."""
+    spec = ln.Linear6DSpec(beta1=(0.55, 0.056, 12.7), beta2=(0.8, 0.072, 90.9), alpha1=(0.08, 0.14, -0.069),
+                           alpha2=(0.0, 0.0, 0.0), dmu=(0.3, 0.4, 0.2), zeta1=(0.01, -0.02, 0.03, -0.01),
+                           eta1=(0.02, 0.01, -0.01, 0.04), R1=(0.01, -0.02, 0.015, 0.005),
+                           zeta2=(-0.01, 0.01, 0.02, 0.03), eta2=(0.01, -0.03, 0.02, -0.01),
+                           R2=(-0.005, 0.01, -0.015, 0.02))
+    assert ln.linear6d_symplectic_ratio(spec.matrix) <= 1.0
+    S6 = np.kron(np.eye(3), np.array([[0.0, 1.0], [-1.0, 0.0]]))
+    M = np.array(spec.matrix).reshape(6, 6)
+    np.testing.assert_allclose(M.T @ S6 @ M, S6, atol=1e-13)
