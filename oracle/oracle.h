@@ -13,6 +13,12 @@
  * (test/runtests.jl:9741-9776), the 4th-vs-2nd order Bassetti-Erskine field
  * test (test/runtests.jl:9628-9693) and the production golden luminosity
  * 1.0254361754701657e+30 (docs/history/cpu_benchmark_history.tsv:2).
+ * Line elements: the reference's element tests (test/runtests.jl:188-240,
+ * 341-508), symplecticity and the boost pair's Jacobian determinants, and the
+ * crossing-angle luminosity anchor (validation/crossing_luminosity_anchor.jl).
+ * Soft-Gaussian solver: the two-Gaussian luminosity, the point-charge far kick,
+ * the rotated kick of a tilted Gaussian, agreement with the PIC solve on
+ * Gaussian beams, and the two forms of the rotation term L/D.
  */
 #ifndef OCTO_ORACLE_H
 #define OCTO_ORACLE_H
