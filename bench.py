@@ -128,14 +128,18 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def _cpu_baseline(steps_hint: int = 1):
-    """The FP64 CPU oracle (a port of the reference's CPU PIC path) on one full turn of the same workload,
-    with every host thread; returns (s/turn, threads, sample description)."""
+def _cpu_baseline(steps_hint: int = 1, start=None):
+    """The FP64 CPU oracle (a port of the reference's CPU PIC path) on full turns of the same workload, with
+    every host thread; returns (s/turn, threads, sample description, luminosity of the first turn).  start:
+    the (e, p) host arrays to begin from (default: the beams built on the host as Beam.jl builds them)."""
     import numpy as np
     from oracle import oracle as orc
     threads = os.cpu_count() or 1
-    e = orc.beam_gaussian(N_E, seed=SEED, rng_id=1, beta=E_BEAM["beta"], sigma=E_BEAM["sigma"])
-    p = orc.beam_gaussian(N_P, seed=SEED, rng_id=2, beta=P_BEAM["beta"], sigma=P_BEAM["sigma"])
+    if start is None:
+        e = orc.beam_gaussian(N_E, seed=SEED, rng_id=1, beta=E_BEAM["beta"], sigma=E_BEAM["sigma"])
+        p = orc.beam_gaussian(N_P, seed=SEED, rng_id=2, beta=P_BEAM["beta"], sigma=P_BEAM["sigma"])
+    else:
+        e, p = (np.ascontiguousarray(a, dtype=np.float64).copy() for a in start)
     pe = orc.beam_params(-1.0, orc.EMASS_EV, 10e9, 1.7e11)
     pp = orc.beam_params(1.0, orc.PMASS_EV, 275e9, 6.9e10)
     oracle = orc.Oracle(orc.OracleOptions(grid=(GRID, GRID), interaction_grid="node", nslices1=SLICES,
@@ -143,13 +147,17 @@ def _cpu_baseline(steps_hint: int = 1):
     me = orc.linear6d_matrix(E_BEAM["beta"], (0, 0, 0), E_TUNES)
     mp = orc.linear6d_matrix(P_BEAM["beta"], (0, 0, 0), P_TUNES)
     times = []
+    first_lum = None
     for _ in range(max(1, steps_hint)):
         t0 = time.perf_counter()
-        oracle.collide(e, p, pe, pp)
+        lum = oracle.collide(e, p, pe, pp)
         orc.linear6d(me, e)
         orc.linear6d(mp, p)
         times.append(time.perf_counter() - t0)
-    return statistics.median(times), threads, f"{len(times)} full turn(s) of the benchmark workload (collide + maps)"
+        if first_lum is None:
+            first_lum = lum
+    return (statistics.median(times), threads, f"{len(times)} full turn(s) of the benchmark workload (collide + maps)",
+            first_lum)
 
 
 def run_reference(args, rank):
@@ -159,9 +167,9 @@ def run_reference(args, rank):
     budget = 180.0
     t0 = time.perf_counter()
     n_warm = max(1, args.warmup)
-    per, threads, _ = _cpu_baseline(n_warm)  # the requested warm-up turns (median turn time sizes the sample)
+    per, threads, _, _ = _cpu_baseline(n_warm)  # the requested warm-up turns (median turn time sizes the sample)
     n_time = max(1, min(args.steps, int(max(1.0, (budget - (time.perf_counter() - t0)) / max(per, 1e-3)))))
-    val, threads, sample = _cpu_baseline(n_time)
+    val, threads, sample, _ = _cpu_baseline(n_time)
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": n_time,
         "warmup": n_warm, "ms_per_step": val * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -258,10 +266,13 @@ def run_ours(args, rank, world, local_rank):
     gc.disable()
     w0 = time.perf_counter()
     ev0.record(stream)
+    lum_from_start = None
     for t in range(e2e_steps):
         e.coords.copy_(he, non_blocking=True)
         p.coords.copy_(hp, non_blocking=True)
         lum_e2e = turn(10_000 + t)
+        if lum_from_start is None:
+            lum_from_start = lum_e2e
         he.copy_(e.coords, non_blocking=True)
         hp.copy_(p.coords, non_blocking=True)
     ev1.record(stream)
@@ -270,6 +281,11 @@ def run_ours(args, rank, world, local_rank):
     wall = (time.perf_counter() - w0) / max(e2e_steps, 1)
     barrier()
     e2e_ms = ev0.elapsed_time(ev1) / e2e_steps if e2e_steps else float("nan")
+    if lum_from_start is None:  # the luminosity of one turn from the workload's initial beams (parity check)
+        e.coords.copy_(e0)
+        p.coords.copy_(p0)
+        lum_from_start = turn(10_000)
+        torch.cuda.synchronize()
 
     # the fast forms on the same workload: float32 beams and the same maps, on the production grid and on a
     # coarse 64^2 :node grid (its RMS field error vs exact Bassetti-Erskine stays below 1 %, reported below)
@@ -386,6 +402,8 @@ def run_ours(args, rank, world, local_rank):
         roof = {"kernel": "k_kick (gather + 6D synchro-beam kick)", "bound": "hbm", "achieved": achieved,
                 "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "traffic_source": "constant: DRAM bytes per field particle from one ncu capture of this kernel "
+                                  "(profiles/kick_node_production.md), scaled to the average launch",
                 "algorithmic_bytes_per_launch": kick_bytes / max(kick_launches, 1),
                 "avg_launch_ms": kick_ms / max(kick_launches, 1),
                 "timing": f"CUDA events around every kick launch on the collide stream, in a pass of {n_kick} "
@@ -421,15 +439,24 @@ def run_ours(args, rank, world, local_rank):
             "phases_ms_per_turn": fast["phases"],
         }
     cpu = None
+    parity = None
     if world == 1 and not args.no_cpu_baseline:
-        v, threads, sample = _cpu_baseline(1)
+        # one oracle turn from the same initial beams the GPU turns started from (the device-built beams,
+        # copied to the host): its luminosity against the GPU's turn from those beams
+        v, threads, sample, lum_oracle = _cpu_baseline(1, start=(e0.cpu().numpy(), p0.cpu().numpy()))
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+        parity = {"luminosity_gpu": lum_from_start, "luminosity_oracle": lum_oracle,
+                  "rel_diff": abs(lum_from_start / lum_oracle - 1.0),
+                  "tolerance": 1e-10,
+                  "what": "luminosity of one turn (collide + maps) from the workload's initial beams, GPU vs the "
+                          "FP64 CPU oracle on identical inputs"}
     beam_bytes = (N_E + N_P) * 6 * 8
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded counter-RNG Gaussian beams)",
-        "config": dict(CONFIG, parallelism=f"replicas{world}"),
+        "config": CONFIG,
+        "parallelism": f"replicas{world}",
         "e2e": {"value": e2e_ms / 1e3 / world, "unit": UNIT, "h2d_bytes_per_step": beam_bytes,
                 "d2h_bytes_per_step": beam_bytes + 8, "wall_s_per_step": wall},
         "gpu_launches": launches,
@@ -439,6 +466,7 @@ def run_ours(args, rank, world, local_rank):
                                     "octo_pic_autotune on copies of the beams before the warm-up"},
         "roofline": roof,
         "cpu_baseline": cpu,
+        "parity": parity,
         "fast_form": fast_line,
         "fast_form_coarse": coarse_line,
         "emittance_growth": emit,

@@ -222,9 +222,22 @@ int32_t octo_beam_moments(octo_ctx *ctx, const octo_beam *beam, const int32_t *p
                           int32_t mask_lost, int64_t turn, double *row, void *stream);
 
 /* Seeded Gaussian beam on the device as Beam(n, backend, Float64; beta, alpha, sigma, cutoff, rng_id)
- * builds it (Beam.jl:475-515; counter RNG counter_rng.jl:154-233). */
+ * builds it (Beam.jl:475-515; counter RNG counter_rng.jl:154-233).  Float64 beams only (dtype 0). */
 int32_t octo_beam_gaussian(octo_ctx *ctx, octo_beam *beam, uint64_t seed, uint64_t rng_id, const double beta[3],
                            const double alpha[3], const double sigma[3], double cutoff, void *stream);
+
+/* Charge-grid capture, a test hook for the bit-exact fixed-point claim (the reference's charge grid is the
+ * one _pic_deposit_drifted_* fills, pic_cpu.jl:2015-2146; its CPU backend exposes it to its own tests only
+ * through the solved fields).  octo_capture_charge_plane arms a copy of one field-solve plane of the next
+ * collide on this context: slice pair (pair_i, pair_j) (1-based), direction 1 (beam-1 slice sources) or 2,
+ * plane 0 = the sL deposit, 1 = the sR deposit, 2 = the third plane (:slice_pair quadratic: the midpoint;
+ * :node with the longitudinal kick: sR on the L mesh).  The copy is taken right after the deposit, before the
+ * solve consumes the grid.  octo_captured_charge_plane synchronises the device and returns the int64 grid
+ * (nx*ny, x fastest: grid[(iy-1)*nx + (ix-1)] is 1-based node (ix, iy)), the mesh it was deposited on
+ * (mesh = {x0, y0, width, height}) and the fixed-point scale (a tap is round(w * 2^fixed_bits)); it fails
+ * with OCTO_ERR_ARG when nothing was captured.  Capturing adds one device copy to that collide. */
+int32_t octo_capture_charge_plane(octo_ctx *ctx, int32_t pair_i, int32_t pair_j, int32_t direction, int32_t plane);
+int32_t octo_captured_charge_plane(octo_ctx *ctx, int64_t *grid, double mesh[4], int32_t *fixed_bits);
 
 /* Message of the last failing call on this context (NUL-terminated, truncated to len). */
 int32_t octo_last_error(octo_ctx *ctx, char *buf, int64_t len);
@@ -264,9 +277,14 @@ int32_t octo_timing_report(octo_ctx *ctx, double ms[OCTO_NPHASES], int64_t launc
  * process exit.  The limit that follows: n <= OCTO_NOALLOC_MAX_PARTICLES particles per call; larger
  * beams are rejected with OCTO_ERR_ARG and a message in err.
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with that
- * device current; make that first call before any stream capture.  All calls share the one array,
+ * device current; make that first call before any stream capture.  The address is cached per device
+ * together with the device's current context: after a device reset (cudaDeviceReset, CUDA.jl's
+ * device_reset!) the new context loads the library's module afresh, and the next call looks the address
+ * up again, so it too belongs before any stream capture.  The call makes `device` current while it runs
+ * and restores the calling thread's current context before it returns.  All calls share the one array,
  * so calls that overlap on the GPU (different streams, threads or processes sharing a context)
- * race: serialise them.  The caller owns beam, and err (may be NULL) receives a message on failure.
+ * race: serialise them.  Float64 beams only (dtype 0).  The caller owns beam, and err (may be NULL)
+ * receives a message on failure.
  * Output matches octo_beam_gaussian to rounding (its reduction uses a different block count). */
 #define OCTO_NOALLOC_PARTICLES_PER_BLOCK 8192
 #define OCTO_NOALLOC_MAX_BLOCKS 4094

@@ -24,6 +24,7 @@
 #include "k_misc.cuh"
 #include "k_pic.cuh"
 #include "k_slicing.cuh"
+#include "noalloc_cache.h"
 
 using namespace octo;
 
@@ -264,6 +265,11 @@ struct octo_ctx {
     double phase_ms[OCTO_NPHASES] = {0};
     long long phase_launches[OCTO_NPHASES] = {0};
     double phase_bytes[OCTO_NPHASES] = {0};
+    // octo_capture_charge_plane: one field-solve charge grid of the next collide, copied right after its
+    // deposit, with the mesh it was deposited on
+    int cap_armed = 0, cap_taken = 0, cap_i = 0, cap_j = 0, cap_dir = 0, cap_kind = 0, cap_bits = 0;
+    DevBuf<long long> cap_q;
+    DevBuf<Grid> cap_grid;
 };
 
 namespace {
@@ -1199,6 +1205,21 @@ void CollideJob::run() {
                 });
             });
         }
+        if (c->cap_armed && !c->cap_taken) {
+            for (int t = F.t0; t < F.t0 + F.nt; ++t) {
+                const Task &T = tasks[t];
+                if (T.i != c->cap_i || T.j != c->cap_j || T.dir != c->cap_dir || c->cap_kind >= T.nplanes) continue;
+                const Plane &P = planes[T.plane0 + c->cap_kind];
+                c->cap_q.ensure(cells);
+                c->cap_grid.ensure(1);
+                CK(cudaMemcpyAsync(c->cap_q.p, c->qgrid.p + (size_t)(T.plane0 + c->cap_kind - F.p0) * cells,
+                                   sizeof(long long) * cells, cudaMemcpyDeviceToDevice, st));
+                const Grid *mesh = P.geom >= 0 ? &(c->nodes.p + P.geom)->sg : &(c->geom.p + t)->sg;
+                CK(cudaMemcpyAsync(c->cap_grid.p, mesh, sizeof(Grid), cudaMemcpyDeviceToDevice, st));
+                c->cap_bits = P.fixed_bits;
+                c->cap_taken = 1;
+            }
+        }
         {
             PhaseScope ps(c, OCTO_PHASE_FFT, st, 2);
             with_real(fp32, [&](auto r) {
@@ -1818,7 +1839,7 @@ void octo_destroy(octo_ctx *c) {
     c->nodenan.release(); c->status.release(); c->ghat.release(); c->qgrid.release(); c->lq.release();
     c->spec.release(); c->fields.release(); c->lum_parts.release(); c->lum_partial.release(); c->node_ref.release(); c->stats.release();
     c->partial.release(); c->soa_ptrs.release();
-    c->first_lum.release(); c->lum_tick.release();
+    c->first_lum.release(); c->lum_tick.release(); c->cap_q.release(); c->cap_grid.release();
     c->hyb.release(); c->hmom.release(); c->hprof.release(); c->hsum.release(); c->qtot.release();
     c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_noderef.release(); c->h_slices.release();
     for (auto e : c->ev_pool) cudaEventDestroy(e);
@@ -2161,6 +2182,36 @@ int32_t octo_beam_gaussian(octo_ctx *c, octo_beam *beam, uint64_t seed, uint64_t
     }
 }
 
+int32_t octo_capture_charge_plane(octo_ctx *c, int32_t pair_i, int32_t pair_j, int32_t direction, int32_t plane) {
+    if (!c) return OCTO_ERR_ARG;
+    if (pair_i < 1 || pair_j < 1 || (direction != 1 && direction != 2) || plane < 0 || plane > 2)
+        return fail(c, OCTO_ERR_ARG, "capture: pair indices are 1-based, direction 1 or 2, plane 0..2");
+    c->cap_armed = 1;
+    c->cap_taken = 0;
+    c->cap_i = pair_i; c->cap_j = pair_j; c->cap_dir = direction; c->cap_kind = plane;
+    return OCTO_OK;
+}
+
+int32_t octo_captured_charge_plane(octo_ctx *c, int64_t *grid, double mesh[4], int32_t *fixed_bits) {
+    if (!c || !grid || !mesh || !fixed_bits) return OCTO_ERR_ARG;
+    if (!c->cap_armed || !c->cap_taken)
+        return fail(c, OCTO_ERR_ARG, "capture: no charge plane was captured (not armed, or the pair did not run)");
+    try {
+        CK(cudaSetDevice(c->device));
+        CK(cudaDeviceSynchronize());
+        Grid g{};
+        CK(cudaMemcpy(grid, c->cap_q.p, sizeof(long long) * (size_t)c->opt.nx * c->opt.ny, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&g, c->cap_grid.p, sizeof(Grid), cudaMemcpyDeviceToHost));
+        mesh[0] = g.x0; mesh[1] = g.y0; mesh[2] = g.w; mesh[3] = g.h;
+        *fixed_bits = c->cap_bits;
+        c->cap_armed = 0;
+        c->cap_taken = 0;
+        return OCTO_OK;
+    } catch (CudaFail &e) {
+        return fail(c, OCTO_ERR_CUDA, e.msg);
+    }
+}
+
 int32_t octo_set_timing_phases(octo_ctx *c, uint32_t mask) {
     if (!c) return OCTO_ERR_ARG;
     c->timing_mask = mask;
@@ -2196,10 +2247,50 @@ static __device__ __align__(256) double g_noalloc_scratch[OCTO_NOALLOC_MAX_BLOCK
 
 namespace {
 constexpr int kNoallocMaxDevices = 64;
-// Device address of g_noalloc_scratch per device, looked up once with that device current.  In host
-// code the symbol itself is only a host-side stand-in, so kernels are always given this address.
-double *g_noalloc_addr[kNoallocMaxDevices] = {nullptr};
-std::mutex g_noalloc_mutex;
+// Device address of g_noalloc_scratch per device and context (see noalloc_cache.h): looked up with the
+// device current, and again whenever the device's current context is not the one it was looked up in.
+SymbolAddressCache<kNoallocMaxDevices> g_noalloc_addr;
+
+// cuCtxGetCurrent / cuCtxSetCurrent, resolved through the runtime so the library needs no link against the
+// driver library.  Both take and return the driver's context handle as an opaque pointer.
+using CtxGetFn = int (*)(void **);
+using CtxSetFn = int (*)(void *);
+struct DriverCtxFns {
+    CtxGetFn get = nullptr;
+    CtxSetFn set = nullptr;
+};
+const DriverCtxFns &driver_ctx_fns() {
+    static DriverCtxFns f = [] {
+        DriverCtxFns r;
+        void *g = nullptr, *s = nullptr;
+        cudaDriverEntryPointQueryResult qg{}, qs{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &g, cudaEnableDefault, &qg) == cudaSuccess &&
+            qg == cudaDriverEntryPointSuccess && g)
+            r.get = (CtxGetFn)g;
+        if (cudaGetDriverEntryPoint("cuCtxSetCurrent", &s, cudaEnableDefault, &qs) == cudaSuccess &&
+            qs == cudaDriverEntryPointSuccess && s)
+            r.set = (CtxSetFn)s;
+        return r;
+    }();
+    return f;
+}
+
+// Saves the calling thread's current CUDA context on entry and makes it current again on every return
+// path, so a host that tracks its own current device (CUDA.jl, PyTorch) sees it unchanged after the call.
+struct CurrentContextGuard {
+    void *saved = nullptr;
+    int saved_device = -1;
+    bool have_ctx = false;
+    CurrentContextGuard() {
+        const DriverCtxFns &f = driver_ctx_fns();
+        if (f.get && f.set && f.get(&saved) == 0) have_ctx = true;
+        else if (cudaGetDevice(&saved_device) != cudaSuccess) saved_device = -1;
+    }
+    ~CurrentContextGuard() {
+        if (have_ctx) driver_ctx_fns().set(saved);
+        else if (saved_device >= 0) cudaSetDevice(saved_device);
+    }
+};
 
 void noalloc_message(char *err, int64_t len, const std::string &m) {
     if (!err || len <= 0) return;
@@ -2235,23 +2326,24 @@ int32_t octo_beam_gaussian_noalloc(int32_t device, octo_beam *beam, uint64_t see
         noalloc_message(err, err_len, "device index out of range");
         return OCTO_ERR_ARG;
     }
+    CurrentContextGuard restore_caller_context;
     if (cudaSetDevice(device) != cudaSuccess) {
         noalloc_message(err, err_len, "cudaSetDevice failed");
         return OCTO_ERR_CUDA;
     }
-    double *scratch;
-    {
-        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_addr[device]) {
-            void *p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess || !p) {
-                noalloc_message(err, err_len, std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
-                return OCTO_ERR_CUDA;
-            }
-            g_noalloc_addr[device] = (double *)p;
-        }
-        scratch = g_noalloc_addr[device];
+    // the device's current context keys the cached address: a reset device gets a new context, whose
+    // module (and scratch array) is looked up again.  cudaSetDevice made the primary context current.
+    void *ctx = nullptr;
+    if (driver_ctx_fns().get) driver_ctx_fns().get(&ctx);
+    cudaError_t lookup_err = cudaSuccess;
+    double *scratch = (double *)g_noalloc_addr.lookup(device, ctx, [&]() -> void * {
+        void *p = nullptr;
+        lookup_err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        return lookup_err == cudaSuccess ? p : nullptr;
+    });
+    if (!scratch) {
+        noalloc_message(err, err_len, std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(lookup_err));
+        return OCTO_ERR_CUDA;
     }
     cudaStream_t st = (cudaStream_t)stream;
     const long long n = beam->n;

@@ -25,7 +25,7 @@ EXPORTS = (
     "octo_pair_luminosity_trace", "octo_linear6d", "octo_beam_gaussian", "octo_last_error",
     "octo_normal_quantile", "octo_erfinv", "octo_version", "octo_set_timing", "octo_timing_report",
     "octo_beam_gaussian_noalloc", "octo_pic_collide_batch", "octo_set_timing_phases", "octo_pic_autotune",
-    "octo_track_line", "octo_beam_moments",
+    "octo_track_line", "octo_beam_moments", "octo_capture_charge_plane", "octo_captured_charge_plane",
 )
 
 PHASES = ("slicing", "bounds", "plan", "green", "luminosity", "deposit", "fft", "field", "kick", "unsort", "node")
@@ -149,6 +149,10 @@ def lib():
     L.octo_version.argtypes = []
     L.octo_beam_gaussian_noalloc.restype = i32
     L.octo_beam_gaussian_noalloc.argtypes = [i32, P(OctoBeam), u64, u64, P(d), P(d), P(d), d, vp, C.c_char_p, i64]
+    L.octo_capture_charge_plane.restype = i32
+    L.octo_capture_charge_plane.argtypes = [vp, i32, i32, i32, i32]
+    L.octo_captured_charge_plane.restype = i32
+    L.octo_captured_charge_plane.argtypes = [vp, P(i64), P(d), P(i32)]
     L.octo_set_timing_phases.restype = i32
     L.octo_set_timing_phases.argtypes = [vp, C.c_uint32]
     L.octo_set_timing.restype = i32

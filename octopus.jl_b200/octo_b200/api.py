@@ -121,6 +121,26 @@ class Context:
         _lib.lib().octo_green_cache_stats(self._ptr, C.byref(h), C.byref(m), C.byref(r))
         return h.value, m.value, r.value
 
+    def capture_charge_plane(self, pair_i: int, pair_j: int, direction: int, plane: int = 0):
+        """Arm a copy of one field-solve charge grid of the next collide (a test hook): slice pair (i, j),
+        direction 1 or 2, plane 0 (sL), 1 (sR) or 2 (the midpoint / :node Z plane)."""
+        rc = _lib.lib().octo_capture_charge_plane(self._ptr, int(pair_i), int(pair_j), int(direction), int(plane))
+        if rc != _lib.OCTO_OK:
+            raise CollisionError(rc, _lib.last_error(self._ptr))
+
+    def captured_charge_plane(self):
+        """The captured int64 grid as an (ny, nx) array (row iy-1 holds nodes (1..nx, iy)), the mesh
+        (x0, y0, width, height) and the fixed-point bits."""
+        nx, ny = self.solver.grid
+        q = np.zeros(nx * ny, dtype=np.int64)
+        mesh = (C.c_double * 4)()
+        bits = C.c_int32()
+        rc = _lib.lib().octo_captured_charge_plane(self._ptr, q.ctypes.data_as(C.POINTER(C.c_int64)), mesh,
+                                                   C.byref(bits))
+        if rc != _lib.OCTO_OK:
+            raise CollisionError(rc, _lib.last_error(self._ptr))
+        return q.reshape(ny, nx), tuple(mesh), bits.value
+
     def set_timing(self, enable: bool = True, phases=None):
         """Per-phase device timing (the reference's pic_timing diagnostics); enabling clears it.  phases: the
         names of the phases to time (default all); each timed launch group records two CUDA events."""

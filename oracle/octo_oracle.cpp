@@ -550,7 +550,19 @@ inline void axis_extent(int method, double &lo, double &hi, double origin, doubl
 
 struct FieldPlanes { std::vector<double> phi, Ex, Ey; void init(int n) { phi.assign(n, 0); Ex.assign(n, 0); Ey.assign(n, 0); } };
 
+// A copy of one field-solve charge grid of a collide, for the bit-exact fixed-point comparison with the
+// product's octo_capture_charge_plane: slice pair (i, j), direction, plane (0 = sL, 1 = sR, 2 = third).
+struct Capture {
+    bool armed = false, taken = false;
+    int i = 0, j = 0, dir = 0, kind = 0;
+    std::vector<int64_t> q;
+    Grid grid{};
+    int bits = 0;
+};
+
 struct Workspace {
+    Capture *cap = nullptr;  // set with cap_kind >= 0 while the captured interaction runs
+    int cap_kind = -1;
     int nx = 0, ny = 0;
     std::vector<double> charge;  // (2nx)*(2ny)
     std::vector<cplx> spectral;
@@ -595,13 +607,21 @@ void green_fft(const Options &O, Workspace &ws, const Grid &sg, const Grid &fg, 
 
 // pic_cpu.jl:1965-1990
 void solve_drifted(const Options &O, Workspace &ws, FieldPlanes &fp, const Coords &src, double s, const Grid &sg,
-                   const std::vector<cplx> &gfft, bool drift = true) {
+                   const std::vector<cplx> &gfft, bool drift = true, int kind = -1) {
     int nx = O.o.nx, ny = O.o.ny;
     double hx = sg.width / (double)(nx - 1), hy = sg.height / (double)(ny - 1);
     std::fill(ws.charge.begin(), ws.charge.end(), 0.0);
+    int64_t *qfix = nullptr;
+    if (ws.cap && kind >= 0 && kind == ws.cap_kind && O.o.fixed_point_deposit) {
+        ws.cap->q.assign((size_t)nx * ny, 0);
+        ws.cap->grid = sg;
+        ws.cap->bits = fixed_bits((int64_t)src.size());
+        ws.cap->taken = true;
+        qfix = ws.cap->q.data();
+    }
     deposit_grid(ws.charge.data(), 2 * nx, O.o.deposit_method, src.x.data(), src.px.data(), src.y.data(),
                  src.py.data(), (int64_t)src.size(), drift, s, sg.x0, sg.y0, hx, hy, nx, ny,
-                 O.o.fixed_point_deposit != 0, nullptr);
+                 O.o.fixed_point_deposit != 0, qfix);
     for (size_t k = 0; k < ws.charge.size(); ++k) ws.spectral[k] = cplx(ws.charge[k], 0.0);
     ws.fft.run(ws.spectral.data(), false);
     for (size_t k = 0; k < ws.spectral.size(); ++k) ws.spectral[k] *= gfft[k];
@@ -793,6 +813,7 @@ struct Ctx {
     std::vector<int> trace_i, trace_j;
     std::vector<double> trace_lum;
     std::string err;
+    Capture cap;
     GreenEntry &entry(int i, int j, int dir) { return cache[((size_t)(dir - 1) * ns1 + (i - 1)) * ns2 + (j - 1)]; }
 };
 
@@ -958,15 +979,15 @@ void interaction(Ctx &C, Workspace &ws, const Coords &source, const SliceParam &
         ws.dropped += count_outside(field.x, field.y, fg.x0, fg.x0 + fg.width, fg.y0, fg.y0 + fg.height);
         ws.dropped += count_outside_drifted(source, sL, sR, sg.x0, sg.x0 + sg.width, sg.y0, sg.y0 + sg.height);
     }
-    solve_drifted(O, ws, ws.left, source, sL, sg, gfft);
-    solve_drifted(O, ws, ws.right, source, sR, sg, gfft);
+    solve_drifted(O, ws, ws.left, source, sL, sg, gfft, true, 0);
+    solve_drifted(O, ws, ws.right, source, sR, sg, gfft, true, 1);
     double ks = 2.0 * kbb;
     double hzi, zbias;
     slice_interp_params(pf.lb, pf.rb, hzi, zbias);
     bool lk = O.o.longitudinal_kick != 0;
     if (O.o.slice_interpolation == 1) {
         double smid = 0.5 * (sL + sR);
-        solve_drifted(O, ws, ws.mid, source, smid, sg, gfft);
+        solve_drifted(O, ws, ws.mid, source, smid, sg, gfft, true, 2);
         for (int k = 0; k < nfield; ++k) {
             double zL = jclamp(-field.z[k] * hzi + zbias, 0.0, 1.0);
             double Kx, Ky, Kz;
@@ -1231,9 +1252,9 @@ void interaction_node(Ctx &C, Workspace &ws, const Coords &source, const SlicePa
     ws.dropped += count_outside_drifted(source, sR, sR, gR.sg.x0, gR.sg.x0 + gR.sg.width, gR.sg.y0,
                                         gR.sg.y0 + gR.sg.height);
     ws.dropped += count_outside(field.x, field.y, gL.fg.x0, gL.fg.x0 + gL.fg.width, gL.fg.y0, gL.fg.y0 + gL.fg.height);
-    solve_drifted(O, ws, ws.left, source, sL, gL.sg, gL.gfft);
-    solve_drifted(O, ws, ws.right, source, sR, gR.sg, gR.gfft);
-    if (lk) solve_drifted(O, ws, ws.mid, source, sR, gL.sg, gL.gfft);
+    solve_drifted(O, ws, ws.left, source, sL, gL.sg, gL.gfft, true, 0);
+    solve_drifted(O, ws, ws.right, source, sR, gR.sg, gR.gfft, true, 1);
+    if (lk) solve_drifted(O, ws, ws.mid, source, sR, gL.sg, gL.gfft, true, 2);
     double ks = 2.0 * kbb;
     double hzi, zbias;
     slice_interp_params(pf.lb, pf.rb, hzi, zbias);
@@ -1470,6 +1491,13 @@ double collide(Ctx &C, double *b1[6], int64_t n1, double *b2[6], int64_t n2, con
                 Coords &coord2 = state2[j - 1];
                 Coords &field2 = scratch2[j - 1];
                 field2 = coord2;
+                // the armed charge-grid capture, if it is one of this pair's interactions
+                auto arm = [&](int dir) {
+                    const bool hit = C.cap.armed && !C.cap.taken && C.cap.i == i && C.cap.j == j && C.cap.dir == dir;
+                    ws.cap = hit ? &C.cap : nullptr;
+                    ws.cap_kind = hit ? C.cap.kind : -1;
+                };
+                arm(1);
                 if (node) {
                     auto &nc1 = node1[i - 1];
                     auto &nc2 = node2[j - 1];
@@ -1477,14 +1505,18 @@ double collide(Ctx &C, double *b1[6], int64_t n1, double *b2[6], int64_t n2, con
                     const NodeMesh &gL1 = nc1[j - 1], &gR1 = nc1[j], &gL2 = nc2[i - 1], &gR2 = nc2[i];
                     if (!gL1.valid || !gR1.valid || !gL2.valid || !gR2.valid) continue;
                     interaction_node(C, ws, coord1, pa1, field2, pa2, kbb2, gL1, gR1, 0);
+                    arm(2);
                     interaction_node(C, ws, coord2, pa2, coord1, pa1, kbb1, gL2, gR2, 1);
                 } else if (O.o.gaussian) {
                     interaction_gaussian(C, ws, coord1, pa1, field2, pa2, kbb2, i, j, 1, 0, counters[p].data());
                     interaction_gaussian(C, ws, coord2, pa2, coord1, pa1, kbb1, i, j, 2, 1, counters[p].data());
                 } else {
                     interaction(C, ws, coord1, pa1, field2, pa2, kbb2, i, j, 1, 0, counters[p].data());
+                    arm(2);
                     interaction(C, ws, coord2, pa2, coord1, pa1, kbb1, i, j, 2, 1, counters[p].data());
                 }
+                ws.cap = nullptr;
+                ws.cap_kind = -1;
                 std::swap(state2[j - 1], scratch2[j - 1]);
                 if (compute_lum) lum_parts[p] = luminosity(O, ws.vx[0], ws.vy[0], ws.vx[1], ws.vy[1], klum, ws);
                 ran[p] = 1;
@@ -1732,6 +1764,21 @@ int64_t oo_pair_trace(void *ctx, int32_t *pi, int32_t *pj, double *lum, int64_t 
     return n;
 }
 const char *oo_last_error(void *ctx) { return ((Ctx *)ctx)->err.c_str(); }
+// Arm / read the charge-grid capture (fixed_point_deposit must be on).  Returns 0 when a grid was captured.
+void oo_capture_plane(void *ctx, int32_t i, int32_t j, int32_t dir, int32_t kind) {
+    Capture &c = ((Ctx *)ctx)->cap;
+    c = Capture();
+    c.armed = true; c.i = i; c.j = j; c.dir = dir; c.kind = kind;
+}
+int32_t oo_captured_plane(void *ctx, int64_t *q, double mesh[4], int32_t *bits) {
+    Capture &c = ((Ctx *)ctx)->cap;
+    if (!c.armed || !c.taken) return OO_ERR_ARG;
+    std::copy(c.q.begin(), c.q.end(), q);
+    mesh[0] = c.grid.x0; mesh[1] = c.grid.y0; mesh[2] = c.grid.width; mesh[3] = c.grid.height;
+    *bits = c.bits;
+    c.armed = false;
+    return OO_OK;
+}
 
 // linear6d.jl:110-121
 void oo_linear6d(const double m[36], double *x, double *px, double *y, double *py, double *z, double *pz, int64_t n) {

@@ -129,6 +129,11 @@ int64_t oo_dropped(void *ctx);
 /* Per-pair luminosity of the last collide in collision order (i, j 1-based); returns count. */
 int64_t oo_pair_trace(void *ctx, int32_t *pi, int32_t *pj, double *lum, int64_t cap);
 const char *oo_last_error(void *ctx);
+/* Capture one field-solve charge grid of the next collide (fixed_point_deposit on): pair (i, j), direction,
+   plane 0 = sL, 1 = sR, 2 = the third (midpoint / :node Z).  oo_captured_plane writes the nx*ny int64 grid
+   (x fastest), the mesh {x0, y0, width, height} and the fixed-point bits; nonzero when nothing was captured. */
+void oo_capture_plane(void *ctx, int32_t i, int32_t j, int32_t dir, int32_t kind);
+int32_t oo_captured_plane(void *ctx, int64_t *q, double mesh[4], int32_t *bits);
 /* collide!(::GaussianPoissonSolver, ...) (src/tasks/strongstrong/gaussian.jl:7-185): the soft-Gaussian solver,
    include_sigma_xy: the coupled covariance; virtual_drift 0 :hirata, 1 :chromatic, 2 :exact; opt gives the slicings, kbb / luminosity-scale overrides and longitudinal_kick. */
 int oo_gaussian_collide(const oo_options *opt, double min_sigma, int32_t gaussian_when_luminosity,

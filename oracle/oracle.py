@@ -126,6 +126,10 @@ def lib():
         L.oo_pair_trace.argtypes = [vp, P(i32), P(i32), P(d), i64]
         L.oo_last_error.restype = C.c_char_p
         L.oo_last_error.argtypes = [vp]
+        L.oo_capture_plane.argtypes = [vp, i32, i32, i32, i32]
+        L.oo_capture_plane.restype = None
+        L.oo_captured_plane.argtypes = [vp, P(i64), P(d), P(i32)]
+        L.oo_captured_plane.restype = i32
         L.oo_linear6d.argtypes = [P(d)] + [P(d)] * 6 + [i64]
         L.oo_linear6d_matrix.argtypes = [P(d), P(d), P(d), P(d)]
         L.oo_gaussian_collide.argtypes = [P(OOOptions), d, i32, i32, i32, i32, i32, P(P(d)), i64, P(P(d)), i64,
@@ -317,6 +321,21 @@ class Oracle:
 
     def dropped(self):
         return lib().oo_dropped(self._ctx)
+
+    def capture_plane(self, i: int, j: int, direction: int, plane: int = 0):
+        """Arm a copy of one field-solve charge grid of the next collide (needs fixed_point_deposit)."""
+        lib().oo_capture_plane(self._ctx, int(i), int(j), int(direction), int(plane))
+
+    def captured_plane(self):
+        """(int64 grid as (ny, nx), mesh (x0, y0, width, height), fixed-point bits) of the captured plane."""
+        nx, ny = self.options.grid
+        q = np.zeros(nx * ny, dtype=np.int64)
+        mesh = (C.c_double * 4)()
+        bits = C.c_int32()
+        rc = lib().oo_captured_plane(self._ctx, q.ctypes.data_as(C.POINTER(C.c_int64)), mesh, C.byref(bits))
+        if rc != OK:
+            raise OracleErrorPy(rc, "no charge plane was captured")
+        return q.reshape(ny, nx), tuple(mesh), bits.value
 
     def pair_trace(self):
         cap = 4096
