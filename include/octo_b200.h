@@ -239,6 +239,28 @@ int32_t octo_beam_gaussian(octo_ctx *ctx, octo_beam *beam, uint64_t seed, uint64
 int32_t octo_capture_charge_plane(octo_ctx *ctx, int32_t pair_i, int32_t pair_j, int32_t direction, int32_t plane);
 int32_t octo_captured_charge_plane(octo_ctx *ctx, int64_t *grid, double mesh[4], int32_t *fixed_bits);
 
+/* BF16 GEMM on the tensor cores (tcgen05.mma with a TMEM accumulator), the contraction of the learned field
+ * correction's convolutions; no reference counterpart.  out[z][m][n] = sum over split z of k of A[m][k] B[n][k]
+ * (fp32, row stride ldc, split z at out + z*M*ldc), or with out_bf16 set (splits = 1):
+ * out_bf16[m*ldo + n] = bf16(relu?(acc + bias[n])).  a_mode 0: A is a dense row-major bf16 matrix (lda, a
+ * multiple of 8); a_mode 1: A is the implicit im2col of a 3x3, padding-1 convolution over the NHWC bf16 tensor
+ * A[M/(H*W)][H][W][C] (C a multiple of 8, K = 9*C, k = (ky*3 + kx)*C + c).  B is row-major bf16 [N][ldb].
+ * Device pointers, 16-byte aligned; K a multiple of 8.  Synchronises the stream; OCTO_ERR_TIMEOUT if a
+ * bounded device wait gave up. */
+typedef struct {
+    int32_t M, N, K, a_mode, H, W, C, splits, relu, pad;
+    const void *A;
+    int64_t lda;
+    const void *B;
+    int64_t ldb;
+    float *out;
+    int64_t ldc;
+    const float *bias;
+    void *out_bf16;
+    int64_t ldo;
+} octo_gemm_desc;
+int32_t octo_gemm_bf16(int32_t device, const octo_gemm_desc *desc, void *stream);
+
 /* Message of the last failing call on this context (NUL-terminated, truncated to len). */
 int32_t octo_last_error(octo_ctx *ctx, char *buf, int64_t len);
 

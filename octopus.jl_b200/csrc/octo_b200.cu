@@ -24,6 +24,7 @@
 #include "k_misc.cuh"
 #include "k_pic.cuh"
 #include "k_slicing.cuh"
+#include "k_umma.cuh"
 #include "noalloc_cache.h"
 
 using namespace octo;
@@ -2240,6 +2241,40 @@ int32_t octo_timing_report(octo_ctx *c, double ms[OCTO_NPHASES], int64_t launche
 
 }  // extern "C"
 
+// ---------------------------------------------------------------- tensor-core GEMM launch
+namespace octo {
+namespace nn {
+// Picks the tile width from N (32, 64, 128 or 256 columns of fp32 accumulator in TMEM).
+void launch_gemm(const GemmArgs &g, int splits, cudaStream_t st) {
+    const int bn = g.N <= 32 ? 32 : (g.N <= 64 ? 64 : (g.N <= 128 ? 128 : 256));
+    const dim3 grid((unsigned)((g.M + kBM - 1) / kBM), (unsigned)((g.N + bn - 1) / bn), (unsigned)splits);
+    const size_t smem = umma_smem_bytes(bn);
+    auto go = [&](void (*kernel)(const GemmArgs)) {
+        CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        launch_pdl(kernel, grid, kGemmThreads, smem, st, g);
+    };
+    if (bn == 32) go(k_umma_gemm<32>);
+    else if (bn == 64) go(k_umma_gemm<64>);
+    else if (bn == 128) go(k_umma_gemm<128>);
+    else go(k_umma_gemm<256>);
+}
+}  // namespace nn
+}  // namespace octo
+
+namespace {
+// Device status word of the tensor-core kernels (set to OCTO_ERR_TIMEOUT by a wait that gave up), one per
+// device, allocated on first use.
+int *nn_error_flag() {
+    static std::mutex mu;
+    static int *flag[64] = {nullptr};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (!flag[dev]) CK(cudaMalloc(&flag[dev], sizeof(int)));
+    return flag[dev];
+}
+}  // namespace
+
 // ---------------------------------------------------------------- allocation-free beam construction
 // Reduction scratch of octo_beam_gaussian_noalloc: OCTO_NOALLOC_MAX_BLOCKS block partial sums followed
 // by the mean and sigma slots.  4096 doubles = 32 KiB, resident on every device that loads the library.
@@ -2369,6 +2404,37 @@ int32_t octo_beam_gaussian_noalloc(int32_t device, octo_beam *beam, uint64_t see
         return OCTO_ERR_CUDA;
     }
     return OCTO_OK;
+}
+
+int32_t octo_gemm_bf16(int32_t device, const octo_gemm_desc *d, void *stream) {
+    if (!d || !d->A || !d->B || (!d->out && !d->out_bf16)) return OCTO_ERR_ARG;
+    if (d->M < 1 || d->N < 1 || d->K < 8 || d->K % 8 || d->splits < 1) return OCTO_ERR_ARG;
+    if (d->a_mode == 1 && (d->C < 8 || d->C % 8 || d->K != 9 * d->C || d->M % (d->H * d->W))) return OCTO_ERR_ARG;
+    if (d->a_mode == 0 && (d->lda % 8 || ((uintptr_t)d->A & 15))) return OCTO_ERR_ARG;
+    if (d->ldb % 8 || ((uintptr_t)d->B & 15)) return OCTO_ERR_ARG;
+    if (d->out_bf16 && d->splits != 1) return OCTO_ERR_ARG;
+    try {
+        CK(cudaSetDevice(device));
+        nn::GemmArgs g{};
+        g.M = d->M; g.N = d->N; g.K = d->K;
+        g.A = (const __nv_bfloat16 *)d->A; g.lda = d->lda; g.a_mode = d->a_mode;
+        g.H = d->H; g.W = d->W; g.C = d->C;
+        g.B = (const __nv_bfloat16 *)d->B; g.ldb = d->ldb;
+        g.out = d->out; g.ldc = d->ldc; g.split_stride = (long long)d->M * d->ldc;
+        const int kchunks = (d->K + nn::kBK - 1) / nn::kBK;
+        g.k_per_split = ((kchunks + d->splits - 1) / d->splits) * nn::kBK;
+        g.bias = d->bias; g.relu = d->relu; g.out_bf16 = (__nv_bfloat16 *)d->out_bf16; g.ldo = d->ldo;
+        g.error = nn_error_flag();
+        cudaStream_t st = (cudaStream_t)stream;
+        CK(cudaMemsetAsync(g.error, 0, sizeof(int), st));
+        nn::launch_gemm(g, d->splits, st);
+        int e = 0;
+        CK(cudaMemcpyAsync(&e, g.error, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return e ? OCTO_ERR_TIMEOUT : OCTO_OK;
+    } catch (CudaFail &) {
+        return OCTO_ERR_CUDA;
+    }
 }
 
 int32_t octo_last_error(octo_ctx *c, char *buf, int64_t len) {

@@ -26,6 +26,7 @@ EXPORTS = (
     "octo_normal_quantile", "octo_erfinv", "octo_version", "octo_set_timing", "octo_timing_report",
     "octo_beam_gaussian_noalloc", "octo_pic_collide_batch", "octo_set_timing_phases", "octo_pic_autotune",
     "octo_track_line", "octo_beam_moments", "octo_capture_charge_plane", "octo_captured_charge_plane",
+    "octo_gemm_bf16",
 )
 
 PHASES = ("slicing", "bounds", "plan", "green", "luminosity", "deposit", "fft", "field", "kick", "unsort", "node")
@@ -100,6 +101,14 @@ class OctoCollideReport(C.Structure):
     ]
 
 
+class OctoGemmDesc(C.Structure):
+    _fields_ = [("M", C.c_int32), ("N", C.c_int32), ("K", C.c_int32), ("a_mode", C.c_int32), ("H", C.c_int32),
+                ("W", C.c_int32), ("C", C.c_int32), ("splits", C.c_int32), ("relu", C.c_int32), ("pad", C.c_int32),
+                ("A", C.c_void_p), ("lda", C.c_int64), ("B", C.c_void_p), ("ldb", C.c_int64),
+                ("out", C.c_void_p), ("ldc", C.c_int64), ("bias", C.c_void_p), ("out_bf16", C.c_void_p),
+                ("ldo", C.c_int64)]
+
+
 _lib = None
 
 
@@ -153,6 +162,8 @@ def lib():
     L.octo_capture_charge_plane.argtypes = [vp, i32, i32, i32, i32]
     L.octo_captured_charge_plane.restype = i32
     L.octo_captured_charge_plane.argtypes = [vp, P(i64), P(d), P(i32)]
+    L.octo_gemm_bf16.restype = i32
+    L.octo_gemm_bf16.argtypes = [i32, P(OctoGemmDesc), vp]
     L.octo_set_timing_phases.restype = i32
     L.octo_set_timing_phases.argtypes = [vp, C.c_uint32]
     L.octo_set_timing.restype = i32
