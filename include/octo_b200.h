@@ -234,10 +234,12 @@ int32_t octo_beam_gaussian(octo_ctx *ctx, octo_beam *beam, uint64_t seed, uint64
  * :node with the longitudinal kick: sR on the L mesh).  The copy is taken right after the deposit, before the
  * solve consumes the grid.  octo_captured_charge_plane synchronises the device and returns the int64 grid
  * (nx*ny, x fastest: grid[(iy-1)*nx + (ix-1)] is 1-based node (ix, iy)), the mesh it was deposited on
- * (mesh = {x0, y0, width, height}) and the fixed-point scale (a tap is round(w * 2^fixed_bits)); it fails
- * with OCTO_ERR_ARG when nothing was captured.  Capturing adds one device copy to that collide. */
+ * (mesh = {x0, y0, width, height}), the field mesh of its interaction (field_mesh, may be NULL) and the
+ * fixed-point scale (a tap is round(w * 2^fixed_bits)); it fails with OCTO_ERR_ARG when nothing was captured.
+ * Capturing adds three device copies to that collide. */
 int32_t octo_capture_charge_plane(octo_ctx *ctx, int32_t pair_i, int32_t pair_j, int32_t direction, int32_t plane);
-int32_t octo_captured_charge_plane(octo_ctx *ctx, int64_t *grid, double mesh[4], int32_t *fixed_bits);
+int32_t octo_captured_charge_plane(octo_ctx *ctx, int64_t *grid, double mesh[4], double field_mesh[4],
+                                   int32_t *fixed_bits);
 
 /* BF16 GEMM on the tensor cores (tcgen05.mma with a TMEM accumulator), the contraction of the learned field
  * correction's convolutions; no reference counterpart.  out[z][m][n] = sum over split z of k of A[m][k] B[n][k]
@@ -260,6 +262,39 @@ typedef struct {
     int64_t ldo;
 } octo_gemm_desc;
 int32_t octo_gemm_bf16(int32_t device, const octo_gemm_desc *desc, void *stream);
+
+/* The learned field correction's network (no reference counterpart): a 4-level U-Net of 3x3 convolutions with
+ * 32 base channels (627k parameters) whose convolutions run on the tensor cores (octo_gemm_bf16's kernel), with
+ * its forward pass, backward pass and Adam update on the GPU.  Input: NHWC bf16 [batch][height][width][8];
+ * output: fp32 [batch][height][width][2].  height and width multiples of 8 (>= 16); batch <= max_batch.
+ * Parameters are an fp32 vector (per layer: weights [Cout][3][3][Cin], then bias [Cout]). */
+typedef struct octo_cnn octo_cnn;
+octo_cnn *octo_cnn_create(int32_t device, int32_t height, int32_t width, int32_t max_batch, uint64_t seed);
+void octo_cnn_destroy(octo_cnn *net);
+int64_t octo_cnn_num_params(const octo_cnn *net);
+int32_t octo_cnn_get_params(octo_cnn *net, float *params, int64_t n);        /* host buffer of n floats */
+int32_t octo_cnn_set_params(octo_cnn *net, const float *params, int64_t n);
+/* input, output: device pointers; synchronises the stream. */
+int32_t octo_cnn_forward(octo_cnn *net, const void *input, int32_t batch, float *output, void *stream);
+/* One training step: forward, the mean-square loss of output channels 0..1 against target (fp32 [batch][h][w][2])
+ * weighted per pixel by mask (fp32 [batch][h][w], NULL = 1) and normalised by the total weight, the gradients of
+ * every parameter, and (update != 0) an Adam step of learning rate lr (beta 0.9 / 0.999, eps 1e-8).  loss and
+ * grads (host, num_params floats) may be NULL.  Synchronises the stream. */
+int32_t octo_cnn_train_step(octo_cnn *net, const void *input, const float *target, const float *mask, int32_t batch,
+                            float lr, int32_t update, double *loss, float *grads, void *stream);
+
+/* Attach the learned field correction to a Gaussian-subtracted hybrid context (options.gaussian = 1; no reference
+ * counterpart, the correction of gaussian_pic.jl's coarse-grid solve).  Every field-solve plane of the context's
+ * collides then gets the network's correction: its charge grid (grid units, the node charges over the plane total
+ * times the node count, with log(hy/hx) as a second channel) goes through the network after the deposit, and
+ * the output (dEx*hx, dEy*hy of a unit charge, times out_scale) is added to the plane's field cells after the
+ * solve, except within `edge` nodes of the mesh border.  The largest correction of a plane is its error
+ * estimate: octo_field_correction_report returns how many planes of the last collide exceeded `tolerance` (the
+ * caller's signal to fall back to the plain solver).  net = NULL detaches.  The network's height x width must be
+ * the grid's ny x nx and its max_batch at least the planes of a wavefront (4 per slice pair of the narrower
+ * beam's slice count).  The context keeps a pointer: destroy the network after detaching it. */
+int32_t octo_set_field_correction(octo_ctx *ctx, octo_cnn *net, float out_scale, float tolerance, int32_t edge);
+int32_t octo_field_correction_report(octo_ctx *ctx, int32_t *planes_over_tolerance);
 
 /* Message of the last failing call on this context (NUL-terminated, truncated to len). */
 int32_t octo_last_error(octo_ctx *ctx, char *buf, int64_t len);

@@ -42,7 +42,8 @@ struct GemmArgs {
     float *out;                   // fp32 result (when out_bf16 is null): out[z * split_stride + m * ldc + n]
     long long ldc, split_stride;
     int k_per_split;              // K range of blockIdx.z: [z * k_per_split, (z + 1) * k_per_split), multiple of kBK
-    const float *bias;            // bf16 epilogue: out_bf16[m * ldo + n] = bf16(max?(0, acc + bias[n]))
+    const float *bias;            // added per column (fp32 output: only without split-K); null = none
+                                  // bf16 epilogue: out_bf16[m * ldo + n] = bf16(max?(0, acc + bias[n]))
     int relu;
     __nv_bfloat16 *out_bf16;
     long long ldo;
@@ -230,8 +231,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_umma_gemm(const GemmArgs g)
                 } else {
                     float *o = g.out + (long long)blockIdx.z * g.split_stride + (long long)row * g.ldc + n0 + c0;
 #pragma unroll
-                    for (int j = 0; j < 32; ++j)
-                        if (n0 + c0 + j < g.N) o[j] = __uint_as_float(r[j]);
+                    for (int j = 0; j < 32; ++j) {
+                        const int n = n0 + c0 + j;
+                        if (n < g.N) o[j] = __uint_as_float(r[j]) + (g.bias ? g.bias[n] : 0.f);
+                    }
                 }
             }
         }

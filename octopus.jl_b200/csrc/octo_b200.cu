@@ -22,6 +22,7 @@
 #include "k_line.cuh"
 #include "k_moments.cuh"
 #include "k_misc.cuh"
+#include "k_learned.cuh"
 #include "k_pic.cuh"
 #include "k_slicing.cuh"
 #include "k_umma.cuh"
@@ -197,6 +198,33 @@ struct BeamWS {
 
 }  // namespace
 
+// ---------------------------------------------------------------- tensor-core GEMM launch
+namespace octo {
+namespace nn {
+// Picks the tile width from N (32, 64, 128 or 256 columns of fp32 accumulator in TMEM).
+void launch_gemm(const GemmArgs &g, int splits, cudaStream_t st) {
+    const int bn = g.N <= 32 ? 32 : (g.N <= 64 ? 64 : (g.N <= 128 ? 128 : 256));
+    const dim3 grid((unsigned)((g.M + kBM - 1) / kBM), (unsigned)((g.N + bn - 1) / bn), (unsigned)splits);
+    const size_t smem = umma_smem_bytes(bn);
+    auto go = [&](void (*kernel)(const GemmArgs)) {
+        CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        launch_pdl(kernel, grid, kGemmThreads, smem, st, g);
+    };
+    if (bn == 32) go(k_umma_gemm<32>);
+    else if (bn == 64) go(k_umma_gemm<64>);
+    else if (bn == 128) go(k_umma_gemm<128>);
+    else go(k_umma_gemm<256>);
+}
+}  // namespace nn
+}  // namespace octo
+
+#include "cnn_host.cuh"
+
+struct octo_cnn {
+    nn::Cnn net;
+    std::string err;
+};
+
 struct octo_ctx {
     int device = 0;
     int num_sms = 148;  // the device's SM count (block-count policies)
@@ -266,11 +294,19 @@ struct octo_ctx {
     double phase_ms[OCTO_NPHASES] = {0};
     long long phase_launches[OCTO_NPHASES] = {0};
     double phase_bytes[OCTO_NPHASES] = {0};
+    // learned field correction (octo_set_field_correction): the attached network (an octo_cnn), the scale of
+    // its outputs, the tolerance of the per-plane correction estimate, the untouched border, and the count of
+    // planes over tolerance in the last collide
+    octo_cnn *cnn = nullptr;
+    float cnn_scale = 1.f, cnn_tol = INFINITY;
+    int cnn_edge = 2;
+    DevBuf<int> cnn_flags;
+    PinBuf<int> h_cnn_flags;
     // octo_capture_charge_plane: one field-solve charge grid of the next collide, copied right after its
     // deposit, with the mesh it was deposited on
     int cap_armed = 0, cap_taken = 0, cap_i = 0, cap_j = 0, cap_dir = 0, cap_kind = 0, cap_bits = 0;
     DevBuf<long long> cap_q;
-    DevBuf<Grid> cap_grid;
+    DevBuf<Grid> cap_grid;  // [0] the source mesh the plane was deposited on, [1] the field mesh of its task
 };
 
 namespace {
@@ -885,6 +921,10 @@ void CollideJob::run() {
     // ---- status reset for this call (cache counters stay cumulative)
     launch_pdl(k_init_bounds, 1, 1, 0, st, nullptr, 0, nullptr, 0, nullptr, c->status.p, 1);
     launches += 1;
+    if (c->cnn) {
+        c->cnn_flags.ensure(1);
+        CK(cudaMemsetAsync(c->cnn_flags.p, 0, sizeof(int), st));
+    }
 
     // ---- node meshes at turn start
     if (node) {
@@ -1206,17 +1246,28 @@ void CollideJob::run() {
                 });
             });
         }
+        const bool learned = gaussian && c->cnn != nullptr;
+        if (learned) {  // the learned correction's input from the front's charge grids, and the network
+            if (F.np > c->cnn->net.maxB)
+                throw OctoFail{OCTO_ERR_ARG, "the field-correction network's max_batch is smaller than a wavefront's "
+                                             "plane count (" + std::to_string(F.np) + ")"};
+            launch_pdl(k_cnn_prep, F.np, 256, 0, st, C, F.p0, c->cnn->net.x0.p);
+            c->cnn->net.forward(F.np, st);
+            launches += 1 + 17;
+        }
         if (c->cap_armed && !c->cap_taken) {
             for (int t = F.t0; t < F.t0 + F.nt; ++t) {
                 const Task &T = tasks[t];
                 if (T.i != c->cap_i || T.j != c->cap_j || T.dir != c->cap_dir || c->cap_kind >= T.nplanes) continue;
                 const Plane &P = planes[T.plane0 + c->cap_kind];
                 c->cap_q.ensure(cells);
-                c->cap_grid.ensure(1);
+                c->cap_grid.ensure(2);
                 CK(cudaMemcpyAsync(c->cap_q.p, c->qgrid.p + (size_t)(T.plane0 + c->cap_kind - F.p0) * cells,
                                    sizeof(long long) * cells, cudaMemcpyDeviceToDevice, st));
                 const Grid *mesh = P.geom >= 0 ? &(c->nodes.p + P.geom)->sg : &(c->geom.p + t)->sg;
+                const Grid *fmesh = P.geom >= 0 ? &(c->nodes.p + P.geom)->fg : &(c->geom.p + t)->fg;
                 CK(cudaMemcpyAsync(c->cap_grid.p, mesh, sizeof(Grid), cudaMemcpyDeviceToDevice, st));
+                CK(cudaMemcpyAsync(c->cap_grid.p + 1, fmesh, sizeof(Grid), cudaMemcpyDeviceToDevice, st));
                 c->cap_bits = P.fixed_bits;
                 c->cap_taken = 1;
             }
@@ -1260,6 +1311,13 @@ void CollideJob::run() {
                     launch_pdl(k_conv_field<R>, dim3((ny + kFieldTile - 1) / kFieldTile, F.np), 128, field_smem(NX, rsz), st, C, F.p0);
                 }
             });
+        }
+        if (learned) {
+            with_real(fp32, [&](auto r) {
+                launch_pdl(k_cnn_apply<decltype(r)>, F.np, 256, 0, st, C, F.p0, (const float *)c->cnn->net.out.p,
+                           1.0f / c->cnn_scale, c->cnn_edge, c->cnn_tol, c->cnn_flags.p);
+            });
+            launches += 1;
         }
         if (lum_forked) CK(cudaStreamWaitEvent(st, c->ev_join, 0));  // the kick changes what the luminosity read
         {
@@ -1841,6 +1899,7 @@ void octo_destroy(octo_ctx *c) {
     c->spec.release(); c->fields.release(); c->lum_parts.release(); c->lum_partial.release(); c->node_ref.release(); c->stats.release();
     c->partial.release(); c->soa_ptrs.release();
     c->first_lum.release(); c->lum_tick.release(); c->cap_q.release(); c->cap_grid.release();
+    c->cnn_flags.release(); c->h_cnn_flags.release();
     c->hyb.release(); c->hmom.release(); c->hprof.release(); c->hsum.release(); c->qtot.release();
     c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_noderef.release(); c->h_slices.release();
     for (auto e : c->ev_pool) cudaEventDestroy(e);
@@ -2183,6 +2242,41 @@ int32_t octo_beam_gaussian(octo_ctx *c, octo_beam *beam, uint64_t seed, uint64_t
     }
 }
 
+int32_t octo_set_field_correction(octo_ctx *c, octo_cnn *net, float out_scale, float tolerance, int32_t edge) {
+    if (!c) return OCTO_ERR_ARG;
+    if (!net) {
+        c->cnn = nullptr;
+        return OCTO_OK;
+    }
+    if (!c->opt.gaussian)
+        return fail(c, OCTO_ERR_UNSUPPORTED, "the learned field correction corrects the Gaussian-subtracted hybrid "
+                                             "(GaussianPICPoissonSolver); this context runs the plain PIC solver");
+    if (net->net.H != c->opt.ny || net->net.W != c->opt.nx)
+        return fail(c, OCTO_ERR_ARG, "the network's height x width must equal the solver grid's ny x nx");
+    if (net->net.device != c->device) return fail(c, OCTO_ERR_ARG, "the network lives on another device");
+    if (!(out_scale > 0.f) || !(tolerance > 0.f) || edge < 0 || 2 * edge >= std::min(c->opt.nx, c->opt.ny))
+        return fail(c, OCTO_ERR_ARG, "out_scale and tolerance must be positive and edge below half the grid");
+    c->cnn = net;
+    c->cnn_scale = out_scale;
+    c->cnn_tol = tolerance;
+    c->cnn_edge = edge;
+    return OCTO_OK;
+}
+
+int32_t octo_field_correction_report(octo_ctx *c, int32_t *planes_over_tolerance) {
+    if (!c || !planes_over_tolerance) return OCTO_ERR_ARG;
+    if (!c->cnn || !c->cnn_flags.p) { *planes_over_tolerance = 0; return OCTO_OK; }
+    try {
+        CK(cudaSetDevice(c->device));
+        c->h_cnn_flags.ensure(1);
+        CK(cudaMemcpy(c->h_cnn_flags.p, c->cnn_flags.p, sizeof(int), cudaMemcpyDeviceToHost));
+        *planes_over_tolerance = c->h_cnn_flags.p[0];
+        return OCTO_OK;
+    } catch (CudaFail &e) {
+        return fail(c, OCTO_ERR_CUDA, e.msg);
+    }
+}
+
 int32_t octo_capture_charge_plane(octo_ctx *c, int32_t pair_i, int32_t pair_j, int32_t direction, int32_t plane) {
     if (!c) return OCTO_ERR_ARG;
     if (pair_i < 1 || pair_j < 1 || (direction != 1 && direction != 2) || plane < 0 || plane > 2)
@@ -2193,17 +2287,19 @@ int32_t octo_capture_charge_plane(octo_ctx *c, int32_t pair_i, int32_t pair_j, i
     return OCTO_OK;
 }
 
-int32_t octo_captured_charge_plane(octo_ctx *c, int64_t *grid, double mesh[4], int32_t *fixed_bits) {
+int32_t octo_captured_charge_plane(octo_ctx *c, int64_t *grid, double mesh[4], double field_mesh[4],
+                                   int32_t *fixed_bits) {
     if (!c || !grid || !mesh || !fixed_bits) return OCTO_ERR_ARG;
     if (!c->cap_armed || !c->cap_taken)
         return fail(c, OCTO_ERR_ARG, "capture: no charge plane was captured (not armed, or the pair did not run)");
     try {
         CK(cudaSetDevice(c->device));
         CK(cudaDeviceSynchronize());
-        Grid g{};
+        Grid g[2]{};
         CK(cudaMemcpy(grid, c->cap_q.p, sizeof(long long) * (size_t)c->opt.nx * c->opt.ny, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(&g, c->cap_grid.p, sizeof(Grid), cudaMemcpyDeviceToHost));
-        mesh[0] = g.x0; mesh[1] = g.y0; mesh[2] = g.w; mesh[3] = g.h;
+        CK(cudaMemcpy(g, c->cap_grid.p, 2 * sizeof(Grid), cudaMemcpyDeviceToHost));
+        mesh[0] = g[0].x0; mesh[1] = g[0].y0; mesh[2] = g[0].w; mesh[3] = g[0].h;
+        if (field_mesh) { field_mesh[0] = g[1].x0; field_mesh[1] = g[1].y0; field_mesh[2] = g[1].w; field_mesh[3] = g[1].h; }
         *fixed_bits = c->cap_bits;
         c->cap_armed = 0;
         c->cap_taken = 0;
@@ -2241,26 +2337,6 @@ int32_t octo_timing_report(octo_ctx *c, double ms[OCTO_NPHASES], int64_t launche
 
 }  // extern "C"
 
-// ---------------------------------------------------------------- tensor-core GEMM launch
-namespace octo {
-namespace nn {
-// Picks the tile width from N (32, 64, 128 or 256 columns of fp32 accumulator in TMEM).
-void launch_gemm(const GemmArgs &g, int splits, cudaStream_t st) {
-    const int bn = g.N <= 32 ? 32 : (g.N <= 64 ? 64 : (g.N <= 128 ? 128 : 256));
-    const dim3 grid((unsigned)((g.M + kBM - 1) / kBM), (unsigned)((g.N + bn - 1) / bn), (unsigned)splits);
-    const size_t smem = umma_smem_bytes(bn);
-    auto go = [&](void (*kernel)(const GemmArgs)) {
-        CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        launch_pdl(kernel, grid, kGemmThreads, smem, st, g);
-    };
-    if (bn == 32) go(k_umma_gemm<32>);
-    else if (bn == 64) go(k_umma_gemm<64>);
-    else if (bn == 128) go(k_umma_gemm<128>);
-    else go(k_umma_gemm<256>);
-}
-}  // namespace nn
-}  // namespace octo
-
 namespace {
 // Device status word of the tensor-core kernels (set to OCTO_ERR_TIMEOUT by a wait that gave up), one per
 // device, allocated on first use.
@@ -2274,6 +2350,7 @@ int *nn_error_flag() {
     return flag[dev];
 }
 }  // namespace
+
 
 // ---------------------------------------------------------------- allocation-free beam construction
 // Reduction scratch of octo_beam_gaussian_noalloc: OCTO_NOALLOC_MAX_BLOCKS block partial sums followed
@@ -2404,6 +2481,128 @@ int32_t octo_beam_gaussian_noalloc(int32_t device, octo_beam *beam, uint64_t see
         return OCTO_ERR_CUDA;
     }
     return OCTO_OK;
+}
+
+octo_cnn *octo_cnn_create(int32_t device, int32_t height, int32_t width, int32_t max_batch, uint64_t seed) {
+    if (height < 16 || width < 16 || height % 8 || width % 8 || max_batch < 1) return nullptr;
+    if ((long long)max_batch * height * width * 64 >= (1LL << 31)) return nullptr;
+    octo_cnn *c = new octo_cnn();
+    try {
+        c->net.create(device, height, width, max_batch, seed);
+        CK(cudaDeviceSynchronize());
+    } catch (CudaFail &) {
+        c->net.release();
+        delete c;
+        return nullptr;
+    }
+    return c;
+}
+
+void octo_cnn_destroy(octo_cnn *c) {
+    if (!c) return;
+    cudaSetDevice(c->net.device);
+    cudaDeviceSynchronize();
+    c->net.release();
+    delete c;
+}
+
+int64_t octo_cnn_num_params(const octo_cnn *c) { return c ? c->net.nparams : 0; }
+
+int32_t octo_cnn_get_params(octo_cnn *c, float *params, int64_t n) {
+    if (!c || !params || n != c->net.nparams) return OCTO_ERR_ARG;
+    try {
+        CK(cudaSetDevice(c->net.device));
+        CK(cudaDeviceSynchronize());
+        CK(cudaMemcpy(params, c->net.master.p, sizeof(float) * n, cudaMemcpyDeviceToHost));
+        return OCTO_OK;
+    } catch (CudaFail &e) {
+        c->err = e.msg;
+        return OCTO_ERR_CUDA;
+    }
+}
+
+int32_t octo_cnn_set_params(octo_cnn *c, const float *params, int64_t n) {
+    if (!c || !params || n != c->net.nparams) return OCTO_ERR_ARG;
+    try {
+        CK(cudaSetDevice(c->net.device));
+        CK(cudaDeviceSynchronize());
+        CK(cudaMemcpy(c->net.master.p, params, sizeof(float) * n, cudaMemcpyHostToDevice));
+        c->net.weights_dirty = true;
+        return OCTO_OK;
+    } catch (CudaFail &e) {
+        c->err = e.msg;
+        return OCTO_ERR_CUDA;
+    }
+}
+
+namespace {
+int cnn_status(octo_cnn *c, cudaStream_t st) {
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, c->net.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (e) {
+        CK(cudaMemsetAsync(c->net.err, 0, sizeof(int), st));
+        c->err = "a tensor-core wait gave up";
+        return OCTO_ERR_TIMEOUT;
+    }
+    return OCTO_OK;
+}
+}  // namespace
+
+int32_t octo_cnn_forward(octo_cnn *c, const void *input, int32_t batch, float *output, void *stream) {
+    if (!c || !input || !output || batch < 1 || batch > c->net.maxB) return OCTO_ERR_ARG;
+    try {
+        nn::Cnn &N = c->net;
+        CK(cudaSetDevice(N.device));
+        cudaStream_t st = (cudaStream_t)stream;
+        const long long M0 = N.ml(0, batch);
+        CK(cudaMemcpyAsync(N.x0.p, input, sizeof(nn::bf16) * M0 * nn::kCnnIn, cudaMemcpyDeviceToDevice, st));
+        N.forward(batch, st);
+        // channels 0 and 1 of the head
+        CK(cudaMemcpy2DAsync(output, 2 * sizeof(float), N.out.p, 8 * sizeof(float), 2 * sizeof(float), (size_t)M0,
+                             cudaMemcpyDeviceToDevice, st));
+        return cnn_status(c, st);
+    } catch (CudaFail &e) {
+        c->err = e.msg;
+        return OCTO_ERR_CUDA;
+    }
+}
+
+int32_t octo_cnn_train_step(octo_cnn *c, const void *input, const float *target, const float *mask, int32_t batch,
+                            float lr, int32_t update, double *loss, float *grads, void *stream) {
+    if (!c || !input || !target || batch < 1 || batch > c->net.maxB) return OCTO_ERR_ARG;
+    try {
+        nn::Cnn &N = c->net;
+        CK(cudaSetDevice(N.device));
+        cudaStream_t st = (cudaStream_t)stream;
+        const long long M0 = N.ml(0, batch);
+        double wt = (double)M0;
+        if (mask) {  // the loss is normalised by the total weight
+            std::vector<float> hm((size_t)M0);
+            CK(cudaMemcpyAsync(hm.data(), mask, sizeof(float) * M0, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            wt = 0.0;
+            for (float v : hm) wt += v;
+        }
+        CK(cudaMemcpyAsync(N.x0.p, input, sizeof(nn::bf16) * M0 * nn::kCnnIn, cudaMemcpyDeviceToDevice, st));
+        N.forward(batch, st);
+        const int nblk = N.backward(batch, target, mask, wt, st);
+        if (loss) {
+            CK(cudaMemcpyAsync(N.h_loss.p, N.loss_part.p, sizeof(double) * 2 * nblk, cudaMemcpyDeviceToHost, st));
+        }
+        if (grads) CK(cudaMemcpyAsync(grads, N.grad.p, sizeof(float) * N.nparams, cudaMemcpyDeviceToHost, st));
+        if (update) N.adam(lr, st);
+        const int rc = cnn_status(c, st);
+        if (loss) {
+            double se = 0.0;
+            for (int b = 0; b < nblk; ++b) se += N.h_loss.p[2 * b];
+            *loss = se / (2.0 * std::max(wt, 1e-300));
+        }
+        return rc;
+    } catch (CudaFail &e) {
+        c->err = e.msg;
+        return OCTO_ERR_CUDA;
+    }
 }
 
 int32_t octo_gemm_bf16(int32_t device, const octo_gemm_desc *d, void *stream) {

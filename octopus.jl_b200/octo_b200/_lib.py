@@ -26,7 +26,9 @@ EXPORTS = (
     "octo_normal_quantile", "octo_erfinv", "octo_version", "octo_set_timing", "octo_timing_report",
     "octo_beam_gaussian_noalloc", "octo_pic_collide_batch", "octo_set_timing_phases", "octo_pic_autotune",
     "octo_track_line", "octo_beam_moments", "octo_capture_charge_plane", "octo_captured_charge_plane",
-    "octo_gemm_bf16",
+    "octo_gemm_bf16", "octo_cnn_create", "octo_cnn_destroy", "octo_cnn_num_params", "octo_cnn_get_params",
+    "octo_cnn_set_params", "octo_cnn_forward", "octo_cnn_train_step", "octo_set_field_correction",
+    "octo_field_correction_report",
 )
 
 PHASES = ("slicing", "bounds", "plan", "green", "luminosity", "deposit", "fft", "field", "kick", "unsort", "node")
@@ -161,9 +163,27 @@ def lib():
     L.octo_capture_charge_plane.restype = i32
     L.octo_capture_charge_plane.argtypes = [vp, i32, i32, i32, i32]
     L.octo_captured_charge_plane.restype = i32
-    L.octo_captured_charge_plane.argtypes = [vp, P(i64), P(d), P(i32)]
+    L.octo_captured_charge_plane.argtypes = [vp, P(i64), P(d), P(d), P(i32)]
     L.octo_gemm_bf16.restype = i32
     L.octo_gemm_bf16.argtypes = [i32, P(OctoGemmDesc), vp]
+    L.octo_cnn_create.restype = vp
+    L.octo_cnn_create.argtypes = [i32, i32, i32, i32, u64]
+    L.octo_cnn_destroy.restype = None
+    L.octo_cnn_destroy.argtypes = [vp]
+    L.octo_cnn_num_params.restype = i64
+    L.octo_cnn_num_params.argtypes = [vp]
+    L.octo_cnn_get_params.restype = i32
+    L.octo_cnn_get_params.argtypes = [vp, P(C.c_float), i64]
+    L.octo_cnn_set_params.restype = i32
+    L.octo_cnn_set_params.argtypes = [vp, P(C.c_float), i64]
+    L.octo_cnn_forward.restype = i32
+    L.octo_cnn_forward.argtypes = [vp, vp, i32, vp, vp]
+    L.octo_cnn_train_step.restype = i32
+    L.octo_cnn_train_step.argtypes = [vp, vp, vp, vp, i32, C.c_float, i32, P(d), P(C.c_float), vp]
+    L.octo_set_field_correction.restype = i32
+    L.octo_set_field_correction.argtypes = [vp, vp, C.c_float, C.c_float, i32]
+    L.octo_field_correction_report.restype = i32
+    L.octo_field_correction_report.argtypes = [vp, P(i32)]
     L.octo_set_timing_phases.restype = i32
     L.octo_set_timing_phases.argtypes = [vp, C.c_uint32]
     L.octo_set_timing.restype = i32

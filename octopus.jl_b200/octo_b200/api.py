@@ -128,17 +128,20 @@ class Context:
         if rc != _lib.OCTO_OK:
             raise CollisionError(rc, _lib.last_error(self._ptr))
 
-    def captured_charge_plane(self):
+    def captured_charge_plane(self, with_field_mesh: bool = False):
         """The captured int64 grid as an (ny, nx) array (row iy-1 holds nodes (1..nx, iy)), the mesh
-        (x0, y0, width, height) and the fixed-point bits."""
+        (x0, y0, width, height) and the fixed-point bits; with_field_mesh: also the interaction's field mesh."""
         nx, ny = self.solver.grid
         q = np.zeros(nx * ny, dtype=np.int64)
         mesh = (C.c_double * 4)()
+        fmesh = (C.c_double * 4)()
         bits = C.c_int32()
-        rc = _lib.lib().octo_captured_charge_plane(self._ptr, q.ctypes.data_as(C.POINTER(C.c_int64)), mesh,
+        rc = _lib.lib().octo_captured_charge_plane(self._ptr, q.ctypes.data_as(C.POINTER(C.c_int64)), mesh, fmesh,
                                                    C.byref(bits))
         if rc != _lib.OCTO_OK:
             raise CollisionError(rc, _lib.last_error(self._ptr))
+        if with_field_mesh:
+            return q.reshape(ny, nx), tuple(mesh), tuple(fmesh), bits.value
         return q.reshape(ny, nx), tuple(mesh), bits.value
 
     def set_timing(self, enable: bool = True, phases=None):
