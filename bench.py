@@ -343,6 +343,8 @@ def run_ours(args, rank, world, local_rank):
     lines = None if args.no_line else time_lines(ob, e0, p0, args, stream, barrier, cpu_side)
     observer = None if args.no_line else time_observer(ob, e0, p0, args, stream)
     soft = None if args.no_line else time_soft_gaussian(ob, e0, p0, me, mp, rt, local_rank, args, stream, cpu_side)
+    learned = None if args.no_fast else time_learned(ob, e0, p0, me, mp, local_rank, args, stream, barrier, ms,
+                                                     world)
     clk = clocks.stop()
 
     # long-term tracking of both forms from the same beams (outside every timed region, one GPU only):
@@ -473,6 +475,7 @@ def run_ours(args, rank, world, local_rank):
         "line_tracking": lines,
         "moment_observer": observer,
         "soft_gaussian": soft,
+        "learned_form": learned,
         "clocks": clk,
         "luminosity": lum,
         "dominant_phase": dom[0],
@@ -554,6 +557,86 @@ def time_lines(ob, e0, p0, args, stream, barrier, cpu_side=True):
             "note": "each launch reads and writes the six FP64 coordinates once; a segment of maps alone runs "
                     "at the HBM bound, the radiation's six Philox draws and three Box-Muller transforms per "
                     "particle make the electron's after-collision segment instruction-issue bound"}
+
+
+def time_learned(ob, e0, p0, me, mp, local_rank, args, stream, barrier, plain_ms, world):
+    """The learned forms on the same workload: a 48x48 coarse solver with the tensor-core network's field
+    correction (octo_b200.learned, weights trained on the GPU by `python -m octo_b200.learned`), falling back
+    to the plain 128x128 :node solver when a plane's correction estimate exceeds twice the largest correction
+    seen in training.  "hybrid": the Gaussian-subtracted hybrid (FP64 beams); "pic": plain PIC in the
+    precision form (float32 beams).  Each: s/turn (collide + maps), the speed-up over the plain form, RMS
+    field error against exact Bassetti-Erskine with and without the correction, fallbacks, and the relative
+    emittance growth after --emittance-turns turns."""
+    import torch
+    from octo_b200 import learned as L
+    from octo_b200.diagnostics import emittances, field_error
+    out = {}
+    slicing = ob.LongitudinalSlicing(nslices=SLICES, method="normal_quantile", center_position="centroid")
+    for coarse, dtype in (("hybrid", torch.float64), ("pic", torch.float32)):
+        try:
+            net, meta = L.load_net(coarse=coarse, max_batch=64, device=local_rank)
+        except FileNotFoundError:
+            continue
+        tol = 2.0 * float(meta.get("max_abs_target", 5.0)) / L.OUT_SCALE
+        sol = L.coarse_solver(coarse, 48, slicing=slicing, deposit_method="CIC")
+        form = L.LearnedForm(sol, _solver(ob), net, tolerance=tol, device=local_rank, dtype=dtype)
+        eX, pX = ob.Beam(e0.to(dtype).clone(), ob.BeamParams(-1.0, ob.EMASS_EV, 10e9, ob.RE, 1.7e11)), \
+            ob.Beam(p0.to(dtype).clone(), ob.BeamParams(1.0, ob.PMASS_EV, 275e9, ob.RE * ob.ME0 / ob.PMASS_EV, 6.9e10))
+
+        def turnX(t):
+            lum = form.collide(eX, pX, turn=t, stream=stream)
+            me.track(eX, stream=stream)
+            mp.track(pX, stream=stream)
+            return lum
+
+        for t in range(args.warmup):
+            turnX(t)
+        torch.cuda.synchronize()
+        barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n0 = form.fallbacks
+        ev0.record(stream)
+        for t in range(args.steps):
+            lum = turnX(args.warmup + t)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        msX = ev0.elapsed_time(ev1) / args.steps
+        fb = form.fallbacks - n0
+        sy = E_BEAM["sigma"][1]
+        errs, errs_raw = {}, {}
+        for aspect in (1.0, 5.0, E_BEAM["sigma"][0] / sy, 25.0):
+            key = f"{aspect:.3g}"
+            errs[key] = field_error(sol, aspect * sy, sy, dtype, local_rank,
+                                    correction=(net, L.OUT_SCALE, 1e30, L.EDGE))["rms"]
+            errs_raw[key] = field_error(sol, aspect * sy, sy, dtype, local_rank)["rms"]
+        grow = None
+        if world == 1 and args.emittance_turns > 0:
+            eX.coords.copy_(e0.to(dtype))
+            pX.coords.copy_(p0.to(dtype))
+            start = (emittances(eX), emittances(pX))
+            for t in range(args.emittance_turns):
+                turnX(30_000 + t)
+            torch.cuda.synchronize()
+            end = (emittances(eX), emittances(pX))
+            grow = {beam: [end[k][q] / start[k][q] - 1.0 for q in range(3)] for k, beam in enumerate(("electron", "proton"))}
+        out[coarse] = {
+            "value": msX / 1e3 / world, "unit": UNIT, "ms_per_step": msX, "speedup_vs_plain": plain_ms / msX,
+            "form": (f"{'Gaussian-subtracted hybrid' if coarse == 'hybrid' else 'plain PIC'} on a 48x48 :slice_pair "
+                     f"grid (no Green cache), {'float64' if dtype == torch.float64 else 'float32'} beams, with the "
+                     "tensor-core CNN's field correction; plain 128x128 :node fallback"),
+            "luminosity": lum, "fallback_collides": fb, "timed_collides": args.steps,
+            "error_estimate_tolerance": tol,
+            "field_rms_err_vs_bassetti_erskine": errs, "field_rms_err_uncorrected": errs_raw,
+            "max_field_rms_err": max(errs.values()),
+            "heldout_rms_err_vs_fine_pic": {"uncorrected": float(meta.get("heldout_uncorrected", float("nan"))),
+                                            "learned": float(meta.get("heldout_learned", float("nan")))},
+            "emittance_growth": grow, "emittance_turns": args.emittance_turns if grow else 0,
+            "network": {"params": net.num_params, "trained_samples": int(meta.get("samples", 0)),
+                        "train_steps": int(meta.get("steps", 0))},
+        }
+        form.close()
+        net.close()
+    return out or None
 
 
 def time_soft_gaussian(ob, e0, p0, me, mp, rt, local_rank, args, stream, cpu_side=True):

@@ -264,7 +264,7 @@ typedef struct {
 int32_t octo_gemm_bf16(int32_t device, const octo_gemm_desc *desc, void *stream);
 
 /* The learned field correction's network (no reference counterpart): a 4-level U-Net of 3x3 convolutions with
- * 32 base channels (627k parameters) whose convolutions run on the tensor cores (octo_gemm_bf16's kernel), with
+ * 32 base channels (641k parameters) whose convolutions run on the tensor cores (octo_gemm_bf16's kernel), with
  * its forward pass, backward pass and Adam update on the GPU.  Input: NHWC bf16 [batch][height][width][8];
  * output: fp32 [batch][height][width][2].  height and width multiples of 8 (>= 16); batch <= max_batch.
  * Parameters are an fp32 vector (per layer: weights [Cout][3][3][Cin], then bias [Cout]). */
@@ -283,8 +283,10 @@ int32_t octo_cnn_forward(octo_cnn *net, const void *input, int32_t batch, float 
 int32_t octo_cnn_train_step(octo_cnn *net, const void *input, const float *target, const float *mask, int32_t batch,
                             float lr, int32_t update, double *loss, float *grads, void *stream);
 
-/* Attach the learned field correction to a Gaussian-subtracted hybrid context (options.gaussian = 1; no reference
- * counterpart, the correction of gaussian_pic.jl's coarse-grid solve).  Every field-solve plane of the context's
+/* Attach the learned field correction to a coarse-grid PIC context -- the Gaussian-subtracted hybrid (options.gaussian
+ * = 1, the correction of gaussian_pic.jl's coarse-grid solve) or the plain PIC solver -- with :slice_pair grids,
+ * linear slice interpolation, the :integrated Green function and green_cache = :none (no reference counterpart).
+ * Every field-solve plane of the context's
  * collides then gets the network's correction: its charge grid (grid units, the node charges over the plane total
  * times the node count, with log(hy/hx) as a second channel) goes through the network after the deposit, and
  * the output (dEx*hx, dEy*hy of a unit charge, times out_scale) is added to the plane's field cells after the

@@ -3,7 +3,7 @@
 // launch_pdl and launch_gemm.
 //
 // Network (a 4-level U-Net, 32 base channels, 3x3 convolutions with padding 1, ReLU, 2x2 average pooling,
-// nearest upsampling with skip concatenation; 627k parameters):
+// nearest upsampling with skip concatenation; 641k parameters):
 //   level 0 (H x W):       e1a 8 -> 32, e1b 32 -> 32 (skip s1)
 //   level 1 (H/2 x W/2):   e2a 32 -> 64, e2b 64 -> 64 (skip s2)
 //   level 2 (H/4 x W/4):   e3a 64 -> 128, e3b 128 -> 128 (skip s3)

@@ -301,6 +301,7 @@ struct octo_ctx {
     float cnn_scale = 1.f, cnn_tol = INFINITY;
     int cnn_edge = 2;
     DevBuf<int> cnn_flags;
+    DevBuf<long long> cnn_q;  // total fixed-point charge per plane of the front
     PinBuf<int> h_cnn_flags;
     // octo_capture_charge_plane: one field-solve charge grid of the next collide, copied right after its
     // deposit, with the mesh it was deposited on
@@ -1246,12 +1247,13 @@ void CollideJob::run() {
                 });
             });
         }
-        const bool learned = gaussian && c->cnn != nullptr;
+        const bool learned = c->cnn != nullptr;
         if (learned) {  // the learned correction's input from the front's charge grids, and the network
             if (F.np > c->cnn->net.maxB)
                 throw OctoFail{OCTO_ERR_ARG, "the field-correction network's max_batch is smaller than a wavefront's "
                                              "plane count (" + std::to_string(F.np) + ")"};
-            launch_pdl(k_cnn_prep, F.np, 256, 0, st, C, F.p0, c->cnn->net.x0.p);
+            c->cnn_q.ensure((size_t)c->cnn->net.maxB);
+            launch_pdl(k_cnn_prep, F.np, 256, 0, st, C, F.p0, c->cnn->net.x0.p, c->cnn_q.p);
             c->cnn->net.forward(F.np, st);
             launches += 1 + 17;
         }
@@ -1315,7 +1317,7 @@ void CollideJob::run() {
         if (learned) {
             with_real(fp32, [&](auto r) {
                 launch_pdl(k_cnn_apply<decltype(r)>, F.np, 256, 0, st, C, F.p0, (const float *)c->cnn->net.out.p,
-                           1.0f / c->cnn_scale, c->cnn_edge, c->cnn_tol, c->cnn_flags.p);
+                           (const long long *)c->cnn_q.p, 1.0f / c->cnn_scale, c->cnn_edge, c->cnn_tol, c->cnn_flags.p);
             });
             launches += 1;
         }
@@ -1899,7 +1901,7 @@ void octo_destroy(octo_ctx *c) {
     c->spec.release(); c->fields.release(); c->lum_parts.release(); c->lum_partial.release(); c->node_ref.release(); c->stats.release();
     c->partial.release(); c->soa_ptrs.release();
     c->first_lum.release(); c->lum_tick.release(); c->cap_q.release(); c->cap_grid.release();
-    c->cnn_flags.release(); c->h_cnn_flags.release();
+    c->cnn_flags.release(); c->h_cnn_flags.release(); c->cnn_q.release();
     c->hyb.release(); c->hmom.release(); c->hprof.release(); c->hsum.release(); c->qtot.release();
     c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_noderef.release(); c->h_slices.release();
     for (auto e : c->ev_pool) cudaEventDestroy(e);
@@ -2248,9 +2250,13 @@ int32_t octo_set_field_correction(octo_ctx *c, octo_cnn *net, float out_scale, f
         c->cnn = nullptr;
         return OCTO_OK;
     }
-    if (!c->opt.gaussian)
-        return fail(c, OCTO_ERR_UNSUPPORTED, "the learned field correction corrects the Gaussian-subtracted hybrid "
-                                             "(GaussianPICPoissonSolver); this context runs the plain PIC solver");
+    if (c->opt.solver != OCTO_SOLVER_PIC || c->opt.interaction_grid != OCTO_GRID_SLICE_PAIR ||
+        c->opt.slice_interpolation != 0 || c->opt.green_cache != OCTO_CACHE_NONE ||
+        c->opt.green_type != OCTO_GREEN_INTEGRATED)
+        return fail(c, OCTO_ERR_UNSUPPORTED,
+                    "the learned field correction runs on a PIC (or Gaussian-subtracted hybrid) collide with "
+                    ":slice_pair grids, linear slice interpolation, the :integrated Green function and "
+                    "green_cache = :none (so every field mesh is its source mesh shifted by whole cells)");
     if (net->net.H != c->opt.ny || net->net.W != c->opt.nx)
         return fail(c, OCTO_ERR_ARG, "the network's height x width must equal the solver grid's ny x nx");
     if (net->net.device != c->device) return fail(c, OCTO_ERR_ARG, "the network lives on another device");

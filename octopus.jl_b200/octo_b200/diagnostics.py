@@ -55,9 +55,10 @@ def quantile_lattice(n: int, sx: float, sy: float) -> Tuple[np.ndarray, np.ndarr
 
 
 def field_error(solver, sx: float, sy: float, dtype: torch.dtype = torch.float64, device: int = 0,
-                n_source: int = 400, n_probe: int = 81, extent: float = 4.0) -> Dict[str, float]:
+                n_source: int = 400, n_probe: int = 81, extent: float = 4.0, correction=None) -> Dict[str, float]:
     """RMS and max field error of one collide of `solver` (slice_pair or node grid, any deposit and
-    derivative) against exact Bassetti-Erskine, for an (sx, sy) Gaussian source slice."""
+    derivative) against exact Bassetti-Erskine, for an (sx, sy) Gaussian source slice.  correction: a learned
+    field correction to attach, (network, out_scale, tolerance, edge) (octo_b200.learned)."""
     from dataclasses import replace
 
     from .api import Context
@@ -81,8 +82,17 @@ def field_error(solver, sx: float, sy: float, dtype: torch.dtype = torch.float64
     b2 = Beam.from_numpy(prb, p, device=dev, dtype=dtype)
     ctx = Context(s, device, dtype)
     try:
+        if correction is not None:
+            from . import _lib
+            net, out_scale, tol, edge = correction
+            rc = _lib.lib().octo_set_field_correction(ctx.ptr, net.ptr, float(out_scale), float(tol), int(edge))
+            if rc != _lib.OCTO_OK:
+                raise RuntimeError(_lib.last_error(ctx.ptr))
         ctx.collide(b1, b2, turn=1, compute_luminosity=False)
     finally:
+        if correction is not None:
+            from . import _lib
+            _lib.lib().octo_set_field_correction(ctx.ptr, None, 1.0, 1.0, 0)
         ctx.close()
     out = b2.coords.to(torch.float64).cpu().numpy()
     # kick = 2 kbb2 / n1 * sum_taps w E(n1 unit charges) = 2 E_unit

@@ -3,7 +3,7 @@ Gaussian-subtracted hybrid solver (GaussianPICPoissonSolver, src/tasks/strongstr
 counterpart in the reference.
 
 ``FieldCorrectionNet`` wraps libocto_b200's network (octo_cnn_*): a 4-level U-Net of 3x3 convolutions, 32 base
-channels, 627k parameters, whose convolutions, gradients and Adam update run on the GPU in the library's own
+channels, 641k parameters, whose convolutions, gradients and Adam update run on the GPU in the library's own
 tcgen05 kernels.  Inputs are NHWC bf16 [batch, height, width, 8]; outputs fp32 [batch, height, width, 2].
 """
 from __future__ import annotations
@@ -134,11 +134,26 @@ def sample_density(kind: str, n: int, aspect: float, gen: torch.Generator, devic
     raise ValueError(kind)
 
 
-def _probe_solvers(grid: int, fine: int):
-    from .solver import GaussianPICPoissonSolver, LongitudinalSlicing, PICPoissonSolver
-    common = dict(green_cache="none", slicing=LongitudinalSlicing(nslices=1, method="normal_quantile"), kbb1=1.0,
-                  kbb2=1.0, luminosity_scale=1.0)
-    return GaussianPICPoissonSolver(grid=(grid, grid), **common), PICPoissonSolver(grid=(fine, fine), **common)
+COARSE = ("hybrid", "pic")  # the coarse solver the network corrects: the Gaussian-subtracted hybrid or plain PIC
+
+
+def coarse_solver(kind: str, grid: int, **kw):
+    """The coarse solver of a learned form: :slice_pair grids, :integrated Green function without the Green
+    cache (every field mesh is its source mesh shifted by whole cells), linear slice interpolation."""
+    from .solver import GaussianPICPoissonSolver, PICPoissonSolver
+    kw = dict(kw, green_cache="none")
+    if kind == "hybrid":
+        return GaussianPICPoissonSolver(grid=(grid, grid), **kw)
+    if kind == "pic":
+        return PICPoissonSolver(grid=(grid, grid), **kw)
+    raise ValueError(kind)
+
+
+def _probe_solvers(grid: int, fine: int, coarse: str = "hybrid"):
+    from .solver import LongitudinalSlicing, PICPoissonSolver
+    common = dict(slicing=LongitudinalSlicing(nslices=1, method="normal_quantile"), kbb1=1.0, kbb2=1.0,
+                  luminosity_scale=1.0)
+    return coarse_solver(coarse, grid, **common), PICPoissonSolver(grid=(fine, fine), green_cache="none", **common)
 
 
 class PairGenerator:
@@ -151,10 +166,10 @@ class PairGenerator:
     which sit at the field mesh's nodes inside that box; field node (i, j) is source node (i + sx, j + sy), the
     field mesh being the source mesh shifted by whole cells (no Green cache, the :integrated alignment)."""
 
-    def __init__(self, grid: int = 48, fine: int = 128, device: int = 0):
+    def __init__(self, grid: int = 48, fine: int = 128, device: int = 0, coarse: str = "hybrid"):
         from .api import Context
         self.grid, self.fine, self.device = grid, fine, device
-        sh, sf = _probe_solvers(grid, fine)
+        sh, sf = _probe_solvers(grid, fine, coarse)
         self.ctx_h = Context(sh, device)
         self.ctx_f = Context(sf, device)
         self.dev = torch.device(f"cuda:{device}")
@@ -222,10 +237,10 @@ class PairGenerator:
 
 
 def make_dataset(n_samples: int, seed: int, grid: int = 48, fine: int = 128, n_src: int = 200_000, device: int = 0,
-                 kinds=KINDS, aspects=(1.0, 25.0)):
+                 kinds=KINDS, aspects=(1.0, 25.0), coarse: str = "hybrid"):
     """n_samples seeded pairs over the density kinds (round robin), aspect ratios log-uniform in `aspects`
     (one in five with the narrow axis along x).  Returns device tensors X (bf16 [N, H, W, 8]), T, M, F."""
-    gen = PairGenerator(grid, fine, device)
+    gen = PairGenerator(grid, fine, device, coarse)
     dev = gen.dev
     tg = torch.Generator(device=dev)
     tg.manual_seed(int(seed))
@@ -272,8 +287,9 @@ def train(net: FieldCorrectionNet, X, T, M, steps: int, batch: int = 64, lr: flo
 
 
 def evaluate(net: FieldCorrectionNet, X, T, M, F, batch: int = 64) -> dict:
-    """RMS field error of the coarse hybrid alone and with the correction, against the fine plain-PIC field at
-    the corrected nodes, each relative to the fine field's RMS (the same units throughout)."""
+    """RMS field error of the coarse solver alone ("hybrid" key, whichever coarse solver made the pairs) and
+    with the correction ("learned"), against the fine plain-PIC field at the corrected nodes, each relative to
+    the fine field's RMS (the same units throughout)."""
     num_h = num_c = den = 0.0
     for s in range(0, X.shape[0], batch):
         x = X[s:s + batch].contiguous()
@@ -286,9 +302,9 @@ def evaluate(net: FieldCorrectionNet, X, T, M, F, batch: int = 64) -> dict:
     return {"hybrid": math.sqrt(num_h / den), "learned": math.sqrt(num_c / den)}
 
 
-def default_weights_path(grid: int = 48) -> str:
+def default_weights_path(grid: int = 48, coarse: str = "hybrid") -> str:
     import os
-    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", f"field_correction_{grid}.npz")
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", f"field_correction_{coarse}_{grid}.npz")
 
 
 def save_weights(net: FieldCorrectionNet, path: str, **meta) -> None:
@@ -298,9 +314,9 @@ def save_weights(net: FieldCorrectionNet, path: str, **meta) -> None:
                         out_scale=OUT_SCALE, edge=EDGE, **{k: np.asarray(v) for k, v in meta.items()})
 
 
-def load_net(path: str = None, max_batch: int = 64, device: int = 0) -> tuple:
+def load_net(path: str = None, max_batch: int = 64, device: int = 0, coarse: str = "hybrid") -> tuple:
     """A network with the saved parameters, and the file's metadata."""
-    path = path or default_weights_path()
+    path = path or default_weights_path(coarse=coarse)
     d = np.load(path)
     net = FieldCorrectionNet(int(d["height"]), int(d["width"]), max_batch=max_batch, device=device)
     net.set_params(d["params"])
@@ -309,17 +325,16 @@ def load_net(path: str = None, max_batch: int = 64, device: int = 0) -> tuple:
 
 # ------------------------------------------------------------------------------------------------ the learned form
 class LearnedForm:
-    """The learned form of the collide: the Gaussian-subtracted hybrid on a coarse grid with the network's
-    field correction, falling back to the plain solver for a collide in which any plane's error estimate (its
-    largest correction) exceeded the tolerance -- the beams are restored from a copy taken before the collide
-    and the plain solver runs instead.  `hybrid` must use green_cache = "none" (so every field mesh is its
-    source mesh shifted by whole cells)."""
+    """The learned form of the collide: a coarse-grid solver (the Gaussian-subtracted hybrid, or plain PIC; see
+    coarse_solver) with the network's field correction, falling back to the plain solver for a collide in which
+    any plane's error estimate (its largest correction) exceeded the tolerance -- the beams are restored from a
+    copy taken before the collide and the plain solver runs instead."""
 
-    def __init__(self, hybrid, plain, net: FieldCorrectionNet, tolerance: float, device: int = 0,
+    def __init__(self, coarse, plain, net: FieldCorrectionNet, tolerance: float, device: int = 0,
                  dtype=torch.float64, out_scale: float = OUT_SCALE, edge: int = EDGE):
         from .api import Context
         self.net = net
-        self.ctx = Context(hybrid, device, dtype)
+        self.ctx = Context(coarse, device, dtype)
         self.fallback = Context(plain, device, dtype)
         rc = _lib.lib().octo_set_field_correction(self.ctx.ptr, net.ptr, float(out_scale), float(tolerance), int(edge))
         if rc != _lib.OCTO_OK:
@@ -364,12 +379,13 @@ def _main(argv=None):
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--grid", type=int, default=48)
     ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--coarse", default="hybrid", choices=COARSE)
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     import time
     t0 = time.time()
-    X, T, M, F = make_dataset(a.samples, a.seed, grid=a.grid)
-    Xh, Th, Mh, Fh = make_dataset(a.heldout, a.seed + 1, grid=a.grid)
+    X, T, M, F = make_dataset(a.samples, a.seed, grid=a.grid, coarse=a.coarse)
+    Xh, Th, Mh, Fh = make_dataset(a.heldout, a.seed + 1, grid=a.grid, coarse=a.coarse)
     t1 = time.time()
     net = FieldCorrectionNet(a.grid, a.grid, max_batch=max(64, a.batch), seed=a.seed)
     before = evaluate(net, Xh, Th, Mh, Fh)
@@ -377,13 +393,14 @@ def _main(argv=None):
     t2 = time.time()
     after = evaluate(net, Xh, Th, Mh, Fh)
     tmax = float((Th.abs() * Mh[..., None]).amax())
-    res = {"samples": a.samples, "heldout": a.heldout, "steps": a.steps, "data_s": t1 - t0, "train_s": t2 - t1,
+    res = {"coarse": a.coarse, "samples": a.samples, "heldout": a.heldout, "steps": a.steps, "data_s": t1 - t0,
+           "train_s": t2 - t1,
            "heldout_rms_err": after, "initial_net_rms_err": before, "final_loss": losses[-1],
            "heldout_max_abs_target": tmax}
     print(json.dumps(res))
-    path = a.out or default_weights_path(a.grid)
-    save_weights(net, path, heldout_hybrid=after["hybrid"], heldout_learned=after["learned"], samples=a.samples,
-                 steps=a.steps, seed=a.seed, max_abs_target=tmax)
+    path = a.out or default_weights_path(a.grid, a.coarse)
+    save_weights(net, path, coarse=a.coarse, heldout_uncorrected=after["hybrid"], heldout_learned=after["learned"],
+                 samples=a.samples, steps=a.steps, seed=a.seed, max_abs_target=tmax)
     print("saved", path)
 
 
