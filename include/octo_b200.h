@@ -43,6 +43,9 @@ extern "C" {
 #define OCTO_GRID_NODE 2
 #define OCTO_SLICING_NORMAL_QUANTILE 0
 #define OCTO_SLICING_SPECIFIED 1
+#define OCTO_SLICING_EQUAL_AREA 2   /* LongitudinalSlicing()'s default (slicing.jl:104-156) */
+#define OCTO_SLICING_EQUAL_COUNT 3  /* slicing.jl:330-365 */
+#define OCTO_SLICING_EQUAL_WIDTH 4  /* also :equal_spaced (slicing.jl:367-388) */
 #define OCTO_CENTER_CENTROID 0
 #define OCTO_CENTER_MIDPOINT 1
 
@@ -101,6 +104,7 @@ typedef struct {
     int32_t virtual_drift;             /* 0 = :hirata, 1 = :chromatic, 2 = :exact (strong_beam.jl:20-30, 517-606) */
     int32_t include_sigma_xy;          /* 1: the full (coupled) transverse slice covariance */
     double min_sigma;                  /* transverse RMS floor, finite and >= 0 */
+    int32_t resolution1, resolution2;  /* LongitudinalSlicing resolution (:equal_area bins per slice); 0 = 100 */
 } octo_pic_options;
 #define OCTO_SOLVER_PIC 0
 #define OCTO_SOLVER_SOFT_GAUSSIAN 1
@@ -154,6 +158,14 @@ int32_t octo_pic_collide_batch(int32_t count, octo_ctx *const *ctx, octo_beam *c
  * kick is its own.  The collides update beam1 and beam2 in place, so pass scratch copies.  rounds: 1..16. */
 int32_t octo_pic_autotune(octo_ctx *ctx, octo_beam *beam1, octo_beam *beam2, const octo_beam_params *p1,
                           const octo_beam_params *p2, int32_t rounds, int32_t *choice, void *stream);
+
+/* Order of the particles inside each slice of a plain PIC context's working copy (no reference counterpart;
+ * the reference keeps caller order, slicing.jl:431-521).  1 (default): grouped by transverse position (a 64 x 64
+ * binning of each slice's box), so the kick's field gathers of a warp touch neighbouring cells; 0: caller order.
+ * The plain PIC collide does not depend on this order -- charge and luminosity grids are exact int64 sums and
+ * every kick is its own particle's -- so both give bit-identical results.  The Gaussian-subtracted hybrid and the
+ * soft-Gaussian solver always keep caller order (their slice moments are ordered floating-point sums). */
+int32_t octo_set_particle_order(octo_ctx *ctx, int32_t order);
 
 /* Green-cache counters (the contract of Contracts.jl:947-960). */
 int32_t octo_green_cache_stats(octo_ctx *ctx, int64_t *hits, int64_t *misses, int64_t *rebuilds);

@@ -691,8 +691,11 @@ __device__ __forceinline__ T *generic_ptr(T *p) {
     return p;
 }
 // TOTAL: also return the sum of the quanta (the hybrid's neutralisation needs the plane's exact charge).
+// rot (CIC): the lane's four atomics start at tap rot & 3 -- particles of a spatially ordered slice share
+// cells with their warp neighbours, and rotating the tap order spreads a warp's simultaneous atomics over
+// four addresses per cell.  Integer sums: the order changes nothing.
 template <class R, int METHOD, bool TOTAL = false>
-__device__ __forceinline__ long long deposit_taps(R u, R v, int nw, int nh, R scale, long long *grid, int ld) {
+__device__ __forceinline__ long long deposit_taps(R u, R v, int nw, int nh, R scale, long long *grid, int ld, int rot = 0) {
     constexpr int NT = METHOD == 0 ? 2 : 3;
     int ix, iy;
     long long total = 0;
@@ -700,16 +703,35 @@ __device__ __forceinline__ long long deposit_taps(R u, R v, int nw, int nh, R sc
     if (METHOD == 0) { cic_weights(u, nw, ix, wx); cic_weights(v, nh, iy, wy); }
     else { tsc_weights(u, nw, ix, wx); tsc_weights(v, nh, iy, wy); }
     const int c0 = (iy - 1) * ld + (ix - 1);
-#pragma unroll
-    for (int m = 0; m < NT; ++m)
-#pragma unroll
-        for (int k = 0; k < NT; ++k) {
-            const long long qv = round_ll(wx[m] * wy[k] * scale);
-            if (TOTAL) total += qv;
-            // a zero quantum (out-of-range particle: base 1, every weight 0) adds nothing; the unconditional
-            // atomic measured faster than the test
-            atomicAdd((unsigned long long *)&grid[c0 + k * ld + m], (unsigned long long)qv);
+    if constexpr (METHOD == 0) {
+        long long q0 = round_ll(wx[0] * wy[0] * scale), q1 = round_ll(wx[0] * wy[1] * scale);
+        long long q2 = round_ll(wx[1] * wy[0] * scale), q3 = round_ll(wx[1] * wy[1] * scale);
+        if (TOTAL) total = q0 + q1 + q2 + q3;
+        int o0 = c0, o1 = c0 + ld, o2 = c0 + 1, o3 = c0 + ld + 1;
+        if (rot & 1) {
+            const int to = o0; o0 = o1; o1 = o2; o2 = o3; o3 = to;
+            const long long tq = q0; q0 = q1; q1 = q2; q2 = q3; q3 = tq;
         }
+        if (rot & 2) {
+            int to = o0; o0 = o2; o2 = to; to = o1; o1 = o3; o3 = to;
+            long long tq = q0; q0 = q2; q2 = tq; tq = q1; q1 = q3; q3 = tq;
+        }
+        atomicAdd((unsigned long long *)&grid[o0], (unsigned long long)q0);
+        atomicAdd((unsigned long long *)&grid[o1], (unsigned long long)q1);
+        atomicAdd((unsigned long long *)&grid[o2], (unsigned long long)q2);
+        atomicAdd((unsigned long long *)&grid[o3], (unsigned long long)q3);
+    } else {
+#pragma unroll
+        for (int m = 0; m < NT; ++m)
+#pragma unroll
+            for (int k = 0; k < NT; ++k) {
+                const long long qv = round_ll(wx[m] * wy[k] * scale);
+                if (TOTAL) total += qv;
+                // a zero quantum (out-of-range particle: base 1, every weight 0) adds nothing; the unconditional
+                // atomic measured faster than the test
+                atomicAdd((unsigned long long *)&grid[c0 + k * ld + m], (unsigned long long)qv);
+            }
+    }
     return total;
 }
 
@@ -758,6 +780,7 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
     const R xlo = x0, xhi = (R)(sg.x0 + sg.w), ylo = y0, yhi = (R)(sg.y0 + sg.h);
     int outside = 0;
     long long total = 0;
+    const int rot = C.o.dep_rotate ? (int)(threadIdx.x & 3) : 0;
     // the next particle's coordinates are loaded before the current one's taps, two loads in flight
     const long long stride = (long long)gridDim.x * blockDim.x;
     auto sweep = [&](auto with_total) {
@@ -775,7 +798,7 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
             const R yd = cy + cpy * s;
             if (P.count_dropped && !(isfinite(xd) && xlo <= xd && xd <= xhi && isfinite(yd) && ylo <= yd && yd <= yhi))
                 ++outside;
-            total += deposit_taps<R, METHOD, TOT>((xd - x0) * hxi, (yd - y0) * hyi, nx, ny, scale, acc, nx);
+            total += deposit_taps<R, METHOD, TOT>((xd - x0) * hxi, (yd - y0) * hyi, nx, ny, scale, acc, nx, rot);
             cx = nx_; cpx = npx; cy = ny_; cpy = npy;
         }
     };
@@ -827,6 +850,7 @@ __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0, int
     const R hxi = (R)(1.0 / L.hx), hyi = (R)(1.0 / L.hy);
     const R x0 = (R)L.x0, y0 = (R)L.y0;
     const long long stride = (long long)gridDim.x * blockDim.x;
+    const int rot = C.o.dep_rotate ? (int)(threadIdx.x & 3) : 0;
     long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     R cx = 0, cpx = 0, cy = 0, cpy = 0;
     if (k < n) { cx = X[st + k]; cpx = PX[st + k]; cy = Y[st + k]; cpy = PY[st + k]; }
@@ -838,7 +862,7 @@ __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0, int
         }
         const R vx = cx + cpx * s;
         const R vy = cy + cpy * s;
-        deposit_taps<R, METHOD>((vx - x0) * hxi, (vy - y0) * hyi, nw, nh, scale, acc, nw);
+        deposit_taps<R, METHOD>((vx - x0) * hxi, (vy - y0) * hyi, nw, nh, scale, acc, nw, rot);
         cx = nx_; cpx = npx; cy = ny_; cpy = npy;
     }
     if (local) {

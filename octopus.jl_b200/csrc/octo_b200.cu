@@ -8,6 +8,8 @@
 // luminosity parts and status are read back once at the end.
 #include <cuda_runtime.h>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -183,6 +185,13 @@ constexpr long long kChunk = 8192;   // particles per slicing block
 
 struct BeamWS {
     DevBuf<double> s[6];  // slice-sorted coordinates (sized in doubles; float elements in the precision form)
+    DevBuf<double> t[6];  // the spatially ordered copy (plain PIC), swapped into s once written
+    DevBuf<unsigned long long> box;  // spatial order: slice boxes
+    DevBuf<int> cursor;              // spatial order: bin counts / cursors
+    DevBuf<long long> hist;          // :equal_area histogram
+    DevBuf<unsigned long long> rkey, rkey_sorted;  // :equal_count rank sort
+    DevBuf<int> rval, rval_sorted;
+    DevBuf<char> sort_tmp;
     DevBuf<int> dest;  // caller index -> slice-sorted position
     DevBuf<SliceInfo> info;
     DevBuf<double> lane_sum, lane_min, lane_max, lanes, q;
@@ -191,6 +200,9 @@ struct BeamWS {
     long long total = 0;
     void release() {
         for (auto &b : s) b.release();
+        for (auto &b : t) b.release();
+        box.release(); cursor.release(); hist.release(); rkey.release(); rkey_sorted.release(); rval.release();
+        rval_sorted.release(); sort_tmp.release();
         dest.release(); info.release(); lane_sum.release(); lane_min.release(); lane_max.release();
         lanes.release(); q.release(); counts.release(); blockoff.release();
     }
@@ -231,6 +243,8 @@ struct octo_ctx {
     // launch shape (octo_pic_autotune): the deposit launches at least dep_waves waves of the SMs per front,
     // the kick sizes its blocks to fill kick_slots times the resident block slots
     int dep_waves = 1, kick_slots = 1;
+    // plain PIC: group each slice's particles by transverse position in the working copy (octo_set_particle_order)
+    int spatial = 1;
     octo_pic_options opt{};
     std::vector<double> pos[2];
     DevOptions dopt{};
@@ -393,8 +407,14 @@ int validate_options(const octo_pic_options &o, std::string &msg) {
         int ns = b == 0 ? o.nslices1 : o.nslices2;
         int m = b == 0 ? o.slicing_method1 : o.slicing_method2;
         if (ns < 1 || ns > kMaxSlices) { msg = "nslices must be in 1..64 on this backend"; return OCTO_ERR_ARG; }
-        if (m != OCTO_SLICING_NORMAL_QUANTILE && m != OCTO_SLICING_SPECIFIED) {
-            msg = "slicing method must be :normal_quantile or :specified on this backend";
+        if (m < OCTO_SLICING_NORMAL_QUANTILE || m > OCTO_SLICING_EQUAL_WIDTH) {
+            msg = "slicing method must be :normal_quantile, :specified, :equal_area, :equal_count or :equal_width";
+            return OCTO_ERR_ARG;
+        }
+        const int res = b == 0 ? o.resolution1 : o.resolution2;
+        if (res < 0) { msg = "slicing resolution must be positive"; return OCTO_ERR_ARG; }
+        if (m == OCTO_SLICING_EQUAL_AREA && (long long)ns * (res > 0 ? res : 100) > 16384) {
+            msg = "this backend's :equal_area histogram holds at most 16384 bins (nslices * resolution)";
             return OCTO_ERR_UNSUPPORTED;
         }
         const double *p = b == 0 ? o.positions1 : o.positions2;
@@ -556,7 +576,21 @@ void slice_beams(octo_ctx *c, const octo_beam &b1, const octo_beam &b2, cudaStre
             A.method[b] = b == 0 ? c->opt.slicing_method1 : c->opt.slicing_method2;
             A.ns[b] = c->ns[b];
             A.cpos[b] = b == 0 ? c->opt.center_position1 : c->opt.center_position2;
+            const int res = b == 0 ? c->opt.resolution1 : c->opt.resolution2;
+            A.resolution[b] = res > 0 ? res : 100;
+            if (A.method[b] == kEqualArea) {
+                W.hist.ensure((size_t)A.ns[b] * A.resolution[b]);
+                CK(cudaMemsetAsync(W.hist.p, 0, sizeof(long long) * A.ns[b] * A.resolution[b], st));
+                A.hist[b] = W.hist.p;
+            }
+            if (A.method[b] == kEqualCount) {
+                W.rkey.ensure(B.n); W.rkey_sorted.ensure(B.n); W.rval.ensure(B.n); W.rval_sorted.ensure(B.n);
+                A.rkey[b] = W.rkey.p; A.rkey_sorted[b] = W.rkey_sorted.p;
+                A.rval[b] = W.rval.p; A.rval_sorted[b] = W.rval_sorted.p;
+            }
         }
+        const bool any_area = A.method[0] == kEqualArea || A.method[1] == kEqualArea;
+        const bool any_count = A.method[0] == kEqualCount || A.method[1] == kEqualCount;
         const long long iters = (std::max(b1.n, b2.n) + kFoldLanes - 1) / kFoldLanes;
         const int rows = (int)std::min<long long>(kLaneFoldRows, std::max<long long>(1, iters));
         const size_t fold_smem = sizeof(double) * 33 * (size_t)rows;
@@ -564,6 +598,35 @@ void slice_beams(octo_ctx *c, const octo_beam &b1, const octo_beam &b2, cudaStre
         launch_pdl(k_fold_stats<R>, 2, 1024, 0, st, A, 0);
         launch_pdl(k_lane_fold<R>, dim3(kFoldLanes / 32, 1, 2), kLaneFoldThreads, fold_smem, st, A, 1, rows);
         launch_pdl(k_fold_stats<R>, 2, 1024, 0, st, A, 1);
+        if (any_area) {  // :equal_area boundaries from the z histogram
+            long long bins = 1;
+            for (int b = 0; b < 2; ++b)
+                if (A.method[b] == kEqualArea) bins = std::max<long long>(bins, (long long)A.ns[b] * A.resolution[b]);
+            CK(cudaFuncSetAttribute(k_area_hist<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * bins)));
+            CK(cudaFuncSetAttribute(k_area_bounds<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(8 * bins)));
+            launch_pdl(k_area_hist<R>, dim3((unsigned)nblk_max, 1, 2), 256, (size_t)(4 * bins), st, A, kChunk);
+            launch_pdl(k_area_bounds<R>, 2, 1024, (size_t)(8 * bins), st, A);
+            launches += 2;
+        }
+        if (any_count) {  // :equal_count: rank order by a stable radix sort of z, then the rank scatter
+            const unsigned kb = (unsigned)std::min<long long>(148 * 8, (std::max(b1.n, b2.n) + 255) / 256);
+            launch_pdl(k_rank_keys<R>, dim3(kb, 1, 2), 256, 0, st, A);
+            for (int b = 0; b < 2; ++b) {
+                if (A.method[b] != kEqualCount) continue;
+                BeamWS &W = c->bw[b];
+                const int n = (int)(b == 0 ? b1.n : b2.n);
+                size_t tmp = 0;
+                CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, W.rkey.p, W.rkey_sorted.p, W.rval.p, W.rval_sorted.p, n,
+                                                   0, 64, st));
+                W.sort_tmp.ensure(tmp);
+                CK(cub::DeviceRadixSort::SortPairs((void *)W.sort_tmp.p, tmp, W.rkey.p, W.rkey_sorted.p, W.rval.p,
+                                                   W.rval_sorted.p, n, 0, 64, st));
+                launches += 4;
+            }
+            launch_pdl(k_rank_bounds<R>, 2, 32, 0, st, A, kAlign);
+            launch_pdl(k_rank_scatter<R>, dim3(kb, 1, 2), 256, 0, st, A);
+            launches += 3;
+        }
         launch_pdl(k_slice_count<R>, dim3((unsigned)nblk_max, 1, 2), 256, 0, st, A, kChunk);
         launch_pdl(k_slice_offsets<R>, 2, 1024, 0, st, A, kAlign);
         launch_pdl(k_slice_scatter<R>, dim3((unsigned)nblk_max, 1, 2), kScatterThreads, 0, st, A, kChunk);
@@ -571,6 +634,38 @@ void slice_beams(octo_ctx *c, const octo_beam &b1, const octo_beam &b2, cudaStre
         launch_pdl(k_slice_finish<R>, dim3(ns_max, 2), 1024, 0, st, A);
     });
     launches += 9;
+    // plain PIC: the working copy in spatial order (the centroid lanes above used the stable copy)
+    if (c->spatial && c->opt.solver == OCTO_SOLVER_PIC && !c->opt.gaussian) {
+        with_real(c->fp32, [&](auto r) {
+            using R = decltype(r);
+            SpatialArgs<R> S{};
+            for (int b = 0; b < 2; ++b) {
+                BeamWS &W = c->bw[b];
+                const octo_beam &B = b == 0 ? b1 : b2;
+                for (auto &a : W.t) a.ensure(W.total);
+                W.box.ensure((size_t)4 * c->ns[b]);
+                W.cursor.ensure((size_t)kSpatialCells * c->ns[b]);
+                CK(cudaMemsetAsync(W.cursor.p, 0, sizeof(int) * kSpatialCells * c->ns[b], st));
+                const void *cc[6] = {B.x, B.px, B.y, B.py, B.z, B.pz};
+                for (int k = 0; k < 6; ++k) { S.c[b][k] = (const R *)cc[k]; S.t[b][k] = (R *)W.t[k].p; }
+                S.dest[b] = W.dest.p;
+                S.info[b] = W.info.p;
+                S.box[b] = W.box.p;
+                S.cursor[b] = W.cursor.p;
+                S.n[b] = B.n;
+                S.nblocks[b] = (B.n + kChunk - 1) / kChunk;
+            }
+            launch_pdl(k_init_boxes, (unsigned)((4 * (c->ns[0] + c->ns[1]) + 255) / 256), 256, 0, st, c->bw[0].box.p,
+                       (long long)4 * c->ns[0], c->bw[1].box.p, (long long)4 * c->ns[1]);
+            launch_pdl(k_spatial_boxes<R>, dim3((unsigned)nblk_max, 1, 2), 256, 0, st, S, kChunk);
+            launch_pdl(k_spatial_count<R>, dim3((unsigned)nblk_max, 1, 2), 256, 0, st, S, kChunk);
+            launch_pdl(k_spatial_scan<R>, dim3(ns_max, 2), 1024, 0, st, S);
+            launch_pdl(k_spatial_scatter<R>, dim3((unsigned)nblk_max, 1, 2), 256, 0, st, S, kChunk);
+        });
+        for (int b = 0; b < 2; ++b)
+            for (int k = 0; k < 6; ++k) std::swap(c->bw[b].s[k], c->bw[b].t[k]);
+        launches += 5;
+    }
     CK(cudaGetLastError());
 }
 
@@ -883,6 +978,7 @@ void CollideJob::run() {
 
     Collide C{};
     C.o = c->dopt;
+    C.o.dep_rotate = (c->spatial && !c->opt.gaussian) ? 1 : 0;  // spatially ordered slices (slice_beams)
     C.klum = klum;
     for (int b = 0; b < 2; ++b)
         for (int k = 0; k < 6; ++k) C.beam[b].c[k] = c->bw[b].s[k].p;
@@ -2242,6 +2338,12 @@ int32_t octo_beam_gaussian(octo_ctx *c, octo_beam *beam, uint64_t seed, uint64_t
     } catch (CudaFail &e) {
         return fail(c, OCTO_ERR_CUDA, e.msg);
     }
+}
+
+int32_t octo_set_particle_order(octo_ctx *c, int32_t order) {
+    if (!c || (order != 0 && order != 1)) return OCTO_ERR_ARG;
+    c->spatial = order;
+    return OCTO_OK;
 }
 
 int32_t octo_set_field_correction(octo_ctx *c, octo_cnn *net, float out_scale, float tolerance, int32_t edge) {

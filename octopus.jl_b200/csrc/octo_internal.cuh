@@ -245,6 +245,7 @@ struct DevOptions {
     int green_type, green_cache, fourth, quadratic, node, longitudinal_kick;
     int dep_global, lum_global;  // charge / luminosity grid larger than shared memory: global atomics
     int gaussian, neutralize;    // GaussianPICPoissonSolver (Gaussian-subtracted hybrid)
+    int dep_rotate;              // rotate each lane's deposit tap order (spatially ordered slices)
     double min_ex, min_ey, quantize, min_ratio, growth;
     double margin;               // hybrid: Gaussian containment half-width in sigmas
 };

@@ -50,6 +50,7 @@ struct OctoPicOptions
     precision::Int32; gaussian::Int32; margin_sigma::Float64; neutralize::Int32
     solver::Int32; gaussian_when_luminosity::Int32; ignore_centroid1::Int32; ignore_centroid2::Int32
     virtual_drift::Int32; include_sigma_xy::Int32; min_sigma::Float64
+    resolution1::Int32; resolution2::Int32
 end
 
 # include/octo_b200.h: octo_collide_report
@@ -114,16 +115,20 @@ _soft_of(s::B200GaussianPoissonSolver) = s.soft
 
 _sym(v, table) = Int32(table[Symbol(v)])
 
+# OCTO_SLICING_* codes; the aliases of interface.jl:793-797 map to their methods
+const _SLICING_CODE = Dict(:normal_quantile => 0, :gaussian => 0, :Gaussian => 0, :specified => 1,
+                           :equal_area => 2, :equal_count => 3, :equal_width => 4, :equal_spaced => 4)
+
 function _slicing_fields(s::LongitudinalSlicing)
-    s.method in (:normal_quantile, :gaussian, :Gaussian, :specified) || throw(ArgumentError(
-        "slicing method $(repr(s.method)) is not implemented by the B200 backend; use :normal_quantile or :specified"))
-    return (s.method === :specified ? Int32(1) : Int32(0), Int32(s.nslices),
-            s.center_position === :centroid ? Int32(0) : Int32(1))
+    haskey(_SLICING_CODE, s.method) || throw(ArgumentError(
+        "unsupported longitudinal slicing method $(repr(s.method))"))
+    return (Int32(_SLICING_CODE[s.method]), Int32(s.nslices), s.center_position === :centroid ? Int32(0) : Int32(1),
+            Int32(s.resolution))
 end
 
 function _options(p::PICPoissonSolver, keep::Vector{Any}, precision::Integer=0, gaussian=nothing; soft=nothing)
-    m1, n1, c1 = _slicing_fields(p.slicing1)
-    m2, n2, c2 = _slicing_fields(p.slicing2)
+    m1, n1, c1, r1 = _slicing_fields(p.slicing1)
+    m2, n2, c2, r2 = _slicing_fields(p.slicing2)
     pos1 = Float64.(p.slicing1.positions); pos2 = Float64.(p.slicing2.positions)
     push!(keep, pos1, pos2)
     lg = p.luminosity_grid === nothing ? (0, 0) : p.luminosity_grid
@@ -152,7 +157,8 @@ function _options(p::PICPoissonSolver, keep::Vector{Any}, precision::Integer=0, 
         Int32(soft === nothing ? 0 : soft.ignore_centroid1), Int32(soft === nothing ? 0 : soft.ignore_centroid2),
         Int32(soft === nothing ? 0 : soft.virtual_drift isa Octopus.ChromaticDrift ? 1 :
               soft.virtual_drift isa Octopus.ExactHamiltonianDrift ? 2 : 0),
-        Int32(soft === nothing ? 0 : soft.include_sigma_xy), soft === nothing ? 0.0 : Float64(soft.min_sigma))
+        Int32(soft === nothing ? 0 : soft.include_sigma_xy), soft === nothing ? 0.0 : Float64(soft.min_sigma),
+        r1, r2)
 end
 
 """Context: device workspaces and the slice-pair Green cache (the twin of task.runtime_cache)."""

@@ -28,7 +28,7 @@ EXPORTS = (
     "octo_track_line", "octo_beam_moments", "octo_capture_charge_plane", "octo_captured_charge_plane",
     "octo_gemm_bf16", "octo_cnn_create", "octo_cnn_destroy", "octo_cnn_num_params", "octo_cnn_get_params",
     "octo_cnn_set_params", "octo_cnn_forward", "octo_cnn_train_step", "octo_set_field_correction",
-    "octo_field_correction_report",
+    "octo_field_correction_report", "octo_set_particle_order",
 )
 
 PHASES = ("slicing", "bounds", "plan", "green", "luminosity", "deposit", "fft", "field", "kick", "unsort", "node")
@@ -88,6 +88,7 @@ class OctoPicOptions(C.Structure):
         ("ignore_centroid1", C.c_int32), ("ignore_centroid2", C.c_int32),
         ("virtual_drift", C.c_int32), ("include_sigma_xy", C.c_int32),
         ("min_sigma", C.c_double),
+        ("resolution1", C.c_int32), ("resolution2", C.c_int32),
     ]
 
 
@@ -184,6 +185,8 @@ def lib():
     L.octo_set_field_correction.argtypes = [vp, vp, C.c_float, C.c_float, i32]
     L.octo_field_correction_report.restype = i32
     L.octo_field_correction_report.argtypes = [vp, P(i32)]
+    L.octo_set_particle_order.restype = i32
+    L.octo_set_particle_order.argtypes = [vp, i32]
     L.octo_set_timing_phases.restype = i32
     L.octo_set_timing_phases.argtypes = [vp, C.c_uint32]
     L.octo_set_timing.restype = i32

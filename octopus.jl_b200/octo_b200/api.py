@@ -116,6 +116,13 @@ class Context:
             raise CollisionError(rc, f"{_lib.ERROR_NAMES.get(rc, rc)}: {_lib.last_error(self._ptr)}", None)
         return choice.value
 
+    def set_particle_order(self, spatial: bool = True):
+        """Plain PIC: keep each slice's particles grouped by transverse position (default) or in caller order;
+        results are bit-identical either way, only the speed differs."""
+        rc = _lib.lib().octo_set_particle_order(self._ptr, 1 if spatial else 0)
+        if rc != _lib.OCTO_OK:
+            raise CollisionError(rc, "octo_set_particle_order failed")
+
     def green_cache_stats(self) -> Tuple[int, int, int]:
         h, m, r = C.c_int64(), C.c_int64(), C.c_int64()
         _lib.lib().octo_green_cache_stats(self._ptr, C.byref(h), C.byref(m), C.byref(r))

@@ -24,6 +24,11 @@ _SLICING_METHODS = ("equal_area", "equal_count", "equal_width", "equal_spaced", 
                     "Gaussian", "specified")
 
 
+# OCTO_SLICING_* codes (the aliases of interface.jl:793-797 map to their methods)
+_METHOD_CODE = {"normal_quantile": 0, "gaussian": 0, "Gaussian": 0, "specified": 1, "equal_area": 2,
+                "equal_count": 3, "equal_width": 4, "equal_spaced": 4}
+
+
 @dataclass(frozen=True)
 class LongitudinalSlicing:
     """LongitudinalSlicing(; nslices=1, method=:equal_area, resolution=100, center_position=:centroid,
@@ -161,7 +166,8 @@ class PICPoissonSolver:
         o.longitudinal_kick = int(bool(self.longitudinal_kick))
         keep = []
         for k, s in ((1, self.resolved_slicing1), (2, self.resolved_slicing2)):
-            setattr(o, f"slicing_method{k}", 1 if s.method == "specified" else 0)
+            setattr(o, f"slicing_method{k}", _METHOD_CODE[s.method])
+            setattr(o, f"resolution{k}", int(s.resolution))
             setattr(o, f"nslices{k}", int(s.nslices))
             setattr(o, f"center_position{k}", 0 if s.center_position == "centroid" else 1)
             if s.method == "specified" and s.positions:
@@ -198,9 +204,9 @@ def _require_gpu_options(s: PICPoissonSolver):
         raise ArgumentError("green_type = :lattice (an experimental CPU study kernel) is not implemented by the GPU "
                             "PIC backend; use :integrated or :standard.")
     for k, sl in ((1, s.resolved_slicing1), (2, s.resolved_slicing2)):
-        if sl.method not in ("normal_quantile", "gaussian", "Gaussian", "specified"):
-            raise ArgumentError(f"slicing{k} method :{sl.method} is not implemented by the GPU PIC backend; use "
-                                ":normal_quantile (the production method) or :specified.")
+        if sl.method == "equal_area" and sl.nslices * sl.resolution > 16384:
+            raise ArgumentError("the GPU PIC backend's :equal_area histogram holds at most 16384 bins "
+                                "(nslices * resolution)")
         if sl.nslices > 64:
             raise ArgumentError("the GPU PIC backend supports at most 64 slices per beam")
     def fft_ok(n):

@@ -698,9 +698,85 @@ double lane_indexed_sum(const double *z, const std::vector<int64_t> &idx) {
     return s;
 }
 
-// slicing.jl:51-75, 405-460, 523-559 and the :specified method slicing.jl:393-403
+// _slice_bin (slicing.jl:177-181): the 1-based bin of zi, 0 for a coordinate with none.  d lies within the
+// live extrema here, so the clamp never meets an overflowing floor.
+int64_t slice_bin(double zi, double zmin, double width, int64_t bins) {
+    const double d = (zi - zmin) / width;
+    if (!(d > -INFINITY && d < INFINITY)) return 0;
+    const double f = std::floor(d);
+    if (f >= (double)bins) return bins;
+    if (f < 0.0) return 1;
+    return jclampi((long)f + 1, 1, (long)bins);
+}
+
+// Julia's collect(range(start, stop; length = len)) for Float64 endpoints (Base twiceprecision.jl,
+// _linspace(start, stop, len)): a reference element of smallest magnitude, a step split into a truncated high
+// part and a low part fitted so both endpoints are reproduced, and each element evaluated in double-double
+// arithmetic around the reference index.  Julia first tries an exact-rational form when both endpoints are
+// ratios of integers below 2^24 (rat / lcm); that branch is not restated: for such endpoints it can differ
+// from this one in the last bit of interior elements.
+std::vector<double> julia_range(double start, double stop, int64_t len) {
+    std::vector<double> out((size_t)len);
+    if (len == 1) { out[0] = start; return out; }
+    if (start == stop) { std::fill(out.begin(), out.end(), start); return out; }
+    auto add12 = [](double x, double y, double &h, double &l) {
+        if (std::fabs(y) > std::fabs(x)) std::swap(x, y);
+        h = x + y;
+        l = (x - h) + y;
+    };
+    double delta = stop - start;
+    int64_t dfac = 1;
+    if (!std::isfinite(delta)) { delta = stop / (double)len - start / (double)len; dfac = len; }
+    const double tmin = -(start / delta) / (double)dfac;
+    int64_t imin = (int64_t)std::nearbyint(tmin * (double)(len - 1) + 1);  // round(Int, x): ties to even
+    double ref, step;
+    if (1 < imin && imin < len) {
+        const double t = (double)(imin - 1) / (double)(len - 1);
+        ref = (1 - t) * start + t * stop;
+        step = imin - 1 < len - imin ? (ref - start) / (double)(imin - 1) : (stop - ref) / (double)(len - imin);
+    } else if (imin <= 1) {
+        imin = 1;
+        ref = start;
+        step = (delta / (double)(len - 1)) * (double)dfac;
+    } else {
+        imin = len;
+        ref = stop;
+        step = (delta / (double)(len - 1)) * (double)dfac;
+    }
+    const double m = std::nextafter(std::numeric_limits<double>::max(), 0.0);
+    const double k = (double)std::max(imin - 1, len - imin);
+    const double lo = jmax(-(m + ref) / k, (-m + ref) / k), hi = jmin((m - ref) / k, (m + ref) / k);
+    const double step_pre = jclamp(step, lo, hi);
+    // nbitslen(Float64, len, imin) = min(cld(53, 2), top_set_bit(max(imin - 1, len - imin) - 1))
+    const uint64_t span = (uint64_t)(std::max(imin - 1, len - imin) - 1);
+    int nb = 0;
+    for (uint64_t v = span; v; v >>= 1) ++nb;
+    nb = std::min(nb, 27);
+    uint64_t bits;
+    std::memcpy(&bits, &step_pre, 8);
+    bits &= (~0ull) << nb;
+    double step_hi;
+    std::memcpy(&step_hi, &bits, 8);
+    double x1h, x1l, x2h, x2l;
+    add12((double)(1 - imin) * step_hi, ref, x1h, x1l);
+    add12((double)(len - imin) * step_hi, ref, x2h, x2l);
+    const double a = (start - x1h) - x1l, b = (stop - x2h) - x2l;
+    const double step_lo = (b - a) / (double)(len - 1);
+    const double ref_lo = a - (double)(1 - imin) * step_lo;
+    for (int64_t i = 1; i <= len; ++i) {
+        const double u = (double)(i - imin);
+        const double sh = u * step_hi, sl = u * step_lo;
+        double xh, xl;
+        add12(ref, sh, xh, xl);
+        out[(size_t)(i - 1)] = xh + (xl + (sl + ref_lo));
+    }
+    return out;
+}
+
+// slicing.jl:51-75, 405-460, 523-559, the :specified method slicing.jl:393-403, :equal_area slicing.jl:104-156,
+// :equal_count slicing.jl:330-365 and :equal_width slicing.jl:367-388
 Slices make_slices(int method, int ns, int center_position, const std::vector<double> &positions, const double *z,
-                   int64_t n) {
+                   int64_t n, int resolution = 100) {
     if (ns <= 0) throw OracleError(OO_ERR_ARG, "nslices must be positive");
     if (n <= 0) throw OracleError(OO_ERR_ARG, "longitudinal slicing requires at least one particle");
     double zmin = INFINITY, zmax = -INFINITY;
@@ -727,6 +803,99 @@ Slices make_slices(int method, int ns, int center_position, const std::vector<do
         b[0] = zmin; b[b.size() - 1] = zmax;
         for (size_t i = 0; i < internal.size(); ++i) b[i + 1] = jclamp(internal[i], b[0], b[b.size() - 1]);
         ns = (int)b.size() - 1;
+    } else if (method == 2) {  // :equal_area
+        if (resolution <= 0) throw OracleError(OO_ERR_ARG, "resolution must be positive");
+        const int64_t bins = (int64_t)ns * resolution;
+        if (zmin == zmax) {
+            std::fill(b.begin(), b.end(), zmin);
+        } else {
+            const double width = (zmax - zmin) / (double)bins;
+            std::vector<int64_t> counts((size_t)bins, 0);
+            for (int64_t i = 0; i < n; ++i) {
+                const int64_t bin = slice_bin(z[i], zmin, width, bins);
+                if (bin) ++counts[(size_t)(bin - 1)];
+            }
+            std::vector<double> cum((size_t)bins);
+            int64_t run = 0;
+            for (int64_t k = 0; k < bins; ++k) {
+                run += counts[(size_t)k];
+                cum[(size_t)k] = (double)run / (double)std::max<int64_t>(n, 1);
+            }
+            cum[(size_t)(bins - 1)] = 1.0;
+            auto center = [&](int64_t i1) { return zmin + ((double)i1 - 0.5) * width; };
+            b[0] = zmin;
+            b[ns] = zmax;
+            int64_t current = 1;
+            for (int s = 1; s <= ns - 1; ++s) {
+                const double target = (double)s / (double)ns;
+                while (current <= bins && cum[(size_t)(current - 1)] <= target) ++current;
+                double x1, x2, y1, y2;
+                if (current <= 1) { x1 = b[0]; x2 = center(1); y1 = 0.0; y2 = cum[0]; }
+                else if (current > bins) { x1 = center(bins); x2 = b[ns]; y1 = cum[(size_t)(bins - 2)]; y2 = 1.0; }
+                else { x1 = center(current - 1); x2 = center(current); y1 = cum[(size_t)(current - 2)]; y2 = cum[(size_t)(current - 1)]; }
+                b[s] = y2 == y1 ? (x1 + x2) / 2 : x2 * (target - y1) / (y2 - y1) + x1 * (target - y2) / (y1 - y2);
+            }
+        }
+    } else if (method == 3) {  // :equal_count: membership by rank (ties by index), boundaries at rank midpoints
+        std::vector<int64_t> order((size_t)n);
+        for (int64_t i = 0; i < n; ++i) order[(size_t)i] = i;
+        auto key = [&](int64_t i) {  // isless order of doubles (-0.0 < +0.0)
+            uint64_t u;
+            std::memcpy(&u, &z[i], 8);
+            return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+        };
+        std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t c) { return key(a) < key(c); });
+        b[0] = zmin;
+        b[ns] = zmax;
+        for (int s = 1; s <= ns - 1; ++s) {
+            const int64_t pos = (int64_t)std::floor((double)((int64_t)s * n) / (double)ns);
+            b[s] = pos == 0 ? z[order[0]] : (pos == n ? z[order[(size_t)(n - 1)]]
+                                                     : (z[order[(size_t)(pos - 1)]] + z[order[(size_t)pos]]) / 2);
+        }
+        for (double v : b)
+            if (!std::isfinite(v)) throw OracleError(OO_ERR_NONFINITE, "non-finite beam coordinate (longitudinal slicing)");
+        Slices S;
+        S.boundary = b;
+        S.indices.assign(ns, {});
+        for (int s = 1; s <= ns; ++s) {
+            const int64_t first = (int64_t)std::floor((double)((int64_t)(s - 1) * n) / (double)ns);
+            const int64_t last = (int64_t)std::floor((double)((int64_t)s * n) / (double)ns);
+            for (int64_t r = first; r < last; ++r) S.indices[s - 1].push_back(order[(size_t)r]);
+        }
+        S.center.resize(ns);
+        S.weight.resize(ns);
+        for (int s = 0; s < ns; ++s) {
+            const auto &idx = S.indices[s];
+            S.weight[s] = (double)idx.size() / (double)n;
+            S.center[s] = center_position == 0 && !idx.empty() ? lane_indexed_sum(z, idx) / (double)idx.size()
+                                                               : (b[s] + b[s + 1]) / 2;
+        }
+        return S;
+    } else if (method == 4) {  // :equal_width
+        if (!(std::isfinite(zmin) && std::isfinite(zmax)))
+            throw OracleError(OO_ERR_NONFINITE, "non-finite beam coordinate (longitudinal slicing)");
+        b = julia_range(zmin, zmax, ns + 1);
+        Slices S;
+        S.boundary = b;
+        S.indices.assign(ns, {});
+        if (zmin == zmax) {
+            for (int64_t i = 0; i < n; ++i) S.indices[0].push_back(i);
+        } else {
+            const double width = (zmax - zmin) / (double)ns;
+            for (int64_t i = 0; i < n; ++i) {
+                const int64_t bin = slice_bin(z[i], zmin, width, ns);
+                if (bin) S.indices[(size_t)(bin - 1)].push_back(i);
+            }
+        }
+        S.center.resize(ns);
+        S.weight.resize(ns);
+        for (int s = 0; s < ns; ++s) {
+            const auto &idx = S.indices[s];
+            S.weight[s] = (double)idx.size() / (double)n;
+            S.center[s] = center_position == 0 && !idx.empty() ? lane_indexed_sum(z, idx) / (double)idx.size()
+                                                               : (b[s] + b[s + 1]) / 2;
+        }
+        return S;
     } else {
         throw OracleError(OO_ERR_UNSUPPORTED, "unsupported slicing method");
     }
@@ -1407,8 +1576,10 @@ double collide(Ctx &C, double *b1[6], int64_t n1, double *b2[6], int64_t n2, con
                const oo_beam_params &p2, bool compute_lum) {
     Options &O = C.O;
     validate(O);
-    Slices s1 = make_slices(O.o.slicing_method1, O.o.nslices1, O.o.center_position1, O.pos1, b1[4], n1);
-    Slices s2 = make_slices(O.o.slicing_method2, O.o.nslices2, O.o.center_position2, O.pos2, b2[4], n2);
+    Slices s1 = make_slices(O.o.slicing_method1, O.o.nslices1, O.o.center_position1, O.pos1, b1[4], n1,
+                            O.o.resolution1 > 0 ? O.o.resolution1 : 100);
+    Slices s2 = make_slices(O.o.slicing_method2, O.o.nslices2, O.o.center_position2, O.pos2, b2[4], n2,
+                            O.o.resolution2 > 0 ? O.o.resolution2 : 100);
     int ns1 = (int)s1.center.size(), ns2 = (int)s2.center.size();
     if (C.cache.empty() || ns1 != C.ns1 || ns2 != C.ns2) {
         C.ns1 = ns1; C.ns2 = ns2;
@@ -1700,12 +1871,18 @@ double oo_luminosity(const oo_options *opt, const double *x1, const double *y1, 
     return lum;
 }
 
+void oo_julia_range(double start, double stop, int64_t len, double *out) {
+    const std::vector<double> r = julia_range(start, stop, len);
+    std::copy(r.begin(), r.end(), out);
+}
+
 int oo_slices(int32_t method, int32_t ns, int32_t center_position, const double *positions, const double *z,
-              int64_t n, double *boundary, double *center, double *weight, int64_t *count, int64_t *order) {
+              int64_t n, double *boundary, double *center, double *weight, int64_t *count, int64_t *order,
+              int32_t resolution) {
     try {
         std::vector<double> pos;
         if (method == 1 && positions) pos.assign(positions, positions + (ns - 1));
-        Slices S = make_slices(method, ns, center_position, pos, z, n);
+        Slices S = make_slices(method, ns, center_position, pos, z, n, resolution > 0 ? resolution : 100);
         int m = (int)S.center.size();
         for (int s = 0; s <= m; ++s) boundary[s] = S.boundary[s];
         int64_t k = 0;
@@ -2297,8 +2474,10 @@ int oo_gaussian_collide(const oo_options *opt, double min_sigma, int32_t gaussia
         std::vector<double> pos1, pos2;
         if (opt->slicing_method1 == 1 && opt->positions1) pos1.assign(opt->positions1, opt->positions1 + opt->nslices1 - 1);
         if (opt->slicing_method2 == 1 && opt->positions2) pos2.assign(opt->positions2, opt->positions2 + opt->nslices2 - 1);
-        Slices s1 = make_slices(opt->slicing_method1, opt->nslices1, opt->center_position1, pos1, b1[4], n1);
-        Slices s2 = make_slices(opt->slicing_method2, opt->nslices2, opt->center_position2, pos2, b2[4], n2);
+        Slices s1 = make_slices(opt->slicing_method1, opt->nslices1, opt->center_position1, pos1, b1[4], n1,
+                                opt->resolution1 > 0 ? opt->resolution1 : 100);
+        Slices s2 = make_slices(opt->slicing_method2, opt->nslices2, opt->center_position2, pos2, b2[4], n2,
+                                opt->resolution2 > 0 ? opt->resolution2 : 100);
         if (!opt->has_kbb1 && !(std::isfinite(p1->E0) && p1->E0 != 0))
             throw OracleError(OO_ERR_ARG, "beam1 E0 must be finite and nonzero when kbb1 is not specified");
         if (!opt->has_kbb2 && !(std::isfinite(p2->E0) && p2->E0 != 0))

@@ -48,7 +48,8 @@ typedef struct {
     double green_min_ratio;            /* slice_pair_green_min_ratio */
     double green_growth;               /* slice_pair_green_growth */
     int32_t longitudinal_kick;
-    int32_t slicing_method1, slicing_method2;  /* 0 = :normal_quantile, 1 = :specified */
+    int32_t slicing_method1, slicing_method2;  /* 0 = :normal_quantile, 1 = :specified, 2 = :equal_area,
+                                                  3 = :equal_count, 4 = :equal_width */
     int32_t nslices1, nslices2;
     int32_t center_position1, center_position2; /* 0 = :centroid, 1 = :midpoint */
     const double *positions1, *positions2;      /* :specified internal positions (nslices-1) */
@@ -59,6 +60,7 @@ typedef struct {
     int32_t gaussian;                  /* 1: GaussianPICPoissonSolver (Gaussian-subtracted hybrid) */
     int32_t neutralize;                /* hybrid: rescale the subtracted Gaussian to the deposited charge */
     double margin_sigma;               /* hybrid: adaptive-box half-width in beam sigmas */
+    int32_t resolution1, resolution2;  /* :equal_area histogram bins per slice (LongitudinalSlicing resolution) */
 } oo_options;
 
 typedef struct { double charge, mc2, E0, r0, npart; } oo_beam_params;
@@ -110,10 +112,14 @@ void oo_interpolate(const oo_options *opt, const double grid[4], double x, doubl
 double oo_luminosity(const oo_options *opt, const double *x1, const double *y1, int64_t n1, const double *x2,
                      const double *y2, int64_t n2, double klum, double *q1, double *q2);
 
-/* Slicing (slicing.jl:51-75, :normal_quantile / :specified). Outputs: boundary[ns+1], center[ns],
-   weight[ns], count[ns], order[n] (slice-major member lists, ascending particle index). */
+/* Slicing (slicing.jl:51-75; methods as slicing_method1). Outputs: boundary[ns+1], center[ns], weight[ns],
+   count[ns], order[n] (slice-major member lists: ascending particle index, rank order for :equal_count).
+   resolution: :equal_area histogram bins per slice (<= 0: the default 100). */
 int oo_slices(int32_t method, int32_t ns, int32_t center_position, const double *positions, const double *z,
-              int64_t n, double *boundary, double *center, double *weight, int64_t *count, int64_t *order);
+              int64_t n, double *boundary, double *center, double *weight, int64_t *count, int64_t *order,
+              int32_t resolution);
+/* Julia's collect(range(start, stop; length = len)) for Float64 endpoints (the :equal_width boundaries). */
+void oo_julia_range(double start, double stop, int64_t len, double *out);
 /* Collision order + wavefront batches (slicing.jl:561-647). pairs[k] = (batch, i, j) 0-based in order
    of batches; returns the number of batches. */
 int32_t oo_pair_batches(const double *c1, int32_t ns1, const double *c2, int32_t ns2, int32_t *batch_of,

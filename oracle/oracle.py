@@ -63,6 +63,7 @@ class OOOptions(C.Structure):
         ("nthreads", C.c_int32),
         ("gaussian", C.c_int32), ("neutralize", C.c_int32),
         ("margin_sigma", C.c_double),
+        ("resolution1", C.c_int32), ("resolution2", C.c_int32),
     ]
 
 
@@ -111,7 +112,9 @@ def lib():
         L.oo_luminosity.restype = d
         L.oo_luminosity.argtypes = [P(OOOptions), P(d), P(d), i64, P(d), P(d), i64, d, P(d), P(d)]
         L.oo_slices.restype = C.c_int
-        L.oo_slices.argtypes = [i32, i32, i32, P(d), P(d), i64, P(d), P(d), P(d), P(i64), P(i64)]
+        L.oo_slices.argtypes = [i32, i32, i32, P(d), P(d), i64, P(d), P(d), P(d), P(i64), P(i64), i32]
+        L.oo_julia_range.restype = None
+        L.oo_julia_range.argtypes = [d, d, i64, P(d)]
         L.oo_pair_batches.restype = i32
         L.oo_pair_batches.argtypes = [P(d), i32, P(d), i32, P(i32), P(i32), P(i32), P(i32), P(i32)]
         L.oo_create.restype = vp
@@ -159,7 +162,8 @@ _SYM = {
     "slice_interpolation": {"linear": 0, "quadratic": 1},
     "interaction_grid": {"slice_pair": 0, "node": 2},
     "grid_extent": {"extrema": 0, "sigma": 1},
-    "method": {"normal_quantile": 0, "gaussian": 0, "Gaussian": 0, "specified": 1},
+    "method": {"normal_quantile": 0, "gaussian": 0, "Gaussian": 0, "specified": 1, "equal_area": 2,
+               "equal_count": 3, "equal_width": 4, "equal_spaced": 4},
     "center_position": {"centroid": 0, "midpoint": 1},
 }
 
@@ -199,6 +203,8 @@ class OracleOptions:
     gaussian: bool = False          # GaussianPICPoissonSolver (the Gaussian-subtracted hybrid)
     neutralize: bool = True
     margin_sigma: float = 5.0
+    resolution1: int = 100
+    resolution2: int = 100
 
     def to_c(self) -> OOOptions:
         o = OOOptions()
@@ -240,6 +246,7 @@ class OracleOptions:
         o.gaussian = int(bool(self.gaussian))
         o.neutralize = int(bool(self.neutralize))
         o.margin_sigma = float(self.margin_sigma)
+        o.resolution1, o.resolution2 = int(self.resolution1), int(self.resolution2)
         return o
 
 
@@ -350,7 +357,13 @@ class OracleErrorPy(Exception):
         self.code = code
 
 
-def slices(z, ns, method="normal_quantile", center_position="centroid", positions=()):
+def julia_range(start, stop, length):
+    out = np.empty(int(length))
+    lib().oo_julia_range(float(start), float(stop), int(length), _dp(out))
+    return out
+
+
+def slices(z, ns, method="normal_quantile", center_position="centroid", positions=(), resolution=100):
     z = np.ascontiguousarray(z, dtype=np.float64)
     n = z.size
     b = np.empty(ns + 1); c = np.empty(ns); w = np.empty(ns)
@@ -358,7 +371,8 @@ def slices(z, ns, method="normal_quantile", center_position="centroid", position
     pos = np.ascontiguousarray(positions, np.float64)
     rc = lib().oo_slices(_SYM["method"][method], ns, _SYM["center_position"][center_position],
                          _dp(pos) if pos.size else None, _dp(z), n, _dp(b), _dp(c), _dp(w),
-                         cnt.ctypes.data_as(C.POINTER(C.c_int64)), order.ctypes.data_as(C.POINTER(C.c_int64)))
+                         cnt.ctypes.data_as(C.POINTER(C.c_int64)), order.ctypes.data_as(C.POINTER(C.c_int64)),
+                         int(resolution))
     if rc != OK:
         raise OracleErrorPy(rc, "slicing")
     return b, c, w, cnt, order

@@ -41,8 +41,7 @@ def oracle_options(solver, nthreads=8, fixed=False):
         slice_pair_green_min_ratio=solver.slice_pair_green_min_ratio,
         slice_pair_green_growth=solver.slice_pair_green_growth, longitudinal_kick=solver.longitudinal_kick,
         nslices1=s1.nslices, nslices2=s2.nslices,
-        method1="specified" if s1.method == "specified" else "normal_quantile",
-        method2="specified" if s2.method == "specified" else "normal_quantile",
+        method1=s1.method, method2=s2.method, resolution1=s1.resolution, resolution2=s2.resolution,
         center_position1=s1.center_position, center_position2=s2.center_position,
         positions1=list(s1.positions), positions2=list(s2.positions),
         kbb1=solver.kbb1, kbb2=solver.kbb2, luminosity_scale=solver.luminosity_scale,

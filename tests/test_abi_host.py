@@ -102,8 +102,11 @@ def test_gpu_backend_rejects_what_it_does_not_implement():
                dict(grid=(80, 80)), dict(grid=(96, 36)), dict(grid=(1024, 64))):
         with pytest.raises(ob.ArgumentError):
             ob.PICPoissonSolver(slicing=sl, **kw).to_c()
-    with pytest.raises(ob.ArgumentError):
-        ob.PICPoissonSolver(slicing=ob.LongitudinalSlicing(nslices=3, method="equal_area")).to_c()
+    with pytest.raises(ob.ArgumentError):  # the :equal_area histogram's shared-memory bound
+        ob.PICPoissonSolver(slicing=ob.LongitudinalSlicing(nslices=64, method="equal_area", resolution=300)).to_c()
+    for m, code in (("equal_area", 2), ("equal_count", 3), ("equal_width", 4), ("equal_spaced", 4), ("gaussian", 0)):
+        o = ob.PICPoissonSolver(slicing=ob.LongitudinalSlicing(nslices=3, method=m, resolution=7)).to_c()
+        assert (o.slicing_method1, o.slicing_method2, o.resolution1) == (code, code, 7)
     for g in ((48, 48), (96, 64), (384, 192), (512, 512)):  # 2^a and 3*2^a FFT lines
         assert ob.PICPoissonSolver(slicing=sl, grid=g).to_c().nx == g[0]
     o = ob.PICPoissonSolver(slicing=sl, deposit_method="TSC", field_derivative="fourth").to_c()
