@@ -746,14 +746,19 @@ def scan_cases(n_cases=64, seed=SEED):
     return cases
 
 
-def run_scan(args, local_rank):
+def run_scan(args, rank, world, local_rank):
     """The batched scan: independent collisions in the precision form, in batches of --scan-batch collides
-    overlapped on their own streams (octo_pic_collide_batch), against the same collides one by one."""
+    overlapped on their own streams (octo_pic_collide_batch), against the same collides one by one.  Under
+    torchrun each rank runs its share of the cases (octo_b200.parallel.partition_collisions, a size-balanced
+    greedy partition; no data-path collective); the time is the max over ranks."""
     import torch
     import octo_b200 as ob
+    from octo_b200.parallel import collision_cost, max_over_ranks, partition_collisions
     dev = torch.device(f"cuda:{local_rank}")
     torch.cuda.set_device(dev)
     cases = scan_cases(args.scan_cases)
+    costs = [collision_cost(c["n1"], c["n2"], max(c["s1"], c["s2"]), c["grid"]) for c in cases]
+    mine = [cases[k] for k in partition_collisions(costs, world)[rank]]
     turns = args.scan_turns
     sy = 8.5e-6
 
@@ -771,38 +776,51 @@ def run_scan(args, local_rank):
     times = {}
     for mode in ("batched", "sequential"):
         total_ms = 0.0
-        for g0 in range(0, len(cases), args.scan_batch):
-            group = [make(c) for c in cases[g0:g0 + args.scan_batch]]
+        for g0 in range(0, len(mine), args.scan_batch):
+            group = [make(c) for c in mine[g0:g0 + args.scan_batch]]
             ctxs = [ob.Context(sol, local_rank, torch.float32) for sol, _, _ in group]
             streams = [torch.cuda.Stream(device=dev) for _ in group]
             for t in range(2):  # warm-up turns (workspaces, Green caches)
                 ob.collide_batch(ctxs, [g[1] for g in group], [g[2] for g in group], turn=t, streams=streams)
             torch.cuda.synchronize()
-            t0 = time.perf_counter()
+            main = torch.cuda.current_stream(dev)
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(main)
+            for st in streams:
+                st.wait_event(ev0)
             for t in range(turns):
                 if mode == "batched":
                     ob.collide_batch(ctxs, [g[1] for g in group], [g[2] for g in group], turn=2 + t, streams=streams)
                 else:
                     for k, (sol, e, p) in enumerate(group):
-                        ctxs[k].collide(e, p, turn=2 + t)
+                        ctxs[k].collide(e, p, turn=2 + t, stream=streams[k])
+            for st in streams:  # the end event follows every stream's work
+                done = torch.cuda.Event()
+                done.record(st)
+                main.wait_event(done)
+            ev1.record(main)
             torch.cuda.synchronize()
-            total_ms += (time.perf_counter() - t0) * 1e3
+            total_ms += ev0.elapsed_time(ev1)
             for c in ctxs:
                 c.close()
             del group
             torch.cuda.empty_cache()
-        times[mode] = total_ms
+        times[mode] = max_over_ranks(total_ms)
+    if rank != 0:
+        return 0
     collide_turns = len(cases) * turns
     line = {
         "metric": "batched scan: s per collision-turn", "value": times["batched"] / 1e3 / collide_turns,
-        "unit": "s/collision-turn", "n_gpus": 1, "higher_is_better": False, "impl": "ours",
+        "unit": "s/collision-turn", "n_gpus": world, "higher_is_better": False, "impl": "ours", "scaling": "strong",
         "sequential_value": times["sequential"] / 1e3 / collide_turns,
         "batching_speedup": times["sequential"] / times["batched"],
         "config": {"workload": "independent collisions, precision form (float32 beams), default PICPoissonSolver "
                                "options (:slice_pair grid, slice-pair Green cache, CIC); N log-uniform 64k-2.56M per "
                                "beam, slices 5..31, grids 64/96/128/256, aspect 1-25",
                    "cases": len(cases), "turns": turns, "batch": args.scan_batch,
-                   "timing": "host wall clock around each group's turns after 2 warm-up turns, synchronized"},
+                   "partition": "size-balanced greedy over ranks (octo_b200.parallel.partition_collisions)",
+                   "timing": "CUDA events spanning every collide stream of each group after 2 warm-up turns, "
+                             "summed over the rank's groups; max over ranks"},
         "particles": sum(c["n1"] + c["n2"] for c in cases),
     }
     print(json.dumps(line), flush=True)
@@ -833,7 +851,7 @@ def main():
         if args.impl == "reference":
             return run_reference(args, rank)
         if args.scan:
-            return run_scan(args, local_rank) if rank == 0 else 0
+            return run_scan(args, rank, world, local_rank)
         return run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:

@@ -45,7 +45,7 @@ struct Cnn {
     DevBuf<float> out;  // head output [M0][8]
     // backward scratch
     DevBuf<bf16> g, gt, colt;
-    DevBuf<float> fa, dc, ds1, ds2, ds3, part;
+    DevBuf<float> fa, dc, ds1, ds2, ds3, part, splitbuf;
     DevBuf<double> loss_part;
     PinBuf<double> h_loss;
     long long part_floats = 0;
@@ -121,7 +121,7 @@ struct Cnn {
         for (auto &b : wf) b.release();
         for (DevBuf<bf16> *b : {&x0, &a0, &s1, &p1, &a2, &s2, &p2, &a4, &s3, &p3, &b6, &u3, &d7, &u2, &d8, &u1, &d9, &g, &gt, &colt})
             b->release();
-        for (DevBuf<float> *b : {&out, &fa, &dc, &ds1, &ds2, &ds3, &part}) b->release();
+        for (DevBuf<float> *b : {&out, &fa, &dc, &ds1, &ds2, &ds3, &part, &splitbuf}) b->release();
         loss_part.release();
         h_loss.release();
         if (err) cudaFree(err);
@@ -148,6 +148,9 @@ struct Cnn {
         weights_dirty = false;
     }
 
+    // A 3x3 convolution layer as one tensor-core GEMM.  Layers with too few output tiles to fill the GPU (the
+    // coarse levels) split K over more CTAs; their fp32 partials are summed in a fixed order by the
+    // bias / ReLU / bf16 epilogue kernel.
     void gemm_conv(int l, const bf16 *in, int B, bf16 *out_bf, float *out_f, cudaStream_t st) {
         const LayerSpec &L = kLayers[l];
         GemmArgs a{};
@@ -159,7 +162,23 @@ struct Cnn {
         a.out_bf16 = out_bf; a.ldo = L.cout;
         a.out = out_f; a.ldc = L.cout; a.split_stride = 0; a.k_per_split = ((a.K + kBK - 1) / kBK) * kBK;
         a.error = err;
-        launch_gemm(a, 1, st);
+        const int bn = L.cout <= 32 ? 32 : (L.cout <= 64 ? 64 : (L.cout <= 128 ? 128 : 256));
+        const long long tiles = ((long long)(a.M + kBM - 1) / kBM) * ((L.cout + bn - 1) / bn);
+        const int chunks = (a.K + kBK - 1) / kBK;
+        const int splits = (out_bf && tiles < 148 && chunks >= 4)
+                               ? (int)std::min<long long>(chunks / 2, (296 + tiles - 1) / tiles) : 1;
+        if (splits <= 1) {
+            launch_gemm(a, 1, st);
+            return;
+        }
+        a.k_per_split = ((chunks + splits - 1) / splits) * kBK;
+        const int used = (chunks * kBK + a.k_per_split - 1) / a.k_per_split;
+        splitbuf.ensure((size_t)used * a.M * L.cout);
+        a.out = splitbuf.p; a.ldc = L.cout; a.split_stride = (long long)a.M * L.cout;
+        a.out_bf16 = nullptr; a.bias = nullptr; a.relu = 0;
+        launch_gemm(a, used, st);
+        launch_pdl(k_umma_split_epilogue, ew_blocks((long long)a.M * L.cout), 256, 0, st, (const float *)splitbuf.p, used,
+                   (long long)a.M, L.cout, (const float *)(master.p + boff[l]), L.relu, out_bf, (long long)L.cout);
     }
 
     void pool(const bf16 *in, bf16 *o, int B, int level, int C, cudaStream_t st) {

@@ -8,11 +8,13 @@
 // row-major bf16 matrix (for a convolution: weights [Cout][ky][kx][Cin]).
 //
 // One CTA of 128 threads computes a 128 x BN tile: the K loop moves 64-wide chunks of A and B from global
-// memory into shared memory (two stages) in the canonical no-swizzle K-major layout -- 8-row x 16-byte core
+// memory into shared memory with 16-byte cp.async copies (four stages, three chunks in flight; zero-filled
+// outside the matrix and the padded image) in the canonical no-swizzle K-major layout -- 8-row x 16-byte core
 // matrices, 128 contiguous bytes each, the two K halves of one instruction LBO = 128 bytes apart and 8-row
 // groups SBO = 1024 bytes apart -- and one thread issues four tcgen05.mma (M = 128, N = BN, K = 16) per
 // chunk into a TMEM accumulator, committing each chunk to the stage's mbarrier so the stage can be refilled
-// while the next chunk's MMAs run.  The epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM
+// once its MMAs are done.  A thread always loads the same eight A rows, so the implicit im2col's pixel
+// coordinates are computed once per CTA.  The epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM
 // lanes 32w..32w+31 = tile rows) and writes fp32 (split-K partials) or bias + ReLU as bf16.
 //
 // Every mbarrier wait is bounded (about one second of the global timer); on expiry the kernel records
@@ -87,18 +89,22 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
 // Byte offset of the 16-byte chunk (row r, k-chunk kc) of a stage tile in the canonical layout.
 __device__ __forceinline__ uint32_t tile_off(int r, int kc) { return (uint32_t)((r >> 3) * 1024 + kc * 128 + (r & 7) * 16); }
 
-// One 16-byte chunk (8 consecutive k) of row m of A, or zeros outside the matrix / the padded image.
-__device__ __forceinline__ uint4 load_a_chunk(const GemmArgs &g, int m, int k) {
-    uint4 v = make_uint4(0, 0, 0, 0);
-    if (m >= g.M || k >= g.K) return v;
-    if (g.a_mode == 0) return *reinterpret_cast<const uint4 *>(g.A + (long long)m * g.lda + k);
-    const int tap = k / g.C, c = k - tap * g.C;
-    const int hw = g.H * g.W;
-    const int b = m / hw, rem = m - b * hw, y = rem / g.W, x = rem - y * g.W;
-    const int yy = y + tap / 3 - 1, xx = x + tap % 3 - 1;
-    if (yy < 0 || yy >= g.H || xx < 0 || xx >= g.W) return v;
-    return *reinterpret_cast<const uint4 *>(g.A + (((long long)b * g.H + yy) * g.W + xx) * g.C + c);
+// 16-byte asynchronous global -> shared copy; src_bytes = 0 writes zeros (padding, tails) without reading.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+constexpr int kStages = 4;
+constexpr int kRowsPerThread = (kBM * 8) / kGemmThreads;  // A rows (one 16-byte k-chunk each) a thread loads
+
+// The thread -> chunk mapping of a stage: chunk c = it * 128 + tid covers row (c & 7) + 8 * (c >> 6) and
+// k-chunk (c >> 3) & 7, so a thread loads the same rows and the same k-chunk column in every stage; a group
+// of 8 consecutive threads writes 8 rows of one k-chunk (128 contiguous bytes of shared memory).
+__device__ __forceinline__ int map_row(int it, int tid) { return (tid & 7) + 8 * (2 * it + (tid >> 6)); }
+__device__ __forceinline__ int map_kc(int tid) { return (tid >> 3) & 7; }
 
 template <int BN>
 __global__ void __launch_bounds__(kGemmThreads, 1) k_umma_gemm(const GemmArgs g) {
@@ -106,7 +112,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_umma_gemm(const GemmArgs g)
     constexpr uint32_t kStageA = kBM * kBK * 2, kStageB = BN * kBK * 2;
     constexpr uint32_t kCols = BN < 32 ? 32 : BN;
     extern __shared__ __align__(1024) unsigned char g_umma_smem[];
-    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ __align__(8) uint64_t bar[kStages];
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
     pdl_wait();
@@ -116,9 +122,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_umma_gemm(const GemmArgs g)
     const int kb = blockIdx.z * g.k_per_split;
     const int ke = min(g.K, kb + g.k_per_split);
     const int nk = ke > kb ? (ke - kb + kBK - 1) / kBK : 0;
-    unsigned char *const smA = g_umma_smem, *const smB = g_umma_smem + 2 * kStageA;  // stage s at + s * size
+    unsigned char *const smA = g_umma_smem, *const smB = g_umma_smem + kStages * kStageA;
+    const uint32_t sA0 = smem_u32(smA), sB0 = smem_u32(smB);
     if (tid == 0) {
-        for (int s = 0; s < 2; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[s])));
+        for (int s = 0; s < kStages; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[s])));
         // the barriers are signalled by tcgen05.commit: make their initialisation visible to that proxy
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -129,47 +136,89 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_umma_gemm(const GemmArgs g)
                      "r"(kCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
+    // this thread's A rows: (y, x) of the pixel and its element offset (a_mode 1), or the row offset (a_mode 0);
+    // rows past M are marked y = -1 (zero fill)
+    const int kc_t = map_kc(tid);
+    long long rbase[kRowsPerThread];
+    int ry[kRowsPerThread], rx[kRowsPerThread];
+#pragma unroll
+    for (int it = 0; it < kRowsPerThread; ++it) {
+        const int m = m0 + map_row(it, tid);
+        ry[it] = -1; rx[it] = 0; rbase[it] = 0;
+        if (m < g.M) {
+            if (g.a_mode == 0) {
+                ry[it] = 0;
+                rbase[it] = (long long)m * g.lda;
+            } else {
+                const int hw = g.H * g.W;
+                const int b = m / hw, rem = m - b * hw, y = rem / g.W, x = rem - y * g.W;
+                ry[it] = y; rx[it] = x;
+                rbase[it] = (((long long)b * g.H + y) * g.W + x) * g.C;
+            }
+        }
+    }
+    // loads of K chunk i into stage s (every thread: its A rows, then its share of B)
+    auto load_stage = [&](int i, int s) {
+        const int k = kb + i * kBK + kc_t * 8;
+        int dy = 0, dx = 0, c = k;
+        if (g.a_mode == 1) {
+            const int tap = k / g.C;
+            c = k - tap * g.C;
+            dy = tap / 3 - 1;
+            dx = tap - 3 * (tap / 3) - 1;
+        }
+        const bool kin = k < g.K;
+#pragma unroll
+        for (int it = 0; it < kRowsPerThread; ++it) {
+            const int r = map_row(it, tid);
+            const __nv_bfloat16 *src = g.A;
+            int bytes = 0;
+            if (kin && ry[it] >= 0) {
+                if (g.a_mode == 0) {
+                    src = g.A + rbase[it] + k;
+                    bytes = 16;
+                } else {
+                    const int yy = ry[it] + dy, xx = rx[it] + dx;
+                    if (yy >= 0 && yy < g.H && xx >= 0 && xx < g.W) {
+                        src = g.A + rbase[it] + ((long long)dy * g.W + dx) * g.C + c;
+                        bytes = 16;
+                    }
+                }
+            }
+            cp_async16(sA0 + s * kStageA + tile_off(r, kc_t), src, bytes);
+        }
+#pragma unroll
+        for (int it = 0; it < (BN * 8 + kGemmThreads - 1) / kGemmThreads; ++it) {
+            const int cc = it * kGemmThreads + tid;
+            if (cc >= BN * 8) break;
+            const int r = (cc & 7) + ((cc >> 6) << 3), kc = (cc >> 3) & 7;
+            const int n = n0 + r, kk = kb + i * kBK + kc * 8;
+            const bool ok = n < g.N && kk < ke;
+            cp_async16(sB0 + s * kStageB + tile_off(r, kc), ok ? (const void *)(g.B + (long long)n * g.ldb + kk) : g.B,
+                       ok ? 16 : 0);
+        }
+    };
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_slot;
     const uint32_t idesc = umma_idesc_bf16(BN);
-    uint32_t commits[2] = {0, 0};  // commits issued per stage (thread 0)
+    uint32_t commits[kStages] = {0, 0, 0, 0};  // commits issued per stage (thread 0)
 
+    // prologue: chunks 0 .. kStages-2 in flight
+#pragma unroll
+    for (int s = 0; s < kStages - 1; ++s) {
+        if (s < nk) load_stage(s, s);
+        cp_async_commit();
+    }
     for (int i = 0; i < nk; ++i) {
-        const int s = i & 1;
-        if (i >= 2) {  // the MMAs that read this stage (chunk i - 2) must be done before it is refilled
-            if (tid == 0 && !mbar_wait(smem_u32(&bar[s]), (commits[s] - 1) & 1)) abort_flag = 1;
-            __syncthreads();
-            if (abort_flag) break;
-        }
-        const int k0 = kb + i * kBK;
-        // A: 128 rows x 8 chunks; a group of 8 consecutive threads writes 8 rows of one k-chunk (128
-        // contiguous bytes of shared memory, conflict-free)
-#pragma unroll
-        for (int it = 0; it < (kBM * 8) / kGemmThreads; ++it) {
-            const int c = it * kGemmThreads + tid;
-            const int r = (c & 7) + ((c >> 6) << 3), kc = (c >> 3) & 7;
-            const uint4 v = load_a_chunk(g, m0 + r, k0 + kc * 8);
-            *reinterpret_cast<uint4 *>(smA + s * kStageA + tile_off(r, kc)) = v;
-        }
-#pragma unroll
-        for (int it = 0; it < (BN * 8 + kGemmThreads - 1) / kGemmThreads; ++it) {
-            const int c = it * kGemmThreads + tid;
-            if (c >= BN * 8) break;
-            const int r = (c & 7) + ((c >> 6) << 3), kc = (c >> 3) & 7;
-            const int n = n0 + r, k = k0 + kc * 8;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (n < g.N && k < ke) v = *reinterpret_cast<const uint4 *>(g.B + (long long)n * g.ldb + k);
-            *reinterpret_cast<uint4 *>(smB + s * kStageB + tile_off(r, kc)) = v;
-        }
-        // A chunks past this split's K range read zeros too: load_a_chunk tests k < K; within the range
-        // the split boundary is a multiple of kBK, so only the last split has a tail
+        const int s = i % kStages;
+        cp_async_wait<kStages - 2>();  // this thread's copies of chunk i have landed
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
+        __syncthreads();  // ... and every thread's
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t a0 = smem_u32(smA + s * kStageA), b0 = smem_u32(smB + s * kStageB);
+            const uint32_t a0 = sA0 + s * kStageA, b0 = sB0 + s * kStageB;
 #pragma unroll
             for (int ks = 0; ks < kBK / 16; ++ks) {
                 const uint64_t da = umma_desc(a0 + ks * 256, 128, 1024);
@@ -186,12 +235,22 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_umma_gemm(const GemmArgs g)
                              smem_u32(&bar[s]))
                          : "memory");
             ++commits[s];
+            // the stage the next load refills held chunk i - 1: its MMAs must be done
+            const int sp = (i + kStages - 1) % kStages;
+            if (i >= 1 && i + kStages - 1 < nk && !mbar_wait(smem_u32(&bar[sp]), (commits[sp] - 1) & 1)) abort_flag = 1;
         }
+        if (i + kStages - 1 < nk) {
+            __syncthreads();
+            if (abort_flag) break;
+            load_stage(i + kStages - 1, (i + kStages - 1) % kStages);
+        }
+        cp_async_commit();
     }
+    cp_async_wait<0>();
     // wait for every stage's last commit (the last one covers all earlier MMAs of the issuing thread)
     if (tid == 0) {
         bool ok = true;
-        for (int s = 0; s < 2; ++s)
+        for (int s = 0; s < kStages; ++s)
             if (commits[s] && !mbar_wait(smem_u32(&bar[s]), (commits[s] - 1) & 1)) ok = false;
         if (!ok) abort_flag = 1;
     }
@@ -250,7 +309,25 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_umma_gemm(const GemmArgs g)
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
 }
 
-inline size_t umma_smem_bytes(int bn) { return 2 * (size_t)(kBM * kBK * 2) + 2 * (size_t)(bn * kBK * 2); }
+// Split-K partials of a convolution summed in a fixed order, plus bias and ReLU, rounded to bf16:
+// out[m * ldo + n] = bf16(relu?(sum_z part[z][m][n] + bias[n])).
+__global__ void k_umma_split_epilogue(const float *__restrict__ part, int splits, long long M, int N,
+                                      const float *__restrict__ bias, int relu, __nv_bfloat16 *__restrict__ out,
+                                      long long ldo) {
+    pdl_wait();
+    pdl_release();
+    const long long n_all = M * N;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_all; i += (long long)gridDim.x * blockDim.x) {
+        float v = 0.f;
+        for (int z = 0; z < splits; ++z) v += part[(long long)z * n_all + i];
+        const int n = (int)(i % N);
+        v += bias ? bias[n] : 0.f;
+        if (relu) v = fmaxf(v, 0.f);
+        out[(i / N) * ldo + n] = __float2bfloat16_rn(v);
+    }
+}
+
+inline size_t umma_smem_bytes(int bn) { return kStages * ((size_t)(kBM * kBK * 2) + (size_t)(bn * kBK * 2)); }
 
 }  // namespace nn
 }  // namespace octo

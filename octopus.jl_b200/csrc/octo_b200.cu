@@ -244,7 +244,7 @@ struct octo_ctx {
     // the kick sizes its blocks to fill kick_slots times the resident block slots
     int dep_waves = 1, kick_slots = 1;
     // plain PIC: group each slice's particles by transverse position in the working copy (octo_set_particle_order)
-    int spatial = 1;
+    int spatial = 0;
     octo_pic_options opt{};
     std::vector<double> pos[2];
     DevOptions dopt{};

@@ -42,3 +42,24 @@ def max_over_ranks(value: float, group=None) -> float:
     t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
     return float(t.item())
+
+
+def scan_partitioned(costs: Sequence[float], run_case, group=None):
+    """Run a scan of independent collisions across the ranks of `group` (the default process group, or one
+    rank when torch.distributed is not initialised): each rank runs its partition_collisions share with
+    run_case(index) -> result, and every rank gets back the merged {index: result} of all ranks.  No
+    data-path collective: the only exchange is this final gather of the (small, picklable) results."""
+    import torch.distributed as dist
+    distributed = dist.is_available() and dist.is_initialized()
+    rank = dist.get_rank(group) if distributed else 0
+    world = dist.get_world_size(group) if distributed else 1
+    mine = partition_collisions(costs, world)[rank]
+    local = {k: run_case(k) for k in mine}
+    if not distributed:
+        return local
+    parts = [None] * world
+    dist.all_gather_object(parts, local, group=group)
+    merged = {}
+    for p in parts:
+        merged.update(p)
+    return merged
