@@ -151,11 +151,15 @@ struct Cnn {
     // A 3x3 convolution layer as one tensor-core GEMM.  Layers with too few output tiles to fill the GPU (the
     // coarse levels) split K over more CTAs; their fp32 partials are summed in a fixed order by the
     // bias / ReLU / bf16 epilogue kernel.
-    void gemm_conv(int l, const bf16 *in, int B, bf16 *out_bf, float *out_f, cudaStream_t st) {
+    // skip != null: the layer's input is [nearest-upsampled in (cu channels), skip] (a decoder level), read
+    // by the GEMM directly instead of a materialised concatenation.
+    void gemm_conv(int l, const bf16 *in, int B, bf16 *out_bf, float *out_f, cudaStream_t st, const bf16 *skip = nullptr,
+                   int cu = 0) {
         const LayerSpec &L = kLayers[l];
         GemmArgs a{};
         a.M = (int)ml(L.level, B); a.N = L.cout; a.K = 9 * L.cin;
-        a.A = in; a.a_mode = 1; a.H = hl(L.level); a.W = wl(L.level); a.C = L.cin;
+        a.A = in; a.a_mode = skip ? 2 : 1; a.H = hl(L.level); a.W = wl(L.level); a.C = L.cin;
+        a.A2 = skip; a.Cu = cu;
         a.B = w[l].p; a.ldb = 9 * L.cin;
         a.bias = master.p + boff[l];
         a.relu = L.relu;
@@ -190,9 +194,28 @@ struct Cnn {
         launch_pdl(k_cnn_upcat, ew_blocks(n), 256, 0, st, coarse, skip, o, B, hl(level), wl(level), Cu, Cs);
     }
 
-    // Forward pass of B inputs already in x0; the head's fp32 output lands in `out` ([M0][8]).
-    void forward(int B, cudaStream_t st) {
+    // Forward pass of B inputs already in x0; the head's fp32 output lands in `out` ([M0][8]).  Inference
+    // (materialize = false) reads each decoder level's [upsampled, skip] input inside the GEMM; training keeps
+    // the concatenations, whose transposed im2col the weight gradients read.
+    void forward(int B, cudaStream_t st, bool materialize = true) {
         if (weights_dirty) refresh_weights(st);
+        if (!materialize) {
+            gemm_conv(L_E1A, x0.p, B, a0.p, nullptr, st);
+            gemm_conv(L_E1B, a0.p, B, s1.p, nullptr, st);
+            pool(s1.p, p1.p, B, 0, 32, st);
+            gemm_conv(L_E2A, p1.p, B, a2.p, nullptr, st);
+            gemm_conv(L_E2B, a2.p, B, s2.p, nullptr, st);
+            pool(s2.p, p2.p, B, 1, 64, st);
+            gemm_conv(L_E3A, p2.p, B, a4.p, nullptr, st);
+            gemm_conv(L_E3B, a4.p, B, s3.p, nullptr, st);
+            pool(s3.p, p3.p, B, 2, 128, st);
+            gemm_conv(L_B, p3.p, B, b6.p, nullptr, st);
+            gemm_conv(L_D3, b6.p, B, d7.p, nullptr, st, s3.p, 128);
+            gemm_conv(L_D2, d7.p, B, d8.p, nullptr, st, s2.p, 64);
+            gemm_conv(L_D1, d8.p, B, d9.p, nullptr, st, s1.p, 32);
+            gemm_conv(L_HEAD, d9.p, B, nullptr, out.p, st);
+            return;
+        }
         gemm_conv(L_E1A, x0.p, B, a0.p, nullptr, st);
         gemm_conv(L_E1B, a0.p, B, s1.p, nullptr, st);
         pool(s1.p, p1.p, B, 0, 32, st);

@@ -11,6 +11,7 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -216,10 +217,23 @@ namespace nn {
 // Picks the tile width from N (32, 64, 128 or 256 columns of fp32 accumulator in TMEM).
 void launch_gemm(const GemmArgs &g, int splits, cudaStream_t st) {
     const int bn = g.N <= 32 ? 32 : (g.N <= 64 ? 64 : (g.N <= 128 ? 128 : 256));
-    const dim3 grid((unsigned)((g.M + kBM - 1) / kBM), (unsigned)((g.N + bn - 1) / bn), (unsigned)splits);
+    const int tiles_m = (g.M + kBM - 1) / kBM, cols = ((g.N + bn - 1) / bn) * splits;
     const size_t smem = umma_smem_bytes(bn);
+    static std::atomic<int> resident[4] = {{0}, {0}, {0}, {0}};  // CTAs per SM of each tile width (one arch)
+    const int slot = bn == 32 ? 0 : (bn == 64 ? 1 : (bn == 128 ? 2 : 3));
     auto go = [&](void (*kernel)(const GemmArgs)) {
         CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // persistent CTAs: as many as are resident at once, spread over the (n, split) columns
+        int dev = 0, sms = 0, per_sm = resident[slot].load();
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        if (per_sm == 0) {
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kGemmThreads, smem));
+            resident[slot].store(per_sm);
+        }
+        const int slots = std::max(1, sms * std::max(1, per_sm));
+        const int gx = std::max(1, std::min(tiles_m, (slots + cols - 1) / cols));
+        const dim3 grid((unsigned)gx, (unsigned)((g.N + bn - 1) / bn), (unsigned)splits);
         launch_pdl(kernel, grid, kGemmThreads, smem, st, g);
     };
     if (bn == 32) go(k_umma_gemm<32>);
@@ -1350,7 +1364,7 @@ void CollideJob::run() {
                                              "plane count (" + std::to_string(F.np) + ")"};
             c->cnn_q.ensure((size_t)c->cnn->net.maxB);
             launch_pdl(k_cnn_prep, F.np, 256, 0, st, C, F.p0, c->cnn->net.x0.p, c->cnn_q.p);
-            c->cnn->net.forward(F.np, st);
+            c->cnn->net.forward(F.np, st, false);
             launches += 1 + 17;
         }
         if (c->cap_armed && !c->cap_taken) {
@@ -1961,10 +1975,14 @@ octo_ctx *octo_create(int32_t device, const octo_pic_options *options) {
         for (int b = 0; b < 2; ++b) {
             int ns = c->ns[b];
             int m = b == 0 ? options->slicing_method1 : options->slicing_method2;
+            // the quantile table of :normal_quantile, the positions of :specified (the other methods use neither)
             std::vector<double> q(kMaxSlices + 1, 0.0);
-            for (int s = 1; s <= ns - 1; ++s)
-                q[s] = m == OCTO_SLICING_NORMAL_QUANTILE ? std::sqrt(2.0) * erfinv_host((double)(2 * s) / (double)ns - 1.0)
-                                                         : c->pos[b][s - 1];
+            for (int s = 1; s <= ns - 1; ++s) {
+                if (m == OCTO_SLICING_NORMAL_QUANTILE)
+                    q[s] = std::sqrt(2.0) * erfinv_host((double)(2 * s) / (double)ns - 1.0);
+                else if (m == OCTO_SLICING_SPECIFIED && (size_t)(s - 1) < c->pos[b].size())
+                    q[s] = c->pos[b][s - 1];
+            }
             c->bw[b].q.ensure(kMaxSlices + 1);
             CK(cudaMemcpy(c->bw[b].q.p, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice));
         }
@@ -2665,7 +2683,7 @@ int32_t octo_cnn_forward(octo_cnn *c, const void *input, int32_t batch, float *o
         cudaStream_t st = (cudaStream_t)stream;
         const long long M0 = N.ml(0, batch);
         CK(cudaMemcpyAsync(N.x0.p, input, sizeof(nn::bf16) * M0 * nn::kCnnIn, cudaMemcpyDeviceToDevice, st));
-        N.forward(batch, st);
+        N.forward(batch, st, false);
         // channels 0 and 1 of the head
         CK(cudaMemcpy2DAsync(output, 2 * sizeof(float), N.out.p, 8 * sizeof(float), 2 * sizeof(float), (size_t)M0,
                              cudaMemcpyDeviceToDevice, st));

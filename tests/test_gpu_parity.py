@@ -84,6 +84,8 @@ def test_route_fixture():
 
 
 @pytest.mark.parametrize("opts", [
+    dict(grid_quantize=0.25),
+    dict(grid_quantize=0.5, green_cache="none"),
     dict(field_derivative="fourth"),
     dict(slice_interpolation="quadratic"),
     dict(green_cache="none"),
@@ -95,6 +97,15 @@ def test_option_variants(opts):
     ob = _gpu()
     s = ob.PICPoissonSolver(grid=(64, 64), slicing=ob.LongitudinalSlicing(nslices=4, method="normal_quantile"), **opts)
     check(run_both(s, 6000, 4000, turns=2))
+
+
+def test_node_mode_grid_quantize():
+    """grid_quantize snaps each mesh's extent to a geometric ladder and its origins to whole cells
+    (pic_cpu.jl:1641-1644, 1686-1701), on the :node meshes too."""
+    ob = _gpu()
+    s = ob.PICPoissonSolver(grid=(64, 64), interaction_grid="node", grid_quantize=0.25,
+                            slicing=ob.LongitudinalSlicing(nslices=5, method="normal_quantile"))
+    check(run_both(s, 20000, 10000, turns=2, e_sigma=(95e-6, 8.5e-6, 0.7e-2), p_sigma=(95e-6, 8.5e-6, 6e-2)))
 
 
 def test_node_mode():
