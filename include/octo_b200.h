@@ -90,7 +90,8 @@ typedef struct {
     double kbb1, kbb2, lum_scale;
     int32_t precision;                 /* 0 = FP64 plain form, 1 = FP32 precision form (float32 beams) */
     /* GaussianPICPoissonSolver (gaussian_pic.jl:87-112): 1 = subtract the drifted reference Gaussian of
-     * each source slice before the solve and add its Bassetti-Erskine kick back analytically */
+     * each source slice before the solve and add its Bassetti-Erskine kick back analytically; in both forms
+     * (the precision form keeps the moments, the reference Gaussians and the add-back in FP64) */
     int32_t gaussian;
     double margin_sigma;               /* hybrid: Gaussian containment half-width in sigmas (default 5) */
     int32_t neutralize;                /* hybrid: rescale the subtracted Gaussian to the deposited charge */

@@ -187,6 +187,8 @@ __global__ void __launch_bounds__(256) k_first_lum_bounds(Collide C, const First
 // Hybrid: transverse moment sums of each task's source slice relative to its first particle
 // (gaussian_pic.jl:432-486), as per-block partials folded in block order by k_plan.  grid: (blocks per
 // side, 2 * pairs in front), the mapping of k_pair_bounds.
+// The sums are FP64 in both forms (the precision form's FP32 coordinates are widened exactly).
+template <class R>
 __global__ void __launch_bounds__(256) k_hyb_moments(Collide C, int task0) {
     pdl_wait();
     pdl_release();
@@ -195,15 +197,14 @@ __global__ void __launch_bounds__(256) k_hyb_moments(Collide C, int task0) {
     const Task &T = C.tasks[t];
     const SoA S = C.beam[T.src_beam];
     const long long st = T.src_start, n = T.src_n;
-    const double *X = col<double>(S, 0) + st, *PX = col<double>(S, 1) + st, *Y = col<double>(S, 2) + st,
-                 *PY = col<double>(S, 3) + st;
+    const R *X = col<R>(S, 0) + st, *PX = col<R>(S, 1) + st, *Y = col<R>(S, 2) + st, *PY = col<R>(S, 3) + st;
     double a[kMomentSums];
 #pragma unroll
     for (int k = 0; k < kMomentSums; ++k) a[k] = 0.0;
     if (n > 0) {
         const double x0 = X[0], px0 = PX[0], y0 = Y[0], py0 = PY[0];
         for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-            const double dx = X[k] - x0, dpx = PX[k] - px0, dy = Y[k] - y0, dpy = PY[k] - py0;
+            const double dx = (double)X[k] - x0, dpx = (double)PX[k] - px0, dy = (double)Y[k] - y0, dpy = (double)PY[k] - py0;
             a[0] += dx; a[1] += dpx; a[2] += dy; a[3] += dpy;
             a[4] += dx * dx; a[5] += dpx * dpx; a[6] += dy * dy; a[7] += dpy * dpy;
             a[8] += dx * dpx; a[9] += dy * dpy;
@@ -259,6 +260,9 @@ __device__ inline void record_error(DevStatus *st, int task, int code, int role)
 // Grid geometry and Green-cache decision per task (pic_cpu.jl:954-1064, 1729-1821).  Hybrid: the source
 // moments (folded by k_hyb_fold), the reference Gaussians at both boundaries, the plain-PIC fallback test
 // and the margin box around the Gaussians joined to the source extent (gaussian_pic.jl:604-660).
+// R: the element type of the beams (the hybrid reads the source slice's first particle, the origin of its
+// moment sums).
+template <class R>
 __global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0) {
     pdl_wait();
     pdl_release();
@@ -288,8 +292,8 @@ __global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0) {
         for (int k = 0; k < kMomentSums; ++k) sum[k] = C.hmom[(long long)t * kMaxBoundBlocks * kMomentSums + k];
         const SoA S = C.beam[T.src_beam];
         const long long st = T.src_start, n = T.src_n;
-        const double x0 = col<double>(S, 0)[st], px0 = col<double>(S, 1)[st], y0 = col<double>(S, 2)[st],
-                     py0 = col<double>(S, 3)[st];
+        const double x0 = (double)col<R>(S, 0)[st], px0 = (double)col<R>(S, 1)[st], y0 = (double)col<R>(S, 2)[st],
+                     py0 = (double)col<R>(S, 3)[st];
         const double invn = 1.0 / (double)n;
         const double dmx = sum[0] * invn, dmpx = sum[1] * invn, dmy = sum[2] * invn, dmpy = sum[3] * invn;
         double m[10];
@@ -940,6 +944,42 @@ __device__ __forceinline__ double gauss_node_weight(int method, double xi, doubl
            1.5 * (m1(lL, lR) - m1(rL, rR)) / h + 0.5 * (m2(lL, lR) + m2(rL, rR)) / (h * h);
 }
 
+// Hybrid: the subtracted reference Gaussian of rows j0, j1 of a plane, amp * gx[i] * gy[j]
+// (gaussian_pic.jl:580-589); amp neutralises it to the plane's deposited charge, else it carries the slice's
+// particle count.  A precision-form difference plane, sgn (q_self - q_other), subtracts the same difference
+// of the two planes' Gaussians: sgn (G_self - G_other).
+struct HybRows {
+    const double *gx = nullptr, *gxo = nullptr;
+    double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;  // amp * gy[j] of this plane (a) and of its partner (b)
+    bool diff = false;
+    __device__ static double amp(const Collide &C, const Plane &P, int pl, double inv) {
+        const double sgx = C.hsum[2 * pl], sgy = C.hsum[2 * pl + 1];
+        double a = (double)P.src_n;
+        if (C.o.neutralize && sgx * sgy > 0.0) a = ((double)(long long)C.qtot[pl] * inv) / (sgx * sgy);
+        return a;
+    }
+    __device__ HybRows(const Collide &C, const Plane &P, int plane0, int pl, bool on, bool diff_plane, double inv, int j0,
+                       int j1) {
+        if (!on) return;
+        const int nx = C.o.nx, ny = C.o.ny;
+        gx = C.hprof + (long long)pl * (nx + ny);
+        const double *gy = gx + nx, am = amp(C, P, pl, inv);
+        a0 = am * gy[j0];
+        if (j1 < ny) a1 = am * gy[j1];
+        diff = diff_plane;
+        if (diff) {
+            const int po = pl + P.other_delta;
+            gxo = C.hprof + (long long)po * (nx + ny);
+            const double *gyo = gxo + nx, ao = amp(C, C.planes[plane0 + po], po, inv);
+            b0 = ao * gyo[j0];
+            if (j1 < ny) b1 = ao * gyo[j1];
+        }
+    }
+    __device__ double g0(int i, long long sgn) const { return diff ? (double)sgn * (gx[i] * a0 - gxo[i] * b0) : gx[i] * a0; }
+    __device__ double g1(int i, long long sgn) const { return diff ? (double)sgn * (gx[i] * a1 - gxo[i] * b1) : gx[i] * a1; }
+};
+
+
 __global__ void __launch_bounds__(256) k_hyb_profiles(Collide C, int plane0) {
     pdl_wait();
     pdl_release();
@@ -1004,15 +1044,7 @@ __global__ void __launch_bounds__(128) k_conv_rows(Collide C, int plane0) {
     // Hybrid: subtract amp * gx[i] * gy[j] (gaussian_pic.jl:580-589); amp neutralises the subtracted
     // Gaussian to the deposited charge, else it carries the slice's particle count.
     const bool hyb = C.o.gaussian && C.hyb[P.task].mode;
-    const double *gx = C.hprof + (long long)pl * (nx + ny), *gy = gx + nx;
-    double gj0 = 0.0, gj1 = 0.0;
-    if (hyb) {
-        const double sgx = C.hsum[2 * pl], sgy = C.hsum[2 * pl + 1];
-        double amp = (double)P.src_n;
-        if (C.o.neutralize && sgx * sgy > 0.0) amp = ((double)(long long)C.qtot[pl] * inv) / (sgx * sgy);
-        gj0 = amp * gy[j0];
-        if (j1 < ny) gj1 = amp * gy[j1];
-    }
+    const HybRows hr(C, P, plane0, pl, hyb, diff, inv, j0, j1);
     for (int i = lane; i < NX; i += 32) {
         C2 v;
         v.x = R(0);
@@ -1020,12 +1052,12 @@ __global__ void __launch_bounds__(128) k_conv_rows(Collide C, int plane0) {
         if (i < nx) {
             long long qa = q[(long long)j0 * nx + i];
             if (diff) qa = sgn * (qa - qo[(long long)j0 * nx + i]);
-            v.x = hyb ? (R)((double)qa * inv - gx[i] * gj0) : (R)((double)qa * inv);
+            v.x = hyb ? (R)((double)qa * inv - hr.g0(i, sgn)) : (R)((double)qa * inv);
             if (!kPrecision && qa) q[(long long)j0 * nx + i] = 0;
             if (j1 < ny) {
                 long long qb = q[(long long)j1 * nx + i];
                 if (diff) qb = sgn * (qb - qo[(long long)j1 * nx + i]);
-                v.y = hyb ? (R)((double)qb * inv - gx[i] * gj1) : (R)((double)qb * inv);
+                v.y = hyb ? (R)((double)qb * inv - hr.g1(i, sgn)) : (R)((double)qb * inv);
                 if (!kPrecision && qb) q[(long long)j1 * nx + i] = 0;
             }
         }
@@ -1304,15 +1336,7 @@ __global__ void __launch_bounds__(128) k_conv_rows_r(Collide C, int plane0) {
     const bool diff = kPrecision && P.other_delta != 0;
     const long long sgn = P.self_first ? 1 : -1;
     const bool hyb = C.o.gaussian && C.hyb[P.task].mode;
-    const double *gx = C.hprof + (long long)pl * (nx + ny), *gy = gx + nx;
-    double gj0 = 0.0, gj1 = 0.0;
-    if (hyb && ok) {
-        const double sgx = C.hsum[2 * pl], sgy = C.hsum[2 * pl + 1];
-        double amp = (double)P.src_n;
-        if (C.o.neutralize && sgx * sgy > 0.0) amp = ((double)(long long)C.qtot[pl] * inv) / (sgx * sgy);
-        gj0 = amp * gy[j0];
-        if (j1 < ny) gj1 = amp * gy[j1];
-    }
+    const HybRows hr(C, P, plane0, pl, hyb && ok, diff, inv, j0, j1);
     C2 v[8];
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
@@ -1322,12 +1346,12 @@ __global__ void __launch_bounds__(128) k_conv_rows_r(Collide C, int plane0) {
         if (m < 4 && ok) {  // i < nx = 4 G
             long long qa = q[(long long)j0 * nx + i];
             if (diff) qa = sgn * (qa - qo[(long long)j0 * nx + i]);
-            v[m].x = hyb ? (R)((double)qa * inv - gx[i] * gj0) : (R)((double)qa * inv);
+            v[m].x = hyb ? (R)((double)qa * inv - hr.g0(i, sgn)) : (R)((double)qa * inv);
             if (!kPrecision && qa) q[(long long)j0 * nx + i] = 0;
             if (j1 < ny) {
                 long long qb = q[(long long)j1 * nx + i];
                 if (diff) qb = sgn * (qb - qo[(long long)j1 * nx + i]);
-                v[m].y = hyb ? (R)((double)qb * inv - gx[i] * gj1) : (R)((double)qb * inv);
+                v[m].y = hyb ? (R)((double)qb * inv - hr.g1(i, sgn)) : (R)((double)qb * inv);
                 if (!kPrecision && qb) q[(long long)j1 * nx + i] = 0;
             }
         }
@@ -1506,7 +1530,7 @@ struct KickJob {
     R c_src, hzi, zbias, ks;
     long long fld_start, fld_n, plane_off;
     int fld_beam, ok;
-    int hyb;               // Gaussian-subtracted hybrid active for this task (FP64 only)
+    int hyb;               // Gaussian-subtracted hybrid active for this task
     HybridTask H;
     int next_pair, next_task;  // luminosity box of the field slice's next pair (:node), or -1
     R next_sM;
@@ -1521,8 +1545,8 @@ __device__ __forceinline__ Coord6<R> load_coord(const SoA &S, long long p) {
     return Coord6<R>{col<R>(S, 0)[p], col<R>(S, 1)[p], col<R>(S, 2)[p], col<R>(S, 3)[p], col<R>(S, 4)[p], col<R>(S, 5)[p]};
 }
 
-// HYB: the Gaussian-subtracted hybrid's add-back is compiled in (FP64 only), a separate instantiation so
-// the plain kernels keep their register budget.
+// HYB: the Gaussian-subtracted hybrid's add-back (FP64 Bassetti-Erskine in both forms) is compiled in, a
+// separate instantiation so the plain kernels keep their register budget.
 template <class R, int METHOD, bool HYB>
 __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R> &J, long long p, const Coord6<R> &q,
                                               R &xo, R &pxo, R &yo, R &pyo) {
@@ -1649,7 +1673,7 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
                 Kz += tp.w[q] * (pl - pr);
             }
         }
-        if (HYB && !kPrecision && J.hyb) {
+        if (HYB && J.hyb) {
             // Analytic add-back of the subtracted Gaussian (gaussian_pic.jl:851-884): half the slice population
             // times the Bassetti-Erskine kick at both boundaries, blended in z, and its longitudinal terms.
             const HybridTask &H = J.H;
@@ -1667,9 +1691,14 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
             if (lk) {
                 const double covL = (HxL * H.rx[0] + HyL * H.ry[0]) / 4.0;
                 const double covR = (HxR * H.rx[1] + HyR * H.ry[1]) / 4.0;
-                pz += ks * Kz * J.hzi;
-                pz += (R)((double)zL * covL + (double)zR * covR);
-                pz += (R)(0.5 * (dpxa * H.mpx + dpya * H.mpy));
+                if (kPrecision) {  // summed in FP64, one rounding into the pz increment
+                    dpz += (R)((double)ks * (double)Kz * (double)J.hzi + ((double)zL * covL + (double)zR * covR) +
+                               0.5 * (dpxa * H.mpx + dpya * H.mpy));
+                } else {
+                    pz += ks * Kz * J.hzi;
+                    pz += (R)((double)zL * covL + (double)zR * covR);
+                    pz += (R)(0.5 * (dpxa * H.mpx + dpya * H.mpy));
+                }
             }
         } else {
             px += ks * Kx;

@@ -162,6 +162,7 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_umma_gemm(const GemmArgs g)
     const int Cs = g.C - g.Cu;
     const int hw = g.H * g.W;
     const float inv_hw = 1.0f / (float)(hw > 0 ? hw : 1), inv_w = 1.0f / (float)(g.W > 0 ? g.W : 1);
+    const bool direct_bf16 = g.out_bf16 != nullptr;  // bf16 (bias, ReLU) straight from the accumulator
     bool failed = false;
 
     // persistent over the M tiles of this (n, split) column
@@ -290,8 +291,12 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_umma_gemm(const GemmArgs g)
         failed = abort_flag != 0;
         if (failed) break;
         // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (tile rows); warps 0-3 take column blocks
-        // 0, 64, ..., warps 4-7 blocks 32, 96, ...
-        const int row = m0 + (warp & 3) * 32 + lane;
+        // 0, 64, ..., warps 4-7 blocks 32, 96, ...  A 32 x 32 block goes through this warp's staging area of
+        // the (now idle) A stages -- row stride 33 words, so the row-wise writes and the chunk-wise reads are
+        // both free of bank conflicts -- and leaves in 16-byte row chunks: one store instruction covers whole
+        // 64-byte (bf16) or 128-byte (fp32) row segments instead of 32 scattered rows.
+        float *stg = reinterpret_cast<float *>(smA) + warp * (32 * 33);
+        const int rbase0 = m0 + (warp & 3) * 32;
         if (nk > 0) {
 #pragma unroll 1
             for (int c0 = (warp >> 2) * 32; c0 < BN; c0 += 64) {
@@ -307,30 +312,58 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_umma_gemm(const GemmArgs g)
                       "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if (row < g.M) {
-                    if (g.out_bf16) {
-                        __nv_bfloat16 *o = g.out_bf16 + (long long)row * g.ldo + n0 + c0;
+                const int nb = n0 + c0;
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const int n = n0 + c0 + j;
-                            if (n < g.N) {
-                                float v = __uint_as_float(r[j]) + (g.bias ? g.bias[n] : 0.f);
-                                if (g.relu) v = fmaxf(v, 0.f);
-                                o[j] = __float2bfloat16_rn(v);
-                            }
+                for (int j = 0; j < 32; ++j) {
+                    float v = __uint_as_float(r[j]);
+                    if (g.bias && nb + j < g.N) v += g.bias[nb + j];
+                    if (direct_bf16 && g.relu) v = fmaxf(v, 0.f);
+                    stg[lane * 33 + j] = v;
+                }
+                __syncwarp();
+                if (direct_bf16) {
+                    // 32 rows x 4 chunks of 8 columns
+                    const bool vec = ((g.ldo & 7) == 0) && ((reinterpret_cast<uintptr_t>(g.out_bf16) & 15) == 0);
+#pragma unroll
+                    for (int it = 0; it < 4; ++it) {
+                        const int q = it * 32 + lane, rr = q >> 2, part = q & 3;
+                        const int m = rbase0 + rr, n = nb + part * 8;
+                        if (m >= g.M || n >= g.N) continue;
+                        const float *src = stg + rr * 33 + part * 8;
+                        __nv_bfloat16 *o = g.out_bf16 + (long long)m * g.ldo + n;
+                        if (vec && n + 8 <= g.N) {
+                            uint4 w;
+                            __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&w);
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) h[e] = __floats2bfloat162_rn(src[2 * e], src[2 * e + 1]);
+                            *reinterpret_cast<uint4 *>(o) = w;
+                        } else {
+                            for (int e = 0; e < 8 && n + e < g.N; ++e) o[e] = __float2bfloat16_rn(src[e]);
                         }
-                    } else {
-                        float *o = g.out + (long long)blockIdx.z * g.split_stride + (long long)row * g.ldc + n0 + c0;
+                    }
+                } else {
+                    // 32 rows x 8 chunks of 4 columns
+                    float *base = g.out + (long long)blockIdx.z * g.split_stride;
+                    const bool vec = ((g.ldc & 3) == 0) && ((g.split_stride & 3) == 0) &&
+                                     ((reinterpret_cast<uintptr_t>(g.out) & 15) == 0);
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const int n = n0 + c0 + j;
-                            if (n < g.N) o[j] = __uint_as_float(r[j]) + (g.bias ? g.bias[n] : 0.f);
+                    for (int it = 0; it < 8; ++it) {
+                        const int q = it * 32 + lane, rr = q >> 3, part = q & 7;
+                        const int m = rbase0 + rr, n = nb + part * 4;
+                        if (m >= g.M || n >= g.N) continue;
+                        const float *src = stg + rr * 33 + part * 4;
+                        float *o = base + (long long)m * g.ldc + n;
+                        if (vec && n + 4 <= g.N) {
+                            *reinterpret_cast<float4 *>(o) = make_float4(src[0], src[1], src[2], src[3]);
+                        } else {
+                            for (int e = 0; e < 4 && n + e < g.N; ++e) o[e] = src[e];
                         }
                     }
                 }
+                __syncwarp();
             }
-        } else if (!g.out_bf16 && warp < 4 && row < g.M) {  // an empty K range contributes zeros
-            float *o = g.out + (long long)blockIdx.z * g.split_stride + (long long)row * g.ldc;
+        } else if (!direct_bf16 && warp < 4 && rbase0 + lane < g.M) {  // an empty K range contributes zeros
+            float *o = g.out + (long long)blockIdx.z * g.split_stride + (long long)(rbase0 + lane) * g.ldc;
             for (int n = n0; n < min(g.N, n0 + BN); ++n) o[n] = 0.f;
         }
         // the next tile's first MMA overwrites the accumulator: every TMEM read of this tile precedes it
@@ -344,7 +377,8 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_umma_gemm(const GemmArgs g)
 }
 
 // Split-K partials of a convolution summed in a fixed order, plus bias and ReLU, rounded to bf16:
-// out[m * ldo + n] = bf16(relu?(sum_z part[z][m][n] + bias[n])).
+// out[m * ldo + n] = bf16(relu?(sum_z part[z][m][n] + bias[n])).  (A fused variant in which the last CTA of a
+// tile reduces measured slower: that CTA's serial reduction lies on the layer's critical path.)
 __global__ void k_umma_split_epilogue(const float *__restrict__ part, int splits, long long M, int N,
                                       const float *__restrict__ bias, int relu, __nv_bfloat16 *__restrict__ out,
                                       long long ldo) {

@@ -223,12 +223,18 @@ void launch_gemm(const GemmArgs &g, int splits, cudaStream_t st) {
     const int slot = bn == 32 ? 0 : (bn == 64 ? 1 : (bn == 128 ? 2 : 3));
     auto go = [&](void (*kernel)(const GemmArgs)) {
         CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // all of the unified L1 / shared array as shared memory, so two CTAs fit on an SM
+        CK(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         // persistent CTAs: as many as are resident at once, spread over the (n, split) columns
         int dev = 0, sms = 0, per_sm = resident[slot].load();
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         if (per_sm == 0) {
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kGemmThreads, smem));
+            // shared memory decides: the kernel's launch bounds guarantee two CTAs' registers, and each CTA
+            // holds its stages, about 1 KB of static shared memory and the 1 KB the driver reserves
+            int sm_bytes = 0;
+            CK(cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+            per_sm = std::max(1, std::min(2, sm_bytes / (int)(smem + 2048)));
             resident[slot].store(per_sm);
         }
         const int slots = std::max(1, sms * std::max(1, per_sm));
@@ -441,10 +447,6 @@ int validate_options(const octo_pic_options &o, std::string &msg) {
             return OCTO_ERR_UNSUPPORTED;
         }
         if (!(o.margin_sigma >= 0.0)) { msg = "margin_sigma must be non-negative"; return OCTO_ERR_ARG; }
-        if (o.precision != 0) {
-            msg = "the Gaussian-subtracted hybrid runs in the FP64 plain form on this backend (float64 beams)";
-            return OCTO_ERR_UNSUPPORTED;
-        }
     }
     if (o.precision != 0 && o.precision != 1) {
         msg = "precision must be 0 (FP64 plain form) or 1 (FP32 precision form)";
@@ -1308,7 +1310,7 @@ void CollideJob::run() {
             PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, gaussian ? 2 : 1, slice_bytes * 5 * rsz);
             with_real(fp32, [&](auto r) { launch_pdl(k_pair_bounds<decltype(r)>, dim3(bps, 2 * npf), 256, 0, st, C, F.t0); });
             if (gaussian) {
-                launch_pdl(k_hyb_moments, dim3(bps, 2 * npf), 256, 0, st, C, F.t0);
+                with_real(fp32, [&](auto r) { launch_pdl(k_hyb_moments<decltype(r)>, dim3(bps, 2 * npf), 256, 0, st, C, F.t0); });
                 launch_pdl(k_hyb_fold, (F.nt * 32 + 127) / 128, 128, 0, st, C, F.t0, F.nt, (int)bps);
             }
             launches += gaussian ? 3 : 1;
@@ -1335,7 +1337,7 @@ void CollideJob::run() {
         if (!node) {
             {
                 PhaseScope ps(c, OCTO_PHASE_PLAN, st, 1);
-                launch_pdl(k_plan, (F.nt + 63) / 64, 64, 0, st, C, F.t0, F.nt, 0);
+                with_real(fp32, [&](auto r) { launch_pdl(k_plan<decltype(r)>, (F.nt + 63) / 64, 64, 0, st, C, F.t0, F.nt, 0); });
             }
             PhaseScope ps(c, OCTO_PHASE_GREEN, st, gaussian ? 3 : 2);
             launch_green(c, C, 0, F.t0, F.nt, st);

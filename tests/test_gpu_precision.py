@@ -141,3 +141,19 @@ def test_precision_form_rejects_float64_beams():
         ctx.collide(ob.Beam.from_numpy(e, pe), ob.Beam.from_numpy(p, pp))
     assert "float32" in str(err.value)
     ctx.close()
+
+
+@pytest.mark.parametrize("opts", [
+    dict(),
+    dict(deposit_method="TSC", field_derivative="fourth"),
+    dict(neutralize=False, margin_sigma=0.0, green_cache="none", grid=(48, 48)),
+])
+def test_precision_form_gaussian_hybrid(opts):
+    """GaussianPICPoissonSolver in the precision form: FP32 particles, residual planes and FFTs (the R plane an
+    exact int64 difference L - R with the difference of the two reference Gaussians subtracted), FP64 moments,
+    reference Gaussians and Bassetti-Erskine add-back; against the oracle's FP64 hybrid under the same bounds."""
+    import octo_b200 as ob
+    kw = dict(grid=(64, 64), slicing=ob.LongitudinalSlicing(nslices=4, method="normal_quantile"))
+    kw.update(opts)
+    s = ob.GaussianPICPoissonSolver(**kw)
+    check(run_precision(s, 6000, 4000, e_sigma=(95e-6, 8.5e-6, 7e-3), p_sigma=(95e-6, 8.5e-6, 6e-2)))
