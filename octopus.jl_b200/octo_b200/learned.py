@@ -366,12 +366,31 @@ class LearnedForm:
         return lum
 
 
+def time_forward(batch: int, grid: int = 48, repeats: int = 50, warmup: int = 5, device: int = 0) -> float:
+    """Device microseconds of one network forward pass over `batch` planes (CUDA events on the launching
+    stream, after `warmup` passes) -- the cost the learned correction adds to each wavefront."""
+    net = FieldCorrectionNet(grid, grid, max_batch=max(64, batch), device=device)
+    x = torch.randn(batch, grid, grid, 8, device=f"cuda:{device}").to(torch.bfloat16)
+    for _ in range(warmup):
+        net.forward(x)
+    torch.cuda.synchronize(device)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(repeats):
+        net.forward(x)
+    b.record()
+    torch.cuda.synchronize(device)
+    net.close()
+    return a.elapsed_time(b) / repeats * 1e3
+
+
 def _main(argv=None):
     """python -m octo_b200.learned --samples N --steps K [--out PATH]: generate pairs, train, evaluate on
-    held-out pairs, save the weights."""
+    held-out pairs, save the weights.  --time-forward B: only time the network's forward pass over B planes."""
     import argparse
     import json
     ap = argparse.ArgumentParser()
+    ap.add_argument("--time-forward", type=int, default=0, metavar="B")
     ap.add_argument("--samples", type=int, default=20000)
     ap.add_argument("--heldout", type=int, default=512)
     ap.add_argument("--steps", type=int, default=6000)
@@ -382,6 +401,9 @@ def _main(argv=None):
     ap.add_argument("--coarse", default="hybrid", choices=COARSE)
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
+    if a.time_forward:
+        print(json.dumps({"batch": a.time_forward, "grid": a.grid, "forward_us": time_forward(a.time_forward, a.grid)}))
+        return
     import time
     t0 = time.time()
     X, T, M, F = make_dataset(a.samples, a.seed, grid=a.grid, coarse=a.coarse)
