@@ -106,6 +106,10 @@ typedef struct {
     int32_t include_sigma_xy;          /* 1: the full (coupled) transverse slice covariance */
     double min_sigma;                  /* transverse RMS floor, finite and >= 0 */
     int32_t resolution1, resolution2;  /* LongitudinalSlicing resolution (:equal_area bins per slice); 0 = 100 */
+    /* hybrid (gaussian = 1): |r_xy| of a drifted source slice above which the coupled (rotated) subtraction runs
+     * (gaussian_pic.jl:94-110, 525-536); INFINITY (the reference's default) always subtracts the separable
+     * Gaussian; must be >= 0.  Zero-initialised structs get 0: set INFINITY for the default. */
+    double coupling_tol;
 } octo_pic_options;
 #define OCTO_SOLVER_PIC 0
 #define OCTO_SOLVER_SOFT_GAUSSIAN 1

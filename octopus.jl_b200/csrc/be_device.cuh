@@ -317,4 +317,65 @@ __device__ __forceinline__ void be_response(double kbb, double sigx, double sigy
     else be_response_principal(kbb, sigy, sigx, y, x, Ky, Kx, Hy, Hx);
 }
 
+// Transverse moments of a Gaussian: its centroid (unused by the kick) and the covariance entries of
+// StrongTransverseMoments (strong_beam.jl:79-90).  Shared by the soft-Gaussian solver and the coupled
+// add-back of the Gaussian-subtracted hybrid.
+struct GMoments {
+    double mx, mpx, my, mpy;            // zero when the beam's centroid is ignored
+    double a0, d0, bxx, bypy, qxx, qyy; // var x, var y, cov(x, px), cov(y, py), var px, var py
+    double b0, bxpy, bypx, qxy;         // coupled: cov(x, y), cov(x, py), cov(px, y), cov(px, py); else zero
+};
+
+// The coupled _cp_covariance_kick (strong_beam.jl:634-682): the transported covariance's principal axes, the
+// rotated kick and potential Hessians, the covariance pz term and the rotation term L / D.
+__device__ __noinline__ void coupled_kick(const GMoments &M, double kbb, double S, double xx, double yy, double &px,
+                                          double &py, double &pz, double &density) {
+    const double a = M.a0 - 2 * S * M.bxx + S * S * M.qxx;
+    const double b = M.b0 - S * (M.bxpy + M.bypx) + S * S * M.qxy;
+    const double d = M.d0 - 2 * S * M.bypy + S * S * M.qyy;
+    const double au = 2 * (M.bxx - S * M.qxx);
+    const double bu = M.bxpy + M.bypx - 2 * S * M.qxy;
+    const double du = 2 * (M.bypy - S * M.qyy);
+    const double detA = a * d - b * b;
+    const double twopi = 6.283185307179586476925286766559005768394338;
+    density = 0.0;
+    if (a <= 0 || d <= 0 || detA <= 0) return;
+    const double adiff = a - d;
+    const double D = hypot(adiff, 2 * b);
+    if (D == 0.0) {
+        const double sigma = sqrt((a + d) / 2);
+        const double expterm = exp(-0.5 * (xx * xx + yy * yy) / (sigma * sigma));
+        double Kx, Ky, Hxx, Hxy, Hyy;
+        be_round(kbb, sigma, xx, yy, expterm, Kx, Ky, Hxx, Hxy, Hyy);
+        px += kbb * Kx;
+        py += kbb * Ky;
+        pz += 0.25 * (Hxx * au + 2 * Hxy * bu + Hyy * du);
+        density = expterm / (twopi * sigma * sigma);
+        return;
+    }
+    const double theta = 0.5 * atan2(2 * b, a - d);
+    double sn, cs;
+    sincos(theta, &sn, &cs);
+    const double lambda1 = (a + d + D) / 2, lambda2 = (a + d - D) / 2;
+    const double sig1 = sqrt(lambda1), sig2 = sqrt(lambda2);
+    const double xh = cs * xx + sn * yy;
+    const double yh = -sn * xx + cs * yy;
+    const double eta = D / (a + d);
+    double inner, outer;
+    be_eta_bounds(inner, outer);
+    double Kxh, Kyh, H11, H22, LoD;
+    if (eta <= inner) be_near_round(kbb, (a + d) / 2, eta, xh, yh, Kxh, Kyh, H11, H22, &LoD);
+    else be_response_principal(kbb, sig1, sig2, xh, yh, Kxh, Kyh, H11, H22, &LoD);
+    const double expterm = exp(-0.5 * (xh * xh / lambda1 + yh * yh / lambda2));
+    const double Fxh = kbb * Kxh, Fyh = kbb * Kyh;
+    px += cs * Fxh - sn * Fyh;
+    py += sn * Fxh + cs * Fyh;
+    const double Du = (adiff * (au - du) + 4 * b * bu) / D;
+    const double traceu = au + du;
+    pz += 0.125 * ((H11 + H22) * traceu + (H11 - H22) * Du);
+    const double rotation_projection = (adiff * bu - b * (au - du)) / D;
+    pz -= 0.5 * kbb * rotation_projection * LoD;
+    density = expterm / (twopi * sig1 * sig2);
+}
+
 }  // namespace octo

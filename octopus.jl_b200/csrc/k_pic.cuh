@@ -50,7 +50,8 @@ struct Collide {           // device pointers for one collide (passed by value)
     HybridTask *hyb;             // [task]
     double *hmom;                // [task][kMaxBoundBlocks][kMomentSums] block partial moment sums
     unsigned long long *qtot;    // [plane-in-front] total fixed-point charge of the plane (two's complement)
-    double *hprof;               // [plane-in-front][nx + ny] reference-Gaussian node profiles
+    double *hprof;               // [plane-in-front][3][nx + ny] reference-Gaussian node profiles (gx | gy, then the
+                                 // coupled subtraction's m1x | dgy and m2x | ddgy)
     double *hsum;                // [plane-in-front][2] profile sums
 };
 
@@ -201,6 +202,7 @@ __global__ void __launch_bounds__(256) k_hyb_moments(Collide C, int task0) {
     double a[kMomentSums];
 #pragma unroll
     for (int k = 0; k < kMomentSums; ++k) a[k] = 0.0;
+    const bool gate = isfinite(C.o.coupling_tol);  // the cross-plane sums only when the coupled path can read them
     if (n > 0) {
         const double x0 = X[0], px0 = PX[0], y0 = Y[0], py0 = PY[0];
         for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
@@ -208,6 +210,7 @@ __global__ void __launch_bounds__(256) k_hyb_moments(Collide C, int task0) {
             a[0] += dx; a[1] += dpx; a[2] += dy; a[3] += dpy;
             a[4] += dx * dx; a[5] += dpx * dpx; a[6] += dy * dy; a[7] += dpy * dpy;
             a[8] += dx * dpx; a[9] += dy * dpy;
+            if (gate) { a[10] += dx * dy; a[11] += dx * dpy; a[12] += dy * dpx; a[13] += dpx * dpy; }
         }
     }
     __shared__ double red[8][kMomentSums];
@@ -250,6 +253,28 @@ __device__ __forceinline__ void hyb_boundary(const double m[10], double s, Hybri
     H.sigy[side] = sqrt(jmax(vary, 0.0));
     H.rx[side] = 2.0 * (m[3] + s * m[4]);
     H.ry[side] = 2.0 * (m[8] + s * m[9]);
+}
+
+// Coupled boundary (gaussian_pic.jl:449-523): the covariance transported to drift s (S = -s in the field-
+// particle convention), its correlation, whether it is resolved (full rank to sqrt(eps)), the conditional slope
+// and sigma.  cv: a0, b0, d0, bxx, bxpy, bypx, bypy, qxx, qxy, qyy.
+__device__ __forceinline__ void hyb_coupled_boundary(const double cv[10], double s, HybridTask &H, int side, double &rxy,
+                                                     bool &resolved) {
+    const double S = -s;
+    const double a = cv[0] - 2 * S * cv[3] + S * S * cv[7];
+    const double b = cv[1] - S * (cv[4] + cv[5]) + S * S * cv[8];
+    const double d = cv[2] - 2 * S * cv[6] + S * S * cv[9];
+    rxy = (a <= 0 || d <= 0) ? 0.0 : (b / sqrt(a)) / sqrt(d);
+    bool ok = isfinite(a) && isfinite(b) && isfinite(d) && a > 0 && d > 0;
+    if (ok) {
+        const double rho = (b / sqrt(a)) / sqrt(d);
+        ok = isfinite(rho) && fma(-rho, rho, 1.0) > 1.4901161193847656e-08;  // sqrt(eps(Float64))
+    }
+    resolved = ok;
+    H.sa[side] = sqrt(a);
+    H.lam[side] = ok ? b / a : 0.0;
+    const double rcv = ok ? jmax(fma(-rxy, rxy, 1.0), 0.0) : 0.0;
+    H.sigc[side] = ok ? sqrt(d * rcv) : 0.0;
 }
 
 __device__ inline void record_error(DevStatus *st, int task, int code, int role) {
@@ -313,7 +338,28 @@ __global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0) {
         bool ok = n >= 2;
         for (int sd = 0; sd < 2; ++sd)
             ok = ok && isfinite(H.sigx[sd]) && isfinite(H.sigy[sd]) && H.sigx[sd] > 0 && H.sigy[sd] > 0;
-        H.mode = ok ? 1 : 0;
+        // the full covariance (gaussian_pic.jl:374-447; cross terms only under a finite coupling_tol) and the
+        // control-variate mode (gaussian_pic.jl:525-536): 0 plain PIC, 1 uncoupled, 2 coupled
+        const bool gate = isfinite(C.o.coupling_tol);
+        double *cv = H.cov;
+        cv[0] = m[2]; cv[2] = m[7]; cv[3] = m[3]; cv[6] = m[8]; cv[7] = m[4]; cv[9] = m[9];
+        cv[1] = gate ? fma(-dmx, dmy, sum[10] * invn) : 0.0;
+        cv[4] = gate ? fma(-dmx, dmpy, sum[11] * invn) : 0.0;
+        cv[5] = gate ? fma(-dmy, dmpx, sum[12] * invn) : 0.0;
+        cv[8] = gate ? fma(-dmpx, dmpy, sum[13] * invn) : 0.0;
+        bool resolved[2] = {false, false};
+        double rxy[2] = {0.0, 0.0};
+        for (int sd = 0; sd < 2; ++sd) {
+            const double sb = sd ? T.sR : T.sL;
+            H.s[sd] = sb;
+            H.sa[sd] = H.lam[sd] = H.sigc[sd] = 0.0;
+            if (!gate) continue;
+            hyb_coupled_boundary(cv, sb, H, sd, rxy[sd], resolved[sd]);
+        }
+        int mode = ok ? 1 : 0;
+        if (ok && gate && jmax(fabs(rxy[0]), fabs(rxy[1])) > C.o.coupling_tol) mode = resolved[0] && resolved[1] ? 2 : 0;
+        H.mode = mode;
+        ok = mode != 0;
         if (ok && C.o.margin > 0) {
             const double mg = C.o.margin;
             sxmin = jmin(sxmin, jmin(H.mux[0] - mg * H.sigx[0], H.mux[1] - mg * H.sigx[1]));
@@ -698,7 +744,7 @@ __device__ __forceinline__ T *generic_ptr(T *p) {
 // rot (CIC): the lane's four atomics start at tap rot & 3 -- particles of a spatially ordered slice share
 // cells with their warp neighbours, and rotating the tap order spreads a warp's simultaneous atomics over
 // four addresses per cell.  Integer sums: the order changes nothing.
-template <class R, int METHOD, bool TOTAL = false>
+template <class R, int METHOD, bool TOTAL = false, bool ROT = false>
 __device__ __forceinline__ long long deposit_taps(R u, R v, int nw, int nh, R scale, long long *grid, int ld, int rot = 0) {
     constexpr int NT = METHOD == 0 ? 2 : 3;
     int ix, iy;
@@ -712,13 +758,15 @@ __device__ __forceinline__ long long deposit_taps(R u, R v, int nw, int nh, R sc
         long long q2 = round_ll(wx[1] * wy[0] * scale), q3 = round_ll(wx[1] * wy[1] * scale);
         if (TOTAL) total = q0 + q1 + q2 + q3;
         int o0 = c0, o1 = c0 + ld, o2 = c0 + 1, o3 = c0 + ld + 1;
-        if (rot & 1) {
-            const int to = o0; o0 = o1; o1 = o2; o2 = o3; o3 = to;
-            const long long tq = q0; q0 = q1; q1 = q2; q2 = q3; q3 = tq;
-        }
-        if (rot & 2) {
-            int to = o0; o0 = o2; o2 = to; to = o1; o1 = o3; o3 = to;
-            long long tq = q0; q0 = q2; q2 = tq; tq = q1; q1 = q3; q3 = tq;
+        if constexpr (ROT) {  // a separate instantiation: the permutation costs the unrotated deposit nothing
+            if (rot & 1) {
+                const int to = o0; o0 = o1; o1 = o2; o2 = o3; o3 = to;
+                const long long tq = q0; q0 = q1; q1 = q2; q2 = q3; q3 = tq;
+            }
+            if (rot & 2) {
+                int to = o0; o0 = o2; o2 = to; to = o1; o1 = o3; o3 = to;
+                long long tq = q0; q0 = q2; q2 = tq; tq = q1; q1 = q3; q3 = tq;
+            }
         }
         atomicAdd((unsigned long long *)&grid[o0], (unsigned long long)q0);
         atomicAdd((unsigned long long *)&grid[o1], (unsigned long long)q1);
@@ -787,8 +835,8 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
     const int rot = C.o.dep_rotate ? (int)(threadIdx.x & 3) : 0;
     // the next particle's coordinates are loaded before the current one's taps, two loads in flight
     const long long stride = (long long)gridDim.x * blockDim.x;
-    auto sweep = [&](auto with_total) {
-        constexpr bool TOT = decltype(with_total)::value;
+    auto sweep = [&](auto with_total, auto rotated) {
+        constexpr bool TOT = decltype(with_total)::value, ROT = decltype(rotated)::value;
         long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
         R cx = 0, cpx = 0, cy = 0, cpy = 0;
         if (k < P.src_n) { const long long p = P.src_start + k; cx = X[p]; cpx = PX[p]; cy = Y[p]; cpy = PY[p]; }
@@ -802,12 +850,14 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
             const R yd = cy + cpy * s;
             if (P.count_dropped && !(isfinite(xd) && xlo <= xd && xd <= xhi && isfinite(yd) && ylo <= yd && yd <= yhi))
                 ++outside;
-            total += deposit_taps<R, METHOD, TOT>((xd - x0) * hxi, (yd - y0) * hyi, nx, ny, scale, acc, nx, rot);
+            total += deposit_taps<R, METHOD, TOT, ROT>((xd - x0) * hxi, (yd - y0) * hyi, nx, ny, scale, acc, nx, rot);
             cx = nx_; cpx = npx; cy = ny_; cpy = npy;
         }
     };
-    if (C.o.gaussian) sweep(std::true_type());
-    else sweep(std::false_type());
+    // (the hybrid's exact plane totals and the rotation for spatially ordered slices never combine)
+    if (C.o.gaussian) sweep(std::true_type(), std::false_type());
+    else if (C.o.dep_rotate) sweep(std::false_type(), std::true_type());
+    else sweep(std::false_type(), std::false_type());
     if (C.o.gaussian) {  // the plane's exact total charge, for the neutralised subtraction
         for (int o = 16; o; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
         if ((threadIdx.x & 31) == 0 && total) atomicAdd(&C.qtot[pl], (unsigned long long)total);
@@ -855,20 +905,25 @@ __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0, int
     const R x0 = (R)L.x0, y0 = (R)L.y0;
     const long long stride = (long long)gridDim.x * blockDim.x;
     const int rot = C.o.dep_rotate ? (int)(threadIdx.x & 3) : 0;
-    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    R cx = 0, cpx = 0, cy = 0, cpy = 0;
-    if (k < n) { cx = X[st + k]; cpx = PX[st + k]; cy = Y[st + k]; cpy = PY[st + k]; }
-    for (; k < n; k += stride) {  // next particle prefetched, as in k_deposit
-        R nx_ = 0, npx = 0, ny_ = 0, npy = 0;
-        if (k + stride < n) {
-            const long long q = st + k + stride;
-            nx_ = X[q]; npx = PX[q]; ny_ = Y[q]; npy = PY[q];
+    auto sweep = [&](auto rotated) {
+        constexpr bool ROT = decltype(rotated)::value;
+        long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        R cx = 0, cpx = 0, cy = 0, cpy = 0;
+        if (k < n) { cx = X[st + k]; cpx = PX[st + k]; cy = Y[st + k]; cpy = PY[st + k]; }
+        for (; k < n; k += stride) {  // next particle prefetched, as in k_deposit
+            R nx_ = 0, npx = 0, ny_ = 0, npy = 0;
+            if (k + stride < n) {
+                const long long q = st + k + stride;
+                nx_ = X[q]; npx = PX[q]; ny_ = Y[q]; npy = PY[q];
+            }
+            const R vx = cx + cpx * s;
+            const R vy = cy + cpy * s;
+            deposit_taps<R, METHOD, false, ROT>((vx - x0) * hxi, (vy - y0) * hyi, nw, nh, scale, acc, nw, rot);
+            cx = nx_; cpx = npx; cy = ny_; cpy = npy;
         }
-        const R vx = cx + cpx * s;
-        const R vy = cy + cpy * s;
-        deposit_taps<R, METHOD>((vx - x0) * hxi, (vy - y0) * hyi, nw, nh, scale, acc, nw, rot);
-        cx = nx_; cpx = npx; cy = ny_; cpy = npy;
-    }
+    };
+    if (C.o.dep_rotate) sweep(std::true_type());
+    else sweep(std::false_type());
     if (local) {
         __syncthreads();
         merge_grid(sq, C.lq + (long long)blockIdx.y * cells, cells);
@@ -944,39 +999,129 @@ __device__ __forceinline__ double gauss_node_weight(int method, double xi, doubl
            1.5 * (m1(lL, lR) - m1(rL, rR)) / h + 0.5 * (m2(lL, lR) + m2(rL, rR)) / (h * h);
 }
 
+// Coupled subtraction (gaussian_pic.jl:240-372): central moments c_0..c_4 of the unit Gaussian over [A, B] by
+// the integration-by-parts recursion, shifted to node-centred moments about xi (d = mu - xi).
+__device__ __forceinline__ void gauss_cell_moments(double A, double B, double mu, double s, double xi, double m[5]) {
+    const double invroot = 1.0 / (s * 1.4142135623730951);
+    const double norm = 1.0 / (s * 2.5066282746310002);  // s * sqrt(2 pi)
+    const double a = A - mu, b = B - mu;
+    const double GA = norm * exp(-(a * a) / (2.0 * s * s));
+    const double GB = norm * exp(-(b * b) / (2.0 * s * s));
+    const double s2 = s * s;
+    double c[5];
+    c[0] = 0.5 * (erf(b * invroot) - erf(a * invroot));
+    c[1] = -s2 * (GB - GA);
+    c[2] = -s2 * (b * GB - a * GA) + s2 * c[0];
+    c[3] = -s2 * (b * b * GB - a * a * GA) + 2.0 * s2 * c[1];
+    c[4] = -s2 * (b * b * b * GB - a * a * a * GA) + 3.0 * s2 * c[2];
+    const double d = mu - xi, d2 = d * d, d3 = d2 * d, d4 = d3 * d;
+    m[0] = c[0];
+    m[1] = c[1] + d * c[0];
+    m[2] = c[2] + 2.0 * d * c[1] + d2 * c[0];
+    m[3] = c[3] + 3.0 * d * c[2] + 3.0 * d2 * c[1] + d3 * c[0];
+    m[4] = c[4] + 4.0 * d * c[3] + 6.0 * d2 * c[2] + 4.0 * d3 * c[1] + d4 * c[0];
+}
+// Assignment-weighted moments W_k = int (x - xi)^k G W(x - xi), k = 0, 1, 2 (gaussian_pic.jl:304-324).
+__device__ __forceinline__ void gauss_weighted_moments(int method, double xi, double h, double mu, double s, double W[3]) {
+    if (method == 0) {
+        double L[5], Rm[5];
+        gauss_cell_moments(xi - h, xi, mu, s, xi, L);
+        gauss_cell_moments(xi, xi + h, mu, s, xi, Rm);
+        for (int k = 0; k < 3; ++k) W[k] = (L[k] + L[k + 1] / h) + (Rm[k] - Rm[k + 1] / h);
+        return;
+    }
+    const double half = h / 2.0;
+    double Cm[5], Lw[5], Rw[5];
+    gauss_cell_moments(xi - half, xi + half, mu, s, xi, Cm);
+    gauss_cell_moments(xi - 3.0 * half, xi - half, mu, s, xi, Lw);
+    gauss_cell_moments(xi + half, xi + 3.0 * half, mu, s, xi, Rw);
+    for (int k = 0; k < 3; ++k) {
+        const double core = 0.75 * Cm[k] - Cm[k + 2] / (h * h);
+        const double wl = 1.125 * Lw[k] + 1.0 * 1.5 * Lw[k + 1] / h + 0.5 * Lw[k + 2] / (h * h);
+        const double wr = 1.125 * Rw[k] + -1.0 * 1.5 * Rw[k + 1] / h + 0.5 * Rw[k + 2] / (h * h);
+        W[k] = core + wl + wr;
+    }
+}
+// Mean-derivatives g', g'' of the 1D node profile (gaussian_pic.jl:330-348).
+__device__ __forceinline__ void gauss_profile_derivs(int method, double yj, double h, double mu, double s, double &dg,
+                                                     double &ddg) {
+    const double invroot = 1.0 / (s * 1.4142135623730951);
+    const double norm = 1.0 / (s * 2.5066282746310002);
+    auto pdf = [&](double y) { return norm * exp(-((y - mu) * (y - mu)) / (2.0 * s * s)); };
+    auto m0 = [&](double A, double B) { return 0.5 * (erf((B - mu) * invroot) - erf((A - mu) * invroot)); };
+    if (method == 0) {
+        dg = (m0(yj - h, yj) - m0(yj, yj + h)) / h;
+        ddg = (pdf(yj - h) - 2.0 * pdf(yj) + pdf(yj + h)) / h;
+        return;
+    }
+    const double half = h / 2.0;
+    double Cm[5], Lw[5], Rw[5];
+    gauss_cell_moments(yj - half, yj + half, mu, s, yj, Cm);
+    gauss_cell_moments(yj - 3.0 * half, yj - half, mu, s, yj, Lw);
+    gauss_cell_moments(yj + half, yj + 3.0 * half, mu, s, yj, Rw);
+    dg = -2.0 * Cm[1] / (h * h) + (1.5 * Lw[0] + Lw[1] / h) / h + (-1.5 * Rw[0] + Rw[1] / h) / h;
+    ddg = (-2.0 * m0(yj - half, yj + half) + m0(yj - 3.0 * half, yj - half) + m0(yj + half, yj + 3.0 * half)) / (h * h);
+}
+
 // Hybrid: the subtracted reference Gaussian of rows j0, j1 of a plane, amp * gx[i] * gy[j]
-// (gaussian_pic.jl:580-589); amp neutralises it to the plane's deposited charge, else it carries the slice's
-// particle count.  A precision-form difference plane, sgn (q_self - q_other), subtracts the same difference
-// of the two planes' Gaussians: sgn (G_self - G_other).
+// (gaussian_pic.jl:580-589), or for the coupled subtraction amp * (gx[i] gy[j] + lambda m1x[i] g'y[j] +
+// lambda^2 / 2 m2x[i] g''y[j]) (gaussian_pic.jl:612-630); amp neutralises it to the plane's deposited charge,
+// else it carries the slice's particle count.  A precision-form difference plane, sgn (q_self - q_other),
+// subtracts the same difference of the two planes' Gaussians: sgn (G_self - G_other).
 struct HybRows {
-    const double *gx = nullptr, *gxo = nullptr;
-    double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;  // amp * gy[j] of this plane (a) and of its partner (b)
-    bool diff = false;
-    __device__ static double amp(const Collide &C, const Plane &P, int pl, double inv) {
-        const double sgx = C.hsum[2 * pl], sgy = C.hsum[2 * pl + 1];
-        double a = (double)P.src_n;
-        if (C.o.neutralize && sgx * sgy > 0.0) a = ((double)(long long)C.qtot[pl] * inv) / (sgx * sgy);
-        return a;
+    struct Side {
+        const double *gx = nullptr, *m1x = nullptr, *m2x = nullptr;
+        double g[2] = {0.0, 0.0}, d[2] = {0.0, 0.0}, e[2] = {0.0, 0.0};  // amp gy, amp lam g'y, amp lam^2/2 g''y
+        __device__ double at(int i, int r, bool cpl) const {
+            return cpl ? gx[i] * g[r] + m1x[i] * d[r] + m2x[i] * e[r] : gx[i] * g[r];
+        }
+    };
+    Side self, other;
+    bool diff = false, cpl = false;
+    __device__ static void load(const Collide &C, const Plane &P, int pl, double inv, bool cpl, int j0, int j1, Side &S) {
+        const int nx = C.o.nx, ny = C.o.ny, L = nx + ny;
+        S.gx = C.hprof + (long long)pl * 3 * L;
+        S.m1x = S.gx + L;
+        S.m2x = S.gx + 2 * L;
+        const double *gy = S.gx + nx, *dgy = S.m1x + nx, *ddgy = S.m2x + nx;
+        double am = (double)P.src_n, lam = 0.0, half_lam2 = 0.0;
+        if (cpl) {
+            const HybridTask &H = C.hyb[P.task];
+            lam = H.lam[P.kind == 0 ? 0 : 1];
+            half_lam2 = 0.5 * lam * lam;
+            const double sg = C.hsum[2 * pl];
+            if (C.o.neutralize && sg != 0.0) am = ((double)(long long)C.qtot[pl] * inv) / sg;
+        } else {
+            const double sgx = C.hsum[2 * pl], sgy = C.hsum[2 * pl + 1];
+            if (C.o.neutralize && sgx * sgy > 0.0) am = ((double)(long long)C.qtot[pl] * inv) / (sgx * sgy);
+        }
+        const int js[2] = {j0, j1};
+        for (int r = 0; r < 2; ++r) {
+            if (js[r] >= ny) continue;
+            S.g[r] = am * gy[js[r]];
+            if (cpl) {
+                S.d[r] = am * lam * dgy[js[r]];
+                S.e[r] = am * half_lam2 * ddgy[js[r]];
+            }
+        }
     }
     __device__ HybRows(const Collide &C, const Plane &P, int plane0, int pl, bool on, bool diff_plane, double inv, int j0,
                        int j1) {
         if (!on) return;
-        const int nx = C.o.nx, ny = C.o.ny;
-        gx = C.hprof + (long long)pl * (nx + ny);
-        const double *gy = gx + nx, am = amp(C, P, pl, inv);
-        a0 = am * gy[j0];
-        if (j1 < ny) a1 = am * gy[j1];
+        cpl = C.hyb[P.task].mode == 2;
+        load(C, P, pl, inv, cpl, j0, j1, self);
         diff = diff_plane;
         if (diff) {
             const int po = pl + P.other_delta;
-            gxo = C.hprof + (long long)po * (nx + ny);
-            const double *gyo = gxo + nx, ao = amp(C, C.planes[plane0 + po], po, inv);
-            b0 = ao * gyo[j0];
-            if (j1 < ny) b1 = ao * gyo[j1];
+            load(C, C.planes[plane0 + po], po, inv, cpl, j0, j1, other);
         }
     }
-    __device__ double g0(int i, long long sgn) const { return diff ? (double)sgn * (gx[i] * a0 - gxo[i] * b0) : gx[i] * a0; }
-    __device__ double g1(int i, long long sgn) const { return diff ? (double)sgn * (gx[i] * a1 - gxo[i] * b1) : gx[i] * a1; }
+    __device__ double g0(int i, long long sgn) const {
+        return diff ? (double)sgn * (self.at(i, 0, cpl) - other.at(i, 0, cpl)) : self.at(i, 0, cpl);
+    }
+    __device__ double g1(int i, long long sgn) const {
+        return diff ? (double)sgn * (self.at(i, 1, cpl) - other.at(i, 1, cpl)) : self.at(i, 1, cpl);
+    }
 };
 
 
@@ -988,11 +1133,43 @@ __global__ void __launch_bounds__(256) k_hyb_profiles(Collide C, int plane0) {
     const TaskGeom &G = C.geom[P.task];
     const HybridTask &H = C.hyb[P.task];
     if (G.green < 0 || !H.mode) return;
-    const int nx = C.o.nx, ny = C.o.ny, side = P.kind == 0 ? 0 : 1;
+    const int nx = C.o.nx, ny = C.o.ny, side = P.kind == 0 ? 0 : 1, L = nx + ny;
     const Grid sg = G.sg;
     const double hx = sg.w / (double)(nx - 1), hy = sg.h / (double)(ny - 1);
-    double *g = C.hprof + (long long)pl * (nx + ny);
-    for (int i = threadIdx.x; i < nx + ny; i += blockDim.x) {
+    double *g = C.hprof + (long long)pl * 3 * L;
+    if (H.mode == 2) {
+        // the tilted Gaussian to second order in lambda (gaussian_pic.jl:350-370, 597-630): x moments about mux
+        // (sigma sqrt(a)), the conditional y profile (sigma sigc) and its mean-derivatives
+        const double mux = H.mux[side], muy = H.muy[side], sa = H.sa[side], sc = H.sigc[side];
+        for (int i = threadIdx.x; i < L; i += blockDim.x) {
+            if (i < nx) {
+                const double xi = sg.x0 + (double)i * hx;
+                double W[3];
+                gauss_weighted_moments(C.o.method, xi, hx, mux, sa, W);
+                const double d = mux - xi;
+                g[i] = W[0];
+                g[L + i] = W[1] - d * W[0];
+                g[2 * L + i] = W[2] - 2.0 * d * W[1] + d * d * W[0];
+            } else {
+                const double yj = sg.y0 + (double)(i - nx) * hy;
+                g[i] = gauss_node_weight(C.o.method, yj, hy, muy, sc);
+                gauss_profile_derivs(C.o.method, yj, hy, muy, sc, g[L + i], g[2 * L + i]);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {  // sequential sums, node order; the subtracted grid's total mass
+            double s[6] = {0, 0, 0, 0, 0, 0};
+            for (int k = 0; k < 3; ++k) {
+                for (int i = 0; i < nx; ++i) s[2 * k] += g[k * L + i];
+                for (int j = 0; j < ny; ++j) s[2 * k + 1] += g[k * L + nx + j];
+            }
+            const double lam = H.lam[side], half_lam2 = 0.5 * lam * lam;
+            C.hsum[2 * pl] = s[0] * s[1] + lam * s[2] * s[3] + half_lam2 * s[4] * s[5];
+            C.hsum[2 * pl + 1] = 0.0;
+        }
+        return;
+    }
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
         if (i < nx) g[i] = gauss_node_weight(C.o.method, sg.x0 + (double)i * hx, hx, H.mux[side], H.sigx[side]);
         else g[i] = gauss_node_weight(C.o.method, sg.y0 + (double)(i - nx) * hy, hy, H.muy[side], H.sigy[side]);
     }
@@ -1673,7 +1850,32 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
                 Kz += tp.w[q] * (pl - pr);
             }
         }
-        if (HYB && J.hyb) {
+        if (HYB && J.hyb == 2) {
+            // Rotated add-back of the tilted Gaussian through _cp_covariance_kick at both boundaries, blended in z
+            // (gaussian_pic.jl:837-854)
+            const HybridTask &H = J.H;
+            const double kbb_eff = (double)ks * H.half_ns;
+            GMoments M{};
+            M.a0 = H.cov[0]; M.b0 = H.cov[1]; M.d0 = H.cov[2]; M.bxx = H.cov[3]; M.bxpy = H.cov[4];
+            M.bypx = H.cov[5]; M.bypy = H.cov[6]; M.qxx = H.cov[7]; M.qxy = H.cov[8]; M.qyy = H.cov[9];
+            double pxL = 0, pyL = 0, pzL = 0, pxR = 0, pyR = 0, pzR = 0, dens;
+            coupled_kick(M, kbb_eff, -H.s[0], (double)x - H.mux[0], (double)y - H.muy[0], pxL, pyL, pzL, dens);
+            coupled_kick(M, kbb_eff, -H.s[1], (double)x - H.mux[1], (double)y - H.muy[1], pxR, pyR, pzR, dens);
+            const double dpxa = (double)zL * pxL + (double)zR * pxR;
+            const double dpya = (double)zL * pyL + (double)zR * pyR;
+            px += (R)((double)ks * (double)Kx + dpxa);
+            py += (R)((double)ks * (double)Ky + dpya);
+            if (lk) {
+                if (kPrecision) {
+                    dpz += (R)((double)ks * (double)Kz * (double)J.hzi + ((double)zL * pzL + (double)zR * pzR) +
+                               0.5 * (dpxa * H.mpx + dpya * H.mpy));
+                } else {
+                    pz += ks * Kz * J.hzi;
+                    pz += (R)((double)zL * pzL + (double)zR * pzR);
+                    pz += (R)(0.5 * (dpxa * H.mpx + dpya * H.mpy));
+                }
+            }
+        } else if (HYB && J.hyb) {
             // Analytic add-back of the subtracted Gaussian (gaussian_pic.jl:851-884): half the slice population
             // times the Bassetti-Erskine kick at both boundaries, blended in z, and its longitudinal terms.
             const HybridTask &H = J.H;

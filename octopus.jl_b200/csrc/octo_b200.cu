@@ -447,6 +447,7 @@ int validate_options(const octo_pic_options &o, std::string &msg) {
             return OCTO_ERR_UNSUPPORTED;
         }
         if (!(o.margin_sigma >= 0.0)) { msg = "margin_sigma must be non-negative"; return OCTO_ERR_ARG; }
+        if (!(o.coupling_tol >= 0.0)) { msg = "coupling_tol must be non-negative (INFINITY: uncoupled)"; return OCTO_ERR_ARG; }
     }
     if (o.precision != 0 && o.precision != 1) {
         msg = "precision must be 0 (FP64 plain form) or 1 (FP32 precision form)";
@@ -1276,7 +1277,7 @@ void CollideJob::run() {
         c->hyb.ensure(std::max(ntasks, 1));
         c->hmom.ensure((size_t)std::max(ntasks, 1) * kMaxBoundBlocks * kMomentSums);
         c->qtot.ensure(max_planes);
-        c->hprof.ensure((size_t)max_planes * (nx + ny));
+        c->hprof.ensure((size_t)max_planes * 3 * (nx + ny));
         c->hsum.ensure((size_t)max_planes * 2);
         C.hyb = c->hyb.p;
         C.hmom = c->hmom.p;
@@ -1961,6 +1962,7 @@ octo_ctx *octo_create(int32_t device, const octo_pic_options *options) {
     d.gaussian = options->gaussian != 0;
     d.neutralize = options->neutralize != 0;
     d.margin = options->margin_sigma;
+    d.coupling_tol = options->coupling_tol;
     try {
         CK(cudaSetDevice(device));
         CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));

@@ -248,17 +248,24 @@ struct DevOptions {
     int dep_rotate;              // rotate each lane's deposit tap order (spatially ordered slices)
     double min_ex, min_ey, quantize, min_ratio, growth;
     double margin;               // hybrid: Gaussian containment half-width in sigmas
+    double coupling_tol;         // hybrid: |r_xy| above which the coupled subtraction runs (inf: never)
 };
 
 // Gaussian-subtracted hybrid state of one directed task (gaussian_pic.jl:604-705): the drifted reference
 // Gaussian of the source slice at the two boundaries of the field slice ([0]: sL, [1]: sR).
 struct HybridTask {
-    int32_t mode;  // 1: subtraction and analytic add-back; 0: plain PIC (degenerate moments)
+    int32_t mode;  // 0: plain PIC (degenerate moments); 1: uncoupled subtraction; 2: coupled (rotated) subtraction
     int32_t pad;
     double half_ns, mpx, mpy;
     double mux[2], muy[2], sigx[2], sigy[2], rx[2], ry[2];
+    // coupled (gaussian_pic.jl:493-523): per boundary the drift s, sqrt of the drifted var x, the conditional
+    // slope lambda = sigma_xy / sigma_x^2 and sigma sigc; the source's covariance for the rotated add-back
+    double s[2], sa[2], lam[2], sigc[2];
+    double cov[10];  // a0, b0, d0, bxx, bxpy, bypx, bypy, qxx, qxy, qyy (StrongTransverseMoments order)
 };
-constexpr int kMomentSums = 10;     // sums of dx, dpx, dy, dpy, dx^2, dpx^2, dy^2, dpy^2, dx dpx, dy dpy
+// sums of dx, dpx, dy, dpy, dx^2, dpx^2, dy^2, dpy^2, dx dpx, dy dpy and, when the coupled subtraction can
+// run (finite coupling_tol), the cross-plane dx dy, dx dpy, dy dpx, dpx dpy
+constexpr int kMomentSums = 14;
 constexpr int kMaxBoundBlocks = 128;  // blocks per slice of the bounds / moments passes
 
 }  // namespace octo

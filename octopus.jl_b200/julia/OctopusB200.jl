@@ -51,6 +51,7 @@ struct OctoPicOptions
     solver::Int32; gaussian_when_luminosity::Int32; ignore_centroid1::Int32; ignore_centroid2::Int32
     virtual_drift::Int32; include_sigma_xy::Int32; min_sigma::Float64
     resolution1::Int32; resolution2::Int32
+    coupling_tol::Float64
 end
 
 # include/octo_b200.h: octo_collide_report
@@ -74,7 +75,8 @@ B200PICPoissonSolver(; kwargs...) = B200PICPoissonSolver(PICPoissonSolver(; kwar
 """
     B200GaussianPICPoissonSolver(; margin_sigma=5.0, neutralize=true, coupling_tol=Inf, kwargs...)
 
-`GaussianPICPoissonSolver(; ...)` (gaussian_pic.jl:87-112) run on libocto_b200 (the uncoupled subtraction).
+`GaussianPICPoissonSolver(; ...)` (gaussian_pic.jl:87-112) run on libocto_b200: the uncoupled subtraction, or
+the coupled (rotated) one above a finite `coupling_tol`.
 """
 struct B200GaussianPICPoissonSolver{T<:Real} <: AbstractPoissonSolver
     gpic::GaussianPICPoissonSolver{T}
@@ -82,8 +84,6 @@ struct B200GaussianPICPoissonSolver{T<:Real} <: AbstractPoissonSolver
 end
 function B200GaussianPICPoissonSolver(; kwargs...)
     g = GaussianPICPoissonSolver(; kwargs...)
-    isfinite(g.coupling_tol) && throw(ArgumentError(
-        "coupling_tol < Inf (the coupled subtraction) is not implemented by the B200 backend"))
     return B200GaussianPICPoissonSolver(g, g.pic)
 end
 """
@@ -158,7 +158,7 @@ function _options(p::PICPoissonSolver, keep::Vector{Any}, precision::Integer=0, 
         Int32(soft === nothing ? 0 : soft.virtual_drift isa Octopus.ChromaticDrift ? 1 :
               soft.virtual_drift isa Octopus.ExactHamiltonianDrift ? 2 : 0),
         Int32(soft === nothing ? 0 : soft.include_sigma_xy), soft === nothing ? 0.0 : Float64(soft.min_sigma),
-        r1, r2)
+        r1, r2, gaussian === nothing ? Inf : Float64(gaussian.coupling_tol))
 end
 
 """Context: device workspaces and the slice-pair Green cache (the twin of task.runtime_cache)."""

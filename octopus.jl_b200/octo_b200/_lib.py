@@ -89,6 +89,7 @@ class OctoPicOptions(C.Structure):
         ("virtual_drift", C.c_int32), ("include_sigma_xy", C.c_int32),
         ("min_sigma", C.c_double),
         ("resolution1", C.c_int32), ("resolution2", C.c_int32),
+        ("coupling_tol", C.c_double),
     ]
 
 

@@ -181,6 +181,7 @@ class PICPoissonSolver:
         o.kbb2 = float(self.kbb2 or 0.0)
         o.lum_scale = float(self.luminosity_scale or 0.0)
         o.precision = 0
+        o.coupling_tol = math.inf  # read by the hybrid only
         o._keep = keep  # positions arrays must outlive octo_create
         return o
 
@@ -222,8 +223,9 @@ class GaussianPICPoissonSolver:
     (gaussian_pic.jl:87-112): a PICPoissonSolver built from the remaining keywords, whose slice-pair
     interactions subtract the drifted reference Gaussian of each source slice before the solve and add its
     Bassetti-Erskine kick back analytically.  The PIC options the hybrid does not read must keep their
-    defaults (gaussian_pic.jl:162-164); this backend implements the default uncoupled subtraction
-    (coupling_tol = Inf)."""
+    defaults (gaussian_pic.jl:162-164).  A finite coupling_tol subtracts the tilted (coupled) reference Gaussian of
+    slices whose drifted |r_xy| exceeds it and adds the rotated Bassetti-Erskine kick back (gaussian_pic.jl:240-372,
+    837-854); Inf, the default, always subtracts the separable Gaussian."""
 
     def __init__(self, margin_sigma: float = 5.0, neutralize: bool = True, coupling_tol: float = math.inf,
                  **kwargs):
@@ -262,13 +264,11 @@ class GaussianPICPoissonSolver:
             raise ArgumentError(
                 "GaussianPICPoissonSolver does not read slice_interpolation, interaction_grid or grid_extent: it "
                 "interpolates linearly on its own :slice_pair box (gaussian_pic.jl:162-164); keep their defaults.")
-        if math.isfinite(self.coupling_tol):
-            raise ArgumentError("coupling_tol < Inf (the coupled, rotated subtraction) is not implemented by this "
-                                "backend; use the default uncoupled subtraction.")
         o = p.to_c()
         o.gaussian = 1
         o.margin_sigma = self.margin_sigma
         o.neutralize = int(self.neutralize)
+        o.coupling_tol = self.coupling_tol
         return o
 
 

@@ -1191,7 +1191,8 @@ void interaction(Ctx &C, Workspace &ws, const Coords &source, const SliceParam &
 
 // pic_cpu.jl:1448-1538
 // ---------------------------------------------------------------- Gaussian-subtracted hybrid
-// GaussianPICPoissonSolver (gaussian_pic.jl), default uncoupled subtraction (coupling_tol = Inf).
+// GaussianPICPoissonSolver (gaussian_pic.jl): the uncoupled subtraction (coupling_tol = Inf, the default) and
+// the coupled (rotated) subtraction above a finite coupling_tol.
 
 // Node-centred erf-integrated profile of a unit 1D Gaussian against the CIC / TSC assignment function
 // (gaussian_pic.jl:206-237); node i sits at x0 + i h.
@@ -1219,23 +1220,165 @@ void gaussian_profile(int method, double x0, double h, double mu, double s, int 
     }
 }
 
+// Central moments c_k = int_A^B (x - mu)^k G(x) dx, k = 0..4, of the normalised Gaussian by the integration-
+// by-parts recursion (gaussian_pic.jl:274-287).
+void central_moments(double A, double B, double mu, double s, double c[5]) {
+    const double invroot = 1.0 / (s * std::sqrt(2.0));
+    const double norm = 1.0 / (s * std::sqrt(2.0 * be::kPi));
+    const double a = A - mu, b = B - mu;
+    const double GA = norm * std::exp(-(a * a) / (2.0 * s * s));
+    const double GB = norm * std::exp(-(b * b) / (2.0 * s * s));
+    const double s2 = s * s;
+    c[0] = 0.5 * (std::erf(b * invroot) - std::erf(a * invroot));
+    c[1] = -s2 * (GB - GA);
+    c[2] = -s2 * (b * GB - a * GA) + s2 * c[0];
+    c[3] = -s2 * (b * b * GB - a * a * GA) + 2.0 * s2 * c[1];
+    c[4] = -s2 * (b * b * b * GB - a * a * a * GA) + 3.0 * s2 * c[2];
+}
+// Node-centred moments about xi from the central ones, d = mu - xi (gaussian_pic.jl:291-299).
+void shift_moments(const double c[5], double d, double m[5]) {
+    const double d2 = d * d, d3 = d2 * d, d4 = d3 * d;
+    m[0] = c[0];
+    m[1] = c[1] + d * c[0];
+    m[2] = c[2] + 2.0 * d * c[1] + d2 * c[0];
+    m[3] = c[3] + 3.0 * d * c[2] + 3.0 * d2 * c[1] + d3 * c[0];
+    m[4] = c[4] + 4.0 * d * c[3] + 6.0 * d2 * c[2] + 4.0 * d3 * c[1] + d4 * c[0];
+}
+void cell_moments(double A, double B, double mu, double s, double xi, double m[5]) {
+    double c[5];
+    central_moments(A, B, mu, s, c);
+    shift_moments(c, mu - xi, m);
+}
+// Assignment-weighted moments W_k = int (x - xi)^k G W(x - xi) dx, k = 0, 1, 2 (gaussian_pic.jl:304-324).
+void weighted_moments(double xi, double h, double mu, double s, int method, double W[3]) {
+    if (method == 0) {
+        double L[5], R[5];
+        cell_moments(xi - h, xi, mu, s, xi, L);
+        cell_moments(xi, xi + h, mu, s, xi, R);
+        for (int k = 0; k < 3; ++k) W[k] = (L[k] + L[k + 1] / h) + (R[k] - R[k + 1] / h);
+        return;
+    }
+    const double half = h / 2.0;
+    double C[5], Lw[5], Rw[5];
+    cell_moments(xi - half, xi + half, mu, s, xi, C);
+    cell_moments(xi - 3.0 * half, xi - half, mu, s, xi, Lw);
+    cell_moments(xi + half, xi + 3.0 * half, mu, s, xi, Rw);
+    auto core = [&](const double *M, int k) { return 0.75 * M[k] - M[k + 2] / (h * h); };
+    auto wing = [&](const double *M, int k, double sgn) {
+        return 1.125 * M[k] + sgn * 1.5 * M[k + 1] / h + 0.5 * M[k + 2] / (h * h);
+    };
+    for (int k = 0; k < 3; ++k) W[k] = core(C, k) + wing(Lw, k, 1.0) + wing(Rw, k, -1.0);
+}
+// Mean-derivatives g' and g'' of the 1D node profile (gaussian_pic.jl:330-348).
+void profile_mean_derivs(double yj, double h, double mu, double s, int method, double &dg, double &ddg) {
+    const double invroot = 1.0 / (s * std::sqrt(2.0));
+    const double norm = 1.0 / (s * std::sqrt(2.0 * be::kPi));
+    auto pdf = [&](double y) { return norm * std::exp(-((y - mu) * (y - mu)) / (2.0 * s * s)); };
+    auto m0 = [&](double A, double B) { return 0.5 * (std::erf((B - mu) * invroot) - std::erf((A - mu) * invroot)); };
+    if (method == 0) {
+        dg = (m0(yj - h, yj) - m0(yj, yj + h)) / h;
+        ddg = (pdf(yj - h) - 2.0 * pdf(yj) + pdf(yj + h)) / h;
+        return;
+    }
+    const double half = h / 2.0;
+    double C[5], Lw[5], Rw[5];
+    cell_moments(yj - half, yj + half, mu, s, yj, C);
+    cell_moments(yj - 3.0 * half, yj - half, mu, s, yj, Lw);
+    cell_moments(yj + half, yj + 3.0 * half, mu, s, yj, Rw);
+    dg = -2.0 * C[1] / (h * h) + (1.5 * Lw[0] + Lw[1] / h) / h + (-1.5 * Rw[0] + Rw[1] / h) / h;
+    ddg = (-2.0 * m0(yj - half, yj + half) + m0(yj - 3.0 * half, yj - half) + m0(yj + half, yj + 3.0 * half)) / (h * h);
+}
+// The six node profiles of the coupled subtraction (gaussian_pic.jl:350-370): x moments about mux, the
+// conditional y profile (sigma = sigc) and its two mean-derivatives.
+void coupled_profiles(int method, double x0, double hx, double mux, double sigx, int nx, double y0, double hy,
+                      double muy, double sigc, int ny, double *gx, double *m1x, double *m2x, double *gy, double *dgy,
+                      double *ddgy) {
+    for (int i = 0; i < nx; ++i) {
+        const double xi = x0 + (double)i * hx;
+        double W[3];
+        weighted_moments(xi, hx, mux, sigx, method, W);
+        const double d = mux - xi;
+        gx[i] = W[0];
+        m1x[i] = W[1] - d * W[0];
+        m2x[i] = W[2] - 2.0 * d * W[1] + d * d * W[0];
+    }
+    gaussian_profile(method, y0, hy, muy, sigc, ny, gy);
+    for (int j = 0; j < ny; ++j) profile_mean_derivs(y0 + (double)j * hy, hy, muy, sigc, method, dgy[j], ddgy[j]);
+}
+
+// Full transverse covariance in StrongTransverseMoments order (strong_beam.jl:79-90).
+struct CovMoments {
+    double a0, b0, d0, bxx, bxpy, bypx, bypy, qxx, qxy, qyy;
+};
+// _cp_covariance_kick, coupled (strong_beam.jl:634-682): adds the kick of the covariance transported by S to
+// px, py and its pz terms to pz; returns the density at (xx, yy) (0 for a degenerate covariance).
+double coupled_covariance_kick(const CovMoments &m, double kbb, double S, double xx, double yy, double &px, double &py,
+                               double &pz) {
+    const double twopi_c = 6.283185307179586476925286766559005768394338;
+    const double a = m.a0 - 2 * S * m.bxx + S * S * m.qxx;
+    const double bb = m.b0 - S * (m.bxpy + m.bypx) + S * S * m.qxy;
+    const double d = m.d0 - 2 * S * m.bypy + S * S * m.qyy;
+    const double au = 2 * (m.bxx - S * m.qxx);
+    const double bu = m.bxpy + m.bypx - 2 * S * m.qxy;
+    const double du = 2 * (m.bypy - S * m.qyy);
+    const double detA = a * d - bb * bb;
+    if (a <= 0 || d <= 0 || detA <= 0) return 0.0;
+    const double adiff = a - d;
+    const double D = std::hypot(adiff, 2 * bb);
+    if (D == 0.0) {
+        const double sigma = std::sqrt((a + d) / 2);
+        const double expterm = std::exp(-0.5 * (xx * xx + yy * yy) / (sigma * sigma));
+        double Kx, Ky, Hxx, Hxy, Hyy;
+        be::round_kick_hessian(kbb, sigma, xx, yy, expterm, Kx, Ky, Hxx, Hxy, Hyy);
+        px += kbb * Kx;
+        py += kbb * Ky;
+        pz += 0.25 * (Hxx * au + 2 * Hxy * bu + Hyy * du);
+        return expterm / (twopi_c * sigma * sigma);
+    }
+    const double theta = 0.5 * std::atan2(2 * bb, a - d);
+    const double c = std::cos(theta), sn = std::sin(theta);
+    const double lambda1 = (a + d + D) / 2, lambda2 = (a + d - D) / 2;
+    const double sig1 = std::sqrt(lambda1), sig2 = std::sqrt(lambda2);
+    const double xh = c * xx + sn * yy, yh = -sn * xx + c * yy;
+    const double eta = D / (a + d);
+    double inner, outer;
+    be::eta_bounds(inner, outer);
+    double Kxh, Kyh, H11, H22, LoD;
+    if (eta <= inner) be::near_round_series(kbb, (a + d) / 2, eta, xh, yh, Kxh, Kyh, H11, H22, &LoD);
+    else be::response_principal(kbb, sig1, sig2, xh, yh, Kxh, Kyh, H11, H22, &LoD);
+    const double expterm = std::exp(-0.5 * (xh * xh / lambda1 + yh * yh / lambda2));
+    const double Fxh = kbb * Kxh, Fyh = kbb * Kyh;
+    px += c * Fxh - sn * Fyh;
+    py += sn * Fxh + c * Fyh;
+    const double Du = (adiff * (au - du) + 4 * bb * bu) / D;
+    const double traceu = au + du;
+    pz += 0.125 * ((H11 + H22) * traceu + (H11 - H22) * Du);
+    const double rotation_projection = (adiff * bu - bb * (au - du)) / D;
+    pz -= 0.5 * kbb * rotation_projection * LoD;
+    return expterm / (twopi_c * sig1 * sig2);
+}
+
 // Transverse moments of the source slice from sums relative to its first particle (gaussian_pic.jl:432-486).
+// coupled: also the four cross-plane sums (only the coupled subtraction reads them).
 struct SourceMoments {
     int64_t n;
     double mx, mpx, varx, cxpx, varpx, my, mpy, vary, cypy, varpy;
+    double cxy, cxpy, cypx, cpxpy;
 };
-SourceMoments source_moments(const Coords &s) {
+SourceMoments source_moments(const Coords &s, bool coupled = false) {
     SourceMoments m{};
     const size_t n = s.size();
     m.n = (int64_t)n;
     const double x0 = s.x[0], px0 = s.px[0], y0 = s.y[0], py0 = s.py[0];
     double sx = 0, spx = 0, sy = 0, spy = 0, sxx = 0, spxpx = 0, syy = 0, spypy = 0, sxpx = 0, sypy = 0;
+    double sxy = 0, sxpy = 0, sypx = 0, spxpy = 0;
     for (size_t i = 0; i < n; ++i) {
         const double dx = s.x[i] - x0, dpx = s.px[i] - px0, dy = s.y[i] - y0, dpy = s.py[i] - py0;
         sx += dx; spx += dpx; sy += dy; spy += dpy;
         sxx += dx * dx; spxpx += dpx * dpx;
         syy += dy * dy; spypy += dpy * dpy;
         sxpx += dx * dpx; sypy += dy * dpy;
+        if (coupled) { sxy += dx * dy; sxpy += dx * dpy; sypx += dy * dpx; spxpy += dpx * dpy; }
     }
     const double invn = 1.0 / (double)n;
     const double dmx = sx * invn, dmpx = spx * invn, dmy = sy * invn, dmpy = spy * invn;
@@ -1247,14 +1390,27 @@ SourceMoments source_moments(const Coords &s) {
     m.varpx = jmax(std::fma(-dmpx, dmpx, spxpx * invn), 0.0);
     m.cypy = std::fma(-dmy, dmpy, sypy * invn);
     m.varpy = jmax(std::fma(-dmpy, dmpy, spypy * invn), 0.0);
+    if (coupled) {
+        m.cxy = std::fma(-dmx, dmy, sxy * invn);
+        m.cxpy = std::fma(-dmx, dmpy, sxpy * invn);
+        m.cypx = std::fma(-dmy, dmpx, sypx * invn);
+        m.cpxpy = std::fma(-dmpx, dmpy, spxpy * invn);
+    }
     return m;
+}
+CovMoments coupled_moments(const SourceMoments &m) {  // _gpic_coupled_moments (gaussian_pic.jl:436-447)
+    return CovMoments{m.varx, m.cxy, m.vary, m.cxpx, m.cxpy, m.cypx, m.cypy, m.varpx, m.cpxpy, m.varpy};
 }
 
 // Drifted reference Gaussian at a slice boundary (gaussian_pic.jl:496-540, uncoupled).
+// coupled: also the drifted covariance (a, b, d), its correlation, whether it is resolved (full rank to the
+// precision-derived tolerance), the conditional slope lambda = b / a and sigma sigc (gaussian_pic.jl:456-523).
 struct Boundary {
     double mux, muy, sigx, sigy, rx, ry, s;
+    double a, b, d, rxy, lam, sigc;
+    bool resolved;
 };
-Boundary boundary(const SourceMoments &m, double s) {
+Boundary boundary(const SourceMoments &m, double s, bool coupled = false) {
     Boundary b{};
     b.s = s;
     b.mux = m.mx + m.mpx * s;
@@ -1265,17 +1421,41 @@ Boundary boundary(const SourceMoments &m, double s) {
     b.sigy = std::sqrt(jmax(vary, 0.0));
     b.rx = 2.0 * (m.cxpx + s * m.varpx);
     b.ry = 2.0 * (m.cypy + s * m.varpy);
+    if (!coupled) return b;
+    const CovMoments c = coupled_moments(m);
+    const double S = -s;  // _transport_transverse_moments with the field-particle convention
+    b.a = c.a0 - 2 * S * c.bxx + S * S * c.qxx;
+    b.b = c.b0 - S * (c.bxpy + c.bypx) + S * S * c.qxy;
+    b.d = c.d0 - 2 * S * c.bypy + S * S * c.qyy;
+    b.rxy = (b.a <= 0 || b.d <= 0) ? 0.0 : (b.b / std::sqrt(b.a)) / std::sqrt(b.d);
+    bool ok = std::isfinite(b.a) && std::isfinite(b.b) && std::isfinite(b.d) && b.a > 0 && b.d > 0;
+    if (ok) {
+        const double rho = (b.b / std::sqrt(b.a)) / std::sqrt(b.d);
+        ok = std::isfinite(rho) && std::fma(-rho, rho, 1.0) > std::sqrt(2.220446049250313e-16);
+    }
+    b.resolved = ok;
+    b.lam = ok ? b.b / b.a : 0.0;
+    const double rcv = ok ? jmax(std::fma(-b.rxy, b.rxy, 1.0), 0.0) : 0.0;
+    b.sigc = ok ? std::sqrt(b.d * rcv) : 0.0;
     return b;
 }
 
-bool boundary_resolved(int64_t n, const Boundary &L, const Boundary &R) {  // gaussian_pic.jl:542-553
+bool boundary_resolved(int64_t n, const Boundary &L, const Boundary &R) {  // gaussian_pic.jl:525-530
     return n >= 2 && std::isfinite(L.sigx) && std::isfinite(L.sigy) && std::isfinite(R.sigx) &&
            std::isfinite(R.sigy) && L.sigx > 0 && L.sigy > 0 && R.sigx > 0 && R.sigy > 0;
 }
+// _gpic_control_variate_mode (gaussian_pic.jl:525-536): 0 plain PIC, 1 uncoupled, 2 coupled.
+int control_variate_mode(int64_t n, double tol, const Boundary &L, const Boundary &R) {
+    if (!boundary_resolved(n, L, R)) return 0;
+    const bool requested = std::isfinite(tol) && jmax(std::fabs(L.rxy), std::fabs(R.rxy)) > tol;
+    if (!requested) return 1;
+    return L.resolved && R.resolved ? 2 : 0;
+}
 
-// Deposit, subtract the (neutralised) erf-integrated reference Gaussian, solve (gaussian_pic.jl:559-597).
+// Deposit, subtract the (neutralised) erf-integrated reference Gaussian -- separable, or the tilted one as three
+// outer products when coupled -- and solve (gaussian_pic.jl:559-640).
 void solve_drifted_gaussian(const Options &O, Workspace &ws, FieldPlanes &fp, const Coords &src, double s,
-                            const Grid &sg, const std::vector<cplx> &gfft, const Boundary &b) {
+                            const Grid &sg, const std::vector<cplx> &gfft, const Boundary &b, bool coupled) {
     const int nx = O.o.nx, ny = O.o.ny;
     const double hx = sg.width / (double)(nx - 1), hy = sg.height / (double)(ny - 1);
     std::fill(ws.charge.begin(), ws.charge.end(), 0.0);
@@ -1283,19 +1463,33 @@ void solve_drifted_gaussian(const Options &O, Workspace &ws, FieldPlanes &fp, co
                  src.py.data(), (int64_t)src.size(), true, s, sg.x0, sg.y0, hx, hy, nx, ny,
                  O.o.fixed_point_deposit != 0, nullptr);
     std::vector<double> gx(nx), gy(ny);
-    gaussian_profile(O.o.deposit_method, sg.x0, hx, b.mux, b.sigx, nx, gx.data());
-    gaussian_profile(O.o.deposit_method, sg.y0, hy, b.muy, b.sigy, ny, gy.data());
-    double sgx = 0, sgy = 0;
-    for (double v : gx) sgx += v;
-    for (double v : gy) sgy += v;
     double qsum = 0;
     for (int j = 0; j < ny; ++j)
         for (int i = 0; i < nx; ++i) qsum += ws.charge[i + (size_t)j * 2 * nx];
-    double amp = (double)src.size();
-    if (O.o.neutralize && sgx * sgy > 0.0) amp = qsum / (sgx * sgy);
-    for (int j = 0; j < ny; ++j) {
-        const double gj = amp * gy[j];
-        for (int i = 0; i < nx; ++i) ws.charge[i + (size_t)j * 2 * nx] -= gx[i] * gj;
+    if (coupled) {  // the tilted Gaussian to second order in lambda (gaussian_pic.jl:597-630)
+        std::vector<double> m1x(nx), m2x(nx), dgy(ny), ddgy(ny);
+        coupled_profiles(O.o.deposit_method, sg.x0, hx, b.mux, std::sqrt(b.a), nx, sg.y0, hy, b.muy, b.sigc, ny,
+                         gx.data(), m1x.data(), m2x.data(), gy.data(), dgy.data(), ddgy.data());
+        const double lam = b.lam, half_lam2 = 0.5 * lam * lam;
+        auto sum = [](const std::vector<double> &v) { double t = 0; for (double e : v) t += e; return t; };
+        const double sgm = sum(gx) * sum(gy) + lam * sum(m1x) * sum(dgy) + half_lam2 * sum(m2x) * sum(ddgy);
+        const double amp = (O.o.neutralize && sgm != 0.0) ? qsum / sgm : (double)src.size();
+        for (int j = 0; j < ny; ++j) {
+            const double gj = amp * gy[j], dj = amp * lam * dgy[j], ddj = amp * half_lam2 * ddgy[j];
+            for (int i = 0; i < nx; ++i) ws.charge[i + (size_t)j * 2 * nx] -= gx[i] * gj + m1x[i] * dj + m2x[i] * ddj;
+        }
+    } else {
+        gaussian_profile(O.o.deposit_method, sg.x0, hx, b.mux, b.sigx, nx, gx.data());
+        gaussian_profile(O.o.deposit_method, sg.y0, hy, b.muy, b.sigy, ny, gy.data());
+        double sgx = 0, sgy = 0;
+        for (double v : gx) sgx += v;
+        for (double v : gy) sgy += v;
+        double amp = (double)src.size();
+        if (O.o.neutralize && sgx * sgy > 0.0) amp = qsum / (sgx * sgy);
+        for (int j = 0; j < ny; ++j) {
+            const double gj = amp * gy[j];
+            for (int i = 0; i < nx; ++i) ws.charge[i + (size_t)j * 2 * nx] -= gx[i] * gj;
+        }
     }
     for (size_t k = 0; k < ws.charge.size(); ++k) ws.spectral[k] = cplx(ws.charge[k], 0.0);
     ws.fft.run(ws.spectral.data(), false);
@@ -1314,12 +1508,16 @@ void interaction_gaussian(Ctx &C, Workspace &ws, const Coords &source, const Sli
     const int nsource = (int)source.size(), nfield = (int)field.size();
     const double sL = 0.5 * (ps.center - pf.lb);
     const double sR = 0.5 * (ps.center - pf.rb);
-    const SourceMoments mom = source_moments(source);
-    const Boundary bL = boundary(mom, sL), bR = boundary(mom, sR);
-    if (!boundary_resolved(mom.n, bL, bR)) {
+    const bool gate = std::isfinite(O.o.coupling_tol);  // the cross-plane sums only when they can be read
+    const SourceMoments mom = source_moments(source, gate);
+    const Boundary bL = boundary(mom, sL, gate), bR = boundary(mom, sR, gate);
+    const int mode = control_variate_mode(mom.n, O.o.coupling_tol, bL, bR);
+    if (mode == 0) {
         interaction(C, ws, source, ps, field, pf, kbb, i, j, dir, vslot, counters);
         return;
     }
+    const bool use_coupled = mode == 2;
+    const CovMoments cmom = coupled_moments(mom);
     const double margin = O.o.margin_sigma;
     double sxl = source.x[0] + source.px[0] * sL, syl = source.y[0] + source.py[0] * sL;
     double sxr = source.x[0] + source.px[0] * sR, syr = source.y[0] + source.py[0] * sR;
@@ -1360,8 +1558,8 @@ void interaction_gaussian(Ctx &C, Workspace &ws, const Coords &source, const Sli
     Bounds sb{sxmin, sxmax, symin, symax}, fb{fxmin, fxmax, fymin, fymax};
     std::vector<cplx> own;
     const std::vector<cplx> &gfft = slice_pair_green(C, ws, i, j, dir, sg, fg, sb, fb, own, counters);
-    solve_drifted_gaussian(O, ws, ws.left, source, sL, sg, gfft, bL);
-    solve_drifted_gaussian(O, ws, ws.right, source, sR, sg, gfft, bR);
+    solve_drifted_gaussian(O, ws, ws.left, source, sL, sg, gfft, bL, use_coupled);
+    solve_drifted_gaussian(O, ws, ws.right, source, sR, sg, gfft, bR, use_coupled);
 
     const double ks = 2.0 * kbb;
     const double half_ns = 0.5 * (double)nsource;
@@ -1374,6 +1572,25 @@ void interaction_gaussian(Ctx &C, Workspace &ws, const Coords &source, const Sli
         const double zR = 1.0 - zL;
         double Kxd, Kyd, Kzd;
         interpolate_kick(O, fg, x, y, ws.left, ws.right, zL, zR, Kxd, Kyd, Kzd);
+        if (use_coupled) {  // rotated analytic add-back through _cp_covariance_kick (gaussian_pic.jl:837-854)
+            double pxL = 0, pyL = 0, pzL = 0, pxR = 0, pyR = 0, pzR = 0;
+            coupled_covariance_kick(cmom, kbb_eff, -bL.s, x - bL.mux, y - bL.muy, pxL, pyL, pzL);
+            coupled_covariance_kick(cmom, kbb_eff, -bR.s, x - bR.mux, y - bR.muy, pxR, pyR, pzR);
+            const double dpxa = zL * pxL + zR * pxR;
+            const double dpya = zL * pyL + zR * pyR;
+            field.px[k] += ks * Kxd + dpxa;
+            field.py[k] += ks * Kyd + dpya;
+            if (lk) {
+                field.pz[k] += ks * Kzd * hzi;
+                field.pz[k] += zL * pzL + zR * pzR;
+                field.pz[k] += 0.5 * (dpxa * mom.mpx + dpya * mom.mpy);
+            }
+            const double s = 0.5 * (ps.center - field.z[k]);
+            field.x[k] += s * field.px[k];
+            field.y[k] += s * field.py[k];
+            if (lk) field.pz[k] += 0.25 * (field.px[k] * field.px[k] + field.py[k] * field.py[k]);
+            continue;
+        }
         double bLx, bLy, HxL = 0, HyL = 0, bRx, bRy, HxR = 0, HyR = 0;
         if (lk) {
             be::response(kbb_eff, bL.sigx, bL.sigy, x - bL.mux, y - bL.muy, bLx, bLy, HxL, HyL);
@@ -1563,6 +1780,7 @@ void validate(const Options &O) {
         throw OracleError(OO_ERR_UNSUPPORTED, "GaussianPICPoissonSolver needs linear slice interpolation on the "
                                               ":slice_pair grid with grid_extent = :extrema");
     if (o.gaussian && !(o.margin_sigma >= 0)) throw OracleError(OO_ERR_ARG, "margin_sigma must be non-negative");
+    if (o.gaussian && !(o.coupling_tol >= 0)) throw OracleError(OO_ERR_ARG, "coupling_tol must be non-negative");
 }
 
 int nslices_of(const oo_options &o, int which) {
@@ -2359,50 +2577,8 @@ double apply_one(double *const b[6], int64_t i, const SoftMoments &m, double cen
     const double px0 = px, py0 = py, pz0 = pz;
     const double twopi_c = 6.283185307179586476925286766559005768394338;
     if (g_coupled) {  // _cp_covariance_kick, coupled (strong_beam.jl:634-682)
-        double density = 0.0;
-        const double a = m.a0 - 2 * S * m.bxx + S * S * m.qxx;
-        const double bb = m.b0 - S * (m.bxpy + m.bypx) + S * S * m.qxy;
-        const double d = m.d0 - 2 * S * m.bypy + S * S * m.qyy;
-        const double au = 2 * (m.bxx - S * m.qxx);
-        const double bu = m.bxpy + m.bypx - 2 * S * m.qxy;
-        const double du = 2 * (m.bypy - S * m.qyy);
-        const double detA = a * d - bb * bb;
-        if (!(a <= 0 || d <= 0 || detA <= 0)) {
-            const double adiff = a - d;
-            const double D = std::hypot(adiff, 2 * bb);
-            if (D == 0.0) {
-                const double sigma = std::sqrt((a + d) / 2);
-                const double expterm = std::exp(-0.5 * (xx * xx + yy * yy) / (sigma * sigma));
-                double Kx, Ky, Hxx, Hxy, Hyy;
-                be::round_kick_hessian(kbb, sigma, xx, yy, expterm, Kx, Ky, Hxx, Hxy, Hyy);
-                px += kbb * Kx;
-                py += kbb * Ky;
-                pz += 0.25 * (Hxx * au + 2 * Hxy * bu + Hyy * du);
-                density = expterm / (twopi_c * sigma * sigma);
-            } else {
-                const double theta = 0.5 * std::atan2(2 * bb, a - d);
-                const double c = std::cos(theta), sn = std::sin(theta);
-                const double lambda1 = (a + d + D) / 2, lambda2 = (a + d - D) / 2;
-                const double sig1 = std::sqrt(lambda1), sig2 = std::sqrt(lambda2);
-                const double xh = c * xx + sn * yy, yh = -sn * xx + c * yy;
-                const double eta = D / (a + d);
-                double inner, outer;
-                be::eta_bounds(inner, outer);
-                double Kxh, Kyh, H11, H22, LoD;
-                if (eta <= inner) be::near_round_series(kbb, (a + d) / 2, eta, xh, yh, Kxh, Kyh, H11, H22, &LoD);
-                else be::response_principal(kbb, sig1, sig2, xh, yh, Kxh, Kyh, H11, H22, &LoD);
-                const double expterm = std::exp(-0.5 * (xh * xh / lambda1 + yh * yh / lambda2));
-                const double Fxh = kbb * Kxh, Fyh = kbb * Kyh;
-                px += c * Fxh - sn * Fyh;
-                py += sn * Fxh + c * Fyh;
-                const double Du = (adiff * (au - du) + 4 * bb * bu) / D;
-                const double traceu = au + du;
-                pz += 0.125 * ((H11 + H22) * traceu + (H11 - H22) * Du);
-                const double rotation_projection = (adiff * bu - bb * (au - du)) / D;
-                pz -= 0.5 * kbb * rotation_projection * LoD;
-                density = expterm / (twopi_c * sig1 * sig2);
-            }
-        }
+        const CovMoments cm{m.a0, m.b0, m.d0, m.bxx, m.bxpy, m.bypx, m.bypy, m.qxx, m.qxy, m.qyy};
+        const double density = coupled_covariance_kick(cm, kbb, S, xx, yy, px, py, pz);
         if (lk) pz += 0.5 * ((px - px0) * m.mpx + (py - py0) * m.mpy);
         else pz = pz0;
         reverse_drift(g_drift_kind, lk, x, px, y, py, z, pz, center);

@@ -61,6 +61,7 @@ typedef struct {
     int32_t neutralize;                /* hybrid: rescale the subtracted Gaussian to the deposited charge */
     double margin_sigma;               /* hybrid: adaptive-box half-width in beam sigmas */
     int32_t resolution1, resolution2;  /* :equal_area histogram bins per slice (LongitudinalSlicing resolution) */
+    double coupling_tol;               /* hybrid: |r_xy| above which the coupled (rotated) subtraction runs; inf = never */
 } oo_options;
 
 typedef struct { double charge, mc2, E0, r0, npart; } oo_beam_params;

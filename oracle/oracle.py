@@ -64,6 +64,7 @@ class OOOptions(C.Structure):
         ("gaussian", C.c_int32), ("neutralize", C.c_int32),
         ("margin_sigma", C.c_double),
         ("resolution1", C.c_int32), ("resolution2", C.c_int32),
+        ("coupling_tol", C.c_double),
     ]
 
 
@@ -205,6 +206,7 @@ class OracleOptions:
     margin_sigma: float = 5.0
     resolution1: int = 100
     resolution2: int = 100
+    coupling_tol: float = float("inf")  # hybrid: coupled (rotated) subtraction above this |r_xy|
 
     def to_c(self) -> OOOptions:
         o = OOOptions()
@@ -247,6 +249,7 @@ class OracleOptions:
         o.neutralize = int(bool(self.neutralize))
         o.margin_sigma = float(self.margin_sigma)
         o.resolution1, o.resolution2 = int(self.resolution1), int(self.resolution2)
+        o.coupling_tol = float(self.coupling_tol)
         return o
 
 

@@ -47,10 +47,19 @@ def oracle_options(solver, nthreads=8, fixed=False):
         kbb1=solver.kbb1, kbb2=solver.kbb2, luminosity_scale=solver.luminosity_scale,
         fixed_point_deposit=fixed, nthreads=nthreads,
         gaussian=hasattr(solver, "margin_sigma"), neutralize=getattr(solver, "neutralize", True),
-        margin_sigma=getattr(solver, "margin_sigma", 5.0))
+        margin_sigma=getattr(solver, "margin_sigma", 5.0), coupling_tol=getattr(solver, "coupling_tol", float("inf")))
 
 
 def within(a, b, atol, rtol):
     """max over elements of |a-b| / (atol + rtol*|b|): <= 1 passes (isapprox per element)."""
     a = np.asarray(a); b = np.asarray(b)
     return float(np.max(np.abs(a - b) / (atol + rtol * np.abs(b))))
+
+
+def tilt(b, angle):
+    """Rotate a beam's transverse plane, (x, y) and (px, py), by `angle` in place: an x-y coupled beam."""
+    c, s = np.cos(angle), np.sin(angle)
+    x, px, y, py = b[0].copy(), b[1].copy(), b[2].copy(), b[3].copy()
+    b[0], b[2] = c * x - s * y, s * x + c * y
+    b[1], b[3] = c * px - s * py, s * px + c * py
+    return b

@@ -26,10 +26,12 @@ def _device_beams(ob, e, p):
     return be, bp
 
 
-def run_both(solver, n1, n2, turns=1, e_sigma=None, p_sigma=None, seed=123456789):
+def run_both(solver, n1, n2, turns=1, e_sigma=None, p_sigma=None, seed=123456789, transform=None):
     from oracle import oracle as orc
     ob = _gpu()
     e, p = beams(n1, n2, e_sigma, p_sigma, seed=seed)
+    if transform is not None:
+        e, p = transform(e), transform(p)
     be, bp = _device_beams(ob, e, p)
     rt = ob.StrongStrongRuntime()
     ctx = rt.context("ip", solver, 0)
@@ -209,3 +211,37 @@ def test_gaussian_hybrid_near_round_regimes(c):
     assert abs(lum_g / lum_o - 1) <= 1e-10
     assert within(be.numpy(), e, ATOL, RTOL) <= 1.0 and within(bp.numpy(), p, ATOL, RTOL) <= 1.0
     rt.close()
+
+
+@pytest.mark.parametrize("opts", [
+    dict(),
+    dict(deposit_method="TSC", field_derivative="fourth"),
+    dict(neutralize=False, margin_sigma=0.0, green_cache="none", grid=(48, 48)),
+])
+def test_gaussian_hybrid_coupled(opts):
+    """The coupled (rotated) subtraction of a finite coupling_tol (gaussian_pic.jl:240-372, 593-640, 837-854) on
+    beams tilted by 0.05 rad (|r_xy| ~ 0.5 > coupling_tol, so every interaction runs it) against the oracle."""
+    from helpers import tilt
+    ob = _gpu()
+    kw = dict(grid=(64, 64), slicing=ob.LongitudinalSlicing(nslices=4, method="normal_quantile"), coupling_tol=0.01)
+    kw.update(opts)
+    s = ob.GaussianPICPoissonSolver(**kw)
+    check(run_both(s, 6000, 4000, turns=2, e_sigma=(95e-6, 8.5e-6, 7e-3), p_sigma=(95e-6, 8.5e-6, 6e-2),
+                   transform=lambda b: tilt(b, 0.05)))
+
+
+def test_gaussian_hybrid_coupled_rank_deficient_falls_back():
+    """y = 0.3 x, py = 0.3 px: the coupled covariance is rank-deficient, so the interactions run plain PIC
+    (gaussian_pic.jl:525-536) on the device as in the oracle.  One slice per beam: both directions of the one pair
+    read the pre-pair sources.  (With more slices the kicks break the proportionality, and a later source whose
+    1 - r_xy^2 is just above the sqrt(eps) threshold takes the coupled path with a conditional sigma near zero --
+    ill-conditioned in the reference algorithm itself.)"""
+    def corr(b):
+        b[2] = 0.3 * b[0]
+        b[3] = 0.3 * b[1]
+        return b
+    ob = _gpu()
+    s = ob.GaussianPICPoissonSolver(grid=(48, 48), slicing=ob.LongitudinalSlicing(nslices=1, method="normal_quantile"),
+                                    coupling_tol=0.5)
+    check(run_both(s, 5000, 4000, turns=1, e_sigma=(95e-6, 8.5e-6, 7e-3), p_sigma=(95e-6, 8.5e-6, 6e-2),
+                   transform=corr))

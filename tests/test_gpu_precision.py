@@ -30,11 +30,13 @@ def _params(ob):
     return pe, pp
 
 
-def run_precision(solver, n1, n2, turns=2, e_sigma=None, p_sigma=None, seed=123456789):
+def run_precision(solver, n1, n2, turns=2, e_sigma=None, p_sigma=None, seed=123456789, transform=None):
     kicks = {"e": solver.resolved_slicing2.nslices, "p": solver.resolved_slicing1.nslices}
     import octo_b200 as ob
     from oracle import oracle as orc
     e, p = beams(n1, n2, e_sigma, p_sigma, seed=seed)
+    if transform is not None:
+        e, p = transform(e), transform(p)
     e = e.astype(np.float32).astype(np.float64)
     p = p.astype(np.float32).astype(np.float64)
     pe, pp = _params(ob)
@@ -157,3 +159,13 @@ def test_precision_form_gaussian_hybrid(opts):
     kw.update(opts)
     s = ob.GaussianPICPoissonSolver(**kw)
     check(run_precision(s, 6000, 4000, e_sigma=(95e-6, 8.5e-6, 7e-3), p_sigma=(95e-6, 8.5e-6, 6e-2)))
+
+
+def test_precision_form_gaussian_hybrid_coupled():
+    """The coupled (rotated) subtraction in the precision form on beams tilted by 0.05 rad."""
+    import octo_b200 as ob
+    from helpers import tilt
+    s = ob.GaussianPICPoissonSolver(grid=(64, 64), slicing=ob.LongitudinalSlicing(nslices=4, method="normal_quantile"),
+                                    coupling_tol=0.01)
+    check(run_precision(s, 6000, 4000, e_sigma=(95e-6, 8.5e-6, 7e-3), p_sigma=(95e-6, 8.5e-6, 6e-2),
+                        transform=lambda b: tilt(b, 0.05)))

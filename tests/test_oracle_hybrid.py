@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 from scipy.special import wofz
 
-from helpers import beams, oracle_params
+from helpers import beams, oracle_params, tilt
 from oracle import oracle as orc
 from octo_b200.diagnostics import bassetti_erskine
 
@@ -85,3 +85,46 @@ def test_hybrid_rejects_options_it_does_not_read():
     for kw in (dict(slice_interpolation="quadratic"), dict(interaction_grid="node")):
         with pytest.raises(orc.OracleErrorPy):
             _collide(orc.OracleOptions(grid=(32, 32), gaussian=True, **kw), e, p)
+
+
+def test_coupled_subtraction_beats_uncoupled_on_tilted_beams():
+    """coupling_tol finite: the tilted reference Gaussian (conditional expansion to second order in
+    lambda = sigma_xy / sigma_x^2, gaussian_pic.jl:240-372) and the rotated Bassetti-Erskine add-back
+    (_cp_covariance_kick).  On a coarse grid and beams tilted by 0.3 rad its kicks are closer to a fine-grid
+    plain-PIC solution than the uncoupled subtraction's.  Beams tilted by 0.05 rad (|r_xy| ~ 0.5 for the 11:1
+    flat beams; lambda sigma_x / sigma_c ~ 0.5, inside the expansion's range): the uncoupled subtraction leaves
+    the tilt to the coarse grid and its vertical kicks degrade; the coupled one removes most of that."""
+    e, p = beams(20000, 20000, (95e-6, 8.5e-6, 7e-3), (95e-6, 8.5e-6, 6e-2))
+    e, p = tilt(e, 0.05), tilt(p, 0.05)
+    kw = dict(nslices1=3, nslices2=3, nthreads=8)
+    fine, _, _ = _collide(orc.OracleOptions(grid=(256, 256), **kw), e, p)
+    unc, _, _ = _collide(orc.OracleOptions(grid=(32, 32), gaussian=True, **kw), e, p)
+    cpl, _, lum = _collide(orc.OracleOptions(grid=(32, 32), gaussian=True, coupling_tol=0.01, **kw), e, p)
+    err = {row: (np.sqrt(np.mean((unc[row] - fine[row]) ** 2)), np.sqrt(np.mean((cpl[row] - fine[row]) ** 2)))
+           for row in (1, 3)}
+    assert err[3][1] < 0.75 * err[3][0], err  # py: the coupled subtraction removes the tilt's error
+    assert err[1][1] <= 1.0 * err[1][0], err  # px: no worse
+    assert np.isfinite(lum) and np.all(np.isfinite(cpl))
+
+
+def test_coupled_tolerance_above_the_correlation_keeps_the_uncoupled_subtraction():
+    """|r_xy| below coupling_tol at both boundaries: the uncoupled subtraction runs, bit for bit."""
+    e, p = beams(4000, 4000, (95e-6, 8.5e-6, 7e-3), (95e-6, 8.5e-6, 6e-2))
+    kw = dict(grid=(32, 32), nslices1=2, nslices2=2, gaussian=True)
+    a = _collide(orc.OracleOptions(**kw), e, p)
+    b = _collide(orc.OracleOptions(coupling_tol=0.99, **kw), e, p)
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+    assert a[2] == b[2]
+
+
+def test_coupled_rank_deficient_source_falls_back_to_plain_pic():
+    """y = 0.3 x, py = 0.3 px: |r_xy| = 1, the coupled covariance is rank-deficient, so the interaction runs
+    plain PIC (gaussian_pic.jl:525-536) and the kicks it gives equal the plain PIC collide's exactly."""
+    e, p = beams(2000, 2000)
+    e[2] = 0.3 * e[0]
+    e[3] = 0.3 * e[1]
+    kw = dict(grid=(32, 32), nslices1=1, nslices2=1)
+    pe1, pp1, l1 = _collide(orc.OracleOptions(gaussian=True, coupling_tol=0.5, **kw), e, p)
+    pe2, pp2, l2 = _collide(orc.OracleOptions(**kw), e, p)
+    np.testing.assert_array_equal(pp1, pp2)
