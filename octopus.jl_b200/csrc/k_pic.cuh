@@ -50,6 +50,8 @@ struct Collide {           // device pointers for one collide (passed by value)
     HybridTask *hyb;             // [task]
     double *hmom;                // [task][kMaxBoundBlocks][kMomentSums] block partial moment sums
     unsigned long long *qtot;    // [plane-in-front] total fixed-point charge of the plane (two's complement)
+    double *esum;                // grid_extent = :sigma: [task][kMaxBoundBlocks][8] block partial sums of the drifted
+                                 // source (x, x^2, y, y^2 over both drifts) and field (x, x^2, y, y^2) offsets
     double *hprof;               // [plane-in-front][3][nx + ny] reference-Gaussian node profiles (gx | gy, then the
                                  // coupled subtraction's m1x | dgy and m2x | ddgy)
     double *hsum;                // [plane-in-front][2] profile sums
@@ -96,6 +98,43 @@ __global__ void __launch_bounds__(256) k_pair_bounds(Collide C, int task0) {
     bool nan_s = false, nan_f = false, nan_l = false;
     const R *X = col<R>(S, 0) + st, *PX = col<R>(S, 1) + st, *Y = col<R>(S, 2) + st, *PY = col<R>(S, 3) + st,
             *Z = col<R>(S, 4) + st;
+    if (C.o.grid_extent) {
+        // grid_extent = :sigma (pic_cpu.jl:954-1010): FP64 sums of the drifted offsets from the slice's first
+        // particle -- source at both drifts (2n samples), field at its collision points -- as per-block partials
+        // folded in block order by k_plan
+        double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (n > 0) {
+            const double sx0 = (double)(X[0] + PX[0] * sL), sy0 = (double)(Y[0] + PY[0] * sL);
+            const R s0 = R(0.5) * (Z[0] - cf);
+            const double fx0 = (double)(X[0] + s0 * PX[0]), fy0 = (double)(Y[0] + s0 * PY[0]);
+            for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+                const R x = X[k], px = PX[k], y = Y[k], py = PY[k];
+                const double dxl = (double)(x + px * sL) - sx0, dxr = (double)(x + px * sR) - sx0;
+                const double dyl = (double)(y + py * sL) - sy0, dyr = (double)(y + py * sR) - sy0;
+                e[0] += dxl + dxr; e[1] += dxl * dxl + dxr * dxr;
+                e[2] += dyl + dyr; e[3] += dyl * dyl + dyr * dyr;
+                const R s = R(0.5) * (Z[k] - cf);
+                const double dx = (double)(x + s * px) - fx0, dy = (double)(y + s * py) - fy0;
+                e[4] += dx; e[5] += dx * dx; e[6] += dy; e[7] += dy * dy;
+            }
+        }
+        __shared__ double ered[8][8];
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            double v = e[q];
+            for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (l == 0) ered[w][q] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < 8) {
+            double v = 0.0;
+            for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) v += ered[ww][threadIdx.x];
+            // source sums belong to the task this slice sources, field sums to the task it is the field of
+            const int task = threadIdx.x < 4 ? (side == 0 ? t1 : t2) : (side == 0 ? t2 : t1);
+            C.esum[((long long)task * kMaxBoundBlocks + blockIdx.x) * 8 + threadIdx.x] = v;
+        }
+    }
 #pragma unroll 4
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
         const R x = X[k], px = PX[k], y = Y[k], py = PY[k];
@@ -287,8 +326,23 @@ __device__ inline void record_error(DevStatus *st, int task, int code, int role)
 // and the margin box around the Gaussians joined to the source extent (gaussian_pic.jl:604-660).
 // R: the element type of the beams (the hybrid reads the source slice's first particle, the origin of its
 // moment sums).
+// grid_extent = :sigma turns a (lo, hi) extent into mean +- k sd from the sums of offsets from `origin`
+// (pic_cpu.jl:1551-1593): degenerate spreads and n < 2 keep the extrema.
+__device__ __forceinline__ void axis_extent_sigma(double &lo, double &hi, double origin, double ds, double ds2,
+                                                  long long n, double k) {
+    if (n < 2) return;
+    const double invn = 1.0 / (double)n;
+    const double mean_offset = ds * invn;
+    const double m = origin + mean_offset;
+    const double var = jmax(fma(-mean_offset, mean_offset, ds2 * invn), 0.0);  // muladd of slicing.jl:667-668
+    const double half = k * sqrt(var);
+    if (!(half > 0)) return;
+    lo = m - half;
+    hi = m + half;
+}
+
 template <class R>
-__global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0) {
+__global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0, int ext_blocks) {
     pdl_wait();
     pdl_release();
     int tl = blockIdx.x * blockDim.x + threadIdx.x;
@@ -309,6 +363,33 @@ __global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0) {
     if ((nf & 2) || !(isfinite(fxmin) && isfinite(fxmax) && isfinite(fymin) && isfinite(fymax))) {
         record_error(C.status, t, 1, 2);
         return;
+    }
+    if (C.o.grid_extent) {
+        double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        const double *es = C.esum + (long long)t * kMaxBoundBlocks * 8;
+        for (int b = 0; b < ext_blocks; ++b)
+            for (int q = 0; q < 8; ++q) e[q] += es[b * 8 + q];
+        const SoA Ss = C.beam[T.src_beam], Sf = C.beam[T.fld_beam];
+        const long long ss = T.src_start, fs = T.fld_start;
+        const R sL = (R)T.sL;
+        const double sx0 = (double)(col<R>(Ss, 0)[ss] + col<R>(Ss, 1)[ss] * sL);
+        const double sy0 = (double)(col<R>(Ss, 2)[ss] + col<R>(Ss, 3)[ss] * sL);
+        const R s0 = R(0.5) * (col<R>(Sf, 4)[fs] - (R)T.c_src);
+        const double fx0 = (double)(col<R>(Sf, 0)[fs] + s0 * col<R>(Sf, 1)[fs]);
+        const double fy0 = (double)(col<R>(Sf, 2)[fs] + s0 * col<R>(Sf, 3)[fs]);
+        const double k = C.o.extent_k;
+        axis_extent_sigma(sxmin, sxmax, sx0, e[0], e[1], 2 * T.src_n, k);
+        axis_extent_sigma(symin, symax, sy0, e[2], e[3], 2 * T.src_n, k);
+        axis_extent_sigma(fxmin, fxmax, fx0, e[4], e[5], T.fld_n, k);
+        axis_extent_sigma(fymin, fymax, fy0, e[6], e[7], T.fld_n, k);
+        if (!(isfinite(sxmin) && isfinite(sxmax) && isfinite(symin) && isfinite(symax))) {
+            record_error(C.status, t, 1, 1);
+            return;
+        }
+        if (!(isfinite(fxmin) && isfinite(fxmax) && isfinite(fymin) && isfinite(fymax))) {
+            record_error(C.status, t, 1, 2);
+            return;
+        }
     }
     if (C.o.gaussian) {
         HybridTask &H = C.hyb[t];
@@ -828,6 +909,7 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
     const SoA S = C.beam[P.src_beam];
     const R *X = col<R>(S, 0), *PX = col<R>(S, 1), *Y = col<R>(S, 2), *PY = col<R>(S, 3);
     const R s = (R)P.s;
+    const R s2 = P.count_dropped == 2 ? (R)C.tasks[P.task].sR : s;
     const R x0 = (R)sg.x0, y0 = (R)sg.y0;
     const R xlo = x0, xhi = (R)(sg.x0 + sg.w), ylo = y0, yhi = (R)(sg.y0 + sg.h);
     int outside = 0;
@@ -850,6 +932,10 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
             const R yd = cy + cpy * s;
             if (P.count_dropped && !(isfinite(xd) && xlo <= xd && xd <= xhi && isfinite(yd) && ylo <= yd && yd <= yhi))
                 ++outside;
+            else if (P.count_dropped == 2) {  // :slice_pair under :sigma: the particle at the other boundary too
+                const R x2 = cx + cpx * s2, y2 = cy + cpy * s2;
+                if (!(isfinite(x2) && xlo <= x2 && x2 <= xhi && isfinite(y2) && ylo <= y2 && y2 <= yhi)) ++outside;
+            }
             total += deposit_taps<R, METHOD, TOT, ROT>((xd - x0) * hxi, (yd - y0) * hyi, nx, ny, scale, acc, nx, rot);
             cx = nx_; cpx = npx; cy = ny_; cpy = npy;
         }
@@ -1757,6 +1843,11 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
     const R zL = jclamp(-z * J.hzi + J.zbias, R(0), R(1));
     const R zR = R(1) - zL;
     const R ks = J.ks;
+    if (!o.node && o.grid_extent) {  // :sigma field meshes need not cover every field particle (pic_cpu.jl:1060-1090)
+        const GridR<R> &gF = J.gL;
+        if (!(isfinite(x) && gF.x0 <= x && x <= gF.x0 + gF.w && isfinite(y) && gF.y0 <= y && y <= gF.y0 + gF.h))
+            atomicAdd((unsigned long long *)&C.status->dropped, 1ull);
+    }
     if (o.node) {
         // L on gL, R on gR, Z (the R drift deposited on gL) on gL; with zL = 1, zR = 0 the reference's
         // single-plane interpolations reduce exactly to w * E (pic_cpu.jl:1517-1528).

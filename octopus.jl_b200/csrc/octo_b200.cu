@@ -294,6 +294,7 @@ struct octo_ctx {
     DevBuf<double> lum_parts, lum_partial, node_ref, stats, partial;
     DevBuf<HybridTask> hyb;            // Gaussian-subtracted hybrid state per task
     DevBuf<double> hmom, hprof, hsum;  // its moment partials, node profiles and profile sums
+    DevBuf<double> esum;               // grid_extent = :sigma: per-block sums of the drifted offsets
     DevBuf<double> mom_partial, mom_means;  // beam moment rows: block partials and the means
     // soft-Gaussian solver: slices, their moments, kick tasks, block maps, partial sums
     DevBuf<GSlice> g_slices;
@@ -412,10 +413,13 @@ int validate_options(const octo_pic_options &o, std::string &msg) {
         msg = "interaction_grid = :source_slice is implemented only by the CPU PICPoissonSolver path (pic_cpu.jl:730-809)";
         return OCTO_ERR_UNSUPPORTED;
     }
-    if (o.grid_extent != 0) {
-        msg = "grid_extent = :sigma is not implemented by the GPU PIC backend; set grid_extent = :extrema";
+    if (o.grid_extent != 0 && o.grid_extent != 1) { msg = "grid_extent must be :extrema or :sigma"; return OCTO_ERR_ARG; }
+    if (o.grid_extent == 1 && o.interaction_grid != OCTO_GRID_SLICE_PAIR) {  // pic_cpu.jl:545-558
+        msg = "grid_extent = :sigma is implemented for interaction_grid = :slice_pair only: :node sizes its meshes "
+              "from per-node extrema and applies no extent estimator";
         return OCTO_ERR_UNSUPPORTED;
     }
+    if (o.grid_extent == 1 && !(o.grid_extent_sigma > 0.0)) { msg = "grid_extent_sigma must be positive"; return OCTO_ERR_ARG; }
     if (o.interaction_grid == OCTO_GRID_NODE && o.slice_interpolation != 0) {
         msg = "slice_interpolation = :quadratic is not implemented for interaction_grid = :node";
         return OCTO_ERR_UNSUPPORTED;
@@ -1118,7 +1122,9 @@ void CollideJob::run() {
                         P.s = k == 0 ? T.sL : (k == 1 ? T.sR : 0.5 * (T.sL + T.sR));
                         P.geom = -1;
                         P.green = -1;
-                        P.count_dropped = 0;
+                        // :sigma meshes need not cover the source: count particles outside at either drift once
+                        // (the L plane checks both)
+                        P.count_dropped = (c->dopt.grid_extent && k == 0) ? 2 : 0;
                         if (fp32 && !quad && k == 1) { P.other_delta = -1; P.self_first = 0; }  // L - R
                         if (fp32 && quad && k < 2) { P.other_delta = 2 - k; P.self_first = 1; }  // L - M, R - M
                     }
@@ -1273,6 +1279,10 @@ void CollideJob::run() {
     // nothing an earlier (failed) collide left on the luminosity stream may overlap this one
     CK(cudaEventRecord(c->ev_join, c->lum_stream));
     CK(cudaStreamWaitEvent(st, c->ev_join, 0));
+    if (c->dopt.grid_extent) {
+        c->esum.ensure((size_t)std::max(ntasks, 1) * kMaxBoundBlocks * 8);
+        C.esum = c->esum.p;
+    }
     if (gaussian) {
         c->hyb.ensure(std::max(ntasks, 1));
         c->hmom.ensure((size_t)std::max(ntasks, 1) * kMaxBoundBlocks * kMomentSums);
@@ -1338,7 +1348,9 @@ void CollideJob::run() {
         if (!node) {
             {
                 PhaseScope ps(c, OCTO_PHASE_PLAN, st, 1);
-                with_real(fp32, [&](auto r) { launch_pdl(k_plan<decltype(r)>, (F.nt + 63) / 64, 64, 0, st, C, F.t0, F.nt, 0); });
+                with_real(fp32, [&](auto r) {
+                    launch_pdl(k_plan<decltype(r)>, (F.nt + 63) / 64, 64, 0, st, C, F.t0, F.nt, 0, (int)bps);
+                });
             }
             PhaseScope ps(c, OCTO_PHASE_GREEN, st, gaussian ? 3 : 2);
             launch_green(c, C, 0, F.t0, F.nt, st);
@@ -1962,6 +1974,8 @@ octo_ctx *octo_create(int32_t device, const octo_pic_options *options) {
     d.gaussian = options->gaussian != 0;
     d.neutralize = options->neutralize != 0;
     d.margin = options->margin_sigma;
+    d.grid_extent = options->grid_extent;
+    d.extent_k = options->grid_extent_sigma;
     d.coupling_tol = options->coupling_tol;
     try {
         CK(cudaSetDevice(device));
@@ -2021,6 +2035,7 @@ void octo_destroy(octo_ctx *c) {
     c->first_lum.release(); c->lum_tick.release(); c->cap_q.release(); c->cap_grid.release();
     c->cnn_flags.release(); c->h_cnn_flags.release(); c->cnn_q.release();
     c->hyb.release(); c->hmom.release(); c->hprof.release(); c->hsum.release(); c->qtot.release();
+    c->esum.release();
     c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_noderef.release(); c->h_slices.release();
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);

@@ -246,6 +246,8 @@ struct DevOptions {
     int dep_global, lum_global;  // charge / luminosity grid larger than shared memory: global atomics
     int gaussian, neutralize;    // GaussianPICPoissonSolver (Gaussian-subtracted hybrid)
     int dep_rotate;              // rotate each lane's deposit tap order (spatially ordered slices)
+    int grid_extent;             // :slice_pair mesh extent: 0 :extrema, 1 :sigma (mean +- extent_k sd)
+    double extent_k;             // grid_extent_sigma
     double min_ex, min_ey, quantize, min_ratio, growth;
     double margin;               // hybrid: Gaussian containment half-width in sigmas
     double coupling_tol;         // hybrid: |r_xy| above which the coupled subtraction runs (inf: never)

@@ -157,7 +157,7 @@ class PICPoissonSolver:
         o.field_derivative = 2 if self.field_derivative == "second" else 4
         o.slice_interpolation = 0 if self.slice_interpolation == "linear" else 1
         o.interaction_grid = {"slice_pair": 0, "node": 2}[self.interaction_grid]
-        o.grid_extent = 0
+        o.grid_extent = 0 if self.grid_extent == "extrema" else 1
         o.grid_extent_sigma = float(self.grid_extent_sigma)
         o.min_extent_x, o.min_extent_y = self.min_transverse_extent
         o.grid_quantize = float(self.grid_quantize)
@@ -198,9 +198,6 @@ def _require_gpu_options(s: PICPoissonSolver):
         raise ArgumentError(
             "interaction_grid = :source_slice is not implemented by the GPU PIC backend; only the CPU "
             "PICPoissonSolver path supports :source_slice. Set interaction_grid = :slice_pair.")
-    if s.grid_extent != "extrema":
-        raise ArgumentError(
-            f"grid_extent = :{s.grid_extent} is not implemented by the GPU PIC backend; set grid_extent = :extrema.")
     if s.green_type == "lattice":
         raise ArgumentError("green_type = :lattice (an experimental CPU study kernel) is not implemented by the GPU "
                             "PIC backend; use :integrated or :standard.")

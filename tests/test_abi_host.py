@@ -99,10 +99,12 @@ def test_solver_defaults_and_validation():
 
 def test_gpu_backend_rejects_what_it_does_not_implement():
     sl = ob.LongitudinalSlicing(nslices=3, method="normal_quantile")
-    for kw in (dict(interaction_grid="source_slice"), dict(grid_extent="sigma"), dict(green_type="lattice"),
+    for kw in (dict(interaction_grid="source_slice"), dict(green_type="lattice"),
                dict(grid=(80, 80)), dict(grid=(96, 36)), dict(grid=(1024, 64))):
         with pytest.raises(ob.ArgumentError):
             ob.PICPoissonSolver(slicing=sl, **kw).to_c()
+    o = ob.PICPoissonSolver(slicing=sl, grid_extent="sigma", grid_extent_sigma=4.5).to_c()  # :slice_pair only
+    assert (o.grid_extent, o.grid_extent_sigma) == (1, 4.5)
     with pytest.raises(ob.ArgumentError):  # the :equal_area histogram's shared-memory bound
         ob.PICPoissonSolver(slicing=ob.LongitudinalSlicing(nslices=64, method="equal_area", resolution=300)).to_c()
     for m, code in (("equal_area", 2), ("equal_count", 3), ("equal_width", 4), ("equal_spaced", 4), ("gaussian", 0)):

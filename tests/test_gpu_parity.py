@@ -94,6 +94,8 @@ def test_route_fixture():
     dict(green_type="standard", green_cache="none"),
     dict(luminosity_deposit_method="TSC", luminosity_grid=(48, 40)),
     dict(deposit_method="TSC", field_derivative="fourth", slice_interpolation="quadratic"),
+    dict(grid_extent="sigma"),
+    dict(grid_extent="sigma", grid_extent_sigma=2.5, green_cache="none", slice_interpolation="quadratic"),
 ])
 def test_option_variants(opts):
     ob = _gpu()
@@ -245,3 +247,27 @@ def test_gaussian_hybrid_coupled_rank_deficient_falls_back():
                                     coupling_tol=0.5)
     check(run_both(s, 5000, 4000, turns=1, e_sigma=(95e-6, 8.5e-6, 7e-3), p_sigma=(95e-6, 8.5e-6, 6e-2),
                    transform=corr))
+
+
+def test_grid_extent_sigma_counts_particles_outside_its_meshes():
+    """grid_extent = :sigma sizes each :slice_pair mesh as mean +- k sd of the drifted particles
+    (pic_cpu.jl:1551-1593), which need not cover them all: with k = 2 many fall outside, and the device counts
+    them as the reference does -- a source particle once if it is outside at either drift, a field particle if
+    it is outside the field mesh (pic_cpu.jl:1060-1090) -- equal to the oracle's count, collide by collide."""
+    from oracle import oracle as orc
+    ob = _gpu()
+    s = ob.PICPoissonSolver(grid=(64, 64), grid_extent="sigma", grid_extent_sigma=2.0,
+                            slicing=ob.LongitudinalSlicing(nslices=4, method="normal_quantile"))
+    e, p = beams(6000, 4000)
+    be, bp = _device_beams(ob, e, p)
+    rt = ob.StrongStrongRuntime()
+    ctx = rt.context("ip", s, 0)
+    oracle = orc.Oracle(oracle_options(s))
+    pe, pp = oracle_params()
+    for t in range(2):
+        lum_g = ctx.collide(be, bp, turn=t + 1)
+        lum_o = oracle.collide(e, p, pe, pp)
+        assert ctx.last_report.dropped == oracle.dropped() > 0, (ctx.last_report.dropped, oracle.dropped())
+        assert abs(lum_g / lum_o - 1) <= 1e-10
+        assert within(be.numpy(), e, ATOL, RTOL) <= 1.0 and within(bp.numpy(), p, ATOL, RTOL) <= 1.0
+    rt.close()
