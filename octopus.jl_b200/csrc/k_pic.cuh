@@ -813,7 +813,8 @@ __global__ void __launch_bounds__(128) k_green_cols_r(Collide C, int mode, int b
 // grid (a block-private shared-memory copy, merged into the plane's grid at the end of the block).
 // The shared grid is addressed through an opaque generic pointer (generic_ptr): measured on B200, a
 // 64-bit atomic add to shared memory issued on a generic address runs at 10.3 per clock per SM (4.1 under
-// 4-way conflicts) against 5.2 (1.6) when the compiler sees the shared address space.  Measured
+// 4-way conflicts) against 5.2 (1.6) when the compiler sees the shared address space (the precision form's
+// 32-bit atomics the other way round: faster on the shared-typed address, 1.45 -> 1.35 ms per turn).  Measured
 // alternatives, all slower on the production turn: 32-bit split accumulators (two atomics per tap),
 // warp-aggregated runs of equal cells, batched loads, and spatially sorted particles.
 template <class T>
@@ -825,8 +826,21 @@ __device__ __forceinline__ T *generic_ptr(T *p) {
 // rot (CIC): the lane's four atomics start at tap rot & 3 -- particles of a spatially ordered slice share
 // cells with their warp neighbours, and rotating the tap order spreads a warp's simultaneous atomics over
 // four addresses per cell.  Integer sums: the order changes nothing.
-template <class R, int METHOD, bool TOTAL = false, bool ROT = false>
-__device__ __forceinline__ long long deposit_taps(R u, R v, int nw, int nh, R scale, long long *grid, int ld, int rot = 0) {
+// Q: the accumulator's element type -- int64 for the plain form and for plane grids in global memory; int32 for
+// the precision form's block-private shared grids, whose fixed-point scale (fixed_bits_for32) keeps a whole
+// slice's charge in one cell below 2^30, so a tap is one 32-bit atomic.
+__device__ __forceinline__ void atom_add(long long *p, long long v) {
+    atomicAdd((unsigned long long *)p, (unsigned long long)v);
+}
+__device__ __forceinline__ void atom_add(int *p, int v) { atomicAdd(p, v); }
+template <class Q, class R>
+__device__ __forceinline__ Q quantize(R x) {
+    if constexpr (sizeof(Q) == 8) return round_ll(x);
+    else if constexpr (sizeof(R) == 4) return __float2int_rn(x);
+    else return __double2int_rn(x);
+}
+template <class R, int METHOD, bool TOTAL = false, bool ROT = false, class Q = long long>
+__device__ __forceinline__ long long deposit_taps(R u, R v, int nw, int nh, R scale, Q *grid, int ld, int rot = 0) {
     constexpr int NT = METHOD == 0 ? 2 : 3;
     int ix, iy;
     long long total = 0;
@@ -835,53 +849,58 @@ __device__ __forceinline__ long long deposit_taps(R u, R v, int nw, int nh, R sc
     else { tsc_weights(u, nw, ix, wx); tsc_weights(v, nh, iy, wy); }
     const int c0 = (iy - 1) * ld + (ix - 1);
     if constexpr (METHOD == 0) {
-        long long q0 = round_ll(wx[0] * wy[0] * scale), q1 = round_ll(wx[0] * wy[1] * scale);
-        long long q2 = round_ll(wx[1] * wy[0] * scale), q3 = round_ll(wx[1] * wy[1] * scale);
-        if (TOTAL) total = q0 + q1 + q2 + q3;
+        Q q0 = quantize<Q>(wx[0] * wy[0] * scale), q1 = quantize<Q>(wx[0] * wy[1] * scale);
+        Q q2 = quantize<Q>(wx[1] * wy[0] * scale), q3 = quantize<Q>(wx[1] * wy[1] * scale);
+        if (TOTAL) total = (long long)q0 + q1 + q2 + q3;
         int o0 = c0, o1 = c0 + ld, o2 = c0 + 1, o3 = c0 + ld + 1;
         if constexpr (ROT) {  // a separate instantiation: the permutation costs the unrotated deposit nothing
             if (rot & 1) {
                 const int to = o0; o0 = o1; o1 = o2; o2 = o3; o3 = to;
-                const long long tq = q0; q0 = q1; q1 = q2; q2 = q3; q3 = tq;
+                const Q tq = q0; q0 = q1; q1 = q2; q2 = q3; q3 = tq;
             }
             if (rot & 2) {
                 int to = o0; o0 = o2; o2 = to; to = o1; o1 = o3; o3 = to;
-                long long tq = q0; q0 = q2; q2 = tq; tq = q1; q1 = q3; q3 = tq;
+                Q tq = q0; q0 = q2; q2 = tq; tq = q1; q1 = q3; q3 = tq;
             }
         }
-        atomicAdd((unsigned long long *)&grid[o0], (unsigned long long)q0);
-        atomicAdd((unsigned long long *)&grid[o1], (unsigned long long)q1);
-        atomicAdd((unsigned long long *)&grid[o2], (unsigned long long)q2);
-        atomicAdd((unsigned long long *)&grid[o3], (unsigned long long)q3);
+        atom_add(&grid[o0], q0);
+        atom_add(&grid[o1], q1);
+        atom_add(&grid[o2], q2);
+        atom_add(&grid[o3], q3);
     } else {
 #pragma unroll
         for (int m = 0; m < NT; ++m)
 #pragma unroll
             for (int k = 0; k < NT; ++k) {
-                const long long qv = round_ll(wx[m] * wy[k] * scale);
+                const Q qv = quantize<Q>(wx[m] * wy[k] * scale);
                 if (TOTAL) total += qv;
                 // a zero quantum (out-of-range particle: base 1, every weight 0) adds nothing; the unconditional
                 // atomic measured faster than the test
-                atomicAdd((unsigned long long *)&grid[c0 + k * ld + m], (unsigned long long)qv);
+                atom_add(&grid[c0 + k * ld + m], qv);
             }
     }
     return total;
 }
 
 // Merge a block's shared-memory grid into the plane's int64 grid.
-__device__ __forceinline__ void merge_grid(const long long *sq, long long *g, int cells) {
+template <class Q>
+__device__ __forceinline__ void merge_grid(const Q *sq, long long *g, int cells) {
     for (int c = threadIdx.x; c < cells; c += blockDim.x) {
         const long long v = sq[c];
         if (v) atomicAdd((unsigned long long *)&g[c], (unsigned long long)v);
     }
 }
+// The block-private shared grid's element type: int32 in the precision form, int64 in the plain form.
+template <class R>
+using ShQ = typename std::conditional<sizeof(R) == 4, int, long long>::type;
 
 // Field-solve planes of a front.  grid: (blocks per plane, planes in front); each block deposits a
 // grid-stride share of its plane's source slice into a private int64 copy of the nx*ny grid in shared
 // memory, then merges it with global atomics (the consumer, k_conv_rows, clears the grid it reads).
 template <class R, int METHOD>
 __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
-    long long *sq = (long long *)g_smem;
+    using Q = ShQ<R>;
+    Q *sq = (Q *)g_smem;
     const int nx = C.o.nx, ny = C.o.ny, cells = nx * ny;
     // grids larger than shared memory (C.o.dep_global) accumulate straight into the plane's grid; the
     // block's shared grid is cleared before the wait (shared memory only)
@@ -902,14 +921,17 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
         sg = G.sg;
     }
     __syncthreads();
-    long long *acc = local ? generic_ptr(sq) : C.qgrid + (long long)pl * cells;
     const double hx = sg.w / (double)(nx - 1), hy = sg.h / (double)(ny - 1);
     const R hxi = (R)(1.0 / hx), hyi = (R)(1.0 / hy);
     const R scale = (R)ldexp(1.0, P.fixed_bits);
     const SoA S = C.beam[P.src_beam];
     const R *X = col<R>(S, 0), *PX = col<R>(S, 1), *Y = col<R>(S, 2), *PY = col<R>(S, 3);
     const R s = (R)P.s;
-    const R s2 = P.count_dropped == 2 ? (R)C.tasks[P.task].sR : s;
+    // the plane's fields in registers: the loop's atomics go through a generic pointer, which the compiler
+    // cannot separate from the plane table in global memory, so it would reload them for every particle
+    const int count_dropped = P.count_dropped;
+    const long long src_n = P.src_n, src_start = P.src_start;
+    const R s2 = count_dropped == 2 ? (R)C.tasks[P.task].sR : s;
     const R x0 = (R)sg.x0, y0 = (R)sg.y0;
     const R xlo = x0, xhi = (R)(sg.x0 + sg.w), ylo = y0, yhi = (R)(sg.y0 + sg.h);
     int outside = 0;
@@ -917,38 +939,47 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
     const int rot = C.o.dep_rotate ? (int)(threadIdx.x & 3) : 0;
     // the next particle's coordinates are loaded before the current one's taps, two loads in flight
     const long long stride = (long long)gridDim.x * blockDim.x;
-    auto sweep = [&](auto with_total, auto rotated) {
+    auto sweep = [&](auto with_total, auto rotated, auto *acc) {
         constexpr bool TOT = decltype(with_total)::value, ROT = decltype(rotated)::value;
+        using QA = typename std::remove_pointer<decltype(acc)>::type;
         long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
         R cx = 0, cpx = 0, cy = 0, cpy = 0;
-        if (k < P.src_n) { const long long p = P.src_start + k; cx = X[p]; cpx = PX[p]; cy = Y[p]; cpy = PY[p]; }
-        for (; k < P.src_n; k += stride) {
+        if (k < src_n) { const long long p = src_start + k; cx = X[p]; cpx = PX[p]; cy = Y[p]; cpy = PY[p]; }
+        for (; k < src_n; k += stride) {
             R nx_ = 0, npx = 0, ny_ = 0, npy = 0;
-            if (k + stride < P.src_n) {
-                const long long q = P.src_start + k + stride;
+            if (k + stride < src_n) {
+                const long long q = src_start + k + stride;
                 nx_ = X[q]; npx = PX[q]; ny_ = Y[q]; npy = PY[q];
             }
             const R xd = cx + cpx * s;
             const R yd = cy + cpy * s;
-            if (P.count_dropped && !(isfinite(xd) && xlo <= xd && xd <= xhi && isfinite(yd) && ylo <= yd && yd <= yhi))
+            if (count_dropped && !(isfinite(xd) && xlo <= xd && xd <= xhi && isfinite(yd) && ylo <= yd && yd <= yhi))
                 ++outside;
-            else if (P.count_dropped == 2) {  // :slice_pair under :sigma: the particle at the other boundary too
+            else if (count_dropped == 2) {  // :slice_pair under :sigma: the particle at the other boundary too
                 const R x2 = cx + cpx * s2, y2 = cy + cpy * s2;
                 if (!(isfinite(x2) && xlo <= x2 && x2 <= xhi && isfinite(y2) && ylo <= y2 && y2 <= yhi)) ++outside;
             }
-            total += deposit_taps<R, METHOD, TOT, ROT>((xd - x0) * hxi, (yd - y0) * hyi, nx, ny, scale, acc, nx, rot);
+            total += deposit_taps<R, METHOD, TOT, ROT, QA>((xd - x0) * hxi, (yd - y0) * hyi, nx, ny, scale, acc, nx, rot);
             cx = nx_; cpx = npx; cy = ny_; cpy = npy;
         }
     };
     // (the hybrid's exact plane totals and the rotation for spatially ordered slices never combine)
-    if (C.o.gaussian) sweep(std::true_type(), std::false_type());
-    else if (C.o.dep_rotate) sweep(std::false_type(), std::true_type());
-    else sweep(std::false_type(), std::false_type());
+    auto run = [&](auto *acc) {
+        if (C.o.gaussian) sweep(std::true_type(), std::false_type(), acc);
+        else if (C.o.dep_rotate) sweep(std::false_type(), std::true_type(), acc);
+        else sweep(std::false_type(), std::false_type(), acc);
+    };
+    if constexpr (sizeof(Q) == 8) {  // one pointer, one instance of the loop
+        run(local ? generic_ptr(sq) : C.qgrid + (long long)pl * cells);
+    } else {  // 32-bit shared atomics measured faster on the shared-typed address than on a generic one
+        if (local) run(sq);
+        else run(C.qgrid + (long long)pl * cells);
+    }
     if (C.o.gaussian) {  // the plane's exact total charge, for the neutralised subtraction
         for (int o = 16; o; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
         if ((threadIdx.x & 31) == 0 && total) atomicAdd(&C.qtot[pl], (unsigned long long)total);
     }
-    if (P.count_dropped) {
+    if (count_dropped) {
         for (int o = 16; o; o >>= 1) outside += __shfl_xor_sync(0xffffffffu, outside, o);
         if ((threadIdx.x & 31) == 0 && outside) atomicAdd((unsigned long long *)&C.status->dropped, (unsigned long long)outside);
     }
@@ -965,7 +996,8 @@ template <class R, int METHOD>
 __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0, int task0) {
     pdl_wait();
     pdl_release();
-    long long *sq = (long long *)g_smem;
+    using Q = ShQ<R>;
+    Q *sq = (Q *)g_smem;
     const int ql = blockIdx.y >> 1, side = blockIdx.y & 1;
     const LumJob &J = C.lumjobs[lj0 + ql];
     LumGeom L;
@@ -981,7 +1013,6 @@ __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0, int
     if (local)
         for (int c = threadIdx.x; c < cells; c += blockDim.x) sq[c] = 0;
     __syncthreads();
-    long long *acc = local ? generic_ptr(sq) : C.lq + (long long)blockIdx.y * cells;
     const SoA S = C.beam[side];
     const R *X = col<R>(S, 0), *PX = col<R>(S, 1), *Y = col<R>(S, 2), *PY = col<R>(S, 3);
     const long long st = side ? J.s2_start : J.s1_start, n = side ? J.s2_n : J.s1_n;
@@ -991,8 +1022,9 @@ __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0, int
     const R x0 = (R)L.x0, y0 = (R)L.y0;
     const long long stride = (long long)gridDim.x * blockDim.x;
     const int rot = C.o.dep_rotate ? (int)(threadIdx.x & 3) : 0;
-    auto sweep = [&](auto rotated) {
+    auto sweep = [&](auto rotated, auto *acc) {
         constexpr bool ROT = decltype(rotated)::value;
+        using QA = typename std::remove_pointer<decltype(acc)>::type;
         long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
         R cx = 0, cpx = 0, cy = 0, cpy = 0;
         if (k < n) { cx = X[st + k]; cpx = PX[st + k]; cy = Y[st + k]; cpy = PY[st + k]; }
@@ -1004,12 +1036,20 @@ __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0, int
             }
             const R vx = cx + cpx * s;
             const R vy = cy + cpy * s;
-            deposit_taps<R, METHOD, false, ROT>((vx - x0) * hxi, (vy - y0) * hyi, nw, nh, scale, acc, nw, rot);
+            deposit_taps<R, METHOD, false, ROT, QA>((vx - x0) * hxi, (vy - y0) * hyi, nw, nh, scale, acc, nw, rot);
             cx = nx_; cpx = npx; cy = ny_; cpy = npy;
         }
     };
-    if (C.o.dep_rotate) sweep(std::true_type());
-    else sweep(std::false_type());
+    auto run = [&](auto *acc) {
+        if (C.o.dep_rotate) sweep(std::true_type(), acc);
+        else sweep(std::false_type(), acc);
+    };
+    if constexpr (sizeof(Q) == 8) {
+        run(local ? generic_ptr(sq) : C.lq + (long long)blockIdx.y * cells);
+    } else {
+        if (local) run(sq);
+        else run(C.lq + (long long)blockIdx.y * cells);
+    }
     if (local) {
         __syncthreads();
         merge_grid(sq, C.lq + (long long)blockIdx.y * cells, cells);

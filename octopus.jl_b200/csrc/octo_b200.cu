@@ -1101,7 +1101,7 @@ void CollideJob::run() {
                 T.plane0 = (int)planes.size();
                 T.nplanes = nplanes_task;
                 const int tid = (int)tasks.size();
-                const int bits = fixed_bits_for(T.src_n);
+                const int bits = fp32 ? fixed_bits_for32(T.src_n) : fixed_bits_for(T.src_n);
                 for (int k = 0; k < nplanes_task; ++k) {
                     Plane P{};
                     P.task = tid;
@@ -1140,8 +1140,8 @@ void CollideJob::run() {
                 J.s2_start = S2.start[j - 1]; J.s2_n = S2.count[j - 1];
                 J.sM1 = 0.5 * (S1.center[i - 1] - S2.center[j - 1]);
                 J.sM2 = 0.5 * (S2.center[j - 1] - S1.center[i - 1]);
-                J.bits1 = fixed_bits_for(J.s1_n);
-                J.bits2 = fixed_bits_for(J.s2_n);
+                J.bits1 = fp32 ? fixed_bits_for32(J.s1_n) : fixed_bits_for(J.s1_n);
+                J.bits2 = fp32 ? fixed_bits_for32(J.s2_n) : fixed_bits_for(J.s2_n);
                 F.maxlum = std::max<long long>(F.maxlum, std::max<long long>(J.s1_n, J.s2_n));
                 lumjobs.push_back(J);
             }
@@ -1307,8 +1307,9 @@ void CollideJob::run() {
         launches += 1;
     }
 
-    const size_t dep_bytes = c->dopt.dep_global ? 0 : cells * sizeof(long long);
-    const size_t lum_bytes = c->dopt.lum_global ? 0 : lcells * sizeof(long long);
+    const size_t qsz = fp32 ? sizeof(int) : sizeof(long long);  // the block-private grids' element
+    const size_t dep_bytes = c->dopt.dep_global ? 0 : cells * qsz;
+    const size_t lum_bytes = c->dopt.lum_global ? 0 : lcells * qsz;
 
     // ---- wavefronts
     for (const Front &F : fronts) {

@@ -238,6 +238,17 @@ inline int fixed_bits_for(int64_t n) {
     int b = 62 - bl;
     return b > 40 ? 40 : b;
 }
+// The precision form's scale: bits = min(40, 30 - bitlength(nsrc)), so a whole slice fits one int32 cell of the
+// block-private shared grids (its int64 plane grids and every integer sum stay exact).  An FP32 weight carries
+// 24 significant bits, so the quanta lose nothing for slices of up to ~64 particles and at most 2^-(bits+1) of a
+// particle's charge per tap beyond (2^-13 at 170,000 particles).
+inline int fixed_bits_for32(int64_t n) {
+    int bl = 0;
+    uint64_t v = (uint64_t)(n < 1 ? 1 : n);
+    while (v) { ++bl; v >>= 1; }
+    int b = 30 - bl;
+    return b > 40 ? 40 : b;
+}
 
 // ---------------------------------------------------------------- options (device copy)
 struct DevOptions {
