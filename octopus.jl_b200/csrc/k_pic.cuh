@@ -989,6 +989,67 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
     }
 }
 
+// The precision form's :node deposit with the three planes of a task in one pass (int32 block grids, all three
+// in shared memory up to 128 x 128): L (the sL drift on the L mesh), R (sR on the R mesh) and Z (sR on the L
+// mesh; only with the longitudinal kick) read the source particle and compute its two drifts once.  grid:
+// (blocks per task, tasks in front); ppt = 2 or 3 planes per task, consecutive.  Every quantum is the
+// expression of k_deposit, so the grids are bit-identical to k_deposit's planes.
+template <class R, int METHOD>
+__global__ void __launch_bounds__(1024, 1) k_deposit_node3(Collide C, int plane0, int ppt) {
+    int *sq = (int *)g_smem;  // L | R | Z
+    const int nx = C.o.nx, ny = C.o.ny, cells = nx * ny;
+    for (int c = threadIdx.x; c < ppt * cells; c += blockDim.x) sq[c] = 0;
+    pdl_wait();
+    pdl_release();
+    const int pl = ppt * blockIdx.y;
+    const bool z = ppt == 3;
+    const Plane &PL = C.planes[plane0 + pl], &PR = C.planes[plane0 + pl + 1];
+    const bool okL = C.nodes[PL.geom].valid != 0, okR = C.nodes[PR.geom].valid != 0;
+    if (!okL && !okR) return;  // block-uniform
+    const Grid gL = C.nodes[PL.geom].sg, gR = C.nodes[PR.geom].sg;
+    __syncthreads();
+    const R hxiL = (R)(1.0 / (gL.w / (double)(nx - 1))), hyiL = (R)(1.0 / (gL.h / (double)(ny - 1)));
+    const R hxiR = (R)(1.0 / (gR.w / (double)(nx - 1))), hyiR = (R)(1.0 / (gR.h / (double)(ny - 1)));
+    const R scale = (R)ldexp(1.0, PL.fixed_bits);
+    const SoA S = C.beam[PL.src_beam];
+    const R *X = col<R>(S, 0), *PX = col<R>(S, 1), *Y = col<R>(S, 2), *PY = col<R>(S, 3);
+    const R sL = (R)PL.s, sR = (R)PR.s;
+    const long long src_n = PL.src_n, src_start = PL.src_start;
+    const R xL0 = (R)gL.x0, yL0 = (R)gL.y0, xR0 = (R)gR.x0, yR0 = (R)gR.y0;
+    const R xLhi = (R)(gL.x0 + gL.w), yLhi = (R)(gL.y0 + gL.h), xRhi = (R)(gR.x0 + gR.w), yRhi = (R)(gR.y0 + gR.h);
+    int outside = 0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    R cx = 0, cpx = 0, cy = 0, cpy = 0;
+    if (k < src_n) { const long long p = src_start + k; cx = X[p]; cpx = PX[p]; cy = Y[p]; cpy = PY[p]; }
+    for (; k < src_n; k += stride) {
+        R nx_ = 0, npx = 0, ny_ = 0, npy = 0;
+        if (k + stride < src_n) {
+            const long long q = src_start + k + stride;
+            nx_ = X[q]; npx = PX[q]; ny_ = Y[q]; npy = PY[q];
+        }
+        const R xl = cx + cpx * sL, yl = cy + cpy * sL;
+        const R xr = cx + cpx * sR, yr = cy + cpy * sR;
+        if (okL) {
+            if (!(isfinite(xl) && xL0 <= xl && xl <= xLhi && isfinite(yl) && yL0 <= yl && yl <= yLhi)) ++outside;
+            deposit_taps<R, METHOD, false, false, int>((xl - xL0) * hxiL, (yl - yL0) * hyiL, nx, ny, scale, sq, nx);
+            if (z)
+                deposit_taps<R, METHOD, false, false, int>((xr - xL0) * hxiL, (yr - yL0) * hyiL, nx, ny, scale, sq + 2 * cells,
+                                                           nx);
+        }
+        if (okR) {
+            if (!(isfinite(xr) && xR0 <= xr && xr <= xRhi && isfinite(yr) && yR0 <= yr && yr <= yRhi)) ++outside;
+            deposit_taps<R, METHOD, false, false, int>((xr - xR0) * hxiR, (yr - yR0) * hyiR, nx, ny, scale, sq + cells, nx);
+        }
+        cx = nx_; cpx = npx; cy = ny_; cpy = npy;
+    }
+    for (int o = 16; o; o >>= 1) outside += __shfl_xor_sync(0xffffffffu, outside, o);
+    if ((threadIdx.x & 31) == 0 && outside) atomicAdd((unsigned long long *)&C.status->dropped, (unsigned long long)outside);
+    __syncthreads();
+    for (int g = 0; g < ppt; ++g)
+        if (g == 1 ? okR : okL) merge_grid(sq + g * cells, C.qgrid + (long long)(pl + g) * cells, cells);
+}
+
 // Luminosity planes: 2 per pair (side 0 = beam-1 slice i at sM1, side 1 = beam-2 slice j at sM2)
 // on the (lnx+1) x (lny+1) overlap mesh (pic_cpu.jl:2724-2735).
 // Every block derives its pair's mesh (lum_geometry); block (0, side 0) publishes it and reports errors.

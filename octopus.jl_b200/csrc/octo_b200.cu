@@ -770,6 +770,10 @@ void set_smem_limits() {
         CK(cudaFuncSetAttribute(k_deposit<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
         CK(cudaFuncSetAttribute(k_lum_deposit<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
         CK(cudaFuncSetAttribute(k_lum_deposit<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        if constexpr (sizeof(R) == 4) {
+            CK(cudaFuncSetAttribute(k_deposit_node3<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+            CK(cudaFuncSetAttribute(k_deposit_node3<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        }
         CK(cudaFuncSetAttribute(k_conv_rows<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
         CK(cudaFuncSetAttribute(k_conv_cols<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
         CK(cudaFuncSetAttribute(k_conv_field<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
@@ -1365,13 +1369,25 @@ void CollideJob::run() {
             PhaseScope ps(c, OCTO_PHASE_DEPOSIT, st, 1, src_bytes * 4 * rsz);
             // blocks per plane: 32768-particle shares, and at least one full wave of the GPU's SMs for the
             // narrow fronts (one block per SM: a block holds its plane's whole int64 grid)
-            const long long wave = ((long long)c->num_sms * c->dep_waves + F.np - 1) / F.np;
+            // the precision form's :node planes of a task in one pass when their three int32 grids fit shared
+            // memory (k_deposit_node3)
+            const int ppt = c->dopt.longitudinal_kick ? 3 : 2;  // :node planes per task (L, R and Z)
+            const bool node3 = fp32 && node && !c->dopt.dep_global && !c->dopt.dep_rotate && ppt * cells * sizeof(int) <= kSmemLimit;
+            const int rows = node3 ? F.np / ppt : F.np;
+            const long long wave = ((long long)c->num_sms * c->dep_waves + rows - 1) / rows;
             unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(32, std::max<long long>((F.maxsrc + 32767) / 32768, wave)));
-            with_real(fp32, [&](auto r) {
+            if (node3) {
                 launch_method(method, [&](auto M) {
-                    launch_pdl(k_deposit<decltype(r), decltype(M)::value>, dim3(bpp, F.np), 1024, dep_bytes, st, C, F.p0);
+                    launch_pdl(k_deposit_node3<float, decltype(M)::value>, dim3(bpp, rows), 1024, ppt * cells * sizeof(int), st, C,
+                               F.p0, ppt);
                 });
-            });
+            } else {
+                with_real(fp32, [&](auto r) {
+                    launch_method(method, [&](auto M) {
+                        launch_pdl(k_deposit<decltype(r), decltype(M)::value>, dim3(bpp, F.np), 1024, dep_bytes, st, C, F.p0);
+                    });
+                });
+            }
         }
         const bool learned = c->cnn != nullptr;
         if (learned) {  // the learned correction's input from the front's charge grids, and the network
