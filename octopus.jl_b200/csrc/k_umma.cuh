@@ -103,6 +103,8 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 constexpr int kStages = 4;
+constexpr int kDepth = kStages - 2;  // K chunks in flight ahead of the one being multiplied (a refill waits for
+                                     // the MMAs of the chunk two back, which are done by then)
 constexpr int kRowsPerThread = (kBM * 8) / kGemmThreads;  // A rows (one 16-byte k-chunk each) a thread loads
 
 // The thread -> chunk mapping of a stage: chunk c = it * kGemmThreads + tid covers row (c & 7) + 8 * (c >> 6)
@@ -238,13 +240,13 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_umma_gemm(const GemmArgs g)
         // prologue: chunks 0 .. kStages-2 in flight.  Every stage's MMAs of the previous tile are complete
         // (the previous tile waited for all of them before its epilogue), so no stage needs a wait here.
 #pragma unroll
-        for (int s = 0; s < kStages - 1; ++s) {
+        for (int s = 0; s < kDepth; ++s) {
             if (s < nk) load_stage(s, s);
             cp_async_commit();
         }
         for (int i = 0; i < nk; ++i) {
             const int s = i % kStages;
-            cp_async_wait<kStages - 2>();  // this thread's copies of chunk i have landed
+            cp_async_wait<kDepth - 1>();  // this thread's copies of chunk i have landed
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncthreads();  // ... and every thread's
             if (tid == 0) {
@@ -266,15 +268,15 @@ __global__ void __launch_bounds__(kGemmThreads, 2) k_umma_gemm(const GemmArgs g)
                                  smem_u32(&bar[s]))
                              : "memory");
                 ++commits[s];
-                // the stage the next load refills held chunk i - 1: its MMAs must be done
-                const int sp = (i + kStages - 1) % kStages;
-                if (i >= 1 && i + kStages - 1 < nk && !mbar_wait(smem_u32(&bar[sp]), (commits[sp] - 1) & 1))
+                // the stage the next load refills held chunk i + kDepth - kStages: its MMAs must be done
+                const int sp = (i + kDepth) % kStages;
+                if (i + kDepth >= kStages && i + kDepth < nk && !mbar_wait(smem_u32(&bar[sp]), (commits[sp] - 1) & 1))
                     abort_flag = 1;
             }
-            if (i + kStages - 1 < nk) {
+            if (i + kDepth < nk) {
                 __syncthreads();
                 if (abort_flag) break;
-                load_stage(i + kStages - 1, (i + kStages - 1) % kStages);
+                load_stage(i + kDepth, (i + kDepth) % kStages);
             }
             cp_async_commit();
         }
