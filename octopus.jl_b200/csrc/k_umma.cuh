@@ -9,7 +9,7 @@
 //
 // A CTA of 256 threads computes 128 x BN tiles (persistent over the M tiles of its column and K range, so
 // the TMEM allocation and the barriers are set up once): the K loop moves 64-wide chunks of A and B from global
-// memory into shared memory with 16-byte cp.async copies (four stages, three chunks in flight; zero-filled
+// memory into shared memory with 16-byte cp.async copies (four stages, two chunks in flight ahead; zero-filled
 // outside the matrix and the padded image) in the canonical no-swizzle K-major layout -- 8-row x 16-byte core
 // matrices, 128 contiguous bytes each, the two K halves of one instruction LBO = 128 bytes apart and 8-row
 // groups SBO = 1024 bytes apart -- and one thread issues four tcgen05.mma (M = 128, N = BN, K = 16) per
