@@ -26,7 +26,8 @@ def _device_beams(ob, e, p):
     return be, bp
 
 
-def run_both(solver, n1, n2, turns=1, e_sigma=None, p_sigma=None, seed=123456789, transform=None):
+def run_both(solver, n1, n2, turns=1, e_sigma=None, p_sigma=None, seed=123456789, transform=None, atol=None,
+             rtol=None):
     from oracle import oracle as orc
     ob = _gpu()
     e, p = beams(n1, n2, e_sigma, p_sigma, seed=seed)
@@ -43,7 +44,8 @@ def run_both(solver, n1, n2, turns=1, e_sigma=None, p_sigma=None, seed=123456789
         lum_o = oracle.collide(e, p, pe, pp)
         out.append(dict(lum_g=lum_g, lum_o=lum_o, cache_g=ctx.green_cache_stats(), cache_o=oracle.cache_stats(),
                         trace_g=ctx.pair_luminosity_trace(), trace_o=oracle.pair_trace(),
-                        e_err=within(be.numpy(), e, ATOL, RTOL), p_err=within(bp.numpy(), p, ATOL, RTOL),
+                        e_err=within(be.numpy(), e, atol or ATOL, rtol or RTOL),
+                        p_err=within(bp.numpy(), p, atol or ATOL, rtol or RTOL),
                         e_abs=float(np.abs(be.numpy() - e).max()), p_abs=float(np.abs(bp.numpy() - p).max())))
     rt.close()
     return out
@@ -271,3 +273,24 @@ def test_grid_extent_sigma_counts_particles_outside_its_meshes():
         assert abs(lum_g / lum_o - 1) <= 1e-10
         assert within(be.numpy(), e, ATOL, RTOL) <= 1.0 and within(bp.numpy(), p, ATOL, RTOL) <= 1.0
     rt.close()
+
+
+@pytest.mark.parametrize("kind", ["plain", "sigma", "hybrid", "hybrid_coupled"])
+def test_sparse_slices(kind):
+    """200 / 160 particles in 8 :equal_width slices: tail slices of two to a few particles, whose hybrid
+    covariance is rank-deficient (coupled: plain PIC, gaussian_pic.jl:525-536) and whose :sigma extents come from
+    a handful of samples (pic_cpu.jl:1581-1593); beams tilted by 0.05 rad so the coupled tolerance applies where
+    the covariance is resolved.  (A one-particle field slice has a zero-width extent whose mesh alignment turns on
+    rounding: the oracle alone moves such a particle's kick by ~2e-6 under one-ulp input changes, so no
+    implementation can meet 1e-10 there and this case avoids it.)  Coordinates at the contract's 1e-10; pair
+    luminosities at 1e-8: the overlap of two-particle slices moves by ~x/h (tens of cells) times the kicked
+    positions' relative differences."""
+    from helpers import tilt
+    ob = _gpu()
+    sl = ob.LongitudinalSlicing(nslices=8, method="equal_width")
+    s = {"plain": lambda: ob.PICPoissonSolver(grid=(32, 32), slicing=sl),
+         "sigma": lambda: ob.PICPoissonSolver(grid=(32, 32), slicing=sl, grid_extent="sigma"),
+         "hybrid": lambda: ob.GaussianPICPoissonSolver(grid=(32, 32), slicing=sl),
+         "hybrid_coupled": lambda: ob.GaussianPICPoissonSolver(grid=(32, 32), slicing=sl, coupling_tol=0.01)}[kind]()
+    check(run_both(s, 200, 160, turns=2, e_sigma=(95e-6, 8.5e-6, 7e-3), p_sigma=(95e-6, 8.5e-6, 6e-2),
+                   transform=lambda b: tilt(b, 0.05)), lum_rtol=1e-8)
