@@ -98,7 +98,8 @@ typedef struct {
     /* GaussianPoissonSolver, the soft-Gaussian strong-strong solver (src/tasks/strongstrong/gaussian.jl,
      * options interface.jl:949-1020): solver = OCTO_SOLVER_SOFT_GAUSSIAN runs it instead of the PIC solve
      * (the grid, deposit, Green and interaction-grid fields are then unused; kbb1/kbb2/lum_scale overrides,
-     * the slicings and longitudinal_kick keep their meaning).  FP64 beams only. */
+     * the slicings and longitudinal_kick keep their meaning).  Float64 beams, or float32 beams with precision = 1
+     * (stored in float, computed in FP64 as the reference promotes them). */
     int32_t solver;                    /* OCTO_SOLVER_PIC / OCTO_SOLVER_SOFT_GAUSSIAN */
     int32_t gaussian_when_luminosity;  /* 1 or 2: the beam whose slice is the Gaussian the luminosity samples */
     int32_t ignore_centroid1, ignore_centroid2;

@@ -37,7 +37,7 @@ struct GTask {
     double klum;            // weight of the source slice x luminosity scale of the field beam
 };
 struct GaussArgs {
-    double *c[2][6];        // slice-sorted coordinates of both beams
+    void *c[2][6];          // slice-sorted coordinates of both beams, element type R of the kernels
     const GSlice *slices;
     GMoments *mom;
     const GTask *tasks;
@@ -110,18 +110,26 @@ __device__ __forceinline__ void drift_reverse(int kind, bool lk, double &x, doub
     z += H0 / ps0 * S;
 }
 
+// R: the beams' element type.  float32 beams (the precision form) are read and written in float and computed in
+// FP64, as the reference promotes a Float32 beam's coordinates against the solver's Float64 moments and scales
+// (gaussian.jl:64-70) and rounds them once on store.
+template <class R>
+__device__ __forceinline__ R *gcol(const GaussArgs &A, int beam, int k) { return static_cast<R *>(A.c[beam][k]); }
+
+template <class R>
 __global__ void __launch_bounds__(kGaussThreads) k_gauss_sums(GaussArgs A) {
     pdl_wait();
     pdl_release();
     const int2 bm = A.blockmap[blockIdx.x];
     const GSlice S = A.slices[bm.x];
-    const double *const *c = A.c[S.beam];
+    const R *c[4] = {gcol<R>(A, S.beam, 0), gcol<R>(A, S.beam, 1), gcol<R>(A, S.beam, 2), gcol<R>(A, S.beam, 3)};
     const double x0 = c[0][S.start], px0 = c[1][S.start], y0 = c[2][S.start], py0 = c[3][S.start];
     double s[kGaussSums] = {};
     const long long end = min(S.n, (long long)bm.y + kGaussChunk);
     for (long long k = bm.y + threadIdx.x; k < end; k += kGaussThreads) {
         const long long i = S.start + k;
-        const double dx = c[0][i] - x0, dpx = c[1][i] - px0, dy = c[2][i] - y0, dpy = c[3][i] - py0;
+        const double dx = (double)c[0][i] - x0, dpx = (double)c[1][i] - px0, dy = (double)c[2][i] - y0,
+                     dpy = (double)c[3][i] - py0;
         s[0] += dx; s[1] += dpx; s[2] += dy; s[3] += dpy;
         s[4] += dx * dx; s[5] += dpx * dpx; s[6] += dy * dy; s[7] += dpy * dpy;
         s[8] += dx * dpx; s[9] += dy * dpy;
@@ -146,6 +154,7 @@ __global__ void __launch_bounds__(kGaussThreads) k_gauss_sums(GaussArgs A) {
 }
 
 // Block b0 .. b0 + nb - 1 of k_gauss_sums belong to slice blockIdx.x (first block index in first[]).
+template <class R>
 __global__ void k_gauss_moments(GaussArgs A, const int *first, const int *count) {
     pdl_wait();
     pdl_release();
@@ -165,8 +174,8 @@ __global__ void k_gauss_moments(GaussArgs A, const int *first, const int *count)
     for (int b = first[si]; b < first[si] + count[si]; ++b)
 #pragma unroll
         for (int q = 0; q < kGaussSums; ++q) s[q] += A.partial[(size_t)b * kGaussSums + q];
-    const double *const *c = A.c[S.beam];
-    const double x0 = c[0][S.start], px0 = c[1][S.start], y0 = c[2][S.start], py0 = c[3][S.start];
+    const double x0 = gcol<R>(A, S.beam, 0)[S.start], px0 = gcol<R>(A, S.beam, 1)[S.start],
+                 y0 = gcol<R>(A, S.beam, 2)[S.start], py0 = gcol<R>(A, S.beam, 3)[S.start];
     // slicing.jl:739-770: means from the shifted sums, variances muladd(-m, m, sum2 / n), floors
     const double invn = 1.0 / (double)S.n;
     const double dmx = s[0] * invn, dmpx = s[1] * invn, dmy = s[2] * invn, dmpy = s[3] * invn;
@@ -202,13 +211,16 @@ __global__ void k_gauss_moments(GaussArgs A, const int *first, const int *count)
 // Three blocks per SM (at most 85 registers): the Bassetti-Erskine response is an FP64 latency chain, and
 // occupancy hides it better than registers do (measured: 10.6 ms per production collide at one block per
 // SM, 9.4 at two, 9.0 at three).
+template <class R>
 __global__ void __launch_bounds__(kGaussThreads, 3) k_gauss_kick(GaussArgs A) {
     pdl_wait();
     pdl_release();
     const int2 bm = A.blockmap[blockIdx.x];
     const GTask T = A.tasks[bm.x];
     const GMoments M = A.mom[T.mom];
-    double *const *c = A.c[T.fld_beam];
+    R *c[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) c[q] = gcol<R>(A, T.fld_beam, q);
     const bool lk = A.longitudinal != 0;
     const double twopi = 6.283185307179586476925286766559005768394338;
     double dens = 0.0;
@@ -240,12 +252,12 @@ __global__ void __launch_bounds__(kGaussThreads, 3) k_gauss_kick(GaussArgs A) {
         if (lk) pz += 0.5 * ((px - px0) * M.mpx + (py - py0) * M.mpy);
         else pz = pz0;
         drift_reverse(A.drift, lk, x, px, y, py, z, pz, T.center);
-        c[0][i] = x;
-        c[1][i] = px;
-        c[2][i] = y;
-        c[3][i] = py;
-        c[4][i] = z;
-        c[5][i] = pz;
+        c[0][i] = (R)x;
+        c[1][i] = (R)px;
+        c[2][i] = (R)y;
+        c[3][i] = (R)py;
+        c[4][i] = (R)z;
+        c[5][i] = (R)pz;
         dens += density * twopi;
     }
     if (!T.lum) return;

@@ -475,8 +475,8 @@ int validate_options(const octo_pic_options &o, std::string &msg) {
             msg = "include_sigma_xy must be 0 or 1";
             return OCTO_ERR_ARG;
         }
-        if (o.precision != 0 || o.gaussian) {
-            msg = "the soft-Gaussian solver runs on float64 beams, without the PIC hybrid";
+        if (o.gaussian) {
+            msg = "the soft-Gaussian solver runs without the PIC hybrid (gaussian = 0)";
             return OCTO_ERR_UNSUPPORTED;
         }
     }
@@ -1625,7 +1625,7 @@ void CollideJob::run_gaussian(const SliceInfo &S1, const SliceInfo &S2) {
     const int *d_ltask = d_scount + scount.size(), *d_lfirst = d_ltask + ltask.size(), *d_lcount = d_lfirst + lfirst.size();
     GaussArgs A{};
     for (int b = 0; b < 2; ++b)
-        for (int k = 0; k < 6; ++k) A.c[b][k] = (double *)c->bw[b].s[k].p;
+        for (int k = 0; k < 6; ++k) A.c[b][k] = (void *)c->bw[b].s[k].p;
     A.slices = c->g_slices.p;
     A.mom = c->g_mom.p;
     A.tasks = c->g_tasks.p;
@@ -1645,12 +1645,16 @@ void CollideJob::run_gaussian(const SliceInfo &S1, const SliceInfo &S2) {
             GaussArgs As = A;
             As.blockmap = c->g_bmap.p + F.sb0;
             As.partial = c->g_partial.p + (size_t)F.sb0 * kGaussSums;
-            if (F.nsb) launch_pdl(k_gauss_sums, F.nsb, kGaussThreads, 0, st, As);
+            with_real(fp32, [&](auto r) {
+                if (F.nsb) launch_pdl(k_gauss_sums<decltype(r)>, F.nsb, kGaussThreads, 0, st, As);
+            });
             // moments: first[] is relative to the front's first sums block
             GaussArgs Am = A;
             Am.slices = c->g_slices.p + F.s0;
             Am.mom = c->g_mom.p + F.s0;
-            launch_pdl(k_gauss_moments, F.ns, 32, 0, st, Am, d_sfirst + F.s0, d_scount + F.s0);
+            with_real(fp32, [&](auto r) {
+                launch_pdl(k_gauss_moments<decltype(r)>, F.ns, 32, 0, st, Am, d_sfirst + F.s0, d_scount + F.s0);
+            });
             launches += (F.nsb ? 1 : 0) + 1;
         }
         {
@@ -1658,7 +1662,9 @@ void CollideJob::run_gaussian(const SliceInfo &S1, const SliceInfo &S2) {
             GaussArgs Ak = A;
             Ak.blockmap = c->g_bmap.p + smap.size() + F.kb0;
             Ak.lum_partial = c->g_lum_partial.p + F.kb0;
-            if (F.nkb) launch_pdl(k_gauss_kick, F.nkb, kGaussThreads, 0, st, Ak);
+            with_real(fp32, [&](auto r) {
+                if (F.nkb) launch_pdl(k_gauss_kick<decltype(r)>, F.nkb, kGaussThreads, 0, st, Ak);
+            });
             // the fold reads the kick partials by their index over all fronts (lfirst)
             if (F.nl) launch_pdl(k_gauss_lum, (F.nl + 31) / 32, 32, 0, st, A, d_ltask + F.l0, d_lfirst + F.l0,
                                  d_lcount + F.l0, F.nl);

@@ -91,7 +91,7 @@ end
 
 `GaussianPoissonSolver(; kwargs...)`, the soft-Gaussian strong-strong solver (interface.jl:949-1020,
 gaussian.jl), run on libocto_b200: the uncoupled or coupled (`include_sigma_xy`) covariance with the
-:hirata, :chromatic or :exact virtual drift, on Float64 beams.  `pic` only carries the slicings, kbb and luminosity-scale overrides and
+:hirata, :chromatic or :exact virtual drift, on Float64 or Float32 beams.  `pic` only carries the slicings, kbb and luminosity-scale overrides and
 `longitudinal_kick` into the shared options struct.
 """
 struct B200GaussianPoissonSolver{T<:Real} <: AbstractPoissonSolver

@@ -274,7 +274,8 @@ class GaussianPoissonSolver:
     """GaussianPoissonSolver(; ...) -- the soft-Gaussian strong-strong solver (interface.jl:949-1020,
     src/tasks/strongstrong/gaussian.jl): each slice pair kicks each slice with the Bassetti-Erskine field of a
     Gaussian carrying the other slice's transverse moments, uncoupled or with the full transverse covariance
-    (include_sigma_xy), with the :hirata, :chromatic and :exact virtual drifts, on float64 beams."""
+    (include_sigma_xy), with the :hirata, :chromatic and :exact virtual drifts, on float64 or float32 beams (the
+    latter stored in float and computed in FP64, as the reference promotes them against its Float64 moments)."""
     kbb1: Optional[float] = None
     kbb2: Optional[float] = None
     luminosity_scale: Optional[float] = None

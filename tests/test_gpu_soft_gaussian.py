@@ -11,8 +11,10 @@ from helpers import beams, oracle_params, within, E_PARAMS, P_PARAMS
 pytestmark = pytest.mark.gpu
 
 
-def run_both(solver, e, p, turns=1):
+def run_both(solver, e, p, turns=1, dtype=None):
     import octo_b200 as ob
+    import torch
+    dtype = dtype or torch.float64
     pe, pp = oracle_params()
     s1, s2 = solver.resolved_slicing1, solver.resolved_slicing2
     opt = orc.OracleOptions(nslices1=s1.nslices, nslices2=s2.nslices,
@@ -23,9 +25,9 @@ def run_both(solver, e, p, turns=1):
                             kbb1=solver.kbb1, kbb2=solver.kbb2, luminosity_scale=solver.luminosity_scale,
                             longitudinal_kick=solver.longitudinal_kick)
     be = ob.Beam.from_numpy(e, ob.BeamParams(E_PARAMS["charge"], E_PARAMS["mass"], E_PARAMS["energy"],
-                                             E_PARAMS["r0"], E_PARAMS["npart"]))
+                                             E_PARAMS["r0"], E_PARAMS["npart"]), dtype=dtype)
     bp = ob.Beam.from_numpy(p, ob.BeamParams(P_PARAMS["charge"], P_PARAMS["mass"], P_PARAMS["energy"],
-                                             P_PARAMS["r0"], P_PARAMS["npart"]))
+                                             P_PARAMS["r0"], P_PARAMS["npart"]), dtype=dtype)
     rt = ob.StrongStrongRuntime()
     oe, op = e.copy(), p.copy()
     lums = []
@@ -36,7 +38,7 @@ def run_both(solver, e, p, turns=1):
                                        solver.include_sigma_xy)
         lums.append((lum, lum_ref))
     rt.close()
-    return be.numpy(), bp.numpy(), oe, op, lums
+    return (be.coords.to(torch.float64).cpu().numpy(), bp.coords.to(torch.float64).cpu().numpy(), oe, op, lums)
 
 
 @pytest.mark.parametrize("kw", [
@@ -94,3 +96,25 @@ def test_nonfinite_and_unsupported():
     assert err.value.code == 1 and "source" in str(err.value)
     with pytest.raises(ob.ArgumentError):
         ob.GaussianPoissonSolver(virtual_drift="paraxial")
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(include_sigma_xy=True, virtual_drift="chromatic")])
+def test_float32_beams_match_oracle(kw):
+    """float32 beams: coordinates stored in float and computed in FP64 (the reference promotes a Float32 beam
+    against the solver's Float64 moments and scales), against the FP64 oracle on the same float32-rounded
+    inputs.  Each kick rounds the stored coordinates once, S times per collide (S the other beam's slices), so a
+    coordinate may differ by (S + 1) half-ulps of float32 of itself, plus a few ulps at its row's scale where it
+    is a small difference of larger drift terms; luminosity within 1e-6."""
+    import octo_b200 as ob
+    import torch
+    e, p = beams(40_000, 24_000)
+    e = e.astype(np.float32).astype(np.float64)
+    p = p.astype(np.float32).astype(np.float64)
+    solver = ob.GaussianPoissonSolver(slicing=ob.LongitudinalSlicing(nslices=7, method="normal_quantile"), **kw)
+    ge, gp, oe, op, lums = run_both(solver, e, p, turns=1, dtype=torch.float32)
+    bound = 8 * 2.0 ** -24
+    for g, o in ((ge, oe), (gp, op)):
+        for row in range(6):
+            scale = 4 * 2.0 ** -24 * np.max(np.abs(o[row]))
+            assert np.max(np.abs(g[row] - o[row]) / (bound * np.abs(o[row]) + scale)) <= 1.0, row
+    assert abs(lums[0][0] / lums[0][1] - 1.0) < 1e-6, lums
