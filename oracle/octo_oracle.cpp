@@ -1087,8 +1087,60 @@ void virtual_positions(const Coords &src, double sM, std::vector<double> &vx, st
 }
 
 // pic_cpu.jl:954-1144
+// interaction_grid = :source_slice (pic_cpu.jl:610-712): the mesh of every pair of a (source slice, direction)
+// is sized from one union box taken at the slice's first use -- the source drifted across the partner beam's
+// whole longitudinal range, every partner particle drifted to its collision point -- while the Green cache's
+// coverage test still sees this pair's own bounds.
+struct UnionBounds {
+    bool valid = false;
+    Bounds sb{}, fb{};
+};
+
+// _pic_union_bounds, the states form the collide loop uses (pic_cpu.jl:665-692), and its source tail
+// (pic_cpu.jl:697-712).  The partner's z range and collision-point extrema come from its CURRENT slice states,
+// so the box depends on how much of the turn has been applied; the source is bounded at its two extreme drifts
+// (the drift is affine in s).  Invalid -- no override, per-pair sizing -- when the partner has no finite z.
+UnionBounds union_bounds(const Coords &source, double center, const std::vector<Coords> &partner) {
+    UnionBounds u;
+    const double c = center;
+    double zmin = INFINITY, zmax = -INFINITY;
+    double fxmin = INFINITY, fxmax = -INFINITY, fymin = INFINITY, fymax = -INFINITY;
+    for (const Coords &fc : partner)
+        for (size_t k = 0; k < fc.size(); ++k) {
+            const double zi = fc.z[k];
+            zmin = jmin(zmin, zi); zmax = jmax(zmax, zi);
+            const double s = 0.5 * (zi - c);
+            const double xv = fc.x[k] + s * fc.px[k], yv = fc.y[k] + s * fc.py[k];
+            fxmin = jmin(fxmin, xv); fxmax = jmax(fxmax, xv);
+            fymin = jmin(fymin, yv); fymax = jmax(fymax, yv);
+        }
+    if (std::isnan(zmin) || !(std::isfinite(fxmin) && std::isfinite(fxmax) && std::isfinite(fymin) &&
+                              std::isfinite(fymax)))
+        for (const Coords &fc : partner)
+            for (size_t k = 0; k < fc.size(); ++k)
+                if (!std::isfinite(fc.z[k]) || !std::isfinite(fc.x[k]) || !std::isfinite(fc.px[k]) ||
+                    !std::isfinite(fc.y[k]) || !std::isfinite(fc.py[k]))
+                    nonfinite("field", fc, "source-slice union bounds");
+    if (!std::isfinite(zmin)) return u;
+    const double sA = 0.5 * (c - zmax), sB = 0.5 * (c - zmin);
+    double sxmin = INFINITY, sxmax = -INFINITY, symin = INFINITY, symax = -INFINITY;
+    for (size_t k = 0; k < source.size(); ++k) {
+        const double xa = source.x[k] + source.px[k] * sA, xb = source.x[k] + source.px[k] * sB;
+        const double ya = source.y[k] + source.py[k] * sA, yb = source.y[k] + source.py[k] * sB;
+        sxmin = jmin(jmin(sxmin, xa), xb); sxmax = jmax(jmax(sxmax, xa), xb);
+        symin = jmin(jmin(symin, ya), yb); symax = jmax(jmax(symax, ya), yb);
+    }
+    if (!(std::isfinite(sxmin) && std::isfinite(sxmax) && std::isfinite(symin) && std::isfinite(symax)))
+        nonfinite("source", source, "source-slice union bounds");
+    u.valid = true;
+    u.sb = {sxmin, sxmax, symin, symax};
+    u.fb = {fxmin, fxmax, fymin, fymax};
+    return u;
+}
+
 void interaction(Ctx &C, Workspace &ws, const Coords &source, const SliceParam &ps, Coords &field,
-                 const SliceParam &pf, double kbb, int i, int j, int dir, int vslot, int64_t counters[3]) {
+                 const SliceParam &pf, double kbb, int i, int j, int dir, int vslot, int64_t counters[3],
+                 const UnionBounds *over = nullptr) {
     const Options &O = C.O;
     const int nsource = (int)source.size(), nfield = (int)field.size();
     double sL = 0.5 * (ps.center - pf.lb);
@@ -1140,11 +1192,19 @@ void interaction(Ctx &C, Workspace &ws, const Coords &source, const SliceParam &
         nonfinite("field", field, pair_ctx(i, j, dir));
 
     Grid sg, fg;
-    interaction_grids(O, sxmin, sxmax, symin, symax, fxmin, fxmax, fymin, fymax, sg, fg);
+    if (over && over->valid)
+        interaction_grids(O, over->sb.xmin, over->sb.xmax, over->sb.ymin, over->sb.ymax, over->fb.xmin, over->fb.xmax,
+                          over->fb.ymin, over->fb.ymax, sg, fg);
+    else
+        interaction_grids(O, sxmin, sxmax, symin, symax, fxmin, fxmax, fymin, fymax, sg, fg);
     Bounds sb{sxmin, sxmax, symin, symax}, fb{fxmin, fxmax, fymin, fymax};
     std::vector<cplx> own;
-    const std::vector<cplx> &gfft = slice_pair_green(C, ws, i, j, dir, sg, fg, sb, fb, own, counters);
-    if (ge != 0) {
+    // :source_slice caches one mesh per (source slice, direction) -- the keys (i, 0, 1) and (j, 0, 2) of
+    // pic_cpu.jl:372-373 -- held in the slot of partner slice 1
+    const bool shared = O.o.interaction_grid == 1;
+    const std::vector<cplx> &gfft = slice_pair_green(C, ws, shared && dir == 2 ? 1 : i, shared && dir == 1 ? 1 : j,
+                                                     dir, sg, fg, sb, fb, own, counters);
+    if (ge != 0 || O.o.interaction_grid == 1) {
         ws.dropped += count_outside(field.x, field.y, fg.x0, fg.x0 + fg.width, fg.y0, fg.y0 + fg.height);
         ws.dropped += count_outside_drifted(source, sL, sR, sg.x0, sg.x0 + sg.width, sg.y0, sg.y0 + sg.height);
     }
@@ -1771,7 +1831,7 @@ void validate(const Options &O) {
     if (o.nx < 5 || o.ny < 5) throw OracleError(OO_ERR_ARG, "PICPoissonSolver grid must be at least (5, 5)");
     if (o.deposit_method < 0 || o.deposit_method > 1) throw OracleError(OO_ERR_ARG, "deposit_method");
     if (o.green_type < 0 || o.green_type > 1) throw OracleError(OO_ERR_UNSUPPORTED, "green_type");
-    if (o.interaction_grid != 0 && o.interaction_grid != 2) throw OracleError(OO_ERR_UNSUPPORTED, "interaction_grid");
+    if (o.interaction_grid < 0 || o.interaction_grid > 2) throw OracleError(OO_ERR_UNSUPPORTED, "interaction_grid");
     if (o.interaction_grid != 0 && o.grid_extent != 0)
         throw OracleError(OO_ERR_UNSUPPORTED, "grid_extent != :extrema with interaction_grid != :slice_pair");
     if (o.interaction_grid == 2 && o.slice_interpolation != 0)
@@ -1859,8 +1919,17 @@ double collide(Ctx &C, double *b1[6], int64_t n1, double *b2[6], int64_t n2, con
     for (size_t p = 0; p < npairs; ++p) pos_of[(size_t)(order[p].i - 1) * ns2 + (order[p].j - 1)] = (int)p;
     std::vector<double> lum_parts(npairs, 0.0);
     std::vector<char> ran(npairs, 0);
-    auto batches = pair_batches(s1.center, s2.center);
+    // :source_slice runs the pairs one at a time in collision order (pic_cpu.jl:54, 240-248): its union boxes are
+    // taken at each source slice's first use, from the states as that pair finds them
+    const bool shared = O.o.interaction_grid == 1;
+    std::vector<std::vector<OrderEntry>> batches;
+    if (shared)
+        for (const OrderEntry &e : order) batches.push_back({e});
+    else
+        batches = pair_batches(s1.center, s2.center);
     std::vector<std::array<int64_t, 3>> counters(npairs, {0, 0, 0});
+    std::vector<UnionBounds> ub1(shared ? ns1 : 0), ub2(shared ? ns2 : 0);
+    std::vector<char> ub1_done(shared ? ns1 : 0, 0), ub2_done(shared ? ns2 : 0, 0);
 
     for (auto &batch : batches) {
 #pragma omp parallel for num_threads(nthreads) schedule(dynamic)
@@ -1900,9 +1969,16 @@ double collide(Ctx &C, double *b1[6], int64_t n1, double *b2[6], int64_t n2, con
                     interaction_gaussian(C, ws, coord1, pa1, field2, pa2, kbb2, i, j, 1, 0, counters[p].data());
                     interaction_gaussian(C, ws, coord2, pa2, coord1, pa1, kbb1, i, j, 2, 1, counters[p].data());
                 } else {
-                    interaction(C, ws, coord1, pa1, field2, pa2, kbb2, i, j, 1, 0, counters[p].data());
+                    const UnionBounds *ov1 = nullptr, *ov2 = nullptr;
+                    if (shared) {  // both boxes before either direction kicks (pic_cpu.jl:368-371)
+                        if (!ub1_done[i - 1]) { ub1[i - 1] = union_bounds(coord1, pa1.center, state2); ub1_done[i - 1] = 1; }
+                        if (!ub2_done[j - 1]) { ub2[j - 1] = union_bounds(coord2, pa2.center, state1); ub2_done[j - 1] = 1; }
+                        ov1 = &ub1[i - 1];
+                        ov2 = &ub2[j - 1];
+                    }
+                    interaction(C, ws, coord1, pa1, field2, pa2, kbb2, i, j, 1, 0, counters[p].data(), ov1);
                     arm(2);
-                    interaction(C, ws, coord2, pa2, coord1, pa1, kbb1, i, j, 2, 1, counters[p].data());
+                    interaction(C, ws, coord2, pa2, coord1, pa1, kbb1, i, j, 2, 1, counters[p].data(), ov2);
                 }
                 ws.cap = nullptr;
                 ws.cap_kind = -1;
@@ -2126,6 +2202,26 @@ int32_t oo_pair_batches(const double *c1, int32_t ns1, const double *c2, int32_t
     for (size_t bi = 0; bi < batches.size(); ++bi)
         for (auto &p : batches[bi]) { batch_of[k] = (int)bi; pi[k] = p.i; pj[k] = p.j; ++k; }
     return (int32_t)batches.size();
+}
+
+int32_t oo_union_bounds(const double *src[4], int64_t ns, double center, const double *part[5], int64_t np,
+                        double out[8], int32_t *valid) {
+    Coords a, b;
+    a.resize((size_t)ns);
+    b.resize((size_t)np);
+    for (int64_t k = 0; k < ns; ++k) { a.x[k] = src[0][k]; a.px[k] = src[1][k]; a.y[k] = src[2][k]; a.py[k] = src[3][k]; }
+    for (int64_t k = 0; k < np; ++k) {
+        b.x[k] = part[0][k]; b.px[k] = part[1][k]; b.y[k] = part[2][k]; b.py[k] = part[3][k]; b.z[k] = part[4][k];
+    }
+    try {
+        UnionBounds u = union_bounds(a, center, std::vector<Coords>{b});
+        *valid = u.valid;
+        const double v[8] = {u.sb.xmin, u.sb.xmax, u.sb.ymin, u.sb.ymax, u.fb.xmin, u.fb.xmax, u.fb.ymin, u.fb.ymax};
+        for (int k = 0; k < 8; ++k) out[k] = v[k];
+    } catch (OracleError &e) {
+        return e.code;
+    }
+    return OO_OK;
 }
 
 void *oo_create(const oo_options *opt) {

@@ -40,7 +40,7 @@ typedef struct {
     int32_t green_cache;               /* 0 = :none, 1 = :slice_pair */
     int32_t field_derivative;          /* 2 = :second, 4 = :fourth */
     int32_t slice_interpolation;       /* 0 = :linear, 1 = :quadratic */
-    int32_t interaction_grid;          /* 0 = :slice_pair, 2 = :node */
+    int32_t interaction_grid;          /* 0 = :slice_pair, 1 = :source_slice, 2 = :node */
     int32_t grid_extent;               /* 0 = :extrema, 1 = :sigma */
     double grid_extent_sigma;
     double min_extent_x, min_extent_y; /* min_transverse_extent */
@@ -125,6 +125,12 @@ void oo_julia_range(double start, double stop, int64_t len, double *out);
    of batches; returns the number of batches. */
 int32_t oo_pair_batches(const double *c1, int32_t ns1, const double *c2, int32_t ns2, int32_t *batch_of,
                         int32_t *pi, int32_t *pj, int32_t *order_i, int32_t *order_j);
+
+/* The :source_slice union box of one source slice (x, px, y, py) against a partner beam (x, px, y, py, z):
+   out = source (xmin, xmax, ymin, ymax) then field (xmin, xmax, ymin, ymax); *valid = 0 when the partner has
+   no finite z.  Returns OO_OK or the error code of a non-finite coordinate. */
+int32_t oo_union_bounds(const double *src[4], int64_t ns, double center, const double *part[5], int64_t np,
+                        double out[8], int32_t *valid);
 
 /* A collide context keeps the slice-pair Green cache across calls, as task.runtime_cache does. */
 void *oo_create(const oo_options *opt);

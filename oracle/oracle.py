@@ -118,6 +118,8 @@ def lib():
         L.oo_julia_range.argtypes = [d, d, i64, P(d)]
         L.oo_pair_batches.restype = i32
         L.oo_pair_batches.argtypes = [P(d), i32, P(d), i32, P(i32), P(i32), P(i32), P(i32), P(i32)]
+        L.oo_union_bounds.restype = i32
+        L.oo_union_bounds.argtypes = [P(P(d)), i64, d, P(P(d)), i64, P(d), P(i32)]
         L.oo_create.restype = vp
         L.oo_create.argtypes = [P(OOOptions)]
         L.oo_destroy.argtypes = [vp]
@@ -161,7 +163,7 @@ _SYM = {
     "green_cache": {"none": 0, "slice_pair": 1},
     "field_derivative": {"second": 2, "fourth": 4},
     "slice_interpolation": {"linear": 0, "quadratic": 1},
-    "interaction_grid": {"slice_pair": 0, "node": 2},
+    "interaction_grid": {"slice_pair": 0, "source_slice": 1, "node": 2},
     "grid_extent": {"extrema": 0, "sigma": 1},
     "method": {"normal_quantile": 0, "gaussian": 0, "Gaussian": 0, "specified": 1, "equal_area": 2,
                "equal_count": 3, "equal_width": 4, "equal_spaced": 4},
@@ -379,6 +381,23 @@ def slices(z, ns, method="normal_quantile", center_position="centroid", position
     if rc != OK:
         raise OracleErrorPy(rc, "slicing")
     return b, c, w, cnt, order
+
+
+def union_bounds(source, center, partner):
+    """The :source_slice union box (pic_cpu.jl:665-712) of a source slice, rows (x, px, y, py), against a
+    partner, rows (x, px, y, py, z): ((sxmin, sxmax, symin, symax), (fxmin, fxmax, fymin, fymax)), or None when
+    the partner has no finite z."""
+    P = C.POINTER(C.c_double)
+    src = [np.ascontiguousarray(source[k], np.float64) for k in range(4)]
+    par = [np.ascontiguousarray(partner[k], np.float64) for k in range(5)]
+    a = (P * 4)(*[_dp(v) for v in src])
+    b = (P * 5)(*[_dp(v) for v in par])
+    out = (C.c_double * 8)()
+    valid = C.c_int32()
+    rc = lib().oo_union_bounds(a, src[0].size, float(center), b, par[0].size, out, C.byref(valid))
+    if rc != OK:
+        raise OracleErrorPy(rc, "source-slice union bounds")
+    return (tuple(out[:4]), tuple(out[4:])) if valid.value else None
 
 
 def pair_batches(c1, c2):
