@@ -40,6 +40,7 @@ extern "C" {
 #define OCTO_CACHE_NONE 0
 #define OCTO_CACHE_SLICE_PAIR 1
 #define OCTO_GRID_SLICE_PAIR 0
+#define OCTO_GRID_SOURCE_SLICE 1    /* one union-sized mesh per source slice; pairs run in collision order */
 #define OCTO_GRID_NODE 2
 #define OCTO_SLICING_NORMAL_QUANTILE 0
 #define OCTO_SLICING_SPECIFIED 1
@@ -74,7 +75,7 @@ typedef struct {
     int32_t green_cache;               /* OCTO_CACHE_* */
     int32_t field_derivative;          /* 2 = :second, 4 = :fourth */
     int32_t slice_interpolation;       /* 0 = :linear, 1 = :quadratic */
-    int32_t interaction_grid;          /* OCTO_GRID_* (:source_slice is CPU-only in the reference too) */
+    int32_t interaction_grid;          /* OCTO_GRID_* */
     int32_t grid_extent;               /* 0 = :extrema (the reference CUDA backend rejects :sigma) */
     double grid_extent_sigma;
     double min_extent_x, min_extent_y; /* min_transverse_extent */

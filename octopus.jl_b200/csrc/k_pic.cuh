@@ -55,6 +55,12 @@ struct Collide {           // device pointers for one collide (passed by value)
     double *hprof;               // [plane-in-front][3][nx + ny] reference-Gaussian node profiles (gx | gy, then the
                                  // coupled subtraction's m1x | dgy and m2x | ddgy)
     double *hsum;                // [plane-in-front][2] profile sums
+    // interaction_grid = :source_slice: per (direction, source slice) union box, row Task::ub of kUnionRow ordered
+    // words (partner z min/max, partner collision-point x and y min/max, source x and y min/max over both extreme
+    // drifts), its flags (kUnion*) and both beams' slice ranges slr[beam][slice] = (start, count)
+    unsigned long long *ubox;
+    int *uflag;
+    const long long *slr;
 };
 
 // ------------------------------------------------------------------ bounds
@@ -178,6 +184,93 @@ __global__ void __launch_bounds__(256) k_pair_bounds(Collide C, int task0) {
         if (any_f) atomicOr(&C.nanflag[side == 0 ? t2 : t1], 2);
         if (any_l) atomicOr(&C.nanflag[side == 0 ? t1 : t2], 4);
     }
+}
+
+// ------------------------------------------------------------------ :source_slice union boxes
+// Block-wide min/max of nq quantities into dst[2q] (min) and dst[2q + 1] (max), as ordered words.
+template <class R>
+__device__ __forceinline__ void reduce_ordered(const R *mn, const R *mx, int nq, unsigned long long *dst) {
+    __shared__ unsigned long long red[8][8];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int q = 0; q < nq; ++q) {
+        unsigned long long a = shfl_min_u64(mn[q] == R(INFINITY) ? kOrdMinInit : ord_encode((double)mn[q]));
+        unsigned long long b = shfl_max_u64(mx[q] == R(-INFINITY) ? kOrdMaxInit : ord_encode((double)mx[q]));
+        if (lane == 0) { red[warp][2 * q] = a; red[warp][2 * q + 1] = b; }
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * nq) {
+        const int k = threadIdx.x;
+        unsigned long long r = red[0][k];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) r = (k & 1) ? max(r, red[w][k]) : min(r, red[w][k]);
+        if (k & 1) atomicMax(dst + k, r); else atomicMin(dst + k, r);
+    }
+}
+
+// _pic_union_bounds, states form (pic_cpu.jl:665-692), for the tasks of a front that are their source slice's
+// first use: every sliced particle of the partner (field) beam, as the pair finds it, drifted to its collision
+// point with the source slice, x + 0.5*(z - c_src)*px.  Flags: kUnionTrig when a drifted position is not finite
+// or z is NaN (the reference's trigger), kUnionBad when an input coordinate is not finite (its search for the
+// offending slice); both set is its error.  grid: (blocks per slice, kMaxSlices, tasks of the front).
+template <class R>
+__global__ void __launch_bounds__(256) k_union_partner(Collide C, int task0) {
+    pdl_wait();
+    pdl_release();
+    const Task &T = C.tasks[task0 + blockIdx.z];
+    if (!T.ub_first) return;
+    const int fb = T.fld_beam, sl = blockIdx.y;
+    const long long *r = C.slr + ((long long)fb * kMaxSlices + sl) * 2;
+    const long long st = r[0], n = r[1];
+    if ((long long)blockIdx.x * blockDim.x >= n) return;  // block-uniform
+    const SoA S = C.beam[fb];
+    const R *X = col<R>(S, 0) + st, *PX = col<R>(S, 1) + st, *Y = col<R>(S, 2) + st, *PY = col<R>(S, 3) + st,
+            *Z = col<R>(S, 4) + st;
+    const R c = (R)T.c_src;
+    R mn[3] = {R(INFINITY), R(INFINITY), R(INFINITY)}, mx[3] = {R(-INFINITY), R(-INFINITY), R(-INFINITY)};
+    bool trig = false, bad = false;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const R x = X[k], px = PX[k], y = Y[k], py = PY[k], z = Z[k];
+        const R s = R(0.5) * (z - c);
+        const R xv = x + s * px, yv = y + s * py;
+        trig |= (z != z) | !isfinite(xv) | !isfinite(yv);
+        bad |= !isfinite(x) | !isfinite(px) | !isfinite(y) | !isfinite(py) | !isfinite(z);
+        mn[0] = fmin(mn[0], z); mx[0] = fmax(mx[0], z);
+        mn[1] = fmin(mn[1], xv); mx[1] = fmax(mx[1], xv);
+        mn[2] = fmin(mn[2], yv); mx[2] = fmax(mx[2], yv);
+    }
+    const int any_t = __syncthreads_or(trig), any_b = __syncthreads_or(bad);
+    reduce_ordered<R>(mn, mx, 3, C.ubox + (long long)T.ub * kUnionRow);
+    if (threadIdx.x == 0 && (any_t || any_b)) atomicOr(&C.uflag[T.ub], (any_t ? kUnionTrig : 0) | (any_b ? kUnionBad : 0));
+}
+
+// _pic_union_bounds_tail (pic_cpu.jl:697-712): the source slice at the two extreme drifts of the partner's z
+// range, sA = 0.5*(c - zmax) and sB = 0.5*(c - zmin) (the drift is affine in s, so they bound every other).
+// No box -- per-pair sizing -- when the partner's zmin is not finite.  grid: (blocks, tasks of the front).
+template <class R>
+__global__ void __launch_bounds__(256) k_union_source(Collide C, int task0) {
+    pdl_wait();
+    pdl_release();
+    const Task &T = C.tasks[task0 + blockIdx.y];
+    if (!T.ub_first) return;
+    unsigned long long *row = C.ubox + (long long)T.ub * kUnionRow;
+    const double zmin = ord_decode(row[0]), zmax = ord_decode(row[1]);
+    if (!isfinite(zmin) || (C.uflag[T.ub] & (kUnionTrig | kUnionBad)) == (kUnionTrig | kUnionBad)) return;
+    const SoA S = C.beam[T.src_beam];
+    const long long st = T.src_start, n = T.src_n;
+    const R *X = col<R>(S, 0) + st, *PX = col<R>(S, 1) + st, *Y = col<R>(S, 2) + st, *PY = col<R>(S, 3) + st;
+    const R c = (R)T.c_src;
+    const R sA = R(0.5) * (c - (R)zmax), sB = R(0.5) * (c - (R)zmin);
+    R mn[2] = {R(INFINITY), R(INFINITY)}, mx[2] = {R(-INFINITY), R(-INFINITY)};
+    bool nan = false;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const R x = X[k], px = PX[k], y = Y[k], py = PY[k];
+        const R xa = x + px * sA, xb = x + px * sB, ya = y + py * sA, yb = y + py * sB;
+        nan |= !isfinite(xa) | !isfinite(xb) | !isfinite(ya) | !isfinite(yb);
+        mn[0] = fmin(mn[0], fmin(xa, xb)); mx[0] = fmax(mx[0], fmax(xa, xb));
+        mn[1] = fmin(mn[1], fmin(ya, yb)); mx[1] = fmax(mx[1], fmax(ya, yb));
+    }
+    const int any = __syncthreads_or(nan);
+    reduce_ordered<R>(mn, mx, 2, row + 6);
+    if (threadIdx.x == 0 && any) atomicOr(&C.uflag[T.ub], kUnionSrcBad);
 }
 
 // Block-wide reduction of a thread's virtual-position extrema into a pair's luminosity box (ordered
@@ -355,6 +448,15 @@ __global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0, int 
     const unsigned long long *b = C.bnd + (long long)t * 8;
     double sxmin = ord_decode(b[0]), sxmax = ord_decode(b[1]), symin = ord_decode(b[2]), symax = ord_decode(b[3]);
     double fxmin = ord_decode(b[4]), fxmax = ord_decode(b[5]), fymin = ord_decode(b[6]), fymax = ord_decode(b[7]);
+    if (C.o.shared_grid) {
+        // :source_slice: a non-finite coordinate met by the union box comes first in the pair (pic_cpu.jl:368-371,
+        // before either interaction): recorded on the pair's direction-1 task with role 0
+        const int uf = C.uflag[T.ub];
+        if ((uf & (kUnionTrig | kUnionBad)) == (kUnionTrig | kUnionBad) || (uf & kUnionSrcBad)) {
+            record_error(C.status, T.dir == 1 ? t : t - 1, 1, 0);
+            return;
+        }
+    }
     int nf = C.nanflag[t];
     if ((nf & 1) || !(isfinite(sxmin) && isfinite(sxmax) && isfinite(symin) && isfinite(symax))) {
         record_error(C.status, t, 1, 1);
@@ -454,7 +556,15 @@ __global__ void k_plan(Collide C, int task0, int ntasks, int slot_scratch0, int 
         }
     }
     Grid sg, fg;
-    if (!interaction_grids(C.o, sxmin, sxmax, symin, symax, fxmin, fxmax, fymin, fymax, sg, fg)) {
+    // :source_slice: the mesh is sized from the source slice's union box (pic_cpu.jl:1036-1048), while the cache's
+    // coverage test below keeps this pair's own bounds.
+    double gs[4] = {sxmin, sxmax, symin, symax}, gf[4] = {fxmin, fxmax, fymin, fymax};
+    if (C.o.shared_grid) {
+        const unsigned long long *row = C.ubox + (long long)T.ub * kUnionRow;
+        if (isfinite(ord_decode(row[0])))
+            for (int q = 0; q < 4; ++q) { gf[q] = ord_decode(row[2 + q]); gs[q] = ord_decode(row[6 + q]); }
+    }
+    if (!interaction_grids(C.o, gs[0], gs[1], gs[2], gs[3], gf[0], gf[1], gf[2], gf[3], sg, fg)) {
         record_error(C.status, t, 3, 0);
         return;
     }
@@ -955,7 +1065,7 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
             const R yd = cy + cpy * s;
             if (count_dropped && !(isfinite(xd) && xlo <= xd && xd <= xhi && isfinite(yd) && ylo <= yd && yd <= yhi))
                 ++outside;
-            else if (count_dropped == 2) {  // :slice_pair under :sigma: the particle at the other boundary too
+            else if (count_dropped == 2) {  // :sigma and :source_slice: the particle at the other boundary too
                 const R x2 = cx + cpx * s2, y2 = cy + cpy * s2;
                 if (!(isfinite(x2) && xlo <= x2 && x2 <= xhi && isfinite(y2) && ylo <= y2 && y2 <= yhi)) ++outside;
             }
@@ -1944,7 +2054,8 @@ __device__ __forceinline__ void kick_particle(const Collide &C, const KickJob<R>
     const R zL = jclamp(-z * J.hzi + J.zbias, R(0), R(1));
     const R zR = R(1) - zL;
     const R ks = J.ks;
-    if (!o.node && o.grid_extent) {  // :sigma field meshes need not cover every field particle (pic_cpu.jl:1060-1090)
+    // :sigma and :source_slice field meshes need not cover every field particle (pic_cpu.jl:1060-1090)
+    if (!o.node && (o.grid_extent || o.shared_grid)) {
         const GridR<R> &gF = J.gL;
         if (!(isfinite(x) && gF.x0 <= x && x <= gF.x0 + gF.w && isfinite(y) && gF.y0 <= y && y <= gF.y0 + gF.h))
             atomicAdd((unsigned long long *)&C.status->dropped, 1ull);

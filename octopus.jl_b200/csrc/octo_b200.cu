@@ -295,6 +295,9 @@ struct octo_ctx {
     DevBuf<HybridTask> hyb;            // Gaussian-subtracted hybrid state per task
     DevBuf<double> hmom, hprof, hsum;  // its moment partials, node profiles and profile sums
     DevBuf<double> esum;               // grid_extent = :sigma: per-block sums of the drifted offsets
+    DevBuf<unsigned long long> ubox;   // :source_slice: union box per (direction, source slice)
+    DevBuf<int> uflag;                 // ... and its non-finite flags
+    DevBuf<long long> slr;             // ... both beams' slice ranges (start, count)
     DevBuf<double> mom_partial, mom_means;  // beam moment rows: block partials and the means
     // soft-Gaussian solver: slices, their moments, kick tasks, block maps, partial sums
     DevBuf<GSlice> g_slices;
@@ -409,14 +412,15 @@ int validate_options(const octo_pic_options &o, std::string &msg) {
     if (o.green_cache != OCTO_CACHE_NONE && o.green_cache != OCTO_CACHE_SLICE_PAIR) { msg = "green_cache must be :none or :slice_pair"; return OCTO_ERR_ARG; }
     if (o.field_derivative != 2 && o.field_derivative != 4) { msg = "field_derivative must be :second or :fourth"; return OCTO_ERR_ARG; }
     if (o.slice_interpolation != 0 && o.slice_interpolation != 1) { msg = "slice_interpolation must be :linear or :quadratic"; return OCTO_ERR_ARG; }
-    if (o.interaction_grid != OCTO_GRID_SLICE_PAIR && o.interaction_grid != OCTO_GRID_NODE) {
-        msg = "interaction_grid = :source_slice is implemented only by the CPU PICPoissonSolver path (pic_cpu.jl:730-809)";
-        return OCTO_ERR_UNSUPPORTED;
+    if (o.interaction_grid != OCTO_GRID_SLICE_PAIR && o.interaction_grid != OCTO_GRID_SOURCE_SLICE &&
+        o.interaction_grid != OCTO_GRID_NODE) {
+        msg = "interaction_grid must be :slice_pair, :source_slice or :node";
+        return OCTO_ERR_ARG;
     }
     if (o.grid_extent != 0 && o.grid_extent != 1) { msg = "grid_extent must be :extrema or :sigma"; return OCTO_ERR_ARG; }
     if (o.grid_extent == 1 && o.interaction_grid != OCTO_GRID_SLICE_PAIR) {  // pic_cpu.jl:545-558
-        msg = "grid_extent = :sigma is implemented for interaction_grid = :slice_pair only: :node sizes its meshes "
-              "from per-node extrema and applies no extent estimator";
+        msg = "grid_extent = :sigma is implemented for interaction_grid = :slice_pair only: :source_slice and :node "
+              "size their meshes from union or per-node extrema and apply no extent estimator";
         return OCTO_ERR_UNSUPPORTED;
     }
     if (o.grid_extent == 1 && !(o.grid_extent_sigma > 0.0)) { msg = "grid_extent_sigma must be positive"; return OCTO_ERR_ARG; }
@@ -1036,7 +1040,16 @@ void CollideJob::run() {
 
     // ---- schedule (slicing.jl:561-647), skipping pairs with an empty slice (pic_cpu.jl:302)
     order = collision_order(S1.center, ns1, S2.center, ns2);
-    batches = pair_batches(order, ns1, ns2);
+    // :source_slice runs one pair per front in collision order (pic_cpu.jl:54, 240-248): a source slice's union
+    // box is taken at its first use, from the beams as that pair finds them
+    const bool shared = c->dopt.shared_grid != 0;
+    if (shared) {
+        batches.clear();
+        for (const OrderEntry &e : order) batches.push_back({e});
+    } else {
+        batches = pair_batches(order, ns1, ns2);
+    }
+    std::vector<char> ub_seen(shared ? ns1 + ns2 : 0, 0);
     std::vector<int> pos_of((size_t)ns1 * ns2);
     for (size_t p = 0; p < order.size(); ++p) pos_of[(size_t)(order[p].i - 1) * ns2 + (order[p].j - 1)] = (int)p;
 
@@ -1084,7 +1097,13 @@ void CollideJob::run() {
                 T.fld_beam = 2 - dir;
                 const SliceInfo &SS = dir == 1 ? S1 : S2, &SF = dir == 1 ? S2 : S1;
                 const int ss = dir == 1 ? i - 1 : j - 1, sf = dir == 1 ? j - 1 : i - 1;
-                T.key = ((dir - 1) * ns1 + (i - 1)) * ns2 + (j - 1);
+                // :source_slice keeps one cache entry per (source slice, direction), the keys (i, 0, 1) and
+                // (j, 0, 2) of pic_cpu.jl:372-373, in the slot of partner slice 1
+                T.key = shared ? (dir == 1 ? (i - 1) * ns2 : ns1 * ns2 + (j - 1))
+                               : ((dir - 1) * ns1 + (i - 1)) * ns2 + (j - 1);
+                T.ub = dir == 1 ? i - 1 : ns1 + (j - 1);
+                T.ub_first = shared && !ub_seen[T.ub];
+                if (shared) ub_seen[T.ub] = 1;
                 T.pair = p;
                 T.front = (int)f;
                 T.src_start = SS.start[ss]; T.src_n = SS.count[ss];
@@ -1126,9 +1145,9 @@ void CollideJob::run() {
                         P.s = k == 0 ? T.sL : (k == 1 ? T.sR : 0.5 * (T.sL + T.sR));
                         P.geom = -1;
                         P.green = -1;
-                        // :sigma meshes need not cover the source: count particles outside at either drift once
-                        // (the L plane checks both)
-                        P.count_dropped = (c->dopt.grid_extent && k == 0) ? 2 : 0;
+                        // :sigma and :source_slice meshes need not cover the source: count particles outside at
+                        // either drift once (the L plane checks both)
+                        P.count_dropped = ((c->dopt.grid_extent || shared) && k == 0) ? 2 : 0;
                         if (fp32 && !quad && k == 1) { P.other_delta = -1; P.self_first = 0; }  // L - R
                         if (fp32 && quad && k < 2) { P.other_delta = 2 - k; P.self_first = 1; }  // L - M, R - M
                     }
@@ -1239,8 +1258,22 @@ void CollideJob::run() {
         CK(cudaMemsetAsync(c->lq.p, 0, sizeof(long long) * c->lq.n, st));
     }
     c->first_lum.ensure(std::max<size_t>(first_lum.size(), 1));
+    std::vector<long long> slr;
+    if (shared) {
+        slr.assign((size_t)2 * kMaxSlices * 2, 0);
+        for (int b = 0; b < 2; ++b)
+            for (int sl = 0; sl < (b == 0 ? ns1 : ns2); ++sl) {
+                const SliceInfo &SB = b == 0 ? S1 : S2;
+                slr[((size_t)b * kMaxSlices + sl) * 2] = SB.start[sl];
+                slr[((size_t)b * kMaxSlices + sl) * 2 + 1] = SB.count[sl];
+            }
+        c->ubox.ensure((size_t)(ns1 + ns2) * kUnionRow);
+        c->uflag.ensure(ns1 + ns2);
+        c->slr.ensure(slr.size());
+    }
     const size_t bytes = sizeof(Task) * tasks.size() + sizeof(Plane) * planes.size() + sizeof(LumJob) * lumjobs.size() +
-                         sizeof(int2) * blockmap.size() + sizeof(FirstLum) * first_lum.size() + 64;
+                         sizeof(int2) * blockmap.size() + sizeof(FirstLum) * first_lum.size() +
+                         sizeof(long long) * slr.size() + 64;
     c->stage.ensure(bytes);
     char *h = c->stage.p;
     auto put = [&](void *dst, const void *src, size_t nbytes) {
@@ -1254,6 +1287,16 @@ void CollideJob::run() {
     put(c->lumjobs.p, lumjobs.data(), sizeof(LumJob) * lumjobs.size());
     put(c->blockmap.p, blockmap.data(), sizeof(int2) * blockmap.size());
     put(c->first_lum.p, first_lum.data(), sizeof(FirstLum) * first_lum.size());
+    if (shared) {
+        put(c->slr.p, slr.data(), sizeof(long long) * slr.size());
+        const long long nu = (long long)(ns1 + ns2) * kUnionRow;
+        launch_pdl(k_init_boxes, (unsigned)((nu + 255) / 256), 256, 0, st, c->ubox.p, nu, (unsigned long long *)nullptr, 0ll);
+        CK(cudaMemsetAsync(c->uflag.p, 0, sizeof(int) * (ns1 + ns2), st));
+        launches += 1;
+        C.ubox = c->ubox.p;
+        C.uflag = c->uflag.p;
+        C.slr = c->slr.p;
+    }
     CK(cudaMemsetAsync(c->lum_parts.p, 0, sizeof(double) * npairs_total, st));
     launch_pdl(k_init_bounds, (std::max(ntasks, npairs_total) + 255) / 256, 256, 0, st, c->bnd.p, ntasks, c->lumb.p, npairs_total,
                                                                                 c->nanflag.p, c->status.p, 0);
@@ -1322,6 +1365,30 @@ void CollideJob::run() {
         for (int t = F.t0; t < F.t0 + F.nt; t += 2) slice_bytes += (double)(tasks[t].src_n + tasks[t].fld_n);
         for (int t = F.t0; t < F.t0 + F.nt; ++t) { src_bytes += (double)tasks[t].src_n; fld_bytes += (double)tasks[t].fld_n; }
         const unsigned bps = (unsigned)std::max<long long>(1, std::min<long long>(kMaxBoundBlocks, (F.maxsrc + 2047) / 2048));
+        bool union_first = false;
+        for (int t = F.t0; t < F.t0 + F.nt; ++t) union_first = union_first || tasks[t].ub_first;
+        if (union_first) {
+            // the source slice's union box at its first use: the whole partner beam, then the source slice
+            double pbytes = 0.0;
+            long long pmax = 1;
+            for (int t = F.t0; t < F.t0 + F.nt; ++t) {
+                if (!tasks[t].ub_first) continue;
+                const SliceInfo &SP = tasks[t].fld_beam == 0 ? S1 : S2;
+                for (int sl = 0; sl < (tasks[t].fld_beam == 0 ? ns1 : ns2); ++sl) {
+                    pbytes += (double)SP.count[sl];
+                    pmax = std::max<long long>(pmax, SP.count[sl]);
+                }
+                pbytes += (double)tasks[t].src_n;
+            }
+            PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, 2, pbytes * 5 * rsz);
+            const unsigned bxp = (unsigned)std::max<long long>(1, std::min<long long>(kMaxBoundBlocks, (pmax + 2047) / 2048));
+            with_real(fp32, [&](auto r) {
+                launch_pdl(k_union_partner<decltype(r)>, dim3(bxp, (unsigned)std::max(ns1, ns2), (unsigned)F.nt), 256, 0, st, C,
+                           F.t0);
+                launch_pdl(k_union_source<decltype(r)>, dim3(bps, (unsigned)F.nt), 256, 0, st, C, F.t0);
+            });
+            launches += 2;
+        }
         if (!node) {
             PhaseScope ps(c, OCTO_PHASE_BOUNDS, st, gaussian ? 2 : 1, slice_bytes * 5 * rsz);
             with_real(fp32, [&](auto r) { launch_pdl(k_pair_bounds<decltype(r)>, dim3(bps, 2 * npf), 256, 0, st, C, F.t0); });
@@ -1702,6 +1769,16 @@ double CollideJob::finish() {
                      bb, (long long)turn);
             throw OctoFail{OCTO_ERR_NONFINITE, m};
         }
+        if (code == OCTO_ERR_NONFINITE && t < ntasks && role == 0) {  // :source_slice union box (pic_cpu.jl:665-712)
+            const Task &T = tasks[t];
+            long long f2 = first_nonfinite_host(*b2, st, false), f1 = first_nonfinite_host(*b1, st, false);
+            const int bb = f2 >= 0 ? 2 : 1;
+            const long long first = f2 >= 0 ? f2 : f1;
+            if (rep) { rep->role = 0; rep->pair_i = T.i; rep->pair_j = T.j; rep->direction = T.dir; rep->first_index = first + 1; }
+            snprintf(m, sizeof m, "non-finite coordinate at particle %lld of beam%d (source-slice union bounds, slice pair "
+                                  "(%d, %d), turn %lld)", first + 1, bb, T.i, T.j, (long long)turn);
+            throw OctoFail{OCTO_ERR_NONFINITE, m};
+        }
         if (code == OCTO_ERR_NONFINITE && t < ntasks) {
             const Task &T = tasks[t];
             if (rep) { rep->role = role; rep->pair_i = T.i; rep->pair_j = T.j; rep->direction = T.dir; }
@@ -1988,6 +2065,7 @@ octo_ctx *octo_create(int32_t device, const octo_pic_options *options) {
     d.fourth = options->field_derivative == 4;
     d.quadratic = options->slice_interpolation == 1;
     d.node = options->interaction_grid == OCTO_GRID_NODE;
+    d.shared_grid = options->interaction_grid == OCTO_GRID_SOURCE_SLICE;
     d.longitudinal_kick = options->longitudinal_kick;
     d.min_ex = options->min_extent_x;
     d.min_ey = options->min_extent_y;
@@ -2058,7 +2136,7 @@ void octo_destroy(octo_ctx *c) {
     c->first_lum.release(); c->lum_tick.release(); c->cap_q.release(); c->cap_grid.release();
     c->cnn_flags.release(); c->h_cnn_flags.release(); c->cnn_q.release();
     c->hyb.release(); c->hmom.release(); c->hprof.release(); c->hsum.release(); c->qtot.release();
-    c->esum.release();
+    c->esum.release(); c->ubox.release(); c->uflag.release(); c->slr.release();
     c->stage.release(); c->h_lum.release(); c->h_status.release(); c->h_noderef.release(); c->h_slices.release();
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);

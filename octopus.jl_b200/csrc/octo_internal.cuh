@@ -40,7 +40,14 @@ struct Task {
     // next_task, drift next_sM); -1 when the slice has no later pair.
     int32_t next_pair, next_task;
     double next_sM;
+    // interaction_grid = :source_slice: the row of this task's (direction, source slice) union box, and 1 when
+    // this task is the source slice's first use (it computes the box)
+    int32_t ub, ub_first;
 };
+
+// :source_slice union box rows: partner z, partner x, partner y, source x, source y (min, max each)
+constexpr int kUnionRow = 10;
+constexpr int kUnionTrig = 1, kUnionBad = 2, kUnionSrcBad = 4;
 
 // :node with luminosity: virtual-position extrema of each slice for its first pair of the collide.
 struct FirstLum {
@@ -258,6 +265,7 @@ struct DevOptions {
     int gaussian, neutralize;    // GaussianPICPoissonSolver (Gaussian-subtracted hybrid)
     int dep_rotate;              // rotate each lane's deposit tap order (spatially ordered slices)
     int grid_extent;             // :slice_pair mesh extent: 0 :extrema, 1 :sigma (mean +- extent_k sd)
+    int shared_grid;             // interaction_grid = :source_slice: one union-sized mesh per source slice
     double extent_k;             // grid_extent_sigma
     double min_ex, min_ey, quantize, min_ratio, growth;
     double margin;               // hybrid: Gaussian containment half-width in sigmas

@@ -134,14 +134,12 @@ function _options(p::PICPoissonSolver, keep::Vector{Any}, precision::Integer=0, 
     lg = p.luminosity_grid === nothing ? (0, 0) : p.luminosity_grid
     ldm = p.luminosity_deposit_method === nothing ? Int32(-1) : _sym(p.luminosity_deposit_method, Dict(:CIC => 0, :TSC => 1))
     ig = Symbol(p.interaction_grid)
-    ig === :source_slice && throw(ArgumentError(
-        "interaction_grid = :source_slice is implemented only by the CPU PICPoissonSolver path"))
     return OctoPicOptions(
         Int32(p.grid[1]), Int32(p.grid[2]), _sym(p.deposit_method, Dict(:CIC => 0, :TSC => 1)), ldm,
         Int32(lg[1]), Int32(lg[2]), _sym(p.green_type, Dict(:integrated => 0, :standard => 1, :lattice => 2)),
         _sym(p.green_cache, Dict(:none => 0, :slice_pair => 1)),
         p.field_derivative === :fourth ? Int32(4) : Int32(2), p.slice_interpolation === :quadratic ? Int32(1) : Int32(0),
-        ig === :node ? Int32(2) : Int32(0), p.grid_extent === :extrema ? Int32(0) : Int32(1),
+        _sym(ig, Dict(:slice_pair => 0, :source_slice => 1, :node => 2)), p.grid_extent === :extrema ? Int32(0) : Int32(1),
         Float64(p.grid_extent_sigma), Float64(p.min_transverse_extent[1]), Float64(p.min_transverse_extent[2]),
         Float64(p.grid_quantize), Float64(p.slice_pair_green_min_ratio), Float64(p.slice_pair_green_growth),
         Int32(p.longitudinal_kick), m1, m2, n1, n2, c1, c2,

@@ -156,7 +156,7 @@ class PICPoissonSolver:
         o.green_cache = {"none": 0, "slice_pair": 1}[self.green_cache]
         o.field_derivative = 2 if self.field_derivative == "second" else 4
         o.slice_interpolation = 0 if self.slice_interpolation == "linear" else 1
-        o.interaction_grid = {"slice_pair": 0, "node": 2}[self.interaction_grid]
+        o.interaction_grid = {"slice_pair": 0, "source_slice": 1, "node": 2}[self.interaction_grid]
         o.grid_extent = 0 if self.grid_extent == "extrema" else 1
         o.grid_extent_sigma = float(self.grid_extent_sigma)
         o.min_extent_x, o.min_extent_y = self.min_transverse_extent
@@ -194,10 +194,6 @@ def _choice(name, value, allowed):
 
 def _require_gpu_options(s: PICPoissonSolver):
     """The GPU backend's route checks (the reference CUDA backend's, pic_cpu.jl:730-777)."""
-    if s.interaction_grid == "source_slice":
-        raise ArgumentError(
-            "interaction_grid = :source_slice is not implemented by the GPU PIC backend; only the CPU "
-            "PICPoissonSolver path supports :source_slice. Set interaction_grid = :slice_pair.")
     if s.green_type == "lattice":
         raise ArgumentError("green_type = :lattice (an experimental CPU study kernel) is not implemented by the GPU "
                             "PIC backend; use :integrated or :standard.")

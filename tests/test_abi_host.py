@@ -99,10 +99,13 @@ def test_solver_defaults_and_validation():
 
 def test_gpu_backend_rejects_what_it_does_not_implement():
     sl = ob.LongitudinalSlicing(nslices=3, method="normal_quantile")
-    for kw in (dict(interaction_grid="source_slice"), dict(green_type="lattice"),
-               dict(grid=(80, 80)), dict(grid=(96, 36)), dict(grid=(1024, 64))):
+    for kw in (dict(green_type="lattice"), dict(grid=(80, 80)), dict(grid=(96, 36)), dict(grid=(1024, 64))):
         with pytest.raises(ob.ArgumentError):
             ob.PICPoissonSolver(slicing=sl, **kw).to_c()
+    for ig, code in (("slice_pair", 0), ("source_slice", 1), ("node", 2)):
+        assert ob.PICPoissonSolver(slicing=sl, interaction_grid=ig).to_c().interaction_grid == code
+    with pytest.raises(ob.ArgumentError):  # union-sized meshes apply no extent estimator
+        ob.PICPoissonSolver(slicing=sl, interaction_grid="source_slice", grid_extent="sigma")
     o = ob.PICPoissonSolver(slicing=sl, grid_extent="sigma", grid_extent_sigma=4.5).to_c()  # :slice_pair only
     assert (o.grid_extent, o.grid_extent_sigma) == (1, 4.5)
     with pytest.raises(ob.ArgumentError):  # the :equal_area histogram's shared-memory bound

@@ -1,7 +1,7 @@
 """The plain PIC collide does not depend on the order of particles inside a slice: the working copy grouped by
 transverse position (the default, octo_set_particle_order(1)) and the caller order give bit-identical
 coordinates, luminosities, per-pair luminosity traces and Green-cache counters, over several turns, for
-:slice_pair and :node grids, CIC and TSC, and the float32 precision form."""
+:slice_pair, :source_slice and :node grids, CIC and TSC, and the float32 precision form."""
 import pytest
 
 from helpers import beams, E_PARAMS, P_PARAMS
@@ -34,6 +34,7 @@ def _run(solver, spatial, dtype, turns=2):
     (dict(deposit_method="TSC", field_derivative="fourth"), "float64"),
     (dict(interaction_grid="node"), "float32"),
     (dict(slice_interpolation="quadratic"), "float32"),
+    (dict(interaction_grid="source_slice"), "float64"),
 ])
 def test_spatial_order_is_bit_identical(opts, dtype_name):
     import torch

@@ -294,3 +294,69 @@ def test_sparse_slices(kind):
          "hybrid_coupled": lambda: ob.GaussianPICPoissonSolver(grid=(32, 32), slicing=sl, coupling_tol=0.01)}[kind]()
     check(run_both(s, 200, 160, turns=2, e_sigma=(95e-6, 8.5e-6, 7e-3), p_sigma=(95e-6, 8.5e-6, 6e-2),
                    transform=lambda b: tilt(b, 0.05)), lum_rtol=1e-8)
+
+
+@pytest.mark.parametrize("opts", [
+    dict(),
+    dict(slice_interpolation="quadratic"),
+    dict(green_cache="none"),
+    dict(deposit_method="TSC", field_derivative="fourth", green_type="standard"),
+])
+def test_source_slice(opts):
+    """interaction_grid = :source_slice (pic_cpu.jl:30-60, 360-380, 602-712): pairs one at a time in collision
+    order, each source slice's mesh sized from its union box taken at first use -- the partner beam as that pair
+    finds it -- with one Green-cache entry per (source slice, direction) whose coverage test keeps each pair's
+    own bounds.  Coordinates, luminosities and the cache history against the oracle at the contract's 1e-10."""
+    ob = _gpu()
+    s = ob.PICPoissonSolver(grid=(64, 64), interaction_grid="source_slice",
+                            slicing=ob.LongitudinalSlicing(nslices=5, method="normal_quantile"), **opts)
+    out = run_both(s, 6000, 4000, turns=2, e_sigma=(95e-6, 8.5e-6, 7e-3), p_sigma=(95e-6, 8.5e-6, 6e-2))
+    check(out)
+    if s.green_cache == "slice_pair":
+        assert out[0]["cache_o"][1] == 10  # one entry per source slice of either beam
+
+
+def test_source_slice_counts_particles_that_leave_the_union_box():
+    """The union box is taken at the source slice's first use and the partner is kicked afterwards, so with no
+    cache growth a few particles leave it; they are counted as the oracle counts them (pic_cpu.jl:1064-1096)."""
+    from oracle import oracle as orc
+    ob = _gpu()
+    s = ob.PICPoissonSolver(grid=(64, 64), interaction_grid="source_slice", slice_pair_green_growth=0.0,
+                            slicing=ob.LongitudinalSlicing(nslices=4, method="normal_quantile"))
+    e, p = beams(5000, 5000)
+    be, bp = _device_beams(ob, e, p)
+    rt = ob.StrongStrongRuntime()
+    ctx = rt.context("ip", s, 0)
+    oracle = orc.Oracle(oracle_options(s))
+    pe, pp = oracle_params()
+    drops = []
+    for t in range(2):
+        lum_g = ctx.collide(be, bp, turn=t + 1)
+        lum_o = oracle.collide(e, p, pe, pp)
+        assert ctx.last_report.dropped == oracle.dropped(), (ctx.last_report.dropped, oracle.dropped())
+        drops.append(oracle.dropped())
+        assert abs(lum_g / lum_o - 1) <= 1e-10
+        assert within(be.numpy(), e, ATOL, RTOL) <= 1.0 and within(bp.numpy(), p, ATOL, RTOL) <= 1.0
+    assert sum(drops) > 0
+    rt.close()
+
+
+def test_source_slice_nonfinite_partner_fails_at_the_union_bounds():
+    """A NaN anywhere in the partner beam fails the first pair at its union box (pic_cpu.jl:665-692), before
+    either interaction; the context stays usable."""
+    ob = _gpu()
+    e, p = beams(3000, 2000)
+    e[2, 1234] = np.nan
+    be, bp = _device_beams(ob, e, p)
+    s = ob.PICPoissonSolver(grid=(32, 32), interaction_grid="source_slice",
+                            slicing=ob.LongitudinalSlicing(nslices=4, method="normal_quantile"))
+    rt = ob.StrongStrongRuntime()
+    ctx = rt.context("ip", s, 0)
+    with pytest.raises(ob.CollisionError) as err:
+        ctx.collide(be, bp, turn=3)
+    assert err.value.code == 1 and "union bounds" in str(err.value) and "1235 of beam1" in str(err.value), str(err.value)
+    assert err.value.report.role == 0
+    e2, p2 = beams(3000, 2000)
+    be2, bp2 = _device_beams(ob, e2, p2)
+    assert np.isfinite(ctx.collide(be2, bp2, turn=4))
+    rt.close()

@@ -104,6 +104,14 @@ def test_precision_form_slice_pair_tsc_fourth_quadratic():
     check(run_precision(s, 6000, 4000))
 
 
+def test_precision_form_source_slice():
+    """interaction_grid = :source_slice in the precision form: the union boxes from float32 coordinates."""
+    import octo_b200 as ob
+    s = ob.PICPoissonSolver(grid=(64, 64), interaction_grid="source_slice",
+                            slicing=ob.LongitudinalSlicing(nslices=5, method="normal_quantile"))
+    check(run_precision(s, 6000, 4000, e_sigma=(95e-6, 8.5e-6, 0.7e-2), p_sigma=(95e-6, 8.5e-6, 6e-2)))
+
+
 @pytest.mark.parametrize("aspect", [1, 5, 11, 25])
 def test_field_error_vs_bassetti_erskine_both_forms(aspect):
     import octo_b200 as ob
