@@ -119,7 +119,8 @@ typedef struct {
 /* What a collide reports besides the luminosity. */
 typedef struct {
     int32_t status;
-    int32_t role;            /* 0 none, 1 source, 2 field, 3 beam (slicing), 4 node-mesh build */
+    int32_t role;            /* 0 none, 1 source, 2 field, 3 beam (slicing), 4 node-mesh build,
+                                5 :source_slice union box */
     int32_t pair_i, pair_j;  /* 1-based slice pair of the first failure */
     int32_t direction;       /* 1 or 2 */
     int32_t n_batches;       /* wavefronts executed */

@@ -1774,7 +1774,7 @@ double CollideJob::finish() {
             long long f2 = first_nonfinite_host(*b2, st, false), f1 = first_nonfinite_host(*b1, st, false);
             const int bb = f2 >= 0 ? 2 : 1;
             const long long first = f2 >= 0 ? f2 : f1;
-            if (rep) { rep->role = 0; rep->pair_i = T.i; rep->pair_j = T.j; rep->direction = T.dir; rep->first_index = first + 1; }
+            if (rep) { rep->role = 5; rep->pair_i = T.i; rep->pair_j = T.j; rep->direction = T.dir; rep->first_index = first + 1; }
             snprintf(m, sizeof m, "non-finite coordinate at particle %lld of beam%d (source-slice union bounds, slice pair "
                                   "(%d, %d), turn %lld)", first + 1, bb, T.i, T.j, (long long)turn);
             throw OctoFail{OCTO_ERR_NONFINITE, m};

@@ -355,7 +355,7 @@ def test_source_slice_nonfinite_partner_fails_at_the_union_bounds():
     with pytest.raises(ob.CollisionError) as err:
         ctx.collide(be, bp, turn=3)
     assert err.value.code == 1 and "union bounds" in str(err.value) and "1235 of beam1" in str(err.value), str(err.value)
-    assert err.value.report.role == 0
+    assert err.value.report.role == 5
     e2, p2 = beams(3000, 2000)
     be2, bp2 = _device_beams(ob, e2, p2)
     assert np.isfinite(ctx.collide(be2, bp2, turn=4))
