@@ -129,6 +129,8 @@ typedef struct {
     int64_t dropped;         /* particles outside their mesh (pic_cpu.jl:394-457) */
     int64_t green_hits, green_misses, green_rebuilds;  /* cumulative, as Contracts.jl:947-960 compares */
     int64_t kernel_launches; /* device kernels this call launched */
+    int32_t replayed;        /* 1 when the collide ran as its captured graph (octo_set_collide_graph) */
+    int32_t pad;
 } octo_collide_report;
 
 typedef struct octo_ctx octo_ctx;
@@ -174,6 +176,18 @@ int32_t octo_pic_autotune(octo_ctx *ctx, octo_beam *beam1, octo_beam *beam2, con
  * every kick is its own particle's -- so both give bit-identical results.  The Gaussian-subtracted hybrid and the
  * soft-Gaussian solver always keep caller order (their slice moments are ordered floating-point sums). */
 int32_t octo_set_particle_order(octo_ctx *ctx, int32_t order);
+/* Captured collide graphs, on by default for the plain PIC collide (no reference counterpart: the reference
+ * schedules each collide on the host, pic_cpu.jl:82-275).  Once two consecutive collides of a context have the
+ * same schedule -- slice counts and starts, collision order -- the next one captures its kernels into a CUDA
+ * graph; later collides launch it behind a one-block device guard that checks the schedule and recomputes the
+ * slice drifts, so a collide costs one host synchronisation instead of two and no schedule upload.  A collide
+ * whose schedule differs, a changed beam address, interaction scale, launch shape or workspace falls back to
+ * the ordinary path on the untouched beams.  Results are bit-identical either way.  enable: 1 (default) or 0;
+ * setting it synchronises the device and drops the current graph. */
+int32_t octo_set_collide_graph(octo_ctx *ctx, int32_t enable);
+/* out = graphs captured, collides replayed, replays the guard declined, capture failures (two failures turn
+ * the graphs off for the context). */
+int32_t octo_collide_graph_stats(octo_ctx *ctx, int64_t out[4]);
 
 /* Green-cache counters (the contract of Contracts.jl:947-960). */
 int32_t octo_green_cache_stats(octo_ctx *ctx, int64_t *hits, int64_t *misses, int64_t *rebuilds);

@@ -59,7 +59,8 @@ mutable struct OctoCollideReport
     status::Int32; role::Int32; pair_i::Int32; pair_j::Int32; direction::Int32; n_batches::Int32
     turn::Int64; first_index::Int64; dropped::Int64
     green_hits::Int64; green_misses::Int64; green_rebuilds::Int64; kernel_launches::Int64
-    OctoCollideReport() = new(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
+    replayed::Int32; pad::Int32
+    OctoCollideReport() = new(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
 end
 
 """

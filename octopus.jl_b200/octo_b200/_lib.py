@@ -28,7 +28,7 @@ EXPORTS = (
     "octo_track_line", "octo_beam_moments", "octo_capture_charge_plane", "octo_captured_charge_plane",
     "octo_gemm_bf16", "octo_cnn_create", "octo_cnn_destroy", "octo_cnn_num_params", "octo_cnn_get_params",
     "octo_cnn_set_params", "octo_cnn_forward", "octo_cnn_train_step", "octo_set_field_correction",
-    "octo_field_correction_report", "octo_set_particle_order",
+    "octo_field_correction_report", "octo_set_particle_order", "octo_set_collide_graph", "octo_collide_graph_stats",
 )
 
 PHASES = ("slicing", "bounds", "plan", "green", "luminosity", "deposit", "fft", "field", "kick", "unsort", "node")
@@ -101,7 +101,7 @@ class OctoCollideReport(C.Structure):
         ("status", C.c_int32), ("role", C.c_int32), ("pair_i", C.c_int32), ("pair_j", C.c_int32),
         ("direction", C.c_int32), ("n_batches", C.c_int32), ("turn", C.c_int64), ("first_index", C.c_int64),
         ("dropped", C.c_int64), ("green_hits", C.c_int64), ("green_misses", C.c_int64),
-        ("green_rebuilds", C.c_int64), ("kernel_launches", C.c_int64),
+        ("green_rebuilds", C.c_int64), ("kernel_launches", C.c_int64), ("replayed", C.c_int32), ("pad", C.c_int32),
     ]
 
 
@@ -188,6 +188,10 @@ def lib():
     L.octo_field_correction_report.argtypes = [vp, P(i32)]
     L.octo_set_particle_order.restype = i32
     L.octo_set_particle_order.argtypes = [vp, i32]
+    L.octo_set_collide_graph.restype = i32
+    L.octo_set_collide_graph.argtypes = [vp, i32]
+    L.octo_collide_graph_stats.restype = i32
+    L.octo_collide_graph_stats.argtypes = [vp, C.POINTER(C.c_int64)]
     L.octo_set_timing_phases.restype = i32
     L.octo_set_timing_phases.argtypes = [vp, C.c_uint32]
     L.octo_set_timing.restype = i32

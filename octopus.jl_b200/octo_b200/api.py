@@ -123,6 +123,19 @@ class Context:
         if rc != _lib.OCTO_OK:
             raise CollisionError(rc, "octo_set_particle_order failed")
 
+    def set_collide_graph(self, enable: bool = True):
+        """Plain PIC: replay each collide as a captured CUDA graph once its schedule repeats (default), or always
+        run the ordinary host-scheduled path; results are bit-identical either way."""
+        rc = _lib.lib().octo_set_collide_graph(self._ptr, 1 if enable else 0)
+        if rc != _lib.OCTO_OK:
+            raise CollisionError(rc, f"octo_set_collide_graph failed: {_lib.last_error(self._ptr)}")
+
+    def collide_graph_stats(self) -> Tuple[int, int, int, int]:
+        """(graphs captured, collides replayed, replays the device guard declined, capture failures)."""
+        out = (C.c_int64 * 4)()
+        _lib.lib().octo_collide_graph_stats(self._ptr, out)
+        return tuple(out)
+
     def green_cache_stats(self) -> Tuple[int, int, int]:
         h, m, r = C.c_int64(), C.c_int64(), C.c_int64()
         _lib.lib().octo_green_cache_stats(self._ptr, C.byref(h), C.byref(m), C.byref(r))

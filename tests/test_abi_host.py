@@ -41,7 +41,7 @@ int main(void) {
   F(octo_pic_options, kbb1) F(octo_pic_options, precision) F(octo_beam, x) F(octo_beam, pz)
   F(octo_pic_options, solver) F(octo_pic_options, include_sigma_xy) F(octo_pic_options, min_sigma)
   F(octo_pic_options, resolution2) F(octo_pic_options, coupling_tol)
-  F(octo_collide_report, turn) F(octo_collide_report, kernel_launches)
+  F(octo_collide_report, turn) F(octo_collide_report, kernel_launches) F(octo_collide_report, replayed)
   F(octo_element, rng_id) F(octo_element, p)
   return 0;
 }
