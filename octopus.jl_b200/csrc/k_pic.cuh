@@ -2231,8 +2231,10 @@ __global__ void __launch_bounds__(kKickThreads, sizeof(R) == 8 ? 2 : 4)
     pdl_wait();
     pdl_release();
     __shared__ KickJob<R> J;
+    const int2 bm0 = blockmap[blockIdx.x];
+    if (bm0.x < 0) return;  // a spare entry of a collide that may be captured (block-uniform)
     if (threadIdx.x == 0) {
-        const int2 bm = blockmap[blockIdx.x];
+        const int2 bm = bm0;
         const Task &T = C.tasks[bm.x];
         J.ok = 1;
         Grid gL, gR;
@@ -2310,7 +2312,7 @@ __global__ void __launch_bounds__(kKickThreads, sizeof(R) == 8 ? 2 : 4)
 constexpr int kBoxTile = 512, kBoxLanes = 16, kBoxGroups = 4, kBoxThreads = 256;
 struct NodeBoxArgs {
     const void *x[2], *px[2], *y[2], *py[2], *z[2];  // slice-sorted coordinates, element type R
-    long long start[2][kMaxSlices], count[2][kMaxSlices];
+    const SliceInfo *info[2];                         // the device slice tables (slice starts and counts)
     const double *ref[2];
     unsigned long long *sbox[2], *fbox[2];
     int *nanf;
@@ -2328,9 +2330,9 @@ __global__ void __launch_bounds__(kBoxThreads) k_node_boxes(NodeBoxArgs A) {
     const int sl = bm ? (int)blockIdx.y - A.ns[0] : (int)blockIdx.y;
     const int o = A.ns[1 - bm], nb = o + 1, nref = nb + o;
     const int g0 = blockIdx.z * kBoxGroups;
-    const long long n = A.count[bm][sl], k0 = (long long)blockIdx.x * A.chunk;
+    const long long n = A.info[bm]->count[sl], k0 = (long long)blockIdx.x * A.chunk;
     if (k0 >= n || g0 * kBoxLanes >= nref) return;  // block-uniform
-    const long long k1 = min(n, k0 + A.chunk), st = A.start[bm][sl];
+    const long long k1 = min(n, k0 + A.chunk), st = A.info[bm]->start[sl];
     const int ng = min(kBoxGroups, (nref - g0 * kBoxLanes + kBoxLanes - 1) / kBoxLanes);
     const R *X = (const R *)A.x[bm], *PX = (const R *)A.px[bm], *Y = (const R *)A.y[bm],
             *PY = (const R *)A.py[bm], *Z = (const R *)A.z[bm];

@@ -12,19 +12,6 @@
 
 namespace octo {
 
-struct SliceInfo {          // device-resident, read back once per collide
-    double boundary[kMaxSlices + 1];
-    double center[kMaxSlices];
-    double weight[kMaxSlices];
-    long long count[kMaxSlices];
-    long long start[kMaxSlices];
-    double mu, sigma, zmin, zmax;
-    int ns;
-    int zero_width;
-    int nonfinite;
-    int pad;
-};
-
 // Both beams are sliced by the same launches: blockIdx.z (or blockIdx.x for the one-block kernels)
 // selects the beam, so the two serial lane folds run side by side.
 template <class R>

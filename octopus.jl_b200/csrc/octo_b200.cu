@@ -373,11 +373,13 @@ struct octo_ctx {
         std::vector<Task> tasks;
         int ntasks = 0, npairs_total = 0;
         long long body_launches = 0;
+        std::vector<int> pos_of;          // pair index (i-1)*ns2 + (j-1) -> its position in the captured order
         std::vector<long long> sig;       // schedule of the captured collide (k_replay_check's layout)
         std::vector<long long> last_sig;  // schedule of the last ordinary collide
         long long builds = 0, replays = 0, declined = 0, failures = 0;
     } rp;
     DevBuf<long long> rp_sig;
+    DevBuf<FrontKick> rp_fronts;
     DevBuf<int> rp_ok;
     PinBuf<int> h_rp_ok;
     cudaStream_t cap_stream = nullptr;  // the stream graphs are captured on (never the legacy default stream)
@@ -385,6 +387,8 @@ struct octo_ctx {
 };
 
 namespace {
+
+bool replay_eligible(const octo_ctx *c);
 
 // ---- per-phase timing: a scope records an event pair on the stream around a launch group
 cudaEvent_t take_event(octo_ctx *c) {
@@ -867,7 +871,7 @@ void launch_green(const octo_ctx *c, const Collide &C, int mode, int base, int c
 // per-direction drift tables and slice counts are staged in pinned memory owned by the context, and
 // mesh validity is known on the host from the slice counts (node_mesh_valid).
 void build_node_meshes(octo_ctx *c, Collide &C, const SliceInfo &S1, const SliceInfo &S2, cudaStream_t st,
-                       long long &launches, bool capture) {
+                       long long &launches, bool capture, bool padded, long long &node_cap) {
     const int ns1 = c->ns[0], ns2 = c->ns[1];
     const int nnode = ns1 * (ns2 + 1) + ns2 * (ns1 + 1);
     c->nodes.ensure(nnode);
@@ -910,19 +914,20 @@ void build_node_meshes(octo_ctx *c, Collide &C, const SliceInfo &S1, const Slice
         const BeamWS &W = c->bw[bm];
         const SliceInfo &SS = bm == 0 ? S1 : S2;
         A.x[bm] = W.s[0].p; A.px[bm] = W.s[1].p; A.y[bm] = W.s[2].p; A.py[bm] = W.s[3].p; A.z[bm] = W.s[4].p;
-        for (int s = 0; s < c->ns[bm]; ++s) {
-            A.start[bm][s] = SS.start[s];
-            A.count[bm][s] = SS.count[s];
-            maxn = std::max(maxn, SS.count[s]);
-        }
+        A.info[bm] = W.info.p;
+        for (int s = 0; s < c->ns[bm]; ++s) maxn = std::max(maxn, SS.count[s]);
         A.ns[bm] = c->ns[bm];
     }
+    // a collide that may be captured keeps this chunking for later turns: room for slices a sixteenth larger
+    // (the graph's guard checks that every slice still fits)
+    if (padded) maxn += maxn / 16 + kBoxTile;
     A.ref[0] = c->node_ref.p; A.ref[1] = c->node_ref.p + off2;
     A.sbox[0] = sbox1; A.sbox[1] = sbox2;
     A.fbox[0] = fbox2; A.fbox[1] = fbox1;
     A.nanf = c->nodenan.p;
     const long long bx = std::min<long long>(256, (maxn + 4095) / 4096);
     A.chunk = ((maxn + bx - 1) / bx + kBoxTile - 1) / kBoxTile * kBoxTile;
+    node_cap = bx * A.chunk;
     const int gz = (std::max(nref1, nref2) + kBoxLanes * kBoxGroups - 1) / (kBoxLanes * kBoxGroups);
     with_real(c->fp32, [&](auto r) {
         launch_pdl(k_node_boxes<decltype(r)>, dim3((unsigned)bx, ns1 + ns2, gz), kBoxThreads, 0, st, A);
@@ -975,6 +980,9 @@ struct CollideJob {
     // synchronisation, no uploads and no copies back (the captured graph's own nodes do those)
     bool capture = false;
     int nplanes_total = 0, nlum_total = 0, nfirst_total = 0;  // the schedule tables' lengths (run)
+    std::vector<int> slot;  // replayed graph: order position -> the captured position its pair's results use
+    std::vector<FrontKick> fkick;  // per wavefront: its tasks and kick block map entries (run)
+    long long node_cap = 0;        // :node: the largest slice the node-box chunking covers (run)
     void begin();
     void run();
     void run_gaussian(const SliceInfo &S1, const SliceInfo &S2);
@@ -1046,6 +1054,9 @@ void CollideJob::run() {
     const bool quad = o.slice_interpolation == 1;
     const int method = o.deposit_method;
     const int lmethod = c->dopt.lum_method;
+    // a collide that may be captured sizes what depends on the slice counts with room to spare (the kick's
+    // block map, the node boxes' chunking), so that its graph fits later turns whose counts differ a little
+    const bool padded = replay_eligible(c);
 
     Collide C{};
     C.o = c->dopt;
@@ -1106,7 +1117,7 @@ void CollideJob::run() {
     // ---- node meshes at turn start
     if (node) {
         PhaseScope ps(c, OCTO_PHASE_NODE, st, 16);
-        build_node_meshes(c, C, S1, S2, st, launches, capture);
+        build_node_meshes(c, C, S1, S2, st, launches, capture, padded, node_cap);
     }
     auto node_id = [&](int dir, int src_slice0, int node1) {
         return dir == 1 ? src_slice0 * (ns2 + 1) + (node1 - 1) : ns1 * (ns2 + 1) + src_slice0 * (ns1 + 1) + (node1 - 1);
@@ -1115,14 +1126,15 @@ void CollideJob::run() {
     std::vector<Plane> planes;
     std::vector<LumJob> lumjobs;
     std::vector<int2> blockmap;
-    struct Front { int t0, nt, p0, np, l0, nl, b0, nb; long long maxsrc, maxlum; int kchunk; };
+    // nb: the front's kick block map entries; cap: with the spare entries (the kick's grid)
+    struct Front { int t0, nt, p0, np, l0, nl, b0, nb; long long maxsrc, maxlum; int kchunk; int cap; };
     std::vector<Front> fronts;
     const int nplanes_task = node ? (lk ? 3 : 2) : (quad ? 3 : 2);
     ran.assign(order.size(), 0);
     tasks.clear();
     for (size_t f = 0; f < batches.size(); ++f) {
         Front F{(int)tasks.size(), 0, (int)planes.size(), 0, (int)lumjobs.size(), 0, (int)blockmap.size(), 0, 1, 1,
-                kKickChunk};
+                kKickChunk, 0};
         for (const OrderEntry &pr : batches[f]) {
             const int i = pr.i, j = pr.j;
             if (S1.count[i - 1] == 0 || S2.count[j - 1] == 0) continue;
@@ -1223,11 +1235,18 @@ void CollideJob::run() {
                                                                                            kKickThreads * kKickThreads));
         for (int t = F.t0; t < F.t0 + F.nt; ++t)
             for (long long off = 0; off < tasks[t].fld_n; off += F.kchunk) blockmap.push_back(make_int2(t, (int)off));
+        F.nb = (int)blockmap.size() - F.b0;
+        if (padded && F.nt) {  // room for one more block per task and a sixteenth more, unused here
+            const int spare = F.nt + F.nb / 16;
+            for (int k = 0; k < spare; ++k) blockmap.push_back(make_int2(-1, 0));
+        }
+        F.cap = (int)blockmap.size() - F.b0;
         F.np = (int)planes.size() - F.p0;
         F.nl = (int)lumjobs.size() - F.l0;
-        F.nb = (int)blockmap.size() - F.b0;
         if (F.nt) fronts.push_back(F);
     }
+    fkick.clear();
+    for (const Front &F : fronts) fkick.push_back(FrontKick{F.t0, F.nt, F.b0, F.cap, F.kchunk, 0});
     ntasks = (int)tasks.size();
     npairs_total = (int)order.size();
     // :node with luminosity: each kick reduces its field slice's virtual positions for that slice's next pair,
@@ -1586,8 +1605,9 @@ void CollideJob::run() {
                 launch_method(method, [&](auto M) {
                     using R = decltype(r);
                     constexpr int MM = decltype(M)::value;
-                    if (gaussian) launch_pdl(k_kick<R, MM, true>, F.nb, kKickThreads, 0, st, C, F.p0, c->blockmap.p + F.b0, F.kchunk);
-                    else launch_pdl(k_kick<R, MM, false>, F.nb, kKickThreads, 0, st, C, F.p0, c->blockmap.p + F.b0, F.kchunk);
+                    // F.cap blocks: the front's block map, spare entries included (they return at once)
+                    if (gaussian) launch_pdl(k_kick<R, MM, true>, F.cap, kKickThreads, 0, st, C, F.p0, c->blockmap.p + F.b0, F.kchunk);
+                    else launch_pdl(k_kick<R, MM, false>, F.cap, kKickThreads, 0, st, C, F.p0, c->blockmap.p + F.b0, F.kchunk);
                 });
             });
         }
@@ -1850,11 +1870,13 @@ double CollideJob::finish() {
     if (compute_lum) {
         lum = 0.0;
         for (size_t p = 0; p < order.size(); ++p) {
-            if (!ran[p]) continue;
-            lum += c->h_lum.p[p];
+            // a replayed graph stores each pair's luminosity in the slot of its place in the captured order
+            const size_t q = slot.empty() ? p : (size_t)slot[p];
+            if (!ran[q]) continue;
+            lum += c->h_lum.p[q];
             c->trace_i.push_back(order[p].i);
             c->trace_j.push_back(order[p].j);
-            c->trace_lum.push_back(c->h_lum.p[p]);
+            c->trace_lum.push_back(c->h_lum.p[q]);
         }
     }
     return lum;
@@ -1866,12 +1888,14 @@ int fail(octo_ctx *c, int code, const std::string &m) {
 }
 
 // ---- captured collide graph
-// Plain PIC only: the hybrid's and the learned correction's extra state, :source_slice's sequential union
-// boxes, per-phase timing and a charge-plane capture keep the ordinary path.
+// Plain PIC only: the hybrid's and the learned correction's extra state, :sigma extents, :source_slice's
+// sequential union boxes, per-phase timing and a charge-plane capture keep the ordinary path.
 bool replay_eligible(const octo_ctx *c) {
     const octo_pic_options &o = c->opt;
-    return c->rp.enabled && o.solver == OCTO_SOLVER_PIC && !o.gaussian && !c->cnn && !c->dopt.shared_grid &&
-           !c->timing && !c->cap_armed && !c->in_autotune;
+    // the hybrid's moments and :sigma's extents are FP64 sums over blocks whose split follows the slice counts
+    return c->rp.enabled && o.solver == OCTO_SOLVER_PIC && !o.gaussian && !c->dopt.grid_extent && !c->cnn &&
+           !c->dopt.shared_grid && !c->timing && !c->cap_armed && !c->in_autotune &&
+           c->ns[0] * c->ns[1] <= kReplayMaxPairs;
 }
 
 void drop_replay(octo_ctx *c) {
@@ -1883,18 +1907,20 @@ void drop_replay(octo_ctx *c) {
     R.valid = 0;
 }
 
-// The schedule of a collide in k_replay_check's layout: slice counts and starts of both beams, then the
-// collision order as pair indices.
+// The schedule of a collide in k_replay_check's layout: which slices of both beams hold particles, then for
+// every pair index (i-1)*ns2 + (j-1) its wavefront and its place in it.
 std::vector<long long> schedule_sig(const octo_ctx *c, const SliceInfo &S1, const SliceInfo &S2,
-                                    const std::vector<OrderEntry> &order) {
+                                    const std::vector<std::vector<OrderEntry>> &batches) {
     const int ns1 = c->ns[0], ns2 = c->ns[1];
     std::vector<long long> v;
-    v.reserve(2 * (size_t)(ns1 + ns2) + order.size());
-    for (int k = 0; k < ns1; ++k) v.push_back(S1.count[k]);
-    for (int k = 0; k < ns1; ++k) v.push_back(S1.start[k]);
-    for (int k = 0; k < ns2; ++k) v.push_back(S2.count[k]);
-    for (int k = 0; k < ns2; ++k) v.push_back(S2.start[k]);
-    for (const OrderEntry &e : order) v.push_back((long long)(e.i - 1) * ns2 + (e.j - 1));
+    v.reserve((size_t)(ns1 + ns2) + (size_t)ns1 * ns2);
+    for (int k = 0; k < ns1; ++k) v.push_back(S1.count[k] > 0);
+    for (int k = 0; k < ns2; ++k) v.push_back(S2.count[k] > 0);
+    const size_t base = v.size();
+    v.resize(base + (size_t)ns1 * ns2, -1);
+    for (size_t f = 0; f < batches.size(); ++f)
+        for (size_t q = 0; q < batches[f].size(); ++q)
+            v[base + (size_t)(batches[f][q].i - 1) * ns2 + (batches[f][q].j - 1)] = (long long)f * 65536 + (long long)q;
     return v;
 }
 
@@ -1931,11 +1957,14 @@ void build_replay(octo_ctx *c, const CollideJob &job, const std::vector<long lon
     try {
         if (!c->cap_stream) CK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
         c->rp_sig.ensure(sig.size());
+        c->rp_fronts.ensure(std::max<size_t>(job.fkick.size(), 1));
         c->rp_ok.ensure(1);
         c->h_rp_ok.ensure(1);
         c->h_lum.ensure(std::max(job.npairs_total, 1));
         c->h_status.ensure(1);
         CK(cudaMemcpy(c->rp_sig.p, sig.data(), sizeof(long long) * sig.size(), cudaMemcpyHostToDevice));
+        if (!job.fkick.empty())
+            CK(cudaMemcpy(c->rp_fronts.p, job.fkick.data(), sizeof(FrontKick) * job.fkick.size(), cudaMemcpyHostToDevice));
         CK(cudaGraphCreate(&g, 0));
         cudaGraphConditionalHandle h;
         CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
@@ -1954,6 +1983,15 @@ void build_replay(octo_ctx *c, const CollideJob &job, const std::vector<long lon
         A.first = c->first_lum.p;
         A.nfirst = job.nfirst_total;
         A.node_ref = c->dopt.node ? c->node_ref.p : nullptr;
+        A.fp32 = c->fp32;
+        A.fronts = c->rp_fronts.p;
+        A.nfronts = (int)job.fkick.size();
+        A.blockmap = c->blockmap.p;
+        A.node_cap = job.node_cap;
+        // k_node_plan reads the slice counts staged after the drift references (build_node_meshes)
+        A.node_counts = c->dopt.node ? (long long *)(c->node_ref.p + (size_t)c->ns[0] * (2 * c->ns[1] + 1) +
+                                                     (size_t)c->ns[1] * (2 * c->ns[0] + 1))
+                                     : nullptr;
         A.ok = c->rp_ok.p;
         A.handle = h;
         void *args[] = {&A};
@@ -1999,6 +2037,9 @@ void build_replay(octo_ctx *c, const CollideJob &job, const std::vector<long lon
         R.exec = ex;
         R.valid = 1;
         R.sig = sig;
+        R.pos_of.assign((size_t)c->ns[0] * c->ns[1], -1);
+        for (size_t q = 0; q < job.order.size(); ++q)
+            R.pos_of[(size_t)(job.order[q].i - 1) * c->ns[1] + (job.order[q].j - 1)] = (int)q;
         R.order = job.order;
         R.batches = job.batches;
         R.ran = job.ran;
@@ -2036,7 +2077,7 @@ void build_replay(octo_ctx *c, const CollideJob &job, const std::vector<long lon
 // fits it.
 void maybe_build_replay(octo_ctx *c, const CollideJob &job) {
     auto &R = c->rp;
-    std::vector<long long> sig = schedule_sig(c, c->h_slices.p[0], c->h_slices.p[1], job.order);
+    std::vector<long long> sig = schedule_sig(c, c->h_slices.p[0], c->h_slices.p[1], job.batches);
     const bool repeat = sig == R.last_sig;
     R.last_sig = sig;
     if (!repeat) return;
@@ -2373,7 +2414,7 @@ void octo_destroy(octo_ctx *c) {
     if (c->lum_stream) cudaStreamDestroy(c->lum_stream);
     drop_replay(c);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
-    c->rp_sig.release(); c->rp_ok.release(); c->h_rp_ok.release();
+    c->rp_sig.release(); c->rp_fronts.release(); c->rp_ok.release(); c->h_rp_ok.release();
     delete c;
 }
 
@@ -2403,13 +2444,24 @@ int32_t octo_pic_collide(octo_ctx *c, octo_beam *beam1, octo_beam *beam2, const 
             CK(cudaStreamSynchronize(job.st));
             if (*c->h_rp_ok.p) {
                 R.replays++;
+                // this collide's order (the guard found its wavefronts equal to the captured ones); each pair's
+                // results sit in the slot of its captured position
+                const SliceInfo &S1 = c->h_slices.p[0], &S2 = c->h_slices.p[1];
+                job.order = collision_order(S1.center, c->ns[0], S2.center, c->ns[1]);
+                job.slot.resize(job.order.size());
+                for (size_t q = 0; q < job.order.size(); ++q)
+                    job.slot[q] = R.pos_of[(size_t)(job.order[q].i - 1) * c->ns[1] + (job.order[q].j - 1)];
                 lum = job.finish();
                 done = true;
                 if (report) report->replayed = 1;
             } else {
+                // the guard found another schedule, or slices the graph has no room for: the ordinary path,
+                // after which the next repeat of a schedule is captured afresh
                 R.declined++;
+                drop_replay(c);
                 job.launches = sliced + 1;
                 job.order.clear();
+                job.slot.clear();
                 job.batches.clear();
                 job.ran.clear();
                 job.tasks.clear();

@@ -45,6 +45,26 @@ struct Task {
     int32_t ub, ub_first;
 };
 
+// One beam's slice table, computed on the device by the slicing kernels and read back once per collide.
+struct SliceInfo {
+    double boundary[kMaxSlices + 1];
+    double center[kMaxSlices];
+    double weight[kMaxSlices];
+    long long count[kMaxSlices];
+    long long start[kMaxSlices];
+    double mu, sigma, zmin, zmax;
+    int ns;
+    int zero_width;
+    int nonfinite;
+    int pad;
+};
+
+// The kick blocks of one wavefront: tasks t0 .. t0+nt-1, block map entries b0 .. b0+cap-1 of kchunk field
+// particles each (a captured collide graph's map carries spare entries, task -1, for slices that grow).
+struct FrontKick {
+    int32_t t0, nt, b0, cap, kchunk, pad;
+};
+
 // :source_slice union box rows: partner z, partner x, partner y, source x, source y (min, max each)
 constexpr int kUnionRow = 10;
 constexpr int kUnionTrig = 1, kUnionBad = 2, kUnionSrcBad = 4;
@@ -238,7 +258,7 @@ __device__ __forceinline__ void tsc_weights(R u, int n, int &base, R w[3]) {
 
 // Fixed-point scale: taps are rounded to multiples of 2^-bits with
 // bits = min(40, 62 - bitlength(nsrc)), so a whole slice fits one int64 cell.
-inline int fixed_bits_for(int64_t n) {
+__host__ __device__ inline int fixed_bits_for(int64_t n) {
     int bl = 0;
     uint64_t v = (uint64_t)(n < 1 ? 1 : n);
     while (v) { ++bl; v >>= 1; }
@@ -249,7 +269,7 @@ inline int fixed_bits_for(int64_t n) {
 // block-private shared grids (its int64 plane grids and every integer sum stay exact).  An FP32 weight carries
 // 24 significant bits, so the quanta lose nothing for slices of up to ~64 particles and at most 2^-(bits+1) of a
 // particle's charge per tap beyond (2^-13 at 170,000 particles).
-inline int fixed_bits_for32(int64_t n) {
+__host__ __device__ inline int fixed_bits_for32(int64_t n) {
     int bl = 0;
     uint64_t v = (uint64_t)(n < 1 ? 1 : n);
     while (v) { ++bl; v >>= 1; }

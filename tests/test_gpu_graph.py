@@ -22,7 +22,7 @@ def _params(ob):
     return pe, pp
 
 
-def _run(solver, graph, dtype_name, turns=6, n1=40000, n2=20000):
+def _run(solver, graph, dtype_name, turns=6, n1=40000, n2=20000, ztunes=(0.0, 0.0)):
     import torch
     import octo_b200 as ob
     dtype = getattr(torch, dtype_name)
@@ -30,8 +30,8 @@ def _run(solver, graph, dtype_name, turns=6, n1=40000, n2=20000):
     pe, pp = _params(ob)
     be = ob.Beam.from_numpy(e, pe, dtype=dtype)
     bp = ob.Beam.from_numpy(p, pp, dtype=dtype)
-    me = ob.Linear6D(E_BEAM["beta"], E_BEAM["alpha"], E_BEAM["tune"])
-    mp = ob.Linear6D(P_BEAM["beta"], P_BEAM["alpha"], P_BEAM["tune"])
+    me = ob.Linear6D(E_BEAM["beta"], E_BEAM["alpha"], E_BEAM["tune"][:2] + (ztunes[0],))
+    mp = ob.Linear6D(P_BEAM["beta"], P_BEAM["alpha"], P_BEAM["tune"][:2] + (ztunes[1],))
     ctx = ob.Context(solver, 0, dtype)
     ctx.set_collide_graph(graph)
     out = []
@@ -68,6 +68,25 @@ def test_replayed_collides_are_bit_identical(opts, dtype_name):
     assert [x[5] for x in a[2]] == [0, 0, 1, 1, 1, 1], a[2]
     assert a[3][:2] == (1, 4) and a[3][2:] == (0, 0), a[3]
     assert [x[5] for x in b[2]] == [0] * 6 and b[3] == (0, 0, 0, 0)
+
+
+def test_replay_across_reordered_collisions():
+    """Longitudinal tunes move the slice centroids every turn, and pairs with nearly equal collision times
+    change places in the collision order; as long as the wavefronts are unchanged the guard accepts the graph
+    and the host folds the pair luminosities in the new order.  Bit-identical to the ordinary path over 16
+    turns, with at least one replayed turn whose order differs from the previous turn's."""
+    import torch
+    import octo_b200 as ob
+    solver = ob.PICPoissonSolver(grid=(64, 64), interaction_grid="node",
+                                 slicing=ob.LongitudinalSlicing(nslices=15, method="normal_quantile"))
+    a = _run(solver, True, "float64", turns=16, ztunes=(-0.069, -0.01))
+    b = _run(solver, False, "float64", turns=16, ztunes=(-0.069, -0.01))
+    assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
+    assert [x[:5] for x in a[2]] == [x[:5] for x in b[2]]
+    assert a[3][1] >= 1, a[3]
+    orders = [[(i, j) for i, j, _ in x[1]] for x in a[2]]
+    reordered = [t for t in range(1, 16) if a[2][t][5] and orders[t] != orders[t - 1]]
+    assert reordered, (a[3], [x[5] for x in a[2]])
 
 
 def _oracle_turns(solver, states, ob):
@@ -118,16 +137,39 @@ def test_replayed_collides_match_the_oracle(grid_mode):
     assert [r["replayed"] for r in out] == [0, 0, 1, 1, 1] and stats == (1, 3, 0, 0), (out, stats)
 
 
-def test_a_changed_schedule_is_declined():
+def test_changed_counts_replay_and_a_changed_schedule_is_declined():
     """:equal_width slices: the counts follow the z distribution.  Two collides of one beam pair capture the
-    graph; another proton sample has other counts, the guard declines it and the ordinary path runs; the
-    collide after it is declined too, repeats that schedule and captures anew."""
+    graph.  Another proton sample has other slice counts and starts but the same wavefronts and no empty slice:
+    the guard rewrites the ranges, fixed-point scales and kick block map and replays it.  A proton bunch with a
+    gap of six sigma in z leaves two of its slices empty, which changes the schedule: the guard declines it, the
+    graph is dropped and the ordinary path runs; the next collide repeats that schedule and captures anew.
+    Every collide against the oracle at 1e-10."""
     import octo_b200 as ob
     s = ob.PICPoissonSolver(grid=(64, 64), slicing=ob.LongitudinalSlicing(nslices=6, method="equal_width"))
     e, p = beams(6000, 4000, e_sigma=(95e-6, 8.5e-6, 7e-3), p_sigma=(95e-6, 8.5e-6, 6e-2))
     _, p2 = beams(6000, 4000, e_sigma=(95e-6, 8.5e-6, 7e-3), p_sigma=(95e-6, 8.5e-6, 6e-2), seed=7)
-    out, stats = _oracle_turns(s, [(e, p), (e, p), (e, p), (e, p2), (e, p2), (e, p2)], ob)
+    p3 = p.copy()
+    p3[4] = np.where(p3[4] > 0, p3[4] + 6 * 6e-2, p3[4])
+    out, stats = _oracle_turns(s, [(e, p), (e, p), (e, p2), (e, p3), (e, p3), (e, p3)], ob)
     _check(out)
-    # turn 4 and 5: the guard declines the first graph; turn 5 repeats the new schedule and captures it
     assert [r["replayed"] for r in out] == [0, 0, 1, 0, 0, 1], out
-    assert stats == (2, 2, 2, 0), stats
+    assert stats == (2, 2, 1, 0), stats
+
+
+def test_slices_that_outgrow_the_graph_are_declined_and_recaptured():
+    """The same schedule with an end slice grown seventyfold (1000 protons of the third :equal_width slice moved into
+    the first, the bunch's extent unchanged): the kick's block map has no room for it, the guard declines, the
+    ordinary path runs and captures the schedule again with room for the new counts, and the next collide replays
+    that graph."""
+    from oracle import oracle as orc
+    import octo_b200 as ob
+    s = ob.PICPoissonSolver(grid=(64, 64), slicing=ob.LongitudinalSlicing(nslices=6, method="equal_width"))
+    e, p = beams(6000, 4000, e_sigma=(95e-6, 8.5e-6, 7e-3), p_sigma=(95e-6, 8.5e-6, 6e-2))
+    b = orc.slices(p[4], 6, method="equal_width")[0]
+    third = np.where((p[4] >= b[2]) & (p[4] < b[3]))[0]
+    p5 = p.copy()
+    p5[4, third[:1000]] = 0.5 * (b[0] + b[1])
+    out, stats = _oracle_turns(s, [(e, p), (e, p), (e, p), (e, p5), (e, p5)], ob)
+    _check(out)
+    assert [r["replayed"] for r in out] == [0, 0, 1, 0, 1], out
+    assert stats == (2, 2, 1, 0), stats
