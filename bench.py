@@ -232,6 +232,7 @@ def run_ours(args, rank, world, local_rank):
     # collection inside the timed loops
     gc.collect()
     gc.disable()
+    graph0 = ctx.collide_graph_stats()
     ev0.record(stream)
     for t in range(args.steps):
         lum = turn(args.warmup + t)
@@ -241,6 +242,7 @@ def run_ours(args, rank, world, local_rank):
     gc.enable()
     barrier()
     ms = ev0.elapsed_time(ev1) / args.steps
+    graph1 = ctx.collide_graph_stats()
     n_kick = max(3, min(args.steps, 20))
     ctx.set_timing(True, phases=["kick"])
     for t in range(n_kick):
@@ -462,6 +464,9 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": e2e_ms / 1e3 / world, "unit": UNIT, "h2d_bytes_per_step": beam_bytes,
                 "d2h_bytes_per_step": beam_bytes + 8, "wall_s_per_step": wall},
         "gpu_launches": launches,
+        # timed collides that ran as the captured graph behind its device guard (octo_set_collide_graph)
+        "collide_graph": {"replayed_turns": graph1[1] - graph0[1], "declined_turns": graph1[2] - graph0[2],
+                          "timed_turns": args.steps, "captures": graph1[0]},
         "launch_shape": {"chosen": list(ctx.AUTOTUNE_SHAPES[shape]),
                          "chosen_fast_form": list(ctx.AUTOTUNE_SHAPES[shape32]) if fast else None,
                          "meaning": "(deposit waves of SMs per wavefront, kick resident-slot multiple), picked by "
