@@ -1007,6 +1007,14 @@ using ShQ = typename std::conditional<sizeof(R) == 4, int, long long>::type;
 // Field-solve planes of a front.  grid: (blocks per plane, planes in front); each block deposits a
 // grid-stride share of its plane's source slice into a private int64 copy of the nx*ny grid in shared
 // memory, then merges it with global atomics (the consumer, k_conv_rows, clears the grid it reads).
+// Blocks of a k_deposit_node3 row: ceil(n / per_block), at most the grid (per_block <= 0: the whole grid).  A row
+// of a large slice gets more blocks than one of a small slice, so a front's blocks fill whole waves of the SMs.
+__device__ __forceinline__ int row_blocks(long long n, long long per_block) {
+    if (per_block <= 0) return (int)gridDim.x;
+    const long long b = (n + per_block - 1) / per_block;
+    return (int)max(1ll, min((long long)gridDim.x, b));
+}
+
 template <class R, int METHOD>
 __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
     using Q = ShQ<R>;
@@ -1105,7 +1113,7 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
 // (blocks per task, tasks in front); ppt = 2 or 3 planes per task, consecutive.  Every quantum is the
 // expression of k_deposit, so the grids are bit-identical to k_deposit's planes.
 template <class R, int METHOD>
-__global__ void __launch_bounds__(1024, 1) k_deposit_node3(Collide C, int plane0, int ppt) {
+__global__ void __launch_bounds__(1024, 1) k_deposit_node3(Collide C, int plane0, int ppt, long long per_block) {
     int *sq = (int *)g_smem;  // L | R | Z
     const int nx = C.o.nx, ny = C.o.ny, cells = nx * ny;
     for (int c = threadIdx.x; c < ppt * cells; c += blockDim.x) sq[c] = 0;
@@ -1114,6 +1122,8 @@ __global__ void __launch_bounds__(1024, 1) k_deposit_node3(Collide C, int plane0
     const int pl = ppt * blockIdx.y;
     const bool z = ppt == 3;
     const Plane &PL = C.planes[plane0 + pl], &PR = C.planes[plane0 + pl + 1];
+    const int nblk = row_blocks(PL.src_n, per_block);
+    if ((int)blockIdx.x >= nblk) return;  // block-uniform: this row needs fewer blocks than the grid has
     const bool okL = C.nodes[PL.geom].valid != 0, okR = C.nodes[PR.geom].valid != 0;
     if (!okL && !okR) return;  // block-uniform
     const Grid gL = C.nodes[PL.geom].sg, gR = C.nodes[PR.geom].sg;
@@ -1128,7 +1138,7 @@ __global__ void __launch_bounds__(1024, 1) k_deposit_node3(Collide C, int plane0
     const R xL0 = (R)gL.x0, yL0 = (R)gL.y0, xR0 = (R)gR.x0, yR0 = (R)gR.y0;
     const R xLhi = (R)(gL.x0 + gL.w), yLhi = (R)(gL.y0 + gL.h), xRhi = (R)(gR.x0 + gR.w), yRhi = (R)(gR.y0 + gR.h);
     int outside = 0;
-    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long stride = (long long)nblk * blockDim.x;
     long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     R cx = 0, cpx = 0, cy = 0, cpy = 0;
     if (k < src_n) { const long long p = src_start + k; cx = X[p]; cpx = PX[p]; cy = Y[p]; cpy = PY[p]; }

@@ -1502,19 +1502,45 @@ void CollideJob::run() {
         }
         {
             PhaseScope ps(c, OCTO_PHASE_DEPOSIT, st, 1, src_bytes * 4 * rsz);
-            // blocks per plane: 32768-particle shares, and at least one full wave of the GPU's SMs for the
-            // narrow fronts (one block per SM: a block holds its plane's whole int64 grid)
             // the precision form's :node planes of a task in one pass when their three int32 grids fit shared
             // memory (k_deposit_node3)
             const int ppt = c->dopt.longitudinal_kick ? 3 : 2;  // :node planes per task (L, R and Z)
             const bool node3 = fp32 && node && !c->dopt.dep_global && !c->dopt.dep_rotate && ppt * cells * sizeof(int) <= kSmemLimit;
             const int rows = node3 ? F.np / ppt : F.np;
-            const long long wave = ((long long)c->num_sms * c->dep_waves + rows - 1) / rows;
-            unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(32, std::max<long long>((F.maxsrc + 32767) / 32768, wave)));
+            // k_deposit_node3 (a task's three int32 planes per block): a row gets ceil(src_n / per_block) blocks,
+            // so rows of large slices get more blocks than rows of small ones.  One block runs per SM (it holds its
+            // planes' whole grids); for w = dep_waves .. 8 waves per_block is the smallest share that fits the
+            // front's blocks into w waves, and the w with the least (waves run) x (share + the block's fixed cost:
+            // clearing and merging its grids, counted as cells / 4 particles per grid) is taken.  k_deposit (one
+            // plane per row) keeps a uniform count per row: 32768-particle shares, and at least dep_waves waves
+            // for the narrow fronts (its 64-bit atomic loop measured 19 % slower with the per-row stride).
+            std::vector<long long> rn(rows);
+            long long sum_src = 0, max_src = 1;
+            for (int r = 0; r < rows; ++r) {
+                rn[r] = planes[F.p0 + r * (node3 ? ppt : 1)].src_n;
+                sum_src += rn[r];
+                max_src = std::max(max_src, rn[r]);
+            }
+            const long long S = c->num_sms, fixed = (long long)cells * (node3 ? ppt : 1) / 4;
+            long long per_block = std::max<long long>(1024, max_src);
+            double best = 1e300;
+            for (int w = std::max(1, c->dep_waves); w <= 8; ++w) {
+                const long long room = std::max<long long>(1, S * w - rows);
+                const long long pb = std::max<long long>(1024, (sum_src + room - 1) / room);
+                long long T = 0;
+                for (long long n : rn) T += std::min<long long>(32, std::max<long long>(1, (n + pb - 1) / pb));
+                const double cost = (double)((T + S - 1) / S) * (double)(pb + fixed);
+                if (cost < best) { best = cost; per_block = pb; }
+            }
+            unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(32, (max_src + per_block - 1) / per_block));
+            if (!node3) {
+                const long long wave = ((long long)c->num_sms * c->dep_waves + rows - 1) / rows;
+                bpp = (unsigned)std::max<long long>(1, std::min<long long>(32, std::max<long long>((F.maxsrc + 32767) / 32768, wave)));
+            }
             if (node3) {
                 launch_method(method, [&](auto M) {
                     launch_pdl(k_deposit_node3<float, decltype(M)::value>, dim3(bpp, rows), 1024, ppt * cells * sizeof(int), st, C,
-                               F.p0, ppt);
+                               F.p0, ppt, per_block);
                 });
             } else {
                 with_real(fp32, [&](auto r) {
