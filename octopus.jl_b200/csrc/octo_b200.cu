@@ -867,6 +867,33 @@ void launch_green(const octo_ctx *c, const Collide &C, int mode, int base, int c
     }
 }
 
+// Particles per block for a launch whose rows (planes or slice sides) take ceil(n / share) blocks each, one block
+// resident per SM (it holds its rows' whole grids): for w = min_waves .. 8 waves the share is the smallest that
+// fits the blocks into w waves of the SMs, and the w with the least (waves run) x (share + a block's fixed cost,
+// `fixed` particles' worth of clearing and merging its grid) is taken.
+long long wave_share(const std::vector<long long> &rn, long long fixed, long long sms, int min_waves) {
+    long long sum = 0, mx = 1;
+    for (long long n : rn) { sum += n; mx = std::max(mx, n); }
+    const long long rows = (long long)rn.size();
+    long long share = std::max<long long>(1024, mx);
+    double best = 1e300;
+    for (int w = std::max(1, min_waves); w <= 8; ++w) {
+        const long long room = std::max<long long>(1, sms * w - rows);
+        const long long pb = std::max<long long>(1024, (sum + room - 1) / room);
+        long long T = 0;
+        for (long long n : rn) T += std::min<long long>(32, std::max<long long>(1, (n + pb - 1) / pb));
+        const double cost = (double)((T + sms - 1) / sms) * (double)(pb + fixed);
+        if (cost < best) { best = cost; share = pb; }
+    }
+    return share;
+}
+// The grid's blocks per row for that share: enough for the largest row (at most 32).
+unsigned share_blocks(const std::vector<long long> &rn, long long share) {
+    long long mx = 1;
+    for (long long n : rn) mx = std::max(mx, n);
+    return (unsigned)std::max<long long>(1, std::min<long long>(32, (mx + share - 1) / share));
+}
+
 // Enqueue the node meshes of both directions (pic_cpu.jl:1404-1419) with no host synchronisation: the
 // per-direction drift tables and slice counts are staged in pinned memory owned by the context, and
 // mesh validity is known on the host from the slice counts (node_mesh_valid).
@@ -1472,6 +1499,8 @@ void CollideJob::run() {
             CK(cudaStreamWaitEvent(c->lum_stream, c->ev_fork, 0));
             {
                 PhaseScope ps(c, OCTO_PHASE_LUMINOSITY, c->lum_stream, 2, slice_bytes * 4 * rsz);
+                // uniform blocks per side: this stream runs beside the front's deposit and convolution and wants
+                // parallelism (blocks in proportion to each side's slice, sized to whole waves, measured slower)
                 unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(8, (F.maxlum + 32767) / 32768));
                 with_real(fp32, [&](auto r) {
                     launch_method(lmethod, [&](auto M) {
@@ -1515,24 +1544,9 @@ void CollideJob::run() {
             // plane per row) keeps a uniform count per row: 32768-particle shares, and at least dep_waves waves
             // for the narrow fronts (its 64-bit atomic loop measured 19 % slower with the per-row stride).
             std::vector<long long> rn(rows);
-            long long sum_src = 0, max_src = 1;
-            for (int r = 0; r < rows; ++r) {
-                rn[r] = planes[F.p0 + r * (node3 ? ppt : 1)].src_n;
-                sum_src += rn[r];
-                max_src = std::max(max_src, rn[r]);
-            }
-            const long long S = c->num_sms, fixed = (long long)cells * (node3 ? ppt : 1) / 4;
-            long long per_block = std::max<long long>(1024, max_src);
-            double best = 1e300;
-            for (int w = std::max(1, c->dep_waves); w <= 8; ++w) {
-                const long long room = std::max<long long>(1, S * w - rows);
-                const long long pb = std::max<long long>(1024, (sum_src + room - 1) / room);
-                long long T = 0;
-                for (long long n : rn) T += std::min<long long>(32, std::max<long long>(1, (n + pb - 1) / pb));
-                const double cost = (double)((T + S - 1) / S) * (double)(pb + fixed);
-                if (cost < best) { best = cost; per_block = pb; }
-            }
-            unsigned bpp = (unsigned)std::max<long long>(1, std::min<long long>(32, (max_src + per_block - 1) / per_block));
+            for (int r = 0; r < rows; ++r) rn[r] = planes[F.p0 + r * (node3 ? ppt : 1)].src_n;
+            const long long per_block = wave_share(rn, (long long)cells * (node3 ? ppt : 1) / 4, c->num_sms, c->dep_waves);
+            unsigned bpp = share_blocks(rn, per_block);
             if (!node3) {
                 const long long wave = ((long long)c->num_sms * c->dep_waves + rows - 1) / rows;
                 bpp = (unsigned)std::max<long long>(1, std::min<long long>(32, std::max<long long>((F.maxsrc + 32767) / 32768, wave)));
