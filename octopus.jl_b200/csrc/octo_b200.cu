@@ -2480,6 +2480,10 @@ int32_t octo_pic_collide(octo_ctx *c, octo_beam *beam1, octo_beam *beam2, const 
             job.ntasks = R.ntasks;
             job.npairs_total = R.npairs_total;
             job.launches = sliced + 1 + R.body_launches;
+            // nothing an earlier (failed) collide left on the luminosity stream may overlap the graph's own
+            // luminosity work, as in the ordinary path
+            CK(cudaEventRecord(c->ev_join, c->lum_stream));
+            CK(cudaStreamWaitEvent(job.st, c->ev_join, 0));
             CK(cudaGraphLaunch(R.exec, job.st));
             CK(cudaStreamSynchronize(job.st));
             if (*c->h_rp_ok.p) {

@@ -173,3 +173,39 @@ def test_slices_that_outgrow_the_graph_are_declined_and_recaptured():
     _check(out)
     assert [r["replayed"] for r in out] == [0, 0, 1, 0, 1], out
     assert stats == (2, 2, 1, 0), stats
+
+
+def test_a_nonfinite_coordinate_during_replays_is_reported():
+    """A NaN that reaches the beams after the graph was captured: the slicing flags it, the guard declines and
+    drops the graph, and the ordinary path reports it as a collide without a graph would (OCTO_ERR_NONFINITE,
+    the particle, the turn).  The context then collides clean beams again: the first of them repeats the last
+    ordinary schedule and captures anew, the next ones replay."""
+    import torch
+    import octo_b200 as ob
+    s = ob.PICPoissonSolver(grid=(32, 32), slicing=ob.LongitudinalSlicing(nslices=4, method="normal_quantile"))
+    e, p = beams(3000, 2000)
+    pe, pp = _params(ob)
+    be = ob.Beam.from_numpy(e, pe)
+    bp = ob.Beam.from_numpy(p, pp)
+    ctx = ob.Context(s, 0, torch.float64)
+    for t in range(3):
+        be.coords.copy_(torch.from_numpy(e))
+        bp.coords.copy_(torch.from_numpy(p))
+        ctx.collide(be, bp, turn=t + 1)
+    assert ctx.last_report.replayed == 1
+    bad = e.copy()
+    bad[4, 1234] = np.nan
+    be.coords.copy_(torch.from_numpy(bad))
+    bp.coords.copy_(torch.from_numpy(p))
+    with pytest.raises(ob.CollisionError) as err:
+        ctx.collide(be, bp, turn=4)
+    assert err.value.code == 1 and "1235" in str(err.value) and "turn 4" in str(err.value), str(err.value)
+    assert err.value.report.role == 3 and err.value.report.replayed == 0
+    out = []
+    for t in range(3):
+        be.coords.copy_(torch.from_numpy(e))
+        bp.coords.copy_(torch.from_numpy(p))
+        out.append((ctx.collide(be, bp, turn=5 + t), ctx.last_report.replayed))
+    assert all(np.isfinite(l) for l, _ in out) and [r for _, r in out] == [0, 1, 1], out
+    assert ctx.collide_graph_stats()[2] == 1
+    ctx.close()
