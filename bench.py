@@ -832,6 +832,36 @@ def run_scan(args, rank, world, local_rank):
     return 0
 
 
+def run_profile_form(args, local_rank):
+    """Profiling runs: `args.steps` turns of one form of the workload (plain: FP64 at 128^2; fast: the precision
+    form at 128^2; coarse: the precision form at 64^2) with the collide's ordinary launches -- a captured graph's
+    kernels are not listed one by one by a kernel profiler -- and no output line."""
+    import torch
+    import octo_b200 as ob
+
+    dev = torch.device(f"cuda:{local_rank}")
+    torch.cuda.set_device(dev)
+    grid = COARSE_GRID if args.profile_form == "coarse" else GRID
+    dtype = torch.float64 if args.profile_form == "plain" else torch.float32
+    e = ob.Beam.gaussian(N_E, seed=SEED, charge=-1.0, mc2=ob.EMASS_EV, E0=10e9, npart=1.7e11, device=dev, **E_BEAM)
+    p = ob.Beam.gaussian(N_P, seed=SEED, charge=1.0, mc2=ob.PMASS_EV, E0=275e9, npart=6.9e10, device=dev, **P_BEAM)
+    if dtype == torch.float32:
+        e, p = e.astype(dtype), p.astype(dtype)
+    me = ob.Linear6D(E_BEAM["beta"], (0, 0, 0), E_TUNES)
+    mp = ob.Linear6D(P_BEAM["beta"], (0, 0, 0), P_TUNES)
+    rt = ob.StrongStrongRuntime()
+    ctx = rt.context("ip", _solver(ob, grid), local_rank, dtype)
+    ctx.set_collide_graph(False)
+    stream = torch.cuda.current_stream(dev)
+    for t in range(args.steps):
+        ctx.collide(e, p, turn=t, stream=stream)
+        me.track(e, stream=stream)
+        mp.track(p, stream=stream)
+    torch.cuda.synchronize()
+    rt.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -846,6 +876,8 @@ def main():
     ap.add_argument("--scan-cases", type=int, default=64)
     ap.add_argument("--scan-turns", type=int, default=20)
     ap.add_argument("--scan-batch", type=int, default=8)
+    ap.add_argument("--profile-form", choices=["plain", "fast", "coarse"], default=None,
+                    help="profiling runs: --steps turns of one form with ordinary launches, no output line")
     ap.add_argument("--emittance-turns", type=int, default=1000,
                     help="turns of the emittance-growth comparison of both forms (0 skips it; one GPU only)")
     args = ap.parse_args()
@@ -857,6 +889,8 @@ def main():
             return run_reference(args, rank)
         if args.scan:
             return run_scan(args, rank, world, local_rank)
+        if args.profile_form:
+            return run_profile_form(args, local_rank)
         return run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
