@@ -209,3 +209,42 @@ def test_a_nonfinite_coordinate_during_replays_is_reported():
     assert all(np.isfinite(l) for l, _ in out) and [r for _, r in out] == [0, 1, 1], out
     assert ctx.collide_graph_stats()[2] == 1
     ctx.close()
+
+
+def test_two_interaction_points_replay_side_by_side():
+    """Two contexts of one runtime (two interaction points, different grids) collided in turn, with Linear6D maps
+    between: a buffer reallocated by one context invalidates the other's graph until both have settled, after
+    which both replay.  Bit-identical to the same sequence with collide graphs off."""
+    import torch
+    import octo_b200 as ob
+
+    def run(graph):
+        e, p = beams(20000, 10000, e_sigma=(95e-6, 8.5e-6, 7e-3), p_sigma=(95e-6, 8.5e-6, 6e-2))
+        pe, pp = _params(ob)
+        be = ob.Beam.from_numpy(e, pe)
+        bp = ob.Beam.from_numpy(p, pp)
+        me = ob.Linear6D(E_BEAM["beta"], E_BEAM["alpha"], E_BEAM["tune"])
+        mp = ob.Linear6D(P_BEAM["beta"], P_BEAM["alpha"], P_BEAM["tune"])
+        rt = ob.StrongStrongRuntime()
+        sl = ob.LongitudinalSlicing(nslices=5, method="normal_quantile")
+        ctx = [rt.context("ip1", ob.PICPoissonSolver(grid=(64, 64), interaction_grid="node", slicing=sl), 0),
+               rt.context("ip2", ob.PICPoissonSolver(grid=(32, 32), slicing=sl), 0)]
+        for c in ctx:
+            c.set_collide_graph(graph)
+        lums, replayed = [], []
+        for t in range(8):
+            for c in ctx:
+                lums.append(c.collide(be, bp, turn=t + 1))
+                replayed.append(c.last_report.replayed)
+                me.track(be)
+                mp.track(bp)
+        stats = [c.collide_graph_stats() for c in ctx]
+        out = (be.coords.clone(), bp.coords.clone(), lums, replayed, stats)
+        rt.close()
+        return out
+
+    a, b = run(True), run(False)
+    assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1]) and a[2] == b[2]
+    assert a[3][-4:] == [1, 1, 1, 1], a[3]
+    assert all(s[1] >= 2 for s in a[4]) and all(s[3] == 0 for s in a[4]), a[4]
+    assert b[3] == [0] * 16
