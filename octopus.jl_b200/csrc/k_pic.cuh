@@ -2024,9 +2024,24 @@ template <class R>
 struct Coord6 {
     R x, px, y, py, z, pz;
 };
+// A global load that does not allocate in L1.
+__device__ __forceinline__ double ld_no_l1(const double *p) {
+    double v;
+    asm("ld.global.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float ld_no_l1(const float *p) {
+    float v;
+    asm("ld.global.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+
 template <class R>
 __device__ __forceinline__ Coord6<R> load_coord(const SoA &S, long long p) {
-    return Coord6<R>{col<R>(S, 0)[p], col<R>(S, 1)[p], col<R>(S, 2)[p], col<R>(S, 3)[p], col<R>(S, 4)[p], col<R>(S, 5)[p]};
+    // read once per kick: no L1 allocation, so L1 keeps the field cells the taps gather from (L2 as usual, where
+    // the next front's deposits find the kicked slices)
+    return Coord6<R>{ld_no_l1(col<R>(S, 0) + p), ld_no_l1(col<R>(S, 1) + p), ld_no_l1(col<R>(S, 2) + p),
+                     ld_no_l1(col<R>(S, 3) + p), ld_no_l1(col<R>(S, 4) + p), ld_no_l1(col<R>(S, 5) + p)};
 }
 
 // HYB: the Gaussian-subtracted hybrid's add-back (FP64 Bassetti-Erskine in both forms) is compiled in, a
