@@ -1987,7 +1987,7 @@ bool replay_key_matches(const octo_ctx *c, const CollideJob &J) {
 
 // Capture the ordinary collide just finished (its schedule tables are resident, its slice tables still in
 // pinned memory) as: guard kernel -> IF(body: the collide's kernels) -> copies of the pair luminosities, the
-// status and the guard's verdict.  Any failure leaves the ordinary path in charge.
+// status and the guard's result.  Any failure leaves the ordinary path in charge.
 void build_replay(octo_ctx *c, const CollideJob &job, const std::vector<long long> &sig) {
     auto &R = c->rp;
     drop_replay(c);

@@ -1,4 +1,4 @@
-"""Exact Bassetti-Erskine field used to judge the solver's field error (the precision form's accuracy
+"""Exact Bassetti-Erskine field used to assess the solver's field error (the precision form's accuracy
 criterion), checked against its round closed form and far-field limit, and the FP64 oracle's PIC field
 checked against it on flat beams (128^2, CIC, second-order derivative: the production solver)."""
 import math
