@@ -1004,9 +1004,18 @@ __device__ __forceinline__ void merge_grid(const Q *sq, long long *g, int cells)
 template <class R>
 using ShQ = typename std::conditional<sizeof(R) == 4, int, long long>::type;
 
-// Field-solve planes of a front.  grid: (blocks per plane, planes in front); each block deposits a
-// grid-stride share of its plane's source slice into a private int64 copy of the nx*ny grid in shared
-// memory, then merges it with global atomics (the consumer, k_conv_rows, clears the grid it reads).
+// A global load that does not allocate in L1.
+__device__ __forceinline__ double ld_no_l1(const double *p) {
+    double v;
+    asm("ld.global.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float ld_no_l1(const float *p) {
+    float v;
+    asm("ld.global.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+
 // Blocks of a k_deposit_node3 row: ceil(n / per_block), at most the grid (per_block <= 0: the whole grid).  A row
 // of a large slice gets more blocks than one of a small slice, so a front's blocks fill whole waves of the SMs.
 __device__ __forceinline__ int row_blocks(long long n, long long per_block) {
@@ -1015,6 +1024,14 @@ __device__ __forceinline__ int row_blocks(long long n, long long per_block) {
     return (int)max(1ll, min((long long)gridDim.x, b));
 }
 
+// A deposit's source coordinate, read once per plane pass: the FP64 form skips L1 allocation (measured faster
+// on the full turn), the FP32 form loads as usual (the hint measured slightly slower on its 64x64 grid).
+__device__ __forceinline__ double ld_src(const double *p) { return ld_no_l1(p); }
+__device__ __forceinline__ float ld_src(const float *p) { return *p; }
+
+// Field-solve planes of a front.  grid: (blocks per plane, planes in front); each block deposits a
+// grid-stride share of its plane's source slice into a private int64 copy of the nx*ny grid in shared
+// memory, then merges it with global atomics (the consumer, k_conv_rows, clears the grid it reads).
 template <class R, int METHOD>
 __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
     using Q = ShQ<R>;
@@ -1062,12 +1079,15 @@ __global__ void __launch_bounds__(1024, 1) k_deposit(Collide C, int plane0) {
         using QA = typename std::remove_pointer<decltype(acc)>::type;
         long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
         R cx = 0, cpx = 0, cy = 0, cpy = 0;
-        if (k < src_n) { const long long p = src_start + k; cx = X[p]; cpx = PX[p]; cy = Y[p]; cpy = PY[p]; }
+        if (k < src_n) {
+            const long long p = src_start + k;
+            cx = ld_src(X + p); cpx = ld_src(PX + p); cy = ld_src(Y + p); cpy = ld_src(PY + p);
+        }
         for (; k < src_n; k += stride) {
             R nx_ = 0, npx = 0, ny_ = 0, npy = 0;
             if (k + stride < src_n) {
                 const long long q = src_start + k + stride;
-                nx_ = X[q]; npx = PX[q]; ny_ = Y[q]; npy = PY[q];
+                nx_ = ld_src(X + q); npx = ld_src(PX + q); ny_ = ld_src(Y + q); npy = ld_src(PY + q);
             }
             const R xd = cx + cpx * s;
             const R yd = cy + cpy * s;
@@ -1141,12 +1161,15 @@ __global__ void __launch_bounds__(1024, 1) k_deposit_node3(Collide C, int plane0
     const long long stride = (long long)nblk * blockDim.x;
     long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     R cx = 0, cpx = 0, cy = 0, cpy = 0;
-    if (k < src_n) { const long long p = src_start + k; cx = X[p]; cpx = PX[p]; cy = Y[p]; cpy = PY[p]; }
+    if (k < src_n) {
+        const long long p = src_start + k;
+        cx = ld_src(X + p); cpx = ld_src(PX + p); cy = ld_src(Y + p); cpy = ld_src(PY + p);
+    }
     for (; k < src_n; k += stride) {
         R nx_ = 0, npx = 0, ny_ = 0, npy = 0;
         if (k + stride < src_n) {
             const long long q = src_start + k + stride;
-            nx_ = X[q]; npx = PX[q]; ny_ = Y[q]; npy = PY[q];
+            nx_ = ld_src(X + q); npx = ld_src(PX + q); ny_ = ld_src(Y + q); npy = ld_src(PY + q);
         }
         const R xl = cx + cpx * sL, yl = cy + cpy * sL;
         const R xr = cx + cpx * sR, yr = cy + cpy * sR;
@@ -1208,12 +1231,15 @@ __global__ void __launch_bounds__(1024, 1) k_lum_deposit(Collide C, int lj0, int
         using QA = typename std::remove_pointer<decltype(acc)>::type;
         long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
         R cx = 0, cpx = 0, cy = 0, cpy = 0;
-        if (k < n) { cx = X[st + k]; cpx = PX[st + k]; cy = Y[st + k]; cpy = PY[st + k]; }
+        if (k < n) {
+            const long long p = st + k;
+            cx = ld_src(X + p); cpx = ld_src(PX + p); cy = ld_src(Y + p); cpy = ld_src(PY + p);
+        }
         for (; k < n; k += stride) {  // next particle prefetched, as in k_deposit
             R nx_ = 0, npx = 0, ny_ = 0, npy = 0;
             if (k + stride < n) {
                 const long long q = st + k + stride;
-                nx_ = X[q]; npx = PX[q]; ny_ = Y[q]; npy = PY[q];
+                nx_ = ld_src(X + q); npx = ld_src(PX + q); ny_ = ld_src(Y + q); npy = ld_src(PY + q);
             }
             const R vx = cx + cpx * s;
             const R vy = cy + cpy * s;
@@ -2024,18 +2050,6 @@ template <class R>
 struct Coord6 {
     R x, px, y, py, z, pz;
 };
-// A global load that does not allocate in L1.
-__device__ __forceinline__ double ld_no_l1(const double *p) {
-    double v;
-    asm("ld.global.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
-    return v;
-}
-__device__ __forceinline__ float ld_no_l1(const float *p) {
-    float v;
-    asm("ld.global.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
-    return v;
-}
-
 template <class R>
 __device__ __forceinline__ Coord6<R> load_coord(const SoA &S, long long p) {
     // read once per kick: no L1 allocation, so L1 keeps the field cells the taps gather from (L2 as usual, where
