@@ -339,7 +339,7 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_fast:
         fast = time_form(solver)
         fast_coarse = time_form(solver_coarse)
-        shape32 = fast["shape"]
+        shape32, shape32c = fast["shape"], fast_coarse["shape"]
     # the oracle's CPU timings of these passes run once, on a single-GPU run
     cpu_side = world == 1 and not args.no_cpu_baseline
     lines = None if args.no_line else time_lines(ob, e0, p0, args, stream, barrier, cpu_side)
@@ -469,6 +469,7 @@ def run_ours(args, rank, world, local_rank):
                           "timed_turns": args.steps, "captures": graph1[0]},
         "launch_shape": {"chosen": list(ctx.AUTOTUNE_SHAPES[shape]),
                          "chosen_fast_form": list(ctx.AUTOTUNE_SHAPES[shape32]) if fast else None,
+                         "chosen_fast_form_coarse": list(ctx.AUTOTUNE_SHAPES[shape32c]) if fast else None,
                          "meaning": "(deposit waves of SMs per wavefront, kick resident-slot multiple), picked by "
                                     "octo_pic_autotune on copies of the beams before the warm-up"},
         "roofline": roof,
