@@ -41,7 +41,7 @@ struct SliceArgs {
 // grid (128, 1, 2); dynamic shared memory rows x 33 doubles.
 constexpr int kLaneFoldThreads = 512, kLaneFoldRows = 640;
 template <class R>
-__global__ void __launch_bounds__(kLaneFoldThreads) k_lane_fold(const SliceArgs<R> A, int square, int rows) {
+__global__ void __launch_bounds__(kLaneFoldThreads, 1) k_lane_fold(const SliceArgs<R> A, int square, int rows) {
     pdl_wait();
     pdl_release();
     const int bm = blockIdx.z;
@@ -59,18 +59,26 @@ __global__ void __launch_bounds__(kLaneFoldThreads) k_lane_fold(const SliceArgs<
     double s = 0.0, lo = INFINITY, hi = -INFINITY;
     for (long long k0 = 0; k0 < iters; k0 += rows) {
         const int nr = (int)min((long long)rows, iters - k0);
-        for (int e = t; e < nr * 32; e += blockDim.x) {
-            const int kk = e >> 5;
-            const long long k = k0 + kk;
-            double v = 0.0;
-            if (k < cnt) {
-                v = (double)z[k * kFoldLanes + first];
-                if (!square) {
-                    lo = jmin(lo, v);
-                    hi = jmax(hi, v);
-                }
+        // eight independent loads in flight per thread before any of them is folded or staged
+        for (int e0 = t; e0 < nr * 32; e0 += 8 * blockDim.x) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int e = e0 + u * (int)blockDim.x;
+                const long long k = k0 + (e >> 5);
+                v[u] = e < nr * 32 && k < cnt ? (double)z[k * kFoldLanes + first] : 0.0;
             }
-            tile[kk * 33 + l] = v;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int e = e0 + u * (int)blockDim.x;
+                if (e >= nr * 32) break;
+                const int kk = e >> 5;
+                if (!square && k0 + kk < cnt) {
+                    lo = jmin(lo, v[u]);
+                    hi = jmax(hi, v[u]);
+                }
+                tile[kk * 33 + l] = v[u];
+            }
         }
         __syncthreads();
         if (t < 32) {
@@ -320,8 +328,18 @@ __global__ void k_slice_count(const SliceArgs<R> A, long long chunk) {
     __syncthreads();
     int zw = info->zero_width;
     long long lo = (long long)blockIdx.x * chunk, hi = min(n, lo + chunk);
-    for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x)
-        atomicAdd(&c[slice_member((double)z[i], b, ns, zw, method)], 1);
+    // eight independent loads in flight per thread before any of them is counted
+    for (long long i0 = lo + threadIdx.x; i0 < hi; i0 += 8LL * blockDim.x) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const long long i = i0 + (long long)u * blockDim.x;
+            v[u] = i < hi ? (double)z[i] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (i0 + (long long)u * blockDim.x < hi) atomicAdd(&c[slice_member(v[u], b, ns, zw, method)], 1);
+    }
     __syncthreads();
     for (int t = threadIdx.x; t < ns; t += blockDim.x) A.counts[bm][(long long)blockIdx.x * ns + t] = c[t];
 }
