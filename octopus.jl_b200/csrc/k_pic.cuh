@@ -2397,18 +2397,29 @@ __global__ void __launch_bounds__(kBoxThreads) k_node_boxes(NodeBoxArgs A) {
             tile[0][j] = X[p]; tile[1][j] = PX[p]; tile[2][j] = Y[p]; tile[3][j] = PY[p]; tile[4][j] = Z[p];
         }
         __syncthreads();
-        for (int j = prow; j < tn; j += kRows) {
-            const R x = tile[0][j], px = tile[1][j], y = tile[2][j], py = tile[3][j], z = tile[4][j];
+        // the rows for a block-uniform count of live reference groups, so groups past it issue nothing
+        auto rows = [&](auto groups) {
+            constexpr int NG = decltype(groups)::value;
+            for (int j = prow; j < tn; j += kRows) {
+                const R x = tile[0][j], px = tile[1][j], y = tile[2][j], py = tile[3][j], z = tile[4][j];
 #pragma unroll
-            for (int g = 0; g < kBoxGroups; ++g) {
-                if (g < ng && live[g]) {
-                    const R s = fld[g] ? R(0.5) * (z - sref[g]) : sref[g];
-                    const R xv = x + s * px, yv = y + s * py;
-                    nan |= (xv != xv) | (yv != yv);
-                    mnx[g] = fmin(mnx[g], xv); mxx[g] = fmax(mxx[g], xv);
-                    mny[g] = fmin(mny[g], yv); mxy[g] = fmax(mxy[g], yv);
+                for (int g = 0; g < NG; ++g) {
+                    if (live[g]) {
+                        const R s = fld[g] ? R(0.5) * (z - sref[g]) : sref[g];
+                        const R xv = x + s * px, yv = y + s * py;
+                        nan |= (xv != xv) | (yv != yv);
+                        mnx[g] = fmin(mnx[g], xv); mxx[g] = fmax(mxx[g], xv);
+                        mny[g] = fmin(mny[g], yv); mxy[g] = fmax(mxy[g], yv);
+                    }
                 }
             }
+        };
+        static_assert(kBoxGroups == 4, "the dispatch below covers 1..4 groups");
+        switch (ng) {
+        case 1: rows(std::integral_constant<int, 1>{}); break;
+        case 2: rows(std::integral_constant<int, 2>{}); break;
+        case 3: rows(std::integral_constant<int, 3>{}); break;
+        default: rows(std::integral_constant<int, 4>{}); break;
         }
     }
     if (__syncthreads_or(nan) && threadIdx.x == 0) atomicOr(A.nanf, 1);
